@@ -1,0 +1,326 @@
+"""Benchmark of the RT-TDDFT propagation hot path on the periodic-bulk workload.
+
+Workload (one bench step): the periodic bulk system -- cubic cell a = 10.26
+bohr, 8 atoms at diamond positions with 4 Gaussian KB projectors each,
+16^3 grid, 64 k-points (4^3 Monkhorst-Pack), 32 complex128 orbitals per k --
+propagated ``--nt`` (default 2000) middlepoint Taylor-4 steps under an
+Asin2cos vector potential (omega = 1.55 eV, peak A/c = 1e-3 au), with J(t)
+computed every step.  Metric: grid-point x orbital Taylor steps per second
+(16^3 x 2048 x nt units per bench step), whole job over all ranks.
+
+* ``value``: orbitals resident in HBM before the timed region (the device
+  loop of sb200_rt_propagate, captured as CUDA graphs).
+* ``e2e``: the same metric through the reference-facing C ABI with host
+  buffers: per bench step the pinned reference-layout orbitals are uploaded
+  (sb200_orbitals_from_ref), propagated, and J(t) plus the final orbitals are
+  read back to the host (sb200_orbitals_to_ref).
+* ``roofline``: the fused stencil kernel (k_hpsi), timed with CUDA events on
+  the library's stream in an instrumented replay right after the timed
+  region; algorithmic bytes 224 B per unit per Taylor step over its 4 launches.
+* ``cpu_baseline``: the CPU oracle (a C++/OpenMP restatement of the
+  reference's Fortran path) on a bounded sample of the same workload.
+
+``--impl reference`` times the reference's CPU path instead (the oracle port:
+the Fortran reference cannot be compiled on these machines).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+UNIT_BYTES_FP64 = 224.0  # algorithmic bytes per grid-point x orbital Taylor step (FP64 form)
+METRIC = "grid-pt*orbital Taylor steps/s"
+UNIT = "grid-pt*orbital*step/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="native", choices=["native", "reference"])
+    ap.add_argument("--nt", type=int, default=2000, help="Taylor time steps per bench step")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--cpu-steps", type=int, default=4, help="Taylor steps in each CPU-baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--small", action="store_true", help="8 k-points instead of 64 (quick check)")
+    return ap.parse_args()
+
+
+def workload(args, rank=0, world=1):
+    from salmon2_b200 import synth
+    nkgrid = 2 if args.small else 4
+    s = synth.periodic_system(a=10.26, num=16, nkgrid=nkgrid, no=32, seed=2, name="periodic_bulk")
+    if world > 1:
+        # weak scaling: rank r owns a shifted copy of the k-mesh (a denser
+        # mesh overall); J(t) is summed over ranks with weights 1/(nk*world)
+        shift = (2.0 * np.pi / 10.26) * (rank / world) / nkgrid
+        s.vec_k[:] = s.vec_k + shift
+        s.wtk[:] = s.wtk / world
+    nt = args.nt
+    dt = 0.08
+    omega = 1.55 / synth.AU_ENERGY_EV
+    Ac = synth.asin2cos(nt, dt, omega=omega, f0=omega * 1e-3, tw=nt * dt)
+    zc = synth.taylor_zc(dt)
+    return s, nt, dt, Ac, zc
+
+
+def config_dict(args, s, nt, world):
+    units = int(np.prod(s.grid.shape)) * s.norb * nt
+    return {
+        "workload": (f"periodic bulk a=10.26 bohr, {s.pp.natom} atoms (diamond), {s.grid.shape[0]}^3 grid, "
+                     f"{s.nk} k-points, {s.no} complex128 orbitals/k, Asin2cos A(t) omega=1.55 eV "
+                     f"peak 1e-3 au, {nt} Taylor-4 steps per bench step, J(t) every step"),
+        "grid": list(s.grid.shape), "k_points": s.nk, "orbitals_per_k": s.no, "atoms": s.pp.natom,
+        "projectors": s.pp.nlma, "taylor_steps_per_bench_step": nt, "units_per_bench_step_per_rank": units,
+        "precision": args.precision, "parallelism": f"k-point shards x{world}",
+        "l2": "inputs larger than L2 (3 orbital blocks of %.0f MB each)" % (units / nt * 16 / 1e6),
+        "seed": s.seed,
+    }
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        try:
+            rows = [r.split(",") for r in open(self.path).read().strip().splitlines()]
+        except Exception:
+            return None
+        rows = [[c.strip() for c in r] for r in rows if len(r) >= 9]
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic():
+    """DRAM bytes per k_hpsi launch from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "k_hpsi_periodic_bulk.md")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.strip().startswith("traffic_bytes_per_launch_full_workload:"):
+            try:
+                return float(line.split(":", 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+def cpu_baseline(args, s, dt, Ac, zc, nsteps):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle import Oracle, lib as olib
+    threads = os.cpu_count() or 1
+    O = Oracle(s, threads=threads)
+    Ac_s = Ac[:, : nsteps + 2].copy(order="F")
+    t0 = time.perf_counter()
+    O.rt_run(s.psi, nsteps, dt, zc, Ac_ext=Ac_s)
+    el = time.perf_counter() - t0
+    units = int(np.prod(s.grid.shape)) * s.norb * nsteps
+    return {"value": units / el, "unit": UNIT, "cores": int(olib().sbo_get_threads()), "kind": "port",
+            "sample": f"{nsteps} Taylor steps of the full workload ({units} units) in {el:.2f} s"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    s, nt, dt, Ac, zc = workload(args)
+    n = max(1, args.cpu_steps)
+    vals = []
+    for i in range(args.warmup + args.steps):
+        cb = cpu_baseline(args, s, dt, Ac, zc, n)
+        if i >= args.warmup:
+            vals.append(cb["value"])
+    v = float(np.mean(vals))
+    units = int(np.prod(s.grid.shape)) * s.norb * n
+    out = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": units / v * 1e3, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)", "impl": "reference",
+           "config": config_dict(args, s, n, 1),
+           "cpu_baseline": {"value": v, "unit": UNIT, "cores": cb["cores"], "kind": "port",
+                            "sample": f"{n} Taylor steps of the full workload per bench step"},
+           "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from salmon2_b200.rt import Context
+
+    s, nt, dt, Ac, zc = workload(args, rank, world)
+    ctx = Context(s, device=local, precision=args.precision)
+    stream = torch.cuda.Stream(device=local)
+    ctx.set_stream(stream)
+    a, b, w = ctx.upload(s.psi), ctx.zeros(), ctx.zeros()
+    units_rank = int(np.prod(s.grid.shape)) * s.norb * nt
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def one_step():
+        res = ctx.rt_propagate(a, b, w, nt, dt, zc, Ac_ext=Ac)
+        if world > 1:  # the exchange step of the path: J(t) summed over k shards
+            j = torch.from_numpy(np.ascontiguousarray(res["curr"])).cuda()
+            dist.all_reduce(j)
+        return res
+
+    for _ in range(args.warmup):
+        one_step()
+    barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(local) as clk:
+        barrier()
+        ev0.record(stream)
+        for _ in range(args.steps):
+            res = one_step()
+        ev1.record(stream)
+        barrier()
+    ms = ev0.elapsed_time(ev1)
+    t = torch.tensor([ms], device=f"cuda:{local}")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = units_rank * world * args.steps / (ms_max / 1e3)
+    launches_per_tstep = 1 + 2 * 4 + 3
+    gpu_launches = launches_per_tstep * nt * args.steps
+
+    # e2e: host (pinned, reference layout) -> device -> propagate -> host
+    host_in = torch.from_numpy(np.ascontiguousarray(s.psi.ravel(order="F").view(np.float64))).pin_memory()
+    host_out = torch.empty_like(host_in).pin_memory()
+    bytes_io = host_in.numel() * 8
+
+    def e2e_step():
+        ctx.upload(host_in, out=a)
+        res = ctx.rt_propagate(a, b, w, nt, dt, zc, Ac_ext=Ac)
+        if world > 1:
+            j = torch.from_numpy(np.ascontiguousarray(res["curr"])).cuda()
+            dist.all_reduce(j)
+        ctx.download(res["psi"], out=host_out)
+        return res
+
+    e2e_step()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ne2e = max(1, min(args.steps, 3))
+    e0.record(stream)
+    for _ in range(ne2e):
+        e2e_step()
+    e1.record(stream)
+    barrier()
+    te = torch.tensor([e0.elapsed_time(e1)], device=f"cuda:{local}")
+    if world > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_value = units_rank * world * ne2e / (float(te.item()) / 1e3)
+
+    # instrumented replay for per-kernel device times (roofline + shares)
+    ctx.set_timing(True)
+    ctx.kernel_times(reset=True)
+    nt_i = min(nt, 200)
+    ctx.rt_propagate(a, b, w, nt_i, dt, zc, Ac_ext=Ac[:, : nt_i + 2])
+    kt = ctx.kernel_times(reset=True)
+    ctx.set_timing(False)
+    peak, peak_kind = measured_peaks()
+    h_ms, h_cnt = kt.get("hpsi", (float("nan"), 1))
+    units_per_launch = int(np.prod(s.grid.shape)) * s.norb
+    bytes_per_launch = UNIT_BYTES_FP64 / 4.0 * units_per_launch
+    avg_ms = h_ms / h_cnt
+    achieved = bytes_per_launch / (avg_ms / 1e3) / 1e9
+    traffic = ncu_traffic()
+    total_ms = sum(v[0] for v in kt.values())
+    shares = {k: round(v[0] / total_ms, 4) for k, v in kt.items()}
+
+    if rank == 0:
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            cpu = cpu_baseline(args, s, dt, Ac, zc, max(1, args.cpu_steps))
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f64+f32",
+            "data": "synthetic (seeded; shapes of the periodic-bulk configuration)",
+            "config": config_dict(args, s, nt, world),
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": bytes_io + Ac.nbytes,
+                    "d2h_bytes_per_step": bytes_io + 3 * nt * 8 + 4 * nt * 8},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
+                         "kernel": "k_hpsi", "avg_launch_ms": avg_ms,
+                         "algorithmic_bytes_per_launch": bytes_per_launch},
+            "kernel_shares": shares,
+            "gpu_launches": gpu_launches,
+            "clocks": clk.summary(),
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(out), flush=True)
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,190 @@
+/*
+ * salmon_b200.h -- C ABI of the B200-native RT-TDDFT propagation library.
+ *
+ * Drop-in boundary for SALMON's hpsi / taylor hot path (SALMON v2.2.0).  The
+ * entry points take plain pointers and sizes only.  Host arrays use the
+ * reference's own layout (Fortran column-major, x fastest, the caller's
+ * is_array:ie_array bounds, complex(8) as interleaved re/im doubles).  Orbital
+ * arrays that the compute entry points read and write are DEVICE arrays in the
+ * library's resident layout ("orbital block"):
+ *
+ *     psi[o][iz][iy][ix]  complex double, o = ispin-1 + nspin*((io-1) + no*(ik-1)),
+ *     ix in 0..nx-1 fastest (interior points only, no halo, no padding),
+ *
+ * sized by sb200_orbital_block_bytes().  sb200_orbitals_from_ref /
+ * sb200_orbitals_to_ref convert between the two layouts.
+ *
+ * Every function returns 0 on success or one of the SB200_ERR_* codes; a
+ * description of the last failure on the calling thread is returned by
+ * sb200_last_error().  A context is used from one host thread at a time; all
+ * work is ordered on the context's stream.  Compute entry points are
+ * asynchronous unless stated otherwise.
+ */
+#ifndef SALMON_B200_H
+#define SALMON_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SB200_OK 0
+#define SB200_ERR_INVALID_ARG 1  /* null pointer, bad enum, inconsistent sizes          */
+#define SB200_ERR_BAD_SHAPE 2    /* grid / orbital / table shape the path cannot take   */
+#define SB200_ERR_UNSUPPORTED 3  /* valid reference input outside this path's scope     */
+#define SB200_ERR_OOM 4          /* device allocation failed                           */
+#define SB200_ERR_CUDA 5         /* CUDA runtime / launch error                        */
+#define SB200_ERR_TIMEOUT 6      /* a bounded device wait expired                       */
+#define SB200_ERR_STATE 7        /* call order: e.g. hpsi before set_grid               */
+
+#define SB200_PREC_FP64 0  /* plain FP64 form                                          */
+#define SB200_PREC_MIXED 1 /* FP32 stencil for Taylor terms n >= 2, FP64 accumulation  */
+
+#define SB200_TRANS_TR 0 /* trans_longi = 'tr': no induced field                      */
+#define SB200_TRANS_LO 1 /* trans_longi = 'lo': A_ind from the current                  */
+
+typedef struct sb200_ctx sb200_ctx;
+
+/* Kernel classes reported by sb200_kernel_times.                              */
+#define SB200_KIND_PREP 0      /* k+A coefficients and projector phases        */
+#define SB200_KIND_PROJECT 1   /* KB projections <beta|psi>                     */
+#define SB200_KIND_HPSI 2      /* fused stencil + V + KB scatter + Taylor term  */
+#define SB200_KIND_OBS 3       /* density / current / dipole partial sums       */
+#define SB200_KIND_MOMENTS 4   /* nonlocal current projections                  */
+#define SB200_KIND_FINAL 5     /* per-step reduction and field update           */
+#define SB200_KIND_COUNT 8
+
+/* ---- context ------------------------------------------------------------ */
+
+/* New context on CUDA device `device`, with its own non-blocking stream.      */
+int sb200_ctx_create(int device, sb200_ctx** out);
+int sb200_ctx_destroy(sb200_ctx* ctx);
+/* Replace the context's stream by a caller-owned cudaStream_t (NULL restores
+ * the context's own stream).                                                   */
+int sb200_ctx_set_stream(sb200_ctx* ctx, void* stream);
+/* Block until all work of the context has finished; reports deferred errors.  */
+int sb200_ctx_sync(sb200_ctx* ctx);
+/* Message of the last failure on this thread ("" if none).                    */
+const char* sb200_last_error(void);
+/* Library version string.                                                     */
+const char* sb200_version(void);
+/* Device-time accounting: with enable = 1, every kernel the context launches
+ * is bracketed by CUDA events on its stream and sb200_rt_propagate runs its
+ * steps without graph capture (one stream synchronisation per step); the
+ * accumulated milliseconds and launch counts per SB200_KIND_* are read with
+ * sb200_kernel_times (reset = 1 clears them).  Off by default.              */
+int sb200_set_timing(sb200_ctx* ctx, int enable);
+int sb200_kernel_times(sb200_ctx* ctx, double ms[SB200_KIND_COUNT], long count[SB200_KIND_COUNT], int reset);
+
+/* ---- set-up (replaces the device-side data SALMON's init builds) -------- */
+
+/* s_rgrid + s_stencil of one r-space domain holding the whole grid.
+ * Replaces: init_grid_parallel (src/common/initialization.f90:508-611) and the
+ * stencil coefficients (src/common/initialization.f90:241-256).
+ *   is, ie, is_array, ie_array : mg%is, mg%ie, mg%is_array, mg%ie_array (3 each)
+ *   idx, idy, idz : mg%idx(is-4:ie+4) etc.; must be the identity map with a
+ *                   4-deep halo (isolated, zero Dirichlet halo) or the modular
+ *                   map of a periodic grid (anything else: SB200_ERR_UNSUPPORTED)
+ *   lg_num        : lg%num (global grid size; selects calc_dip's coordinate shift)
+ *   hgs           : system%Hgs;  hvol : system%Hvol
+ *   coef_lap0, coef_lap(4,3), coef_nab(4,3) : stencil%coef_lap0 / coef_lap / coef_nab */
+int sb200_set_grid(sb200_ctx* ctx, const int is[3], const int ie[3], const int is_array[3],
+                   const int ie_array[3], const int* idx, const int* idy, const int* idz,
+                   const int lg_num[3], const double hgs[3], double hvol, double coef_lap0,
+                   const double coef_lap[12], const double coef_nab[12]);
+
+/* Orbital block: nspin, io = 1..no, ik = 1..nk (info%io_s..io_e, ik_s..ik_e
+ * re-based to 1; im = 1), the k-points system%vec_k(3,nk), occupations
+ * system%rocc(no,nk,nspin) and weights system%wtk(nk) (src/common/structures.f90:126-203). */
+int sb200_set_orbitals(sb200_ctx* ctx, int nspin, int no, int nk, const double* vec_k,
+                       const double* rocc, const double* wtk);
+
+/* V_local(is:ie, nspin) interior values, host pointer (s_scalar%f per spin;
+ * src/common/hamiltonian.f90:813-843 builds it).                               */
+int sb200_set_vlocal(sb200_ctx* ctx, const double* V_local);
+
+/* Kleinman-Bylander projector tables of s_pp_grid (src/common/structures.f90:254-319;
+ * built by init_ps, src/atom/pp/prep_pp.f90:280-525): mps(natom),
+ * jxyz(3,nps,natom) (grid indices in is..ie), rxyz(3,nps,natom),
+ * uv(nps,nlma), ia_tbl(nlma) (1-based), rinv_uvu(nlma).  Host pointers.
+ * natom = 0 / nlma = 0 disables the nonlocal term.                              */
+int sb200_set_pp(sb200_ctx* ctx, int natom, int nps, int nlma, const int* mps, const int* jxyz,
+                 const double* rxyz, const double* uv, const int* ia_tbl, const double* rinv_uvu);
+
+/* system%vec_Ac (A/c) used by sb200_hpsi: recomputes k+A stencil coefficients
+ * and the projector phases (update_kvector_nonlocalpt,
+ * src/common/hamiltonian.f90:847-903).  Isolated grids ignore it.              */
+int sb200_set_vec_Ac(sb200_ctx* ctx, const double vec_Ac[3]);
+
+/* Arithmetic form of sb200_taylor / sb200_rt_propagate (SB200_PREC_*).          */
+int sb200_set_precision(sb200_ctx* ctx, int mode);
+
+/* ---- orbital blocks ------------------------------------------------------ */
+
+/* Bytes of one orbital block in the resident layout (norb*nx*ny*nz*16).       */
+size_t sb200_orbital_block_bytes(const sb200_ctx* ctx);
+/* zwf(is_array:ie_array, nspin, no, nk) in the reference layout (host or
+ * device memory) -> resident device block.  Synchronous with respect to the
+ * source buffer (it may be reused when the call returns).                     */
+int sb200_orbitals_from_ref(sb200_ctx* ctx, const double* zwf_ref, double* psi_dev);
+/* Resident device block -> zwf in the reference layout (host or device);
+ * halo and padding points of zwf are written as zero.  Synchronous.          */
+int sb200_orbitals_to_ref(sb200_ctx* ctx, const double* psi_dev, double* zwf_ref);
+
+/* ---- the hot path --------------------------------------------------------- */
+
+/* htpsi = H tpsi for every orbital of the block: 25-point Laplacian, Bloch
+ * k+A gradient, V_local and the KB nonlocal term.
+ * Replaces: hpsi (src/common/hamiltonian.f90:27-235 orthogonal branch,
+ * :424-435 nonlocal), zstencil_typical_* (src/common/zstencil_core/typical/seq.f90:17-127)
+ * and zpseudo / zpseudo_cuda (src/common/nonlocal_potential.f90:175-390,
+ * src/common/zpseudo.cu:132-191).  tpsi and htpsi are distinct device blocks. */
+int sb200_hpsi(sb200_ctx* ctx, const double* tpsi, double* htpsi);
+
+/* tspsi_out = sum_{n=0}^{n_hamil} zc(n) H^n tspsi_in, zc(0) = 1, with zc the
+ * complex(n_hamil) array rt%zc (interleaved re/im, host pointer).
+ * Replaces: taylor (src/rt/taylor.f90:21-121).  tspsi_in and sshtpsi are
+ * scratch on return (the reference also leaves intermediate H^n psi there).  */
+int sb200_taylor(sb200_ctx* ctx, double* tspsi_in, double* tspsi_out, double* sshtpsi,
+                 const double* zc, int n_hamil);
+
+/* rho(is:ie, nspin) = sum_{k,o} rocc*wtk*|psi|^2 into a host or device array.
+ * Replaces: calc_density (src/common/density_matrix.f90:26-236).  Synchronous. */
+int sb200_calc_density(sb200_ctx* ctx, const double* psi, double* rho);
+
+/* curr(3,nspin) (host) for the current A = vec_Ac; the nonlocal part uses the
+ * projector phases of the last sb200_set_vec_Ac, as the reference's
+ * calc_current reads the zekr_uV of the step.  Periodic grids only.
+ * Replaces: calc_current (src/common/density_matrix.f90:240-463) and
+ * stencil_current_core_gpu (src/common/stencil_current.cu:81-142).  Synchronous. */
+int sb200_calc_current(sb200_ctx* ctx, const double* psi, const double vec_Ac[3], double* curr);
+
+/* rbox(4) of calc_dip (src/rt/dip.f90:114-225) for rho(is:ie,nspin) (host or
+ * device).  Synchronous.                                                       */
+int sb200_calc_dip(sb200_ctx* ctx, const double* rho, double rbox[4]);
+
+/* nt steps of time_evolution_step (src/rt/time_evolution_step.f90:102-312) for
+ * the fixed-potential linear-response path with the middlepoint propagator:
+ * per step A_mid = (Ac_tot(itt)+Ac_tot(itt-1))/2, update_kvector_nonlocalpt,
+ * taylor, calc_current with Ac_tot(itt) and calc_emfields (periodic), calc_dip
+ * (both), all on the device.
+ *   psi_a      : device block holding psi(itt0-1... ) on entry
+ *   psi_b, work: device blocks (scratch)
+ *   *psi_final : set to psi_a or psi_b, whichever holds the result
+ *   zc         : complex(n_hamil), host
+ *   Ac_ext     : (3, 0:nt+1) host, Ac_ext(:,i) at t = i*dt
+ *   trans_longi: SB200_TRANS_TR or SB200_TRANS_LO
+ *   curr_out   : (3, nt) host or NULL; J(itt) summed over spin
+ *   rbox_out   : (4, nt) host or NULL; calc_dip rbox for rho(itt)
+ *   Ac_tot_out : (3, 0:nt+1) host or NULL
+ * The whole loop is issued as CUDA graphs; synchronous on return.            */
+int sb200_rt_propagate(sb200_ctx* ctx, double* psi_a, double* psi_b, double* work, int nt,
+                       double dt, const double* zc, int n_hamil, const double* Ac_ext,
+                       int trans_longi, double* curr_out, double* rbox_out,
+                       double* Ac_tot_out, double** psi_final);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SALMON_B200_H */

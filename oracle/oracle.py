@@ -1,0 +1,216 @@
+"""ctypes binding of the CPU oracle (test infrastructure only).
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline
+leg import this module, and only as the checker or the timed CPU baseline.
+The product library never calls it.  See ``salmon_oracle.h`` for what each
+function restates and for the parity status of the oracle.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libsalmon_oracle.so")
+_SOURCES = ("salmon_oracle.cpp", "salmon_oracle_gs.cpp", "salmon_oracle.h")
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+
+
+class SboSystem(C.Structure):
+    _fields_ = [
+        ("is_", C.c_int * 3), ("ie", C.c_int * 3), ("is_array", C.c_int * 3), ("ie_array", C.c_int * 3),
+        ("idx", _ip), ("idy", _ip), ("idz", _ip),
+        ("lg_num", C.c_int * 3),
+        ("coef_lap0", C.c_double), ("coef_lap", C.c_double * 12), ("coef_nab", C.c_double * 12),
+        ("periodic", C.c_int), ("nspin", C.c_int), ("no", C.c_int), ("nk", C.c_int),
+        ("hgs", C.c_double * 3), ("hvol", C.c_double), ("ngrid", C.c_int),
+        ("vec_k", _dp), ("vec_Ac", C.c_double * 3), ("rocc", _dp), ("wtk", _dp),
+        ("BT", C.c_double * 9), ("V_local", _dp),
+        ("natom", C.c_int), ("nps", C.c_int), ("nlma", C.c_int),
+        ("mps", _ip), ("jxyz", _ip), ("rxyz", _dp), ("uv", _dp), ("ia_tbl", _ip), ("rinv_uvu", _dp),
+        ("zekr", _dp),
+        ("stencil_rgrid_mode", C.c_int),
+    ]
+
+
+def build(force: bool = False) -> str:
+    src_mtime = max(os.path.getmtime(os.path.join(HERE, f)) for f in _SOURCES)
+    if force or not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < src_mtime:
+        subprocess.run(["make", "-s", "-C", HERE], check=True, env=dict(os.environ, ORACLE_CXX="g++"))
+    return LIB_PATH
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        L = C.CDLL(LIB_PATH)
+        for name in ("sbo_zstencil", "sbo_dstencil", "sbo_update_kvector_nonlocalpt", "sbo_zpseudo",
+                     "sbo_dpseudo", "sbo_zprojections", "sbo_hpsi", "sbo_hpsi_real", "sbo_taylor",
+                     "sbo_calc_density", "sbo_calc_current", "sbo_current_parts", "sbo_calc_dip",
+                     "sbo_calc_Ac_ext_t", "sbo_rt_run", "sbo_set_threads", "sbo_get_threads"):
+            getattr(L, name)
+        L.sbo_rt_run.restype = C.c_int
+        L.sbo_get_threads.restype = C.c_int
+        _lib = L
+    return _lib
+
+
+def _p(a, t=_dp):
+    return a.ctypes.data_as(t)
+
+
+class Oracle:
+    """Holds one ``sbo_system`` built from a :class:`salmon2_b200.synth.System`."""
+
+    def __init__(self, system, threads: int | None = None, rgrid_mode: bool | None = None):
+        self.sys = system
+        g, pp = system.grid, system.pp
+        self._keep = []
+        s = SboSystem()
+        for d in range(3):
+            s.is_[d], s.ie[d] = int(g.is_[d]), int(g.ie[d])
+            s.is_array[d], s.ie_array[d] = int(g.is_array[d]), int(g.ie_array[d])
+            s.lg_num[d] = int(g.num[d])
+            s.hgs[d] = float(g.hgs[d])
+        self.idx, self.idy, self.idz = (np.ascontiguousarray(a, dtype=np.int32) for a in (g.idx, g.idy, g.idz))
+        s.idx, s.idy, s.idz = _p(self.idx, _ip), _p(self.idy, _ip), _p(self.idz, _ip)
+        s.coef_lap0 = g.coef_lap0
+        for i, v in enumerate(np.asarray(g.coef_lap).ravel(order="F")):
+            s.coef_lap[i] = v
+        for i, v in enumerate(np.asarray(g.coef_nab).ravel(order="F")):
+            s.coef_nab[i] = v
+        s.periodic = 1 if g.periodic else 0
+        s.nspin, s.no, s.nk = system.nspin, system.no, system.nk
+        s.hvol = g.hvol
+        s.ngrid = system.ngrid
+        self.vec_k = np.asfortranarray(system.vec_k, dtype=np.float64)
+        self.rocc = np.asfortranarray(system.rocc, dtype=np.float64)
+        self.wtk = np.ascontiguousarray(system.wtk, dtype=np.float64)
+        self.V = np.asfortranarray(system.V_local, dtype=np.float64)
+        s.vec_k, s.rocc, s.wtk, s.V_local = _p(self.vec_k), _p(self.rocc), _p(self.wtk), _p(self.V)
+        for i in range(9):
+            s.BT[i] = 1.0 if i in (0, 4, 8) else 0.0
+        s.natom, s.nps, s.nlma = pp.natom, pp.nps, pp.nlma
+        self.mps = np.ascontiguousarray(pp.mps, dtype=np.int32)
+        self.jxyz = np.asfortranarray(pp.jxyz, dtype=np.int32)
+        self.rxyz = np.asfortranarray(pp.rxyz, dtype=np.float64)
+        self.uv = np.asfortranarray(pp.uv, dtype=np.float64)
+        self.ia_tbl = np.ascontiguousarray(pp.ia_tbl, dtype=np.int32)
+        self.rinv = np.ascontiguousarray(pp.rinv_uvu, dtype=np.float64)
+        nk_z = system.nk if g.periodic else 1
+        self.zekr = np.zeros((max(pp.nps, 1), max(pp.nlma, 1), nk_z), dtype=np.complex128, order="F")
+        s.mps, s.jxyz, s.rxyz, s.uv = _p(self.mps, _ip), _p(self.jxyz, _ip), _p(self.rxyz), _p(self.uv)
+        s.ia_tbl, s.rinv_uvu, s.zekr = _p(self.ia_tbl, _ip), _p(self.rinv), _p(self.zekr)
+        if rgrid_mode is None:  # code_optimization.f90:59-63
+            rgrid_mode = int(np.prod(g.shape)) >= 32 ** 3
+        s.stencil_rgrid_mode = 1 if rgrid_mode else 0
+        self.s = s
+        if threads:
+            lib().sbo_set_threads(int(threads))
+        self.set_vec_Ac((0.0, 0.0, 0.0))
+
+    # -- state ------------------------------------------------------------
+    def set_vec_Ac(self, ac):
+        for d in range(3):
+            self.s.vec_Ac[d] = float(ac[d])
+        if self.sys.pp.nlma > 0:
+            lib().sbo_update_kvector_nonlocalpt(C.byref(self.s))
+
+    def set_vec_Ac_local_only(self, ac):
+        """Change system%vec_Ac without refreshing zekr (calc_current's order)."""
+        for d in range(3):
+            self.s.vec_Ac[d] = float(ac[d])
+
+    # -- operators ---------------------------------------------------------
+    def _orb(self, psi):
+        a = np.asfortranarray(psi, dtype=np.complex128)
+        assert a.shape[:3] == self.sys.grid.shape_array
+        return a
+
+    def hpsi(self, psi):
+        a = self._orb(psi)
+        out = np.zeros_like(a, order="F")
+        lib().sbo_hpsi(C.byref(self.s), _p(a), _p(out))
+        return out
+
+    def hpsi_real(self, psi):
+        a = np.asfortranarray(psi, dtype=np.float64)
+        out = np.zeros_like(a, order="F")
+        lib().sbo_hpsi_real(C.byref(self.s), _p(a), _p(out))
+        return out
+
+    def zpseudo(self, psi):
+        """Nonlocal term alone: zpseudo applied to a zero htpsi."""
+        a = self._orb(psi)
+        out = np.zeros_like(a, order="F")
+        lib().sbo_zpseudo(C.byref(self.s), _p(a), _p(out))
+        return out
+
+    def projections(self, psi):
+        a = self._orb(psi)
+        out = np.zeros((self.sys.pp.nlma, self.sys.norb), dtype=np.complex128, order="F")
+        lib().sbo_zprojections(C.byref(self.s), _p(a), _p(out))
+        return out
+
+    def taylor(self, psi, zc):
+        tin = self._orb(psi).copy(order="F")
+        tout = np.zeros_like(tin, order="F")
+        work = np.zeros_like(tin, order="F")
+        zc = np.ascontiguousarray(zc, dtype=np.complex128)
+        lib().sbo_taylor(C.byref(self.s), _p(tin), _p(tout),
+                         _p(work), _p(zc), C.c_int(len(zc)))
+        return tout
+
+    def density(self, psi):
+        a = self._orb(psi)
+        rho = np.zeros(self.sys.grid.shape + (self.sys.nspin,), order="F")
+        lib().sbo_calc_density(C.byref(self.s), _p(a), _p(rho))
+        return rho
+
+    def current(self, psi):
+        a = self._orb(psi)
+        cur = np.zeros((3, self.sys.nspin), order="F")
+        lib().sbo_calc_current(C.byref(self.s), _p(a), _p(cur))
+        return cur
+
+    def current_parts(self, psi):
+        a = self._orb(psi)
+        out = np.zeros((10, self.sys.norb), order="F")
+        lib().sbo_current_parts(C.byref(self.s), _p(a), _p(out))
+        return out
+
+    def dip(self, rho):
+        r = np.asfortranarray(rho, dtype=np.float64)
+        out = np.zeros(4)
+        lib().sbo_calc_dip(C.byref(self.s), _p(r), _p(out))
+        return out
+
+    def rt_run(self, psi0, nt, dt, zc, Ac_ext=None, trans_longi=0):
+        """nt steps of time_evolution_step; returns dict of histories + psi."""
+        a = self._orb(psi0).copy(order="F")
+        b = np.zeros_like(a, order="F")
+        work = np.zeros_like(a, order="F")
+        if Ac_ext is None:
+            Ac_ext = np.zeros((3, nt + 2), order="F")
+        Ac_ext = np.asfortranarray(Ac_ext, dtype=np.float64)
+        Ac_ind = np.zeros_like(Ac_ext, order="F")
+        Ac_tot = Ac_ext.copy(order="F")
+        curr = np.zeros((3, nt), order="F")
+        rbox = np.zeros((4, nt), order="F")
+        rho = np.zeros(self.sys.grid.shape + (self.sys.nspin,), order="F")
+        zc = np.ascontiguousarray(zc, dtype=np.complex128)
+        which = lib().sbo_rt_run(C.byref(self.s), _p(a), _p(b),
+                                 _p(work), C.c_int(nt), C.c_double(dt),
+                                 _p(zc), C.c_int(len(zc)), _p(Ac_ext), _p(Ac_ind),
+                                 _p(Ac_tot), C.c_int(trans_longi), _p(curr), _p(rbox), _p(rho))
+        psi = a if which == 0 else b
+        return dict(psi=psi, curr=curr, rbox=rbox, Ac_tot=Ac_tot, Ac_ind=Ac_ind, rho=rho)

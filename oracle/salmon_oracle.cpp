@@ -1,0 +1,603 @@
+// salmon_oracle.cpp -- CPU oracle (test infrastructure only) for the SALMON
+// RT-TDDFT propagation hot path.  Each function restates one reference routine
+// (SALMON v2.2.0 file:line cited at the function) with the same loop nesting
+// and summation order, on the reference's own array layout.  See
+// salmon_oracle.h for the parity status.
+#include "salmon_oracle.h"
+
+#include <cmath>
+#include <complex>
+#include <cstring>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+typedef std::complex<double> zc_t;
+
+namespace {
+
+constexpr int Nd = 4;
+
+struct Idx {
+  const sbo_system* s;
+  long nxa, nya, nza, vol;
+  long nx, ny, nz;
+  explicit Idx(const sbo_system* s_) : s(s_) {
+    nxa = s->ie_array[0] - s->is_array[0] + 1;
+    nya = s->ie_array[1] - s->is_array[1] + 1;
+    nza = s->ie_array[2] - s->is_array[2] + 1;
+    vol = nxa * nya * nza;
+    nx = s->ie[0] - s->is[0] + 1;
+    ny = s->ie[1] - s->is[1] + 1;
+    nz = s->ie[2] - s->is[2] + 1;
+  }
+  // offset of (ix,iy,iz) inside one orbital block (Fortran bounds)
+  inline long a(int ix, int iy, int iz) const {
+    return (ix - s->is_array[0]) + nxa * ((iy - s->is_array[1]) + nya * (long)(iz - s->is_array[2]));
+  }
+  // offset inside an interior-shaped (is:ie) scalar field
+  inline long r(int ix, int iy, int iz) const {
+    return (ix - s->is[0]) + nx * ((iy - s->is[1]) + ny * (long)(iz - s->is[2]));
+  }
+  inline int X(int j) const { return s->idx[j - (s->is[0] - Nd)]; }
+  inline int Y(int j) const { return s->idy[j - (s->is[1] - Nd)]; }
+  inline int Z(int j) const { return s->idz[j - (s->is[2] - Nd)]; }
+  // orbital block index of (ispin, io, ik), all 1-based
+  inline long orb(int ispin, int io, int ik) const {
+    return (ispin - 1) + (long)s->nspin * ((io - 1) + (long)s->no * (ik - 1));
+  }
+  long norb() const { return (long)s->nspin * s->no * s->nk; }
+};
+
+inline zc_t ld(const double* p, long off) { return zc_t(p[2 * off], p[2 * off + 1]); }
+inline void st(double* p, long off, zc_t v) { p[2 * off] = v.real(); p[2 * off + 1] = v.imag(); }
+
+// Fortran complex*complex is (ac-bd, ad+bc); std::complex operator* on gcc may
+// take the C99 Annex G NaN-recovery path, which only differs for inf/nan.
+inline zc_t cmul(zc_t a, zc_t b) {
+  return zc_t(a.real() * b.real() - a.imag() * b.imag(),
+              a.real() * b.imag() + a.imag() * b.real());
+}
+inline zc_t rmul(double r, zc_t a) { return zc_t(r * a.real(), r * a.imag()); }
+// abs(z)**2 as the reference evaluates it (hypot, then square)
+inline double abs2(zc_t a) { double h = std::hypot(a.real(), a.imag()); return h * h; }
+
+// One orbital of the 25-point complex stencil.
+// zstencil_core/typical/seq.f90:17-127 (and omp.f90:22-164 when rgrid-parallel).
+void zstencil_one(const sbo_system* s, const Idx& I, const double* tpsi, double* htpsi,
+                  const double* V, double lap0, const double* lapt, const double* nabt,
+                  bool omp_grid) {
+  const int zs = s->is[2], ze = s->ie[2], ys = s->is[1], ye = s->ie[1];
+  const int xs = s->is[0], xe = s->ie[0];
+#pragma omp parallel for collapse(2) if (omp_grid)
+  for (int iz = zs; iz <= ze; ++iz)
+    for (int iy = ys; iy <= ye; ++iy)
+      for (int ix = xs; ix <= xe; ++ix) {
+        zc_t t[8];
+        // x: t(1..8) = psi(x+4 .. x+1, x-1 .. x-4)
+        t[0] = ld(tpsi, I.a(I.X(ix + 4), iy, iz));
+        t[1] = ld(tpsi, I.a(I.X(ix + 3), iy, iz));
+        t[2] = ld(tpsi, I.a(I.X(ix + 2), iy, iz));
+        t[3] = ld(tpsi, I.a(I.X(ix + 1), iy, iz));
+        t[4] = ld(tpsi, I.a(I.X(ix - 1), iy, iz));
+        t[5] = ld(tpsi, I.a(I.X(ix - 2), iy, iz));
+        t[6] = ld(tpsi, I.a(I.X(ix - 3), iy, iz));
+        t[7] = ld(tpsi, I.a(I.X(ix - 4), iy, iz));
+        zc_t v = rmul(lapt[0], t[3] + t[4]) + rmul(lapt[1], t[2] + t[5]) +
+                 rmul(lapt[2], t[1] + t[6]) + rmul(lapt[3], t[0] + t[7]);
+        zc_t w = rmul(nabt[0], t[3] - t[4]) + rmul(nabt[1], t[2] - t[5]) +
+                 rmul(nabt[2], t[1] - t[6]) + rmul(nabt[3], t[0] - t[7]);
+        // y: t(1..4) = psi(y+1..y+4), t(5..8) = psi(y-1..y-4)
+        for (int k = 0; k < 4; ++k) {
+          t[k] = ld(tpsi, I.a(ix, I.Y(iy + k + 1), iz));
+          t[k + 4] = ld(tpsi, I.a(ix, I.Y(iy - k - 1), iz));
+        }
+        v = (rmul(lapt[4], t[0] + t[4]) + rmul(lapt[5], t[1] + t[5]) +
+             rmul(lapt[6], t[2] + t[6]) + rmul(lapt[7], t[3] + t[7])) + v;
+        w = (rmul(nabt[4], t[0] - t[4]) + rmul(nabt[5], t[1] - t[5]) +
+             rmul(nabt[6], t[2] - t[6]) + rmul(nabt[7], t[3] - t[7])) + w;
+        for (int k = 0; k < 4; ++k) {
+          t[k] = ld(tpsi, I.a(ix, iy, I.Z(iz + k + 1)));
+          t[k + 4] = ld(tpsi, I.a(ix, iy, I.Z(iz - k - 1)));
+        }
+        v = (rmul(lapt[8], t[0] + t[4]) + rmul(lapt[9], t[1] + t[5]) +
+             rmul(lapt[10], t[2] + t[6]) + rmul(lapt[11], t[3] + t[7])) + v;
+        w = (rmul(nabt[8], t[0] - t[4]) + rmul(nabt[9], t[1] - t[5]) +
+             rmul(nabt[10], t[2] - t[6]) + rmul(nabt[11], t[3] - t[7])) + w;
+        const zc_t c = ld(tpsi, I.a(ix, iy, iz));
+        const double vl = V[I.r(ix, iy, iz)];
+        // V*psi + lap0*psi - 0.5*v - zI*w ;  zI*w = (-w_i, w_r)
+        zc_t h = rmul(vl, c) + rmul(lap0, c) - rmul(0.5, v) - zc_t(-w.imag(), w.real());
+        st(htpsi, I.a(ix, iy, iz), h);
+      }
+}
+
+// One orbital of the real 25-point stencil.  stencil.f90:30-80.
+void dstencil_one(const sbo_system* s, const Idx& I, const double* tpsi, double* htpsi,
+                  const double* V, double lap0, const double* lapt, bool omp_grid) {
+#pragma omp parallel for collapse(2) if (omp_grid)
+  for (int iz = s->is[2]; iz <= s->ie[2]; ++iz)
+    for (int iy = s->is[1]; iy <= s->ie[1]; ++iy)
+      for (int ix = s->is[0]; ix <= s->ie[0]; ++ix) {
+        auto T = [&](int x, int y, int z) { return tpsi[I.a(x, y, z)]; };
+        double v = lapt[0] * (T(I.X(ix + 1), iy, iz) + T(I.X(ix - 1), iy, iz)) +
+                   lapt[1] * (T(I.X(ix + 2), iy, iz) + T(I.X(ix - 2), iy, iz)) +
+                   lapt[2] * (T(I.X(ix + 3), iy, iz) + T(I.X(ix - 3), iy, iz)) +
+                   lapt[3] * (T(I.X(ix + 4), iy, iz) + T(I.X(ix - 4), iy, iz));
+        v = lapt[4] * (T(ix, I.Y(iy + 1), iz) + T(ix, I.Y(iy - 1), iz)) +
+            lapt[5] * (T(ix, I.Y(iy + 2), iz) + T(ix, I.Y(iy - 2), iz)) +
+            lapt[6] * (T(ix, I.Y(iy + 3), iz) + T(ix, I.Y(iy - 3), iz)) +
+            lapt[7] * (T(ix, I.Y(iy + 4), iz) + T(ix, I.Y(iy - 4), iz)) + v;
+        v = lapt[8] * (T(ix, iy, I.Z(iz + 1)) + T(ix, iy, I.Z(iz - 1))) +
+            lapt[9] * (T(ix, iy, I.Z(iz + 2)) + T(ix, iy, I.Z(iz - 2))) +
+            lapt[10] * (T(ix, iy, I.Z(iz + 3)) + T(ix, iy, I.Z(iz - 3))) +
+            lapt[11] * (T(ix, iy, I.Z(iz + 4)) + T(ix, iy, I.Z(iz - 4))) + v;
+        htpsi[I.a(ix, iy, iz)] = (V[I.r(ix, iy, iz)] + lap0) * T(ix, iy, iz) - 0.5 * v;
+      }
+}
+
+inline long jx_off(const sbo_system* s, int c, int j, int ia) {
+  return (c - 1) + 3L * ((j - 1) + (long)s->nps * (ia - 1));
+}
+inline long zekr_off(const sbo_system* s, int j, int ilma, int ik) {
+  return (j - 1) + (long)s->nps * ((ilma - 1) + (long)s->nlma * (ik - 1));
+}
+
+// k+A dependent stencil coefficients. hamiltonian.f90:146-155.
+void kac_coefs(const sbo_system* s, int ik, const double* vac, double* kAc, double& k_lap0,
+               double* k_nabt) {
+  if (s->periodic) {
+    for (int d = 0; d < 3; ++d) kAc[d] = s->vec_k[3 * (ik - 1) + d] + vac[d];
+    k_lap0 = s->coef_lap0 + 0.5 * (kAc[0] * kAc[0] + kAc[1] * kAc[1] + kAc[2] * kAc[2]);
+    for (int d = 0; d < 3; ++d)
+      for (int i = 0; i < 4; ++i) k_nabt[4 * d + i] = kAc[d] * s->coef_nab[4 * d + i];
+  } else {
+    kAc[0] = kAc[1] = kAc[2] = 0.0;
+    k_lap0 = s->coef_lap0;
+    for (int i = 0; i < 12; ++i) k_nabt[i] = 0.0;
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+void sbo_set_threads(int n) {
+#ifdef _OPENMP
+  if (n > 0) omp_set_num_threads(n);
+#else
+  (void)n;
+#endif
+}
+
+int sbo_get_threads(void) {
+#ifdef _OPENMP
+  return omp_get_max_threads();
+#else
+  return 1;
+#endif
+}
+
+void sbo_zstencil(const sbo_system* s, const double* tpsi, double* htpsi, const double* V_local,
+                  double lap0, const double* lapt, const double* nabt) {
+  Idx I(s);
+  zstencil_one(s, I, tpsi, htpsi, V_local, lap0, lapt, nabt, s->stencil_rgrid_mode != 0);
+}
+
+void sbo_dstencil(const sbo_system* s, const double* tpsi, double* htpsi, const double* V_local,
+                  double lap0, const double* lapt) {
+  Idx I(s);
+  dstencil_one(s, I, tpsi, htpsi, V_local, lap0, lapt, s->stencil_rgrid_mode != 0);
+}
+
+// update_kvector_nonlocalpt, hamiltonian.f90:847-903 (periodic);
+// prep_pp.f90:618-619 (isolated: zekr_uV = uV, one k).
+void sbo_update_kvector_nonlocalpt(sbo_system* s) {
+  const int nk = s->periodic ? s->nk : 1;
+#pragma omp parallel for collapse(2)
+  for (int ik = 1; ik <= nk; ++ik)
+    for (int ilma = 1; ilma <= s->nlma; ++ilma) {
+      const int ia = s->ia_tbl[ilma - 1];
+      double kAc[3];
+      if (s->periodic) {
+        for (int d = 0; d < 3; ++d) kAc[d] = s->vec_k[3 * (ik - 1) + d] + s->vec_Ac[d];
+      }
+      for (int j = 1; j <= s->mps[ia - 1]; ++j) {
+        const double uv = s->uv[(j - 1) + (long)s->nps * (ilma - 1)];
+        zc_t z;
+        if (s->periodic) {
+          const double x = s->rxyz[jx_off(s, 1, j, ia)];
+          const double y = s->rxyz[jx_off(s, 2, j, ia)];
+          const double zz = s->rxyz[jx_off(s, 3, j, ia)];
+          const double th = kAc[0] * x + kAc[1] * y + kAc[2] * zz;
+          // ekr = exp(zi*th); zekr = conjg(ekr)*uv
+          z = zc_t(std::cos(th) * uv, -std::sin(th) * uv);
+        } else {
+          z = zc_t(uv, 0.0);
+        }
+        st(s->zekr, zekr_off(s, j, ilma, ik), z);
+      }
+    }
+}
+
+// Projections only: uvpsi(ilma, orb) = rinv_uvu * sum_j conj(zekr) psi(jxyz).
+void sbo_zprojections(const sbo_system* s, const double* tpsi, double* uvpsi) {
+  Idx I(s);
+  const long norb = I.norb();
+#pragma omp parallel for
+  for (long o = 0; o < norb; ++o) {
+    const int ik_eff = s->periodic ? (int)(o / ((long)s->nspin * s->no)) + 1 : 1;
+    const double* psi = tpsi + 2 * I.vol * o;
+    for (int ilma = 1; ilma <= s->nlma; ++ilma) {
+      const int ia = s->ia_tbl[ilma - 1];
+      zc_t u(0.0, 0.0);
+      for (int j = 1; j <= s->mps[ia - 1]; ++j) {
+        const int ix = s->jxyz[jx_off(s, 1, j, ia)];
+        const int iy = s->jxyz[jx_off(s, 2, j, ia)];
+        const int iz = s->jxyz[jx_off(s, 3, j, ia)];
+        const zc_t zk = std::conj(ld(s->zekr, zekr_off(s, j, ilma, ik_eff)));
+        u = u + cmul(zk, ld(psi, I.a(ix, iy, iz)));
+      }
+      u = rmul(s->rinv_uvu[ilma - 1], u);
+      st(uvpsi, (ilma - 1) + (long)s->nlma * o, u);
+    }
+  }
+}
+
+// zpseudo CPU branch, nonlocal_potential.f90:351-382.
+void sbo_zpseudo(const sbo_system* s, const double* tpsi, double* htpsi) {
+  Idx I(s);
+  const long norb = I.norb();
+#pragma omp parallel for
+  for (long o = 0; o < norb; ++o) {
+    const int ik = (int)(o / ((long)s->nspin * s->no)) + 1;
+    const int ik_eff = s->periodic ? ik : 1;
+    const double* psi = tpsi + 2 * I.vol * o;
+    double* hpsi = htpsi + 2 * I.vol * o;
+    for (int ilma = 1; ilma <= s->nlma; ++ilma) {
+      const int ia = s->ia_tbl[ilma - 1];
+      zc_t u(0.0, 0.0);
+      for (int j = 1; j <= s->mps[ia - 1]; ++j) {
+        const int ix = s->jxyz[jx_off(s, 1, j, ia)];
+        const int iy = s->jxyz[jx_off(s, 2, j, ia)];
+        const int iz = s->jxyz[jx_off(s, 3, j, ia)];
+        const zc_t zk = std::conj(ld(s->zekr, zekr_off(s, j, ilma, ik_eff)));
+        u = u + cmul(zk, ld(psi, I.a(ix, iy, iz)));
+      }
+      u = rmul(s->rinv_uvu[ilma - 1], u);
+      for (int j = 1; j <= s->mps[ia - 1]; ++j) {
+        const int ix = s->jxyz[jx_off(s, 1, j, ia)];
+        const int iy = s->jxyz[jx_off(s, 2, j, ia)];
+        const int iz = s->jxyz[jx_off(s, 3, j, ia)];
+        const zc_t wrk = cmul(u, ld(s->zekr, zekr_off(s, j, ilma, ik_eff)));
+        const long off = I.a(ix, iy, iz);
+        st(hpsi, off, ld(hpsi, off) + wrk);
+      }
+    }
+  }
+}
+
+// dpseudo, nonlocal_potential.f90:26-171 (single r-space domain branch).
+void sbo_dpseudo(const sbo_system* s, const double* tpsi, double* htpsi) {
+  Idx I(s);
+  const long norb = I.norb();
+#pragma omp parallel for
+  for (long o = 0; o < norb; ++o) {
+    const double* psi = tpsi + I.vol * o;
+    double* hpsi = htpsi + I.vol * o;
+    for (int ilma = 1; ilma <= s->nlma; ++ilma) {
+      const int ia = s->ia_tbl[ilma - 1];
+      double u = 0.0;
+      for (int j = 1; j <= s->mps[ia - 1]; ++j) {
+        const int ix = s->jxyz[jx_off(s, 1, j, ia)];
+        const int iy = s->jxyz[jx_off(s, 2, j, ia)];
+        const int iz = s->jxyz[jx_off(s, 3, j, ia)];
+        u = u + s->uv[(j - 1) + (long)s->nps * (ilma - 1)] * psi[I.a(ix, iy, iz)];
+      }
+      u = u * s->rinv_uvu[ilma - 1];
+      for (int j = 1; j <= s->mps[ia - 1]; ++j) {
+        const int ix = s->jxyz[jx_off(s, 1, j, ia)];
+        const int iy = s->jxyz[jx_off(s, 2, j, ia)];
+        const int iz = s->jxyz[jx_off(s, 3, j, ia)];
+        hpsi[I.a(ix, iy, iz)] += u * s->uv[(j - 1) + (long)s->nps * (ilma - 1)];
+      }
+    }
+  }
+}
+
+// hpsi, complex, orthogonal lattice: hamiltonian.f90:139-235 then zpseudo :424-435.
+void sbo_hpsi(const sbo_system* s, const double* tpsi, double* htpsi) {
+  Idx I(s);
+  const bool grid_mode = s->stencil_rgrid_mode != 0;
+  const long nxy = I.nx * I.ny * I.nz;
+  if (grid_mode) {
+    for (int ik = 1; ik <= s->nk; ++ik) {
+      double kAc[3], k_lap0, k_nabt[12];
+      kac_coefs(s, ik, s->vec_Ac, kAc, k_lap0, k_nabt);
+      for (int io = 1; io <= s->no; ++io)
+        for (int is = 1; is <= s->nspin; ++is) {
+          const long o = I.orb(is, io, ik);
+          zstencil_one(s, I, tpsi + 2 * I.vol * o, htpsi + 2 * I.vol * o,
+                       s->V_local + nxy * (is - 1), k_lap0, s->coef_lap, k_nabt, true);
+        }
+    }
+  } else {
+#pragma omp parallel for collapse(3)
+    for (int ik = 1; ik <= s->nk; ++ik)
+      for (int io = 1; io <= s->no; ++io)
+        for (int is = 1; is <= s->nspin; ++is) {
+          double kAc[3], k_lap0, k_nabt[12];
+          kac_coefs(s, ik, s->vec_Ac, kAc, k_lap0, k_nabt);
+          const long o = I.orb(is, io, ik);
+          zstencil_one(s, I, tpsi + 2 * I.vol * o, htpsi + 2 * I.vol * o,
+                       s->V_local + nxy * (is - 1), k_lap0, s->coef_lap, k_nabt, false);
+        }
+  }
+  if (s->nlma > 0) sbo_zpseudo(s, tpsi, htpsi);
+}
+
+// hpsi, real orbitals: hamiltonian.f90:88-125 (dstencil + dpseudo).
+void sbo_hpsi_real(const sbo_system* s, const double* tpsi, double* htpsi) {
+  Idx I(s);
+  const long nxy = I.nx * I.ny * I.nz;
+  const long norb = I.norb();
+  if (s->stencil_rgrid_mode) {
+    for (long o = 0; o < norb; ++o) {
+      const int is = (int)(o % s->nspin) + 1;
+      dstencil_one(s, I, tpsi + I.vol * o, htpsi + I.vol * o, s->V_local + nxy * (is - 1),
+                   s->coef_lap0, s->coef_lap, true);
+    }
+  } else {
+#pragma omp parallel for
+    for (long o = 0; o < norb; ++o) {
+      const int is = (int)(o % s->nspin) + 1;
+      dstencil_one(s, I, tpsi + I.vol * o, htpsi + I.vol * o, s->V_local + nxy * (is - 1),
+                   s->coef_lap0, s->coef_lap, false);
+    }
+  }
+  if (s->nlma > 0) sbo_dpseudo(s, tpsi, htpsi);
+}
+
+// taylor, taylor.f90:21-121 (tspsi_in is reused as scratch for even terms).
+void sbo_taylor(const sbo_system* s, double* tspsi_in, double* tspsi_out, double* sshtpsi,
+                const double* zc, int n_hamil) {
+  Idx I(s);
+  const long norb = I.norb();
+  for (int nn = 1; nn <= n_hamil; ++nn) {
+    const zc_t c(zc[2 * (nn - 1)], zc[2 * (nn - 1) + 1]);
+    const bool odd = (nn % 2) == 1;
+    if (odd) sbo_hpsi(s, tspsi_in, sshtpsi);
+    else sbo_hpsi(s, sshtpsi, tspsi_in);
+    const double* h = odd ? sshtpsi : tspsi_in;
+#pragma omp parallel for collapse(3)
+    for (long o = 0; o < norb; ++o)
+      for (int iz = s->is[2]; iz <= s->ie[2]; ++iz)
+        for (int iy = s->is[1]; iy <= s->ie[1]; ++iy)
+          for (int ix = s->is[0]; ix <= s->ie[0]; ++ix) {
+            const long off = I.vol * o + I.a(ix, iy, iz);
+            if (nn == 1)
+              st(tspsi_out, off, ld(tspsi_in, off) + cmul(c, ld(h, off)));
+            else
+              st(tspsi_out, off, ld(tspsi_out, off) + cmul(c, ld(h, off)));
+          }
+  }
+}
+
+// calc_density, density_matrix.f90:150-232 (fixed summation order over k, o).
+void sbo_calc_density(const sbo_system* s, const double* psi, double* rho) {
+  Idx I(s);
+  const long n = I.nx * I.ny * I.nz;
+  for (int is = 1; is <= s->nspin; ++is) {
+    double* r = rho + n * (is - 1);
+#pragma omp parallel for collapse(2)
+    for (int iz = s->is[2]; iz <= s->ie[2]; ++iz)
+      for (int iy = s->is[1]; iy <= s->ie[1]; ++iy)
+        for (int ix = s->is[0]; ix <= s->ie[0]; ++ix) {
+          double acc = 0.0;
+          for (int ik = 1; ik <= s->nk; ++ik)
+            for (int io = 1; io <= s->no; ++io) {
+              const long o = I.orb(is, io, ik);
+              const double w2 = abs2(ld(psi, I.vol * o + I.a(ix, iy, iz)));
+              acc = acc + w2 * s->rocc[(io - 1) + (long)s->no * ((ik - 1) + (long)s->nk * (is - 1))] *
+                              s->wtk[ik - 1];
+            }
+          r[I.r(ix, iy, iz)] = acc;
+        }
+  }
+}
+
+// Per-orbital current pieces: stencil_current (density_matrix.f90:465-530) and
+// calc_current_nonlocal (:532-591).
+void sbo_current_parts(const sbo_system* s, const double* psi_all, double* out) {
+  Idx I(s);
+  const long norb = I.norb();
+#pragma omp parallel for
+  for (long o = 0; o < norb; ++o) {
+    const int is = (int)(o % s->nspin) + 1;
+    const int io = (int)((o / s->nspin) % s->no) + 1;
+    const int ik = (int)(o / ((long)s->nspin * s->no)) + 1;
+    const double* psi = psi_all + 2 * I.vol * o;
+    const double* nab = s->coef_nab;
+    double rtmp = 0.0;
+    zc_t xt(0, 0), yt(0, 0), zt(0, 0);
+    for (int iz = s->is[2]; iz <= s->ie[2]; ++iz)
+      for (int iy = s->is[1]; iy <= s->ie[1]; ++iy) {
+        for (int ix = s->is[0]; ix <= s->ie[0]; ++ix) rtmp = rtmp + abs2(ld(psi, I.a(ix, iy, iz)));
+        for (int ix = s->is[0]; ix <= s->ie[0]; ++ix) {
+          const zc_t cp = std::conj(ld(psi, I.a(ix, iy, iz)));
+          xt = xt + cmul(rmul(nab[0], cp), ld(psi, I.a(I.X(ix + 1), iy, iz))) +
+               cmul(rmul(nab[1], cp), ld(psi, I.a(I.X(ix + 2), iy, iz))) +
+               cmul(rmul(nab[2], cp), ld(psi, I.a(I.X(ix + 3), iy, iz))) +
+               cmul(rmul(nab[3], cp), ld(psi, I.a(I.X(ix + 4), iy, iz)));
+        }
+        for (int ix = s->is[0]; ix <= s->ie[0]; ++ix) {
+          const zc_t cp = std::conj(ld(psi, I.a(ix, iy, iz)));
+          yt = yt + cmul(rmul(nab[4], cp), ld(psi, I.a(ix, I.Y(iy + 1), iz))) +
+               cmul(rmul(nab[5], cp), ld(psi, I.a(ix, I.Y(iy + 2), iz))) +
+               cmul(rmul(nab[6], cp), ld(psi, I.a(ix, I.Y(iy + 3), iz))) +
+               cmul(rmul(nab[7], cp), ld(psi, I.a(ix, I.Y(iy + 4), iz)));
+        }
+        for (int ix = s->is[0]; ix <= s->ie[0]; ++ix) {
+          const zc_t cp = std::conj(ld(psi, I.a(ix, iy, iz)));
+          zt = zt + cmul(rmul(nab[8], cp), ld(psi, I.a(ix, iy, I.Z(iz + 1)))) +
+               cmul(rmul(nab[9], cp), ld(psi, I.a(ix, iy, I.Z(iz + 2)))) +
+               cmul(rmul(nab[10], cp), ld(psi, I.a(ix, iy, I.Z(iz + 3)))) +
+               cmul(rmul(nab[11], cp), ld(psi, I.a(ix, iy, I.Z(iz + 4))));
+        }
+      }
+    double kAc[3];
+    for (int d = 0; d < 3; ++d) kAc[d] = s->vec_k[3 * (ik - 1) + d] + s->vec_Ac[d];
+    double j1[3], j2[3], j2b[3], jw[3] = {0, 0, 0};
+    for (int d = 0; d < 3; ++d) j1[d] = kAc[d] * rtmp;
+    j2[0] = (xt * 2.0).imag();
+    j2[1] = (yt * 2.0).imag();
+    j2[2] = (zt * 2.0).imag();
+    for (int d = 0; d < 3; ++d)
+      j2b[d] = s->BT[d] * j2[0] + s->BT[d + 3] * j2[1] + s->BT[d + 6] * j2[2];
+    // calc_current_nonlocal
+    for (int ilma = 1; ilma <= s->nlma; ++ilma) {
+      const int ia = s->ia_tbl[ilma - 1];
+      zc_t u(0, 0), ur[3] = {zc_t(0, 0), zc_t(0, 0), zc_t(0, 0)};
+      for (int j = 1; j <= s->mps[ia - 1]; ++j) {
+        const double r[3] = {s->rxyz[jx_off(s, 1, j, ia)], s->rxyz[jx_off(s, 2, j, ia)],
+                             s->rxyz[jx_off(s, 3, j, ia)]};
+        const int ix = s->jxyz[jx_off(s, 1, j, ia)];
+        const int iy = s->jxyz[jx_off(s, 2, j, ia)];
+        const int iz = s->jxyz[jx_off(s, 3, j, ia)];
+        const zc_t zk = std::conj(ld(s->zekr, zekr_off(s, j, ilma, ik)));
+        const zc_t p = ld(psi, I.a(ix, iy, iz));
+        u = u + cmul(zk, p);
+        for (int d = 0; d < 3; ++d) ur[d] = ur[d] + cmul(rmul(r[d], zk), p);
+      }
+      u = rmul(s->rinv_uvu[ilma - 1], u);
+      for (int d = 0; d < 3; ++d) jw[d] = jw[d] + cmul(std::conj(ur[d]), u).imag();
+    }
+    for (int d = 0; d < 3; ++d) jw[d] = jw[d] * 2.0;
+    const double wgt = s->rocc[(io - 1) + (long)s->no * ((ik - 1) + (long)s->nk * (is - 1))] *
+                       s->wtk[ik - 1];
+    double* op = out + 10 * o;
+    op[0] = rtmp;
+    op[1] = j2[0];
+    op[2] = j2[1];
+    op[3] = j2[2];
+    for (int d = 0; d < 3; ++d) op[4 + d] = jw[d];
+    for (int d = 0; d < 3; ++d) op[7 + d] = (j1[d] + j2b[d] + jw[d]) * wgt;
+  }
+}
+
+// calc_current, density_matrix.f90:240-463 (single domain, CPU branch).
+void sbo_calc_current(const sbo_system* s, const double* psi, double* curr) {
+  Idx I(s);
+  const long norb = I.norb();
+  std::vector<double> parts(10 * norb);
+  sbo_current_parts(s, psi, parts.data());
+  for (int is = 1; is <= s->nspin; ++is) {
+    double w4[3] = {0, 0, 0};
+    for (int ik = 1; ik <= s->nk; ++ik)
+      for (int io = 1; io <= s->no; ++io) {
+        const long o = I.orb(is, io, ik);
+        for (int d = 0; d < 3; ++d) w4[d] = w4[d] + parts[10 * o + 7 + d];
+      }
+    for (int d = 0; d < 3; ++d) curr[3 * (is - 1) + d] = w4[d] / (double)s->ngrid;
+  }
+}
+
+// calc_dip, dip.f90:114-225.
+void sbo_calc_dip(const sbo_system* s, const double* rho, double* rbox) {
+  Idx I(s);
+  const long n = I.nx * I.ny * I.nz;
+  for (int d = 0; d < 3; ++d) {
+    const double shift = (s->lg_num[d] % 2 == 1) ? 0.0 : 0.5;
+    double acc = 0.0;
+    for (int is = 1; is <= s->nspin; ++is)
+      for (int iz = s->is[2]; iz <= s->ie[2]; ++iz)
+        for (int iy = s->is[1]; iy <= s->ie[1]; ++iy)
+          for (int ix = s->is[0]; ix <= s->ie[0]; ++ix) {
+            const int c = d == 0 ? ix : (d == 1 ? iy : iz);
+            acc = acc + ((double)c - shift) * rho[n * (is - 1) + I.r(ix, iy, iz)];
+          }
+    rbox[d] = acc;
+  }
+  double acc = 0.0;
+  for (int is = 1; is <= s->nspin; ++is)
+    for (long p = 0; p < n; ++p) acc = acc + rho[n * (is - 1) + p];
+  rbox[3] = acc;
+}
+
+// calc_Ac_ext_t, em_field.f90:86-306 (impulse, Acos2, Asin2cos).
+void sbo_calc_Ac_ext_t(int shape, double t0, double delta_t, int is, int ie, const double* epdir,
+                       double f0, double omega, double tw, double phi_cep, double t1_start,
+                       double e_impulse, double* Ac) {
+  const double pi = 3.141592653589793238462643383279502884;
+  for (int i = is; i <= ie; ++i) {
+    double* a = Ac + 3L * (i - is);
+    a[0] = a[1] = a[2] = 0.0;
+    const double t = t0 + i * delta_t;
+    if (shape == 0) {
+      if (0.0 <= t)
+        for (int d = 0; d < 3; ++d) a[d] = epdir[d] * e_impulse;
+    } else if (shape == 1) {  // Asin2cos
+      const double tt = t;
+      if (tt < tw) {
+        const double sn = std::sin(pi * tt / tw);
+        for (int d = 0; d < 3; ++d)
+          a[d] = -epdir[d] * f0 / omega * (sn * sn) * std::cos(omega * tt + phi_cep * 2.0 * pi);
+      }
+    } else if (shape == 2) {  // Acos2 with real polarisation
+      const double tt = t - 0.5 * tw - t1_start;
+      if (std::fabs(tt) < 0.5 * tw) {
+        const double cs = std::cos(pi * tt / tw);
+        // aimag(epdir * exp(i(omega tt + 2 pi phi)))
+        const double ph = std::sin(omega * tt + phi_cep * 2.0 * pi);
+        for (int d = 0; d < 3; ++d) a[d] = -f0 / omega * (cs * cs) * (epdir[d] * ph);
+      }
+    }
+  }
+}
+
+// time loop body, time_evolution_step.f90:102-312, linear response
+// (yn_fix_func='y' path: V_local fixed), middlepoint propagator.
+int sbo_rt_run(sbo_system* s, double* psi_a, double* psi_b, double* work, int nt, double dt,
+               const double* zc, int n_hamil, const double* Ac_ext, double* Ac_ind,
+               double* Ac_tot, int trans_longi, double* curr, double* rbox, double* rho_work) {
+  const double pi = 3.141592653589793238462643383279502884;
+  double* in = psi_a;
+  double* out = psi_b;
+  int which = 1;
+  for (int itt = 1; itt <= nt; ++itt) {
+    if (s->periodic) {
+      for (int d = 0; d < 3; ++d)
+        s->vec_Ac[d] = 0.5 * (Ac_tot[3 * itt + d] + Ac_tot[3 * (itt - 1) + d]);
+      if (s->nlma > 0) sbo_update_kvector_nonlocalpt(s);
+    }
+    sbo_taylor(s, in, out, work, zc, n_hamil);
+    sbo_calc_density(s, out, rho_work);
+    if (s->periodic) {
+      for (int d = 0; d < 3; ++d) s->vec_Ac[d] = Ac_tot[3 * itt + d];
+      double c[6] = {0, 0, 0, 0, 0, 0};
+      sbo_calc_current(s, out, c);
+      double ctot[3];
+      for (int d = 0; d < 3; ++d) ctot[d] = s->nspin == 2 ? c[d] + c[3 + d] : c[d];
+      for (int d = 0; d < 3; ++d) curr[3 * (itt - 1) + d] = ctot[d];
+      // calc_emfields, em_field.f90:24-70
+      for (int d = 0; d < 3; ++d) {
+        if (trans_longi == 1)
+          Ac_ind[3 * (itt + 1) + d] = 2.0 * Ac_ind[3 * itt + d] - Ac_ind[3 * (itt - 1) + d] -
+                                      4.0 * pi * ctot[d] * dt * dt;
+        else
+          Ac_ind[3 * (itt + 1) + d] = 0.0;
+        Ac_tot[3 * (itt + 1) + d] = Ac_ext[3 * (itt + 1) + d] + Ac_ind[3 * (itt + 1) + d];
+      }
+    }
+    sbo_calc_dip(s, rho_work, rbox + 4 * (itt - 1));
+    double* t = in;
+    in = out;
+    out = t;
+    which = 1 - which;
+  }
+  // after the last swap "in" holds the newest orbitals
+  return (in == psi_a) ? 0 : 1;
+}
+
+}  // extern "C"

@@ -1,0 +1,95 @@
+"""ctypes loader for ``libsalmon_b200.so`` (the sm_100a CUDA library).
+
+The library is built in-tree (``make -C salmon2_b200/csrc``).  There is no CPU
+fallback: if the shared object is missing or cannot be loaded, every entry
+point raises :class:`SB200Error`.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libsalmon_b200.so")
+HEADER = os.path.join(os.path.dirname(HERE), "include", "salmon_b200.h")
+
+SB200_OK = 0
+ERROR_NAMES = {1: "INVALID_ARG", 2: "BAD_SHAPE", 3: "UNSUPPORTED", 4: "OOM", 5: "CUDA", 6: "TIMEOUT", 7: "STATE"}
+PREC_FP64, PREC_MIXED = 0, 1
+TRANS_TR, TRANS_LO = 0, 1
+KIND_NAMES = ["prep", "project", "hpsi", "observables", "moments", "finalize", "k6", "k7"]
+
+
+class SB200Error(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"salmon_b200 error {code} ({ERROR_NAMES.get(code, '?')}): {msg}")
+        self.code = code
+
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+_vp = C.c_void_p
+
+# name -> (restype, argtypes); mirrors include/salmon_b200.h
+SIGNATURES = {
+    "sb200_ctx_create": (C.c_int, [C.c_int, C.POINTER(C.c_void_p)]),
+    "sb200_ctx_destroy": (C.c_int, [_vp]),
+    "sb200_ctx_set_stream": (C.c_int, [_vp, _vp]),
+    "sb200_ctx_sync": (C.c_int, [_vp]),
+    "sb200_last_error": (C.c_char_p, []),
+    "sb200_version": (C.c_char_p, []),
+    "sb200_set_timing": (C.c_int, [_vp, C.c_int]),
+    "sb200_kernel_times": (C.c_int, [_vp, _dp, C.POINTER(C.c_long), C.c_int]),
+    "sb200_set_grid": (C.c_int, [_vp, _ip, _ip, _ip, _ip, _ip, _ip, _ip, _ip, _dp, C.c_double, C.c_double, _dp, _dp]),
+    "sb200_set_orbitals": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, _dp, _dp, _dp]),
+    "sb200_set_vlocal": (C.c_int, [_vp, _dp]),
+    "sb200_set_pp": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, _ip, _ip, _dp, _dp, _ip, _dp]),
+    "sb200_set_vec_Ac": (C.c_int, [_vp, _dp]),
+    "sb200_set_precision": (C.c_int, [_vp, C.c_int]),
+    "sb200_orbital_block_bytes": (C.c_size_t, [_vp]),
+    "sb200_orbitals_from_ref": (C.c_int, [_vp, _vp, _vp]),
+    "sb200_orbitals_to_ref": (C.c_int, [_vp, _vp, _vp]),
+    "sb200_hpsi": (C.c_int, [_vp, _vp, _vp]),
+    "sb200_taylor": (C.c_int, [_vp, _vp, _vp, _vp, _dp, C.c_int]),
+    "sb200_calc_density": (C.c_int, [_vp, _vp, _vp]),
+    "sb200_calc_current": (C.c_int, [_vp, _vp, _dp, _dp]),
+    "sb200_calc_dip": (C.c_int, [_vp, _vp, _dp]),
+    "sb200_rt_propagate": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int, C.c_double, _dp, C.c_int, _dp, C.c_int, _dp,
+                                     _dp, _dp, C.POINTER(C.c_void_p)]),
+}
+
+
+def build(force: bool = False) -> str:
+    """Compile the CUDA library for sm_100a with nvcc (no GPU needed)."""
+    cmd = ["make", "-s", "-C", os.path.join(HERE, "csrc")]
+    if force:
+        subprocess.run(cmd + ["clean"], check=True)
+    subprocess.run(cmd + ["-j4"], check=True)
+    return LIB_PATH
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise SB200Error(5, f"{LIB_PATH} is missing: build it with `make -C salmon2_b200/csrc`")
+        try:
+            L = C.CDLL(LIB_PATH)
+        except OSError as e:  # no CUDA driver / runtime
+            raise SB200Error(5, f"cannot load {LIB_PATH}: {e}") from e
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(rc: int):
+    if rc != SB200_OK:
+        raise SB200Error(rc, lib().sb200_last_error().decode())
+    return rc

@@ -1,0 +1,171 @@
+// sb200_internal.cuh -- shared declarations of the B200 RT-TDDFT library.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/salmon_b200.h"
+
+namespace sb200 {
+
+constexpr int ND = 4;            // stencil half-width (Nd of the reference)
+constexpr int KC = 16;           // doubles per k-point coefficient record
+constexpr int OBS_NQ = 7;        // per-orbital local observables (see k_observables)
+constexpr int OBS_THREADS = 256;
+constexpr int OBS_PTS_PER_THREAD = 8;
+
+// Per-k coefficient record written by k_prep_k (hamiltonian.f90:146-155):
+//   [0..2] kAc, [3] k_lap0, [4..15] k_nabt(4,3) column-major.
+
+struct GridInfo {
+  bool set = false;
+  int nx = 0, ny = 0, nz = 0;
+  long npts = 0;
+  int periodic = 0;
+  int is[3], ie[3], is_array[3], ie_array[3], lg_num[3];
+  double hgs[3], hvol = 0, coef_lap0 = 0, coef_lap[12], coef_nab[12];
+  long vol_array() const {
+    return (long)(ie_array[0] - is_array[0] + 1) * (ie_array[1] - is_array[1] + 1) *
+           (ie_array[2] - is_array[2] + 1);
+  }
+};
+
+struct OrbInfo {
+  bool set = false;
+  int nspin = 0, no = 0, nk = 0, norb = 0;
+  std::vector<double> vec_k;   // (3,nk)
+  std::vector<double> weight;  // per orbital rocc*wtk, orbital order
+};
+
+// Kleinman-Bylander tables, re-indexed for the device.
+struct PPInfo {
+  int natom = 0, nps = 0, nlma = 0, totpts = 0, nprojmax = 0;
+  int nvi = 0, nent = 0;
+  // per atom
+  int* d_atom_start = nullptr;  // first flat sphere point of the atom
+  int* d_mps = nullptr;
+  int* d_lma_start = nullptr;   // first (0-based) ilma of the atom
+  int* d_nproj = nullptr;       // projectors of the atom
+  // per flat sphere point
+  int* d_pt_lin = nullptr;      // linear resident-layout point index
+  double* d_pt_r = nullptr;     // rxyz, 3 per point
+  // per projector
+  double* d_uv = nullptr;       // uv(j, ilma) at [ilma*nps + j]
+  double* d_rinv = nullptr;     // rinv_uvu
+  // scatter inverse map: point -> entries (ilma, flat point, uv), ilma ascending
+  int* d_map = nullptr;         // [npts] -> vi or -1
+  int* d_vi_start = nullptr;    // [nvi+1]
+  int* d_ent_lma = nullptr;
+  int* d_ent_pt = nullptr;
+  double* d_ent_uv = nullptr;
+  // projector phases exp(i kAc.r): [nk_phase][totpts]
+  double2* d_phase = nullptr;
+  int nk_phase = 0;
+};
+
+struct RTBuffers {
+  int cap_nt = -1;
+  double* d_Ac_ext = nullptr;   // (3, 0:nt+1)
+  double* d_Ac_ind = nullptr;
+  double* d_Ac_tot = nullptr;
+  double* d_curr = nullptr;     // (3, nt)
+  double* d_rbox = nullptr;     // (4, nt)
+  int* d_step = nullptr;        // current itt
+  double2* d_zc = nullptr;      // n_hamil coefficients
+};
+
+}  // namespace sb200
+
+struct sb200_ctx {
+  int device = 0;
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;
+  int precision = SB200_PREC_FP64;
+  sb200::GridInfo g;
+  sb200::OrbInfo orb;
+  sb200::PPInfo pp;
+  sb200::RTBuffers rt;
+  double vec_Ac[3] = {0, 0, 0};
+  // device tables
+  double* d_vloc = nullptr;     // [nspin][npts]
+  float* d_vloc32 = nullptr;    // FP32 copy for the mixed form
+  double* d_vec_k = nullptr;    // [nk][3]
+  double* d_weight = nullptr;   // [norb]
+  double* d_kcoef = nullptr;    // [nk][KC] for the hpsi coefficients in use
+  double* d_kcoef_cur = nullptr;// [nk][KC] for calc_current's A
+  // scratch
+  double2* d_proj = nullptr;    // [norb][nlma] projections of the current input
+  double* d_jw = nullptr;       // [norb][natom][3] nonlocal current pieces
+  double* d_obs = nullptr;      // [norb][obs_blocks][OBS_NQ] partial sums
+  double* d_result = nullptr;   // small result area (8 doubles)
+  int obs_blocks = 0;
+  void* d_stage = nullptr;      // relayout staging
+  size_t stage_bytes = 0;
+  bool vloc_set = false;
+  // optional per-kernel-class device timing (sb200_set_timing)
+  bool timing = false;
+  std::vector<cudaEvent_t> ev;  // pairs (start, stop)
+  std::vector<int> ev_kind;
+  int ev_used = 0;
+  double kt_ms[SB200_KIND_COUNT] = {0};
+  long kt_count[SB200_KIND_COUNT] = {0};
+};
+
+namespace sb200 {
+
+// error reporting
+int set_error(int code, const std::string& msg);
+int cuda_error(cudaError_t e, const char* where);
+#define SB_CUDA(call)                                                  \
+  do {                                                                 \
+    cudaError_t _e = (call);                                           \
+    if (_e != cudaSuccess) return ::sb200::cuda_error(_e, #call);      \
+  } while (0)
+#define SB_LAUNCH_CHECK(what)                                          \
+  do {                                                                 \
+    cudaError_t _e = cudaGetLastError();                               \
+    if (_e != cudaSuccess) return ::sb200::cuda_error(_e, what);       \
+  } while (0)
+
+template <typename T>
+int dalloc(T** p, size_t count) {
+  *p = nullptr;
+  if (count == 0) return SB200_OK;
+  cudaError_t e = cudaMalloc((void**)p, count * sizeof(T));
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    *p = nullptr;
+    return set_error(SB200_ERR_OOM, std::string("cudaMalloc failed: ") + cudaGetErrorString(e));
+  }
+  return SB200_OK;
+}
+template <typename T>
+void dfree(T*& p) {
+  if (p) cudaFree((void*)p);
+  p = nullptr;
+}
+
+// ---- kernel launchers (sb200_kernels.cu) ----
+struct HpsiLaunch {
+  const double2* in;
+  double2* hout;        // may be null when mode == 3
+  double2* out;         // Taylor accumulator (modes 1..3)
+  double2 zc;
+  int mode;             // 0: h; 1: h, out = in + zc h; 2: h, out += zc h; 3: out += zc h;
+                        // 4: out = in + zc h (no h store)
+};
+int launch_prep_k(sb200_ctx* c, const double* d_A, int a_mode, int itt_from_device,
+                  double* d_kcoef, bool phases);
+int launch_project(sb200_ctx* c, const double2* in, double2* proj);
+int launch_hpsi(sb200_ctx* c, const HpsiLaunch& L);
+int launch_observables(sb200_ctx* c, const double2* psi);
+int launch_project_moments(sb200_ctx* c, const double2* psi);
+int launch_finalize(sb200_ctx* c, int itt_host, int nt, int trans_longi, double dt, int spin_filter);
+int launch_density(sb200_ctx* c, const double2* psi, double* rho);
+int launch_dip(sb200_ctx* c, const double* rho, double* d_out4);
+int launch_relayout(sb200_ctx* c, const void* src, void* dst, int norb_chunk, bool to_ref);
+
+}  // namespace sb200

@@ -1,0 +1,748 @@
+// sb200_kernels.cu -- device kernels of the FP64 hpsi / Taylor / observables
+// path on the resident orbital layout psi[o][z][y][x] (complex double).
+#include <cuda_runtime.h>
+
+#include "sb200_internal.cuh"
+
+namespace sb200 {
+namespace {
+
+constexpr double PI = 3.141592653589793238462643383279502884;
+
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double2 cscal(double r, double2 a) { return make_double2(r * a.x, r * a.y); }
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+// neighbour coordinate along an axis of length n; periodic wrap or Dirichlet.
+__device__ __forceinline__ int nbr(int c, int s, int n, int periodic, bool& ok) {
+  int q = c + s;
+  if (periodic) {
+    q = q < 0 ? q + n : (q >= n ? q - n : q);
+    ok = true;
+  } else {
+    ok = (q >= 0) && (q < n);
+  }
+  return q;
+}
+
+__device__ __forceinline__ double2 ldz(const double2* __restrict__ p, long i, bool ok) {
+  return ok ? __ldg(p + i) : make_double2(0.0, 0.0);
+}
+
+// ---------------------------------------------------------------------------
+// k-point coefficients and projector phases (hamiltonian.f90:146-155,847-903)
+// ---------------------------------------------------------------------------
+struct PrepArgs {
+  int nk, totpts, periodic, a_mode;
+  int itt;                      // < 0: read *step
+  double coef_lap0, coef_nab[12];
+  const double* vec_k;          // [nk][3]
+  const double* A;              // a_mode 0: A[3]; else Ac_tot(3, 0:nt+1)
+  const int* step;
+  const double* pt_r;           // [totpts][3]
+  double* kcoef;                // [nk][KC]
+  double2* phase;               // [nk][totpts] or null
+};
+
+__global__ void k_prep(PrepArgs a) {
+  const int per = a.totpts > 0 ? a.totpts : 1;
+  const long items = (long)a.nk * per;
+  int itt = a.itt;
+  if (a.a_mode != 0 && itt < 0) itt = *a.step;
+  double A[3];
+  for (int d = 0; d < 3; ++d) {
+    if (a.a_mode == 0) A[d] = a.A[d];
+    else if (a.a_mode == 1) A[d] = 0.5 * (a.A[3 * itt + d] + a.A[3 * (itt - 1) + d]);
+    else A[d] = a.A[3 * itt + d];
+  }
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < items; i += (long)gridDim.x * blockDim.x) {
+    const int k = (int)(i / per);
+    const int j = (int)(i % per);
+    double kAc[3];
+    for (int d = 0; d < 3; ++d) kAc[d] = a.periodic ? a.vec_k[3 * k + d] + A[d] : 0.0;
+    if (j == 0) {
+      double* kc = a.kcoef + (long)KC * k;
+      kc[0] = kAc[0];
+      kc[1] = kAc[1];
+      kc[2] = kAc[2];
+      kc[3] = a.periodic ? a.coef_lap0 + 0.5 * (kAc[0] * kAc[0] + kAc[1] * kAc[1] + kAc[2] * kAc[2])
+                         : a.coef_lap0;
+      for (int q = 0; q < 12; ++q) kc[4 + q] = a.periodic ? kAc[q / 4] * a.coef_nab[q] : 0.0;
+    }
+    if (a.phase != nullptr && a.totpts > 0) {
+      const double* r = a.pt_r + 3L * j;
+      const double th = kAc[0] * r[0] + kAc[1] * r[1] + kAc[2] * r[2];
+      double s, c;
+      sincos(th, &s, &c);
+      a.phase[(long)k * a.totpts + j] = make_double2(c, s);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// KB projections P(o, ilma) = rinv_uvu * sum_j conj(zekr_uV(j,ilma,k)) psi(jxyz)
+// (nonlocal_potential.f90:358-367).  One warp per (orbital, atom); the
+// projectors of the atom are processed NP at a time so psi is gathered once
+// per pass; deterministic butterfly reduction over the warp.
+// ---------------------------------------------------------------------------
+struct ProjArgs {
+  long npts;
+  int natom, nlma, nps, totpts, nspin_no, phase_per_k;
+  const int *atom_start, *mps, *lma_start, *nproj, *pt_lin;
+  const double *uv, *rinv, *pt_r;
+  const double2* phase;
+};
+
+template <int NP>
+__global__ void __launch_bounds__(128) k_project(const double2* __restrict__ in, double2* __restrict__ proj,
+                                                 ProjArgs a) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int atom = blockIdx.x * 4 + warp;
+  if (atom >= a.natom) return;
+  const int o = blockIdx.y;
+  const int ik = o / a.nspin_no;
+  const double2* psi = in + (long)o * a.npts;
+  const int start = a.atom_start[atom], m = a.mps[atom];
+  const int lma0 = a.lma_start[atom], np = a.nproj[atom];
+  const double2* ph = a.phase + (a.phase_per_k ? (long)ik * a.totpts : 0L) + start;
+  for (int q0 = 0; q0 < np; q0 += NP) {
+    double2 acc[NP];
+#pragma unroll
+    for (int q = 0; q < NP; ++q) acc[q] = make_double2(0.0, 0.0);
+    for (int j = lane; j < m; j += 32) {
+      const double2 v = __ldg(psi + a.pt_lin[start + j]);
+      const double2 e = __ldg(ph + j);
+#pragma unroll
+      for (int q = 0; q < NP; ++q) {
+        if (q0 + q < np) {
+          const double uv = __ldg(a.uv + (long)(lma0 + q0 + q) * a.nps + j);
+          const double2 zk = make_double2(e.x * uv, e.y * uv);  // conj(zekr_uV)
+          acc[q] = cadd(acc[q], cmul(zk, v));
+        }
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < NP; ++q) {
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) {
+        acc[q].x += __shfl_xor_sync(0xffffffffu, acc[q].x, off);
+        acc[q].y += __shfl_xor_sync(0xffffffffu, acc[q].y, off);
+      }
+    }
+    if (lane == 0) {
+#pragma unroll
+      for (int q = 0; q < NP; ++q)
+        if (q0 + q < np) {
+          const int lma = lma0 + q0 + q;
+          proj[(long)o * a.nlma + lma] = cscal(a.rinv[lma], acc[q]);
+        }
+    }
+  }
+}
+
+// Nonlocal current pieces per (orbital, atom): sum over the atom's projectors
+// of Im(conj(<r_d zekr|psi>) * rinv <zekr|psi>)  (density_matrix.f90:532-591).
+template <int NP>
+__global__ void __launch_bounds__(128) k_project_moments(const double2* __restrict__ in, double* __restrict__ jw,
+                                                         ProjArgs a) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int atom = blockIdx.x * 4 + warp;
+  if (atom >= a.natom) return;
+  const int o = blockIdx.y;
+  const int ik = o / a.nspin_no;
+  const double2* psi = in + (long)o * a.npts;
+  const int start = a.atom_start[atom], m = a.mps[atom];
+  const int lma0 = a.lma_start[atom], np = a.nproj[atom];
+  const double2* ph = a.phase + (a.phase_per_k ? (long)ik * a.totpts : 0L) + start;
+  double jx = 0.0, jy = 0.0, jz = 0.0;
+  for (int q0 = 0; q0 < np; q0 += NP) {
+    double2 u[NP], ur[NP][3];
+#pragma unroll
+    for (int q = 0; q < NP; ++q) {
+      u[q] = make_double2(0.0, 0.0);
+      ur[q][0] = ur[q][1] = ur[q][2] = make_double2(0.0, 0.0);
+    }
+    for (int j = lane; j < m; j += 32) {
+      const double2 v = __ldg(psi + a.pt_lin[start + j]);
+      const double2 e = __ldg(ph + j);
+      const double* r = a.pt_r + 3L * (start + j);
+      const double r0 = r[0], r1 = r[1], r2 = r[2];
+#pragma unroll
+      for (int q = 0; q < NP; ++q) {
+        if (q0 + q < np) {
+          const double uv = __ldg(a.uv + (long)(lma0 + q0 + q) * a.nps + j);
+          const double2 zk = make_double2(e.x * uv, e.y * uv);
+          const double2 t = cmul(zk, v);
+          u[q] = cadd(u[q], t);
+          ur[q][0] = cadd(ur[q][0], cmul(cscal(r0, zk), v));
+          ur[q][1] = cadd(ur[q][1], cmul(cscal(r1, zk), v));
+          ur[q][2] = cadd(ur[q][2], cmul(cscal(r2, zk), v));
+        }
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < NP; ++q) {
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) {
+        u[q].x += __shfl_xor_sync(0xffffffffu, u[q].x, off);
+        u[q].y += __shfl_xor_sync(0xffffffffu, u[q].y, off);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          ur[q][d].x += __shfl_xor_sync(0xffffffffu, ur[q][d].x, off);
+          ur[q][d].y += __shfl_xor_sync(0xffffffffu, ur[q][d].y, off);
+        }
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < NP; ++q) {
+      if (q0 + q < np) {
+        const double2 us = cscal(a.rinv[lma0 + q0 + q], u[q]);
+        // Im(conj(ur) * us)
+        jx += ur[q][0].x * us.y - ur[q][0].y * us.x;
+        jy += ur[q][1].x * us.y - ur[q][1].y * us.x;
+        jz += ur[q][2].x * us.y - ur[q][2].y * us.x;
+      }
+    }
+  }
+  if (lane == 0) {
+    double* out = jw + 3L * ((long)o * a.natom + atom);
+    out[0] = jx;
+    out[1] = jy;
+    out[2] = jz;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// hpsi: 25-point Laplacian + Bloch gradient + V_local (zstencil_typical_seq,
+// seq.f90:65-122) + KB scatter through the inverse map (one owner thread per
+// point, ilma ascending as in nonlocal_potential.f90:368-375), with the Taylor
+// accumulation of taylor.f90:47-117 fused as an epilogue.
+// ---------------------------------------------------------------------------
+struct HArgs {
+  int nx, ny, nz, periodic, nspin, nspin_no, nlma, totpts, phase_per_k;
+  long npts;
+  double lapt[12];
+  const double* kcoef;
+  const double* vloc;
+  const int *map, *vi_start, *ent_lma, *ent_pt;
+  const double* ent_uv;
+  const double2* phase;
+  const double2* proj;
+  double2 zc;
+};
+
+template <int MODE>
+__global__ void __launch_bounds__(256) k_hpsi(const double2* __restrict__ in, double2* __restrict__ hout,
+                                              double2* __restrict__ acc, HArgs a) {
+  const long p = blockIdx.x * 256L + threadIdx.x;
+  if (p >= a.npts) return;
+  const int o = blockIdx.y;
+  const int x = (int)(p % a.nx);
+  const int y = (int)((p / a.nx) % a.ny);
+  const int z = (int)(p / ((long)a.nx * a.ny));
+  const double2* src = in + (long)o * a.npts;
+  const int ik = o / a.nspin_no;
+  const int ispin = o % a.nspin;
+  const double* kc = a.kcoef + (long)KC * ik;
+  const long sy = a.nx, sz = (long)a.nx * a.ny;
+
+  double2 v = make_double2(0.0, 0.0), w = make_double2(0.0, 0.0);
+  {  // x
+    double2 vx = make_double2(0.0, 0.0), wx = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int s = 1; s <= ND; ++s) {
+      bool okp, okm;
+      const int xp = nbr(x, s, a.nx, a.periodic, okp);
+      const int xm = nbr(x, -s, a.nx, a.periodic, okm);
+      const double2 tp = ldz(src, p - x + xp, okp);
+      const double2 tm = ldz(src, p - x + xm, okm);
+      vx = cadd(vx, cscal(a.lapt[s - 1], cadd(tp, tm)));
+      wx = cadd(wx, cscal(kc[4 + s - 1], csub(tp, tm)));
+    }
+    v = vx;
+    w = wx;
+  }
+  {  // y
+    double2 vy = make_double2(0.0, 0.0), wy = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int s = 1; s <= ND; ++s) {
+      bool okp, okm;
+      const int yp = nbr(y, s, a.ny, a.periodic, okp);
+      const int ym = nbr(y, -s, a.ny, a.periodic, okm);
+      const double2 tp = ldz(src, p + (long)(yp - y) * sy, okp);
+      const double2 tm = ldz(src, p + (long)(ym - y) * sy, okm);
+      vy = cadd(vy, cscal(a.lapt[4 + s - 1], cadd(tp, tm)));
+      wy = cadd(wy, cscal(kc[8 + s - 1], csub(tp, tm)));
+    }
+    v = cadd(vy, v);
+    w = cadd(wy, w);
+  }
+  {  // z
+    double2 vz = make_double2(0.0, 0.0), wz = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int s = 1; s <= ND; ++s) {
+      bool okp, okm;
+      const int zp = nbr(z, s, a.nz, a.periodic, okp);
+      const int zm = nbr(z, -s, a.nz, a.periodic, okm);
+      const double2 tp = ldz(src, p + (long)(zp - z) * sz, okp);
+      const double2 tm = ldz(src, p + (long)(zm - z) * sz, okm);
+      vz = cadd(vz, cscal(a.lapt[8 + s - 1], cadd(tp, tm)));
+      wz = cadd(wz, cscal(kc[12 + s - 1], csub(tp, tm)));
+    }
+    v = cadd(vz, v);
+    w = cadd(wz, w);
+  }
+  const double2 c = __ldg(src + p);
+  const double vl = __ldg(a.vloc + (long)ispin * a.npts + p);
+  const double lap0 = kc[3];
+  double2 h;
+  h.x = vl * c.x + lap0 * c.x - 0.5 * v.x + w.y;
+  h.y = vl * c.y + lap0 * c.y - 0.5 * v.y - w.x;
+
+  if (a.nlma > 0) {
+    const int vi = __ldg(a.map + p);
+    if (vi >= 0) {
+      const int e1 = __ldg(a.vi_start + vi + 1);
+      const double2* pj = a.proj + (long)o * a.nlma;
+      const double2* ph = a.phase + (a.phase_per_k ? (long)ik * a.totpts : 0L);
+      for (int e = __ldg(a.vi_start + vi); e < e1; ++e) {
+        const double uv = __ldg(a.ent_uv + e);
+        const double2 phs = __ldg(ph + __ldg(a.ent_pt + e));
+        const double2 zk = make_double2(phs.x * uv, -phs.y * uv);  // zekr_uV
+        h = cadd(h, cmul(pj[__ldg(a.ent_lma + e)], zk));
+      }
+    }
+  }
+  const long gi = (long)o * a.npts + p;
+  if (MODE <= 2) hout[gi] = h;
+  if (MODE == 1 || MODE == 4) acc[gi] = cadd(c, cmul(a.zc, h));
+  if (MODE == 2 || MODE == 3) acc[gi] = cadd(acc[gi], cmul(a.zc, h));
+}
+
+// ---------------------------------------------------------------------------
+// Local observables per orbital (stencil_current, density_matrix.f90:465-530;
+// calc_dip moments, dip.f90:114-225): [sum |psi|^2, Im-sums x/y/z of
+// conj(psi) * sum_s nab(s,d) psi(+s), sum (i_d - shift_d) |psi|^2 (d=x,y,z)].
+// Deterministic: fixed per-thread order, fixed tree over the block.
+// ---------------------------------------------------------------------------
+struct ObsArgs {
+  int nx, ny, nz, periodic, nblk;
+  long npts;
+  double nab[12];
+  double off[3];   // is_d - shift_d
+};
+
+__global__ void __launch_bounds__(OBS_THREADS) k_observables(const double2* __restrict__ in, double* __restrict__ part,
+                                                             ObsArgs a) {
+  __shared__ double red[OBS_NQ][OBS_THREADS];
+  const int o = blockIdx.y;
+  const double2* src = in + (long)o * a.npts;
+  double q[OBS_NQ];
+#pragma unroll
+  for (int i = 0; i < OBS_NQ; ++i) q[i] = 0.0;
+  const long base = (long)blockIdx.x * OBS_THREADS * OBS_PTS_PER_THREAD;
+  for (int it = 0; it < OBS_PTS_PER_THREAD; ++it) {
+    const long p = base + (long)it * OBS_THREADS + threadIdx.x;
+    if (p >= a.npts) break;
+    const int x = (int)(p % a.nx);
+    const int y = (int)((p / a.nx) % a.ny);
+    const int z = (int)(p / ((long)a.nx * a.ny));
+    const double2 c = __ldg(src + p);
+    const double r2 = c.x * c.x + c.y * c.y;
+    q[0] += r2;
+    double ix = 0.0, iy = 0.0, iz = 0.0;
+#pragma unroll
+    for (int s = 1; s <= ND; ++s) {
+      bool ok;
+      const int xp = nbr(x, s, a.nx, a.periodic, ok);
+      const double2 tx = ldz(src, p - x + xp, ok);
+      ix += a.nab[s - 1] * (c.x * tx.y - c.y * tx.x);
+      const int yp = nbr(y, s, a.ny, a.periodic, ok);
+      const double2 ty = ldz(src, p + (long)(yp - y) * a.nx, ok);
+      iy += a.nab[4 + s - 1] * (c.x * ty.y - c.y * ty.x);
+      const int zp = nbr(z, s, a.nz, a.periodic, ok);
+      const double2 tz = ldz(src, p + (long)(zp - z) * a.nx * a.ny, ok);
+      iz += a.nab[8 + s - 1] * (c.x * tz.y - c.y * tz.x);
+    }
+    q[1] += ix;
+    q[2] += iy;
+    q[3] += iz;
+    q[4] += ((double)x + a.off[0]) * r2;
+    q[5] += ((double)y + a.off[1]) * r2;
+    q[6] += ((double)z + a.off[2]) * r2;
+  }
+#pragma unroll
+  for (int i = 0; i < OBS_NQ; ++i) red[i][threadIdx.x] = q[i];
+  __syncthreads();
+  for (int s = OBS_THREADS / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) {
+#pragma unroll
+      for (int i = 0; i < OBS_NQ; ++i) red[i][threadIdx.x] += red[i][threadIdx.x + s];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x < OBS_NQ)
+    part[((long)o * a.nblk + blockIdx.x) * OBS_NQ + threadIdx.x] = red[threadIdx.x][0];
+}
+
+// ---------------------------------------------------------------------------
+// Final per-step reduction in one block: current J (calc_current), calc_dip
+// rbox, calc_emfields; advances the device step counter.
+// ---------------------------------------------------------------------------
+struct FinArgs {
+  int norb, nspin, nspin_no, nblk, natom, periodic, itt, trans_longi, advance, spin_filter;
+  double ngrid_inv, dt;
+  const double* part;
+  const double* jw;        // [norb][natom][3] or null
+  const double* weight;
+  const double* vec_k;
+  const double* Ac_cur;    // a_mode: itt-indexed Ac_tot (history) or direct A[3] when itt_direct
+  int A_direct;
+  double* Ac_ind;
+  double* Ac_tot;
+  const double* Ac_ext;
+  double* curr_hist;       // (3, nt) or null
+  double* rbox_hist;       // (4, nt) or null
+  double* result;          // [8] direct results (J3, rbox4) or null
+  int* step;
+};
+
+__global__ void __launch_bounds__(256) k_finalize(FinArgs a) {
+  __shared__ double red[7][256];
+  int itt = a.itt;
+  if (itt < 0) itt = *a.step;
+  double A[3] = {0.0, 0.0, 0.0};
+  if (a.periodic) {
+    for (int d = 0; d < 3; ++d) A[d] = a.A_direct ? a.Ac_cur[d] : a.Ac_cur[3 * itt + d];
+  }
+  double s[7] = {0, 0, 0, 0, 0, 0, 0};
+  for (int o = threadIdx.x; o < a.norb; o += blockDim.x) {
+    if (a.spin_filter >= 0 && (o % a.nspin) != a.spin_filter) continue;
+    double q[OBS_NQ] = {0, 0, 0, 0, 0, 0, 0};
+    for (int b = 0; b < a.nblk; ++b)
+      for (int i = 0; i < OBS_NQ; ++i) q[i] += a.part[((long)o * a.nblk + b) * OBS_NQ + i];
+    const double w = a.weight[o];
+    if (a.periodic) {
+      const int ik = o / a.nspin_no;
+      double jw[3] = {0.0, 0.0, 0.0};
+      if (a.jw != nullptr)
+        for (int at = 0; at < a.natom; ++at)
+          for (int d = 0; d < 3; ++d) jw[d] += a.jw[3L * ((long)o * a.natom + at) + d];
+      for (int d = 0; d < 3; ++d) {
+        const double kAc = a.vec_k[3 * ik + d] + A[d];
+        s[d] += (kAc * q[0] + 2.0 * q[1 + d] + 2.0 * jw[d]) * w;
+      }
+    }
+    for (int d = 0; d < 3; ++d) s[3 + d] += q[4 + d] * w;
+    s[6] += q[0] * w;
+  }
+  for (int i = 0; i < 7; ++i) red[i][threadIdx.x] = s[i];
+  __syncthreads();
+  for (int st = 128; st > 0; st >>= 1) {
+    if (threadIdx.x < st)
+      for (int i = 0; i < 7; ++i) red[i][threadIdx.x] += red[i][threadIdx.x + st];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    double J[3], rb[4];
+    for (int d = 0; d < 3; ++d) J[d] = red[d][0] * a.ngrid_inv;
+    for (int d = 0; d < 3; ++d) rb[d] = red[3 + d][0];
+    rb[3] = red[6][0];
+    if (a.result) {
+      for (int d = 0; d < 3; ++d) a.result[d] = J[d];
+      for (int d = 0; d < 4; ++d) a.result[3 + d] = rb[d];
+    }
+    if (a.curr_hist)
+      for (int d = 0; d < 3; ++d) a.curr_hist[3L * (itt - 1) + d] = J[d];
+    if (a.rbox_hist)
+      for (int d = 0; d < 4; ++d) a.rbox_hist[4L * (itt - 1) + d] = rb[d];
+    if (a.periodic && a.Ac_tot) {  // calc_emfields, em_field.f90:47-67
+      for (int d = 0; d < 3; ++d) {
+        double ind;
+        if (a.trans_longi == SB200_TRANS_LO)
+          ind = 2.0 * a.Ac_ind[3 * itt + d] - a.Ac_ind[3 * (itt - 1) + d] - 4.0 * PI * J[d] * a.dt * a.dt;
+        else
+          ind = 0.0;
+        a.Ac_ind[3 * (itt + 1) + d] = ind;
+        a.Ac_tot[3 * (itt + 1) + d] = a.Ac_ext[3 * (itt + 1) + d] + ind;
+      }
+    }
+    if (a.advance) *a.step = itt + 1;
+  }
+}
+
+// rho(p, ispin) = sum_{ik, io} w |psi|^2 (density_matrix.f90:150-232)
+__global__ void k_density(const double2* __restrict__ in, double* __restrict__ rho, long npts, int nspin,
+                          int no, int nk, const double* __restrict__ weight) {
+  const long p = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (p >= npts) return;
+  for (int is = 0; is < nspin; ++is) {
+    double acc = 0.0;
+    for (int ik = 0; ik < nk; ++ik)
+      for (int io = 0; io < no; ++io) {
+        const long o = is + (long)nspin * (io + (long)no * ik);
+        const double2 c = __ldg(in + o * npts + p);
+        acc += (c.x * c.x + c.y * c.y) * weight[o];
+      }
+    rho[(long)is * npts + p] = acc;
+  }
+}
+
+// calc_dip partial sums over a rho field (dip.f90:114-225).
+__global__ void __launch_bounds__(256) k_dip_part(const double* __restrict__ rho, double* __restrict__ part,
+                                                  long npts, int nspin, int nx, int ny, double o0, double o1,
+                                                  double o2) {
+  __shared__ double red[4][256];
+  double q[4] = {0, 0, 0, 0};
+  for (long i = blockIdx.x * 256L + threadIdx.x; i < npts * nspin; i += (long)gridDim.x * 256) {
+    const long p = i % npts;
+    const int x = (int)(p % nx), y = (int)((p / nx) % ny), z = (int)(p / ((long)nx * ny));
+    const double r = rho[i];
+    q[0] += ((double)x + o0) * r;
+    q[1] += ((double)y + o1) * r;
+    q[2] += ((double)z + o2) * r;
+    q[3] += r;
+  }
+  for (int i = 0; i < 4; ++i) red[i][threadIdx.x] = q[i];
+  __syncthreads();
+  for (int st = 128; st > 0; st >>= 1) {
+    if (threadIdx.x < st)
+      for (int i = 0; i < 4; ++i) red[i][threadIdx.x] += red[i][threadIdx.x + st];
+    __syncthreads();
+  }
+  if (threadIdx.x < 4) part[blockIdx.x * 4 + threadIdx.x] = red[threadIdx.x][0];
+}
+
+__global__ void k_dip_final(const double* __restrict__ part, int nblk, double* __restrict__ out) {
+  if (threadIdx.x < 4) {
+    double acc = 0.0;
+    for (int b = 0; b < nblk; ++b) acc += part[b * 4 + threadIdx.x];
+    out[threadIdx.x] = acc;
+  }
+}
+
+// reference layout <-> resident layout for a chunk of orbitals
+__global__ void k_relayout(const double2* __restrict__ src, double2* __restrict__ dst, int nx, int ny, int nz,
+                           int nxa, int nya, long vola, int ox, int oy, int oz, int norb, int to_ref) {
+  const long npts = (long)nx * ny * nz;
+  const long total = npts * norb;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+    const long o = i / npts, p = i % npts;
+    const int x = (int)(p % nx), y = (int)((p / nx) % ny), z = (int)(p / ((long)nx * ny));
+    const long r = o * vola + (x + ox) + (long)nxa * ((y + oy) + (long)nya * (z + oz));
+    if (to_ref) dst[r] = src[i];
+    else dst[i] = src[r];
+  }
+}
+
+int grid_for(long items, int threads) {
+  long b = (items + threads - 1) / threads;
+  if (b > 148L * 64) b = 148L * 64;
+  if (b < 1) b = 1;
+  return (int)b;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+int launch_prep_k(sb200_ctx* c, const double* d_A, int a_mode, int itt, double* d_kcoef, bool phases) {
+  PrepArgs a;
+  a.nk = c->orb.nk;
+  a.totpts = c->pp.totpts;
+  a.periodic = c->g.periodic;
+  a.a_mode = a_mode;
+  a.itt = itt;
+  a.coef_lap0 = c->g.coef_lap0;
+  for (int i = 0; i < 12; ++i) a.coef_nab[i] = c->g.coef_nab[i];
+  a.vec_k = c->d_vec_k;
+  a.A = d_A;
+  a.step = c->rt.d_step;
+  a.pt_r = c->pp.d_pt_r;
+  a.kcoef = d_kcoef;
+  a.phase = (phases && c->g.periodic && c->pp.totpts > 0) ? c->pp.d_phase : nullptr;
+  const long items = (long)a.nk * (a.totpts > 0 ? a.totpts : 1);
+  k_prep<<<grid_for(items, 256), 256, 0, c->stream>>>(a);
+  SB_LAUNCH_CHECK("k_prep");
+  return SB200_OK;
+}
+
+static ProjArgs proj_args(sb200_ctx* c) {
+  ProjArgs a;
+  a.npts = c->g.npts;
+  a.natom = c->pp.natom;
+  a.nlma = c->pp.nlma;
+  a.nps = c->pp.nps;
+  a.totpts = c->pp.totpts;
+  a.nspin_no = c->orb.nspin * c->orb.no;
+  a.phase_per_k = c->g.periodic;
+  a.atom_start = c->pp.d_atom_start;
+  a.mps = c->pp.d_mps;
+  a.lma_start = c->pp.d_lma_start;
+  a.nproj = c->pp.d_nproj;
+  a.pt_lin = c->pp.d_pt_lin;
+  a.uv = c->pp.d_uv;
+  a.rinv = c->pp.d_rinv;
+  a.pt_r = c->pp.d_pt_r;
+  a.phase = c->pp.d_phase;
+  return a;
+}
+
+int launch_project(sb200_ctx* c, const double2* in, double2* proj) {
+  if (c->pp.nlma == 0) return SB200_OK;
+  ProjArgs a = proj_args(c);
+  dim3 grid((a.natom + 3) / 4, c->orb.norb);
+  k_project<4><<<grid, 128, 0, c->stream>>>(in, proj, a);
+  SB_LAUNCH_CHECK("k_project");
+  return SB200_OK;
+}
+
+int launch_project_moments(sb200_ctx* c, const double2* psi) {
+  if (c->pp.nlma == 0) return SB200_OK;
+  ProjArgs a = proj_args(c);
+  dim3 grid((a.natom + 3) / 4, c->orb.norb);
+  k_project_moments<2><<<grid, 128, 0, c->stream>>>(psi, c->d_jw, a);
+  SB_LAUNCH_CHECK("k_project_moments");
+  return SB200_OK;
+}
+
+int launch_hpsi(sb200_ctx* c, const HpsiLaunch& L) {
+  HArgs a;
+  a.nx = c->g.nx;
+  a.ny = c->g.ny;
+  a.nz = c->g.nz;
+  a.periodic = c->g.periodic;
+  a.nspin = c->orb.nspin;
+  a.nspin_no = c->orb.nspin * c->orb.no;
+  a.nlma = c->pp.nlma;
+  a.totpts = c->pp.totpts;
+  a.phase_per_k = c->g.periodic;
+  a.npts = c->g.npts;
+  for (int i = 0; i < 12; ++i) a.lapt[i] = c->g.coef_lap[i];
+  a.kcoef = c->d_kcoef;
+  a.vloc = c->d_vloc;
+  a.map = c->pp.d_map;
+  a.vi_start = c->pp.d_vi_start;
+  a.ent_lma = c->pp.d_ent_lma;
+  a.ent_pt = c->pp.d_ent_pt;
+  a.ent_uv = c->pp.d_ent_uv;
+  a.phase = c->pp.d_phase;
+  a.proj = c->d_proj;
+  a.zc = L.zc;
+  dim3 grid((unsigned)((c->g.npts + 255) / 256), c->orb.norb);
+  switch (L.mode) {
+    case 0: k_hpsi<0><<<grid, 256, 0, c->stream>>>(L.in, L.hout, L.out, a); break;
+    case 1: k_hpsi<1><<<grid, 256, 0, c->stream>>>(L.in, L.hout, L.out, a); break;
+    case 2: k_hpsi<2><<<grid, 256, 0, c->stream>>>(L.in, L.hout, L.out, a); break;
+    case 3: k_hpsi<3><<<grid, 256, 0, c->stream>>>(L.in, L.hout, L.out, a); break;
+    default: k_hpsi<4><<<grid, 256, 0, c->stream>>>(L.in, L.hout, L.out, a); break;
+  }
+  SB_LAUNCH_CHECK("k_hpsi");
+  return SB200_OK;
+}
+
+int launch_observables(sb200_ctx* c, const double2* psi) {
+  ObsArgs a;
+  a.nx = c->g.nx;
+  a.ny = c->g.ny;
+  a.nz = c->g.nz;
+  a.periodic = c->g.periodic;
+  a.npts = c->g.npts;
+  a.nblk = c->obs_blocks;
+  for (int i = 0; i < 12; ++i) a.nab[i] = c->g.coef_nab[i];
+  for (int d = 0; d < 3; ++d) a.off[d] = (double)c->g.is[d] - ((c->g.lg_num[d] % 2 == 1) ? 0.0 : 0.5);
+  dim3 grid(c->obs_blocks, c->orb.norb);
+  k_observables<<<grid, OBS_THREADS, 0, c->stream>>>(psi, c->d_obs, a);
+  SB_LAUNCH_CHECK("k_observables");
+  return SB200_OK;
+}
+
+// itt >= 0: history index given by the host (API calls), results to d_result;
+// itt < 0: RT loop, index from the device step counter.
+int launch_finalize(sb200_ctx* c, int itt, int nt, int trans_longi, double dt, int spin_filter) {
+  FinArgs a;
+  a.norb = c->orb.norb;
+  a.nspin = c->orb.nspin;
+  a.spin_filter = spin_filter;
+  a.nspin_no = c->orb.nspin * c->orb.no;
+  a.nblk = c->obs_blocks;
+  a.natom = c->pp.natom;
+  a.periodic = c->g.periodic;
+  a.itt = itt;
+  a.trans_longi = trans_longi;
+  a.ngrid_inv = 1.0 / (double)((long)c->g.lg_num[0] * c->g.lg_num[1] * c->g.lg_num[2]);
+  a.dt = dt;
+  a.part = c->d_obs;
+  a.jw = (c->pp.nlma > 0 && c->g.periodic) ? c->d_jw : nullptr;
+  a.weight = c->d_weight;
+  a.vec_k = c->d_vec_k;
+  a.step = c->rt.d_step;
+  if (itt < 0) {
+    a.Ac_cur = c->rt.d_Ac_tot;
+    a.A_direct = 0;
+    a.Ac_ind = c->rt.d_Ac_ind;
+    a.Ac_tot = c->rt.d_Ac_tot;
+    a.Ac_ext = c->rt.d_Ac_ext;
+    a.curr_hist = c->rt.d_curr;
+    a.rbox_hist = c->rt.d_rbox;
+    a.result = nullptr;
+    a.advance = 1;
+  } else {
+    a.Ac_cur = c->d_result + 8;  // A for the current is staged in result[8..10]
+    a.A_direct = 1;
+    a.Ac_ind = nullptr;
+    a.Ac_tot = nullptr;
+    a.Ac_ext = nullptr;
+    a.curr_hist = nullptr;
+    a.rbox_hist = nullptr;
+    a.result = c->d_result;
+    a.advance = 0;
+  }
+  (void)nt;
+  k_finalize<<<1, 256, 0, c->stream>>>(a);
+  SB_LAUNCH_CHECK("k_finalize");
+  return SB200_OK;
+}
+
+int launch_density(sb200_ctx* c, const double2* psi, double* rho) {
+  const long n = c->g.npts;
+  k_density<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(psi, rho, n, c->orb.nspin, c->orb.no, c->orb.nk,
+                                                               c->d_weight);
+  SB_LAUNCH_CHECK("k_density");
+  return SB200_OK;
+}
+
+int launch_dip(sb200_ctx* c, const double* rho, double* d_out4) {
+  const long n = c->g.npts * c->orb.nspin;
+  int nblk = (int)((n + 255) / 256);
+  const int cap = (int)((size_t)c->orb.norb * c->obs_blocks * OBS_NQ / 4);
+  if (nblk > cap) nblk = cap;
+  if (nblk > 1024) nblk = 1024;
+  if (nblk < 1) nblk = 1;
+  double o[3];
+  for (int d = 0; d < 3; ++d) o[d] = (double)c->g.is[d] - ((c->g.lg_num[d] % 2 == 1) ? 0.0 : 0.5);
+  k_dip_part<<<nblk, 256, 0, c->stream>>>(rho, c->d_obs, c->g.npts, c->orb.nspin, c->g.nx, c->g.ny, o[0], o[1],
+                                          o[2]);
+  SB_LAUNCH_CHECK("k_dip_part");
+  k_dip_final<<<1, 32, 0, c->stream>>>(c->d_obs, nblk, d_out4);
+  SB_LAUNCH_CHECK("k_dip_final");
+  return SB200_OK;
+}
+
+int launch_relayout(sb200_ctx* c, const void* src, void* dst, int norb_chunk, bool to_ref) {
+  const GridInfo& g = c->g;
+  const int nxa = g.ie_array[0] - g.is_array[0] + 1;
+  const int nya = g.ie_array[1] - g.is_array[1] + 1;
+  const long total = g.npts * norb_chunk;
+  k_relayout<<<grid_for(total, 256), 256, 0, c->stream>>>(
+      (const double2*)src, (double2*)dst, g.nx, g.ny, g.nz, nxa, nya, g.vol_array(), g.is[0] - g.is_array[0],
+      g.is[1] - g.is_array[1], g.is[2] - g.is_array[2], norb_chunk, to_ref ? 1 : 0);
+  SB_LAUNCH_CHECK("k_relayout");
+  return SB200_OK;
+}
+
+}  // namespace sb200

@@ -1,0 +1,191 @@
+"""Host-side mirror of SALMON's hpsi / taylor call surface over the C ABI.
+
+``Context`` holds one device-resident copy of the tables the reference passes
+to ``hpsi`` (``src/common/hamiltonian.f90:27``) and ``taylor``
+(``src/rt/taylor.f90:21``): the grid and stencil (``s_rgrid``, ``s_stencil``),
+the orbital block (``info``/``system``: nspin, io, ik, vec_k, rocc, wtk),
+``V_local`` and the projector tables (``s_pp_grid``).  Orbitals live on the GPU
+in the library's resident layout as torch ``complex128`` tensors of shape
+``[norb, nz, ny, nx]``; :meth:`Context.upload` / :meth:`Context.download`
+convert from / to the reference's Fortran layout.
+
+Errors raise :class:`salmon2_b200._lib.SB200Error` (the reference stops the
+program; here the caller gets the library's status code and message).  PyTorch
+only provides device memory and streams; all arithmetic runs in
+``libsalmon_b200.so``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import SB200Error, check, lib  # noqa: F401
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+
+
+def _ptr(a, t=_dp):
+    return a.ctypes.data_as(t)
+
+
+def _i3(v):
+    return (C.c_int * 3)(*[int(x) for x in v])
+
+
+class Context:
+    """Device context for one orbital block (one ``(ik, io, ispin)`` set)."""
+
+    def __init__(self, system, device: int = 0, precision: str = "fp64"):
+        import torch
+
+        self.torch = torch
+        self.sys = system
+        self.device = device
+        h = C.c_void_p()
+        check(lib().sb200_ctx_create(int(device), C.byref(h)))
+        self.h = h
+        g = system.grid
+        self._keep = []
+        idx = [np.ascontiguousarray(a, dtype=np.int32) for a in (g.idx, g.idy, g.idz)]
+        lap = np.ascontiguousarray(np.asarray(g.coef_lap).ravel(order="F"))
+        nab = np.ascontiguousarray(np.asarray(g.coef_nab).ravel(order="F"))
+        hgs = np.ascontiguousarray(g.hgs, dtype=np.float64)
+        check(lib().sb200_set_grid(self.h, _i3(g.is_), _i3(g.ie), _i3(g.is_array), _i3(g.ie_array),
+                                   _ptr(idx[0], _ip), _ptr(idx[1], _ip), _ptr(idx[2], _ip), _i3(g.num),
+                                   _ptr(hgs), g.hvol, g.coef_lap0, _ptr(lap), _ptr(nab)))
+        vec_k = np.asfortranarray(system.vec_k, dtype=np.float64)
+        rocc = np.asfortranarray(system.rocc, dtype=np.float64)
+        wtk = np.ascontiguousarray(system.wtk, dtype=np.float64)
+        check(lib().sb200_set_orbitals(self.h, system.nspin, system.no, system.nk, _ptr(vec_k), _ptr(rocc),
+                                       _ptr(wtk)))
+        V = np.asfortranarray(system.V_local, dtype=np.float64)
+        check(lib().sb200_set_vlocal(self.h, _ptr(V)))
+        self.set_pp(system.pp)
+        self.set_precision(precision)
+        self.shape = (system.norb, g.shape[2], g.shape[1], g.shape[0])
+
+    # -- set-up -------------------------------------------------------------
+    def set_pp(self, pp):
+        mps = np.ascontiguousarray(pp.mps, dtype=np.int32)
+        jxyz = np.asfortranarray(pp.jxyz, dtype=np.int32)
+        rxyz = np.asfortranarray(pp.rxyz, dtype=np.float64)
+        uv = np.asfortranarray(pp.uv, dtype=np.float64)
+        ia = np.ascontiguousarray(pp.ia_tbl, dtype=np.int32)
+        rinv = np.ascontiguousarray(pp.rinv_uvu, dtype=np.float64)
+        check(lib().sb200_set_pp(self.h, pp.natom, pp.nps, pp.nlma, _ptr(mps, _ip), _ptr(jxyz, _ip), _ptr(rxyz),
+                                 _ptr(uv), _ptr(ia, _ip), _ptr(rinv)))
+
+    def set_vec_Ac(self, vec_Ac):
+        a = np.ascontiguousarray(vec_Ac, dtype=np.float64)
+        check(lib().sb200_set_vec_Ac(self.h, _ptr(a)))
+
+    def set_precision(self, precision: str):
+        mode = {"fp64": _lib.PREC_FP64, "mixed": _lib.PREC_MIXED}[precision]
+        check(lib().sb200_set_precision(self.h, mode))
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().sb200_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def sync(self):
+        check(lib().sb200_ctx_sync(self.h))
+
+    def set_stream(self, stream):
+        """Run on a caller-owned stream (a torch.cuda.Stream), or None."""
+        check(lib().sb200_ctx_set_stream(self.h, None if stream is None else C.c_void_p(stream.cuda_stream)))
+
+    def set_timing(self, enable: bool):
+        check(lib().sb200_set_timing(self.h, 1 if enable else 0))
+
+    def kernel_times(self, reset: bool = True):
+        ms = (C.c_double * 8)()
+        cnt = (C.c_long * 8)()
+        check(lib().sb200_kernel_times(self.h, ms, cnt, 1 if reset else 0))
+        return {_lib.KIND_NAMES[i]: (ms[i], cnt[i]) for i in range(8) if cnt[i] > 0}
+
+    # -- orbital blocks -------------------------------------------------------
+    def empty(self):
+        return self.torch.empty(self.shape, dtype=self.torch.complex128, device=f"cuda:{self.device}")
+
+    def zeros(self):
+        return self.torch.zeros(self.shape, dtype=self.torch.complex128, device=f"cuda:{self.device}")
+
+    def upload(self, zwf_ref, out=None):
+        """Reference-layout orbitals (numpy, Fortran order, or a pinned torch
+        tensor holding the same bytes) -> resident device block."""
+        out = self.empty() if out is None else out
+        if isinstance(zwf_ref, np.ndarray):
+            src = np.asfortranarray(zwf_ref, dtype=np.complex128)
+            check(lib().sb200_orbitals_from_ref(self.h, C.c_void_p(src.ctypes.data), C.c_void_p(out.data_ptr())))
+        else:
+            check(lib().sb200_orbitals_from_ref(self.h, C.c_void_p(zwf_ref.data_ptr()),
+                                                C.c_void_p(out.data_ptr())))
+        return out
+
+    def download(self, psi, out=None):
+        g = self.sys.grid
+        if out is None:
+            out = np.zeros(g.shape_array + (self.sys.nspin, self.sys.no, self.sys.nk), dtype=np.complex128,
+                           order="F")
+            check(lib().sb200_orbitals_to_ref(self.h, C.c_void_p(psi.data_ptr()), C.c_void_p(out.ctypes.data)))
+        else:
+            check(lib().sb200_orbitals_to_ref(self.h, C.c_void_p(psi.data_ptr()), C.c_void_p(out.data_ptr())))
+        return out
+
+    # -- the hot path -----------------------------------------------------------
+    def hpsi(self, tpsi, htpsi):
+        check(lib().sb200_hpsi(self.h, C.c_void_p(tpsi.data_ptr()), C.c_void_p(htpsi.data_ptr())))
+        return htpsi
+
+    def taylor(self, tspsi_in, tspsi_out, sshtpsi, zc):
+        z = np.ascontiguousarray(zc, dtype=np.complex128)
+        check(lib().sb200_taylor(self.h, C.c_void_p(tspsi_in.data_ptr()), C.c_void_p(tspsi_out.data_ptr()),
+                                 C.c_void_p(sshtpsi.data_ptr()), z.ctypes.data_as(_dp), len(z)))
+        return tspsi_out
+
+    def calc_density(self, psi):
+        g = self.sys.grid
+        rho = np.zeros(g.shape + (self.sys.nspin,), order="F")
+        check(lib().sb200_calc_density(self.h, C.c_void_p(psi.data_ptr()), C.c_void_p(rho.ctypes.data)))
+        return rho
+
+    def calc_current(self, psi, vec_Ac):
+        a = np.ascontiguousarray(vec_Ac, dtype=np.float64)
+        cur = np.zeros((3, self.sys.nspin), order="F")
+        check(lib().sb200_calc_current(self.h, C.c_void_p(psi.data_ptr()), _ptr(a), _ptr(cur)))
+        return cur
+
+    def calc_dip(self, rho):
+        if isinstance(rho, np.ndarray):
+            r = np.asfortranarray(rho, dtype=np.float64)
+            p = C.c_void_p(r.ctypes.data)
+        else:
+            p = C.c_void_p(rho.data_ptr())
+        out = np.zeros(4)
+        check(lib().sb200_calc_dip(self.h, p, _ptr(out)))
+        return out
+
+    def rt_propagate(self, psi_a, psi_b, work, nt, dt, zc, Ac_ext=None, trans_longi="tr"):
+        z = np.ascontiguousarray(zc, dtype=np.complex128)
+        ac = None if Ac_ext is None else np.asfortranarray(Ac_ext, dtype=np.float64)
+        curr = np.zeros((3, max(nt, 1)), order="F")
+        rbox = np.zeros((4, max(nt, 1)), order="F")
+        act = np.zeros((3, nt + 2), order="F")
+        fin = C.c_void_p()
+        tl = {"tr": _lib.TRANS_TR, "lo": _lib.TRANS_LO}[trans_longi]
+        check(lib().sb200_rt_propagate(self.h, C.c_void_p(psi_a.data_ptr()), C.c_void_p(psi_b.data_ptr()),
+                                       C.c_void_p(work.data_ptr()), int(nt), float(dt), z.ctypes.data_as(_dp),
+                                       len(z), None if ac is None else _ptr(ac), tl, _ptr(curr), _ptr(rbox),
+                                       _ptr(act), C.byref(fin)))
+        final = psi_a if fin.value == psi_a.data_ptr() else psi_b
+        return dict(psi=final, curr=curr[:, :nt], rbox=rbox[:, :nt], Ac_tot=act)

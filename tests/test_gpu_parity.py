@@ -1,0 +1,153 @@
+"""GPU parity of the FP64 path against the CPU oracle, through the C ABI.
+
+Tolerances (FP64 form): 1e-12 relative (max-norm) per H psi and per Taylor
+step; 1e-10 relative on the current J(t) and the dipole over the time loop.
+"""
+import numpy as np
+import pytest
+
+import _systems as S
+from oracle import Oracle
+
+pytestmark = pytest.mark.gpu
+
+TOL_H = 1e-12
+TOL_OBS = 1e-10
+
+
+def _ctx(system, precision="fp64"):
+    from salmon2_b200.rt import Context
+    return Context(system, device=0, precision=precision)
+
+
+SYSTEMS = [S.periodic_small, S.periodic_c2_like, S.isolated_small, S.isolated_odd]
+
+
+@pytest.mark.parametrize("make", SYSTEMS, ids=lambda f: f.__name__)
+def test_relayout_round_trip(make):
+    sysm = make()
+    ctx = _ctx(sysm)
+    psi = ctx.upload(sysm.psi)
+    back = ctx.download(psi)
+    assert np.array_equal(back, sysm.psi)
+
+
+@pytest.mark.parametrize("make", SYSTEMS, ids=lambda f: f.__name__)
+@pytest.mark.parametrize("with_pp", [True, False])
+def test_hpsi_parity(make, with_pp):
+    sysm = make() if with_pp else S.no_pp(make())
+    O = Oracle(sysm)
+    ctx = _ctx(sysm)
+    ac = (0.013, -0.021, 0.034)
+    O.set_vec_Ac(ac)
+    ctx.set_vec_Ac(ac)
+    ref = O.hpsi(sysm.psi)
+    t = ctx.upload(sysm.psi)
+    h = ctx.zeros()
+    ctx.hpsi(t, h)
+    got = ctx.download(h)
+    assert S.rel_err(got, ref) < TOL_H
+
+
+def test_hpsi_parity_two_spins():
+    sysm = S.periodic_small(nspin=2)
+    O = Oracle(sysm)
+    ctx = _ctx(sysm)
+    ref = O.hpsi(sysm.psi)
+    h = ctx.zeros()
+    ctx.hpsi(ctx.upload(sysm.psi), h)
+    assert S.rel_err(ctx.download(h), ref) < TOL_H
+
+
+@pytest.mark.parametrize("make", SYSTEMS, ids=lambda f: f.__name__)
+def test_taylor_parity(make):
+    from salmon2_b200 import synth
+    sysm = make()
+    O = Oracle(sysm)
+    ctx = _ctx(sysm)
+    ac = (0.0, 0.0, 0.02)
+    O.set_vec_Ac(ac)
+    ctx.set_vec_Ac(ac)
+    zc = synth.taylor_zc(0.05)
+    ref = O.taylor(sysm.psi, zc)
+    a = ctx.upload(sysm.psi)
+    out, work = ctx.zeros(), ctx.zeros()
+    ctx.taylor(a, out, work, zc)
+    assert S.rel_err(ctx.download(out), ref) < TOL_H
+
+
+@pytest.mark.parametrize("make", SYSTEMS, ids=lambda f: f.__name__)
+def test_density_and_dip(make):
+    sysm = make()
+    O = Oracle(sysm)
+    ctx = _ctx(sysm)
+    psi = ctx.upload(sysm.psi)
+    rho = ctx.calc_density(psi)
+    rho_ref = O.density(sysm.psi)
+    assert S.rel_err(rho, rho_ref) < TOL_H
+    rb = ctx.calc_dip(rho_ref)
+    rb_ref = O.dip(rho_ref)
+    assert np.max(np.abs(rb - rb_ref)) <= 1e-11 * np.max(np.abs(rb_ref))
+
+
+@pytest.mark.parametrize("make", [S.periodic_small, S.periodic_c2_like], ids=lambda f: f.__name__)
+def test_current(make):
+    sysm = make()
+    O = Oracle(sysm)
+    ctx = _ctx(sysm)
+    a_mid, a_cur = (0.01, 0.02, -0.03), (0.011, 0.019, -0.029)
+    O.set_vec_Ac(a_mid)
+    ctx.set_vec_Ac(a_mid)
+    O.set_vec_Ac_local_only(a_cur)
+    ref = O.current(sysm.psi)
+    got = ctx.calc_current(ctx.upload(sysm.psi), a_cur)
+    assert np.max(np.abs(got - ref)) <= TOL_OBS * max(np.max(np.abs(ref)), 1e-30)
+
+
+@pytest.mark.parametrize("trans", ["tr", "lo"])
+def test_rt_propagate_periodic(trans):
+    from salmon2_b200 import synth
+    sysm = S.periodic_small()
+    nt, dt = 40, 0.08
+    Ac = synth.asin2cos(nt, dt, omega=0.05696, f0=0.05696 * 2e-2, tw=nt * dt)
+    zc = synth.taylor_zc(dt)
+    O = Oracle(sysm)
+    ref = O.rt_run(sysm.psi, nt, dt, zc, Ac_ext=Ac, trans_longi=1 if trans == "lo" else 0)
+    ctx = _ctx(sysm)
+    a, b, w = ctx.upload(sysm.psi), ctx.zeros(), ctx.zeros()
+    res = ctx.rt_propagate(a, b, w, nt, dt, zc, Ac_ext=Ac, trans_longi=trans)
+    jmax = np.max(np.abs(ref["curr"]))
+    assert jmax > 0
+    assert np.max(np.abs(res["curr"] - ref["curr"])) <= TOL_OBS * jmax
+    assert S.rel_err(res["rbox"], ref["rbox"]) < TOL_OBS
+    assert S.rel_err(ctx.download(res["psi"]), ref["psi"]) < 1e-11
+    if trans == "lo":
+        assert np.max(np.abs(res["Ac_tot"] - ref["Ac_tot"])) <= 1e-10 * np.max(np.abs(ref["Ac_tot"]))
+
+
+def test_rt_propagate_isolated_kick():
+    from salmon2_b200 import synth
+    sysm = S.isolated_small()
+    psi0 = synth.impulse_kick(sysm.grid, sysm.psi, 1e-3)
+    nt, dt = 30, 0.05
+    zc = synth.taylor_zc(dt)
+    O = Oracle(sysm)
+    ref = O.rt_run(psi0, nt, dt, zc)
+    ctx = _ctx(sysm)
+    a, b, w = ctx.upload(psi0), ctx.zeros(), ctx.zeros()
+    res = ctx.rt_propagate(a, b, w, nt, dt, zc)
+    # dipole response relative to the static dipole (dDp_e of dip.f90:62-63)
+    d_ref = ref["rbox"][:3] - ref["rbox"][:3, :1]
+    d_got = res["rbox"][:3] - res["rbox"][:3, :1]
+    assert np.max(np.abs(d_got - d_ref)) <= TOL_OBS * np.max(np.abs(ref["rbox"][:3]))
+    assert np.max(np.abs(res["rbox"][3] - ref["rbox"][3])) <= 1e-12 * ref["rbox"][3, 0]
+
+
+def test_error_codes():
+    from salmon2_b200.rt import SB200Error
+    sysm = S.periodic_small()
+    ctx = _ctx(sysm)
+    a = ctx.upload(sysm.psi)
+    with pytest.raises(SB200Error) as e:
+        ctx.hpsi(a, a)  # aliased input / output
+    assert e.value.code == 1

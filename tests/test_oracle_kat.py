@@ -1,0 +1,161 @@
+"""Known-answer and property tests of the CPU oracle (CPU only).
+
+These pin the restated arithmetic where the reference's own tests hold no
+vectors at the hpsi / taylor boundary: plane-wave eigenvalues of the
+finite-difference Bloch operator, the Taylor polynomial on an eigenstate,
+Hermiticity of H (stencil + KB), the density sum rule, the plane-wave current
+and the dipole of a uniform density.
+"""
+import dataclasses
+
+import numpy as np
+import pytest
+
+import _systems as S
+from oracle import Oracle
+from salmon2_b200 import synth
+
+
+def plane_wave_system(num=12, kvec=(0.1, 0.2, -0.05)):
+    s = S.no_pp(synth.periodic_system(a=10.26, num=num, nkgrid=1, no=1, seed=3))
+    s.V_local[:] = 0.0
+    s.vec_k[:, 0] = kvec
+    return s
+
+
+def fd_energy(g, q, kap):
+    E = 0.0
+    s_ = np.arange(1, 5)
+    for d in range(3):
+        h = g.hgs[d]
+        lam = (synth.CN4[0] + 2 * np.sum(synth.CN4[1:] * np.cos(s_ * q[d] * h))) / h ** 2
+        D = 2 * np.sum(synth.BN4 * np.sin(s_ * q[d] * h)) / h
+        E += -0.5 * lam + 0.5 * kap[d] ** 2 + kap[d] * D
+    return E
+
+
+def pw(g, m):
+    L = g.num * g.hgs
+    q = 2 * np.pi * np.asarray(m) / L
+    X, Y, Z = np.meshgrid(g.coordinate(0), g.coordinate(1), g.coordinate(2), indexing="ij")
+    psi = np.zeros(g.shape_array + (1, 1, 1), complex, order="F")
+    psi[g.interior_slices() + (0, 0, 0)] = np.exp(1j * (q[0] * X + q[1] * Y + q[2] * Z)) / np.sqrt(np.prod(L))
+    return psi, q
+
+
+@pytest.mark.parametrize("m", [(0, 0, 0), (1, 2, -3), (5, -4, 6)])
+def test_plane_wave_eigenvalue(m):
+    s = plane_wave_system()
+    O = Oracle(s)
+    ac = np.array([0.0, 0.0, 0.03])
+    O.set_vec_Ac(ac)
+    psi, q = pw(s.grid, m)
+    h = O.hpsi(psi)
+    sl = s.grid.interior_slices() + (0, 0, 0)
+    E = fd_energy(s.grid, q, s.vec_k[:, 0] + ac)
+    np.testing.assert_allclose(h[sl], E * psi[sl], rtol=0, atol=1e-13 * np.abs(psi[sl]).max() * max(1, abs(E)))
+
+
+def test_taylor_on_eigenstate():
+    s = plane_wave_system()
+    O = Oracle(s)
+    psi, q = pw(s.grid, (1, 0, 2))
+    E = fd_energy(s.grid, q, s.vec_k[:, 0])
+    dt = 0.08
+    zc = synth.taylor_zc(dt)
+    out = O.taylor(psi, zc)
+    factor = 1 + sum(zc[n - 1] * E ** n for n in range(1, 5))
+    sl = s.grid.interior_slices() + (0, 0, 0)
+    np.testing.assert_allclose(out[sl], factor * psi[sl], rtol=1e-13, atol=1e-15)
+
+
+@pytest.mark.parametrize("make", [S.periodic_small, S.isolated_small, S.isolated_odd], ids=lambda f: f.__name__)
+def test_hermiticity(make):
+    s = make()
+    O = Oracle(s)
+    O.set_vec_Ac((0.01, -0.02, 0.015))
+    h = O.hpsi(s.psi)
+    sl = s.grid.interior_slices()
+    a, b = s.psi[sl + (0, 0, 0)], s.psi[sl + (0, 1, 0)]
+    ha, hb = h[sl + (0, 0, 0)], h[sl + (0, 1, 0)]
+    lhs, rhs = np.vdot(a, hb), np.conj(np.vdot(b, ha))
+    assert abs(lhs - rhs) <= 1e-12 * max(abs(lhs), np.abs(ha).max())
+
+
+def test_density_sum_rule():
+    s = S.periodic_small()
+    O = Oracle(s)
+    rho = O.density(s.psi)
+    ne = rho.sum() * s.grid.hvol
+    # orthonormal orbitals, occupation 2, k-weights summing to 1
+    assert abs(ne - 2.0 * s.no) < 1e-10
+
+
+def test_plane_wave_current():
+    s = plane_wave_system()
+    O = Oracle(s)
+    ac = np.array([0.0, 0.0, 0.02])
+    O.set_vec_Ac(ac)
+    psi, q = pw(s.grid, (1, -2, 1))
+    cur = O.current(psi)[:, 0]
+    g = s.grid
+    s_ = np.arange(1, 5)
+    D = np.array([2 * np.sum(synth.BN4 * np.sin(s_ * q[d] * g.hgs[d])) / g.hgs[d] for d in range(3)])
+    kac = s.vec_k[:, 0] + ac
+    # J = occ * (kAc * <|psi|^2> + D) summed over the grid, / ngrid
+    norm = np.sum(np.abs(psi) ** 2)
+    expect = 2.0 * (kac * norm + D * norm) / s.ngrid
+    np.testing.assert_allclose(cur, expect, rtol=1e-12, atol=1e-18)
+
+
+def test_dipole_of_uniform_density():
+    s = S.isolated_odd()
+    O = Oracle(s)
+    rho = np.ones(s.grid.shape + (1,), order="F")
+    rb = O.dip(rho)
+    g = s.grid
+    for d in range(3):
+        shift = 0.0 if g.num[d] % 2 == 1 else 0.5
+        idx = np.arange(g.is_[d], g.ie[d] + 1) - shift
+        expect = idx.sum() * np.prod(g.shape) / g.shape[d]
+        assert abs(rb[d] - expect) < 1e-9
+    assert rb[3] == np.prod(g.shape)
+
+
+def test_norm_drift_taylor4():
+    """Taylor-4 is not unitary: the norm drifts by O((dt*E)^6) per step."""
+    s = S.periodic_small()
+    O = Oracle(s)
+    dt = 0.02
+    out = O.taylor(s.psi, synth.taylor_zc(dt))
+    sl = s.grid.interior_slices()
+    n0 = np.sum(np.abs(s.psi[sl]) ** 2)
+    n1 = np.sum(np.abs(out[sl]) ** 2)
+    assert abs(n1 / n0 - 1.0) < 1e-5
+
+
+def test_rt_run_matches_repeated_taylor():
+    s = S.periodic_small()
+    nt, dt = 3, 0.08
+    Ac = synth.asin2cos(nt, dt, omega=0.05696, f0=0.05696 * 1e-2, tw=nt * dt)
+    zc = synth.taylor_zc(dt)
+    O = Oracle(s)
+    res = O.rt_run(s.psi, nt, dt, zc, Ac_ext=Ac)
+    O2 = Oracle(s)
+    psi = s.psi
+    for itt in range(1, nt + 1):
+        O2.set_vec_Ac(0.5 * (Ac[:, itt] + Ac[:, itt - 1]))
+        psi = O2.taylor(psi, zc)
+        O2.set_vec_Ac_local_only(Ac[:, itt])
+        np.testing.assert_allclose(O2.current(psi)[:, 0], res["curr"][:, itt - 1], rtol=1e-12, atol=1e-18)
+    np.testing.assert_array_equal(psi, res["psi"])
+
+
+def test_pp_tables_inside_grid():
+    for s in (S.periodic_small(), S.isolated_small(), S.isolated_odd()):
+        g, pp = s.grid, s.pp
+        for ia in range(pp.natom):
+            j = pp.jxyz[:, : pp.mps[ia], ia]
+            assert np.all(j >= g.is_[:, None]) and np.all(j <= g.ie[:, None])
+        # projectors of each atom are contiguous in ilma (set_lma ordering)
+        assert np.all(np.diff(pp.ia_tbl) >= 0)

@@ -93,7 +93,9 @@ class Clocks:
     """nvidia-smi sampling during the timed region."""
 
     def __init__(self, index):
-        self.index = index
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+        ids = [v.strip() for v in vis.split(",") if v.strip()]
+        self.index = ids[index] if index < len(ids) else str(index)
         self.proc = None
         self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
 

@@ -56,7 +56,9 @@ def lib():
         for name in ("sbo_zstencil", "sbo_dstencil", "sbo_update_kvector_nonlocalpt", "sbo_zpseudo",
                      "sbo_dpseudo", "sbo_zprojections", "sbo_hpsi", "sbo_hpsi_real", "sbo_taylor",
                      "sbo_calc_density", "sbo_calc_current", "sbo_current_parts", "sbo_calc_dip",
-                     "sbo_calc_Ac_ext_t", "sbo_rt_run", "sbo_set_threads", "sbo_get_threads"):
+                     "sbo_calc_Ac_ext_t", "sbo_rt_run", "sbo_set_threads", "sbo_get_threads",
+                     "sbo_precond_real", "sbo_gscg_rwf", "sbo_gram_schmidt_real", "sbo_gram_schmidt_complex",
+                     "sbo_subspace_diag_real", "sbo_inner_product_real"):
             getattr(L, name)
         L.sbo_rt_run.restype = C.c_int
         L.sbo_get_threads.restype = C.c_int
@@ -214,3 +216,45 @@ class Oracle:
                                  _p(Ac_tot), C.c_int(trans_longi), _p(curr), _p(rbox), _p(rho))
         psi = a if which == 0 else b
         return dict(psi=psi, curr=curr, rbox=rbox, Ac_tot=Ac_tot, Ac_ind=Ac_ind, rho=rho)
+
+    # -- ground state (real orbitals, one k) --------------------------------
+    def _real(self, psi):
+        a = np.asfortranarray(psi, dtype=np.float64)
+        assert a.shape[:3] == self.sys.grid.shape_array
+        return a
+
+    def precond_real(self, g, alpha=0.6):
+        a = self._real(g)
+        out = np.zeros_like(a, order="F")
+        lib().sbo_precond_real(C.byref(self.s), _p(a), _p(out), C.c_double(alpha))
+        return out
+
+    def gscg(self, psi, ncg=4, precondition=False, alpha=0.6):
+        a = self._real(psi).copy(order="F")
+        work = np.zeros((7,) + a.shape, order="F")
+        esp = np.zeros(self.sys.nspin * self.sys.no)
+        lib().sbo_gscg_rwf(C.byref(self.s), C.c_int(ncg), _p(a), _p(work), C.c_int(1 if precondition else 0),
+                           C.c_double(alpha), _p(esp))
+        return a, esp
+
+    def gram_schmidt_real(self, psi):
+        a = self._real(psi).copy(order="F")
+        lib().sbo_gram_schmidt_real(C.byref(self.s), _p(a))
+        return a
+
+    def gram_schmidt_complex(self, psi):
+        a = self._orb(psi).copy(order="F")
+        lib().sbo_gram_schmidt_complex(C.byref(self.s), _p(a))
+        return a
+
+    def subspace_diag_real(self, psi):
+        a = self._real(psi).copy(order="F")
+        work = np.zeros_like(a, order="F")
+        ev = np.zeros(self.sys.nspin * self.sys.no)
+        lib().sbo_subspace_diag_real(C.byref(self.s), _p(a), _p(work), _p(ev))
+        return a, ev
+
+    def inner_real(self, x, y):
+        out = np.zeros(self.sys.nspin * self.sys.no)
+        lib().sbo_inner_product_real(C.byref(self.s), _p(self._real(x)), _p(self._real(y)), _p(out))
+        return out

@@ -126,6 +126,21 @@ int sbo_rt_run(sbo_system* s, double* psi_a, double* psi_b, double* work,
                const double* Ac_ext, double* Ac_ind, double* Ac_tot,
                int trans_longi, double* curr, double* rbox, double* rho_work);
 
+/* Ground state, real orbitals, one k (salmon_oracle_gs.cpp).
+ * dstencil_preconditioning (src/gs/preconditioning.f90:25-77) on every orbital */
+void sbo_precond_real(const sbo_system* s, const double* gk, double* pre_gk, double alpha);
+/* gscg_rwf (src/gs/conjugate_gradient.f90:21-466); work = 7 orbital blocks;
+ * esp_out(nspin*no) = final Rayleigh quotients.                              */
+void sbo_gscg_rwf(const sbo_system* s, int ncg, double* psi, double* work, int precondition,
+                  double alpha_pre, double* esp_out);
+/* classical Gram-Schmidt (src/gs/gram_schmidt_orth.f90:59-230, 1069-1242)     */
+void sbo_gram_schmidt_real(const sbo_system* s, double* psi);
+void sbo_gram_schmidt_complex(const sbo_system* s, double* psi);
+/* ssdg_rwf (src/gs/subspace_diagonalization.f90:62-238) with a Jacobi
+ * eigensolver instead of LAPACK dsyev; work = one orbital block.             */
+void sbo_subspace_diag_real(const sbo_system* s, double* psi, double* work, double* evals);
+void sbo_inner_product_real(const sbo_system* s, const double* x, const double* y, double* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -4,6 +4,7 @@
 
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -242,6 +243,7 @@ int sb200_ctx_create(int device, sb200_ctx** out) {
     return cuda_error(e, "cudaStreamCreate");
   }
   c->stream = c->own_stream;
+  if (const char* v = getenv("SB200_STENCIL")) c->stencil_variant = (v[0] == 'n') ? 0 : 1;
   int r = dalloc(&c->d_result, 16);
   if (r == SB200_OK) r = dalloc(&c->rt.d_step, 1);
   if (r != SB200_OK) {

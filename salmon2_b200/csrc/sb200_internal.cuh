@@ -105,6 +105,7 @@ struct sb200_ctx {
   void* d_stage = nullptr;      // relayout staging
   size_t stage_bytes = 0;
   bool vloc_set = false;
+  int stencil_variant = 1;     // 0: per-point reference kernel, 1: tiled 2.5-D sweep
   // optional per-kernel-class device timing (sb200_set_timing)
   bool timing = false;
   std::vector<cudaEvent_t> ev;  // pairs (start, stop)
@@ -161,6 +162,7 @@ int launch_prep_k(sb200_ctx* c, const double* d_A, int a_mode, int itt_from_devi
                   double* d_kcoef, bool phases);
 int launch_project(sb200_ctx* c, const double2* in, double2* proj);
 int launch_hpsi(sb200_ctx* c, const HpsiLaunch& L);
+int launch_hpsi_tiled(sb200_ctx* c, const HpsiLaunch& L);  // sb200_stencil.cu
 int launch_observables(sb200_ctx* c, const double2* psi);
 int launch_project_moments(sb200_ctx* c, const double2* psi);
 int launch_finalize(sb200_ctx* c, int itt_host, int nt, int trans_longi, double dt, int spin_filter);

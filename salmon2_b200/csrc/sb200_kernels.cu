@@ -611,6 +611,7 @@ int launch_project_moments(sb200_ctx* c, const double2* psi) {
 }
 
 int launch_hpsi(sb200_ctx* c, const HpsiLaunch& L) {
+  if (c->stencil_variant == 1) return launch_hpsi_tiled(c, L);
   HArgs a;
   a.nx = c->g.nx;
   a.ny = c->g.ny;

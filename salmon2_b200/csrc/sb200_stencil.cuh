@@ -1,0 +1,23 @@
+// sb200_stencil.cuh -- argument block of the tiled hpsi kernel.
+#pragma once
+#include <cuda_runtime.h>
+
+namespace sb200 {
+
+struct TiledArgs {
+  int nx, ny, nz, periodic, nspin, nspin_no, nlma, totpts, phase_per_k, zchunk;
+  long npts;
+  double lapt[12];
+  const double* kcoef;
+  const double* vloc;
+  const int *map, *vi_start, *ent_lma, *ent_pt;
+  const double* ent_uv;
+  const double2* phase;
+  const double2* proj;
+  double2 zc;
+};
+
+struct HpsiLaunch;
+struct sb200_ctx_fwd;
+
+}  // namespace sb200

@@ -1,0 +1,178 @@
+!
+! salmon_b200.f90 -- ISO_C_BINDING interface to libsalmon_b200 (the B200
+! RT-TDDFT propagation library), for SALMON's Fortran host.
+!
+! Every routine binds one entry point of include/salmon_b200.h.  Integer
+! status codes are returned as c_int (0 = success); salmon_b200_check turns a
+! non-zero status into SALMON's usual `stop` with the library's message.
+!
+! This module is shipped as source; it is not compiled in this repository
+! (the build machines have no Fortran compiler).  Its argument lists follow
+! the C prototypes one to one.
+!
+module salmon_b200
+  use iso_c_binding
+  implicit none
+
+  integer(c_int), parameter :: SB200_OK = 0
+  integer(c_int), parameter :: SB200_PREC_FP64 = 0, SB200_PREC_MIXED = 1
+  integer(c_int), parameter :: SB200_TRANS_TR = 0, SB200_TRANS_LO = 1
+
+  interface
+    integer(c_int) function sb200_ctx_create(device, ctx) bind(c, name="sb200_ctx_create")
+      import
+      integer(c_int), value :: device
+      type(c_ptr) :: ctx
+    end function
+
+    integer(c_int) function sb200_ctx_destroy(ctx) bind(c, name="sb200_ctx_destroy")
+      import
+      type(c_ptr), value :: ctx
+    end function
+
+    integer(c_int) function sb200_ctx_sync(ctx) bind(c, name="sb200_ctx_sync")
+      import
+      type(c_ptr), value :: ctx
+    end function
+
+    type(c_ptr) function sb200_last_error() bind(c, name="sb200_last_error")
+      import
+    end function
+
+    ! s_rgrid + s_stencil (initialization.f90:241-256,508-611)
+    integer(c_int) function sb200_set_grid(ctx, is, ie, is_array, ie_array, idx, idy, idz, lg_num, hgs, hvol, &
+                                           coef_lap0, coef_lap, coef_nab) bind(c, name="sb200_set_grid")
+      import
+      type(c_ptr), value :: ctx
+      integer(c_int), intent(in) :: is(3), ie(3), is_array(3), ie_array(3)
+      integer(c_int), intent(in) :: idx(*), idy(*), idz(*)
+      integer(c_int), intent(in) :: lg_num(3)
+      real(c_double), intent(in) :: hgs(3)
+      real(c_double), value :: hvol, coef_lap0
+      real(c_double), intent(in) :: coef_lap(4,3), coef_nab(4,3)
+    end function
+
+    integer(c_int) function sb200_set_orbitals(ctx, nspin, no, nk, vec_k, rocc, wtk) &
+        bind(c, name="sb200_set_orbitals")
+      import
+      type(c_ptr), value :: ctx
+      integer(c_int), value :: nspin, no, nk
+      real(c_double), intent(in) :: vec_k(3,*), rocc(*), wtk(*)
+    end function
+
+    integer(c_int) function sb200_set_vlocal(ctx, V_local) bind(c, name="sb200_set_vlocal")
+      import
+      type(c_ptr), value :: ctx
+      real(c_double), intent(in) :: V_local(*)
+    end function
+
+    integer(c_int) function sb200_set_pp(ctx, natom, nps, nlma, mps, jxyz, rxyz, uv, ia_tbl, rinv_uvu) &
+        bind(c, name="sb200_set_pp")
+      import
+      type(c_ptr), value :: ctx
+      integer(c_int), value :: natom, nps, nlma
+      integer(c_int), intent(in) :: mps(*), jxyz(3,nps,*), ia_tbl(*)
+      real(c_double), intent(in) :: rxyz(3,nps,*), uv(nps,*), rinv_uvu(*)
+    end function
+
+    integer(c_int) function sb200_set_vec_Ac(ctx, vec_Ac) bind(c, name="sb200_set_vec_Ac")
+      import
+      type(c_ptr), value :: ctx
+      real(c_double), intent(in) :: vec_Ac(3)
+    end function
+
+    integer(c_int) function sb200_set_precision(ctx, mode) bind(c, name="sb200_set_precision")
+      import
+      type(c_ptr), value :: ctx
+      integer(c_int), value :: mode
+    end function
+
+    integer(c_size_t) function sb200_orbital_block_bytes(ctx) bind(c, name="sb200_orbital_block_bytes")
+      import
+      type(c_ptr), value :: ctx
+    end function
+
+    ! zwf(is_array:ie_array, nspin, io_s:io_e, ik_s:ik_e, 1) <-> resident device block
+    integer(c_int) function sb200_orbitals_from_ref(ctx, zwf, psi_dev) bind(c, name="sb200_orbitals_from_ref")
+      import
+      type(c_ptr), value :: ctx
+      complex(c_double_complex), intent(in) :: zwf(*)
+      type(c_ptr), value :: psi_dev
+    end function
+
+    integer(c_int) function sb200_orbitals_to_ref(ctx, psi_dev, zwf) bind(c, name="sb200_orbitals_to_ref")
+      import
+      type(c_ptr), value :: ctx
+      type(c_ptr), value :: psi_dev
+      complex(c_double_complex), intent(inout) :: zwf(*)
+    end function
+
+    ! hpsi (hamiltonian.f90:27) on resident device blocks
+    integer(c_int) function sb200_hpsi(ctx, tpsi, htpsi) bind(c, name="sb200_hpsi")
+      import
+      type(c_ptr), value :: ctx, tpsi, htpsi
+    end function
+
+    ! taylor (taylor.f90:21) on resident device blocks; zc = rt%zc
+    integer(c_int) function sb200_taylor(ctx, tspsi_in, tspsi_out, sshtpsi, zc, n_hamil) &
+        bind(c, name="sb200_taylor")
+      import
+      type(c_ptr), value :: ctx, tspsi_in, tspsi_out, sshtpsi
+      complex(c_double_complex), intent(in) :: zc(*)
+      integer(c_int), value :: n_hamil
+    end function
+
+    integer(c_int) function sb200_calc_density(ctx, psi, rho) bind(c, name="sb200_calc_density")
+      import
+      type(c_ptr), value :: ctx, psi
+      real(c_double), intent(inout) :: rho(*)
+    end function
+
+    integer(c_int) function sb200_calc_current(ctx, psi, vec_Ac, curr) bind(c, name="sb200_calc_current")
+      import
+      type(c_ptr), value :: ctx, psi
+      real(c_double), intent(in) :: vec_Ac(3)
+      real(c_double), intent(inout) :: curr(3,*)
+    end function
+
+    integer(c_int) function sb200_calc_dip(ctx, rho, rbox) bind(c, name="sb200_calc_dip")
+      import
+      type(c_ptr), value :: ctx
+      real(c_double), intent(in) :: rho(*)
+      real(c_double), intent(inout) :: rbox(4)
+    end function
+
+    integer(c_int) function sb200_rt_propagate(ctx, psi_a, psi_b, work, nt, dt, zc, n_hamil, Ac_ext, &
+                                               trans_longi, curr, rbox, Ac_tot, psi_final) &
+        bind(c, name="sb200_rt_propagate")
+      import
+      type(c_ptr), value :: ctx, psi_a, psi_b, work
+      integer(c_int), value :: nt, n_hamil, trans_longi
+      real(c_double), value :: dt
+      complex(c_double_complex), intent(in) :: zc(*)
+      real(c_double), intent(in) :: Ac_ext(3,0:*)
+      real(c_double), intent(inout) :: curr(3,*), rbox(4,*), Ac_tot(3,0:*)
+      type(c_ptr) :: psi_final
+    end function
+  end interface
+
+contains
+
+  subroutine salmon_b200_check(rc, where)
+    integer(c_int), intent(in) :: rc
+    character(*), intent(in) :: where
+    character(kind=c_char), pointer :: msg(:)
+    character(len=512) :: text
+    integer :: i
+    if (rc == SB200_OK) return
+    call c_f_pointer(sb200_last_error(), msg, [512])
+    text = ''
+    do i = 1, 512
+      if (msg(i) == c_null_char) exit
+      text(i:i) = msg(i)
+    end do
+    write(*,*) 'salmon_b200 error in ', where, ': ', trim(text)
+    stop 'salmon_b200'
+  end subroutine salmon_b200_check
+
+end module salmon_b200

@@ -191,8 +191,23 @@ int timing_flush(sb200_ctx* c) {
 
 // One Taylor step tspsi_in -> tspsi_out (taylor.f90:43-119) with the
 // projections of each term's input computed first.
-int issue_taylor(sb200_ctx* c, double2* tin, double2* tout, double2* work, const double2* zc, int n_hamil) {
+int issue_taylor(sb200_ctx* c, double2* tin, double2* tout, double2* work, const double2* zc, int n_hamil,
+                 bool last_with_obs = false) {
+  const bool orbital = orbital_kernel_applies(c);
   for (int nn = 1; nn <= n_hamil; ++nn) {
+    if (orbital) {  // one CTA per orbital: projections and observables in-kernel
+      const bool odd = (nn % 2) == 1;
+      HpsiLaunch L;
+      L.in = odd ? tin : work;
+      L.hout = odd ? work : tin;
+      L.out = tout;
+      L.zc = zc[nn - 1];
+      const bool last = nn == n_hamil;
+      if (nn == 1) L.mode = last ? 4 : 1;
+      else L.mode = last ? 3 : 2;
+      TIMED(c, SB200_KIND_HPSI, launch_term_orbital(c, L, last && last_with_obs));
+      continue;
+    }
     const bool odd = (nn % 2) == 1;
     double2* src = odd ? tin : work;
     double2* dst = odd ? work : tin;
@@ -214,6 +229,11 @@ int issue_taylor(sb200_ctx* c, double2* tin, double2* tout, double2* work, const
 int issue_rt_step(sb200_ctx* c, double2* in, double2* out, double2* work, const double2* zc, int n_hamil,
                   int trans_longi, double dt) {
   if (c->g.periodic) TIMED(c, SB200_KIND_PREP, launch_prep_k(c, c->rt.d_Ac_tot, 1, -1, c->d_kcoef, true));
+  if (orbital_kernel_applies(c)) {  // observables fused into the last Taylor term
+    TRY(issue_taylor(c, in, out, work, zc, n_hamil, true));
+    TIMED(c, SB200_KIND_FINAL, launch_finalize(c, -1, 0, trans_longi, dt, -1, true));
+    return SB200_OK;
+  }
   TRY(issue_taylor(c, in, out, work, zc, n_hamil));
   TIMED(c, SB200_KIND_OBS, launch_observables(c, out));
   if (c->g.periodic) TIMED(c, SB200_KIND_MOMENTS, launch_project_moments(c, out));

@@ -163,9 +163,12 @@ int launch_prep_k(sb200_ctx* c, const double* d_A, int a_mode, int itt_from_devi
 int launch_project(sb200_ctx* c, const double2* in, double2* proj);
 int launch_hpsi(sb200_ctx* c, const HpsiLaunch& L);
 int launch_hpsi_tiled(sb200_ctx* c, const HpsiLaunch& L);  // sb200_stencil.cu
+bool orbital_kernel_applies(const sb200_ctx* c);             // sb200_orbital.cu
+int launch_term_orbital(sb200_ctx* c, const HpsiLaunch& L, bool with_obs);
 int launch_observables(sb200_ctx* c, const double2* psi);
 int launch_project_moments(sb200_ctx* c, const double2* psi);
-int launch_finalize(sb200_ctx* c, int itt_host, int nt, int trans_longi, double dt, int spin_filter);
+int launch_finalize(sb200_ctx* c, int itt_host, int nt, int trans_longi, double dt, int spin_filter,
+                    bool fused_obs = false);
 int launch_density(sb200_ctx* c, const double2* psi, double* rho);
 int launch_dip(sb200_ctx* c, const double* rho, double* d_out4);
 int launch_relayout(sb200_ctx* c, const void* src, void* dst, int norb_chunk, bool to_ref);

@@ -394,6 +394,7 @@ __global__ void __launch_bounds__(OBS_THREADS) k_observables(const double2* __re
 // ---------------------------------------------------------------------------
 struct FinArgs {
   int norb, nspin, nspin_no, nblk, natom, periodic, itt, trans_longi, advance, spin_filter;
+  int jw_natom;            // atoms per orbital in jw (1 when already summed)
   double ngrid_inv, dt;
   const double* part;
   const double* jw;        // [norb][natom][3] or null
@@ -429,8 +430,8 @@ __global__ void __launch_bounds__(256) k_finalize(FinArgs a) {
       const int ik = o / a.nspin_no;
       double jw[3] = {0.0, 0.0, 0.0};
       if (a.jw != nullptr)
-        for (int at = 0; at < a.natom; ++at)
-          for (int d = 0; d < 3; ++d) jw[d] += a.jw[3L * ((long)o * a.natom + at) + d];
+        for (int at = 0; at < a.jw_natom; ++at)
+          for (int d = 0; d < 3; ++d) jw[d] += a.jw[3L * ((long)o * a.jw_natom + at) + d];
       for (int d = 0; d < 3; ++d) {
         const double kAc = a.vec_k[3 * ik + d] + A[d];
         s[d] += (kAc * q[0] + 2.0 * q[1 + d] + 2.0 * jw[d]) * w;
@@ -664,13 +665,14 @@ int launch_observables(sb200_ctx* c, const double2* psi) {
 
 // itt >= 0: history index given by the host (API calls), results to d_result;
 // itt < 0: RT loop, index from the device step counter.
-int launch_finalize(sb200_ctx* c, int itt, int nt, int trans_longi, double dt, int spin_filter) {
+int launch_finalize(sb200_ctx* c, int itt, int nt, int trans_longi, double dt, int spin_filter, bool fused_obs) {
   FinArgs a;
   a.norb = c->orb.norb;
+  a.jw_natom = fused_obs ? 1 : c->pp.natom;
   a.nspin = c->orb.nspin;
   a.spin_filter = spin_filter;
   a.nspin_no = c->orb.nspin * c->orb.no;
-  a.nblk = c->obs_blocks;
+  a.nblk = fused_obs ? 1 : c->obs_blocks;
   a.natom = c->pp.natom;
   a.periodic = c->g.periodic;
   a.itt = itt;

@@ -1,0 +1,328 @@
+// sb200_orbital.cu -- orbital-resident Taylor-term kernel for small periodic
+// grids (one CTA owns one whole 16^3 orbital).
+//
+// Each CTA loads its orbital once from HBM (16 independent 16-byte loads per
+// thread: a full z column), keeps the column in registers for the z
+// neighbours and all 16 xy planes in shared memory for the x / y neighbours.
+// Because the CTA owns the whole orbital it also computes, from shared memory:
+//   * the KB projections <beta|h> of its own input before the stencil (no
+//     separate projection pass, nonlocal_potential.f90:358-367);
+//   * in the last Taylor term, the observables of the new orbital: sum |psi|^2,
+//     the forward-difference current sums (density_matrix.f90:465-530), the
+//     dipole moments (dip.f90:114-225) and the nonlocal current projections
+//     (density_matrix.f90:532-591), with the projector phases of this step.
+// The arithmetic per point is that of zstencil_typical_seq
+// (zstencil_core/typical/seq.f90:65-122) plus the owner-computes KB scatter and
+// the Taylor epilogue (taylor.f90:47-117); HBM traffic is the algorithmic
+// 48/64/64/48 bytes per point of the four Taylor terms.
+#include <cuda_runtime.h>
+
+#include "sb200_internal.cuh"
+#include "sb200_orbital.cuh"
+
+namespace sb200 {
+namespace {
+
+constexpr int N = 16, NP = N * N, NT = NP;  // 16^3 grid, one thread per (x, y) column
+
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double2 cscal(double r, double2 a) { return make_double2(r * a.x, r * a.y); }
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+// Projections P(lma) = rinv * sum_j conj(zekr_uV) v(pt_j) of the orbital held
+// in shared memory: one warp per atom, projectors four at a time.
+__device__ void project_from_smem(const double2* __restrict__ sm, double2* __restrict__ Ps, const OrbArgs& a,
+                                  int ik) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const double2* ph = a.phase + (long)ik * a.totpts;
+  for (int atom = warp; atom < a.natom; atom += NT / 32) {
+    const int start = a.atom_start[atom], m = a.mps[atom];
+    const int lma0 = a.lma_start[atom], np = a.nproj[atom];
+    for (int q0 = 0; q0 < np; q0 += 4) {
+      double2 acc[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc[q] = make_double2(0.0, 0.0);
+      for (int j = lane; j < m; j += 32) {
+        const double2 v = sm[__ldg(a.pt_lin + start + j)];
+        const double2 e = __ldg(ph + start + j);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          if (q0 + q < np) {
+            const double uv = __ldg(a.uv + (long)(lma0 + q0 + q) * a.nps + j);
+            acc[q] = cadd(acc[q], cmul(make_double2(e.x * uv, e.y * uv), v));
+          }
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+          acc[q].x += __shfl_xor_sync(0xffffffffu, acc[q].x, off);
+          acc[q].y += __shfl_xor_sync(0xffffffffu, acc[q].y, off);
+        }
+      }
+      if (lane == 0) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+          if (q0 + q < np) Ps[lma0 + q0 + q] = cscal(__ldg(a.rinv + lma0 + q0 + q), acc[q]);
+      }
+    }
+  }
+}
+
+// Nonlocal current pieces sum_lma Im(conj(<r_d zekr|v>) rinv <zekr|v>) of the
+// orbital in shared memory; result reduced over the block into red3[0..2].
+__device__ void current_nonlocal_from_smem(const double2* __restrict__ sm, const OrbArgs& a, int ik,
+                                           double* __restrict__ wsum /* [NT/32][3] */) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const double2* ph = a.phase + (long)ik * a.totpts;
+  double jx = 0.0, jy = 0.0, jz = 0.0;
+  for (int atom = warp; atom < a.natom; atom += NT / 32) {
+    const int start = a.atom_start[atom], m = a.mps[atom];
+    const int lma0 = a.lma_start[atom], np = a.nproj[atom];
+    for (int q = 0; q < np; ++q) {
+      double2 u = make_double2(0.0, 0.0), u0 = u, u1 = u, u2 = u;
+      for (int j = lane; j < m; j += 32) {
+        const double2 v = sm[__ldg(a.pt_lin + start + j)];
+        const double2 e = __ldg(ph + start + j);
+        const double uv = __ldg(a.uv + (long)(lma0 + q) * a.nps + j);
+        const double2 zk = make_double2(e.x * uv, e.y * uv);
+        const double* r = a.pt_r + 3L * (start + j);
+        u = cadd(u, cmul(zk, v));
+        u0 = cadd(u0, cmul(cscal(__ldg(r), zk), v));
+        u1 = cadd(u1, cmul(cscal(__ldg(r + 1), zk), v));
+        u2 = cadd(u2, cmul(cscal(__ldg(r + 2), zk), v));
+      }
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) {
+        u.x += __shfl_xor_sync(0xffffffffu, u.x, off);
+        u.y += __shfl_xor_sync(0xffffffffu, u.y, off);
+        u0.x += __shfl_xor_sync(0xffffffffu, u0.x, off);
+        u0.y += __shfl_xor_sync(0xffffffffu, u0.y, off);
+        u1.x += __shfl_xor_sync(0xffffffffu, u1.x, off);
+        u1.y += __shfl_xor_sync(0xffffffffu, u1.y, off);
+        u2.x += __shfl_xor_sync(0xffffffffu, u2.x, off);
+        u2.y += __shfl_xor_sync(0xffffffffu, u2.y, off);
+      }
+      const double2 us = cscal(__ldg(a.rinv + lma0 + q), u);
+      jx += u0.x * us.y - u0.y * us.x;
+      jy += u1.x * us.y - u1.y * us.x;
+      jz += u2.x * us.y - u2.y * us.x;
+    }
+  }
+  if (lane == 0) {
+    wsum[warp * 3 + 0] = jx;
+    wsum[warp * 3 + 1] = jy;
+    wsum[warp * 3 + 2] = jz;
+  }
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(NT, 2) k_term_orbital(const double2* __restrict__ in, double2* __restrict__ hout,
+                                                        double2* __restrict__ acc, OrbArgs a) {
+  extern __shared__ double2 smem[];
+  double2* sm = smem;            // N planes of N x N
+  double2* Ps = smem + N * NP;   // nlma projections
+  const int o = blockIdx.x;
+  const int t = threadIdx.x;
+  const int tx = t & (N - 1), ty = t >> 4;
+  const int ik = o / a.nspin_no;
+  const int ispin = o % a.nspin;
+  const double* kc = a.kcoef + (long)KC * ik;
+  const double2* src = in + (long)o * a.npts;
+
+  double2 col[N];
+#pragma unroll
+  for (int z = 0; z < N; ++z) col[z] = __ldg(src + z * NP + t);
+#pragma unroll
+  for (int z = 0; z < N; ++z) sm[z * NP + t] = col[z];
+  __syncthreads();
+  if (a.nlma > 0) {
+    project_from_smem(sm, Ps, a, ik);
+    __syncthreads();
+  }
+  const double lap0 = kc[3];
+  double nab[12];
+#pragma unroll
+  for (int q = 0; q < 12; ++q) nab[q] = kc[4 + q];
+  int oxp[ND], oxm[ND], oyp[ND], oym[ND];
+#pragma unroll
+  for (int s = 1; s <= ND; ++s) {
+    oxp[s - 1] = ty * N + ((tx + s) & (N - 1));
+    oxm[s - 1] = ty * N + ((tx - s) & (N - 1));
+    oyp[s - 1] = (((ty + s) & (N - 1)) << 4) + tx;
+    oym[s - 1] = (((ty - s) & (N - 1)) << 4) + tx;
+  }
+  const double* vloc = a.vloc + (long)ispin * a.npts;
+  const double2* ph = a.phase + (long)ik * a.totpts;
+  double2* hdst = hout + (long)o * a.npts;
+  double2* adst = acc + (long)o * a.npts;
+#pragma unroll
+  for (int z = 0; z < N; ++z) {
+    const double2* P = sm + z * NP;
+    double2 vx = make_double2(0.0, 0.0), wx = vx, vy = vx, wy = vx, vz = vx, wz = vx;
+#pragma unroll
+    for (int s = 0; s < ND; ++s) {
+      const double2 tp = P[oxp[s]], tm = P[oxm[s]];
+      vx = cadd(vx, cscal(a.lapt[s], cadd(tp, tm)));
+      wx = cadd(wx, cscal(nab[s], csub(tp, tm)));
+    }
+#pragma unroll
+    for (int s = 0; s < ND; ++s) {
+      const double2 tp = P[oyp[s]], tm = P[oym[s]];
+      vy = cadd(vy, cscal(a.lapt[4 + s], cadd(tp, tm)));
+      wy = cadd(wy, cscal(nab[4 + s], csub(tp, tm)));
+    }
+#pragma unroll
+    for (int s = 0; s < ND; ++s) {
+      const double2 tp = col[(z + s + 1) & (N - 1)], tm = col[(z - s - 1) & (N - 1)];
+      vz = cadd(vz, cscal(a.lapt[8 + s], cadd(tp, tm)));
+      wz = cadd(wz, cscal(nab[8 + s], csub(tp, tm)));
+    }
+    const double2 v = cadd(vz, cadd(vy, vx));
+    const double2 w = cadd(wz, cadd(wy, wx));
+    const double2 c = col[z];
+    const int p = z * NP + t;
+    const double vl = __ldg(vloc + p);
+    double2 h;
+    h.x = vl * c.x + lap0 * c.x - 0.5 * v.x + w.y;
+    h.y = vl * c.y + lap0 * c.y - 0.5 * v.y - w.x;
+    if (a.nlma > 0) {
+      const int vi = __ldg(a.map + p);
+      if (vi >= 0) {
+        const int e1 = __ldg(a.vi_start + vi + 1);
+        for (int e = __ldg(a.vi_start + vi); e < e1; ++e) {
+          const double uv = __ldg(a.ent_uv + e);
+          const double2 phs = __ldg(ph + __ldg(a.ent_pt + e));
+          h = cadd(h, cmul(Ps[__ldg(a.ent_lma + e)], make_double2(phs.x * uv, -phs.y * uv)));
+        }
+      }
+    }
+    if (MODE == 1 || MODE == 2) hdst[p] = h;
+    if (MODE == 1 || MODE == 4) adst[p] = cadd(c, cmul(a.zc, h));
+    else adst[p] = cadd(adst[p], cmul(a.zc, h));
+  }
+  if (MODE != 3 && MODE != 4) return;
+  if (a.obs == nullptr) return;
+  // ---- observables of the new orbital (last Taylor term) ----
+  __shared__ double red[OBS_NQ][NT / 32];
+  __syncthreads();  // all reads of the input planes are done
+  // the new orbital: this thread's own column, just written (program order)
+#pragma unroll
+  for (int z = 0; z < N; ++z) sm[z * NP + t] = adst[z * NP + t];
+  __syncthreads();
+  double q[OBS_NQ];
+#pragma unroll
+  for (int i = 0; i < OBS_NQ; ++i) q[i] = 0.0;
+#pragma unroll 4
+  for (int z = 0; z < N; ++z) {
+    const double2 c = sm[z * NP + t];
+    const double r2 = c.x * c.x + c.y * c.y;
+    q[0] += r2;
+    double ix = 0.0, iy = 0.0, iz = 0.0;
+#pragma unroll
+    for (int s = 1; s <= ND; ++s) {
+      const double2 txv = sm[z * NP + ty * N + ((tx + s) & (N - 1))];
+      const double2 tyv = sm[z * NP + (((ty + s) & (N - 1)) << 4) + tx];
+      const double2 tzv = sm[((z + s) & (N - 1)) * NP + t];
+      ix += a.nab[s - 1] * (c.x * txv.y - c.y * txv.x);
+      iy += a.nab[4 + s - 1] * (c.x * tyv.y - c.y * tyv.x);
+      iz += a.nab[8 + s - 1] * (c.x * tzv.y - c.y * tzv.x);
+    }
+    q[1] += ix;
+    q[2] += iy;
+    q[3] += iz;
+    q[4] += ((double)tx + a.off[0]) * r2;
+    q[5] += ((double)ty + a.off[1]) * r2;
+    q[6] += ((double)z + a.off[2]) * r2;
+  }
+  // warp tree (deterministic), then warps in order
+#pragma unroll
+  for (int i = 0; i < OBS_NQ; ++i) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) q[i] += __shfl_xor_sync(0xffffffffu, q[i], off);
+  }
+  const int warp = t >> 5, lane = t & 31;
+  if (lane == 0)
+    for (int i = 0; i < OBS_NQ; ++i) red[i][warp] = q[i];
+  __shared__ double jws[NT / 32][3];
+  if (a.nlma > 0) current_nonlocal_from_smem(sm, a, ik, &jws[0][0]);
+  __syncthreads();
+  if (t < OBS_NQ) {
+    double s = 0.0;
+    for (int w = 0; w < NT / 32; ++w) s += red[t][w];
+    a.obs[(long)o * OBS_NQ + t] = s;
+  } else if (t >= 32 && t < 35) {
+    double s = 0.0;
+    if (a.nlma > 0)
+      for (int w = 0; w < NT / 32; ++w) s += jws[w][t - 32];
+    a.jw[3L * o + (t - 32)] = s;
+  }
+}
+
+}  // namespace
+
+bool orbital_kernel_applies(const sb200_ctx* c) {
+  const GridInfo& g = c->g;
+  return g.periodic && g.nx == N && g.ny == N && g.nz == N && c->stencil_variant == 1 &&
+         c->pp.nlma <= ORB_MAX_NLMA;
+}
+
+int launch_term_orbital(sb200_ctx* c, const HpsiLaunch& L, bool with_obs) {
+  static bool attr_set = false;
+  const size_t smem = (size_t)N * NP * sizeof(double2) + (size_t)ORB_MAX_NLMA * sizeof(double2);
+  if (!attr_set) {
+    SB_CUDA(cudaFuncSetAttribute(k_term_orbital<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    SB_CUDA(cudaFuncSetAttribute(k_term_orbital<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    SB_CUDA(cudaFuncSetAttribute(k_term_orbital<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    SB_CUDA(cudaFuncSetAttribute(k_term_orbital<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    attr_set = true;
+  }
+  OrbArgs a;
+  a.npts = c->g.npts;
+  a.nspin = c->orb.nspin;
+  a.nspin_no = c->orb.nspin * c->orb.no;
+  a.nlma = c->pp.nlma;
+  a.natom = c->pp.natom;
+  a.nps = c->pp.nps;
+  a.totpts = c->pp.totpts;
+  for (int i = 0; i < 12; ++i) {
+    a.lapt[i] = c->g.coef_lap[i];
+    a.nab[i] = c->g.coef_nab[i];
+  }
+  for (int d = 0; d < 3; ++d) a.off[d] = (double)c->g.is[d] - ((c->g.lg_num[d] % 2 == 1) ? 0.0 : 0.5);
+  a.kcoef = c->d_kcoef;
+  a.vloc = c->d_vloc;
+  a.map = c->pp.d_map;
+  a.vi_start = c->pp.d_vi_start;
+  a.ent_lma = c->pp.d_ent_lma;
+  a.ent_pt = c->pp.d_ent_pt;
+  a.ent_uv = c->pp.d_ent_uv;
+  a.phase = c->pp.d_phase;
+  a.atom_start = c->pp.d_atom_start;
+  a.mps = c->pp.d_mps;
+  a.lma_start = c->pp.d_lma_start;
+  a.nproj = c->pp.d_nproj;
+  a.pt_lin = c->pp.d_pt_lin;
+  a.pt_r = c->pp.d_pt_r;
+  a.uv = c->pp.d_uv;
+  a.rinv = c->pp.d_rinv;
+  a.zc = L.zc;
+  a.obs = with_obs ? c->d_obs : nullptr;
+  a.jw = with_obs ? c->d_jw : nullptr;
+  dim3 grid(c->orb.norb);
+  switch (L.mode) {
+    case 1: k_term_orbital<1><<<grid, NT, smem, c->stream>>>(L.in, L.hout, L.out, a); break;
+    case 2: k_term_orbital<2><<<grid, NT, smem, c->stream>>>(L.in, L.hout, L.out, a); break;
+    case 3: k_term_orbital<3><<<grid, NT, smem, c->stream>>>(L.in, L.hout, L.out, a); break;
+    case 4: k_term_orbital<4><<<grid, NT, smem, c->stream>>>(L.in, L.hout, L.out, a); break;
+    default: return set_error(SB200_ERR_INVALID_ARG, "orbital kernel: unsupported mode");
+  }
+  SB_LAUNCH_CHECK("k_term_orbital");
+  return SB200_OK;
+}
+
+}  // namespace sb200

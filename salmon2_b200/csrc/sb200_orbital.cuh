@@ -1,0 +1,25 @@
+// sb200_orbital.cuh -- argument block of the orbital-resident Taylor-term kernel.
+#pragma once
+#include <cuda_runtime.h>
+
+namespace sb200 {
+
+constexpr int ORB_MAX_NLMA = 1024;  // projections held in shared memory
+
+struct OrbArgs {
+  long npts;
+  int nspin, nspin_no, nlma, natom, nps, totpts;
+  double lapt[12], nab[12], off[3];
+  const double* kcoef;
+  const double* vloc;
+  const int *map, *vi_start, *ent_lma, *ent_pt;
+  const double* ent_uv;
+  const double2* phase;
+  const int *atom_start, *mps, *lma_start, *nproj, *pt_lin;
+  const double *pt_r, *uv, *rinv;
+  double2 zc;
+  double* obs;  // [norb][OBS_NQ] or null
+  double* jw;   // [norb][3] or null
+};
+
+}  // namespace sb200

@@ -151,3 +151,23 @@ def test_error_codes():
     with pytest.raises(SB200Error) as e:
         ctx.hpsi(a, a)  # aliased input / output
     assert e.value.code == 1
+
+
+@pytest.mark.parametrize("trans", ["tr", "lo"])
+def test_rt_propagate_periodic16_orbital_kernel(trans):
+    """16^3 periodic grids take the orbital-resident kernel with the
+    observables fused into the last Taylor term."""
+    from salmon2_b200 import synth
+    sysm = synth.periodic_system(a=10.26, num=16, nkgrid=2, no=2, seed=31, name="periodic16k8")
+    nt, dt = 24, 0.08
+    Ac = synth.asin2cos(nt, dt, omega=0.05696, f0=0.05696 * 2e-2, tw=nt * dt)
+    zc = synth.taylor_zc(dt)
+    O = Oracle(sysm)
+    ref = O.rt_run(sysm.psi, nt, dt, zc, Ac_ext=Ac, trans_longi=1 if trans == "lo" else 0)
+    ctx = _ctx(sysm)
+    a, b, w = ctx.upload(sysm.psi), ctx.zeros(), ctx.zeros()
+    res = ctx.rt_propagate(a, b, w, nt, dt, zc, Ac_ext=Ac, trans_longi=trans)
+    jmax = np.max(np.abs(ref["curr"]))
+    assert np.max(np.abs(res["curr"] - ref["curr"])) <= TOL_OBS * jmax
+    assert S.rel_err(res["rbox"], ref["rbox"]) < TOL_OBS
+    assert S.rel_err(ctx.download(res["psi"]), ref["psi"]) < 1e-11

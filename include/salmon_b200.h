@@ -184,6 +184,38 @@ int sb200_rt_propagate(sb200_ctx* ctx, double* psi_a, double* psi_b, double* wor
                        int trans_longi, double* curr_out, double* rbox_out,
                        double* Ac_tot_out, double** psi_final);
 
+/* ---- H psi without device allocation ---------------------------------------- */
+
+/* No counterpart in the reference.  For callers that cannot allocate device
+ * memory themselves -- hosts whose device arrays belong to another runtime
+ * (OpenACC / OpenMP-offload programs that map their own arrays), memory-capped
+ * or pre-sized environments, and code that must not allocate inside a time
+ * loop -- this computes the same H psi as sb200_hpsi without a context and
+ * without any allocation (no cudaMalloc, cudaFree or allocating library call).
+ * Every array is caller-owned device memory, in the resident orbital layout
+ * for tpsi / htpsi and in the reference's layout for the projector tables:
+ *   V_local (nx*ny*nz, nspin); kAc (3, nk) = vec_k + vec_Ac (periodic only);
+ *   mps(natom), jxyz(3,nps,natom) (grid indices in is..ie), rxyz(3,nps,natom),
+ *   uv(nps,nlma), ia_tbl(nlma) (1-based), rinv_uvu(nlma); host values for
+ *   is[3], coef_lap0, coef_lap(4,3), coef_nab(4,3).  periodic = 0 means the
+ *   zero Dirichlet boundary of an isolated grid.  Work is queued on `stream`
+ *   (a cudaStream_t, NULL for the legacy default stream).
+ * Its only scratch, the projections <beta|psi> of all orbitals, is a fixed
+ * device array inside the library of SB200_NOALLOC_MAX_PROJECTIONS complex
+ * values (4 MiB), held by every GPU that loads the library until the process
+ * exits; norb*nlma above that limit returns SB200_ERR_BAD_SHAPE.  The first
+ * call on each device looks up that array's device address; make the first
+ * call before any stream capture.  All calls share the array and every call
+ * overwrites the entries it uses, so calls whose GPU work overlaps (other
+ * streams, other host threads) race and must be serialised by the caller.    */
+#define SB200_NOALLOC_MAX_PROJECTIONS 262144
+int sb200_hpsi_noalloc(int nx, int ny, int nz, int periodic, int nspin, int no, int nk, const int is[3],
+                       double coef_lap0, const double coef_lap[12], const double coef_nab[12],
+                       const double* kAc, const double* V_local, int natom, int nps, int nlma,
+                       const int* mps, const int* jxyz, const double* rxyz, const double* uv,
+                       const int* ia_tbl, const double* rinv_uvu, const double* tpsi, double* htpsi,
+                       void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -57,6 +57,9 @@ SIGNATURES = {
     "sb200_calc_dip": (C.c_int, [_vp, _vp, _dp]),
     "sb200_rt_propagate": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int, C.c_double, _dp, C.c_int, _dp, C.c_int, _dp,
                                      _dp, _dp, C.POINTER(C.c_void_p)]),
+    "sb200_hpsi_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _ip,
+                                     C.c_double, _dp, _dp, _vp, _vp, C.c_int, C.c_int, C.c_int, _vp, _vp, _vp,
+                                     _vp, _vp, _vp, _vp, _vp, _vp]),
 }
 
 

@@ -54,17 +54,24 @@ def parse():
     ap.add_argument("--cpu-steps", type=int, default=4, help="Taylor steps in each CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--small", action="store_true", help="8 k-points instead of 64 (quick check)")
+    ap.add_argument("--workload", default="bulk", choices=["bulk", "supercell"],
+                    help="bulk: 16^3 x 64 k x 32 orbitals; supercell: its 2x2x2 supercell, 32^3 x 8 k x 256")
     return ap.parse_args()
 
 
 def workload(args, rank=0, world=1):
     from salmon2_b200 import synth
-    nkgrid = 2 if args.small else 4
-    s = synth.periodic_system(a=10.26, num=16, nkgrid=nkgrid, no=32, seed=2, name="periodic_bulk")
+    if args.workload == "supercell":
+        nkgrid = 1 if args.small else 2
+        s = synth.periodic_system(a=10.26, num=16, nkgrid=nkgrid, no=256, supercell=2, seed=3,
+                                  name="periodic_supercell")
+    else:
+        nkgrid = 2 if args.small else 4
+        s = synth.periodic_system(a=10.26, num=16, nkgrid=nkgrid, no=32, seed=2, name="periodic_bulk")
     if world > 1:
         # weak scaling: rank r owns a shifted copy of the k-mesh (a denser
         # mesh overall); J(t) is summed over ranks with weights 1/(nk*world)
-        shift = (2.0 * np.pi / 10.26) * (rank / world) / nkgrid
+        shift = (2.0 * np.pi / (10.26 * (2 if args.workload == "supercell" else 1))) * (rank / world) / nkgrid
         s.vec_k[:] = s.vec_k + shift
         s.wtk[:] = s.wtk / world
     nt = args.nt

@@ -113,6 +113,8 @@ void free_pp(PPInfo& p) {
   dfree(p.d_ent_pt);
   dfree(p.d_ent_uv);
   dfree(p.d_phase);
+  dfree(p.d_pmap);
+  dfree(p.d_ent_zk);
   p = PPInfo();
 }
 
@@ -206,6 +208,29 @@ int issue_taylor(sb200_ctx* c, double2* tin, double2* tout, double2* work, const
       if (nn == 1) L.mode = last ? 4 : 1;
       else L.mode = last ? 3 : 2;
       TIMED(c, SB200_KIND_HPSI, launch_term_orbital(c, L, last && last_with_obs));
+      continue;
+    }
+    if (c->precision == SB200_PREC_MIXED && n_hamil > 1) {
+      // mixed form: term 1 in FP64 (h1 stored as complex64 in the first half
+      // of work), terms n >= 2 in FP32 ping-ponging between the two halves of
+      // work, their sum in an FP32 correction kept in tspsi_in (free after
+      // term 1) and added to psi_out in FP64 by the last term.
+      const long n = c->g.npts * c->orb.norb;
+      float2* w1 = (float2*)work;
+      float2* w2 = (float2*)work + n;
+      float2* corr = (float2*)tin;
+      const void* src = (nn == 1) ? (const void*)tin : (const void*)((nn % 2) == 0 ? w1 : w2);
+      void* dst = (nn % 2) == 1 ? (void*)w1 : (void*)w2;
+      TIMED(c, SB200_KIND_PROJECT, launch_project(c, src, c->d_proj, nn > 1));
+      HpsiLaunch L;
+      L.in = src;
+      L.hout = dst;
+      L.out = tout;
+      L.d32 = corr;
+      L.zc = zc[nn - 1];
+      const bool last = nn == n_hamil;
+      L.mode = (nn == 1) ? 5 : (last ? 8 : (nn == 2 ? 6 : 7));
+      TIMED(c, SB200_KIND_HPSI, launch_hpsi(c, L));
       continue;
     }
     const bool odd = (nn % 2) == 1;
@@ -433,8 +458,10 @@ int sb200_set_orbitals(sb200_ctx* c, int nspin, int no, int nk, const double* ve
   TRY(dalloc(&c->d_kcoef_cur, (size_t)KC * nk));
   if (nk_changed && c->pp.totpts > 0 && c->g.periodic) {
     dfree(c->pp.d_phase);
+    dfree(c->pp.d_ent_zk);
     c->pp.nk_phase = nk;
     TRY(dalloc(&c->pp.d_phase, (size_t)nk * c->pp.totpts));
+    TRY(dalloc(&c->pp.d_ent_zk, (size_t)nk * (c->pp.nent > 0 ? c->pp.nent : 1)));
   }
   TRY(ensure_work(c));
   TRY(refresh_k(c));
@@ -567,9 +594,22 @@ int sb200_set_pp(sb200_ctx* c, int natom, int nps, int nlma, const int* mps, con
   TRY(upload(&p.d_ent_uv, ent_uv));
   p.nk_phase = g.periodic ? c->orb.nk : 1;
   TRY(dalloc(&p.d_phase, (size_t)p.nk_phase * (tot > 0 ? tot : 1)));
+  // packed point map: (first entry << 8) | count
+  std::vector<int> pmap(g.npts, -1);
+  for (int v = 0; v < nvi; ++v) {
+    const int cnt = vi_start[v + 1] - vi_start[v];
+    if (cnt > 255 || vi_start[v] >= (1 << 23))
+      return set_error(SB200_ERR_UNSUPPORTED, "more than 255 projector entries on one grid point");
+    pmap[vi_pt[v]] = (vi_start[v] << 8) | cnt;
+  }
+  TRY(upload(&p.d_pmap, pmap));
+  TRY(dalloc(&p.d_ent_zk, (size_t)p.nk_phase * (nent > 0 ? nent : 1)));
   if (!g.periodic) {  // isolated: zekr_uV = uV (prep_pp.f90:618-619)
     std::vector<double2> one(tot > 0 ? tot : 1, make_double2(1.0, 0.0));
     TRY(upload(&p.d_phase, one));
+    std::vector<double2> zk(nent > 0 ? nent : 1, make_double2(0.0, 0.0));
+    for (int e = 0; e < nent; ++e) zk[e] = make_double2(ent_uv[e], 0.0);
+    SB_CUDA(cudaMemcpy(p.d_ent_zk, zk.data(), zk.size() * sizeof(double2), cudaMemcpyHostToDevice));
   }
   TRY(ensure_work(c));
   TRY(refresh_k(c));

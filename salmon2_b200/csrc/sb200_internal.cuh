@@ -64,6 +64,10 @@ struct PPInfo {
   // projector phases exp(i kAc.r): [nk_phase][totpts]
   double2* d_phase = nullptr;
   int nk_phase = 0;
+  // per grid point: (first entry << 8) | entry count, or -1 outside every sphere
+  int* d_pmap = nullptr;
+  // zekr_uV of every scatter entry for every k: [nk_phase][nent] (k_prep)
+  double2* d_ent_zk = nullptr;
 };
 
 struct RTBuffers {
@@ -151,16 +155,17 @@ void dfree(T*& p) {
 
 // ---- kernel launchers (sb200_kernels.cu) ----
 struct HpsiLaunch {
-  const double2* in;
-  double2* hout;        // may be null when mode == 3
-  double2* out;         // Taylor accumulator (modes 1..3)
+  const void* in;       // double2 (FP64 modes) or float2 (modes 6..8)
+  void* hout;           // double2 (modes 0..2) or float2 (modes 5..7); unused otherwise
+  double2* out;         // FP64 Taylor accumulator psi_out
+  float2* d32 = nullptr;// FP32 correction accumulator of the mixed form
   double2 zc;
   int mode;             // 0: h; 1: h, out = in + zc h; 2: h, out += zc h; 3: out += zc h;
-                        // 4: out = in + zc h (no h store)
+                        // 4: out = in + zc h (no h store); 5..8: mixed form, see sb200_stencil.cu
 };
 int launch_prep_k(sb200_ctx* c, const double* d_A, int a_mode, int itt_from_device,
                   double* d_kcoef, bool phases);
-int launch_project(sb200_ctx* c, const double2* in, double2* proj);
+int launch_project(sb200_ctx* c, const void* in, double2* proj, bool in32 = false);
 int launch_hpsi(sb200_ctx* c, const HpsiLaunch& L);
 int launch_hpsi_tiled(sb200_ctx* c, const HpsiLaunch& L);  // sb200_stencil.cu
 bool orbital_kernel_applies(const sb200_ctx* c);             // sb200_orbital.cu

@@ -45,6 +45,10 @@ struct PrepArgs {
   const double* pt_r;           // [totpts][3]
   double* kcoef;                // [nk][KC]
   double2* phase;               // [nk][totpts] or null
+  int nent;                     // scatter entries (0: none)
+  const int* ent_pt;
+  const double* ent_uv;
+  double2* ent_zk;              // [nk][nent] zekr_uV per entry, or null
 };
 
 __global__ void k_prep(PrepArgs a) {
@@ -80,6 +84,22 @@ __global__ void k_prep(PrepArgs a) {
       a.phase[(long)k * a.totpts + j] = make_double2(c, s);
     }
   }
+  // zekr_uV = conj(exp(i kAc.r)) uV of every scatter entry (same sincos as the phase)
+  if (a.ent_zk != nullptr && a.nent > 0) {
+    const long ne = (long)a.nk * a.nent;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < ne; i += (long)gridDim.x * blockDim.x) {
+      const int k = (int)(i / a.nent);
+      const int e = (int)(i % a.nent);
+      const double* r = a.pt_r + 3L * a.ent_pt[e];
+      double kAc[3];
+      for (int d = 0; d < 3; ++d) kAc[d] = a.vec_k[3 * k + d] + A[d];
+      const double th = kAc[0] * r[0] + kAc[1] * r[1] + kAc[2] * r[2];
+      double s, c;
+      sincos(th, &s, &c);
+      const double uv = a.ent_uv[e];
+      a.ent_zk[i] = make_double2(c * uv, -s * uv);
+    }
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -96,15 +116,15 @@ struct ProjArgs {
   const double2* phase;
 };
 
-template <int NP>
-__global__ void __launch_bounds__(128) k_project(const double2* __restrict__ in, double2* __restrict__ proj,
+template <int NP, typename TIN>
+__global__ void __launch_bounds__(128) k_project(const TIN* __restrict__ in, double2* __restrict__ proj,
                                                  ProjArgs a) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int atom = blockIdx.x * 4 + warp;
   if (atom >= a.natom) return;
   const int o = blockIdx.y;
   const int ik = o / a.nspin_no;
-  const double2* psi = in + (long)o * a.npts;
+  const TIN* psi = in + (long)o * a.npts;
   const int start = a.atom_start[atom], m = a.mps[atom];
   const int lma0 = a.lma_start[atom], np = a.nproj[atom];
   const double2* ph = a.phase + (a.phase_per_k ? (long)ik * a.totpts : 0L) + start;
@@ -113,7 +133,8 @@ __global__ void __launch_bounds__(128) k_project(const double2* __restrict__ in,
 #pragma unroll
     for (int q = 0; q < NP; ++q) acc[q] = make_double2(0.0, 0.0);
     for (int j = lane; j < m; j += 32) {
-      const double2 v = __ldg(psi + a.pt_lin[start + j]);
+      const TIN vi = __ldg(psi + a.pt_lin[start + j]);
+      const double2 v = make_double2((double)vi.x, (double)vi.y);
       const double2 e = __ldg(ph + j);
 #pragma unroll
       for (int q = 0; q < NP; ++q) {
@@ -222,14 +243,13 @@ __global__ void __launch_bounds__(128) k_project_moments(const double2* __restri
 // accumulation of taylor.f90:47-117 fused as an epilogue.
 // ---------------------------------------------------------------------------
 struct HArgs {
-  int nx, ny, nz, periodic, nspin, nspin_no, nlma, totpts, phase_per_k;
+  int nx, ny, nz, periodic, nspin, nspin_no, nlma, nent, phase_per_k;
   long npts;
   double lapt[12];
   const double* kcoef;
   const double* vloc;
-  const int *map, *vi_start, *ent_lma, *ent_pt;
-  const double* ent_uv;
-  const double2* phase;
+  const int *pmap, *ent_lma;
+  const double2* ent_zk;
   const double2* proj;
   double2 zc;
 };
@@ -303,17 +323,12 @@ __global__ void __launch_bounds__(256) k_hpsi(const double2* __restrict__ in, do
   h.y = vl * c.y + lap0 * c.y - 0.5 * v.y - w.x;
 
   if (a.nlma > 0) {
-    const int vi = __ldg(a.map + p);
-    if (vi >= 0) {
-      const int e1 = __ldg(a.vi_start + vi + 1);
+    const int pm = __ldg(a.pmap + p);
+    if (pm >= 0) {
       const double2* pj = a.proj + (long)o * a.nlma;
-      const double2* ph = a.phase + (a.phase_per_k ? (long)ik * a.totpts : 0L);
-      for (int e = __ldg(a.vi_start + vi); e < e1; ++e) {
-        const double uv = __ldg(a.ent_uv + e);
-        const double2 phs = __ldg(ph + __ldg(a.ent_pt + e));
-        const double2 zk = make_double2(phs.x * uv, -phs.y * uv);  // zekr_uV
-        h = cadd(h, cmul(pj[__ldg(a.ent_lma + e)], zk));
-      }
+      const double2* zk = a.ent_zk + (a.phase_per_k ? (long)ik * a.nent : 0L);
+      const int e1 = (pm >> 8) + (pm & 255);
+      for (int e = pm >> 8; e < e1; ++e) h = cadd(h, cmul(pj[__ldg(a.ent_lma + e)], __ldg(zk + e)));
     }
   }
   const long gi = (long)o * a.npts + p;
@@ -566,7 +581,12 @@ int launch_prep_k(sb200_ctx* c, const double* d_A, int a_mode, int itt, double* 
   a.pt_r = c->pp.d_pt_r;
   a.kcoef = d_kcoef;
   a.phase = (phases && c->g.periodic && c->pp.totpts > 0) ? c->pp.d_phase : nullptr;
-  const long items = (long)a.nk * (a.totpts > 0 ? a.totpts : 1);
+  a.nent = c->pp.nent;
+  a.ent_pt = c->pp.d_ent_pt;
+  a.ent_uv = c->pp.d_ent_uv;
+  a.ent_zk = (phases && c->g.periodic && c->pp.nent > 0) ? c->pp.d_ent_zk : nullptr;
+  long items = (long)a.nk * (a.totpts > 0 ? a.totpts : 1);
+  if ((long)a.nk * a.nent > items) items = (long)a.nk * a.nent;
   k_prep<<<grid_for(items, 256), 256, 0, c->stream>>>(a);
   SB_LAUNCH_CHECK("k_prep");
   return SB200_OK;
@@ -593,11 +613,12 @@ static ProjArgs proj_args(sb200_ctx* c) {
   return a;
 }
 
-int launch_project(sb200_ctx* c, const double2* in, double2* proj) {
+int launch_project(sb200_ctx* c, const void* in, double2* proj, bool in32) {
   if (c->pp.nlma == 0) return SB200_OK;
   ProjArgs a = proj_args(c);
   dim3 grid((a.natom + 3) / 4, c->orb.norb);
-  k_project<4><<<grid, 128, 0, c->stream>>>(in, proj, a);
+  if (in32) k_project<4, float2><<<grid, 128, 0, c->stream>>>((const float2*)in, proj, a);
+  else k_project<4, double2><<<grid, 128, 0, c->stream>>>((const double2*)in, proj, a);
   SB_LAUNCH_CHECK("k_project");
   return SB200_OK;
 }
@@ -612,7 +633,9 @@ int launch_project_moments(sb200_ctx* c, const double2* psi) {
 }
 
 int launch_hpsi(sb200_ctx* c, const HpsiLaunch& L) {
-  if (c->stencil_variant == 1) return launch_hpsi_tiled(c, L);
+  if (c->stencil_variant == 1 || L.mode >= 5) return launch_hpsi_tiled(c, L);
+  const double2* IN = (const double2*)L.in;
+  double2* HOUT = (double2*)L.hout;
   HArgs a;
   a.nx = c->g.nx;
   a.ny = c->g.ny;
@@ -621,27 +644,25 @@ int launch_hpsi(sb200_ctx* c, const HpsiLaunch& L) {
   a.nspin = c->orb.nspin;
   a.nspin_no = c->orb.nspin * c->orb.no;
   a.nlma = c->pp.nlma;
-  a.totpts = c->pp.totpts;
+  a.nent = c->pp.nent;
   a.phase_per_k = c->g.periodic;
   a.npts = c->g.npts;
   for (int i = 0; i < 12; ++i) a.lapt[i] = c->g.coef_lap[i];
   a.kcoef = c->d_kcoef;
   a.vloc = c->d_vloc;
-  a.map = c->pp.d_map;
-  a.vi_start = c->pp.d_vi_start;
+  a.pmap = c->pp.d_pmap;
   a.ent_lma = c->pp.d_ent_lma;
-  a.ent_pt = c->pp.d_ent_pt;
-  a.ent_uv = c->pp.d_ent_uv;
-  a.phase = c->pp.d_phase;
+  a.ent_zk = c->pp.d_ent_zk;
   a.proj = c->d_proj;
   a.zc = L.zc;
   dim3 grid((unsigned)((c->g.npts + 255) / 256), c->orb.norb);
   switch (L.mode) {
-    case 0: k_hpsi<0><<<grid, 256, 0, c->stream>>>(L.in, L.hout, L.out, a); break;
-    case 1: k_hpsi<1><<<grid, 256, 0, c->stream>>>(L.in, L.hout, L.out, a); break;
-    case 2: k_hpsi<2><<<grid, 256, 0, c->stream>>>(L.in, L.hout, L.out, a); break;
-    case 3: k_hpsi<3><<<grid, 256, 0, c->stream>>>(L.in, L.hout, L.out, a); break;
-    default: k_hpsi<4><<<grid, 256, 0, c->stream>>>(L.in, L.hout, L.out, a); break;
+    case 0: k_hpsi<0><<<grid, 256, 0, c->stream>>>(IN, HOUT, L.out, a); break;
+    case 1: k_hpsi<1><<<grid, 256, 0, c->stream>>>(IN, HOUT, L.out, a); break;
+    case 2: k_hpsi<2><<<grid, 256, 0, c->stream>>>(IN, HOUT, L.out, a); break;
+    case 3: k_hpsi<3><<<grid, 256, 0, c->stream>>>(IN, HOUT, L.out, a); break;
+    case 4: k_hpsi<4><<<grid, 256, 0, c->stream>>>(IN, HOUT, L.out, a); break;
+    default: return set_error(SB200_ERR_UNSUPPORTED, "per-point hpsi kernel has no mixed-precision modes");
   }
   SB_LAUNCH_CHECK("k_hpsi");
   return SB200_OK;

@@ -157,11 +157,24 @@ __global__ void __launch_bounds__(NT, 2) k_term_orbital(const double2* __restric
     oym[s - 1] = (((ty - s) & (N - 1)) << 4) + tx;
   }
   const double* vloc = a.vloc + (long)ispin * a.npts;
-  const double2* ph = a.phase + (long)ik * a.totpts;
+  const double2* zkk = a.ent_zk + (long)ik * a.nent;
   double2* hdst = hout + (long)o * a.npts;
   double2* adst = acc + (long)o * a.npts;
+  // per-point operands of plane z+1 are loaded while plane z is computed
+  double vl_n = __ldg(vloc + t);
+  int pm_n = a.nlma > 0 ? __ldg(a.pmap + t) : -1;
+  double2 ac_n = make_double2(0.0, 0.0);
+  if (MODE == 2 || MODE == 3) ac_n = adst[t];
 #pragma unroll
   for (int z = 0; z < N; ++z) {
+    const double vl = vl_n;
+    const int pm = pm_n;
+    const double2 ac = ac_n;
+    if (z + 1 < N) {
+      vl_n = __ldg(vloc + (z + 1) * NP + t);
+      if (a.nlma > 0) pm_n = __ldg(a.pmap + (z + 1) * NP + t);
+      if (MODE == 2 || MODE == 3) ac_n = adst[(z + 1) * NP + t];
+    }
     const double2* P = sm + z * NP;
     double2 vx = make_double2(0.0, 0.0), wx = vx, vy = vx, wy = vx, vz = vx, wz = vx;
 #pragma unroll
@@ -186,24 +199,18 @@ __global__ void __launch_bounds__(NT, 2) k_term_orbital(const double2* __restric
     const double2 w = cadd(wz, cadd(wy, wx));
     const double2 c = col[z];
     const int p = z * NP + t;
-    const double vl = __ldg(vloc + p);
     double2 h;
     h.x = vl * c.x + lap0 * c.x - 0.5 * v.x + w.y;
     h.y = vl * c.y + lap0 * c.y - 0.5 * v.y - w.x;
     if (a.nlma > 0) {
-      const int vi = __ldg(a.map + p);
-      if (vi >= 0) {
-        const int e1 = __ldg(a.vi_start + vi + 1);
-        for (int e = __ldg(a.vi_start + vi); e < e1; ++e) {
-          const double uv = __ldg(a.ent_uv + e);
-          const double2 phs = __ldg(ph + __ldg(a.ent_pt + e));
-          h = cadd(h, cmul(Ps[__ldg(a.ent_lma + e)], make_double2(phs.x * uv, -phs.y * uv)));
-        }
+      if (pm >= 0) {
+        const int e1 = (pm >> 8) + (pm & 255);
+        for (int e = pm >> 8; e < e1; ++e) h = cadd(h, cmul(Ps[__ldg(a.ent_lma + e)], __ldg(zkk + e)));
       }
     }
     if (MODE == 1 || MODE == 2) hdst[p] = h;
     if (MODE == 1 || MODE == 4) adst[p] = cadd(c, cmul(a.zc, h));
-    else adst[p] = cadd(adst[p], cmul(a.zc, h));
+    else adst[p] = cadd(ac, cmul(a.zc, h));
   }
   if (MODE != 3 && MODE != 4) return;
   if (a.obs == nullptr) return;
@@ -268,7 +275,7 @@ __global__ void __launch_bounds__(NT, 2) k_term_orbital(const double2* __restric
 bool orbital_kernel_applies(const sb200_ctx* c) {
   const GridInfo& g = c->g;
   return g.periodic && g.nx == N && g.ny == N && g.nz == N && c->stencil_variant == 1 &&
-         c->pp.nlma <= ORB_MAX_NLMA;
+         c->pp.nlma <= ORB_MAX_NLMA && c->precision == SB200_PREC_FP64;
 }
 
 int launch_term_orbital(sb200_ctx* c, const HpsiLaunch& L, bool with_obs) {
@@ -296,11 +303,10 @@ int launch_term_orbital(sb200_ctx* c, const HpsiLaunch& L, bool with_obs) {
   for (int d = 0; d < 3; ++d) a.off[d] = (double)c->g.is[d] - ((c->g.lg_num[d] % 2 == 1) ? 0.0 : 0.5);
   a.kcoef = c->d_kcoef;
   a.vloc = c->d_vloc;
-  a.map = c->pp.d_map;
-  a.vi_start = c->pp.d_vi_start;
+  a.pmap = c->pp.d_pmap;
   a.ent_lma = c->pp.d_ent_lma;
-  a.ent_pt = c->pp.d_ent_pt;
-  a.ent_uv = c->pp.d_ent_uv;
+  a.ent_zk = c->pp.d_ent_zk;
+  a.nent = c->pp.nent;
   a.phase = c->pp.d_phase;
   a.atom_start = c->pp.d_atom_start;
   a.mps = c->pp.d_mps;
@@ -314,11 +320,13 @@ int launch_term_orbital(sb200_ctx* c, const HpsiLaunch& L, bool with_obs) {
   a.obs = with_obs ? c->d_obs : nullptr;
   a.jw = with_obs ? c->d_jw : nullptr;
   dim3 grid(c->orb.norb);
+  const double2* IN = (const double2*)L.in;
+  double2* HOUT = (double2*)L.hout;
   switch (L.mode) {
-    case 1: k_term_orbital<1><<<grid, NT, smem, c->stream>>>(L.in, L.hout, L.out, a); break;
-    case 2: k_term_orbital<2><<<grid, NT, smem, c->stream>>>(L.in, L.hout, L.out, a); break;
-    case 3: k_term_orbital<3><<<grid, NT, smem, c->stream>>>(L.in, L.hout, L.out, a); break;
-    case 4: k_term_orbital<4><<<grid, NT, smem, c->stream>>>(L.in, L.hout, L.out, a); break;
+    case 1: k_term_orbital<1><<<grid, NT, smem, c->stream>>>(IN, HOUT, L.out, a); break;
+    case 2: k_term_orbital<2><<<grid, NT, smem, c->stream>>>(IN, HOUT, L.out, a); break;
+    case 3: k_term_orbital<3><<<grid, NT, smem, c->stream>>>(IN, HOUT, L.out, a); break;
+    case 4: k_term_orbital<4><<<grid, NT, smem, c->stream>>>(IN, HOUT, L.out, a); break;
     default: return set_error(SB200_ERR_INVALID_ARG, "orbital kernel: unsupported mode");
   }
   SB_LAUNCH_CHECK("k_term_orbital");

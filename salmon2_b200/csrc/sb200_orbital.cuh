@@ -8,12 +8,12 @@ constexpr int ORB_MAX_NLMA = 1024;  // projections held in shared memory
 
 struct OrbArgs {
   long npts;
-  int nspin, nspin_no, nlma, natom, nps, totpts;
+  int nspin, nspin_no, nlma, natom, nps, totpts, nent;
   double lapt[12], nab[12], off[3];
   const double* kcoef;
   const double* vloc;
-  const int *map, *vi_start, *ent_lma, *ent_pt;
-  const double* ent_uv;
+  const int *pmap, *ent_lma;
+  const double2* ent_zk;
   const double2* phase;
   const int *atom_start, *mps, *lma_start, *nproj, *pt_lin;
   const double *pt_r, *uv, *rinv;

@@ -5,14 +5,14 @@
 namespace sb200 {
 
 struct TiledArgs {
-  int nx, ny, nz, periodic, nspin, nspin_no, nlma, totpts, phase_per_k, zchunk;
+  int nx, ny, nz, periodic, nspin, nspin_no, nlma, nent, phase_per_k, zchunk;
   long npts;
   double lapt[12];
   const double* kcoef;
   const double* vloc;
-  const int *map, *vi_start, *ent_lma, *ent_pt;
-  const double* ent_uv;
-  const double2* phase;
+  const float* vloc32;
+  const int *pmap, *ent_lma;
+  const double2* ent_zk;
   const double2* proj;
   double2 zc;
 };

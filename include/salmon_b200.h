@@ -41,6 +41,10 @@ extern "C" {
 #define SB200_PREC_FP64 0  /* plain FP64 form                                          */
 #define SB200_PREC_MIXED 1 /* FP32 stencil for Taylor terms n >= 2, FP64 accumulation  */
 
+#define SB200_PRECOND_NONE 0    /* gscg without preconditioner (yn_preconditioning='n')  */
+#define SB200_PRECOND_LOWPASS 1 /* preconditioning_rgk low-pass filter, alpha_pre         */
+#define SB200_PRECOND_LEARNED 2 /* learned 3-D convolutional preconditioner               */
+
 #define SB200_TRANS_TR 0 /* trans_longi = 'tr': no induced field                      */
 #define SB200_TRANS_LO 1 /* trans_longi = 'lo': A_ind from the current                  */
 
@@ -183,6 +187,57 @@ int sb200_rt_propagate(sb200_ctx* ctx, double* psi_a, double* psi_b, double* wor
                        double dt, const double* zc, int n_hamil, const double* Ac_ext,
                        int trans_longi, double* curr_out, double* rbox_out,
                        double* Ac_tot_out, double** psi_final);
+
+/* ---- ground state: real orbitals, one k-point ------------------------------- */
+
+/* The context's orbital block (sb200_set_orbitals with nk = 1) holds real
+ * orbitals psi[o][z][y][x] (double, o = ispin + nspin*io) for these calls.
+ * rwf(is_array:ie_array, nspin, no) in the reference layout <-> device block.  */
+int sb200_gs_from_ref(sb200_ctx* ctx, const double* rwf_ref, double* psi_dev);
+int sb200_gs_to_ref(sb200_ctx* ctx, const double* psi_dev, double* rwf_ref);
+/* htpsi = H tpsi, real orbitals: dstencil + dpseudo.
+ * Replaces: hpsi real branch (src/common/hamiltonian.f90:88-125),
+ * dstencil (src/common/stencil.f90:30-80), dpseudo (src/common/nonlocal_potential.f90:26-171). */
+int sb200_hpsi_real(sb200_ctx* ctx, const double* tpsi, double* htpsi);
+/* ncg iterations of the band-by-band CG with 2x2 Rayleigh-Ritz per orbital;
+ * precondition = SB200_PRECOND_*; esp (host, nspin*no) gets <x|H|x>/<x|x>.
+ * Replaces: gscg_rwf (src/gs/conjugate_gradient.f90:21-466) and
+ * preconditioning_rgk / dstencil_preconditioning (src/gs/preconditioning.f90:25-77). */
+int sb200_gscg(sb200_ctx* ctx, double* psi, int ncg, int precondition, double alpha_pre, double* esp);
+/* Classical column Gram-Schmidt.
+ * Replaces: gram_schmidt_col_real8 (src/gs/gram_schmidt_orth.f90:59-230).          */
+int sb200_gram_schmidt_real(sb200_ctx* ctx, double* psi);
+/* Subspace diagonalisation (nspin = 1); evals (host, no) ascending.
+ * Replaces: ssdg_rwf (src/gs/subspace_diagonalization.f90:62-238) with
+ * eigen_dsyev (src/gs/eigen_subdiag_lapack.f90:23-38).                          */
+int sb200_subspace_diag_real(sb200_ctx* ctx, double* psi, double* evals);
+
+/* ---- learned preconditioner for sb200_gscg ------------------------------------ */
+
+/* A 3-layer 3-D convolutional network (3x3x3 kernels, SB200_LEARNED_CHANNELS
+ * hidden channels, BF16 weights in the forward pass with FP32 accumulation)
+ * maps the normalised residual g/rms(g) and V_local of an orbital to a
+ * correction of the low-pass preconditioner: pre_g = lowpass(g) + rms(g) * y.
+ * It takes the place of preconditioning_rgk (src/gs/conjugate_gradient.f90:427-464)
+ * when sb200_gscg is called with SB200_PRECOND_LEARNED.
+ * Parameters (FP32, SB200_LEARNED_NPARAM): W1(C,2,27) b1(C) W2(C,C,27) b2(C)
+ * W3(1,C,27) b3(1); NULL initialises them to zero (= plain low-pass).
+ * batch = orbitals per network pass (activation buffers are sized for it).   */
+#define SB200_LEARNED_CHANNELS 16
+#define SB200_LEARNED_NPARAM 8241
+int sb200_learned_init(sb200_ctx* ctx, const float* params, int nparam, int batch);
+int sb200_learned_get_params(sb200_ctx* ctx, float* params, int nparam);
+/* Training / checking interfaces on device (or host) float arrays:
+ * x0 (batch, 2, npts) network inputs, offset and target (batch, npts),
+ * y (batch, npts).                                                             */
+int sb200_learned_forward(sb200_ctx* ctx, const float* x0, float* y, int batch);
+/* loss = sum_b 1 - <p,t>^2/(<p,p><t,t>) with p = offset + y (offset may be
+ * NULL); grad (host, NPARAM) may be NULL.                                      */
+int sb200_learned_loss_grad(sb200_ctx* ctx, const float* x0, const float* offset, const float* target,
+                            int batch, double* loss, float* grad);
+/* One Adam step (beta 0.9 / 0.999) with learning rate lr.                     */
+int sb200_learned_train_step(sb200_ctx* ctx, const float* x0, const float* offset, const float* target,
+                             int batch, float lr, double* loss);
 
 /* ---- H psi without device allocation ---------------------------------------- */
 

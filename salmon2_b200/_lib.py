@@ -18,6 +18,8 @@ SB200_OK = 0
 ERROR_NAMES = {1: "INVALID_ARG", 2: "BAD_SHAPE", 3: "UNSUPPORTED", 4: "OOM", 5: "CUDA", 6: "TIMEOUT", 7: "STATE"}
 PREC_FP64, PREC_MIXED = 0, 1
 TRANS_TR, TRANS_LO = 0, 1
+PRECOND_NONE, PRECOND_LOWPASS, PRECOND_LEARNED = 0, 1, 2
+LEARNED_CHANNELS, LEARNED_NPARAM = 16, 8241
 KIND_NAMES = ["prep", "project", "hpsi", "observables", "moments", "finalize", "k6", "k7"]
 
 
@@ -57,6 +59,17 @@ SIGNATURES = {
     "sb200_calc_dip": (C.c_int, [_vp, _vp, _dp]),
     "sb200_rt_propagate": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int, C.c_double, _dp, C.c_int, _dp, C.c_int, _dp,
                                      _dp, _dp, C.POINTER(C.c_void_p)]),
+    "sb200_gs_from_ref": (C.c_int, [_vp, _vp, _vp]),
+    "sb200_gs_to_ref": (C.c_int, [_vp, _vp, _vp]),
+    "sb200_hpsi_real": (C.c_int, [_vp, _vp, _vp]),
+    "sb200_gscg": (C.c_int, [_vp, _vp, C.c_int, C.c_int, C.c_double, _dp]),
+    "sb200_gram_schmidt_real": (C.c_int, [_vp, _vp]),
+    "sb200_subspace_diag_real": (C.c_int, [_vp, _vp, _dp]),
+    "sb200_learned_init": (C.c_int, [_vp, _vp, C.c_int, C.c_int]),
+    "sb200_learned_get_params": (C.c_int, [_vp, _vp, C.c_int]),
+    "sb200_learned_forward": (C.c_int, [_vp, _vp, _vp, C.c_int]),
+    "sb200_learned_loss_grad": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int, _dp, _vp]),
+    "sb200_learned_train_step": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int, C.c_float, _dp]),
     "sb200_hpsi_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _ip,
                                      C.c_double, _dp, _dp, _vp, _vp, C.c_int, C.c_int, C.c_int, _vp, _vp, _vp,
                                      _vp, _vp, _vp, _vp, _vp, _vp]),

@@ -323,6 +323,14 @@ int sb200_ctx_destroy(sb200_ctx* c) {
   dfree(c->rt.d_step);
   dfree(c->rt.d_zc);
   if (c->d_stage) cudaFree(c->d_stage);
+  dfree(c->gs.d_proj);
+  dfree(c->gs.d_part);
+  dfree(c->gs.d_dots);
+  dfree(c->gs.d_coef);
+  dfree(c->gs.d_work);
+  dfree(c->gs.d_gram);
+  dfree(c->gs.d_mat);
+  learned_free(c);
   for (cudaEvent_t e : c->ev) cudaEventDestroy(e);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
   delete c;

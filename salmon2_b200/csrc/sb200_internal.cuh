@@ -81,6 +81,24 @@ struct RTBuffers {
   double2* d_zc = nullptr;      // n_hamil coefficients
 };
 
+// ground-state (real orbital) work state, sb200_gs.cu
+constexpr int CG_NC = 12;  // per-orbital CG coefficients
+enum { CG_XKHXK = 0, CG_GKGK, CG_UK, CG_ZS, CG_SUM, CG_CX, CG_CP, CG_XKXK };
+struct GSState {
+  long n = 0;         // npts * norb of the buffers below
+  int norb = 0, nblk = 0;
+  bool have_work = false;
+  double* d_proj = nullptr;   // [norb][nlma] real projections
+  double* d_part = nullptr;   // [norb][nblk][3] dot partials
+  double* d_dots = nullptr;   // [norb][3]
+  double* d_coef = nullptr;   // [norb][CG_NC]
+  double* d_work = nullptr;   // 7 orbital blocks for the CG
+  double* d_gram = nullptr;   // Gram partials
+  size_t gram_cap = 0;
+  double* d_mat = nullptr;    // small matrices (Gram results, eigenvectors)
+  size_t mat_cap = 0;
+};
+
 }  // namespace sb200
 
 struct sb200_ctx {
@@ -92,6 +110,7 @@ struct sb200_ctx {
   sb200::OrbInfo orb;
   sb200::PPInfo pp;
   sb200::RTBuffers rt;
+  sb200::GSState gs;
   double vec_Ac[3] = {0, 0, 0};
   // device tables
   double* d_vloc = nullptr;     // [nspin][npts]
@@ -117,6 +136,9 @@ struct sb200_ctx {
   int ev_used = 0;
   double kt_ms[SB200_KIND_COUNT] = {0};
   long kt_count[SB200_KIND_COUNT] = {0};
+  // learned preconditioner (sb200_learned.cu)
+  bool learned_set = false;
+  void* learned = nullptr;
 };
 
 namespace sb200 {
@@ -177,5 +199,10 @@ int launch_finalize(sb200_ctx* c, int itt_host, int nt, int trans_longi, double 
 int launch_density(sb200_ctx* c, const double2* psi, double* rho);
 int launch_dip(sb200_ctx* c, const double* rho, double* d_out4);
 int launch_relayout(sb200_ctx* c, const void* src, void* dst, int norb_chunk, bool to_ref);
+// low-pass preconditioner of the ground-state CG (sb200_gs.cu)
+int gs_precond(sb200_ctx* c, const double* g, double* pre, double alpha);
+// learned preconditioner: pre = net(g, V_local) for every orbital (sb200_learned.cu)
+int learned_precond_apply(sb200_ctx* c, const double* g, double* pre);
+void learned_free(sb200_ctx* c);
 
 }  // namespace sb200

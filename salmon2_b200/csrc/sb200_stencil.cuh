@@ -7,7 +7,7 @@ namespace sb200 {
 struct TiledArgs {
   int nx, ny, nz, periodic, nspin, nspin_no, nlma, nent, phase_per_k, zchunk;
   long npts;
-  double lapt[12];
+  double lapt[12], nab[12];  // coef_lap, coef_nab (k+A applied in the kernel)
   const double* kcoef;
   const double* vloc;
   const float* vloc32;

@@ -1,0 +1,308 @@
+// sb200_tiled_body.cuh -- the tiled 2.5-D hpsi sweep as a device function,
+// shared by the per-system kernel (sb200_stencil.cu) and the batched
+// persistent kernel (sb200_batch.cu).  See sb200_stencil.cu for the design.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <type_traits>
+
+#include "sb200_internal.cuh"
+#include "sb200_stencil.cuh"
+
+// resident CTAs per SM the tiled kernel is compiled for (register budget):
+// FP64 stencils keep 2 (no spills), FP32 stencils fit 3
+#ifndef SB200_TILED_MINB64
+#define SB200_TILED_MINB64 2
+#endif
+#ifndef SB200_TILED_MINB32
+#define SB200_TILED_MINB32 3
+#endif
+
+namespace sb200 {
+namespace tiled {
+
+template <typename R>
+struct Cx;
+template <>
+struct Cx<double> {
+  using T = double2;
+  static __device__ __forceinline__ T make(double x, double y) { return make_double2(x, y); }
+};
+template <>
+struct Cx<float> {
+  using T = float2;
+  static __device__ __forceinline__ T make(float x, float y) { return make_float2(x, y); }
+};
+
+template <typename T>
+__device__ __forceinline__ T cadd(T a, T b) {
+  T r;
+  r.x = a.x + b.x;
+  r.y = a.y + b.y;
+  return r;
+}
+template <typename T>
+__device__ __forceinline__ T csub(T a, T b) {
+  T r;
+  r.x = a.x - b.x;
+  r.y = a.y - b.y;
+  return r;
+}
+template <typename T, typename R>
+__device__ __forceinline__ T cscal(R s, T a) {
+  T r;
+  r.x = s * a.x;
+  r.y = s * a.y;
+  return r;
+}
+template <typename T>
+__device__ __forceinline__ T cmul(T a, T b) {
+  T r;
+  r.x = a.x * b.x - a.y * b.y;
+  r.y = a.x * b.y + a.y * b.x;
+  return r;
+}
+
+// wrap (periodic) or test (Dirichlet) a coordinate that may be up to 4 outside
+__device__ __forceinline__ int wrapc(int q, int n, int periodic, bool& ok) {
+  if (periodic) {
+    q = q < 0 ? q + n : (q >= n ? q - n : q);
+    ok = true;
+  } else {
+    ok = (q >= 0) && (q < n);
+  }
+  return q;
+}
+
+template <int MODE>
+struct ModeT {
+  using R = typename std::conditional<(MODE >= 6), float, double>::type;
+  static constexpr bool store_h = (MODE <= 2) || (MODE >= 5 && MODE <= 7);
+  static constexpr bool h32 = (MODE >= 5);  // h stored as complex64
+};
+
+template <int TX, int TY, bool FULL, int MODE>
+__device__ __forceinline__ void tiled_body(const typename Cx<typename ModeT<MODE>::R>::T* __restrict__ in,
+                                           void* __restrict__ hout, double2* __restrict__ acc,
+                                           float2* __restrict__ d32, const TiledArgs& a, const int bx,
+                                           const int by, const int bz) {
+  using R = typename ModeT<MODE>::R;
+  using C2 = typename Cx<R>::T;
+  constexpr int HX = FULL ? 0 : ND;                 // halo width in shared memory
+  constexpr int SX = TX + 2 * HX, SY = TY + 2 * HX;  // staged plane extents
+  constexpr int NT = TX * TY;
+  constexpr int NH0 = (SX * SY - NT + NT - 1) / NT;  // halo cells per thread
+  constexpr int NH = NH0 > 0 ? NH0 : 1;
+  constexpr int HXD = HX > 0 ? HX : 1;              // divisor guard for the full-plane case
+  __shared__ C2 plane[2][SY * SX];
+
+  const int tx = threadIdx.x % TX, ty = threadIdx.x / TX;
+  const int ntx = (a.nx + TX - 1) / TX;
+  const int x0 = (bx % ntx) * TX, y0 = (bx / ntx) * TY;
+  const int x = x0 + tx, y = y0 + ty;
+  const bool active = (x < a.nx) && (y < a.ny);
+  const int zc0 = by * a.zchunk;
+  const int zc1 = min(a.nz, zc0 + a.zchunk);
+  const int o = bz;
+  const long sz = (long)a.nx * a.ny;
+  const C2* src = in + (long)o * a.npts;
+  const int ik = o / a.nspin_no;
+  const int ispin = o % a.nspin;
+  const double* kc = a.kcoef + (long)KC * ik;
+  // k+A factored out of the gradient: w_d = kAc_d * sum_s nab_s (t+ - t-)
+  const R kx = (R)kc[0], ky = (R)kc[1], kz = (R)kc[2], lap0 = (R)kc[3];
+  const int ctr = (ty + HX) * SX + (tx + HX);
+  const long pxy = (long)y * a.nx + x;
+  // column value at any plane index (prefetches run up to 7 planes past the
+  // chunk): periodic wrap by repeated add / subtract, no integer division
+  auto colval = [&](int z) -> C2 {
+    int zz = z;
+    bool ok = true;
+    if (a.periodic) {
+      while (zz < 0) zz += a.nz;
+      while (zz >= a.nz) zz -= a.nz;
+    } else {
+      ok = (z >= 0) && (z < a.nz);
+    }
+    return (ok && active) ? __ldg(src + (long)zz * sz + pxy) : Cx<R>::make(0, 0);
+  };
+  // halo cells owned by this thread (fixed over the sweep): shared-memory slot
+  // and in-plane offset, or -1 when the cell lies outside a Dirichlet grid
+  int hslot[NH];
+  long hoff[NH];
+#pragma unroll
+  for (int k = 0; k < NH; ++k) {
+    hslot[k] = -1;
+    hoff[k] = -1;
+    if (FULL) continue;
+    // enumerate the halo ring in a fixed order and take every NT-th cell
+    const int idx = threadIdx.x + k * NT;
+    if (idx >= SX * SY - NT) continue;
+    int c = idx;  // c-th cell of the ring: rows above/below first, then sides
+    int hx, hy;
+    if (c < HX * SX) {
+      hy = c / SX;
+      hx = c % SX;
+    } else if (c < 2 * HX * SX) {
+      c -= HX * SX;
+      hy = HX + TY + c / SX;
+      hx = c % SX;
+    } else {
+      c -= 2 * HX * SX;
+      hy = HX + c / (2 * HXD);
+      const int side = c % (2 * HXD);
+      hx = side < HX ? side : TX + side;
+    }
+    bool okx, oky;
+    const int gx = wrapc(x0 + hx - HX, a.nx, a.periodic, okx);
+    const int gy = wrapc(y0 + hy - HX, a.ny, a.periodic, oky);
+    hslot[k] = hy * SX + hx;
+    hoff[k] = (okx && oky) ? (long)gy * a.nx + gx : -1;
+  }
+  // in-tile cells past the grid edge hold the wrapped (or zero) neighbours
+  long eoff = -1;
+  if (!active && x < a.nx + ND && y < a.ny + ND) {
+    bool okx, oky;
+    const int gx = wrapc(x, a.nx, a.periodic, okx);
+    const int gy = wrapc(y, a.ny, a.periodic, oky);
+    if (okx && oky) eoff = (long)gy * a.nx + gx;
+  }
+  auto planeval = [&](long off, int z) -> C2 {
+    return (off >= 0) ? __ldg(src + (long)z * sz + off) : Cx<R>::make(0, 0);
+  };
+  // sliding window w[k] = psi(x, y, z - 4 + k); prefetch queue of two planes
+  C2 w[2 * ND + 1];
+#pragma unroll
+  for (int k = 0; k < 2 * ND + 1; ++k) w[k] = colval(zc0 - ND + k);
+  C2 q1 = colval(zc0 + ND + 1);
+  C2 q2 = colval(zc0 + ND + 2);
+  const C2 czc = Cx<R>::make((R)a.zc.x, (R)a.zc.y);
+  // operands of plane z prefetched one plane ahead
+  C2 hq[NH];
+  C2 eq = Cx<R>::make(0, 0);
+#pragma unroll
+  for (int k = 0; k < NH; ++k) hq[k] = planeval(hoff[k], zc0);
+  if (!active) eq = planeval(eoff, zc0);
+  const R* vsrc;
+  if (sizeof(R) == 8) vsrc = (const R*)(a.vloc + (long)ispin * a.npts);
+  else vsrc = (const R*)(a.vloc32 + (long)ispin * a.npts);
+  R vl_n = active ? __ldg(vsrc + (long)zc0 * sz + pxy) : (R)0;
+  int pm_n = (active && a.nlma > 0) ? __ldg(a.pmap + (long)zc0 * sz + pxy) : -1;
+
+  int buf = 0;
+  for (int z = zc0; z < zc1; ++z) {
+    C2* P = plane[buf];
+    if (active) P[ctr] = w[ND];
+    else P[ctr] = eq;
+#pragma unroll
+    for (int k = 0; k < NH; ++k)
+      if (hslot[k] >= 0) P[hslot[k]] = hq[k];
+    const R vl = vl_n;
+    const int pm = pm_n;
+    if (z + 1 < zc1) {  // next plane's halo and per-point operands
+#pragma unroll
+      for (int k = 0; k < NH; ++k) hq[k] = planeval(hoff[k], z + 1);
+      if (!active) eq = planeval(eoff, z + 1);
+      if (active) {
+        vl_n = __ldg(vsrc + (long)(z + 1) * sz + pxy);
+        if (a.nlma > 0) pm_n = __ldg(a.pmap + (long)(z + 1) * sz + pxy);
+      }
+    }
+    __syncthreads();
+    if (active) {
+      C2 vx = Cx<R>::make(0, 0), wx = vx, vy = vx, wy = vx, vz = vx, wz = vx;
+#pragma unroll
+      for (int s = 1; s <= ND; ++s) {
+        int ip, im;
+        if (FULL) {
+          ip = ty * SX + (tx + s) % TX;
+          im = ty * SX + (tx - s + TX) % TX;
+        } else {
+          ip = ctr + s;
+          im = ctr - s;
+        }
+        const C2 tp = P[ip], tm = P[im];
+        vx = cadd(vx, cscal((R)a.lapt[s - 1], cadd(tp, tm)));
+        wx = cadd(wx, cscal((R)a.nab[s - 1], csub(tp, tm)));
+      }
+#pragma unroll
+      for (int s = 1; s <= ND; ++s) {
+        int ip, im;
+        if (FULL) {
+          ip = ((ty + s) % TY) * SX + tx;
+          im = ((ty - s + TY) % TY) * SX + tx;
+        } else {
+          ip = ctr + s * SX;
+          im = ctr - s * SX;
+        }
+        const C2 tp = P[ip], tm = P[im];
+        vy = cadd(vy, cscal((R)a.lapt[4 + s - 1], cadd(tp, tm)));
+        wy = cadd(wy, cscal((R)a.nab[4 + s - 1], csub(tp, tm)));
+      }
+#pragma unroll
+      for (int s = 0; s < ND; ++s) {
+        const C2 tp = w[ND + 1 + s], tm = w[ND - 1 - s];
+        vz = cadd(vz, cscal((R)a.lapt[8 + s], cadd(tp, tm)));
+        wz = cadd(wz, cscal((R)a.nab[8 + s], csub(tp, tm)));
+      }
+      const C2 v = cadd(vz, cadd(vy, vx));
+      const C2 ww = cadd(cscal(kz, wz), cadd(cscal(ky, wy), cscal(kx, wx)));
+      const C2 c = w[ND];
+      const long p = (long)z * sz + pxy;
+      C2 h;
+      h.x = vl * c.x + lap0 * c.x - (R)0.5 * v.x + ww.y;
+      h.y = vl * c.y + lap0 * c.y - (R)0.5 * v.y - ww.x;
+      if (a.nlma > 0 && pm >= 0) {
+        const double2* pj = a.proj + (long)o * a.nlma;
+        const double2* zk = a.ent_zk + (a.phase_per_k ? (long)ik * a.nent : 0L);
+        const int e1 = (pm >> 8) + (pm & 255);
+        for (int e = pm >> 8; e < e1; ++e) {
+          const double2 pv = pj[__ldg(a.ent_lma + e)];
+          const double2 zv = __ldg(zk + e);
+          h = cadd(h, cmul(Cx<R>::make((R)pv.x, (R)pv.y), Cx<R>::make((R)zv.x, (R)zv.y)));
+        }
+      }
+      const long gi = (long)o * a.npts + p;
+      if (ModeT<MODE>::store_h) {
+        if (ModeT<MODE>::h32) ((float2*)hout)[gi] = make_float2((float)h.x, (float)h.y);
+        else ((double2*)hout)[gi] = make_double2((double)h.x, (double)h.y);
+      }
+      if (MODE == 1 || MODE == 4 || MODE == 5) {
+        const double2 cd = make_double2((double)c.x, (double)c.y);
+        const double2 hd = make_double2((double)h.x, (double)h.y);
+        acc[gi] = cadd(cd, cmul(a.zc, hd));
+      } else if (MODE == 2 || MODE == 3) {
+        const double2 hd = make_double2((double)h.x, (double)h.y);
+        acc[gi] = cadd(acc[gi], cmul(a.zc, hd));
+      } else if (MODE == 6) {
+        const C2 t = cmul(czc, h);
+        d32[gi] = make_float2((float)t.x, (float)t.y);
+      } else if (MODE == 7) {
+        const float2 dd = d32[gi];
+        const C2 t = cadd(Cx<R>::make((R)dd.x, (R)dd.y), cmul(czc, h));
+        d32[gi] = make_float2((float)t.x, (float)t.y);
+      } else if (MODE == 8) {
+        const float2 dd = d32[gi];
+        const C2 t = cadd(Cx<R>::make((R)dd.x, (R)dd.y), cmul(czc, h));
+        acc[gi] = cadd(acc[gi], make_double2((double)t.x, (double)t.y));
+      }
+    }
+    // advance the window; the next plane's loads were issued two planes ago
+#pragma unroll
+    for (int k = 0; k < 2 * ND; ++k) w[k] = w[k + 1];
+    w[2 * ND] = q1;
+    q1 = q2;
+    q2 = colval(z + ND + 3);
+    buf ^= 1;
+  }
+}
+
+template <int TX, int TY, bool FULL, int MODE>
+__global__ void __launch_bounds__(TX * TY, (MODE >= 6) ? SB200_TILED_MINB32 : SB200_TILED_MINB64)
+    k_hpsi_tiled(const typename Cx<typename ModeT<MODE>::R>::T* __restrict__ in, void* __restrict__ hout,
+                 double2* __restrict__ acc, float2* __restrict__ d32, TiledArgs a) {
+  tiled_body<TX, TY, FULL, MODE>(in, hout, acc, d32, a, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+}  // namespace tiled
+}  // namespace sb200

@@ -189,3 +189,39 @@ class Context:
                                        _ptr(act), C.byref(fin)))
         final = psi_a if fin.value == psi_a.data_ptr() else psi_b
         return dict(psi=final, curr=curr[:, :nt], rbox=rbox[:, :nt], Ac_tot=act)
+
+    # -- ground state: real orbitals, one k-point ---------------------------------
+    def gs_empty(self):
+        return self.torch.empty(self.shape, dtype=self.torch.float64, device=f"cuda:{self.device}")
+
+    def gs_upload(self, rwf_ref, out=None):
+        out = self.gs_empty() if out is None else out
+        src = np.asfortranarray(rwf_ref, dtype=np.float64)
+        check(lib().sb200_gs_from_ref(self.h, C.c_void_p(src.ctypes.data), C.c_void_p(out.data_ptr())))
+        return out
+
+    def gs_download(self, psi):
+        g = self.sys.grid
+        out = np.zeros(g.shape_array + (self.sys.nspin, self.sys.no, 1), order="F")
+        check(lib().sb200_gs_to_ref(self.h, C.c_void_p(psi.data_ptr()), C.c_void_p(out.ctypes.data)))
+        return out
+
+    def hpsi_real(self, tpsi, htpsi):
+        check(lib().sb200_hpsi_real(self.h, C.c_void_p(tpsi.data_ptr()), C.c_void_p(htpsi.data_ptr())))
+        return htpsi
+
+    def gscg(self, psi, ncg=4, precondition="none", alpha=0.6):
+        mode = {"none": _lib.PRECOND_NONE, "lowpass": _lib.PRECOND_LOWPASS, "learned": _lib.PRECOND_LEARNED}[
+            precondition]
+        esp = np.zeros(self.sys.nspin * self.sys.no)
+        check(lib().sb200_gscg(self.h, C.c_void_p(psi.data_ptr()), int(ncg), mode, float(alpha), _ptr(esp)))
+        return esp
+
+    def gram_schmidt_real(self, psi):
+        check(lib().sb200_gram_schmidt_real(self.h, C.c_void_p(psi.data_ptr())))
+        return psi
+
+    def subspace_diag_real(self, psi):
+        ev = np.zeros(self.sys.no)
+        check(lib().sb200_subspace_diag_real(self.h, C.c_void_p(psi.data_ptr()), _ptr(ev)))
+        return ev

@@ -1,0 +1,79 @@
+"""GPU parity of the ground-state path (real orbitals) against the oracle:
+real hpsi, the CG eigensolver (with and without the low-pass
+preconditioner), classical Gram-Schmidt and the subspace diagonalisation."""
+import functools
+
+import numpy as np
+import pytest
+
+import _systems as S
+from oracle import Oracle
+from salmon2_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+
+@functools.lru_cache(maxsize=None)
+def gs_system():
+    return synth.isolated_system(num=24, no=6, natom=2, seed=41, real=True, name="gs24")
+
+
+def _ctx(s):
+    from salmon2_b200.rt import Context
+    return Context(s)
+
+
+def test_hpsi_real_parity():
+    s = gs_system()
+    O = Oracle(s)
+    ref = O.hpsi_real(s.psi)
+    ctx = _ctx(s)
+    t = ctx.gs_upload(s.psi)
+    h = ctx.gs_empty()
+    ctx.hpsi_real(t, h)
+    assert S.rel_err(ctx.gs_download(h), ref) < 1e-12
+
+
+def test_gs_relayout_round_trip():
+    s = gs_system()
+    ctx = _ctx(s)
+    assert np.array_equal(ctx.gs_download(ctx.gs_upload(s.psi)), s.psi)
+
+
+@pytest.mark.parametrize("pre", ["none", "lowpass"])
+def test_gscg_parity(pre):
+    s = gs_system()
+    O = Oracle(s)
+    psi0 = O.gram_schmidt_real(s.psi)
+    ref, esp_ref = O.gscg(psi0, ncg=4, precondition=(pre == "lowpass"))
+    ctx = _ctx(s)
+    psi = ctx.gs_upload(psi0)
+    esp = ctx.gscg(psi, ncg=4, precondition=pre)
+    np.testing.assert_allclose(esp, esp_ref, rtol=1e-10, atol=1e-12)
+    assert S.rel_err(ctx.gs_download(psi), ref) < 1e-9
+
+
+def test_gram_schmidt_real_parity():
+    s = gs_system()
+    rng = np.random.default_rng(5)
+    psi0 = s.psi + 0.3 * rng.standard_normal(s.psi.shape) * (s.psi != 0)
+    O = Oracle(s)
+    ref = O.gram_schmidt_real(psi0)
+    ctx = _ctx(s)
+    psi = ctx.gs_upload(psi0)
+    ctx.gram_schmidt_real(psi)
+    assert S.rel_err(ctx.gs_download(psi), ref) < 1e-11
+
+
+def test_subspace_diag_parity():
+    s = gs_system()
+    O = Oracle(s)
+    psi0 = O.gram_schmidt_real(s.psi)
+    ref, ev_ref = O.subspace_diag_real(psi0)
+    ctx = _ctx(s)
+    psi = ctx.gs_upload(psi0)
+    ev = ctx.subspace_diag_real(psi)
+    np.testing.assert_allclose(ev, ev_ref, rtol=1e-10, atol=1e-12)
+    got = ctx.gs_download(psi)
+    # eigenvectors are defined up to sign; both sides fix the largest component positive
+    assert S.rel_err(got, ref) < 1e-8

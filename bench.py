@@ -38,7 +38,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-UNIT_BYTES_FP64 = 224.0  # algorithmic bytes per grid-point x orbital Taylor step (FP64 form)
+UNIT_BYTES = {"fp64": 224.0, "mixed": 144.0}  # algorithmic bytes per grid-point x orbital Taylor step
 METRIC = "grid-pt*orbital Taylor steps/s"
 UNIT = "grid-pt*orbital*step/s"
 
@@ -49,13 +49,15 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="native", choices=["native", "reference"])
-    ap.add_argument("--nt", type=int, default=2000, help="Taylor time steps per bench step")
+    ap.add_argument("--nt", type=int, default=None,
+                    help="Taylor time steps per bench step (default 2000; 40 for the batch workload)")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--cpu-steps", type=int, default=4, help="Taylor steps in each CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--small", action="store_true", help="8 k-points instead of 64 (quick check)")
-    ap.add_argument("--workload", default="bulk", choices=["bulk", "supercell"],
-                    help="bulk: 16^3 x 64 k x 32 orbitals; supercell: its 2x2x2 supercell, 32^3 x 8 k x 256")
+    ap.add_argument("--workload", default="bulk", choices=["bulk", "supercell", "batch"],
+                    help="bulk: 16^3 x 64 k x 32 orbitals; supercell: its 2x2x2 supercell, 32^3 x 8 k x 256; "
+                         "batch: 16 isolated systems 32^3..96^3 x 4..64 orbitals in one batch")
     return ap.parse_args()
 
 
@@ -153,9 +155,15 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def ncu_traffic():
-    """DRAM bytes per k_hpsi launch from the committed ncu summary, if any."""
-    p = os.path.join(ROOT, "profiles", "k_hpsi_periodic_bulk.md")
+def orbital_path(s, args):
+    """The one-CTA-per-orbital kernel runs periodic 16^3 grids in FP64."""
+    return s.grid.periodic and tuple(s.grid.shape) == (16, 16, 16) and args.precision == "fp64"
+
+
+def ncu_traffic(kernel, workload):
+    """DRAM bytes per launch of `kernel` on `workload` from the committed ncu
+    summary profiles/<kernel>_<workload>.md, if present."""
+    p = os.path.join(ROOT, "profiles", f"{kernel}_{workload}.md")
     if not os.path.exists(p):
         return None
     for line in open(p):
@@ -204,8 +212,169 @@ def run_reference(args):
     print(json.dumps(out), flush=True)
 
 
+def batch_workload(args):
+    from salmon2_b200 import synth
+    systems = synth.uneven_batch(4 if args.small else 16, seed=4)
+    psi0 = [synth.impulse_kick(s.grid, s.psi, 1e-3) for s in systems]
+    return systems, psi0, 0.05, synth.taylor_zc(0.05)
+
+
+def batch_config(args, systems, nt):
+    units = sum(int(np.prod(s.grid.shape)) * s.norb for s in systems)
+    return {
+        "workload": (f"{len(systems)} independent isolated systems (seed 4), grids "
+                     f"{min(s.grid.shape[0] for s in systems)}^3..{max(s.grid.shape[0] for s in systems)}^3, "
+                     f"{min(s.no for s in systems)}..{max(s.no for s in systems)} complex128 orbitals, "
+                     f"{min(s.pp.natom for s in systems)}..{max(s.pp.natom for s in systems)} atoms, "
+                     f"h=0.25 A, Dirichlet, kick 1e-3 au, dt=0.05 au, {nt} Taylor-4 steps per bench step, "
+                     f"dipole every step, one batch (autotuned tiles)"),
+        "systems": [[int(s.grid.shape[0]), int(s.no), int(s.pp.natom)] for s in systems],
+        "units_per_taylor_step": units, "taylor_steps_per_bench_step": nt, "precision": args.precision,
+        "parallelism": "replicas" if int(os.environ.get("WORLD_SIZE", "1")) > 1 else "single GPU",
+        "l2": "inputs larger than L2 (%.1f GB per orbital array set)" % (units * 16 / 1e9),
+    }
+
+
+def main_batch(args):
+    """Uneven batch: every system advanced by one persistent launch per Taylor
+    term (sb200_batch_propagate), against the same systems run one after the
+    other through their own sb200_rt_propagate."""
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        systems, psi0, dt, zc = batch_workload(args)
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        from oracle import Oracle, lib as olib
+        n = max(1, args.cpu_steps // 2)
+        vals = []
+        for i in range(args.warmup + args.steps):
+            s = systems[i % len(systems)]
+            O = Oracle(s, threads=os.cpu_count() or 1)
+            t0 = time.perf_counter()
+            O.rt_run(psi0[i % len(systems)], n, dt, zc)
+            el = time.perf_counter() - t0
+            if i >= args.warmup:
+                vals.append(int(np.prod(s.grid.shape)) * s.norb * n / el)
+        v = float(np.mean(vals))
+        cb = {"value": v, "unit": UNIT, "cores": int(olib().sbo_get_threads()), "kind": "port",
+              "sample": f"{n} Taylor steps of one system of the batch per bench step (systems in turn)"}
+        print(json.dumps({"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+                          "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
+                          "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+                          "impl": "reference", "config": batch_config(args, systems, args.nt),
+                          "cpu_baseline": cb,
+                          "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}),
+              flush=True)
+        return
+    import torch
+    torch.cuda.set_device(local)
+    from salmon2_b200.rt import Batch, Context
+    systems, psi0, dt, zc = batch_workload(args)
+    nt = args.nt
+    ctxs = [Context(s, device=local, precision=args.precision) for s in systems]
+    stream = torch.cuda.Stream(device=local)
+    for c in ctxs:
+        c.set_stream(stream)
+    A = [c.upload(p) for c, p in zip(ctxs, psi0)]
+    B = [c.zeros() for c in ctxs]
+    W = [c.zeros() for c in ctxs]
+    units = sum(int(np.prod(s.grid.shape)) * s.norb for s in systems) * nt
+    batch = Batch(ctxs)
+    tiles = batch.autotune(A, W, reps=3)
+
+    def timed(fn, k):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(k):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    def batch_step():
+        batch.propagate(A, B, W, nt, dt, zc, rbox=False)
+
+    def solo_step():
+        for c, a, b, w in zip(ctxs, A, B, W):
+            c.rt_propagate(a, b, w, nt, dt, zc)
+
+    for _ in range(args.warmup):
+        batch_step()
+    with Clocks(local) as clk:
+        ms = timed(batch_step, args.steps)
+    value = units * args.steps / (ms / 1e3)
+    solo_step()
+    ms_solo = timed(solo_step, max(1, args.steps // 2))
+    solo_value = units * max(1, args.steps // 2) / (ms_solo / 1e3)
+
+    # e2e through the C ABI with host buffers: upload every system from pinned
+    # reference-layout arrays, propagate the batch, read every psi(t) back
+    host = [torch.from_numpy(np.ascontiguousarray(p.ravel(order="F").view(np.float64))).pin_memory() for p in psi0]
+    back = [torch.empty_like(h).pin_memory() for h in host]
+    bytes_io = sum(h.numel() * 8 for h in host)
+
+    def e2e_step():
+        for c, h, a in zip(ctxs, host, A):
+            c.upload(h, out=a)
+        res = batch.propagate(A, B, W, nt, dt, zc)
+        for c, p, o in zip(ctxs, res["psi"], back):
+            c.download(p, out=o)
+
+    e2e_step()
+    ne = max(1, min(args.steps, 3))
+    ms_e2e = timed(e2e_step, ne)
+    e2e_value = units * ne / (ms_e2e / 1e3)
+
+    # instrumented replay: per-kernel device times through the first context
+    ctxs[0].set_timing(True)
+    ctxs[0].kernel_times(reset=True)
+    nt_i = min(nt, 20)
+    batch.propagate(A, B, W, nt_i, dt, zc, rbox=False)
+    kt = ctxs[0].kernel_times(reset=True)
+    ctxs[0].set_timing(False)
+    peak, peak_kind = measured_peaks()
+    h_ms, h_cnt = kt.get("hpsi", (float("nan"), 1))
+    avg_ms = h_ms / h_cnt
+    bytes_per_launch = UNIT_BYTES[args.precision] / 4.0 * units / nt
+    achieved = bytes_per_launch / (avg_ms / 1e3) / 1e9
+    total_ms = sum(v[0] for v in kt.values())
+    launches_per_tstep = sum(v[1] for v in kt.values()) / nt_i
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f64+f32",
+        "data": "synthetic (seeded; shapes of the uneven-batch configuration)",
+        "config": batch_config(args, systems, nt),
+        "solo_value": solo_value, "batch_over_solo": value / solo_value,
+        "tiles": {"shape": tiles[0].tolist(), "zchunk": tiles[1].tolist()},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": bytes_io,
+                "d2h_bytes_per_step": bytes_io + 4 * nt * 8 * len(systems)},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": ncu_traffic("k_hpsi_batch", "batch"), "peak_source": peak_kind,
+                     "kernel": "k_hpsi_batch", "avg_launch_ms": avg_ms,
+                     "algorithmic_bytes_per_launch": bytes_per_launch},
+        "kernel_shares": {k: round(v[0] / total_ms, 4) for k, v in kt.items()},
+        "gpu_launches": int(round(launches_per_tstep * nt * args.steps)),
+        "clocks": clk.summary(),
+        "cpu_baseline": None,
+    }
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    batch.close()
+    for c in ctxs:
+        c.close()
+
+
 def main():
     args = parse()
+    if args.nt is None:
+        args.nt = 40 if args.workload == "batch" else 2000
+    if args.workload == "batch":
+        return main_batch(args)
     if args.impl == "reference":
         return run_reference(args)
     import torch
@@ -256,8 +425,6 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     ms_max = float(t.item())
     value = units_rank * world * args.steps / (ms_max / 1e3)
-    launches_per_tstep = 1 + 2 * 4 + 3
-    gpu_launches = launches_per_tstep * nt * args.steps
 
     # e2e: host (pinned, reference layout) -> device -> propagate -> host
     host_in = torch.from_numpy(np.ascontiguousarray(s.psi.ravel(order="F").view(np.float64))).pin_memory()
@@ -294,13 +461,16 @@ def main():
     ctx.rt_propagate(a, b, w, nt_i, dt, zc, Ac_ext=Ac[:, : nt_i + 2])
     kt = ctx.kernel_times(reset=True)
     ctx.set_timing(False)
+    launches_per_tstep = sum(v[1] for v in kt.values()) / nt_i
+    gpu_launches = int(round(launches_per_tstep * nt * args.steps))
+    hpsi_kernel = "k_term_orbital" if orbital_path(s, args) else "k_hpsi_tiled"
     peak, peak_kind = measured_peaks()
     h_ms, h_cnt = kt.get("hpsi", (float("nan"), 1))
     units_per_launch = int(np.prod(s.grid.shape)) * s.norb
-    bytes_per_launch = UNIT_BYTES_FP64 / 4.0 * units_per_launch
+    bytes_per_launch = UNIT_BYTES[args.precision] / 4.0 * units_per_launch
     avg_ms = h_ms / h_cnt
     achieved = bytes_per_launch / (avg_ms / 1e3) / 1e9
-    traffic = ncu_traffic()
+    traffic = ncu_traffic(hpsi_kernel, args.workload)
     total_ms = sum(v[0] for v in kt.values())
     shares = {k: round(v[0] / total_ms, 4) for k, v in kt.items()}
 
@@ -318,7 +488,7 @@ def main():
                     "d2h_bytes_per_step": bytes_io + 3 * nt * 8 + 4 * nt * 8},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
-                         "kernel": "k_hpsi", "avg_launch_ms": avg_ms,
+                         "kernel": hpsi_kernel, "avg_launch_ms": avg_ms,
                          "algorithmic_bytes_per_launch": bytes_per_launch},
             "kernel_shares": shares,
             "gpu_launches": gpu_launches,

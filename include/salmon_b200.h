@@ -239,6 +239,39 @@ int sb200_learned_loss_grad(sb200_ctx* ctx, const float* x0, const float* offset
 int sb200_learned_train_step(sb200_ctx* ctx, const float* x0, const float* offset, const float* target,
                              int batch, float lr, double* loss);
 
+/* ---- batches of independent isolated systems ------------------------------- */
+
+/* No single counterpart in the reference, which runs one system per process;
+ * each system here is one fully set-up context (sb200_set_grid, _orbitals,
+ * _vlocal and optionally _pp) of an isolated grid, and a batch advances all of
+ * them together through the loop of sb200_rt_propagate (time_evolution_step,
+ * src/rt/time_evolution_step.f90:102-264, 'tr', no external field): per Taylor
+ * term one launch of the KB projections and one persistent hpsi launch over
+ * the tiles of every system, per step one observable and one final launch,
+ * two steps captured as a CUDA graph.  Every system's results (psi, rbox
+ * history) equal those of its own sb200_rt_propagate.  All contexts must live
+ * on one device with one precision; work runs on the first context's stream.
+ * The batch keeps pointers to the contexts: destroy it before them.          */
+typedef struct sb200_batch sb200_batch;
+#define SB200_TILE_32x8 0
+#define SB200_TILE_16x16 1
+int sb200_batch_create(sb200_ctx* const* systems, int nsys, sb200_batch** out);
+int sb200_batch_destroy(sb200_batch* batch);
+/* Per-system hpsi tiling: shape SB200_TILE_* and z planes per work item.     */
+int sb200_batch_set_tiles(sb200_batch* batch, const int* shape, const int* zchunk);
+int sb200_batch_get_tiles(sb200_batch* batch, int* shape, int* zchunk);
+/* Time every tiling candidate of every system at full occupancy (`reps`
+ * launches each) and keep the fastest; psi[s] is read, work[s] overwritten.
+ * shape_out / zchunk_out (nsys entries each) may be NULL.                    */
+int sb200_batch_autotune(sb200_batch* batch, const double* const* psi, double* const* work, int reps,
+                         int* shape_out, int* zchunk_out);
+/* nt steps of every system: per system s the buffers psi_a[s] (input),
+ * psi_b[s], work[s] as in sb200_rt_propagate; rbox_out[s] (4, nt) host or
+ * device, may be NULL; psi_final[s] receives the buffer holding psi(nt).     */
+int sb200_batch_propagate(sb200_batch* batch, double* const* psi_a, double* const* psi_b, double* const* work,
+                          int nt, double dt, const double* zc, int n_hamil, double* const* rbox_out,
+                          double** psi_final);
+
 /* ---- H psi without device allocation ---------------------------------------- */
 
 /* No counterpart in the reference.  For callers that cannot allocate device

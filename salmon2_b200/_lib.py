@@ -70,6 +70,12 @@ SIGNATURES = {
     "sb200_learned_forward": (C.c_int, [_vp, _vp, _vp, C.c_int]),
     "sb200_learned_loss_grad": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int, _dp, _vp]),
     "sb200_learned_train_step": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int, C.c_float, _dp]),
+    "sb200_batch_create": (C.c_int, [_vp, C.c_int, C.POINTER(C.c_void_p)]),
+    "sb200_batch_destroy": (C.c_int, [_vp]),
+    "sb200_batch_set_tiles": (C.c_int, [_vp, _ip, _ip]),
+    "sb200_batch_get_tiles": (C.c_int, [_vp, _ip, _ip]),
+    "sb200_batch_autotune": (C.c_int, [_vp, _vp, _vp, C.c_int, _ip, _ip]),
+    "sb200_batch_propagate": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int, C.c_double, _dp, C.c_int, _vp, _vp]),
     "sb200_hpsi_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _ip,
                                      C.c_double, _dp, _dp, _vp, _vp, C.c_int, C.c_int, C.c_int, _vp, _vp, _vp,
                                      _vp, _vp, _vp, _vp, _vp, _vp]),

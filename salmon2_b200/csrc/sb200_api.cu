@@ -268,6 +268,12 @@ int issue_rt_step(sb200_ctx* c, double2* in, double2* out, double2* work, const 
 
 }  // namespace
 
+namespace sb200 {
+int rt_alloc(sb200_ctx* c, int nt) { return alloc_rt(c, nt); }
+int kernel_timing_mark(sb200_ctx* c, int kind, bool start) { return timing_mark(c, kind, start); }
+int kernel_timing_flush(sb200_ctx* c) { return timing_flush(c); }
+}  // namespace sb200
+
 extern "C" {
 
 const char* sb200_last_error(void) { return g_last_error.c_str(); }

@@ -1,0 +1,725 @@
+// sb200_batch.cu -- many independent isolated systems of uneven grid, orbital
+// and projector counts advanced together through the real-time loop.
+//
+// Each system keeps its own context (grid, orbitals, V_local, KB tables and
+// histories).  Per Taylor term all systems share
+//   * one launch of the KB projections (one warp per (system, orbital, atom)),
+//   * one persistent hpsi launch: 1-2 CTAs per SM pull work items (a tile x
+//     z-chunk x orbital of some system) from a device work queue, stage that
+//     system's argument block in shared memory and run the tiled 2.5-D sweep
+//     (sb200_tiled_body.cuh) with the system's own tile shape and z-chunk;
+// and per time step one launch of the observable partial sums and one of the
+// final reductions (one CTA per system).  Two time steps are captured as one
+// CUDA graph and replayed.  Tile shape and z-chunk of every system are picked
+// by a measured autotuner (sb200_batch_autotune).
+//
+// The arithmetic of every point is the per-system path's (same device
+// functions, same summation order), so a batched run reproduces each system's
+// own sb200_rt_propagate bit for bit.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstddef>
+#include <cstring>
+#include <numeric>
+#include <vector>
+
+#include "sb200_bodies.cuh"
+#include "sb200_internal.cuh"
+#include "sb200_stencil.cuh"
+#include "sb200_tiled_body.cuh"
+
+namespace sb200 {
+namespace {
+
+using namespace body;
+using namespace tiled;
+
+#define TRY_B(x)                    \
+  do {                              \
+    int _r = (x);                   \
+    if (_r != SB200_OK) return _r;  \
+  } while (0)
+
+constexpr int SHAPE_32x8 = 0;   // 32 x 8 column tiles
+constexpr int SHAPE_16x16 = 1;  // 16 x 16 column tiles
+constexpr int MAX_SYS = 256;    // systems per batch (work-item lookup table in shared memory)
+
+// hpsi work of one system: argument block (zc set per launch) and tiling
+struct BHSys {
+  TiledArgs a;
+  int shape, ntiles, nzc, norb;
+};
+// per-launch buffers of one system
+struct BPtr {
+  const void* in;
+  void* hout;
+  double2* acc;
+  float2* d32;
+};
+struct BPSys {  // projections of one system
+  ProjArgs a;
+  double2* proj;
+};
+struct BOSys {  // observables of one system
+  ObsArgs a;
+  double* part;
+};
+
+// largest s with first[s] <= w (first[] ascending, zero-length systems skipped)
+__device__ __forceinline__ int find_sys(const long* first, int nsys, long w) {
+  int lo = 0, hi = nsys - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (first[mid] <= w) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(256, (MODE >= 6) ? SB200_TILED_MINB32 : SB200_TILED_MINB64)
+    k_hpsi_batch(const BHSys* __restrict__ sys, const long* __restrict__ first, const BPtr* __restrict__ ptr,
+                 int nsys, double2 zc, unsigned int* __restrict__ queue) {
+  using C2 = typename Cx<typename ModeT<MODE>::R>::T;
+  __shared__ TiledArgs sa;
+  __shared__ long sfirst[MAX_SYS + 1];
+  __shared__ long s_w;
+  __shared__ int s_s;
+  if (nsys < 1 || nsys > MAX_SYS) return;  // the host never launches this
+  for (int i = threadIdx.x; i <= nsys; i += blockDim.x) sfirst[i] = first[i];
+  __syncthreads();
+  const long total = sfirst[nsys];
+  constexpr int NW = (int)(offsetof(TiledArgs, zc) / sizeof(int));
+  for (;;) {
+    if (threadIdx.x == 0) {
+      const long w = (long)atomicAdd(queue, 1u);
+      s_w = w;
+      s_s = w < total ? find_sys(sfirst, nsys, w) : -1;
+    }
+    __syncthreads();
+    const long w = s_w;
+    const int s = s_s;
+    if (w >= total) break;
+    {  // stage the system's argument block; zc is the launch's
+      const int* src = (const int*)&sys[s].a;
+      int* dst = (int*)&sa;
+      for (int i = threadIdx.x; i < NW; i += blockDim.x) dst[i] = __ldg(src + i);
+      if (threadIdx.x == 0) sa.zc = zc;
+    }
+    __syncthreads();
+    const int ntiles = __ldg(&sys[s].ntiles), nzc = __ldg(&sys[s].nzc), shape = __ldg(&sys[s].shape);
+    const long l = w - sfirst[s];
+    const long per_o = (long)ntiles * nzc;
+    const int o = (int)(l / per_o);
+    const int r = (int)(l % per_o);
+    const BPtr p = ptr[s];
+    if (shape == SHAPE_32x8)
+      tiled_body<32, 8, false, MODE>((const C2*)p.in, p.hout, p.acc, p.d32, sa, r % ntiles, r / ntiles, o);
+    else
+      tiled_body<16, 16, false, MODE>((const C2*)p.in, p.hout, p.acc, p.d32, sa, r % ntiles, r / ntiles, o);
+    __syncthreads();  // plane buffers and the argument block are reused by the next item
+  }
+  // the last CTA to leave resets the queue for the next launch
+  if (threadIdx.x == 0) {
+    __threadfence();
+    const unsigned int done = atomicAdd(queue + 1, 1u);
+    if (done == gridDim.x - 1) {
+      atomicExch(queue, 0u);
+      atomicExch(queue + 1, 0u);
+    }
+  }
+}
+
+template <typename TIN>
+__global__ void __launch_bounds__(128) k_project_batch(const BPSys* __restrict__ sys, const long* __restrict__ first,
+                                                       const void* const* __restrict__ in, int nsys) {
+  const long w = (long)blockIdx.x * 4 + (threadIdx.x >> 5);
+  if (w >= first[nsys]) return;
+  const int s = find_sys(first, nsys, w);
+  const long l = w - first[s];
+  const int natom = sys[s].a.natom;
+  project_atom<4, TIN>((const TIN*)in[s], sys[s].proj, sys[s].a, (int)(l % natom), (int)(l / natom));
+}
+
+__global__ void __launch_bounds__(OBS_THREADS) k_observables_batch(const BOSys* __restrict__ sys,
+                                                                   const long* __restrict__ first,
+                                                                   const double2* const* __restrict__ psi, int nsys) {
+  const long w = blockIdx.x;
+  const int s = find_sys(first, nsys, w);
+  const long l = w - first[s];
+  const int nblk = sys[s].a.nblk;
+  obs_block(psi[s], sys[s].part, sys[s].a, (int)(l % nblk), (int)(l / nblk));
+}
+
+__global__ void __launch_bounds__(256) k_finalize_batch(const FinArgs* __restrict__ args) {
+  finalize_body(args[blockIdx.x]);
+}
+
+struct Cand {
+  int shape, zchunk;
+};
+
+// host -> device copy ordered before later work on `st` (the streams are non-blocking)
+int h2d(void* d, const void* h, size_t bytes, cudaStream_t st) {
+  SB_CUDA(cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, st));
+  SB_CUDA(cudaStreamSynchronize(st));
+  return SB200_OK;
+}
+
+int ceil_div(int a, int b) { return (a + b - 1) / b; }
+
+int tiles_of(const sb200_ctx* c, int shape) {
+  const int tx = shape == SHAPE_32x8 ? 32 : 16, ty = shape == SHAPE_32x8 ? 8 : 16;
+  return ceil_div(c->g.nx, tx) * ceil_div(c->g.ny, ty);
+}
+
+BHSys hsys_of(const sb200_ctx* c, int shape, int zchunk) {
+  BHSys h;
+  h.a = make_tiled_args(c, make_double2(0.0, 0.0));
+  h.a.zchunk = zchunk;
+  h.shape = shape;
+  h.ntiles = tiles_of(c, shape);
+  h.nzc = ceil_div(c->g.nz, zchunk);
+  h.norb = c->orb.norb;
+  return h;
+}
+
+}  // namespace
+}  // namespace sb200
+
+using namespace sb200;
+
+struct sb200_batch {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int precision = SB200_PREC_FP64;
+  std::vector<sb200_ctx*> sys;
+  std::vector<int> shape, zchunk;
+  std::vector<int> order;  // hpsi queue order of the systems (costliest items first)
+  int nsys = 0;
+  int grid64 = 0, grid32 = 0;  // persistent hpsi grids (FP64 / FP32 stencil modes)
+  unsigned int* d_queue = nullptr;
+  BHSys* d_hsys = nullptr;
+  long* d_hfirst = nullptr;
+  BPSys* d_psys = nullptr;
+  long* d_pfirst = nullptr;
+  BOSys* d_osys = nullptr;
+  long* d_ofirst = nullptr;
+  FinArgs* d_fin = nullptr;
+  long p_total = 0, o_total = 0, h_total = 0;
+  // per-launch pointer tables: [parity][term][nsys] (hpsi in queue order)
+  BPtr* d_hptr = nullptr;
+  const void** d_pin = nullptr;
+  const double2** d_opsi = nullptr;
+  int tab_nh = 0;
+};
+
+namespace {
+
+void batch_free_tables(sb200_batch* b) {
+  dfree(b->d_hptr);
+  dfree(b->d_pin);
+  dfree(b->d_opsi);
+  b->tab_nh = 0;
+}
+
+// hpsi descriptors in queue order (items with the deepest z-chunk first)
+int build_hpsi_tables(sb200_batch* b) {
+  const int n = b->nsys;
+  std::vector<int> ord(n);
+  std::iota(ord.begin(), ord.end(), 0);
+  std::stable_sort(ord.begin(), ord.end(), [&](int x, int y) {
+    return b->zchunk[x] > b->zchunk[y];  // every tile is 256 columns: cost ~ z chunk
+  });
+  b->order = ord;
+  std::vector<BHSys> hs(n);
+  std::vector<long> first(n + 1, 0);
+  for (int i = 0; i < n; ++i) {
+    const int s = ord[i];
+    hs[i] = hsys_of(b->sys[s], b->shape[s], b->zchunk[s]);
+    first[i + 1] = first[i] + (long)hs[i].ntiles * hs[i].nzc * hs[i].norb;
+  }
+  b->h_total = first[n];
+  if (b->h_total >= (1L << 31)) return set_error(SB200_ERR_UNSUPPORTED, "batch: too many hpsi work items");
+  TRY_B(h2d(b->d_hsys, hs.data(), n * sizeof(BHSys), b->stream));
+  TRY_B(h2d(b->d_hfirst, first.data(), (n + 1) * sizeof(long), b->stream));
+  batch_free_tables(b);  // pointer tables follow the queue order
+  return SB200_OK;
+}
+
+int batch_ensure_tables(sb200_batch* b, int n_hamil) {
+  if (b->tab_nh >= n_hamil) return SB200_OK;
+  batch_free_tables(b);
+  TRY_B(dalloc(&b->d_hptr, (size_t)2 * n_hamil * b->nsys));
+  TRY_B(dalloc(&b->d_pin, (size_t)2 * n_hamil * b->nsys));
+  TRY_B(dalloc(&b->d_opsi, (size_t)2 * b->nsys));
+  b->tab_nh = n_hamil;
+  return SB200_OK;
+}
+
+// Taylor-term buffers of the per-system path (issue_taylor): FP64 form
+// ping-pongs tspsi_in / work, the mixed form keeps h as complex64 in the two
+// halves of work and an FP32 correction in tspsi_in.
+void term_buffers(const sb200_ctx* c, int precision, int nn, int n_hamil, double2* tin, double2* tout,
+                  double2* work, BPtr& hp, const void*& pin) {
+  if (precision == SB200_PREC_MIXED && n_hamil > 1) {
+    const long n = c->g.npts * c->orb.norb;
+    float2* w1 = (float2*)work;
+    float2* w2 = (float2*)work + n;
+    const void* src = (nn == 1) ? (const void*)tin : (const void*)((nn % 2) == 0 ? w1 : w2);
+    hp.in = src;
+    hp.hout = (nn % 2) == 1 ? (void*)w1 : (void*)w2;
+    hp.acc = tout;
+    hp.d32 = (float2*)tin;
+    pin = src;
+    return;
+  }
+  const bool odd = (nn % 2) == 1;
+  hp.in = odd ? tin : work;
+  hp.hout = odd ? (void*)work : (void*)tin;
+  hp.acc = tout;
+  hp.d32 = nullptr;
+  pin = hp.in;
+}
+
+int term_mode(int precision, int nn, int n_hamil) {
+  const bool last = nn == n_hamil;
+  if (precision == SB200_PREC_MIXED && n_hamil > 1) return (nn == 1) ? 5 : (last ? 8 : (nn == 2 ? 6 : 7));
+  if (nn == 1) return last ? 4 : 1;
+  return last ? 3 : 2;
+}
+
+template <int MODE>
+void launch_hb(sb200_batch* b, const BHSys* hsys, const long* hfirst, const BPtr* ptr, int nsys, double2 zc,
+               int grid) {
+  k_hpsi_batch<MODE><<<grid, 256, 0, b->stream>>>(hsys, hfirst, ptr, nsys, zc, b->d_queue);
+}
+
+int launch_hpsi_batch(sb200_batch* b, int mode, const BHSys* hsys, const long* hfirst, const BPtr* ptr, int nsys,
+                      double2 zc) {
+  const int grid = mode >= 6 ? b->grid32 : b->grid64;
+  switch (mode) {
+    case 0: launch_hb<0>(b, hsys, hfirst, ptr, nsys, zc, grid); break;
+    case 1: launch_hb<1>(b, hsys, hfirst, ptr, nsys, zc, grid); break;
+    case 2: launch_hb<2>(b, hsys, hfirst, ptr, nsys, zc, grid); break;
+    case 3: launch_hb<3>(b, hsys, hfirst, ptr, nsys, zc, grid); break;
+    case 4: launch_hb<4>(b, hsys, hfirst, ptr, nsys, zc, grid); break;
+    case 5: launch_hb<5>(b, hsys, hfirst, ptr, nsys, zc, grid); break;
+    case 6: launch_hb<6>(b, hsys, hfirst, ptr, nsys, zc, grid); break;
+    case 7: launch_hb<7>(b, hsys, hfirst, ptr, nsys, zc, grid); break;
+    case 8: launch_hb<8>(b, hsys, hfirst, ptr, nsys, zc, grid); break;
+    default: return set_error(SB200_ERR_INVALID_ARG, "batch hpsi: unknown mode");
+  }
+  SB_LAUNCH_CHECK("k_hpsi_batch");
+  return SB200_OK;
+}
+
+template <int MODE>
+int occupancy_grid(int* grid) {
+  int dev = 0, sms = 0, nb = 0;
+  SB_CUDA(cudaGetDevice(&dev));
+  SB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  SB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_hpsi_batch<MODE>, 256, 0));
+  if (nb < 1) nb = 1;
+  *grid = sms * nb;
+  return SB200_OK;
+}
+
+// one time step of every system: psi(A) -> psi(B) (parity 0) or back (1)
+#define TIMED_B(c, kind, call)                  \
+  do {                                          \
+    TRY_B(kernel_timing_mark((c), (kind), true));  \
+    TRY_B(call);                                \
+    TRY_B(kernel_timing_mark((c), (kind), false)); \
+  } while (0)
+
+int launch_project_batch(sb200_batch* b, bool in32, size_t t) {
+  const unsigned g = (unsigned)((b->p_total + 3) / 4);
+  if (in32) k_project_batch<float2><<<g, 128, 0, b->stream>>>(b->d_psys, b->d_pfirst, b->d_pin + t, b->nsys);
+  else k_project_batch<double2><<<g, 128, 0, b->stream>>>(b->d_psys, b->d_pfirst, b->d_pin + t, b->nsys);
+  SB_LAUNCH_CHECK("k_project_batch");
+  return SB200_OK;
+}
+
+int launch_obs_final_batch(sb200_batch* b, int parity, int which) {
+  if (which == 0) {
+    k_observables_batch<<<(unsigned)b->o_total, OBS_THREADS, 0, b->stream>>>(
+        b->d_osys, b->d_ofirst, b->d_opsi + (size_t)parity * b->nsys, b->nsys);
+    SB_LAUNCH_CHECK("k_observables_batch");
+  } else {
+    k_finalize_batch<<<b->nsys, 256, 0, b->stream>>>(b->d_fin);
+    SB_LAUNCH_CHECK("k_finalize_batch");
+  }
+  return SB200_OK;
+}
+
+// one time step of every system: psi(A) -> psi(B) (parity 0) or back (1).
+// Kernel times go to the first system's context when its timing is on.
+int issue_batch_step(sb200_batch* b, int parity, const double2* zc, int n_hamil) {
+  const int n = b->nsys;
+  sb200_ctx* c0 = b->sys[0];
+  for (int nn = 1; nn <= n_hamil; ++nn) {
+    const size_t t = ((size_t)parity * n_hamil + (nn - 1)) * n;
+    const int mode = term_mode(b->precision, nn, n_hamil);
+    if (b->p_total > 0) TIMED_B(c0, SB200_KIND_PROJECT, launch_project_batch(b, mode >= 6, t));
+    TIMED_B(c0, SB200_KIND_HPSI, launch_hpsi_batch(b, mode, b->d_hsys, b->d_hfirst, b->d_hptr + t, n, zc[nn - 1]));
+  }
+  TIMED_B(c0, SB200_KIND_OBS, launch_obs_final_batch(b, parity, 0));
+  TIMED_B(c0, SB200_KIND_FINAL, launch_obs_final_batch(b, parity, 1));
+  return SB200_OK;
+}
+
+std::vector<Cand> candidates(const sb200_ctx* c) {
+  std::vector<Cand> v;
+  const int nz = c->g.nz;
+  for (int shape = 0; shape < 2; ++shape) {
+    if (shape == SHAPE_32x8 && c->g.nx <= 16) continue;
+    for (int div = 1; div <= 8; div *= 2) {
+      const int zc = ceil_div(nz, div);
+      if (div > 1 && zc < 8) break;
+      v.push_back({shape, zc});
+    }
+  }
+  return v;
+}
+
+}  // namespace
+
+extern "C" {
+
+int sb200_batch_create(sb200_ctx* const* systems, int nsys, sb200_batch** out) {
+  if (!out) return set_error(SB200_ERR_INVALID_ARG, "null out pointer");
+  *out = nullptr;
+  if (!systems || nsys < 1 || nsys > MAX_SYS)
+    return set_error(SB200_ERR_INVALID_ARG, "sb200_batch_create: 1..256 systems required");
+  sb200_ctx* c0 = systems[0];
+  for (int s = 0; s < nsys; ++s) {
+    sb200_ctx* c = systems[s];
+    if (!c) return set_error(SB200_ERR_INVALID_ARG, "null system context");
+    if (!c->g.set || !c->orb.set || !c->vloc_set)
+      return set_error(SB200_ERR_STATE, "every system needs its grid, orbitals and V_local set");
+    if (c->g.periodic) return set_error(SB200_ERR_UNSUPPORTED, "batched propagation covers isolated systems");
+    if (c->device != c0->device) return set_error(SB200_ERR_INVALID_ARG, "systems on different devices");
+    if (c->precision != c0->precision) return set_error(SB200_ERR_INVALID_ARG, "systems with different precision");
+    for (int t = 0; t < s; ++t)
+      if (systems[t] == c) return set_error(SB200_ERR_INVALID_ARG, "a system appears twice in the batch");
+  }
+  int prev = -1;
+  cudaGetDevice(&prev);
+  cudaSetDevice(c0->device);
+  sb200_batch* b = new sb200_batch();
+  b->device = c0->device;
+  b->stream = c0->stream;
+  b->precision = c0->precision;
+  b->sys.assign(systems, systems + nsys);
+  b->nsys = nsys;
+  b->shape.resize(nsys);
+  b->zchunk.resize(nsys);
+  for (int s = 0; s < nsys; ++s) {  // untuned default: the per-system path's tile, whole z sweeps
+    b->shape[s] = systems[s]->g.nx <= 16 ? SHAPE_16x16 : SHAPE_32x8;
+    b->zchunk[s] = systems[s]->g.nz;
+  }
+  auto fail = [&](int rc) {
+    sb200_batch_destroy(b);
+    if (prev >= 0) cudaSetDevice(prev);
+    return rc;
+  };
+  int rc = SB200_OK;
+  if ((rc = occupancy_grid<1>(&b->grid64)) != SB200_OK) return fail(rc);
+  if ((rc = occupancy_grid<7>(&b->grid32)) != SB200_OK) return fail(rc);
+  if ((rc = dalloc(&b->d_queue, 2)) != SB200_OK) return fail(rc);
+  const unsigned int zq[2] = {0u, 0u};
+  if ((rc = h2d(b->d_queue, zq, sizeof(zq), b->stream)) != SB200_OK) return fail(rc);
+  if ((rc = dalloc(&b->d_hsys, nsys)) != SB200_OK) return fail(rc);
+  if ((rc = dalloc(&b->d_hfirst, nsys + 1)) != SB200_OK) return fail(rc);
+  if ((rc = dalloc(&b->d_psys, nsys)) != SB200_OK) return fail(rc);
+  if ((rc = dalloc(&b->d_pfirst, nsys + 1)) != SB200_OK) return fail(rc);
+  if ((rc = dalloc(&b->d_osys, nsys)) != SB200_OK) return fail(rc);
+  if ((rc = dalloc(&b->d_ofirst, nsys + 1)) != SB200_OK) return fail(rc);
+  if ((rc = dalloc(&b->d_fin, nsys)) != SB200_OK) return fail(rc);
+  // projection and observable descriptors (natural order)
+  std::vector<BPSys> ps(nsys);
+  std::vector<BOSys> os(nsys);
+  std::vector<long> pf(nsys + 1, 0), of(nsys + 1, 0);
+  for (int s = 0; s < nsys; ++s) {
+    const sb200_ctx* c = systems[s];
+    ps[s].a = make_proj_args(c);
+    ps[s].proj = c->d_proj;
+    const long np = c->pp.nlma > 0 ? (long)c->orb.norb * c->pp.natom : 0;
+    pf[s + 1] = pf[s] + np;
+    os[s].a = make_obs_args(c);
+    os[s].part = c->d_obs;
+    of[s + 1] = of[s] + (long)c->orb.norb * c->obs_blocks;
+  }
+  b->p_total = pf[nsys];
+  b->o_total = of[nsys];
+  if (b->o_total >= (1L << 31) || b->p_total >= (1L << 33)) return fail(set_error(SB200_ERR_UNSUPPORTED, "batch too large"));
+  if ((rc = h2d(b->d_psys, ps.data(), nsys * sizeof(BPSys), b->stream)) != SB200_OK ||
+      (rc = h2d(b->d_pfirst, pf.data(), (nsys + 1) * sizeof(long), b->stream)) != SB200_OK ||
+      (rc = h2d(b->d_osys, os.data(), nsys * sizeof(BOSys), b->stream)) != SB200_OK ||
+      (rc = h2d(b->d_ofirst, of.data(), (nsys + 1) * sizeof(long), b->stream)) != SB200_OK)
+    return fail(rc);
+  if ((rc = build_hpsi_tables(b)) != SB200_OK) return fail(rc);
+  if (prev >= 0) cudaSetDevice(prev);
+  *out = b;
+  return SB200_OK;
+}
+
+int sb200_batch_destroy(sb200_batch* b) {
+  if (!b) return SB200_OK;
+  int prev = -1;
+  cudaGetDevice(&prev);
+  cudaSetDevice(b->device);
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  batch_free_tables(b);
+  dfree(b->d_queue);
+  dfree(b->d_hsys);
+  dfree(b->d_hfirst);
+  dfree(b->d_psys);
+  dfree(b->d_pfirst);
+  dfree(b->d_osys);
+  dfree(b->d_ofirst);
+  dfree(b->d_fin);
+  delete b;
+  if (prev >= 0) cudaSetDevice(prev);
+  return SB200_OK;
+}
+
+int sb200_batch_set_tiles(sb200_batch* b, const int* shape, const int* zchunk) {
+  if (!b || !shape || !zchunk) return set_error(SB200_ERR_INVALID_ARG, "bad argument");
+  for (int s = 0; s < b->nsys; ++s) {
+    if (shape[s] != SHAPE_32x8 && shape[s] != SHAPE_16x16)
+      return set_error(SB200_ERR_INVALID_ARG, "tile shape must be 0 (32x8) or 1 (16x16)");
+    if (zchunk[s] < 1 || zchunk[s] > b->sys[s]->g.nz) return set_error(SB200_ERR_INVALID_ARG, "z chunk out of range");
+  }
+  int prev = -1;
+  cudaGetDevice(&prev);
+  cudaSetDevice(b->device);
+  SB_CUDA(cudaStreamSynchronize(b->stream));
+  b->shape.assign(shape, shape + b->nsys);
+  b->zchunk.assign(zchunk, zchunk + b->nsys);
+  const int rc = build_hpsi_tables(b);
+  if (prev >= 0) cudaSetDevice(prev);
+  return rc;
+}
+
+int sb200_batch_get_tiles(sb200_batch* b, int* shape, int* zchunk) {
+  if (!b || !shape || !zchunk) return set_error(SB200_ERR_INVALID_ARG, "bad argument");
+  for (int s = 0; s < b->nsys; ++s) {
+    shape[s] = b->shape[s];
+    zchunk[s] = b->zchunk[s];
+  }
+  return SB200_OK;
+}
+
+// Measured choice of tile shape and z chunk per system: every candidate runs
+// the batch hpsi kernel on a work list that holds the system `R` times (R
+// chosen to give >= 4 waves of the persistent grid), so each candidate is
+// timed at full occupancy; the cheapest time per grid point x orbital wins.
+// psi[s] is read and work[s] overwritten (both orbital blocks of system s).
+int sb200_batch_autotune(sb200_batch* b, const double* const* psi, double* const* work, int reps, int* shape_out,
+                         int* zchunk_out) {
+  if (!b || !psi || !work) return set_error(SB200_ERR_INVALID_ARG, "bad argument");
+  if (reps < 1) reps = 1;
+  for (int s = 0; s < b->nsys; ++s)
+    if (!psi[s] || !work[s] || (const void*)psi[s] == (const void*)work[s])
+      return set_error(SB200_ERR_INVALID_ARG, "autotune needs distinct psi and work buffers per system");
+  int prev = -1;
+  cudaGetDevice(&prev);
+  cudaSetDevice(b->device);
+  b->stream = b->sys[0]->stream;
+  const bool mixed = b->precision == SB200_PREC_MIXED;
+  const int mode = mixed ? 7 : 0;  // stencil of the inner Taylor terms
+  const int grid = mixed ? b->grid32 : b->grid64;
+  const long want = 4L * grid;
+  const int RMAX = MAX_SYS;  // replicas share the kernel's per-system lookup table
+  BHSys* d_rep = nullptr;
+  long* d_rf = nullptr;
+  BPtr* d_rp = nullptr;
+  int rc = SB200_OK;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  auto cleanup = [&]() {
+    dfree(d_rep);
+    dfree(d_rf);
+    dfree(d_rp);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (prev >= 0) cudaSetDevice(prev);
+  };
+  if ((rc = dalloc(&d_rep, RMAX)) != SB200_OK || (rc = dalloc(&d_rf, RMAX + 1)) != SB200_OK ||
+      (rc = dalloc(&d_rp, RMAX)) != SB200_OK) {
+    cleanup();
+    return rc;
+  }
+  if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+    cleanup();
+    return cuda_error(cudaGetLastError(), "cudaEventCreate");
+  }
+  std::vector<BHSys> rep;
+  std::vector<long> rf;
+  std::vector<BPtr> rp;
+  for (int s = 0; s < b->nsys && rc == SB200_OK; ++s) {
+    sb200_ctx* c = b->sys[s];
+    const long n = c->g.npts * c->orb.norb;
+    // FP64 form: mode 0 (h only); mixed form: mode 7 (FP32 input in the first
+    // half of psi, h and the correction in the two halves of work)
+    BPtr p;
+    p.in = psi[s];
+    p.hout = work[s];
+    p.acc = nullptr;
+    p.d32 = mixed ? (float2*)work[s] + n : nullptr;
+    double best = 1e300;
+    Cand bc = {b->shape[s], b->zchunk[s]};
+    for (const Cand& cd : candidates(c)) {
+      BHSys h = hsys_of(c, cd.shape, cd.zchunk);
+      const long items = (long)h.ntiles * h.nzc * h.norb;
+      int R = (int)std::min<long>(RMAX, std::max<long>(1, (want + items - 1) / items));
+      if ((long)R * items >= (1L << 31)) R = (int)((1L << 31) / items - 1);
+      rep.assign(R, h);
+      rf.resize(R + 1);
+      for (int i = 0; i <= R; ++i) rf[i] = (long)i * items;
+      rp.assign(R, p);
+      if ((rc = h2d(d_rep, rep.data(), R * sizeof(BHSys), b->stream)) != SB200_OK ||
+          (rc = h2d(d_rf, rf.data(), (R + 1) * sizeof(long), b->stream)) != SB200_OK ||
+          (rc = h2d(d_rp, rp.data(), R * sizeof(BPtr), b->stream)) != SB200_OK)
+        break;
+      const double2 zc = make_double2(0.0, -1e-3);
+      if ((rc = launch_hpsi_batch(b, mode, d_rep, d_rf, d_rp, R, zc)) != SB200_OK) break;
+      cudaEventRecord(e0, b->stream);
+      for (int i = 0; i < reps && rc == SB200_OK; ++i) rc = launch_hpsi_batch(b, mode, d_rep, d_rf, d_rp, R, zc);
+      cudaEventRecord(e1, b->stream);
+      if (rc != SB200_OK) break;
+      if (cudaEventSynchronize(e1) != cudaSuccess) {
+        rc = cuda_error(cudaGetLastError(), "autotune launch");
+        break;
+      }
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      const double cost = ms / ((double)reps * R * (double)n);
+      if (cost < best) {
+        best = cost;
+        bc = cd;
+      }
+    }
+    b->shape[s] = bc.shape;
+    b->zchunk[s] = bc.zchunk;
+  }
+  if (rc == SB200_OK) rc = build_hpsi_tables(b);
+  if (rc == SB200_OK && shape_out && zchunk_out) rc = sb200_batch_get_tiles(b, shape_out, zchunk_out);
+  cleanup();
+  return rc;
+}
+
+int sb200_batch_propagate(sb200_batch* b, double* const* psi_a, double* const* psi_b, double* const* work, int nt,
+                          double dt, const double* zc, int n_hamil, double* const* rbox_out, double** psi_final) {
+  if (!b || !psi_a || !psi_b || !work || !zc || nt < 0 || n_hamil < 1 || n_hamil > 16)
+    return set_error(SB200_ERR_INVALID_ARG, "sb200_batch_propagate: bad argument");
+  const int n = b->nsys;
+  for (int s = 0; s < n; ++s) {
+    if (!psi_a[s] || !psi_b[s] || !work[s]) return set_error(SB200_ERR_INVALID_ARG, "null orbital buffer");
+    if (psi_a[s] == psi_b[s] || psi_a[s] == work[s] || psi_b[s] == work[s])
+      return set_error(SB200_ERR_INVALID_ARG, "orbital buffers must be distinct");
+    if (b->sys[s]->precision != b->precision)
+      return set_error(SB200_ERR_STATE, "a system's precision changed after sb200_batch_create");
+  }
+  int prev = -1;
+  cudaGetDevice(&prev);
+  cudaSetDevice(b->device);
+  struct Restore {
+    int p;
+    ~Restore() {
+      if (p >= 0) cudaSetDevice(p);
+    }
+  } restore{prev};
+  // per-system state: histories, step counter, k coefficients (A = 0)
+  b->stream = b->sys[0]->stream;
+  std::vector<FinArgs> fin(n);
+  const double zero3[3] = {0.0, 0.0, 0.0};
+  const int one = 1;
+  for (int s = 0; s < n; ++s) {
+    sb200_ctx* c = b->sys[s];
+    SB_CUDA(cudaStreamSynchronize(c->stream));
+    TRY_B(rt_alloc(c, nt));
+    SB_CUDA(cudaMemcpyAsync(c->rt.d_step, &one, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    SB_CUDA(cudaMemcpyAsync(c->d_result + 8, zero3, 3 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    TRY_B(launch_prep_k(c, c->d_result + 8, 0, 0, c->d_kcoef, false));
+    SB_CUDA(cudaStreamSynchronize(c->stream));
+    fin[s] = make_fin_args(c, -1, SB200_TRANS_TR, dt, -1, false);
+  }
+  TRY_B(h2d(b->d_fin, fin.data(), n * sizeof(FinArgs), b->stream));
+  // pointer tables of both parities
+  TRY_B(batch_ensure_tables(b, n_hamil));
+  std::vector<BPtr> hp((size_t)2 * n_hamil * n);
+  std::vector<const void*> pin((size_t)2 * n_hamil * n);
+  std::vector<const double2*> opsi((size_t)2 * n);
+  for (int parity = 0; parity < 2; ++parity)
+    for (int s = 0; s < n; ++s) {
+      double2* tin = (double2*)(parity == 0 ? psi_a[s] : psi_b[s]);
+      double2* tout = (double2*)(parity == 0 ? psi_b[s] : psi_a[s]);
+      opsi[(size_t)parity * n + s] = tout;
+      for (int nn = 1; nn <= n_hamil; ++nn) {
+        BPtr p;
+        const void* pi;
+        term_buffers(b->sys[s], b->precision, nn, n_hamil, tin, tout, (double2*)work[s], p, pi);
+        const size_t t = ((size_t)parity * n_hamil + (nn - 1)) * n;
+        pin[t + s] = pi;
+        // hpsi table in queue order
+        const int q = (int)(std::find(b->order.begin(), b->order.end(), s) - b->order.begin());
+        hp[t + q] = p;
+      }
+    }
+  TRY_B(h2d(b->d_hptr, hp.data(), hp.size() * sizeof(BPtr), b->stream));
+  TRY_B(h2d(b->d_pin, pin.data(), pin.size() * sizeof(void*), b->stream));
+  TRY_B(h2d(b->d_opsi, opsi.data(), opsi.size() * sizeof(void*), b->stream));
+  std::vector<double2> z(n_hamil);
+  for (int i = 0; i < n_hamil; ++i) z[i] = make_double2(zc[2 * i], zc[2 * i + 1]);
+
+  // two steps (A -> B -> A) as one CUDA graph; instrumented runs (timing on
+  // the first context) launch step by step instead
+  const bool timing = b->sys[0]->timing;
+  const int pairs = timing ? 0 : nt / 2;
+  int rc = SB200_OK;
+  if (timing) {
+    for (int i = 0; i + 1 < nt; i += 2) {
+      TRY_B(issue_batch_step(b, 0, z.data(), n_hamil));
+      TRY_B(issue_batch_step(b, 1, z.data(), n_hamil));
+      TRY_B(kernel_timing_flush(b->sys[0]));
+    }
+  }
+  if (pairs > 0) {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    SB_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    rc = issue_batch_step(b, 0, z.data(), n_hamil);
+    if (rc == SB200_OK) rc = issue_batch_step(b, 1, z.data(), n_hamil);
+    cudaError_t e = cudaStreamEndCapture(b->stream, &graph);
+    if (rc != SB200_OK) {
+      if (graph) cudaGraphDestroy(graph);
+      return rc;
+    }
+    if (e != cudaSuccess) return cuda_error(e, "cudaStreamEndCapture");
+    e = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return cuda_error(e, "cudaGraphInstantiate");
+    for (int i = 0; i < pairs && rc == SB200_OK; ++i) {
+      e = cudaGraphLaunch(exec, b->stream);
+      if (e != cudaSuccess) rc = cuda_error(e, "cudaGraphLaunch");
+    }
+    cudaGraphExecDestroy(exec);
+    if (rc != SB200_OK) return rc;
+  }
+  if (nt % 2 == 1) TRY_B(issue_batch_step(b, 0, z.data(), n_hamil));
+  TRY_B(kernel_timing_flush(b->sys[0]));
+  for (int s = 0; s < n; ++s) {
+    if (rbox_out && rbox_out[s] && nt > 0)
+      SB_CUDA(cudaMemcpyAsync(rbox_out[s], b->sys[s]->rt.d_rbox, 4 * (size_t)nt * sizeof(double), cudaMemcpyDefault,
+                              b->stream));
+    if (psi_final) psi_final[s] = (nt % 2 == 1) ? psi_b[s] : psi_a[s];
+  }
+  SB_CUDA(cudaStreamSynchronize(b->stream));
+  SB_CUDA(cudaGetLastError());
+  return SB200_OK;
+}
+
+}  // extern "C"

@@ -1,7 +1,7 @@
 // sb200_bodies.cuh -- device-function bodies shared by the per-system kernels
 // (sb200_kernels.cu) and the batched persistent kernels (sb200_batch.cu):
 // KB projections of one (orbital, atom) and the observable partial sums of
-// one (orbital, point block).
+// one (orbital, point block), and the per-step final reduction.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -9,6 +9,8 @@
 
 namespace sb200 {
 namespace body {
+
+constexpr double PI = 3.141592653589793238462643383279502884;
 
 __device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
@@ -152,5 +154,100 @@ __device__ __forceinline__ void obs_block(const double2* __restrict__ in, double
   __syncthreads();  // red is reused by the next call of a persistent caller
 }
 
+// ---------------------------------------------------------------------------
+// Final per-step reduction in one block: current J (calc_current), calc_dip
+// rbox, calc_emfields; advances the device step counter.
+// ---------------------------------------------------------------------------
+struct FinArgs {
+  int norb, nspin, nspin_no, nblk, natom, periodic, itt, trans_longi, advance, spin_filter;
+  int jw_natom;            // atoms per orbital in jw (1 when already summed)
+  double ngrid_inv, dt;
+  const double* part;
+  const double* jw;        // [norb][natom][3] or null
+  const double* weight;
+  const double* vec_k;
+  const double* Ac_cur;    // a_mode: itt-indexed Ac_tot (history) or direct A[3] when itt_direct
+  int A_direct;
+  double* Ac_ind;
+  double* Ac_tot;
+  const double* Ac_ext;
+  double* curr_hist;       // (3, nt) or null
+  double* rbox_hist;       // (4, nt) or null
+  double* result;          // [8] direct results (J3, rbox4) or null
+  int* step;
+};
+
+// Called by one CTA of 256 threads.
+__device__ __forceinline__ void finalize_body(const FinArgs& a) {
+  __shared__ double red[7][256];
+  int itt = a.itt;
+  if (itt < 0) itt = *a.step;
+  double A[3] = {0.0, 0.0, 0.0};
+  if (a.periodic) {
+    for (int d = 0; d < 3; ++d) A[d] = a.A_direct ? a.Ac_cur[d] : a.Ac_cur[3 * itt + d];
+  }
+  double s[7] = {0, 0, 0, 0, 0, 0, 0};
+  for (int o = threadIdx.x; o < a.norb; o += blockDim.x) {
+    if (a.spin_filter >= 0 && (o % a.nspin) != a.spin_filter) continue;
+    double q[OBS_NQ] = {0, 0, 0, 0, 0, 0, 0};
+    for (int b = 0; b < a.nblk; ++b)
+      for (int i = 0; i < OBS_NQ; ++i) q[i] += a.part[((long)o * a.nblk + b) * OBS_NQ + i];
+    const double w = a.weight[o];
+    if (a.periodic) {
+      const int ik = o / a.nspin_no;
+      double jw[3] = {0.0, 0.0, 0.0};
+      if (a.jw != nullptr)
+        for (int at = 0; at < a.jw_natom; ++at)
+          for (int d = 0; d < 3; ++d) jw[d] += a.jw[3L * ((long)o * a.jw_natom + at) + d];
+      for (int d = 0; d < 3; ++d) {
+        const double kAc = a.vec_k[3 * ik + d] + A[d];
+        s[d] += (kAc * q[0] + 2.0 * q[1 + d] + 2.0 * jw[d]) * w;
+      }
+    }
+    for (int d = 0; d < 3; ++d) s[3 + d] += q[4 + d] * w;
+    s[6] += q[0] * w;
+  }
+  for (int i = 0; i < 7; ++i) red[i][threadIdx.x] = s[i];
+  __syncthreads();
+  for (int st = 128; st > 0; st >>= 1) {
+    if (threadIdx.x < st)
+      for (int i = 0; i < 7; ++i) red[i][threadIdx.x] += red[i][threadIdx.x + st];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    double J[3], rb[4];
+    for (int d = 0; d < 3; ++d) J[d] = red[d][0] * a.ngrid_inv;
+    for (int d = 0; d < 3; ++d) rb[d] = red[3 + d][0];
+    rb[3] = red[6][0];
+    if (a.result) {
+      for (int d = 0; d < 3; ++d) a.result[d] = J[d];
+      for (int d = 0; d < 4; ++d) a.result[3 + d] = rb[d];
+    }
+    if (a.curr_hist)
+      for (int d = 0; d < 3; ++d) a.curr_hist[3L * (itt - 1) + d] = J[d];
+    if (a.rbox_hist)
+      for (int d = 0; d < 4; ++d) a.rbox_hist[4L * (itt - 1) + d] = rb[d];
+    if (a.periodic && a.Ac_tot) {  // calc_emfields, em_field.f90:47-67
+      for (int d = 0; d < 3; ++d) {
+        double ind;
+        if (a.trans_longi == SB200_TRANS_LO)
+          ind = 2.0 * a.Ac_ind[3 * itt + d] - a.Ac_ind[3 * (itt - 1) + d] - 4.0 * PI * J[d] * a.dt * a.dt;
+        else
+          ind = 0.0;
+        a.Ac_ind[3 * (itt + 1) + d] = ind;
+        a.Ac_tot[3 * (itt + 1) + d] = a.Ac_ext[3 * (itt + 1) + d] + ind;
+      }
+    }
+    if (a.advance) *a.step = itt + 1;
+  }
+}
+
 }  // namespace body
+
+// argument blocks of one context (sb200_kernels.cu)
+body::ProjArgs make_proj_args(const sb200_ctx* c);
+body::ObsArgs make_obs_args(const sb200_ctx* c);
+// itt >= 0: host-given history index, results to d_result; itt < 0: RT loop
+body::FinArgs make_fin_args(const sb200_ctx* c, int itt, int trans_longi, double dt, int spin_filter,
+                            bool fused_obs);
 }  // namespace sb200

@@ -199,6 +199,11 @@ int launch_finalize(sb200_ctx* c, int itt_host, int nt, int trans_longi, double 
 int launch_density(sb200_ctx* c, const double2* psi, double* rho);
 int launch_dip(sb200_ctx* c, const double* rho, double* d_out4);
 int launch_relayout(sb200_ctx* c, const void* src, void* dst, int norb_chunk, bool to_ref);
+// time-loop histories of capacity nt (sb200_api.cu)
+int rt_alloc(sb200_ctx* c, int nt);
+// per-kernel-class event timing on c->stream when c->timing is set (sb200_api.cu)
+int kernel_timing_mark(sb200_ctx* c, int kind, bool start);
+int kernel_timing_flush(sb200_ctx* c);
 // low-pass preconditioner of the ground-state CG (sb200_gs.cu)
 int gs_precond(sb200_ctx* c, const double* g, double* pre, double alpha);
 // learned preconditioner: pre = net(g, V_local) for every orbital (sb200_learned.cu)

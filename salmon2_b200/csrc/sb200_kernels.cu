@@ -10,8 +10,6 @@ namespace {
 
 using namespace body;
 
-constexpr double PI = 3.141592653589793238462643383279502884;
-
 // ---------------------------------------------------------------------------
 // k-point coefficients and projector phases (hamiltonian.f90:146-155,847-903)
 // ---------------------------------------------------------------------------
@@ -268,92 +266,7 @@ __global__ void __launch_bounds__(OBS_THREADS) k_observables(const double2* __re
   obs_block(in, part, a, blockIdx.x, blockIdx.y);
 }
 
-// ---------------------------------------------------------------------------
-// Final per-step reduction in one block: current J (calc_current), calc_dip
-// rbox, calc_emfields; advances the device step counter.
-// ---------------------------------------------------------------------------
-struct FinArgs {
-  int norb, nspin, nspin_no, nblk, natom, periodic, itt, trans_longi, advance, spin_filter;
-  int jw_natom;            // atoms per orbital in jw (1 when already summed)
-  double ngrid_inv, dt;
-  const double* part;
-  const double* jw;        // [norb][natom][3] or null
-  const double* weight;
-  const double* vec_k;
-  const double* Ac_cur;    // a_mode: itt-indexed Ac_tot (history) or direct A[3] when itt_direct
-  int A_direct;
-  double* Ac_ind;
-  double* Ac_tot;
-  const double* Ac_ext;
-  double* curr_hist;       // (3, nt) or null
-  double* rbox_hist;       // (4, nt) or null
-  double* result;          // [8] direct results (J3, rbox4) or null
-  int* step;
-};
-
-__global__ void __launch_bounds__(256) k_finalize(FinArgs a) {
-  __shared__ double red[7][256];
-  int itt = a.itt;
-  if (itt < 0) itt = *a.step;
-  double A[3] = {0.0, 0.0, 0.0};
-  if (a.periodic) {
-    for (int d = 0; d < 3; ++d) A[d] = a.A_direct ? a.Ac_cur[d] : a.Ac_cur[3 * itt + d];
-  }
-  double s[7] = {0, 0, 0, 0, 0, 0, 0};
-  for (int o = threadIdx.x; o < a.norb; o += blockDim.x) {
-    if (a.spin_filter >= 0 && (o % a.nspin) != a.spin_filter) continue;
-    double q[OBS_NQ] = {0, 0, 0, 0, 0, 0, 0};
-    for (int b = 0; b < a.nblk; ++b)
-      for (int i = 0; i < OBS_NQ; ++i) q[i] += a.part[((long)o * a.nblk + b) * OBS_NQ + i];
-    const double w = a.weight[o];
-    if (a.periodic) {
-      const int ik = o / a.nspin_no;
-      double jw[3] = {0.0, 0.0, 0.0};
-      if (a.jw != nullptr)
-        for (int at = 0; at < a.jw_natom; ++at)
-          for (int d = 0; d < 3; ++d) jw[d] += a.jw[3L * ((long)o * a.jw_natom + at) + d];
-      for (int d = 0; d < 3; ++d) {
-        const double kAc = a.vec_k[3 * ik + d] + A[d];
-        s[d] += (kAc * q[0] + 2.0 * q[1 + d] + 2.0 * jw[d]) * w;
-      }
-    }
-    for (int d = 0; d < 3; ++d) s[3 + d] += q[4 + d] * w;
-    s[6] += q[0] * w;
-  }
-  for (int i = 0; i < 7; ++i) red[i][threadIdx.x] = s[i];
-  __syncthreads();
-  for (int st = 128; st > 0; st >>= 1) {
-    if (threadIdx.x < st)
-      for (int i = 0; i < 7; ++i) red[i][threadIdx.x] += red[i][threadIdx.x + st];
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) {
-    double J[3], rb[4];
-    for (int d = 0; d < 3; ++d) J[d] = red[d][0] * a.ngrid_inv;
-    for (int d = 0; d < 3; ++d) rb[d] = red[3 + d][0];
-    rb[3] = red[6][0];
-    if (a.result) {
-      for (int d = 0; d < 3; ++d) a.result[d] = J[d];
-      for (int d = 0; d < 4; ++d) a.result[3 + d] = rb[d];
-    }
-    if (a.curr_hist)
-      for (int d = 0; d < 3; ++d) a.curr_hist[3L * (itt - 1) + d] = J[d];
-    if (a.rbox_hist)
-      for (int d = 0; d < 4; ++d) a.rbox_hist[4L * (itt - 1) + d] = rb[d];
-    if (a.periodic && a.Ac_tot) {  // calc_emfields, em_field.f90:47-67
-      for (int d = 0; d < 3; ++d) {
-        double ind;
-        if (a.trans_longi == SB200_TRANS_LO)
-          ind = 2.0 * a.Ac_ind[3 * itt + d] - a.Ac_ind[3 * (itt - 1) + d] - 4.0 * PI * J[d] * a.dt * a.dt;
-        else
-          ind = 0.0;
-        a.Ac_ind[3 * (itt + 1) + d] = ind;
-        a.Ac_tot[3 * (itt + 1) + d] = a.Ac_ext[3 * (itt + 1) + d] + ind;
-      }
-    }
-    if (a.advance) *a.step = itt + 1;
-  }
-}
+__global__ void __launch_bounds__(256) k_finalize(FinArgs a) { finalize_body(a); }
 
 // rho(p, ispin) = sum_{ik, io} w |psi|^2 (density_matrix.f90:150-232)
 __global__ void k_density(const double2* __restrict__ in, double* __restrict__ rho, long npts, int nspin,
@@ -457,7 +370,7 @@ int launch_prep_k(sb200_ctx* c, const double* d_A, int a_mode, int itt, double* 
   return SB200_OK;
 }
 
-static ProjArgs proj_args(sb200_ctx* c) {
+ProjArgs make_proj_args(const sb200_ctx* c) {
   ProjArgs a;
   a.npts = c->g.npts;
   a.natom = c->pp.natom;
@@ -480,7 +393,7 @@ static ProjArgs proj_args(sb200_ctx* c) {
 
 int launch_project(sb200_ctx* c, const void* in, double2* proj, bool in32) {
   if (c->pp.nlma == 0) return SB200_OK;
-  ProjArgs a = proj_args(c);
+  ProjArgs a = make_proj_args(c);
   dim3 grid((a.natom + 3) / 4, c->orb.norb);
   if (in32) k_project<4, float2><<<grid, 128, 0, c->stream>>>((const float2*)in, proj, a);
   else k_project<4, double2><<<grid, 128, 0, c->stream>>>((const double2*)in, proj, a);
@@ -490,7 +403,7 @@ int launch_project(sb200_ctx* c, const void* in, double2* proj, bool in32) {
 
 int launch_project_moments(sb200_ctx* c, const double2* psi) {
   if (c->pp.nlma == 0) return SB200_OK;
-  ProjArgs a = proj_args(c);
+  ProjArgs a = make_proj_args(c);
   dim3 grid((a.natom + 3) / 4, c->orb.norb);
   k_project_moments<2><<<grid, 128, 0, c->stream>>>(psi, c->d_jw, a);
   SB_LAUNCH_CHECK("k_project_moments");
@@ -533,7 +446,7 @@ int launch_hpsi(sb200_ctx* c, const HpsiLaunch& L) {
   return SB200_OK;
 }
 
-int launch_observables(sb200_ctx* c, const double2* psi) {
+ObsArgs make_obs_args(const sb200_ctx* c) {
   ObsArgs a;
   a.nx = c->g.nx;
   a.ny = c->g.ny;
@@ -543,6 +456,11 @@ int launch_observables(sb200_ctx* c, const double2* psi) {
   a.nblk = c->obs_blocks;
   for (int i = 0; i < 12; ++i) a.nab[i] = c->g.coef_nab[i];
   for (int d = 0; d < 3; ++d) a.off[d] = (double)c->g.is[d] - ((c->g.lg_num[d] % 2 == 1) ? 0.0 : 0.5);
+  return a;
+}
+
+int launch_observables(sb200_ctx* c, const double2* psi) {
+  ObsArgs a = make_obs_args(c);
   dim3 grid(c->obs_blocks, c->orb.norb);
   k_observables<<<grid, OBS_THREADS, 0, c->stream>>>(psi, c->d_obs, a);
   SB_LAUNCH_CHECK("k_observables");
@@ -551,7 +469,7 @@ int launch_observables(sb200_ctx* c, const double2* psi) {
 
 // itt >= 0: history index given by the host (API calls), results to d_result;
 // itt < 0: RT loop, index from the device step counter.
-int launch_finalize(sb200_ctx* c, int itt, int nt, int trans_longi, double dt, int spin_filter, bool fused_obs) {
+FinArgs make_fin_args(const sb200_ctx* c, int itt, int trans_longi, double dt, int spin_filter, bool fused_obs) {
   FinArgs a;
   a.norb = c->orb.norb;
   a.jw_natom = fused_obs ? 1 : c->pp.natom;
@@ -591,7 +509,12 @@ int launch_finalize(sb200_ctx* c, int itt, int nt, int trans_longi, double dt, i
     a.result = c->d_result;
     a.advance = 0;
   }
+  return a;
+}
+
+int launch_finalize(sb200_ctx* c, int itt, int nt, int trans_longi, double dt, int spin_filter, bool fused_obs) {
   (void)nt;
+  FinArgs a = make_fin_args(c, itt, trans_longi, dt, spin_filter, fused_obs);
   k_finalize<<<1, 256, 0, c->stream>>>(a);
   SB_LAUNCH_CHECK("k_finalize");
   return SB200_OK;

@@ -55,7 +55,7 @@ int launch_tiled_t(const HpsiLaunch& L, const TiledArgs& a, dim3 grid, cudaStrea
 
 }  // namespace
 
-int launch_hpsi_tiled(sb200_ctx* c, const HpsiLaunch& L) {
+TiledArgs make_tiled_args(const sb200_ctx* c, double2 zc) {
   TiledArgs a;
   a.nx = c->g.nx;
   a.ny = c->g.ny;
@@ -78,7 +78,13 @@ int launch_hpsi_tiled(sb200_ctx* c, const HpsiLaunch& L) {
   a.ent_lma = c->pp.d_ent_lma;
   a.ent_zk = c->pp.d_ent_zk;
   a.proj = c->d_proj;
-  a.zc = L.zc;
+  a.zc = zc;
+  a.zchunk = c->g.nz;
+  return a;
+}
+
+int launch_hpsi_tiled(sb200_ctx* c, const HpsiLaunch& L) {
+  TiledArgs a = make_tiled_args(c, L.zc);
   // tile choice: the whole plane for 16x16 periodic grids, else 32x8 (16x16
   // when the x extent is at most 16)
   const GridInfo& g = c->g;

@@ -17,7 +17,11 @@ struct TiledArgs {
   double2 zc;
 };
 
-struct HpsiLaunch;
-struct sb200_ctx_fwd;
 
+}  // namespace sb200
+
+struct sb200_ctx;
+namespace sb200 {
+// coefficient / table block of one context for the tiled kernel (z chunk = nz)
+TiledArgs make_tiled_args(const sb200_ctx* c, double2 zc);
 }  // namespace sb200

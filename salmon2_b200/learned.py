@@ -42,26 +42,35 @@ def _lowpass(torch, g, shape, hgs, alpha=0.6):
     return (omega / d * (2.0 * G - omega / d * (-0.5 * lap))).reshape(B, -1)
 
 
-def converge(ctx, psi, tol=1e-8, max_outer=400, precondition="lowpass", ncg=4, record=None):
-    """Outer loop gscg + Gram-Schmidt + subspace diagonalisation until
-    max |eps_i - eps_i(previous)| <= tol (Hartree).  Returns a dict with the
-    eigenvalues, outer iterations, CG iterations and wall time."""
+def converge(ctx, psi, tol=1e-8, max_outer=400, precondition="lowpass", ncg=4, record=None, ref=None):
+    """Outer loop gscg + Gram-Schmidt + subspace diagonalisation.  Stops when
+    max_i |eps_i - ref_i| <= tol (Hartree) if reference eigenvalues ``ref`` are
+    given, else when max_i |eps_i - eps_i(previous outer iteration)| <= tol.
+    Returns a dict with the eigenvalues, outer iterations, CG iterations, wall
+    time and whether the criterion was met."""
     torch = ctx.torch
     prev = None
+    torch.cuda.synchronize()
     t0 = time.perf_counter()
     it = 0
     ev = None
+    done = False
     for it in range(1, max_outer + 1):
         if record is not None:
             record(psi)
         ctx.gscg(psi, ncg=ncg, precondition=precondition)
         ctx.gram_schmidt_real(psi)
         ev = ctx.subspace_diag_real(psi)
-        if prev is not None and np.max(np.abs(ev - prev)) <= tol:
+        if ref is not None:
+            if np.max(np.abs(ev - ref)) <= tol:
+                done = True
+                break
+        elif prev is not None and np.max(np.abs(ev - prev)) <= tol:
+            done = True
             break
         prev = ev
     torch.cuda.synchronize()
-    return dict(evals=ev, outer=it, cg_iters=it * ncg, seconds=time.perf_counter() - t0)
+    return dict(evals=ev, outer=it, cg_iters=it * ncg, seconds=time.perf_counter() - t0, converged=done)
 
 
 def collect_samples(ctx, psi0, n_outer=12, ncg=4, tol=1e-10):
@@ -98,7 +107,23 @@ def collect_samples(ctx, psi0, n_outer=12, ncg=4, tol=1e-10):
     return torch.cat(x0s), torch.cat(offs), torch.cat(tgts)
 
 
+def initial_params(seed=0, channels=None):
+    """Training start: He-normal hidden layers, zero biases and a zero output
+    layer (so the starting network is the low-pass preconditioner and every
+    layer receives gradient).  Layout [W1, b1, W2, b2, W3, b3] with W1
+    (C, 2, 27), W2 (C, C, 27), W3 (1, C, 27) as in sb200_learned.cu."""
+    C_ = _lib.LEARNED_CHANNELS if channels is None else channels
+    rng = np.random.default_rng(seed)
+    w1 = rng.standard_normal(C_ * 2 * 27) * np.sqrt(2.0 / (2 * 27))
+    w2 = rng.standard_normal(C_ * C_ * 27) * np.sqrt(2.0 / (C_ * 27))
+    p = np.concatenate([w1, np.zeros(C_), w2, np.zeros(C_), np.zeros(C_ * 27), np.zeros(1)]).astype(np.float32)
+    assert p.size == _lib.LEARNED_NPARAM
+    return p
+
+
 def init(ctx, batch, params=None):
+    """Load parameters (None: all zero, the network that adds nothing to the
+    low-pass preconditioner)."""
     p = None if params is None else np.ascontiguousarray(params, dtype=np.float32)
     check(lib().sb200_learned_init(ctx.h, None if p is None else C.c_void_p(p.ctypes.data), _lib.LEARNED_NPARAM,
                                    int(batch)))

@@ -225,3 +225,60 @@ class Context:
         ev = np.zeros(self.sys.no)
         check(lib().sb200_subspace_diag_real(self.h, C.c_void_p(psi.data_ptr()), _ptr(ev)))
         return ev
+
+
+class Batch:
+    """Independent isolated systems advanced together (sb200_batch_*).
+
+    ``contexts`` are fully set-up :class:`Context` objects of isolated grids;
+    the batch keeps references to them so they outlive it."""
+
+    def __init__(self, contexts):
+        self.ctxs = list(contexts)
+        self.n = len(self.ctxs)
+        arr = (C.c_void_p * self.n)(*[c.h for c in self.ctxs])
+        h = C.c_void_p()
+        check(lib().sb200_batch_create(arr, self.n, C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().sb200_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _ptrs(self, tensors):
+        return (C.c_void_p * self.n)(*[t.data_ptr() for t in tensors])
+
+    def tiles(self):
+        sh = np.zeros(self.n, np.int32)
+        zc = np.zeros(self.n, np.int32)
+        check(lib().sb200_batch_get_tiles(self.h, sh.ctypes.data_as(_ip), zc.ctypes.data_as(_ip)))
+        return sh, zc
+
+    def set_tiles(self, shape, zchunk):
+        sh = np.ascontiguousarray(shape, np.int32)
+        zc = np.ascontiguousarray(zchunk, np.int32)
+        check(lib().sb200_batch_set_tiles(self.h, sh.ctypes.data_as(_ip), zc.ctypes.data_as(_ip)))
+
+    def autotune(self, psi, work, reps=3):
+        sh = np.zeros(self.n, np.int32)
+        zc = np.zeros(self.n, np.int32)
+        check(lib().sb200_batch_autotune(self.h, self._ptrs(psi), self._ptrs(work), int(reps),
+                                         sh.ctypes.data_as(_ip), zc.ctypes.data_as(_ip)))
+        return sh, zc
+
+    def propagate(self, psi_a, psi_b, work, nt, dt, zc, rbox=True):
+        z = np.ascontiguousarray(zc, dtype=np.complex128)
+        boxes = [np.zeros((4, max(nt, 1)), order="F") for _ in range(self.n)]
+        rb = (C.c_void_p * self.n)(*[b.ctypes.data for b in boxes]) if rbox else None
+        fin = (C.c_void_p * self.n)()
+        check(lib().sb200_batch_propagate(self.h, self._ptrs(psi_a), self._ptrs(psi_b), self._ptrs(work), int(nt),
+                                          float(dt), z.ctypes.data_as(_dp), len(z), rb, fin))
+        finals = [a if fin[i] == a.data_ptr() else b for i, (a, b) in enumerate(zip(psi_a, psi_b))]
+        return dict(psi=finals, rbox=[b[:, :nt] for b in boxes] if rbox else None)

@@ -227,9 +227,21 @@ def gaussian_potential(grid: Grid, centers: np.ndarray, amps, widths, cell=None)
     return V
 
 
-def random_orbitals(grid: Grid, rng, nspin, no, nk, envelope_width=None, real=False) -> np.ndarray:
+def _cholesky_qr2(a):
+    """Orthonormal columns spanning a (tall, well conditioned): two passes of
+    Cholesky QR (Gram matrix, Cholesky factor, triangular inverse)."""
+    for _ in range(2):
+        g = a.conj().T @ a
+        L = np.linalg.cholesky(g)
+        a = a @ np.linalg.inv(L).conj().T
+    return a
+
+
+def random_orbitals(grid: Grid, rng, nspin, no, nk, envelope_width=None, real=False,
+                    fast=False) -> np.ndarray:
     """Seeded orbitals, orthonormal per (k, spin) in the hvol metric, in the
-    reference array layout with a zero halo (structures.f90:646-669)."""
+    reference array layout with a zero halo (structures.f90:646-669).
+    fast=True orthonormalises by Cholesky QR instead of Householder QR."""
     nx, ny, nz = grid.shape
     X, Y, Z = np.meshgrid(grid.coordinate(0), grid.coordinate(1), grid.coordinate(2), indexing="ij")
     if envelope_width is None:
@@ -249,7 +261,7 @@ def random_orbitals(grid: Grid, rng, nspin, no, nk, envelope_width=None, real=Fa
             if not real:
                 a = a + 1j * rng.standard_normal((npt, no))
             a *= env.reshape(-1, order="F")[:, None]
-            q, _ = np.linalg.qr(a)
+            q = _cholesky_qr2(a) if fast else np.linalg.qr(a)[0]
             q = q / math.sqrt(grid.hvol)
             for io in range(no):
                 out[sl + (isp, io, ik)] = q[:, io].reshape((nx, ny, nz), order="F")
@@ -306,7 +318,7 @@ def asin2cos(nt: int, dt: float, omega: float, f0: float, tw: float, epdir=(0.0,
 # --------------------------------------------------------------------------
 
 def isolated_system(num=64, h_aa=0.25, no=5, natom=4, seed=1, rc_aa=1.2, nspin=1,
-                    real=False, name="isolated") -> System:
+                    real=False, name="isolated", fast=False) -> System:
     """Isolated molecule: Dirichlet box, seeded atoms in the central 60 %."""
     rng = np.random.default_rng(seed)
     h = h_aa / AU_LENGTH_AA
@@ -319,10 +331,26 @@ def isolated_system(num=64, h_aa=0.25, no=5, natom=4, seed=1, rc_aa=1.2, nspin=1
                  inorm=rng.choice([-1, 1], size=(natom, 2)))
     V = gaussian_potential(grid, rion, rng.uniform(-2.0, -0.5, natom), rng.uniform(0.8, 1.6, natom))
     V_local = np.asfortranarray(np.repeat(V[..., None], nspin, axis=3))
-    psi = random_orbitals(grid, rng, nspin, no, 1, envelope_width=0.2 * L, real=real)
+    psi = random_orbitals(grid, rng, nspin, no, 1, envelope_width=0.2 * L, real=real, fast=fast)
     return System(grid, pp, nspin, no, 1, np.zeros((3, 1), order="F"),
                   np.asfortranarray(np.full((no, 1, nspin), 2.0)), np.ones(1), V_local, rion, psi,
                   int(np.prod(grid.num)), seed, name)
+
+
+def uneven_batch(nsys=16, seed=4):
+    """Independent isolated systems of uneven size from one seed: cubic grids
+    n^3 with n in {32, 40, ..., 96}, 4..64 orbitals, 2..16 atoms (h = 0.25 A,
+    Gaussian KB projectors, seeded Gaussian V_local), as in the batch workload
+    of the propagation benchmark."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(nsys):
+        n = int(rng.choice(np.arange(32, 97, 8)))
+        no = int(rng.integers(4, 65))
+        natom = int(rng.integers(2, 17))
+        out.append(isolated_system(num=n, no=no, natom=natom, seed=int(rng.integers(1 << 30)),
+                                   name=f"batch{i}_{n}^3_{no}orb_{natom}at", fast=True))
+    return out
 
 
 DIAMOND = np.array([[0, 0, 0], [0.5, 0.5, 0], [0.5, 0, 0.5], [0, 0.5, 0.5],

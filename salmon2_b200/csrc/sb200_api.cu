@@ -98,10 +98,22 @@ int require_ready(sb200_ctx* c, bool need_vloc = true) {
   return SB200_OK;
 }
 
+// after a stream synchronisation: did a kernel give up a bounded wait?
+int check_device_flag(sb200_ctx* c) {
+  int flag = 0;
+  SB_CUDA(cudaMemcpy(&flag, c->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (flag != 0) {
+    SB_CUDA(cudaMemset(c->d_err, 0, sizeof(int)));
+    return set_error(SB200_ERR_TIMEOUT, "a bounded device wait expired (a bulk copy did not complete)");
+  }
+  return SB200_OK;
+}
+
 void free_pp(PPInfo& p) {
   dfree(p.d_atom_start);
   dfree(p.d_mps);
   dfree(p.d_lma_start);
+  dfree(p.d_lma_atom);
   dfree(p.d_nproj);
   dfree(p.d_pt_lin);
   dfree(p.d_pt_r);
@@ -295,8 +307,12 @@ int sb200_ctx_create(int device, sb200_ctx** out) {
   }
   c->stream = c->own_stream;
   if (const char* v = getenv("SB200_STENCIL")) c->stencil_variant = (v[0] == 'n') ? 0 : 1;
+  if (const char* v = getenv("SB200_ORBITAL")) c->orbital_variant = (v[0] == 'p') ? 1 : 0;
+  if (const char* v = getenv("SB200_TMA")) c->tma_variant = (v[0] == 'o' && v[1] == 'f') ? 0 : 1;
   int r = dalloc(&c->d_result, 16);
   if (r == SB200_OK) r = dalloc(&c->rt.d_step, 1);
+  if (r == SB200_OK) r = dalloc(&c->d_err, 1);
+  if (r == SB200_OK && cudaMemset(c->d_err, 0, sizeof(int)) != cudaSuccess) r = cuda_error(cudaGetLastError(), "cudaMemset");
   if (r != SB200_OK) {
     sb200_ctx_destroy(c);
     return r;
@@ -327,6 +343,7 @@ int sb200_ctx_destroy(sb200_ctx* c) {
   dfree(c->rt.d_curr);
   dfree(c->rt.d_rbox);
   dfree(c->rt.d_step);
+  dfree(c->d_err);
   dfree(c->rt.d_zc);
   if (c->d_stage) cudaFree(c->d_stage);
   dfree(c->gs.d_proj);
@@ -378,7 +395,7 @@ int sb200_ctx_sync(sb200_ctx* c) {
   DeviceGuard dg(c->device);
   SB_CUDA(cudaStreamSynchronize(c->stream));
   SB_CUDA(cudaGetLastError());
-  return SB200_OK;
+  return check_device_flag(c);
 }
 
 int sb200_set_grid(sb200_ctx* c, const int is[3], const int ie[3], const int is_array[3], const int ie_array[3],
@@ -596,6 +613,11 @@ int sb200_set_pp(sb200_ctx* c, int natom, int nps, int nlma, const int* mps, con
   TRY(upload(&p.d_atom_start, atom_start));
   TRY(upload(&p.d_mps, hmps));
   TRY(upload(&p.d_lma_start, lma_start));
+  {
+    std::vector<int> lma_atom(nlma);
+    for (int l = 0; l < nlma; ++l) lma_atom[l] = ia_tbl[l] - 1;
+    TRY(upload(&p.d_lma_atom, lma_atom));
+  }
   TRY(upload(&p.d_nproj, nproj));
   TRY(upload(&p.d_pt_lin, pt_lin));
   TRY(upload(&p.d_pt_r, pt_r));
@@ -853,6 +875,7 @@ int sb200_rt_propagate(sb200_ctx* c, double* psi_a, double* psi_b, double* work,
     SB_CUDA(cudaMemcpyAsync(Ac_tot_out, r.d_Ac_tot, na * sizeof(double), cudaMemcpyDefault, c->stream));
   SB_CUDA(cudaStreamSynchronize(c->stream));
   SB_CUDA(cudaGetLastError());
+  TRY(check_device_flag(c));
   if (psi_final) *psi_final = (double*)final_buf;
   // leave hpsi coefficients consistent with system%vec_Ac for later hpsi calls
   TRY(refresh_k(c));

@@ -7,7 +7,8 @@
 //   * one persistent hpsi launch: 1-2 CTAs per SM pull work items (a tile x
 //     z-chunk x orbital of some system) from a device work queue, stage that
 //     system's argument block in shared memory and run the tiled 2.5-D sweep
-//     (sb200_tiled_body.cuh) with the system's own tile shape and z-chunk;
+//     (sb200_tiled_body.cuh, without the Bloch gradient terms that vanish on
+//     isolated grids) with the system's own tile shape and z-chunk;
 // and per time step one launch of the observable partial sums and one of the
 // final reductions (one CTA per system).  Two time steps are captured as one
 // CUDA graph and replayed.  Tile shape and z-chunk of every system are picked
@@ -115,9 +116,9 @@ __global__ void __launch_bounds__(256, (MODE >= 6) ? SB200_TILED_MINB32 : SB200_
     const int r = (int)(l % per_o);
     const BPtr p = ptr[s];
     if (shape == SHAPE_32x8)
-      tiled_body<32, 8, false, MODE>((const C2*)p.in, p.hout, p.acc, p.d32, sa, r % ntiles, r / ntiles, o);
+      tiled_body<32, 8, false, MODE, false>((const C2*)p.in, p.hout, p.acc, p.d32, sa, r % ntiles, r / ntiles, o);
     else
-      tiled_body<16, 16, false, MODE>((const C2*)p.in, p.hout, p.acc, p.d32, sa, r % ntiles, r / ntiles, o);
+      tiled_body<16, 16, false, MODE, false>((const C2*)p.in, p.hout, p.acc, p.d32, sa, r % ntiles, r / ntiles, o);
     __syncthreads();  // plane buffers and the argument block are reused by the next item
   }
   // the last CTA to leave resets the queue for the next launch

@@ -48,6 +48,7 @@ struct PPInfo {
   int* d_atom_start = nullptr;  // first flat sphere point of the atom
   int* d_mps = nullptr;
   int* d_lma_start = nullptr;   // first (0-based) ilma of the atom
+  int* d_lma_atom = nullptr;    // atom (0-based) of each ilma
   int* d_nproj = nullptr;       // projectors of the atom
   // per flat sphere point
   int* d_pt_lin = nullptr;      // linear resident-layout point index
@@ -124,11 +125,14 @@ struct sb200_ctx {
   double* d_jw = nullptr;       // [norb][natom][3] nonlocal current pieces
   double* d_obs = nullptr;      // [norb][obs_blocks][OBS_NQ] partial sums
   double* d_result = nullptr;   // small result area (8 doubles)
+  int* d_err = nullptr;         // device error flag: a bounded wait expired
   int obs_blocks = 0;
   void* d_stage = nullptr;      // relayout staging
   size_t stage_bytes = 0;
   bool vloc_set = false;
   int stencil_variant = 1;     // 0: per-point reference kernel, 1: tiled 2.5-D sweep
+  int orbital_variant = 0;     // 16^3 periodic grids: 0 one CTA per orbital, 1 persistent with bulk copies
+  int tma_variant = 1;         // tiled hpsi fed by tensor copies where it applies (0: register-prefetch sweep)
   // optional per-kernel-class device timing (sb200_set_timing)
   bool timing = false;
   std::vector<cudaEvent_t> ev;  // pairs (start, stop)
@@ -190,6 +194,8 @@ int launch_prep_k(sb200_ctx* c, const double* d_A, int a_mode, int itt_from_devi
 int launch_project(sb200_ctx* c, const void* in, double2* proj, bool in32 = false);
 int launch_hpsi(sb200_ctx* c, const HpsiLaunch& L);
 int launch_hpsi_tiled(sb200_ctx* c, const HpsiLaunch& L);  // sb200_stencil.cu
+// tensor-copy-fed tiled kernel; SB200_ERR_UNSUPPORTED when it does not apply (sb200_tma_stencil.cu)
+int launch_hpsi_tma(sb200_ctx* c, const HpsiLaunch& L);
 bool orbital_kernel_applies(const sb200_ctx* c);             // sb200_orbital.cu
 int launch_term_orbital(sb200_ctx* c, const HpsiLaunch& L, bool with_obs);
 int launch_observables(sb200_ctx* c, const double2* psi);

@@ -7,7 +7,9 @@
 //   x1 = relu(conv3(x0; W1, b1))                C channels
 //   x2 = relu(conv3(x1; W2, b2))                C channels
 //   y  = conv3(x2; W3, b3)                      1 channel
-//   pre_g = lowpass(g) + rms(g) * y             (lowpass = preconditioning.f90:25-77)
+//   p     = lowpass(g) + rms(g) * y             (lowpass = preconditioning.f90:25-77)
+//   pre_g = +p or -p, whichever keeps <pre_g, g> >= <lowpass(g), g> / 5,
+//           else lowpass(g) (k_apply_direction)
 // conv3 is a 3x3x3 convolution.  Weights are kept as FP32 masters and used as
 // BF16 in the forward pass, with FP32 accumulation; gradients and Adam are FP32.
 // The last layer starts at zero, so the untrained network is the reference's
@@ -63,6 +65,7 @@ struct Net {
   float* d_wpart = nullptr;   // weight-gradient partials
   long wpart_cap = 0;
   float* d_scale = nullptr;   // per-orbital rms(g)
+  double* d_dots = nullptr;   // CG hook: per-orbital <pre, g> partials [B][32][2]
 };
 
 // ---- conv forward: out[co][p] = b[co] + sum_ci sum_k W[co][ci][k] in[ci][p+k] ----
@@ -299,12 +302,60 @@ __global__ void k_make_input(const double* __restrict__ g, const double* __restr
   }
 }
 
-__global__ void k_add_correction(double* __restrict__ pre, const float* __restrict__ y, const float* __restrict__ scale,
-                                 long npts, int o0) {
+// Partial sums of d0 = <lowpass(g), g> and d1 = <rms(g) y, g> per orbital.
+__global__ void __launch_bounds__(256) k_dir_dots_part(const double* __restrict__ pre, const double* __restrict__ g,
+                                                       const float* __restrict__ y, const float* __restrict__ scale,
+                                                       long npts, int o0, double* __restrict__ part, int nblk) {
+  __shared__ double r0[256], r1[256];
   const int b = blockIdx.y;
+  const long o = o0 + b;
+  const double sc = scale[b];
+  double s0 = 0.0, s1 = 0.0;
+  for (long p = blockIdx.x * 256L + threadIdx.x; p < npts; p += (long)nblk * 256) {
+    const double gv = g[o * npts + p];
+    s0 += pre[o * npts + p] * gv;
+    s1 += sc * (double)y[(long)b * npts + p] * gv;
+  }
+  r0[threadIdx.x] = s0;
+  r1[threadIdx.x] = s1;
+  __syncthreads();
+  for (int st = 128; st > 0; st >>= 1) {
+    if (threadIdx.x < st) {
+      r0[threadIdx.x] += r0[threadIdx.x + st];
+      r1[threadIdx.x] += r1[threadIdx.x + st];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    part[((long)b * nblk + blockIdx.x) * 2 + 0] = r0[0];
+    part[((long)b * nblk + blockIdx.x) * 2 + 1] = r1[0];
+  }
+}
+
+// The network direction p = lowpass(g) + rms(g) y is used only on the side of
+// g that keeps <pre, g> clearly positive (the CG's conjugation coefficients
+// are ratios of these products): with D = <p, g> and d0 = <lowpass(g), g>,
+// pre = p if D >= d0 / 5, pre = -p if D <= -d0 / 5 (the same search line),
+// else the low-pass direction alone.
+__global__ void k_apply_direction(double* __restrict__ pre, const float* __restrict__ y,
+                                  const float* __restrict__ scale, const double* __restrict__ part, int nblk,
+                                  long npts, int o0) {
+  const int b = blockIdx.y;
+  double d0 = 0.0, d1 = 0.0;
+  for (int k = 0; k < nblk; ++k) {
+    d0 += part[((long)b * nblk + k) * 2 + 0];
+    d1 += part[((long)b * nblk + k) * 2 + 1];
+  }
+  const double D = d0 + d1;
+  double sign;
+  if (D >= 0.2 * d0) sign = 1.0;
+  else if (D <= -0.2 * d0) sign = -1.0;
+  else return;
   const double s = scale[b];
-  for (long p = blockIdx.x * 256L + threadIdx.x; p < npts; p += (long)gridDim.x * 256)
-    pre[(long)(o0 + b) * npts + p] += s * (double)y[(long)b * npts + p];
+  for (long p = blockIdx.x * 256L + threadIdx.x; p < npts; p += (long)gridDim.x * 256) {
+    const long i = (long)(o0 + b) * npts + p;
+    pre[i] = sign * (pre[i] + s * (double)y[(long)b * npts + p]);
+  }
 }
 
 int gsz(long n) {
@@ -323,7 +374,8 @@ int net_ensure(sb200_ctx* c, int batch) {
     // d_red holds the loss partials (batch * (64*3 + 1) <= 1024 * 193) and the
     // CG hook's rms partials (norb * 32 <= 65536)
     if (dalloc(&n->d_w, NPARAM) || dalloc(&n->d_wb, NPARAM) || dalloc(&n->d_g, NPARAM) || dalloc(&n->d_m, NPARAM) ||
-        dalloc(&n->d_v, NPARAM) || dalloc(&n->d_red, (size_t)1024 * 193 + 65536) || dalloc(&n->d_scale, 4096))
+        dalloc(&n->d_v, NPARAM) || dalloc(&n->d_red, (size_t)1024 * 193 + 65536) || dalloc(&n->d_scale, 4096) ||
+        dalloc(&n->d_dots, (size_t)1024 * 32 * 2))
       return SB200_ERR_OOM;
     SB_CUDA(cudaMemset(n->d_w, 0, NPARAM * sizeof(float)));
     SB_CUDA(cudaMemset(n->d_m, 0, NPARAM * sizeof(float)));
@@ -445,7 +497,8 @@ int learned_precond_apply(sb200_ctx* c, const double* g, double* pre) {
     dim3 gi((unsigned)((np + 255) / 256 < 1024 ? (np + 255) / 256 : 1024), b);
     k_make_input<<<gi, 256, 0, c->stream>>>(g, c->d_vloc, np, n->d_red, nblk, o0, n->x0, n->d_scale);
     TRY_L(net_forward(c, b));
-    k_add_correction<<<gi, 256, 0, c->stream>>>(pre, n->y, n->d_scale, np, o0);
+    k_dir_dots_part<<<dim3(nblk, b), 256, 0, c->stream>>>(pre, g, n->y, n->d_scale, np, o0, n->d_dots, nblk);
+    k_apply_direction<<<gi, 256, 0, c->stream>>>(pre, n->y, n->d_scale, n->d_dots, nblk, np, o0);
   }
   SB_LAUNCH_CHECK("learned_precond_apply");
   return SB200_OK;
@@ -471,6 +524,7 @@ void learned_free(sb200_ctx* c) {
   dfree(n->d_red);
   dfree(n->d_wpart);
   dfree(n->d_scale);
+  dfree(n->d_dots);
   delete n;
   c->learned = nullptr;
   c->learned_set = false;

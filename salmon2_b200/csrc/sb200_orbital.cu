@@ -19,6 +19,7 @@
 
 #include "sb200_internal.cuh"
 #include "sb200_orbital.cuh"
+#include "sb200_tma.cuh"
 
 namespace sb200 {
 namespace {
@@ -75,12 +76,13 @@ __device__ void project_from_smem(const double2* __restrict__ sm, double2* __res
 
 // Nonlocal current pieces sum_lma Im(conj(<r_d zekr|v>) rinv <zekr|v>) of the
 // orbital in shared memory; result reduced over the block into red3[0..2].
+template <int NWARP>
 __device__ void current_nonlocal_from_smem(const double2* __restrict__ sm, const OrbArgs& a, int ik,
-                                           double* __restrict__ wsum /* [NT/32][3] */) {
+                                           double* __restrict__ wsum /* [NWARP][3] */) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const double2* ph = a.phase + (long)ik * a.totpts;
   double jx = 0.0, jy = 0.0, jz = 0.0;
-  for (int atom = warp; atom < a.natom; atom += NT / 32) {
+  for (int atom = warp; atom < a.natom; atom += NWARP) {
     const int start = a.atom_start[atom], m = a.mps[atom];
     const int lma0 = a.lma_start[atom], np = a.nproj[atom];
     for (int q = 0; q < np; ++q) {
@@ -256,7 +258,7 @@ __global__ void __launch_bounds__(NT, 2) k_term_orbital(const double2* __restric
   if (lane == 0)
     for (int i = 0; i < OBS_NQ; ++i) red[i][warp] = q[i];
   __shared__ double jws[NT / 32][3];
-  if (a.nlma > 0) current_nonlocal_from_smem(sm, a, ik, &jws[0][0]);
+  if (a.nlma > 0) current_nonlocal_from_smem<NT / 32>(sm, a, ik, &jws[0][0]);
   __syncthreads();
   if (t < OBS_NQ) {
     double s = 0.0;
@@ -270,6 +272,243 @@ __global__ void __launch_bounds__(NT, 2) k_term_orbital(const double2* __restric
   }
 }
 
+
+// ---------------------------------------------------------------------------
+// Persistent form: one CTA of 256 threads per SM walks orbitals
+// o = blockIdx.x, blockIdx.x + gridDim.x, ...  Whole orbitals (64 KB) arrive
+// by bulk copy (TMA, cp.async.bulk) into two shared-memory buffers, so the
+// copy of orbital i+1 overlaps the stencil of orbital i; the Taylor
+// accumulator psi_out of the orbital (modes 2, 3) is copied in the same way
+// into a third buffer.  Thread t owns column (x, y) = t and keeps its whole z
+// column in registers (up to 255 registers per thread at one CTA per SM).
+// The Bloch gradient is applied as kAc_d * sum_s nab_s (psi(+s) - psi(-s)).
+// ---------------------------------------------------------------------------
+constexpr int NT2 = NP;
+constexpr unsigned ORB_BYTES = N * NP * sizeof(double2);
+
+// KB projections of the orbital in shared memory: one warp per projector.
+__device__ void project_lma_from_smem(const double2* __restrict__ sm, double2* __restrict__ Ps, const OrbArgs& a,
+                                      int ik) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const double2* ph = a.phase + (long)ik * a.totpts;
+  for (int lma = warp; lma < a.nlma; lma += NT2 / 32) {
+    const int atom = __ldg(a.lma_atom + lma);
+    const int start = __ldg(a.atom_start + atom), m = __ldg(a.mps + atom);
+    const double* uvr = a.uv + (long)lma * a.nps;
+    double2 acc = make_double2(0.0, 0.0);
+#pragma unroll 4
+    for (int j = lane; j < m; j += 32) {
+      const double2 v = sm[__ldg(a.pt_lin + start + j)];
+      const double2 e = __ldg(ph + start + j);
+      const double uv = __ldg(uvr + j);
+      acc = cadd(acc, cmul(make_double2(e.x * uv, e.y * uv), v));
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      acc.x += __shfl_xor_sync(0xffffffffu, acc.x, off);
+      acc.y += __shfl_xor_sync(0xffffffffu, acc.y, off);
+    }
+    if (lane == 0) Ps[lma] = cscal(__ldg(a.rinv + lma), acc);
+  }
+}
+
+// Stencil + KB scatter + Taylor epilogue of the 16 planes of one column.
+template <int MODE>
+__device__ __forceinline__ void column_all(const double2* __restrict__ sm, const double2* __restrict__ Ps,
+                                           double2* __restrict__ accb, const double2 (&colv)[N], const OrbArgs& a,
+                                           int col, int tx, int ty, int ispin, int ik, double2* __restrict__ hdst,
+                                           double2* __restrict__ adst) {
+  constexpr bool READ_ACC = (MODE == 2 || MODE == 3);
+  const double* kc = a.kcoef + (long)KC * ik;
+  const double kx = kc[0], ky = kc[1], kz = kc[2], lap0 = kc[3];
+  const double* vloc = a.vloc + (long)ispin * a.npts;
+  const double2* zkk = a.ent_zk + (long)ik * a.nent;
+  double vl_n = __ldg(vloc + col);
+  int pm_n = a.nlma > 0 ? __ldg(a.pmap + col) : -1;
+#pragma unroll
+  for (int z = 0; z < N; ++z) {
+    const double vl = vl_n;
+    const int pm = pm_n;
+    if (z + 1 < N) {
+      vl_n = __ldg(vloc + (z + 1) * NP + col);
+      if (a.nlma > 0) pm_n = __ldg(a.pmap + (z + 1) * NP + col);
+    }
+    const double2* P = sm + z * NP;
+    double2 vx = make_double2(0.0, 0.0), wx = vx, vy = vx, wy = vx, vz = vx, wz = vx;
+#pragma unroll
+    for (int s = 1; s <= ND; ++s) {
+      const double2 tp = P[ty * N + ((tx + s) & (N - 1))], tm = P[ty * N + ((tx - s) & (N - 1))];
+      vx = cadd(vx, cscal(a.lapt[s - 1], cadd(tp, tm)));
+      wx = cadd(wx, cscal(a.nab[s - 1], csub(tp, tm)));
+    }
+#pragma unroll
+    for (int s = 1; s <= ND; ++s) {
+      const double2 tp = P[(((ty + s) & (N - 1)) << 4) + tx], tm = P[(((ty - s) & (N - 1)) << 4) + tx];
+      vy = cadd(vy, cscal(a.lapt[4 + s - 1], cadd(tp, tm)));
+      wy = cadd(wy, cscal(a.nab[4 + s - 1], csub(tp, tm)));
+    }
+#pragma unroll
+    for (int s = 0; s < ND; ++s) {
+      const double2 tp = colv[(z + s + 1) & (N - 1)], tm = colv[(z - s - 1) & (N - 1)];
+      vz = cadd(vz, cscal(a.lapt[8 + s], cadd(tp, tm)));
+      wz = cadd(wz, cscal(a.nab[8 + s], csub(tp, tm)));
+    }
+    const double2 v = cadd(vz, cadd(vy, vx));
+    const double2 w = cadd(cscal(kz, wz), cadd(cscal(ky, wy), cscal(kx, wx)));
+    const double2 c = colv[z];
+    const int p = z * NP + col;
+    double2 h;
+    h.x = vl * c.x + lap0 * c.x - 0.5 * v.x + w.y;
+    h.y = vl * c.y + lap0 * c.y - 0.5 * v.y - w.x;
+    if (a.nlma > 0 && pm >= 0) {
+      const int e1 = (pm >> 8) + (pm & 255);
+      for (int e = pm >> 8; e < e1; ++e) h = cadd(h, cmul(Ps[__ldg(a.ent_lma + e)], __ldg(zkk + e)));
+    }
+    if (MODE == 1 || MODE == 2) hdst[p] = h;
+    double2 nv;
+    if (READ_ACC) nv = cadd(accb[p], cmul(a.zc, h));
+    else nv = cadd(c, cmul(a.zc, h));
+    adst[p] = nv;
+    if (MODE == 3 || MODE == 4) accb[p] = nv;  // the new orbital, for the observables
+  }
+}
+
+// Observables of the new orbital held in shared memory (last Taylor term).
+__device__ __forceinline__ void observables_smem(const double2* __restrict__ sm, const OrbArgs& a, int o, int ik,
+                                                 double (*red)[NT2 / 32], double (*jws)[3]) {
+  const int t = threadIdx.x;
+  const int tx = t & 15, ty = t >> 4;
+  double q[OBS_NQ];
+#pragma unroll
+  for (int i = 0; i < OBS_NQ; ++i) q[i] = 0.0;
+#pragma unroll 4
+  for (int z = 0; z < N; ++z) {
+    const double2 c = sm[z * NP + t];
+    const double r2 = c.x * c.x + c.y * c.y;
+    q[0] += r2;
+    double ix = 0.0, iy = 0.0, iz = 0.0;
+#pragma unroll
+    for (int s = 1; s <= ND; ++s) {
+      const double2 txv = sm[z * NP + ty * N + ((tx + s) & (N - 1))];
+      const double2 tyv = sm[z * NP + (((ty + s) & (N - 1)) << 4) + tx];
+      const double2 tzv = sm[((z + s) & (N - 1)) * NP + t];
+      ix += a.nab[s - 1] * (c.x * txv.y - c.y * txv.x);
+      iy += a.nab[4 + s - 1] * (c.x * tyv.y - c.y * tyv.x);
+      iz += a.nab[8 + s - 1] * (c.x * tzv.y - c.y * tzv.x);
+    }
+    q[1] += ix;
+    q[2] += iy;
+    q[3] += iz;
+    q[4] += ((double)tx + a.off[0]) * r2;
+    q[5] += ((double)ty + a.off[1]) * r2;
+    q[6] += ((double)z + a.off[2]) * r2;
+  }
+#pragma unroll
+  for (int i = 0; i < OBS_NQ; ++i) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) q[i] += __shfl_xor_sync(0xffffffffu, q[i], off);
+  }
+  const int warp = t >> 5, lane = t & 31;
+  if (lane == 0)
+    for (int i = 0; i < OBS_NQ; ++i) red[i][warp] = q[i];
+  if (a.nlma > 0) current_nonlocal_from_smem<NT2 / 32>(sm, a, ik, &jws[0][0]);
+  __syncthreads();
+  if (t < OBS_NQ) {
+    double s = 0.0;
+    for (int w = 0; w < NT2 / 32; ++w) s += red[t][w];
+    a.obs[(long)o * OBS_NQ + t] = s;
+  } else if (t >= 32 && t < 35) {
+    double s = 0.0;
+    if (a.nlma > 0)
+      for (int w = 0; w < NT2 / 32; ++w) s += jws[w][t - 32];
+    a.jw[3L * o + (t - 32)] = s;
+  }
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(NT2, 1) k_term_orbital_tma(const double2* __restrict__ in,
+                                                             double2* __restrict__ hout, double2* __restrict__ acc,
+                                                             OrbArgs a, int norb, int* __restrict__ err) {
+  constexpr bool READ_ACC = (MODE == 2 || MODE == 3);
+  extern __shared__ __align__(128) unsigned char smraw[];
+  double2* bufs = (double2*)smraw;         // two orbital buffers
+  double2* accb = bufs + 2 * N * NP;        // psi_out of the orbital / the new orbital
+  double2* Ps = accb + N * NP;              // projections
+  __shared__ __align__(8) uint64_t bar[3];  // buffer 0, buffer 1, accumulator
+  __shared__ double red[OBS_NQ][NT2 / 32];
+  __shared__ double jws[NT2 / 32][3];
+  const int t = threadIdx.x;
+  const int tx = t & 15, ty = t >> 4;
+  const int G = gridDim.x;
+  const int nmine = ((int)blockIdx.x < norb) ? (norb - (int)blockIdx.x + G - 1) / G : 0;
+  const bool obs = (MODE == 3 || MODE == 4) && a.obs != nullptr;
+  if (t == 0) {
+    tma::mbar_init(&bar[0], 1);
+    tma::mbar_init(&bar[1], 1);
+    tma::mbar_init(&bar[2], 1);
+    tma::fence_barrier_init();
+  }
+  __syncthreads();
+  if (t == 0) {
+    for (int i = 0; i < 2 && i < nmine; ++i) {
+      const long o = blockIdx.x + (long)i * G;
+      tma::mbar_arrive_expect_tx(&bar[i], ORB_BYTES);
+      tma::bulk_load(bufs + i * N * NP, in + o * a.npts, ORB_BYTES, &bar[i]);
+    }
+    if (READ_ACC && nmine > 0) {
+      tma::mbar_arrive_expect_tx(&bar[2], ORB_BYTES);
+      tma::bulk_load(accb, acc + (long)blockIdx.x * a.npts, ORB_BYTES, &bar[2]);
+    }
+  }
+  // orbital buffers issued so far (the same count in every thread)
+  int psi_issued = nmine < 2 ? nmine : 2;
+  for (int i = 0; i < nmine; ++i) {
+    const int o = blockIdx.x + i * G;
+    const int b = i & 1;
+    const double2* sm = bufs + b * N * NP;
+    bool ok = tma::mbar_wait(&bar[b], (unsigned)((i >> 1) & 1));
+    if (READ_ACC) ok = tma::mbar_wait(&bar[2], (unsigned)(i & 1)) && ok;
+    if (!__syncthreads_and(ok)) {
+      // a copy did not arrive in time: flag it, wait (bounded) for the other
+      // orbital copy this CTA has in flight, and leave
+      if (t == 0) {
+        atomicExch(err, 1);
+        for (int k = i + 1; k < psi_issued; ++k) tma::mbar_wait(&bar[k & 1], (unsigned)((k >> 1) & 1));
+      }
+      __syncthreads();
+      return;
+    }
+    const int ik = o / a.nspin_no;
+    const int ispin = o % a.nspin;
+    if (a.nlma > 0) {
+      project_lma_from_smem(sm, Ps, a, ik);
+      __syncthreads();
+    }
+    double2 colv[N];
+#pragma unroll
+    for (int z = 0; z < N; ++z) colv[z] = sm[z * NP + t];
+    column_all<MODE>(sm, Ps, accb, colv, a, t, tx, ty, ispin, ik, hout + (long)o * a.npts, acc + (long)o * a.npts);
+    __syncthreads();  // buffer b, accb and Ps are free (accb holds the new orbital in modes 3, 4)
+    if (obs) {
+      observables_smem(accb, a, o, ik, red, jws);
+      __syncthreads();
+    }
+    if (t == 0) {  // refill: orbital i+2 into buffer b, psi_out of orbital i+1 into accb
+      tma::fence_proxy_async_smem();
+      if (i + 2 < nmine) {
+        const long o2 = blockIdx.x + (long)(i + 2) * G;
+        tma::mbar_arrive_expect_tx(&bar[b], ORB_BYTES);
+        tma::bulk_load(bufs + b * N * NP, in + o2 * a.npts, ORB_BYTES, &bar[b]);
+      }
+      if (READ_ACC && i + 1 < nmine) {
+        const long o1 = blockIdx.x + (long)(i + 1) * G;
+        tma::mbar_arrive_expect_tx(&bar[2], ORB_BYTES);
+        tma::bulk_load(accb, acc + o1 * a.npts, ORB_BYTES, &bar[2]);
+      }
+    }
+    if (i + 2 < nmine) psi_issued = i + 3;
+  }
+}
 }  // namespace
 
 bool orbital_kernel_applies(const sb200_ctx* c) {
@@ -279,14 +518,23 @@ bool orbital_kernel_applies(const sb200_ctx* c) {
 }
 
 int launch_term_orbital(sb200_ctx* c, const HpsiLaunch& L, bool with_obs) {
-  static bool attr_set = false;
+  static bool attr_set = false, attr_set2 = false;
   const size_t smem = (size_t)N * NP * sizeof(double2) + (size_t)ORB_MAX_NLMA * sizeof(double2);
-  if (!attr_set) {
+  const size_t smem2 = 3 * (size_t)ORB_BYTES + (size_t)ORB_MAX_NLMA * sizeof(double2);
+  const bool persistent = c->orbital_variant == 1;
+  if (!persistent && !attr_set) {
     SB_CUDA(cudaFuncSetAttribute(k_term_orbital<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     SB_CUDA(cudaFuncSetAttribute(k_term_orbital<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     SB_CUDA(cudaFuncSetAttribute(k_term_orbital<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     SB_CUDA(cudaFuncSetAttribute(k_term_orbital<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     attr_set = true;
+  }
+  if (persistent && !attr_set2) {
+    SB_CUDA(cudaFuncSetAttribute(k_term_orbital_tma<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2));
+    SB_CUDA(cudaFuncSetAttribute(k_term_orbital_tma<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2));
+    SB_CUDA(cudaFuncSetAttribute(k_term_orbital_tma<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2));
+    SB_CUDA(cudaFuncSetAttribute(k_term_orbital_tma<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2));
+    attr_set2 = true;
   }
   OrbArgs a;
   a.npts = c->g.npts;
@@ -313,15 +561,31 @@ int launch_term_orbital(sb200_ctx* c, const HpsiLaunch& L, bool with_obs) {
   a.lma_start = c->pp.d_lma_start;
   a.nproj = c->pp.d_nproj;
   a.pt_lin = c->pp.d_pt_lin;
+  a.lma_atom = c->pp.d_lma_atom;
   a.pt_r = c->pp.d_pt_r;
   a.uv = c->pp.d_uv;
   a.rinv = c->pp.d_rinv;
   a.zc = L.zc;
   a.obs = with_obs ? c->d_obs : nullptr;
   a.jw = with_obs ? c->d_jw : nullptr;
-  dim3 grid(c->orb.norb);
   const double2* IN = (const double2*)L.in;
   double2* HOUT = (double2*)L.hout;
+  if (persistent) {
+    int sms = 148;
+    SB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
+    const int norb = c->orb.norb;
+    const int g2 = norb < sms ? norb : sms;
+    switch (L.mode) {
+      case 1: k_term_orbital_tma<1><<<g2, NT2, smem2, c->stream>>>(IN, HOUT, L.out, a, norb, c->d_err); break;
+      case 2: k_term_orbital_tma<2><<<g2, NT2, smem2, c->stream>>>(IN, HOUT, L.out, a, norb, c->d_err); break;
+      case 3: k_term_orbital_tma<3><<<g2, NT2, smem2, c->stream>>>(IN, HOUT, L.out, a, norb, c->d_err); break;
+      case 4: k_term_orbital_tma<4><<<g2, NT2, smem2, c->stream>>>(IN, HOUT, L.out, a, norb, c->d_err); break;
+      default: return set_error(SB200_ERR_INVALID_ARG, "orbital kernel: unsupported mode");
+    }
+    SB_LAUNCH_CHECK("k_term_orbital_tma");
+    return SB200_OK;
+  }
+  dim3 grid(c->orb.norb);
   switch (L.mode) {
     case 1: k_term_orbital<1><<<grid, NT, smem, c->stream>>>(IN, HOUT, L.out, a); break;
     case 2: k_term_orbital<2><<<grid, NT, smem, c->stream>>>(IN, HOUT, L.out, a); break;

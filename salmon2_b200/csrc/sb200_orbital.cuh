@@ -16,6 +16,7 @@ struct OrbArgs {
   const double2* ent_zk;
   const double2* phase;
   const int *atom_start, *mps, *lma_start, *nproj, *pt_lin;
+  const int* lma_atom;
   const double *pt_r, *uv, *rinv;
   double2 zc;
   double* obs;  // [norb][OBS_NQ] or null

@@ -30,24 +30,24 @@ namespace {
 
 using namespace tiled;
 
-template <int TX, int TY, bool FULL, int MODE>
+template <int TX, int TY, bool FULL, int MODE, bool GRAD>
 void launch_mode(const HpsiLaunch& L, const TiledArgs& a, dim3 grid, cudaStream_t st) {
   using C2 = typename Cx<typename ModeT<MODE>::R>::T;
-  k_hpsi_tiled<TX, TY, FULL, MODE><<<grid, TX * TY, 0, st>>>((const C2*)L.in, (void*)L.hout, L.out, L.d32, a);
+  k_hpsi_tiled<TX, TY, FULL, MODE, GRAD><<<grid, TX * TY, 0, st>>>((const C2*)L.in, (void*)L.hout, L.out, L.d32, a);
 }
 
-template <int TX, int TY, bool FULL>
+template <int TX, int TY, bool FULL, bool GRAD>
 int launch_tiled_t(const HpsiLaunch& L, const TiledArgs& a, dim3 grid, cudaStream_t st) {
   switch (L.mode) {
-    case 0: launch_mode<TX, TY, FULL, 0>(L, a, grid, st); break;
-    case 1: launch_mode<TX, TY, FULL, 1>(L, a, grid, st); break;
-    case 2: launch_mode<TX, TY, FULL, 2>(L, a, grid, st); break;
-    case 3: launch_mode<TX, TY, FULL, 3>(L, a, grid, st); break;
-    case 4: launch_mode<TX, TY, FULL, 4>(L, a, grid, st); break;
-    case 5: launch_mode<TX, TY, FULL, 5>(L, a, grid, st); break;
-    case 6: launch_mode<TX, TY, FULL, 6>(L, a, grid, st); break;
-    case 7: launch_mode<TX, TY, FULL, 7>(L, a, grid, st); break;
-    case 8: launch_mode<TX, TY, FULL, 8>(L, a, grid, st); break;
+    case 0: launch_mode<TX, TY, FULL, 0, GRAD>(L, a, grid, st); break;
+    case 1: launch_mode<TX, TY, FULL, 1, GRAD>(L, a, grid, st); break;
+    case 2: launch_mode<TX, TY, FULL, 2, GRAD>(L, a, grid, st); break;
+    case 3: launch_mode<TX, TY, FULL, 3, GRAD>(L, a, grid, st); break;
+    case 4: launch_mode<TX, TY, FULL, 4, GRAD>(L, a, grid, st); break;
+    case 5: launch_mode<TX, TY, FULL, 5, GRAD>(L, a, grid, st); break;
+    case 6: launch_mode<TX, TY, FULL, 6, GRAD>(L, a, grid, st); break;
+    case 7: launch_mode<TX, TY, FULL, 7, GRAD>(L, a, grid, st); break;
+    case 8: launch_mode<TX, TY, FULL, 8, GRAD>(L, a, grid, st); break;
     default: return set_error(SB200_ERR_INVALID_ARG, "tiled hpsi: unknown mode");
   }
   return SB200_OK;
@@ -84,6 +84,8 @@ TiledArgs make_tiled_args(const sb200_ctx* c, double2 zc) {
 }
 
 int launch_hpsi_tiled(sb200_ctx* c, const HpsiLaunch& L) {
+  const int rt = launch_hpsi_tma(c, L);
+  if (rt != SB200_ERR_UNSUPPORTED) return rt;
   TiledArgs a = make_tiled_args(c, L.zc);
   // tile choice: the whole plane for 16x16 periodic grids, else 32x8 (16x16
   // when the x extent is at most 16)
@@ -100,9 +102,12 @@ int launch_hpsi_tiled(sb200_ctx* c, const HpsiLaunch& L) {
   const int nzc = (g.nz + a.zchunk - 1) / a.zchunk;
   dim3 grid(ntiles, nzc, c->orb.norb);
   int r;
-  if (full16) r = launch_tiled_t<16, 16, true>(L, a, grid, c->stream);
-  else if (TXv == 16) r = launch_tiled_t<16, 16, false>(L, a, grid, c->stream);
-  else r = launch_tiled_t<32, 8, false>(L, a, grid, c->stream);
+  // isolated grids (k + A = 0) skip the gradient terms
+  if (full16) r = launch_tiled_t<16, 16, true, true>(L, a, grid, c->stream);
+  else if (TXv == 16) r = g.periodic ? launch_tiled_t<16, 16, false, true>(L, a, grid, c->stream)
+                                     : launch_tiled_t<16, 16, false, false>(L, a, grid, c->stream);
+  else r = g.periodic ? launch_tiled_t<32, 8, false, true>(L, a, grid, c->stream)
+                      : launch_tiled_t<32, 8, false, false>(L, a, grid, c->stream);
   if (r != SB200_OK) return r;
   SB_LAUNCH_CHECK("k_hpsi_tiled");
   return SB200_OK;

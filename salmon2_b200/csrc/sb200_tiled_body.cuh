@@ -81,7 +81,9 @@ struct ModeT {
   static constexpr bool h32 = (MODE >= 5);  // h stored as complex64
 };
 
-template <int TX, int TY, bool FULL, int MODE>
+// GRAD = false drops the Bloch gradient terms, which vanish identically on
+// isolated grids (k + A = 0).
+template <int TX, int TY, bool FULL, int MODE, bool GRAD = true>
 __device__ __forceinline__ void tiled_body(const typename Cx<typename ModeT<MODE>::R>::T* __restrict__ in,
                                            void* __restrict__ hout, double2* __restrict__ acc,
                                            float2* __restrict__ d32, const TiledArgs& a, const int bx,
@@ -223,7 +225,7 @@ __device__ __forceinline__ void tiled_body(const typename Cx<typename ModeT<MODE
         }
         const C2 tp = P[ip], tm = P[im];
         vx = cadd(vx, cscal((R)a.lapt[s - 1], cadd(tp, tm)));
-        wx = cadd(wx, cscal((R)a.nab[s - 1], csub(tp, tm)));
+        if (GRAD) wx = cadd(wx, cscal((R)a.nab[s - 1], csub(tp, tm)));
       }
 #pragma unroll
       for (int s = 1; s <= ND; ++s) {
@@ -237,29 +239,41 @@ __device__ __forceinline__ void tiled_body(const typename Cx<typename ModeT<MODE
         }
         const C2 tp = P[ip], tm = P[im];
         vy = cadd(vy, cscal((R)a.lapt[4 + s - 1], cadd(tp, tm)));
-        wy = cadd(wy, cscal((R)a.nab[4 + s - 1], csub(tp, tm)));
+        if (GRAD) wy = cadd(wy, cscal((R)a.nab[4 + s - 1], csub(tp, tm)));
       }
 #pragma unroll
       for (int s = 0; s < ND; ++s) {
         const C2 tp = w[ND + 1 + s], tm = w[ND - 1 - s];
         vz = cadd(vz, cscal((R)a.lapt[8 + s], cadd(tp, tm)));
-        wz = cadd(wz, cscal((R)a.nab[8 + s], csub(tp, tm)));
+        if (GRAD) wz = cadd(wz, cscal((R)a.nab[8 + s], csub(tp, tm)));
       }
       const C2 v = cadd(vz, cadd(vy, vx));
       const C2 ww = cadd(cscal(kz, wz), cadd(cscal(ky, wy), cscal(kx, wx)));
       const C2 c = w[ND];
       const long p = (long)z * sz + pxy;
       C2 h;
-      h.x = vl * c.x + lap0 * c.x - (R)0.5 * v.x + ww.y;
-      h.y = vl * c.y + lap0 * c.y - (R)0.5 * v.y - ww.x;
+      h.x = vl * c.x + lap0 * c.x - (R)0.5 * v.x;
+      h.y = vl * c.y + lap0 * c.y - (R)0.5 * v.y;
+      if (GRAD) {
+        h.x += ww.y;
+        h.y -= ww.x;
+      }
       if (a.nlma > 0 && pm >= 0) {
         const double2* pj = a.proj + (long)o * a.nlma;
         const double2* zk = a.ent_zk + (a.phase_per_k ? (long)ik * a.nent : 0L);
-        const int e1 = (pm >> 8) + (pm & 255);
-        for (int e = pm >> 8; e < e1; ++e) {
-          const double2 pv = pj[__ldg(a.ent_lma + e)];
-          const double2 zv = __ldg(zk + e);
-          h = cadd(h, cmul(Cx<R>::make((R)pv.x, (R)pv.y), Cx<R>::make((R)zv.x, (R)zv.y)));
+        const int e0 = pm >> 8, e1 = e0 + (pm & 255);
+        for (int e = e0; e < e1; e += 4) {  // entries four at a time, summed in entry order
+          double2 pv[4], zv[4];
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            const int ee = min(e + i, e1 - 1);
+            pv[i] = pj[__ldg(a.ent_lma + ee)];
+            zv[i] = __ldg(zk + ee);
+          }
+#pragma unroll
+          for (int i = 0; i < 4; ++i)
+            if (e + i < e1)
+              h = cadd(h, cmul(Cx<R>::make((R)pv[i].x, (R)pv[i].y), Cx<R>::make((R)zv[i].x, (R)zv[i].y)));
         }
       }
       const long gi = (long)o * a.npts + p;
@@ -297,11 +311,11 @@ __device__ __forceinline__ void tiled_body(const typename Cx<typename ModeT<MODE
   }
 }
 
-template <int TX, int TY, bool FULL, int MODE>
+template <int TX, int TY, bool FULL, int MODE, bool GRAD>
 __global__ void __launch_bounds__(TX * TY, (MODE >= 6) ? SB200_TILED_MINB32 : SB200_TILED_MINB64)
     k_hpsi_tiled(const typename Cx<typename ModeT<MODE>::R>::T* __restrict__ in, void* __restrict__ hout,
                  double2* __restrict__ acc, float2* __restrict__ d32, TiledArgs a) {
-  tiled_body<TX, TY, FULL, MODE>(in, hout, acc, d32, a, blockIdx.x, blockIdx.y, blockIdx.z);
+  tiled_body<TX, TY, FULL, MODE, GRAD>(in, hout, acc, d32, a, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 }  // namespace tiled

@@ -253,11 +253,15 @@ int sb200_learned_train_step(sb200_ctx* ctx, const float* x0, const float* offse
  * on one device with one precision; work runs on the first context's stream.
  * The batch keeps pointers to the contexts: destroy it before them.          */
 typedef struct sb200_batch sb200_batch;
-#define SB200_TILE_32x8 0
-#define SB200_TILE_16x16 1
+#define SB200_TILE_32x8 0     /* 32 x 8 tiles, register-prefetch z sweep            */
+#define SB200_TILE_16x16 1    /* 16 x 16 tiles, register-prefetch z sweep           */
+#define SB200_TILE_32x8_TMA 2 /* 32 x 8 tiles fed by tensor copies (all systems or none;
+                                 the default where every system can take it)         */
 int sb200_batch_create(sb200_ctx* const* systems, int nsys, sb200_batch** out);
 int sb200_batch_destroy(sb200_batch* batch);
-/* Per-system hpsi tiling: shape SB200_TILE_* and z planes per work item.     */
+/* Per-system hpsi tiling: shape SB200_TILE_* and z planes per work item.
+ * Autotuning searches the z chunk (and, for the register sweep, the shape)
+ * within the family of the current tiles.                                    */
 int sb200_batch_set_tiles(sb200_batch* batch, const int* shape, const int* zchunk);
 int sb200_batch_get_tiles(sb200_batch* batch, int* shape, int* zchunk);
 /* Time every tiling candidate of every system at full occupancy (`reps`

@@ -29,6 +29,7 @@
 #include "sb200_internal.cuh"
 #include "sb200_stencil.cuh"
 #include "sb200_tiled_body.cuh"
+#include "sb200_tma_body.cuh"
 
 namespace sb200 {
 namespace {
@@ -42,8 +43,9 @@ using namespace tiled;
     if (_r != SB200_OK) return _r;  \
   } while (0)
 
-constexpr int SHAPE_32x8 = 0;   // 32 x 8 column tiles
-constexpr int SHAPE_16x16 = 1;  // 16 x 16 column tiles
+constexpr int SHAPE_32x8 = 0;   // 32 x 8 column tiles, register-prefetch sweep
+constexpr int SHAPE_16x16 = 1;  // 16 x 16 column tiles, register-prefetch sweep
+constexpr int SHAPE_TMA = 2;    // 32 x 8 column tiles fed by tensor copies
 constexpr int MAX_SYS = 256;    // systems per batch (work-item lookup table in shared memory)
 
 // hpsi work of one system: argument block (zc set per launch) and tiling
@@ -115,13 +117,73 @@ __global__ void __launch_bounds__(256, (MODE >= 6) ? SB200_TILED_MINB32 : SB200_
     const int o = (int)(l / per_o);
     const int r = (int)(l % per_o);
     const BPtr p = ptr[s];
-    if (shape == SHAPE_32x8)
+    if (shape != SHAPE_16x16)
       tiled_body<32, 8, false, MODE, false>((const C2*)p.in, p.hout, p.acc, p.d32, sa, r % ntiles, r / ntiles, o);
     else
       tiled_body<16, 16, false, MODE, false>((const C2*)p.in, p.hout, p.acc, p.d32, sa, r % ntiles, r / ntiles, o);
     __syncthreads();  // plane buffers and the argument block are reused by the next item
   }
   // the last CTA to leave resets the queue for the next launch
+  if (threadIdx.x == 0) {
+    __threadfence();
+    const unsigned int done = atomicAdd(queue + 1, 1u);
+    if (done == gridDim.x - 1) {
+      atomicExch(queue, 0u);
+      atomicExch(queue + 1, 0u);
+    }
+  }
+}
+
+// The same work queue with the tensor-copy sweep (sb200_tma_body.cuh): every
+// system in 32 x 8 tiles, its input / accumulator copies described by the
+// tensor maps maps[s] of this launch (global memory, in queue order).  The
+// copy barriers are initialised once and keep their phases across items.
+template <int MODE>
+__global__ void __launch_bounds__(256, (MODE >= 6) ? 3 : 2)
+    k_hpsi_batch_tma(const BHSys* __restrict__ sys, const long* __restrict__ first, const tmak::TmaMaps* maps,
+                     const BPtr* __restrict__ ptr, int nsys, double2 zc, unsigned int* __restrict__ queue,
+                     int* __restrict__ err) {
+  extern __shared__ unsigned char smraw[];
+  __shared__ TiledArgs sa;
+  __shared__ long sfirst[MAX_SYS + 1];
+  __shared__ long s_w;
+  __shared__ int s_s;
+  if (nsys < 1 || nsys > MAX_SYS) return;  // the host never launches this
+  unsigned char* base = tmak::tma_area(smraw);
+  tmak::tma_init_barriers<MODE, false>(base);
+  uint32_t pmask = 0, amask = 0;
+  for (int i = threadIdx.x; i <= nsys; i += blockDim.x) sfirst[i] = first[i];
+  __syncthreads();
+  const long total = sfirst[nsys];
+  constexpr int NW = (int)(offsetof(TiledArgs, zc) / sizeof(int));
+  for (;;) {
+    if (threadIdx.x == 0) {
+      const long w = (long)atomicAdd(queue, 1u);
+      s_w = w;
+      s_s = w < total ? find_sys(sfirst, nsys, w) : -1;
+    }
+    __syncthreads();
+    const long w = s_w;
+    const int s = s_s;
+    if (w >= total) break;
+    {
+      const int* src = (const int*)&sys[s].a;
+      int* dst = (int*)&sa;
+      for (int i = threadIdx.x; i < NW; i += blockDim.x) dst[i] = __ldg(src + i);
+      if (threadIdx.x == 0) sa.zc = zc;
+    }
+    __syncthreads();
+    const int ntiles = __ldg(&sys[s].ntiles), nzc = __ldg(&sys[s].nzc);
+    const long l = w - sfirst[s];
+    const long per_o = (long)ntiles * nzc;
+    const int o = (int)(l / per_o);
+    const int r = (int)(l % per_o);
+    const BPtr p = ptr[s];
+    const bool ok = tmak::tma_body<MODE, false>(maps[s], p.hout, p.acc, p.d32, sa, err, r % ntiles, r / ntiles, o,
+                                                base, pmask, amask);
+    __syncthreads();  // the argument block is reused by the next item
+    if (!ok) break;   // a copy timed out: the flag is set, leave the queue to the others
+  }
   if (threadIdx.x == 0) {
     __threadfence();
     const unsigned int done = atomicAdd(queue + 1, 1u);
@@ -171,7 +233,7 @@ int h2d(void* d, const void* h, size_t bytes, cudaStream_t st) {
 int ceil_div(int a, int b) { return (a + b - 1) / b; }
 
 int tiles_of(const sb200_ctx* c, int shape) {
-  const int tx = shape == SHAPE_32x8 ? 32 : 16, ty = shape == SHAPE_32x8 ? 8 : 16;
+  const int tx = shape == SHAPE_16x16 ? 16 : 32, ty = shape == SHAPE_16x16 ? 16 : 8;
   return ceil_div(c->g.nx, tx) * ceil_div(c->g.ny, ty);
 }
 
@@ -200,6 +262,10 @@ struct sb200_batch {
   std::vector<int> order;  // hpsi queue order of the systems (costliest items first)
   int nsys = 0;
   int grid64 = 0, grid32 = 0;  // persistent hpsi grids (FP64 / FP32 stencil modes)
+  int gridt64 = 0, gridt32 = 0;  // the same for the tensor-copy kernel
+  bool tma_ok = false;          // every system can take the tensor-copy kernel
+  tmak::TmaMaps* d_tmaps = nullptr;  // [parity][term][nsys] tensor maps of one propagation
+  bool tmaps_valid = false;
   unsigned int* d_queue = nullptr;
   BHSys* d_hsys = nullptr;
   long* d_hfirst = nullptr;
@@ -219,6 +285,8 @@ struct sb200_batch {
 namespace {
 
 void batch_free_tables(sb200_batch* b) {
+  dfree(b->d_tmaps);
+  b->tmaps_valid = false;
   dfree(b->d_hptr);
   dfree(b->d_pin);
   dfree(b->d_opsi);
@@ -253,6 +321,7 @@ int batch_ensure_tables(sb200_batch* b, int n_hamil) {
   if (b->tab_nh >= n_hamil) return SB200_OK;
   batch_free_tables(b);
   TRY_B(dalloc(&b->d_hptr, (size_t)2 * n_hamil * b->nsys));
+  TRY_B(dalloc(&b->d_tmaps, (size_t)2 * n_hamil * b->nsys));
   TRY_B(dalloc(&b->d_pin, (size_t)2 * n_hamil * b->nsys));
   TRY_B(dalloc(&b->d_opsi, (size_t)2 * b->nsys));
   b->tab_nh = n_hamil;
@@ -292,28 +361,88 @@ int term_mode(int precision, int nn, int n_hamil) {
 }
 
 template <int MODE>
-void launch_hb(sb200_batch* b, const BHSys* hsys, const long* hfirst, const BPtr* ptr, int nsys, double2 zc,
-               int grid) {
-  k_hpsi_batch<MODE><<<grid, 256, 0, b->stream>>>(hsys, hfirst, ptr, nsys, zc, b->d_queue);
+int launch_hb(sb200_batch* b, const BHSys* hsys, const long* hfirst, const BPtr* ptr, const tmak::TmaMaps* maps,
+              int nsys, double2 zc) {
+  if (maps != nullptr) {
+    using G = tmak::Geo<MODE, false>;
+    const int grid = MODE >= 6 ? b->gridt32 : b->gridt64;
+    k_hpsi_batch_tma<MODE><<<grid, 256, G::SMEM, b->stream>>>(hsys, hfirst, maps, ptr, nsys, zc, b->d_queue,
+                                                               b->sys[0]->d_err);
+    SB_LAUNCH_CHECK("k_hpsi_batch_tma");
+  } else {
+    const int grid = MODE >= 6 ? b->grid32 : b->grid64;
+    k_hpsi_batch<MODE><<<grid, 256, 0, b->stream>>>(hsys, hfirst, ptr, nsys, zc, b->d_queue);
+    SB_LAUNCH_CHECK("k_hpsi_batch");
+  }
+  return SB200_OK;
 }
 
-int launch_hpsi_batch(sb200_batch* b, int mode, const BHSys* hsys, const long* hfirst, const BPtr* ptr, int nsys,
-                      double2 zc) {
-  const int grid = mode >= 6 ? b->grid32 : b->grid64;
+// maps == nullptr: register-prefetch sweep; else the tensor-copy sweep
+int launch_hpsi_batch(sb200_batch* b, int mode, const BHSys* hsys, const long* hfirst, const BPtr* ptr,
+                      const tmak::TmaMaps* maps, int nsys, double2 zc) {
   switch (mode) {
-    case 0: launch_hb<0>(b, hsys, hfirst, ptr, nsys, zc, grid); break;
-    case 1: launch_hb<1>(b, hsys, hfirst, ptr, nsys, zc, grid); break;
-    case 2: launch_hb<2>(b, hsys, hfirst, ptr, nsys, zc, grid); break;
-    case 3: launch_hb<3>(b, hsys, hfirst, ptr, nsys, zc, grid); break;
-    case 4: launch_hb<4>(b, hsys, hfirst, ptr, nsys, zc, grid); break;
-    case 5: launch_hb<5>(b, hsys, hfirst, ptr, nsys, zc, grid); break;
-    case 6: launch_hb<6>(b, hsys, hfirst, ptr, nsys, zc, grid); break;
-    case 7: launch_hb<7>(b, hsys, hfirst, ptr, nsys, zc, grid); break;
-    case 8: launch_hb<8>(b, hsys, hfirst, ptr, nsys, zc, grid); break;
+    case 0: return launch_hb<0>(b, hsys, hfirst, ptr, maps, nsys, zc);
+    case 1: return launch_hb<1>(b, hsys, hfirst, ptr, maps, nsys, zc);
+    case 2: return launch_hb<2>(b, hsys, hfirst, ptr, maps, nsys, zc);
+    case 3: return launch_hb<3>(b, hsys, hfirst, ptr, maps, nsys, zc);
+    case 4: return launch_hb<4>(b, hsys, hfirst, ptr, maps, nsys, zc);
+    case 5: return launch_hb<5>(b, hsys, hfirst, ptr, maps, nsys, zc);
+    case 6: return launch_hb<6>(b, hsys, hfirst, ptr, maps, nsys, zc);
+    case 7: return launch_hb<7>(b, hsys, hfirst, ptr, maps, nsys, zc);
+    case 8: return launch_hb<8>(b, hsys, hfirst, ptr, maps, nsys, zc);
     default: return set_error(SB200_ERR_INVALID_ARG, "batch hpsi: unknown mode");
   }
-  SB_LAUNCH_CHECK("k_hpsi_batch");
+}
+
+template <int MODE>
+int tma_attr() {
+  using G = tmak::Geo<MODE, false>;
+  SB_CUDA(cudaFuncSetAttribute(k_hpsi_batch_tma<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::SMEM));
   return SB200_OK;
+}
+
+int tma_attrs_all() {
+  TRY_B(tma_attr<0>());
+  TRY_B(tma_attr<1>());
+  TRY_B(tma_attr<2>());
+  TRY_B(tma_attr<3>());
+  TRY_B(tma_attr<4>());
+  TRY_B(tma_attr<5>());
+  TRY_B(tma_attr<6>());
+  TRY_B(tma_attr<7>());
+  TRY_B(tma_attr<8>());
+  return SB200_OK;
+}
+
+template <int MODE>
+int occupancy_grid_tma(int* grid) {
+  using G = tmak::Geo<MODE, false>;
+  int dev = 0, sms = 0, nb = 0;
+  SB_CUDA(cudaGetDevice(&dev));
+  SB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  SB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_hpsi_batch_tma<MODE>, 256, G::SMEM));
+  if (nb < 1) nb = 1;
+  *grid = sms * nb;
+  return SB200_OK;
+}
+
+// tensor maps of one system's hpsi launch in the given mode
+bool batch_maps(const sb200_ctx* c, int mode, const BPtr& p, tmak::TmaMaps& m) {
+  memset(&m, 0, sizeof(m));
+  const bool in32 = mode >= 6;
+  const bool acc64 = (mode == 2 || mode == 3 || mode == 8), rd32 = (mode == 7 || mode == 8);
+  const int norb = c->orb.norb;
+  if (!make_tma_map(&m.in, p.in, in32, c->g, norb, 2 * (tmak::TX + 2 * tmak::HALO), tmak::TY + 2 * tmak::HALO))
+    return false;
+  if (acc64 && !make_tma_map(&m.acc, p.acc, false, c->g, norb, 2 * tmak::TX, tmak::TY)) return false;
+  if (rd32 && !make_tma_map(&m.d32, p.d32, true, c->g, norb, 2 * tmak::TX, tmak::TY)) return false;
+  return true;
+}
+
+bool family_tma(const sb200_batch* b) {
+  for (int s = 0; s < b->nsys; ++s)
+    if (b->shape[s] != SHAPE_TMA) return false;
+  return true;
 }
 
 template <int MODE>
@@ -364,17 +493,20 @@ int issue_batch_step(sb200_batch* b, int parity, const double2* zc, int n_hamil)
     const size_t t = ((size_t)parity * n_hamil + (nn - 1)) * n;
     const int mode = term_mode(b->precision, nn, n_hamil);
     if (b->p_total > 0) TIMED_B(c0, SB200_KIND_PROJECT, launch_project_batch(b, mode >= 6, t));
-    TIMED_B(c0, SB200_KIND_HPSI, launch_hpsi_batch(b, mode, b->d_hsys, b->d_hfirst, b->d_hptr + t, n, zc[nn - 1]));
+    const tmak::TmaMaps* maps = b->tmaps_valid ? b->d_tmaps + t : nullptr;
+    TIMED_B(c0, SB200_KIND_HPSI,
+            launch_hpsi_batch(b, mode, b->d_hsys, b->d_hfirst, b->d_hptr + t, maps, n, zc[nn - 1]));
   }
   TIMED_B(c0, SB200_KIND_OBS, launch_obs_final_batch(b, parity, 0));
   TIMED_B(c0, SB200_KIND_FINAL, launch_obs_final_batch(b, parity, 1));
   return SB200_OK;
 }
 
-std::vector<Cand> candidates(const sb200_ctx* c) {
+std::vector<Cand> candidates(const sb200_ctx* c, bool tma) {
   std::vector<Cand> v;
   const int nz = c->g.nz;
-  for (int shape = 0; shape < 2; ++shape) {
+  for (int shape = 0; shape < 3; ++shape) {
+    if (tma != (shape == SHAPE_TMA)) continue;
     if (shape == SHAPE_32x8 && c->g.nx <= 16) continue;
     for (int div = 1; div <= 8; div *= 2) {
       const int zc = ceil_div(nz, div);
@@ -417,8 +549,13 @@ int sb200_batch_create(sb200_ctx* const* systems, int nsys, sb200_batch** out) {
   b->nsys = nsys;
   b->shape.resize(nsys);
   b->zchunk.resize(nsys);
-  for (int s = 0; s < nsys; ++s) {  // untuned default: the per-system path's tile, whole z sweeps
-    b->shape[s] = systems[s]->g.nx <= 16 ? SHAPE_16x16 : SHAPE_32x8;
+  // the tensor-copy sweep takes every isolated grid in FP64; FP32 inputs need
+  // an even x extent (16-byte row pitch)
+  b->tma_ok = c0->tma_variant != 0;
+  for (int s = 0; s < nsys; ++s)
+    if (b->precision == SB200_PREC_MIXED && systems[s]->g.nx % 2 != 0) b->tma_ok = false;
+  for (int s = 0; s < nsys; ++s) {  // untuned default: whole z sweeps
+    b->shape[s] = b->tma_ok ? SHAPE_TMA : (systems[s]->g.nx <= 16 ? SHAPE_16x16 : SHAPE_32x8);
     b->zchunk[s] = systems[s]->g.nz;
   }
   auto fail = [&](int rc) {
@@ -429,6 +566,11 @@ int sb200_batch_create(sb200_ctx* const* systems, int nsys, sb200_batch** out) {
   int rc = SB200_OK;
   if ((rc = occupancy_grid<1>(&b->grid64)) != SB200_OK) return fail(rc);
   if ((rc = occupancy_grid<7>(&b->grid32)) != SB200_OK) return fail(rc);
+  if (b->tma_ok) {
+    if ((rc = tma_attrs_all()) != SB200_OK) return fail(rc);
+    if ((rc = occupancy_grid_tma<1>(&b->gridt64)) != SB200_OK) return fail(rc);
+    if ((rc = occupancy_grid_tma<7>(&b->gridt32)) != SB200_OK) return fail(rc);
+  }
   if ((rc = dalloc(&b->d_queue, 2)) != SB200_OK) return fail(rc);
   const unsigned int zq[2] = {0u, 0u};
   if ((rc = h2d(b->d_queue, zq, sizeof(zq), b->stream)) != SB200_OK) return fail(rc);
@@ -490,8 +632,12 @@ int sb200_batch_destroy(sb200_batch* b) {
 int sb200_batch_set_tiles(sb200_batch* b, const int* shape, const int* zchunk) {
   if (!b || !shape || !zchunk) return set_error(SB200_ERR_INVALID_ARG, "bad argument");
   for (int s = 0; s < b->nsys; ++s) {
-    if (shape[s] != SHAPE_32x8 && shape[s] != SHAPE_16x16)
-      return set_error(SB200_ERR_INVALID_ARG, "tile shape must be 0 (32x8) or 1 (16x16)");
+    if (shape[s] != SHAPE_32x8 && shape[s] != SHAPE_16x16 && shape[s] != SHAPE_TMA)
+      return set_error(SB200_ERR_INVALID_ARG, "tile shape must be 0 (32x8), 1 (16x16) or 2 (32x8, tensor copies)");
+    if ((shape[s] == SHAPE_TMA) != (shape[0] == SHAPE_TMA))
+      return set_error(SB200_ERR_INVALID_ARG, "tensor-copy tiles (2) apply to every system of a batch or to none");
+    if (shape[s] == SHAPE_TMA && !b->tma_ok)
+      return set_error(SB200_ERR_UNSUPPORTED, "the tensor-copy sweep does not apply to this batch");
     if (zchunk[s] < 1 || zchunk[s] > b->sys[s]->g.nz) return set_error(SB200_ERR_INVALID_ARG, "z chunk out of range");
   }
   int prev = -1;
@@ -533,23 +679,26 @@ int sb200_batch_autotune(sb200_batch* b, const double* const* psi, double* const
   const bool mixed = b->precision == SB200_PREC_MIXED;
   const int mode = mixed ? 7 : 0;  // stencil of the inner Taylor terms
   const int grid = mixed ? b->grid32 : b->grid64;
-  const long want = 4L * grid;
+  const long want = 4L * (family_tma(b) ? (mixed ? b->gridt32 : b->gridt64) : grid);
   const int RMAX = MAX_SYS;  // replicas share the kernel's per-system lookup table
+  const bool tma = family_tma(b);
   BHSys* d_rep = nullptr;
   long* d_rf = nullptr;
   BPtr* d_rp = nullptr;
+  tmak::TmaMaps* d_rm = nullptr;
   int rc = SB200_OK;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   auto cleanup = [&]() {
     dfree(d_rep);
     dfree(d_rf);
     dfree(d_rp);
+    dfree(d_rm);
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
     if (prev >= 0) cudaSetDevice(prev);
   };
   if ((rc = dalloc(&d_rep, RMAX)) != SB200_OK || (rc = dalloc(&d_rf, RMAX + 1)) != SB200_OK ||
-      (rc = dalloc(&d_rp, RMAX)) != SB200_OK) {
+      (rc = dalloc(&d_rp, RMAX)) != SB200_OK || (rc = dalloc(&d_rm, RMAX)) != SB200_OK) {
     cleanup();
     return rc;
   }
@@ -570,9 +719,11 @@ int sb200_batch_autotune(sb200_batch* b, const double* const* psi, double* const
     p.hout = work[s];
     p.acc = nullptr;
     p.d32 = mixed ? (float2*)work[s] + n : nullptr;
+    tmak::TmaMaps m;
+    if (tma && !batch_maps(c, mode, p, m)) continue;  // keep this system's tiles
     double best = 1e300;
     Cand bc = {b->shape[s], b->zchunk[s]};
-    for (const Cand& cd : candidates(c)) {
+    for (const Cand& cd : candidates(c, tma)) {
       BHSys h = hsys_of(c, cd.shape, cd.zchunk);
       const long items = (long)h.ntiles * h.nzc * h.norb;
       int R = (int)std::min<long>(RMAX, std::max<long>(1, (want + items - 1) / items));
@@ -585,10 +736,16 @@ int sb200_batch_autotune(sb200_batch* b, const double* const* psi, double* const
           (rc = h2d(d_rf, rf.data(), (R + 1) * sizeof(long), b->stream)) != SB200_OK ||
           (rc = h2d(d_rp, rp.data(), R * sizeof(BPtr), b->stream)) != SB200_OK)
         break;
+      if (tma) {
+        std::vector<tmak::TmaMaps> rm(R, m);
+        if ((rc = h2d(d_rm, rm.data(), R * sizeof(tmak::TmaMaps), b->stream)) != SB200_OK) break;
+      }
+      const tmak::TmaMaps* maps = tma ? d_rm : nullptr;
       const double2 zc = make_double2(0.0, -1e-3);
-      if ((rc = launch_hpsi_batch(b, mode, d_rep, d_rf, d_rp, R, zc)) != SB200_OK) break;
+      if ((rc = launch_hpsi_batch(b, mode, d_rep, d_rf, d_rp, maps, R, zc)) != SB200_OK) break;
       cudaEventRecord(e0, b->stream);
-      for (int i = 0; i < reps && rc == SB200_OK; ++i) rc = launch_hpsi_batch(b, mode, d_rep, d_rf, d_rp, R, zc);
+      for (int i = 0; i < reps && rc == SB200_OK; ++i)
+        rc = launch_hpsi_batch(b, mode, d_rep, d_rf, d_rp, maps, R, zc);
       cudaEventRecord(e1, b->stream);
       if (rc != SB200_OK) break;
       if (cudaEventSynchronize(e1) != cudaSuccess) {
@@ -671,6 +828,24 @@ int sb200_batch_propagate(sb200_batch* b, double* const* psi_a, double* const* p
       }
     }
   TRY_B(h2d(b->d_hptr, hp.data(), hp.size() * sizeof(BPtr), b->stream));
+  // tensor maps of every (parity, term, system) for the tensor-copy sweep; a
+  // buffer the copy engine cannot address sends this call to the
+  // register-prefetch sweep (same arithmetic, same results)
+  b->tmaps_valid = false;
+  if (family_tma(b)) {
+    std::vector<tmak::TmaMaps> tm(hp.size());
+    bool okm = true;
+    for (int parity = 0; parity < 2 && okm; ++parity)
+      for (int nn = 1; nn <= n_hamil && okm; ++nn) {
+        const size_t t = ((size_t)parity * n_hamil + (nn - 1)) * n;
+        const int mode = term_mode(b->precision, nn, n_hamil);
+        for (int q = 0; q < n && okm; ++q) okm = batch_maps(b->sys[b->order[q]], mode, hp[t + q], tm[t + q]);
+      }
+    if (okm) {
+      TRY_B(h2d(b->d_tmaps, tm.data(), tm.size() * sizeof(tmak::TmaMaps), b->stream));
+      b->tmaps_valid = true;
+    }
+  }
   TRY_B(h2d(b->d_pin, pin.data(), pin.size() * sizeof(void*), b->stream));
   TRY_B(h2d(b->d_opsi, opsi.data(), opsi.size() * sizeof(void*), b->stream));
   std::vector<double2> z(n_hamil);

@@ -18,8 +18,8 @@
 // Loss for training samples (input g, V; offset lowpass(g)/rms(g); target
 // direction t): the misalignment 1 - <p,t>^2 / (<p,p><t,t>) of the
 // preconditioned direction p = offset + y with t, summed over the batch; t is
-// the error of the CG iterate against the converged orbital, orthogonalised to
-// the iterate.
+// minus the part of the CG iterate outside the converged occupied subspace
+// (the training driver, salmon2_b200/learned.py, forms it).
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 

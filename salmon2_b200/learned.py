@@ -10,8 +10,9 @@ this module only orchestrates them:
 * ``collect_samples``: residual -> correction pairs from the plain (low-pass
   preconditioned) solver's own runs: for each iterate x and residual
   g = Hx - <x|H|x> x, the network input is [g/rms(g), V_local], the offset is
-  lowpass(g)/rms(g) and the target direction is the error x* - x of the
-  iterate against the converged orbital, orthogonalised to x.
+  lowpass(g)/rms(g) and the target direction is minus the part of x outside
+  the converged occupied subspace span(x*) -- the error that no rotation
+  within the subspace (Gram-Schmidt, subspace diagonalisation) removes.
 * ``train``: Adam steps through ``sb200_learned_train_step`` on the GPU.
 
 Array preparation uses torch tensors on the device; all network arithmetic
@@ -80,6 +81,7 @@ def collect_samples(ctx, psi0, n_outer=12, ncg=4, tol=1e-10):
     ref = psi0.clone()
     converge(ctx, ref, tol=tol, max_outer=600, precondition="lowpass", ncg=ncg)
     xstar = ref.reshape(s.no, -1)
+    hvol = float(s.grid.hvol)
     shape = s.grid.shape
     V = torch.from_numpy(np.ascontiguousarray(s.V_local[..., 0].ravel(order="F"))).to(xstar)
     x0s, offs, tgts = [], [], []
@@ -92,9 +94,10 @@ def collect_samples(ctx, psi0, n_outer=12, ncg=4, tol=1e-10):
         HX = h.reshape(s.no, -1)
         eps = (X * HX).sum(1, keepdim=True) / (X * X).sum(1, keepdim=True)
         g = HX - eps * X
-        sgn = torch.sign((xstar * X).sum(1, keepdim=True))
-        e = sgn * xstar - X
-        e = e - ((e * X).sum(1, keepdim=True) / (X * X).sum(1, keepdim=True)) * X
+        # error of the iterate against the converged subspace: minus its part
+        # outside span(x*), which no rotation inside the subspace removes
+        # (orthonormal x* in the hvol metric: the projector needs hvol)
+        e = -(X - (X @ xstar.T) @ xstar * hvol)
         rms = torch.sqrt((g * g).mean(1, keepdim=True)).clamp_min(1e-300)
         gn = g / rms
         x0 = torch.stack([gn, V.expand_as(gn)], dim=1)

@@ -82,12 +82,16 @@ def test_batch_tiles_do_not_change_results():
     work = [c.zeros() for c in ctxs]
     psi = [c.upload(p) for c, p in zip(ctxs, psi0)]
     sh, zch = batch.autotune(psi, work, reps=2)
-    assert all(s in (0, 1) for s in sh)
+    assert all(s in (0, 1) for s in sh)  # the register-sweep family stays in it
     assert all(1 <= z <= s.grid.num[2] for z, s in zip(zch, systems))
     p2, r2 = _run_batch(ctxs, batch, psi0, 4, dt, zc)
+    batch.set_tiles([2] * n, [s.grid.num[2] for s in systems])  # tensor-copy sweep, whole z columns
+    sh3, zch3 = batch.autotune(psi, work, reps=2)
+    assert all(s == 2 for s in sh3)
+    p3, r3 = _run_batch(ctxs, batch, psi0, 4, dt, zc)
     for i in range(n):
-        assert np.array_equal(p0[i], p1[i]) and np.array_equal(p0[i], p2[i])
-        assert np.array_equal(r0[i], r1[i]) and np.array_equal(r0[i], r2[i])
+        for p_, r_ in ((p1, r1), (p2, r2), (p3, r3)):
+            assert np.array_equal(p0[i], p_[i]) and np.array_equal(r0[i], r_[i])
     batch.close()
 
 
@@ -113,7 +117,10 @@ def test_batch_errors():
     systems, ctxs, psi0, batch = _setup()
     n = len(systems)
     with pytest.raises(SB200Error) as e:
-        batch.set_tiles([2] * n, [8] * n)
+        batch.set_tiles([3] * n, [8] * n)
+    assert e.value.code == 1
+    with pytest.raises(SB200Error) as e:
+        batch.set_tiles([2] + [0] * (n - 1), [8] * n)  # tensor copies for all systems or none
     assert e.value.code == 1
     with pytest.raises(SB200Error) as e:
         batch.set_tiles([0] * n, [10 ** 6] * n)

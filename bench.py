@@ -70,12 +70,9 @@ def workload(args, rank=0, world=1):
     else:
         nkgrid = 2 if args.small else 4
         s = synth.periodic_system(a=10.26, num=16, nkgrid=nkgrid, no=32, seed=2, name="periodic_bulk")
-    if world > 1:
-        # weak scaling: rank r owns a shifted copy of the k-mesh (a denser
-        # mesh overall); J(t) is summed over ranks with weights 1/(nk*world)
-        shift = (2.0 * np.pi / (10.26 * (2 if args.workload == "supercell" else 1))) * (rank / world) / nkgrid
-        s.vec_k[:] = s.vec_k + shift
-        s.wtk[:] = s.wtk / world
+    # weak scaling: rank r owns a shifted copy of the k-mesh (a denser mesh
+    # overall); J(t) is summed over ranks
+    s = synth.kpoint_shard(s, rank, world, 10.26 * (2 if args.workload == "supercell" else 1), nkgrid)
     nt = args.nt
     dt = 0.08
     omega = 1.55 / synth.AU_ENERGY_EV

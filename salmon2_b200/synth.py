@@ -337,6 +337,21 @@ def isolated_system(num=64, h_aa=0.25, no=5, natom=4, seed=1, rc_aa=1.2, nspin=1
                   int(np.prod(grid.num)), seed, name)
 
 
+def kpoint_shard(system: System, rank: int, world: int, a_cell: float, nkgrid: int) -> System:
+    """Weak-scaling shard of a periodic system for rank `rank` of `world`: the
+    k-mesh shifted by rank/world of one mesh spacing along every axis (so the
+    shards together sample a `world`-times denser mesh) and the k-weights
+    divided by `world`; orbitals, grid and potential are shared.  The current
+    of the whole job is the sum of the shards' currents (calc_current sums
+    occupation x k-weight terms, density_matrix.f90:240-463)."""
+    import dataclasses
+    if world <= 1:
+        return system
+    shift = (2.0 * np.pi / a_cell) * (rank / world) / nkgrid
+    return dataclasses.replace(system, vec_k=np.asfortranarray(system.vec_k + shift),
+                               wtk=np.asarray(system.wtk) / world)
+
+
 def uneven_batch(nsys=16, seed=4):
     """Independent isolated systems of uneven size from one seed: cubic grids
     n^3 with n in {32, 40, ..., 96}, 4..64 orbitals, 2..16 atoms (h = 0.25 A,

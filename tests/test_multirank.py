@@ -1,0 +1,63 @@
+"""The k-point sharding of the multi-GPU path, run as two gloo ranks on the
+CPU with the oracle as the per-rank propagator: the all-reduced current of
+the shards equals the current of one run over the merged, denser k-mesh."""
+import dataclasses
+import os
+
+import numpy as np
+import pytest
+
+NT, DT = 3, 0.08
+
+
+def _system():
+    from salmon2_b200 import synth
+    return synth.periodic_system(a=10.26, num=12, nkgrid=1, no=2, seed=41, name="shard12")
+
+
+def _field():
+    from salmon2_b200 import synth
+    return synth.asin2cos(NT, DT, omega=0.05696, f0=0.05696 * 2e-2, tw=NT * DT), synth.taylor_zc(DT)
+
+
+def _rank_main(rank, world, port, out):
+    import torch
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    from oracle import Oracle
+    from salmon2_b200 import synth
+    s = synth.kpoint_shard(_system(), rank, world, 10.26, 1)
+    Ac, zc = _field()
+    cur = Oracle(s, threads=1).rt_run(s.psi, NT, DT, zc, Ac_ext=Ac)["curr"]
+    t = torch.from_numpy(np.ascontiguousarray(cur))
+    dist.all_reduce(t)
+    if rank == 0:
+        np.save(out, t.numpy())
+    dist.destroy_process_group()
+
+
+def test_two_rank_current_equals_merged_kmesh(tmp_path):
+    import socket
+
+    import torch.multiprocessing as mp
+    from oracle import Oracle
+    from salmon2_b200 import synth
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    out = str(tmp_path / "j.npy")
+    mp.start_processes(_rank_main, args=(2, port, out), nprocs=2, join=True, start_method="spawn")
+    j_ranks = np.load(out)
+    # one process over the merged mesh: both shards' k-points, orbitals and weights
+    base = _system()
+    sh = [synth.kpoint_shard(base, r, 2, 10.26, 1) for r in range(2)]
+    merged = dataclasses.replace(
+        base, nk=2, vec_k=np.asfortranarray(np.concatenate([x.vec_k for x in sh], axis=1)),
+        wtk=np.concatenate([x.wtk for x in sh]),
+        rocc=np.asfortranarray(np.concatenate([x.rocc for x in sh], axis=1)),
+        psi=np.asfortranarray(np.concatenate([x.psi for x in sh], axis=5)))
+    assert abs(np.sum(merged.wtk) - 1.0) < 1e-15
+    Ac, zc = _field()
+    j_merged = Oracle(merged, threads=1).rt_run(merged.psi, NT, DT, zc, Ac_ext=Ac)["curr"]
+    assert np.max(np.abs(j_ranks - j_merged)) <= 1e-12 * np.max(np.abs(j_merged))

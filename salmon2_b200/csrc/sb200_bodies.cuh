@@ -63,14 +63,10 @@ __device__ __forceinline__ void project_atom(const TIN* __restrict__ in, double2
     for (int j = lane; j < m; j += 32) {
       const TIN vi = __ldg(psi + a.pt_lin[start + j]);
       const double2 v = make_double2((double)vi.x, (double)vi.y);
-      const double2 e = __ldg(ph + j);
+      const double2 ev = cmul(__ldg(ph + j), v);  // conj(zekr_uV) / uV times psi
 #pragma unroll
       for (int q = 0; q < NP; ++q) {
-        if (q0 + q < np) {
-          const double uv = __ldg(a.uv + (long)(lma0 + q0 + q) * a.nps + j);
-          const double2 zk = make_double2(e.x * uv, e.y * uv);  // conj(zekr_uV)
-          acc[q] = cadd(acc[q], cmul(zk, v));
-        }
+        if (q0 + q < np) acc[q] = cadd(acc[q], cscal(__ldg(a.uv + (long)(lma0 + q0 + q) * a.nps + j), ev));
       }
     }
 #pragma unroll

@@ -48,13 +48,10 @@ __device__ void project_from_smem(const double2* __restrict__ sm, double2* __res
       for (int q = 0; q < 4; ++q) acc[q] = make_double2(0.0, 0.0);
       for (int j = lane; j < m; j += 32) {
         const double2 v = sm[__ldg(a.pt_lin + start + j)];
-        const double2 e = __ldg(ph + start + j);
+        const double2 ev = cmul(__ldg(ph + start + j), v);  // conj(zekr)/uV times psi
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-          if (q0 + q < np) {
-            const double uv = __ldg(a.uv + (long)(lma0 + q0 + q) * a.nps + j);
-            acc[q] = cadd(acc[q], cmul(make_double2(e.x * uv, e.y * uv), v));
-          }
+          if (q0 + q < np) acc[q] = cadd(acc[q], cscal(__ldg(a.uv + (long)(lma0 + q0 + q) * a.nps + j), ev));
         }
       }
 #pragma unroll
@@ -79,40 +76,60 @@ __device__ void project_from_smem(const double2* __restrict__ sm, double2* __res
 template <int NWARP>
 __device__ void current_nonlocal_from_smem(const double2* __restrict__ sm, const OrbArgs& a, int ik,
                                            double* __restrict__ wsum /* [NWARP][3] */) {
+  // one pass over the atom's sphere per four projectors: e psi(pt) once per
+  // point, then <zekr|psi> and <r_d zekr|psi> of each projector
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const double2* ph = a.phase + (long)ik * a.totpts;
   double jx = 0.0, jy = 0.0, jz = 0.0;
   for (int atom = warp; atom < a.natom; atom += NWARP) {
     const int start = a.atom_start[atom], m = a.mps[atom];
     const int lma0 = a.lma_start[atom], np = a.nproj[atom];
-    for (int q = 0; q < np; ++q) {
-      double2 u = make_double2(0.0, 0.0), u0 = u, u1 = u, u2 = u;
+    for (int q0 = 0; q0 < np; q0 += 4) {
+      double2 u[4], ur[4][3];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        u[q] = make_double2(0.0, 0.0);
+        ur[q][0] = ur[q][1] = ur[q][2] = u[q];
+      }
+#pragma unroll 2
       for (int j = lane; j < m; j += 32) {
         const double2 v = sm[__ldg(a.pt_lin + start + j)];
-        const double2 e = __ldg(ph + start + j);
-        const double uv = __ldg(a.uv + (long)(lma0 + q) * a.nps + j);
-        const double2 zk = make_double2(e.x * uv, e.y * uv);
+        const double2 ev = cmul(__ldg(ph + start + j), v);
         const double* r = a.pt_r + 3L * (start + j);
-        u = cadd(u, cmul(zk, v));
-        u0 = cadd(u0, cmul(cscal(__ldg(r), zk), v));
-        u1 = cadd(u1, cmul(cscal(__ldg(r + 1), zk), v));
-        u2 = cadd(u2, cmul(cscal(__ldg(r + 2), zk), v));
+        const double r0 = __ldg(r), r1 = __ldg(r + 1), r2 = __ldg(r + 2);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          if (q0 + q < np) {
+            const double2 tq = cscal(__ldg(a.uv + (long)(lma0 + q0 + q) * a.nps + j), ev);
+            u[q] = cadd(u[q], tq);
+            ur[q][0] = cadd(ur[q][0], cscal(r0, tq));
+            ur[q][1] = cadd(ur[q][1], cscal(r1, tq));
+            ur[q][2] = cadd(ur[q][2], cscal(r2, tq));
+          }
+        }
       }
 #pragma unroll
-      for (int off = 16; off > 0; off >>= 1) {
-        u.x += __shfl_xor_sync(0xffffffffu, u.x, off);
-        u.y += __shfl_xor_sync(0xffffffffu, u.y, off);
-        u0.x += __shfl_xor_sync(0xffffffffu, u0.x, off);
-        u0.y += __shfl_xor_sync(0xffffffffu, u0.y, off);
-        u1.x += __shfl_xor_sync(0xffffffffu, u1.x, off);
-        u1.y += __shfl_xor_sync(0xffffffffu, u1.y, off);
-        u2.x += __shfl_xor_sync(0xffffffffu, u2.x, off);
-        u2.y += __shfl_xor_sync(0xffffffffu, u2.y, off);
+      for (int q = 0; q < 4; ++q) {
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+          u[q].x += __shfl_xor_sync(0xffffffffu, u[q].x, off);
+          u[q].y += __shfl_xor_sync(0xffffffffu, u[q].y, off);
+#pragma unroll
+          for (int d = 0; d < 3; ++d) {
+            ur[q][d].x += __shfl_xor_sync(0xffffffffu, ur[q][d].x, off);
+            ur[q][d].y += __shfl_xor_sync(0xffffffffu, ur[q][d].y, off);
+          }
+        }
       }
-      const double2 us = cscal(__ldg(a.rinv + lma0 + q), u);
-      jx += u0.x * us.y - u0.y * us.x;
-      jy += u1.x * us.y - u1.y * us.x;
-      jz += u2.x * us.y - u2.y * us.x;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        if (q0 + q < np) {
+          const double2 us = cscal(__ldg(a.rinv + lma0 + q0 + q), u[q]);
+          jx += ur[q][0].x * us.y - ur[q][0].y * us.x;
+          jy += ur[q][1].x * us.y - ur[q][1].y * us.x;
+          jz += ur[q][2].x * us.y - ur[q][2].y * us.x;
+        }
+      }
     }
   }
   if (lane == 0) {

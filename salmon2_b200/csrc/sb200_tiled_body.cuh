@@ -63,6 +63,35 @@ __device__ __forceinline__ T cmul(T a, T b) {
   return r;
 }
 
+// Packed FP32 forms (sm_100 f32x2 instructions): one instruction per complex
+// add / scale / fused multiply-add instead of two; every rounding is the
+// scalar one (round to nearest per component).
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) {
+  return __ffma2_rn(b, make_float2(-1.f, -1.f), a);
+}
+__device__ __forceinline__ float2 cscal(float s, float2 a) { return __fmul2_rn(make_float2(s, s), a); }
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return __ffma2_rn(make_float2(-a.y, a.y), make_float2(b.y, b.x), __fmul2_rn(make_float2(a.x, a.x), b));
+}
+
+// acc + l x (fused per component)
+__device__ __forceinline__ double2 cfma(double l, double2 x, double2 acc) {
+  return make_double2(fma(l, x.x, acc.x), fma(l, x.y, acc.y));
+}
+__device__ __forceinline__ float2 cfma(float l, float2 x, float2 acc) {
+  return __ffma2_rn(make_float2(l, l), x, acc);
+}
+
+// vl c + lap0 c - v / 2: the local-potential, k_lap0 and Laplacian part of
+// the stencil value (zstencil_typical_seq, seq.f90:112-118)
+__device__ __forceinline__ double2 hcore(double vl, double lap0, double2 c, double2 v) {
+  return make_double2(fma(-0.5, v.x, fma(vl, c.x, lap0 * c.x)), fma(-0.5, v.y, fma(vl, c.y, lap0 * c.y)));
+}
+__device__ __forceinline__ float2 hcore(float vl, float lap0, float2 c, float2 v) {
+  return __ffma2_rn(make_float2(-0.5f, -0.5f), v, __ffma2_rn(make_float2(vl, vl), c, cscal(lap0, c)));
+}
+
 // wrap (periodic) or test (Dirichlet) a coordinate that may be up to 4 outside
 __device__ __forceinline__ int wrapc(int q, int n, int periodic, bool& ok) {
   if (periodic) {
@@ -224,8 +253,8 @@ __device__ __forceinline__ void tiled_body(const typename Cx<typename ModeT<MODE
           im = ctr - s;
         }
         const C2 tp = P[ip], tm = P[im];
-        vx = cadd(vx, cscal((R)a.lapt[s - 1], cadd(tp, tm)));
-        if (GRAD) wx = cadd(wx, cscal((R)a.nab[s - 1], csub(tp, tm)));
+        vx = cfma((R)a.lapt[s - 1], cadd(tp, tm), vx);
+        if (GRAD) wx = cfma((R)a.nab[s - 1], csub(tp, tm), wx);
       }
 #pragma unroll
       for (int s = 1; s <= ND; ++s) {
@@ -238,22 +267,21 @@ __device__ __forceinline__ void tiled_body(const typename Cx<typename ModeT<MODE
           im = ctr - s * SX;
         }
         const C2 tp = P[ip], tm = P[im];
-        vy = cadd(vy, cscal((R)a.lapt[4 + s - 1], cadd(tp, tm)));
-        if (GRAD) wy = cadd(wy, cscal((R)a.nab[4 + s - 1], csub(tp, tm)));
+        vy = cfma((R)a.lapt[4 + s - 1], cadd(tp, tm), vy);
+        if (GRAD) wy = cfma((R)a.nab[4 + s - 1], csub(tp, tm), wy);
       }
 #pragma unroll
       for (int s = 0; s < ND; ++s) {
         const C2 tp = w[ND + 1 + s], tm = w[ND - 1 - s];
-        vz = cadd(vz, cscal((R)a.lapt[8 + s], cadd(tp, tm)));
-        if (GRAD) wz = cadd(wz, cscal((R)a.nab[8 + s], csub(tp, tm)));
+        vz = cfma((R)a.lapt[8 + s], cadd(tp, tm), vz);
+        if (GRAD) wz = cfma((R)a.nab[8 + s], csub(tp, tm), wz);
       }
       const C2 v = cadd(vz, cadd(vy, vx));
-      const C2 ww = cadd(cscal(kz, wz), cadd(cscal(ky, wy), cscal(kx, wx)));
+      const C2 ww = cfma(kz, wz, cfma(ky, wy, cscal(kx, wx)));
       const C2 c = w[ND];
       const long p = (long)z * sz + pxy;
-      C2 h;
-      h.x = vl * c.x + lap0 * c.x - (R)0.5 * v.x;
-      h.y = vl * c.y + lap0 * c.y - (R)0.5 * v.y;
+      C2 h;  // stencil value, then + KB term
+      h = hcore(vl, lap0, c, v);
       if (GRAD) {
         h.x += ww.y;
         h.y -= ww.x;

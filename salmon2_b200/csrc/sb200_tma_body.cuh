@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <type_traits>
 
 #include "sb200_internal.cuh"
 #include "sb200_stencil.cuh"
@@ -21,6 +22,7 @@ using namespace tiled;
 constexpr int TX = 32, TY = 8, NT = TX * TY, HALO = ND;
 constexpr int RING = 8;   // input planes resident / in flight
 constexpr int ARING = 4;  // accumulator planes in flight
+constexpr int TMA_MAX_NLMA = 512;  // projections staged in shared memory (else read from global)
 
 struct TmaMaps {
   CUtensorMap in;    // input planes: (2 SX) x SY box, or (2 TX) x TY for the periodic centre rows
@@ -45,7 +47,8 @@ struct Geo {
   static constexpr size_t ACC_OFF = RING_OFF + (size_t)RING * PLANE_BYTES;
   static constexpr size_t D32_OFF = ACC_OFF + (size_t)ARING * ACC_BYTES;
   static constexpr size_t BAR_OFF = D32_OFF + (size_t)ARING * D32_BYTES;
-  static constexpr size_t SMEM = BAR_OFF + (RING + ARING) * sizeof(uint64_t) + 128;  // + alignment slack
+  static constexpr size_t PS_OFF = BAR_OFF + 128;  // projections of the item's orbital
+  static constexpr size_t SMEM = PS_OFF + (size_t)TMA_MAX_NLMA * 16 + 128;  // + alignment slack
 };
 
 template <int MODE, bool PER>
@@ -79,6 +82,19 @@ __device__ __forceinline__ void issue_acc(const TmaMaps& m, unsigned char* base,
   if (G::D32) tma::tensor_load_4d(base + G::D32_OFF + (size_t)slot * G::D32_BYTES, &m.d32, 2 * x0, y0, z, o, &abar[slot]);
 }
 
+// f(integral_constant<J>, k0 + J) for J = J0 .. N-1 while k0 + J < nsteps;
+// false as soon as one call returns false
+template <int J, int N, typename F>
+__device__ __forceinline__ bool run_steps(F& f, int k0, int nsteps) {
+  if constexpr (J < N) {
+    if (k0 + J >= nsteps) return true;
+    if (!f(std::integral_constant<int, J>{}, k0 + J)) return false;
+    return run_steps<J + 1, N>(f, k0, nsteps);
+  } else {
+    return true;
+  }
+}
+
 // One work item: tile bx, z chunk by, orbital bz.  `base` is the 128-byte
 // aligned shared-memory area of Geo<MODE, PER>; its barriers are initialised
 // by the caller and keep their phases across items in pmask / amask (bit s =
@@ -97,6 +113,7 @@ __device__ __forceinline__ bool tma_body(const TmaMaps& maps, void* __restrict__
   const double2* accr = (const double2*)(base + G::ACC_OFF);
   const float2* d32r = (const float2*)(base + G::D32_OFF);
   uint64_t* pbar = (uint64_t*)(base + G::BAR_OFF);
+  double2* psm = (double2*)(base + G::PS_OFF);
   uint64_t* abar = pbar + RING;
 
   const int t = threadIdx.x;
@@ -132,6 +149,11 @@ __device__ __forceinline__ bool tma_body(const TmaMaps& maps, void* __restrict__
   p_issued = pro;
   if (G::ACC64 || G::D32) a_issued = nsteps < ARING ? nsteps : ARING;
 
+  // projections of this orbital into shared memory (read before the first
+  // barrier below; the previous item's readers have all passed its last barrier)
+  const bool ps_smem = a.nlma > 0 && a.nlma <= TMA_MAX_NLMA;
+  if (ps_smem)
+    for (int i = t; i < a.nlma; i += NT) psm[i] = a.proj[(long)o * a.nlma + i];
   bool ok = true;
   C2 w[2 * HALO + 1];
   // window planes zc0-4 .. zc0+3
@@ -157,12 +179,19 @@ __device__ __forceinline__ bool tma_body(const TmaMaps& maps, void* __restrict__
     else vsrc = (const R*)(a.vloc32 + (long)ispin * a.npts);
     R vl_n = active ? __ldg(vsrc + (long)zc0 * sz + pxy) : (R)0;
     int pm_n = (active && a.nlma > 0) ? __ldg(a.pmap + (long)zc0 * sz + pxy) : -1;
-    for (int k = 0; k < nsteps; ++k) {
+    // FP64 stencils: the window rotates through the registers -- in step j of
+    // a group of nine, plane z - 4 + i sits in w[(j + i) % 9] (constant
+    // indices, no moves); FP32 stencils (issue-bound, code-size sensitive)
+    // shift the window after each step instead (j = 0 throughout)
+    constexpr int NWIN = 2 * HALO + 1;
+    constexpr bool ROTATE = (MODE < 6);
+    auto step = [&](auto jc, const int k) -> bool {
+      constexpr int j = decltype(jc)::value;
       const int z = zc0 + k;
       const int rf = k + 2 * HALO;  // plane z+4 feeds the window
       ok = tma::mbar_wait(&pbar[rf & (RING - 1)], (pmask >> (rf & (RING - 1))) & 1u) && ok;
       pmask ^= 1u << (rf & (RING - 1));
-      w[2 * HALO] = ring[(size_t)(rf & (RING - 1)) * G::PLANE + ctr];
+      w[(j + 2 * HALO) % NWIN] = ring[(size_t)(rf & (RING - 1)) * G::PLANE + ctr];
       p_waited = rf + 1;
       if (G::ACC64 || G::D32) {
         ok = tma::mbar_wait(&abar[k & (ARING - 1)], (amask >> (k & (ARING - 1))) & 1u) && ok;
@@ -188,47 +217,49 @@ __device__ __forceinline__ bool tma_body(const TmaMaps& maps, void* __restrict__
             tp = P[ctr + s];
             tm = P[ctr - s];
           }
-          vx = cadd(vx, cscal((R)a.lapt[s - 1], cadd(tp, tm)));
-          if (GRAD) wx = cadd(wx, cscal((R)a.nab[s - 1], csub(tp, tm)));
+          vx = cfma((R)a.lapt[s - 1], cadd(tp, tm), vx);
+          if (GRAD) wx = cfma((R)a.nab[s - 1], csub(tp, tm), wx);
         }
 #pragma unroll
         for (int s = 1; s <= HALO; ++s) {
           const C2 tp = P[ctr + s * SX], tm = P[ctr - s * SX];
-          vy = cadd(vy, cscal((R)a.lapt[4 + s - 1], cadd(tp, tm)));
-          if (GRAD) wy = cadd(wy, cscal((R)a.nab[4 + s - 1], csub(tp, tm)));
+          vy = cfma((R)a.lapt[4 + s - 1], cadd(tp, tm), vy);
+          if (GRAD) wy = cfma((R)a.nab[4 + s - 1], csub(tp, tm), wy);
         }
 #pragma unroll
         for (int s = 0; s < HALO; ++s) {
-          const C2 tp = w[HALO + 1 + s], tm = w[HALO - 1 - s];
-          vz = cadd(vz, cscal((R)a.lapt[8 + s], cadd(tp, tm)));
-          if (GRAD) wz = cadd(wz, cscal((R)a.nab[8 + s], csub(tp, tm)));
+          const C2 tp = w[(j + HALO + 1 + s) % NWIN], tm = w[(j + HALO - 1 - s) % NWIN];
+          vz = cfma((R)a.lapt[8 + s], cadd(tp, tm), vz);
+          if (GRAD) wz = cfma((R)a.nab[8 + s], csub(tp, tm), wz);
         }
         const C2 v = cadd(vz, cadd(vy, vx));
-        const C2 c = w[HALO];
-        C2 h;
-        h.x = vl * c.x + lap0 * c.x - (R)0.5 * v.x;
-        h.y = vl * c.y + lap0 * c.y - (R)0.5 * v.y;
+        const C2 c = w[(j + HALO) % NWIN];
+        C2 h;  // stencil value, then + KB term
+        h = hcore(vl, lap0, c, v);
         if (GRAD) {
-          const C2 ww = cadd(cscal(kz, wz), cadd(cscal(ky, wy), cscal(kx, wx)));
+          const C2 ww = cfma(kz, wz, cfma(ky, wy, cscal(kx, wx)));
           h.x += ww.y;
           h.y -= ww.x;
         }
         if (a.nlma > 0 && pm >= 0) {
-          const double2* pj = a.proj + (long)o * a.nlma;
+          const double2* pj = ps_smem ? psm : a.proj + (long)o * a.nlma;
           const double2* zk = a.ent_zk + (a.phase_per_k ? (long)ik * a.nent : 0L);
           const int e0 = pm >> 8, e1 = e0 + (pm & 255);
-          for (int e = e0; e < e1; e += 4) {  // entries four at a time, summed in entry order
-            double2 pv[4], zv[4];
+          for (int e = e0; e < e1; e += 8) {  // entries eight at a time, summed in entry order
+            int l[8];
+            double2 zv[8];
 #pragma unroll
-            for (int i = 0; i < 4; ++i) {
+            for (int i = 0; i < 8; ++i) {
               const int ee = min(e + i, e1 - 1);
-              pv[i] = pj[__ldg(a.ent_lma + ee)];
+              l[i] = __ldg(a.ent_lma + ee);
               zv[i] = __ldg(zk + ee);
             }
 #pragma unroll
-            for (int i = 0; i < 4; ++i)
-              if (e + i < e1)
-                h = cadd(h, cmul(Cx<R>::make((R)pv[i].x, (R)pv[i].y), Cx<R>::make((R)zv[i].x, (R)zv[i].y)));
+            for (int i = 0; i < 8; ++i)
+              if (e + i < e1) {
+                const double2 pv = pj[l[i]];
+                h = cadd(h, cmul(Cx<R>::make((R)pv.x, (R)pv.y), Cx<R>::make((R)zv[i].x, (R)zv[i].y)));
+              }
           }
         }
         const long gi = (long)o * a.npts + (long)z * sz + pxy;
@@ -257,10 +288,8 @@ __device__ __forceinline__ bool tma_body(const TmaMaps& maps, void* __restrict__
           acc[gi] = cadd(accr[ti], make_double2((double)tt.x, (double)tt.y));
         }
       }
-#pragma unroll
-      for (int i = 0; i < 2 * HALO; ++i) w[i] = w[i + 1];
       all_ok = __syncthreads_and(ok);
-      if (!all_ok) break;
+      if (!all_ok) return false;
       if (t == 0) {  // refill the slots of plane z and of accumulator step k
         tma::fence_proxy_async_smem();
         const int rn = k + RING + HALO;  // plane z+8
@@ -270,6 +299,17 @@ __device__ __forceinline__ bool tma_body(const TmaMaps& maps, void* __restrict__
       }
       if (k + RING + HALO < ntot) p_issued = k + RING + HALO + 1;
       if ((G::ACC64 || G::D32) && k + ARING < nsteps) a_issued = k + ARING + 1;
+      return true;
+    };
+    if (ROTATE) {
+      for (int k0 = 0; k0 < nsteps; k0 += NWIN)
+        if (!run_steps<0, NWIN>(step, k0, nsteps)) break;
+    } else {
+      for (int k = 0; k < nsteps; ++k) {
+        if (!step(std::integral_constant<int, 0>{}, k)) break;
+#pragma unroll
+        for (int i = 0; i < 2 * HALO; ++i) w[i] = w[i + 1];
+      }
     }
   }
   if (!all_ok) {

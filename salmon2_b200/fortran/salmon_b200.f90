@@ -17,6 +17,9 @@ module salmon_b200
   integer(c_int), parameter :: SB200_OK = 0
   integer(c_int), parameter :: SB200_PREC_FP64 = 0, SB200_PREC_MIXED = 1
   integer(c_int), parameter :: SB200_TRANS_TR = 0, SB200_TRANS_LO = 1
+  integer(c_int), parameter :: SB200_PRECOND_NONE = 0, SB200_PRECOND_LOWPASS = 1, SB200_PRECOND_LEARNED = 2
+  integer(c_int), parameter :: SB200_TILE_32x8 = 0, SB200_TILE_16x16 = 1, SB200_TILE_32x8_TMA = 2
+  integer(c_int), parameter :: SB200_LEARNED_NPARAM = 8241
 
   interface
     integer(c_int) function sb200_ctx_create(device, ctx) bind(c, name="sb200_ctx_create")
@@ -153,6 +156,83 @@ module salmon_b200
       real(c_double), intent(in) :: Ac_ext(3,0:*)
       real(c_double), intent(inout) :: curr(3,*), rbox(4,*), Ac_tot(3,0:*)
       type(c_ptr) :: psi_final
+    end function
+
+    ! ---- ground state (real orbitals) ----
+    integer(c_int) function sb200_gs_from_ref(ctx, rwf_ref, psi_dev) bind(c, name="sb200_gs_from_ref")
+      import
+      type(c_ptr), value :: ctx, psi_dev
+      real(c_double), intent(in) :: rwf_ref(*)
+    end function
+
+    integer(c_int) function sb200_gs_to_ref(ctx, psi_dev, rwf_ref) bind(c, name="sb200_gs_to_ref")
+      import
+      type(c_ptr), value :: ctx, psi_dev
+      real(c_double), intent(inout) :: rwf_ref(*)
+    end function
+
+    integer(c_int) function sb200_hpsi_real(ctx, tpsi, htpsi) bind(c, name="sb200_hpsi_real")
+      import
+      type(c_ptr), value :: ctx, tpsi, htpsi
+    end function
+
+    integer(c_int) function sb200_gscg(ctx, psi, ncg, precondition, alpha_pre, esp) bind(c, name="sb200_gscg")
+      import
+      type(c_ptr), value :: ctx, psi
+      integer(c_int), value :: ncg, precondition
+      real(c_double), value :: alpha_pre
+      real(c_double), intent(inout) :: esp(*)
+    end function
+
+    integer(c_int) function sb200_gram_schmidt_real(ctx, psi) bind(c, name="sb200_gram_schmidt_real")
+      import
+      type(c_ptr), value :: ctx, psi
+    end function
+
+    integer(c_int) function sb200_subspace_diag_real(ctx, psi, evals) bind(c, name="sb200_subspace_diag_real")
+      import
+      type(c_ptr), value :: ctx, psi
+      real(c_double), intent(inout) :: evals(*)
+    end function
+
+    integer(c_int) function sb200_learned_init(ctx, params, nparam, batch) bind(c, name="sb200_learned_init")
+      import
+      type(c_ptr), value :: ctx
+      real(c_float), intent(in) :: params(*)
+      integer(c_int), value :: nparam, batch
+    end function
+
+    ! ---- batches of independent isolated systems ----
+    integer(c_int) function sb200_batch_create(systems, nsys, batch) bind(c, name="sb200_batch_create")
+      import
+      type(c_ptr), intent(in) :: systems(*)
+      integer(c_int), value :: nsys
+      type(c_ptr) :: batch
+    end function
+
+    integer(c_int) function sb200_batch_destroy(batch) bind(c, name="sb200_batch_destroy")
+      import
+      type(c_ptr), value :: batch
+    end function
+
+    integer(c_int) function sb200_batch_autotune(batch, psi, work, reps, shape, zchunk) &
+        bind(c, name="sb200_batch_autotune")
+      import
+      type(c_ptr), value :: batch
+      type(c_ptr), intent(in) :: psi(*), work(*)
+      integer(c_int), value :: reps
+      integer(c_int), intent(inout) :: shape(*), zchunk(*)
+    end function
+
+    integer(c_int) function sb200_batch_propagate(batch, psi_a, psi_b, work, nt, dt, zc, n_hamil, rbox, psi_final) &
+        bind(c, name="sb200_batch_propagate")
+      import
+      type(c_ptr), value :: batch
+      type(c_ptr), intent(in) :: psi_a(*), psi_b(*), work(*), rbox(*)
+      integer(c_int), value :: nt, n_hamil
+      real(c_double), value :: dt
+      complex(c_double_complex), intent(in) :: zc(*)
+      type(c_ptr), intent(inout) :: psi_final(*)
     end function
   end interface
 

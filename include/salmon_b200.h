@@ -201,6 +201,7 @@ int sb200_gs_to_ref(sb200_ctx* ctx, const double* psi_dev, double* rwf_ref);
 int sb200_hpsi_real(sb200_ctx* ctx, const double* tpsi, double* htpsi);
 /* ncg iterations of the band-by-band CG with 2x2 Rayleigh-Ritz per orbital;
  * precondition = SB200_PRECOND_*; esp (host, nspin*no) gets <x|H|x>/<x|x>.
+ * With SB200_PRECOND_LEARNED the conjugation restarts every iteration.
  * Replaces: gscg_rwf (src/gs/conjugate_gradient.f90:21-466) and
  * preconditioning_rgk / dstencil_preconditioning (src/gs/preconditioning.f90:25-77). */
 int sb200_gscg(sb200_ctx* ctx, double* psi, int ncg, int precondition, double alpha_pre, double* esp);

@@ -183,6 +183,7 @@ __device__ __forceinline__ void finalize_body(const FinArgs& a) {
     for (int d = 0; d < 3; ++d) A[d] = a.A_direct ? a.Ac_cur[d] : a.Ac_cur[3 * itt + d];
   }
   double s[7] = {0, 0, 0, 0, 0, 0, 0};
+#pragma unroll 4
   for (int o = threadIdx.x; o < a.norb; o += blockDim.x) {
     if (a.spin_filter >= 0 && (o % a.nspin) != a.spin_filter) continue;
     double q[OBS_NQ] = {0, 0, 0, 0, 0, 0, 0};

@@ -634,6 +634,22 @@ int gs_rotate(sb200_ctx* c, const double* X, int m, const double* M_dev, int n, 
 }
 
 // y <- y - sum_i coeff[i] * X_i  (exc accumulated in i order, then subtracted)
+// Y -= X (X^T Y) hvol for Y of n orbitals: removes from every column of Y its
+// components along the m orthonormal orbitals X (scratch: the small-matrix area)
+int gs_project_out(sb200_ctx* c, const double* X, int m, double* Y, int n) {
+  if (c->gs.mat_cap < (size_t)m * n) {
+    dfree(c->gs.d_mat);
+    TRY_GS(dalloc(&c->gs.d_mat, (size_t)m * n));
+    c->gs.mat_cap = (size_t)m * n;
+  }
+  // gs_gram(Y, X) stores <Y_j, X_i> at j*m + i: the column-major M(i, j) k_rotate reads
+  TRY_GS(gs_gram(c, Y, n, X, m, c->g.hvol, c->gs.d_mat));
+  dim3 g((unsigned)((c->g.npts + 255) / 256), (n + GT - 1) / GT);
+  k_rotate<<<g, 256, 0, c->stream>>>(X, m, c->gs.d_mat, n, c->g.npts, -1.0, 1.0, Y);
+  SB_LAUNCH_CHECK("k_rotate");
+  return SB200_OK;
+}
+
 int gs_rotate_sub(sb200_ctx* c, const double* X, int m, const double* coeff_dev, double* y) {
   dim3 g((unsigned)((c->g.npts + 255) / 256), 1);
   k_rotate<<<g, 256, 0, c->stream>>>(X, m, coeff_dev, 1, c->g.npts, -1.0, 1.0, y);
@@ -768,13 +784,15 @@ int sb200_gscg(sb200_ctx* c, double* psi, int ncg, int precondition, double alph
       TRY_GS(gs_dots(c, 1, pre, gk));
       g_for_p = pre;
     } else if (precondition == SB200_PRECOND_LEARNED) {
-      TRY_GS(learned_precond_apply(c, gk, pre));
+      TRY_GS(learned_precond_apply(c, gk, xk, pre));
       TRY_GS(gs_dots(c, 1, pre, gk));
       g_for_p = pre;
     } else {
       TRY_GS(gs_dots(c, 1, gk, gk));
     }
-    TRY_GS(gs_scalars(c, 1, iter));
+    // the network direction is not a fixed linear preconditioner: with it the
+    // conjugation restarts every iteration (uk = 0, as in the first iteration)
+    TRY_GS(gs_scalars(c, 1, precondition == SB200_PRECOND_LEARNED ? 1 : iter));
     TRY_GS(gs_update(c, U_PK, pk, (double*)g_for_p));
     TRY_GS(gs_dots(c, 1, xk, pk));
     TRY_GS(gs_scalars(c, 2, iter));

@@ -213,7 +213,9 @@ int kernel_timing_flush(sb200_ctx* c);
 // low-pass preconditioner of the ground-state CG (sb200_gs.cu)
 int gs_precond(sb200_ctx* c, const double* g, double* pre, double alpha);
 // learned preconditioner: pre = net(g, V_local) for every orbital (sb200_learned.cu)
-int learned_precond_apply(sb200_ctx* c, const double* g, double* pre);
+int learned_precond_apply(sb200_ctx* c, const double* g, const double* x, double* pre);
+// Y -= X (X^T Y) hvol: components of n orbitals Y along m orthonormal X removed (sb200_gs.cu)
+int gs_project_out(sb200_ctx* c, const double* X, int m, double* Y, int n);
 void learned_free(sb200_ctx* c);
 
 }  // namespace sb200

@@ -7,7 +7,8 @@
 //   x1 = relu(conv3(x0; W1, b1))                C channels
 //   x2 = relu(conv3(x1; W2, b2))                C channels
 //   y  = conv3(x2; W3, b3)                      1 channel
-//   p     = lowpass(g) + rms(g) * y             (lowpass = preconditioning.f90:25-77)
+//   corr  = rms(g) * y, minus its components along the current orbitals
+//   p     = lowpass(g) + corr                   (lowpass = preconditioning.f90:25-77)
 //   pre_g = +p or -p, whichever keeps <pre_g, g> >= <lowpass(g), g> / 5,
 //           else lowpass(g) (k_apply_direction)
 // conv3 is a 3x3x3 convolution.  Weights are kept as FP32 masters and used as
@@ -65,7 +66,9 @@ struct Net {
   float* d_wpart = nullptr;   // weight-gradient partials
   long wpart_cap = 0;
   float* d_scale = nullptr;   // per-orbital rms(g)
-  double* d_dots = nullptr;   // CG hook: per-orbital <pre, g> partials [B][32][2]
+  double* d_dots = nullptr;   // CG hook: per-orbital <pre, g> partials [norb][32][2]
+  double* d_corr = nullptr;   // CG hook: network corrections of all orbitals [norb][npts]
+  size_t corr_cap = 0;
 };
 
 // ---- conv forward: out[co][p] = b[co] + sum_ci sum_k W[co][ci][k] in[ci][p+k] ----
@@ -302,19 +305,26 @@ __global__ void k_make_input(const double* __restrict__ g, const double* __restr
   }
 }
 
-// Partial sums of d0 = <lowpass(g), g> and d1 = <rms(g) y, g> per orbital.
-__global__ void __launch_bounds__(256) k_dir_dots_part(const double* __restrict__ pre, const double* __restrict__ g,
-                                                       const float* __restrict__ y, const float* __restrict__ scale,
-                                                       long npts, int o0, double* __restrict__ part, int nblk) {
-  __shared__ double r0[256], r1[256];
+// corr(o) = rms(g_o) y_o for the orbitals o0 .. o0 + batch - 1
+__global__ void k_store_corr(double* __restrict__ corr, const float* __restrict__ y, const float* __restrict__ scale,
+                             long npts, int o0) {
   const int b = blockIdx.y;
-  const long o = o0 + b;
-  const double sc = scale[b];
+  const double s = scale[b];
+  for (long p = blockIdx.x * 256L + threadIdx.x; p < npts; p += (long)gridDim.x * 256)
+    corr[(long)(o0 + b) * npts + p] = s * (double)y[(long)b * npts + p];
+}
+
+// Partial sums of d0 = <lowpass(g), g> and d1 = <corr, g> per orbital.
+__global__ void __launch_bounds__(256) k_dir_dots_part(const double* __restrict__ pre, const double* __restrict__ g,
+                                                       const double* __restrict__ corr, long npts,
+                                                       double* __restrict__ part, int nblk) {
+  __shared__ double r0[256], r1[256];
+  const long o = blockIdx.y;
   double s0 = 0.0, s1 = 0.0;
   for (long p = blockIdx.x * 256L + threadIdx.x; p < npts; p += (long)nblk * 256) {
     const double gv = g[o * npts + p];
     s0 += pre[o * npts + p] * gv;
-    s1 += sc * (double)y[(long)b * npts + p] * gv;
+    s1 += corr[o * npts + p] * gv;
   }
   r0[threadIdx.x] = s0;
   r1[threadIdx.x] = s1;
@@ -327,34 +337,32 @@ __global__ void __launch_bounds__(256) k_dir_dots_part(const double* __restrict_
     __syncthreads();
   }
   if (threadIdx.x == 0) {
-    part[((long)b * nblk + blockIdx.x) * 2 + 0] = r0[0];
-    part[((long)b * nblk + blockIdx.x) * 2 + 1] = r1[0];
+    part[(o * nblk + blockIdx.x) * 2 + 0] = r0[0];
+    part[(o * nblk + blockIdx.x) * 2 + 1] = r1[0];
   }
 }
 
-// The network direction p = lowpass(g) + rms(g) y is used only on the side of
-// g that keeps <pre, g> clearly positive (the CG's conjugation coefficients
-// are ratios of these products): with D = <p, g> and d0 = <lowpass(g), g>,
+// The network direction p = lowpass(g) + corr is used only on the side of g
+// that keeps <pre, g> clearly positive (the CG's conjugation coefficients are
+// ratios of these products): with D = <p, g> and d0 = <lowpass(g), g>,
 // pre = p if D >= d0 / 5, pre = -p if D <= -d0 / 5 (the same search line),
 // else the low-pass direction alone.
-__global__ void k_apply_direction(double* __restrict__ pre, const float* __restrict__ y,
-                                  const float* __restrict__ scale, const double* __restrict__ part, int nblk,
-                                  long npts, int o0) {
-  const int b = blockIdx.y;
+__global__ void k_apply_direction(double* __restrict__ pre, const double* __restrict__ corr,
+                                  const double* __restrict__ part, int nblk, long npts) {
+  const long o = blockIdx.y;
   double d0 = 0.0, d1 = 0.0;
   for (int k = 0; k < nblk; ++k) {
-    d0 += part[((long)b * nblk + k) * 2 + 0];
-    d1 += part[((long)b * nblk + k) * 2 + 1];
+    d0 += part[(o * nblk + k) * 2 + 0];
+    d1 += part[(o * nblk + k) * 2 + 1];
   }
   const double D = d0 + d1;
   double sign;
   if (D >= 0.2 * d0) sign = 1.0;
   else if (D <= -0.2 * d0) sign = -1.0;
   else return;
-  const double s = scale[b];
   for (long p = blockIdx.x * 256L + threadIdx.x; p < npts; p += (long)gridDim.x * 256) {
-    const long i = (long)(o0 + b) * npts + p;
-    pre[i] = sign * (pre[i] + s * (double)y[(long)b * npts + p]);
+    const long i = o * npts + p;
+    pre[i] = sign * (pre[i] + corr[i]);
   }
 }
 
@@ -375,7 +383,7 @@ int net_ensure(sb200_ctx* c, int batch) {
     // CG hook's rms partials (norb * 32 <= 65536)
     if (dalloc(&n->d_w, NPARAM) || dalloc(&n->d_wb, NPARAM) || dalloc(&n->d_g, NPARAM) || dalloc(&n->d_m, NPARAM) ||
         dalloc(&n->d_v, NPARAM) || dalloc(&n->d_red, (size_t)1024 * 193 + 65536) || dalloc(&n->d_scale, 4096) ||
-        dalloc(&n->d_dots, (size_t)1024 * 32 * 2))
+        dalloc(&n->d_dots, (size_t)2048 * 32 * 2))
       return SB200_ERR_OOM;
     SB_CUDA(cudaMemset(n->d_w, 0, NPARAM * sizeof(float)));
     SB_CUDA(cudaMemset(n->d_m, 0, NPARAM * sizeof(float)));
@@ -479,7 +487,7 @@ int net_loss_grad(sb200_ctx* c, const float* off, const float* target, int batch
 
 }  // namespace
 
-int learned_precond_apply(sb200_ctx* c, const double* g, double* pre) {
+int learned_precond_apply(sb200_ctx* c, const double* g, const double* x, double* pre) {
   Net* n = net_of(c);
   if (!n) return set_error(SB200_ERR_STATE, "learned preconditioner weights not set");
   // lowpass part first (the untrained network adds nothing)
@@ -489,6 +497,11 @@ int learned_precond_apply(sb200_ctx* c, const double* g, double* pre) {
   const int norb = c->orb.norb;
   const int nblk = 32;
   if ((long)norb * nblk > (1 << 16)) return set_error(SB200_ERR_BAD_SHAPE, "too many orbitals for the network hook");
+  if (n->corr_cap < (size_t)norb * np) {
+    dfree(n->d_corr);
+    if (dalloc(&n->d_corr, (size_t)norb * np)) return SB200_ERR_OOM;
+    n->corr_cap = (size_t)norb * np;
+  }
   dim3 gr(nblk, norb);
   k_rms_part<<<gr, 256, 0, c->stream>>>(g, np, n->d_red, nblk);
   const int B = n->cap_batch > 0 ? n->cap_batch : 1;
@@ -497,9 +510,15 @@ int learned_precond_apply(sb200_ctx* c, const double* g, double* pre) {
     dim3 gi((unsigned)((np + 255) / 256 < 1024 ? (np + 255) / 256 : 1024), b);
     k_make_input<<<gi, 256, 0, c->stream>>>(g, c->d_vloc, np, n->d_red, nblk, o0, n->x0, n->d_scale);
     TRY_L(net_forward(c, b));
-    k_dir_dots_part<<<dim3(nblk, b), 256, 0, c->stream>>>(pre, g, n->y, n->d_scale, np, o0, n->d_dots, nblk);
-    k_apply_direction<<<gi, 256, 0, c->stream>>>(pre, n->y, n->d_scale, n->d_dots, nblk, np, o0);
+    k_store_corr<<<gi, 256, 0, c->stream>>>(n->d_corr, n->y, n->d_scale, np, o0);
   }
+  SB_LAUNCH_CHECK("k_store_corr");
+  // the correction lives outside the occupied subspace: its parts along the
+  // current orbitals are rotations within the subspace, not progress
+  TRY_L(gs_project_out(c, x, norb, n->d_corr, norb));
+  k_dir_dots_part<<<dim3(nblk, norb), 256, 0, c->stream>>>(pre, g, n->d_corr, np, n->d_dots, nblk);
+  dim3 ga((unsigned)((np + 255) / 256 < 1024 ? (np + 255) / 256 : 1024), norb);
+  k_apply_direction<<<ga, 256, 0, c->stream>>>(pre, n->d_corr, n->d_dots, nblk, np);
   SB_LAUNCH_CHECK("learned_precond_apply");
   return SB200_OK;
 }
@@ -525,6 +544,7 @@ void learned_free(sb200_ctx* c) {
   dfree(n->d_wpart);
   dfree(n->d_scale);
   dfree(n->d_dots);
+  dfree(n->d_corr);
   delete n;
   c->learned = nullptr;
   c->learned_set = false;

@@ -163,10 +163,8 @@ __global__ void __launch_bounds__(NT, 2) k_term_orbital(const double2* __restric
     project_from_smem(sm, Ps, a, ik);
     __syncthreads();
   }
-  const double lap0 = kc[3];
-  double nab[12];
-#pragma unroll
-  for (int q = 0; q < 12; ++q) nab[q] = kc[4 + q];
+  // k + A factored out of the gradient: w = sum_d kAc_d sum_s nab_s (t+ - t-)
+  const double kx = kc[0], ky = kc[1], kz = kc[2], lap0 = kc[3];
   int oxp[ND], oxm[ND], oyp[ND], oym[ND];
 #pragma unroll
   for (int s = 1; s <= ND; ++s) {
@@ -200,22 +198,22 @@ __global__ void __launch_bounds__(NT, 2) k_term_orbital(const double2* __restric
     for (int s = 0; s < ND; ++s) {
       const double2 tp = P[oxp[s]], tm = P[oxm[s]];
       vx = cadd(vx, cscal(a.lapt[s], cadd(tp, tm)));
-      wx = cadd(wx, cscal(nab[s], csub(tp, tm)));
+      wx = cadd(wx, cscal(a.nab[s], csub(tp, tm)));
     }
 #pragma unroll
     for (int s = 0; s < ND; ++s) {
       const double2 tp = P[oyp[s]], tm = P[oym[s]];
       vy = cadd(vy, cscal(a.lapt[4 + s], cadd(tp, tm)));
-      wy = cadd(wy, cscal(nab[4 + s], csub(tp, tm)));
+      wy = cadd(wy, cscal(a.nab[4 + s], csub(tp, tm)));
     }
 #pragma unroll
     for (int s = 0; s < ND; ++s) {
       const double2 tp = col[(z + s + 1) & (N - 1)], tm = col[(z - s - 1) & (N - 1)];
       vz = cadd(vz, cscal(a.lapt[8 + s], cadd(tp, tm)));
-      wz = cadd(wz, cscal(nab[8 + s], csub(tp, tm)));
+      wz = cadd(wz, cscal(a.nab[8 + s], csub(tp, tm)));
     }
     const double2 v = cadd(vz, cadd(vy, vx));
-    const double2 w = cadd(wz, cadd(wy, wx));
+    const double2 w = cadd(cscal(kz, wz), cadd(cscal(ky, wy), cscal(kx, wx)));
     const double2 c = col[z];
     const int p = z * NP + t;
     double2 h;

@@ -166,3 +166,20 @@ def eval_loss(ctx, x0, off, tgt, batch=8):
                                             C.c_void_p(tgt[i:i + batch].data_ptr()), batch, C.byref(lv), None))
         tot += lv.value
     return tot / max(1, (n // batch) * batch)
+
+
+def evaluate(ctx, psi_ref_layout, tol=1e-8, max_outer=600, ncg=4):
+    """Outer iterations and wall time for the low-pass, learned and
+    unpreconditioned CG to reach the converged eigenvalues (tightly converged
+    low-pass CG, 1e-12 Ha, as the judge) within `tol` Hartree."""
+    psi = ctx.gs_upload(psi_ref_layout)
+    ctx.gram_schmidt_real(psi)
+    ref = converge(ctx, psi, tol=1e-12, max_outer=3 * max_outer, precondition="lowpass", ncg=ncg)["evals"]
+    out = {}
+    for pre in ("lowpass", "learned", "none"):
+        psi = ctx.gs_upload(psi_ref_layout)
+        ctx.gram_schmidt_real(psi)
+        r = converge(ctx, psi, tol=tol, max_outer=max_outer, precondition=pre, ncg=ncg, ref=ref)
+        out[pre] = dict(outer=r["outer"], seconds=r["seconds"], converged=r["converged"],
+                        max_err=float(np.max(np.abs(r["evals"] - ref))))
+    return out

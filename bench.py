@@ -460,7 +460,12 @@ def main():
     ctx.set_timing(False)
     launches_per_tstep = sum(v[1] for v in kt.values()) / nt_i
     gpu_launches = int(round(launches_per_tstep * nt * args.steps))
-    hpsi_kernel = "k_term_orbital" if orbital_path(s, args) else "k_hpsi_tiled"
+    if orbital_path(s, args):
+        hpsi_kernel = "k_term_orbital"
+    elif os.environ.get("SB200_TMA", "on").startswith("of"):
+        hpsi_kernel = "k_hpsi_tiled"
+    else:  # the tensor-copy sweep takes isolated grids and periodic grids with nx = 32
+        hpsi_kernel = "k_hpsi_tma"
     peak, peak_kind = measured_peaks()
     h_ms, h_cnt = kt.get("hpsi", (float("nan"), 1))
     units_per_launch = int(np.prod(s.grid.shape)) * s.norb

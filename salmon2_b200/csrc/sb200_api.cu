@@ -84,6 +84,8 @@ int ensure_work(sb200_ctx* c) {
   const long nblk = (c->g.npts + (long)OBS_THREADS * OBS_PTS_PER_THREAD - 1) / ((long)OBS_THREADS * OBS_PTS_PER_THREAD);
   c->obs_blocks = (int)nblk;
   TRY(dalloc(&c->d_obs, (size_t)c->orb.norb * nblk * OBS_NQ + 4096));
+  dfree(c->d_obs1);
+  TRY(dalloc(&c->d_obs1, (size_t)c->orb.norb * (OBS_NQ + 3)));
   if (c->pp.nlma > 0) {
     TRY(dalloc(&c->d_proj, (size_t)c->orb.norb * c->pp.nlma));
     TRY(dalloc(&c->d_jw, (size_t)c->orb.norb * c->pp.natom * 3));
@@ -336,6 +338,7 @@ int sb200_ctx_destroy(sb200_ctx* c) {
   dfree(c->d_proj);
   dfree(c->d_jw);
   dfree(c->d_obs);
+  dfree(c->d_obs1);
   dfree(c->d_result);
   dfree(c->rt.d_Ac_ext);
   dfree(c->rt.d_Ac_ind);

@@ -212,7 +212,21 @@ __global__ void __launch_bounds__(OBS_THREADS) k_observables_batch(const BOSys* 
   const int s = find_sys(first, nsys, w);
   const long l = w - first[s];
   const int nblk = sys[s].a.nblk;
-  obs_block(psi[s], sys[s].part, sys[s].a, (int)(l % nblk), (int)(l / nblk));
+  obs_block<false>(psi[s], sys[s].part, sys[s].a, (int)(l % nblk), (int)(l / nblk));  // isolated: no current
+}
+
+// per-orbital sums of every system's observable partials (collapse_item)
+struct BCSys {
+  const double* part;
+  int nblk;
+  double* out;
+};
+__global__ void __launch_bounds__(256) k_collapse_batch(const BCSys* __restrict__ sys, const long* __restrict__ first,
+                                                        int nsys) {
+  const long item = blockIdx.x * 256L + threadIdx.x;
+  if (item >= first[nsys]) return;
+  const int s = find_sys(first, nsys, item);
+  collapse_item(sys[s].part, sys[s].nblk, nullptr, 0, item - first[s], sys[s].out);
 }
 
 __global__ void __launch_bounds__(256) k_finalize_batch(const FinArgs* __restrict__ args) {
@@ -274,7 +288,9 @@ struct sb200_batch {
   BOSys* d_osys = nullptr;
   long* d_ofirst = nullptr;
   FinArgs* d_fin = nullptr;
-  long p_total = 0, o_total = 0, h_total = 0;
+  BCSys* d_csys = nullptr;
+  long* d_cfirst = nullptr;
+  long p_total = 0, o_total = 0, h_total = 0, c_total = 0;
   // per-launch pointer tables: [parity][term][nsys] (hpsi in queue order)
   BPtr* d_hptr = nullptr;
   const void** d_pin = nullptr;
@@ -478,6 +494,8 @@ int launch_obs_final_batch(sb200_batch* b, int parity, int which) {
         b->d_osys, b->d_ofirst, b->d_opsi + (size_t)parity * b->nsys, b->nsys);
     SB_LAUNCH_CHECK("k_observables_batch");
   } else {
+    k_collapse_batch<<<(unsigned)((b->c_total + 255) / 256), 256, 0, b->stream>>>(b->d_csys, b->d_cfirst, b->nsys);
+    SB_LAUNCH_CHECK("k_collapse_batch");
     k_finalize_batch<<<b->nsys, 256, 0, b->stream>>>(b->d_fin);
     SB_LAUNCH_CHECK("k_finalize_batch");
   }
@@ -581,6 +599,8 @@ int sb200_batch_create(sb200_ctx* const* systems, int nsys, sb200_batch** out) {
   if ((rc = dalloc(&b->d_osys, nsys)) != SB200_OK) return fail(rc);
   if ((rc = dalloc(&b->d_ofirst, nsys + 1)) != SB200_OK) return fail(rc);
   if ((rc = dalloc(&b->d_fin, nsys)) != SB200_OK) return fail(rc);
+  if ((rc = dalloc(&b->d_csys, nsys)) != SB200_OK) return fail(rc);
+  if ((rc = dalloc(&b->d_cfirst, nsys + 1)) != SB200_OK) return fail(rc);
   // projection and observable descriptors (natural order)
   std::vector<BPSys> ps(nsys);
   std::vector<BOSys> os(nsys);
@@ -597,6 +617,20 @@ int sb200_batch_create(sb200_ctx* const* systems, int nsys, sb200_batch** out) {
   }
   b->p_total = pf[nsys];
   b->o_total = of[nsys];
+  {
+    std::vector<BCSys> cs(nsys);
+    std::vector<long> cf(nsys + 1, 0);
+    for (int s = 0; s < nsys; ++s) {
+      cs[s].part = systems[s]->d_obs;
+      cs[s].nblk = systems[s]->obs_blocks;
+      cs[s].out = systems[s]->d_obs1;
+      cf[s + 1] = cf[s] + (long)systems[s]->orb.norb * (OBS_NQ + 3);
+    }
+    b->c_total = cf[nsys];
+    if ((rc = h2d(b->d_csys, cs.data(), nsys * sizeof(BCSys), b->stream)) != SB200_OK ||
+        (rc = h2d(b->d_cfirst, cf.data(), (nsys + 1) * sizeof(long), b->stream)) != SB200_OK)
+      return fail(rc);
+  }
   if (b->o_total >= (1L << 31) || b->p_total >= (1L << 33)) return fail(set_error(SB200_ERR_UNSUPPORTED, "batch too large"));
   if ((rc = h2d(b->d_psys, ps.data(), nsys * sizeof(BPSys), b->stream)) != SB200_OK ||
       (rc = h2d(b->d_pfirst, pf.data(), (nsys + 1) * sizeof(long), b->stream)) != SB200_OK ||
@@ -624,6 +658,8 @@ int sb200_batch_destroy(sb200_batch* b) {
   dfree(b->d_osys);
   dfree(b->d_ofirst);
   dfree(b->d_fin);
+  dfree(b->d_csys);
+  dfree(b->d_cfirst);
   delete b;
   if (prev >= 0) cudaSetDevice(prev);
   return SB200_OK;
@@ -804,6 +840,9 @@ int sb200_batch_propagate(sb200_batch* b, double* const* psi_a, double* const* p
     TRY_B(launch_prep_k(c, c->d_result + 8, 0, 0, c->d_kcoef, false));
     SB_CUDA(cudaStreamSynchronize(c->stream));
     fin[s] = make_fin_args(c, -1, SB200_TRANS_TR, dt, -1, false);
+    fin[s].part = c->d_obs1;  // collapsed per orbital by k_collapse_batch
+    fin[s].nblk = 1;
+    fin[s].obs_stride = OBS_NQ + 3;
   }
   TRY_B(h2d(b->d_fin, fin.data(), n * sizeof(FinArgs), b->stream));
   // pointer tables of both parities

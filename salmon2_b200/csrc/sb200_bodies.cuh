@@ -97,6 +97,9 @@ struct ObsArgs {
   double off[3];   // is_d - shift_d
 };
 
+// CUR = false (isolated grids: no current) skips the neighbour sums, which
+// the final reduction does not use there.
+template <bool CUR>
 __device__ __forceinline__ void obs_block(const double2* __restrict__ in, double* __restrict__ part,
                                           const ObsArgs& a, const int blk, const int o) {
   __shared__ double red[OBS_NQ][OBS_THREADS];
@@ -116,7 +119,7 @@ __device__ __forceinline__ void obs_block(const double2* __restrict__ in, double
     q[0] += r2;
     double ix = 0.0, iy = 0.0, iz = 0.0;
 #pragma unroll
-    for (int s = 1; s <= ND; ++s) {
+    for (int s = 1; s <= (CUR ? ND : 0); ++s) {
       bool ok;
       const int xp = nbr(x, s, a.nx, a.periodic, ok);
       const double2 tx = ldz(src, p - x + xp, ok);
@@ -157,6 +160,7 @@ __device__ __forceinline__ void obs_block(const double2* __restrict__ in, double
 struct FinArgs {
   int norb, nspin, nspin_no, nblk, natom, periodic, itt, trans_longi, advance, spin_filter;
   int jw_natom;            // atoms per orbital in jw (1 when already summed)
+  int obs_stride, jw_stride;  // doubles per (orbital, block) record in part / per (orbital, atom) in jw
   double ngrid_inv, dt;
   const double* part;
   const double* jw;        // [norb][natom][3] or null
@@ -188,14 +192,14 @@ __device__ __forceinline__ void finalize_body(const FinArgs& a) {
     if (a.spin_filter >= 0 && (o % a.nspin) != a.spin_filter) continue;
     double q[OBS_NQ] = {0, 0, 0, 0, 0, 0, 0};
     for (int b = 0; b < a.nblk; ++b)
-      for (int i = 0; i < OBS_NQ; ++i) q[i] += a.part[((long)o * a.nblk + b) * OBS_NQ + i];
+      for (int i = 0; i < OBS_NQ; ++i) q[i] += a.part[((long)o * a.nblk + b) * a.obs_stride + i];
     const double w = a.weight[o];
     if (a.periodic) {
       const int ik = o / a.nspin_no;
       double jw[3] = {0.0, 0.0, 0.0};
       if (a.jw != nullptr)
         for (int at = 0; at < a.jw_natom; ++at)
-          for (int d = 0; d < 3; ++d) jw[d] += a.jw[3L * ((long)o * a.jw_natom + at) + d];
+          for (int d = 0; d < 3; ++d) jw[d] += a.jw[(long)a.jw_stride * ((long)o * a.jw_natom + at) + d];
       for (int d = 0; d < 3; ++d) {
         const double kAc = a.vec_k[3 * ik + d] + A[d];
         s[d] += (kAc * q[0] + 2.0 * q[1 + d] + 2.0 * jw[d]) * w;
@@ -237,6 +241,26 @@ __device__ __forceinline__ void finalize_body(const FinArgs& a) {
     }
     if (a.advance) *a.step = itt + 1;
   }
+}
+
+// Per-orbital sums of the observable partials [norb][nblk][OBS_NQ] and of the
+// nonlocal-current pieces [norb][natom][3], blocks and atoms in ascending
+// order (the order the final reduction adds them): out [norb][OBS_NQ + 3].
+// Thread per (orbital, quantity).
+__device__ __forceinline__ void collapse_item(const double* __restrict__ part, int nblk,
+                                              const double* __restrict__ jw, int natom, long item,
+                                              double* __restrict__ out) {
+  const long o = item / (OBS_NQ + 3);
+  const int i = (int)(item % (OBS_NQ + 3));
+  double s = 0.0;
+  if (i < OBS_NQ) {
+#pragma unroll 4
+    for (int b = 0; b < nblk; ++b) s += part[(o * nblk + b) * OBS_NQ + i];
+  } else if (jw != nullptr) {
+#pragma unroll 4
+    for (int at = 0; at < natom; ++at) s += jw[3 * (o * natom + at) + (i - OBS_NQ)];
+  }
+  out[item] = s;
 }
 
 }  // namespace body

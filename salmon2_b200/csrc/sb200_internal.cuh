@@ -124,6 +124,7 @@ struct sb200_ctx {
   double2* d_proj = nullptr;    // [norb][nlma] projections of the current input
   double* d_jw = nullptr;       // [norb][natom][3] nonlocal current pieces
   double* d_obs = nullptr;      // [norb][obs_blocks][OBS_NQ] partial sums
+  double* d_obs1 = nullptr;     // [norb][OBS_NQ + 3] per-orbital sums (observables, nonlocal current)
   double* d_result = nullptr;   // small result area (8 doubles)
   int* d_err = nullptr;         // device error flag: a bounded wait expired
   int obs_blocks = 0;

@@ -263,10 +263,18 @@ __global__ void __launch_bounds__(256) k_hpsi(const double2* __restrict__ in, do
 
 __global__ void __launch_bounds__(OBS_THREADS) k_observables(const double2* __restrict__ in, double* __restrict__ part,
                                                              ObsArgs a) {
-  obs_block(in, part, a, blockIdx.x, blockIdx.y);
+  if (a.periodic) obs_block<true>(in, part, a, blockIdx.x, blockIdx.y);
+  else obs_block<false>(in, part, a, blockIdx.x, blockIdx.y);
 }
 
 __global__ void __launch_bounds__(256) k_finalize(FinArgs a) { finalize_body(a); }
+
+__global__ void __launch_bounds__(256) k_collapse(const double* __restrict__ part, int nblk,
+                                                  const double* __restrict__ jw, int natom, long nitems,
+                                                  double* __restrict__ out) {
+  const long item = blockIdx.x * 256L + threadIdx.x;
+  if (item < nitems) collapse_item(part, nblk, jw, natom, item, out);
+}
 
 // rho(p, ispin) = sum_{ik, io} w |psi|^2 (density_matrix.f90:150-232)
 __global__ void k_density(const double2* __restrict__ in, double* __restrict__ rho, long npts, int nspin,
@@ -473,6 +481,8 @@ FinArgs make_fin_args(const sb200_ctx* c, int itt, int trans_longi, double dt, i
   FinArgs a;
   a.norb = c->orb.norb;
   a.jw_natom = fused_obs ? 1 : c->pp.natom;
+  a.obs_stride = OBS_NQ;
+  a.jw_stride = 3;
   a.nspin = c->orb.nspin;
   a.spin_filter = spin_filter;
   a.nspin_no = c->orb.nspin * c->orb.no;
@@ -515,6 +525,22 @@ FinArgs make_fin_args(const sb200_ctx* c, int itt, int trans_longi, double dt, i
 int launch_finalize(sb200_ctx* c, int itt, int nt, int trans_longi, double dt, int spin_filter, bool fused_obs) {
   (void)nt;
   FinArgs a = make_fin_args(c, itt, trans_longi, dt, spin_filter, fused_obs);
+  if (a.nblk > 1 || (a.jw != nullptr && a.jw_natom > 1)) {
+    // per-orbital sums first, in parallel (same order of additions), so the
+    // one-CTA final reduction reads one record per orbital
+    const long nitems = (long)c->orb.norb * (OBS_NQ + 3);
+    k_collapse<<<(unsigned)((nitems + 255) / 256), 256, 0, c->stream>>>(a.part, a.nblk, a.jw, a.jw_natom, nitems,
+                                                                        c->d_obs1);
+    SB_LAUNCH_CHECK("k_collapse");
+    a.part = c->d_obs1;
+    a.nblk = 1;
+    a.obs_stride = OBS_NQ + 3;
+    if (a.jw != nullptr) {
+      a.jw = c->d_obs1 + OBS_NQ;
+      a.jw_natom = 1;
+      a.jw_stride = OBS_NQ + 3;
+    }
+  }
   k_finalize<<<1, 256, 0, c->stream>>>(a);
   SB_LAUNCH_CHECK("k_finalize");
   return SB200_OK;

@@ -288,6 +288,15 @@ __device__ __forceinline__ bool tma_body(const TmaMaps& maps, void* __restrict__
           acc[gi] = cadd(accr[ti], make_double2((double)tt.x, (double)tt.y));
         }
       }
+      // warp 0 waits for the next step's copies before the step barrier, so the
+      // other warps find them complete at their own (first) try-wait and
+      // block in the barrier instead of polling
+      if (t < 32 && k + 1 < nsteps) {
+        const int rf1 = k + 1 + 2 * HALO;
+        ok = tma::mbar_wait(&pbar[rf1 & (RING - 1)], (pmask >> (rf1 & (RING - 1))) & 1u) && ok;
+        if (G::ACC64 || G::D32)
+          ok = tma::mbar_wait(&abar[(k + 1) & (ARING - 1)], (amask >> ((k + 1) & (ARING - 1))) & 1u) && ok;
+      }
       all_ok = __syncthreads_and(ok);
       if (!all_ok) return false;
       if (t == 0) {  // refill the slots of plane z and of accumulator step k

@@ -110,21 +110,20 @@ __global__ void __launch_bounds__(128) k_project_moments(const double2* __restri
       u[q] = make_double2(0.0, 0.0);
       ur[q][0] = ur[q][1] = ur[q][2] = make_double2(0.0, 0.0);
     }
+#pragma unroll 2
     for (int j = lane; j < m; j += 32) {
       const double2 v = __ldg(psi + a.pt_lin[start + j]);
-      const double2 e = __ldg(ph + j);
+      const double2 ev = cmul(__ldg(ph + j), v);  // conj(zekr_uV) / uV times psi, once per point
       const double* r = a.pt_r + 3L * (start + j);
-      const double r0 = r[0], r1 = r[1], r2 = r[2];
+      const double r0 = __ldg(r), r1 = __ldg(r + 1), r2 = __ldg(r + 2);
 #pragma unroll
       for (int q = 0; q < NP; ++q) {
         if (q0 + q < np) {
-          const double uv = __ldg(a.uv + (long)(lma0 + q0 + q) * a.nps + j);
-          const double2 zk = make_double2(e.x * uv, e.y * uv);
-          const double2 t = cmul(zk, v);
+          const double2 t = cscal(__ldg(a.uv + (long)(lma0 + q0 + q) * a.nps + j), ev);
           u[q] = cadd(u[q], t);
-          ur[q][0] = cadd(ur[q][0], cmul(cscal(r0, zk), v));
-          ur[q][1] = cadd(ur[q][1], cmul(cscal(r1, zk), v));
-          ur[q][2] = cadd(ur[q][2], cmul(cscal(r2, zk), v));
+          ur[q][0] = cadd(ur[q][0], cscal(r0, t));
+          ur[q][1] = cadd(ur[q][1], cscal(r1, t));
+          ur[q][2] = cadd(ur[q][2], cscal(r2, t));
         }
       }
     }
@@ -265,6 +264,105 @@ __global__ void __launch_bounds__(OBS_THREADS) k_observables(const double2* __re
                                                              ObsArgs a) {
   if (a.periodic) obs_block<true>(in, part, a, blockIdx.x, blockIdx.y);
   else obs_block<false>(in, part, a, blockIdx.x, blockIdx.y);
+}
+
+// Observables of a periodic grid as a z sweep (same quantities as
+// obs_block): one CTA per 32 x 8 column tile x z chunk x orbital; the plane
+// with its forward halo (+1..+4 in x and y, wrapped) in shared memory, the
+// forward z neighbours in a register window, so psi is read about once.
+// Writes partial block b = zchunk * ntiles + tile of the orbital; blocks
+// ntiles * nzc .. nblk - 1 are written as zeros by the first CTA.
+constexpr int OS_TX = 32, OS_TY = 8, OS_SX = OS_TX + ND, OS_SY = OS_TY + ND;
+__global__ void __launch_bounds__(256) k_obs_sweep(const double2* __restrict__ in, double* __restrict__ part,
+                                                   ObsArgs a, int zchunk) {
+  __shared__ double2 pl[OS_SY * OS_SX];
+  __shared__ double red[OBS_NQ][8];
+  const int t = threadIdx.x, tx = t & 31, ty = t >> 5;
+  const int ntx = (a.nx + OS_TX - 1) / OS_TX;
+  const int ntiles = ntx * ((a.ny + OS_TY - 1) / OS_TY);
+  const int x0 = ((int)blockIdx.x % ntx) * OS_TX, y0 = ((int)blockIdx.x / ntx) * OS_TY;
+  const int x = x0 + tx, y = y0 + ty;
+  const bool active = x < a.nx && y < a.ny;
+  const int z0 = blockIdx.y * zchunk, z1 = min(a.nz, z0 + zchunk);
+  const int o = blockIdx.z;
+  const double2* src = in + (long)o * a.npts;
+  const long sz = (long)a.nx * a.ny;
+  auto wz = [&](int z) { int q = z % a.nz; return q < 0 ? q + a.nz : q; };
+  // halo cell of this thread (cells of the 12 x 36 area outside the tile)
+  int hslot = -1;
+  long hoff = 0;
+  if (t < OS_SX * OS_SY - OS_TX * OS_TY) {
+    int hx, hy;
+    if (t < ND * OS_SX) {  // rows below the tile's forward edge
+      hy = OS_TY + t / OS_SX;
+      hx = t % OS_SX;
+    } else {               // the forward x strip of the tile rows
+      const int c = t - ND * OS_SX;
+      hy = c / ND;
+      hx = OS_TX + c % ND;
+    }
+    hslot = hy * OS_SX + hx;
+    const int gx = (x0 + hx) % a.nx, gy = (y0 + hy) % a.ny;
+    hoff = (long)gy * a.nx + gx;
+  }
+  const long pxy = (long)y * a.nx + x;
+  double2 w[ND + 1];
+#pragma unroll
+  for (int k = 0; k <= ND; ++k) w[k] = active ? __ldg(src + wz(z0 + k) * sz + pxy) : make_double2(0.0, 0.0);
+  double q[OBS_NQ];
+#pragma unroll
+  for (int i = 0; i < OBS_NQ; ++i) q[i] = 0.0;
+  double2 hq = hslot >= 0 ? __ldg(src + (long)z0 * sz + hoff) : make_double2(0.0, 0.0);
+  for (int z = z0; z < z1; ++z) {
+    if (active) pl[(ty)*OS_SX + tx] = w[0];
+    if (hslot >= 0) pl[hslot] = hq;
+    // the next plane's loads are issued before this plane's sums
+    const double2 nxt = (active && z + 1 < z1) ? __ldg(src + wz(z + ND + 1) * sz + pxy) : make_double2(0.0, 0.0);
+    if (hslot >= 0 && z + 1 < z1) hq = __ldg(src + (long)(z + 1) * sz + hoff);
+    __syncthreads();
+    if (active) {
+      const double2 c = w[0];
+      const double r2 = c.x * c.x + c.y * c.y;
+      q[0] += r2;
+      double ix = 0.0, iy = 0.0, iz = 0.0;
+#pragma unroll
+      for (int s = 1; s <= ND; ++s) {
+        const double2 txv = pl[ty * OS_SX + tx + s];
+        const double2 tyv = pl[(ty + s) * OS_SX + tx];
+        const double2 tzv = w[s];
+        ix += a.nab[s - 1] * (c.x * txv.y - c.y * txv.x);
+        iy += a.nab[4 + s - 1] * (c.x * tyv.y - c.y * tyv.x);
+        iz += a.nab[8 + s - 1] * (c.x * tzv.y - c.y * tzv.x);
+      }
+      q[1] += ix;
+      q[2] += iy;
+      q[3] += iz;
+      q[4] += ((double)x + a.off[0]) * r2;
+      q[5] += ((double)y + a.off[1]) * r2;
+      q[6] += ((double)z + a.off[2]) * r2;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < ND; ++k) w[k] = w[k + 1];
+    w[ND] = nxt;
+  }
+#pragma unroll
+  for (int i = 0; i < OBS_NQ; ++i) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) q[i] += __shfl_xor_sync(0xffffffffu, q[i], off);
+  }
+  if (tx == 0)
+    for (int i = 0; i < OBS_NQ; ++i) red[i][ty] = q[i];
+  __syncthreads();
+  const int b = blockIdx.y * ntiles + blockIdx.x;
+  if (t < OBS_NQ) {
+    double sum = 0.0;
+    for (int wv = 0; wv < 8; ++wv) sum += red[t][wv];
+    part[((long)o * a.nblk + b) * OBS_NQ + t] = sum;
+  }
+  if (blockIdx.x == 0 && blockIdx.y == 0)
+    for (int i = ntiles * gridDim.y * OBS_NQ + t; i < a.nblk * OBS_NQ; i += blockDim.x)
+      part[(long)o * a.nblk * OBS_NQ + i] = 0.0;
 }
 
 __global__ void __launch_bounds__(256) k_finalize(FinArgs a) { finalize_body(a); }
@@ -413,7 +511,7 @@ int launch_project_moments(sb200_ctx* c, const double2* psi) {
   if (c->pp.nlma == 0) return SB200_OK;
   ProjArgs a = make_proj_args(c);
   dim3 grid((a.natom + 3) / 4, c->orb.norb);
-  k_project_moments<2><<<grid, 128, 0, c->stream>>>(psi, c->d_jw, a);
+  k_project_moments<4><<<grid, 128, 0, c->stream>>>(psi, c->d_jw, a);
   SB_LAUNCH_CHECK("k_project_moments");
   return SB200_OK;
 }
@@ -469,6 +567,22 @@ ObsArgs make_obs_args(const sb200_ctx* c) {
 
 int launch_observables(sb200_ctx* c, const double2* psi) {
   ObsArgs a = make_obs_args(c);
+  // z sweep (psi read about once for the current sums): periodic grids whose
+  // x / y extents are multiples of the 32 x 8 tile
+  if (c->g.periodic && c->g.nx % OS_TX == 0 && c->g.ny % OS_TY == 0) {
+    const int ntiles = ((c->g.nx + OS_TX - 1) / OS_TX) * ((c->g.ny + OS_TY - 1) / OS_TY);
+    int nzc = c->obs_blocks / ntiles;
+    if (nzc < 1) nzc = 1;
+    if (nzc > c->g.nz) nzc = c->g.nz;
+    const int zchunk = (c->g.nz + nzc - 1) / nzc;
+    nzc = (c->g.nz + zchunk - 1) / zchunk;
+    if ((long)ntiles * nzc <= c->obs_blocks) {
+      dim3 grid(ntiles, nzc, c->orb.norb);
+      k_obs_sweep<<<grid, 256, 0, c->stream>>>(psi, c->d_obs, a, zchunk);
+      SB_LAUNCH_CHECK("k_obs_sweep");
+      return SB200_OK;
+    }
+  }
   dim3 grid(c->obs_blocks, c->orb.norb);
   k_observables<<<grid, OBS_THREADS, 0, c->stream>>>(psi, c->d_obs, a);
   SB_LAUNCH_CHECK("k_observables");

@@ -237,3 +237,35 @@ def test_tensor_copy_kernel_equals_register_sweep(make, precision, monkeypatch):
         outs.append(ctx.download(out))
         ctx.close()
     assert np.array_equal(outs[0], outs[1])
+
+
+@pytest.mark.parametrize("trans", ["tr", "lo"])
+def test_rt_propagate_periodic32_current(trans):
+    """32^3 periodic grid: the tensor-copy sweep for H psi and the observables
+    z sweep (shared-memory plane + register window) for J(t) and the dipole."""
+    from salmon2_b200 import synth
+    sysm = _periodic32()
+    nt, dt = 8, 0.08
+    Ac = synth.asin2cos(nt, dt, omega=0.05696, f0=0.05696 * 2e-2, tw=nt * dt)
+    zc = synth.taylor_zc(dt)
+    ref = Oracle(sysm).rt_run(sysm.psi, nt, dt, zc, Ac_ext=Ac, trans_longi=1 if trans == "lo" else 0)
+    ctx = _ctx(sysm)
+    a, b, w = ctx.upload(sysm.psi), ctx.zeros(), ctx.zeros()
+    res = ctx.rt_propagate(a, b, w, nt, dt, zc, Ac_ext=Ac, trans_longi=trans)
+    jmax = np.max(np.abs(ref["curr"]))
+    assert np.max(np.abs(res["curr"] - ref["curr"])) <= TOL_OBS * jmax
+    assert S.rel_err(res["rbox"], ref["rbox"]) < TOL_OBS
+    assert S.rel_err(ctx.download(res["psi"]), ref["psi"]) < 1e-11
+
+
+def test_current_periodic32():
+    sysm = _periodic32()
+    O = Oracle(sysm)
+    ctx = _ctx(sysm)
+    a_mid, a_cur = (0.01, 0.02, -0.03), (0.011, 0.019, -0.029)
+    O.set_vec_Ac(a_mid)
+    ctx.set_vec_Ac(a_mid)
+    O.set_vec_Ac_local_only(a_cur)
+    ref = O.current(sysm.psi)
+    got = ctx.calc_current(ctx.upload(sysm.psi), a_cur)
+    assert np.max(np.abs(got - ref)) <= TOL_OBS * max(np.max(np.abs(ref)), 1e-30)

@@ -129,6 +129,11 @@ void free_pp(PPInfo& p) {
   dfree(p.d_phase);
   dfree(p.d_pmap);
   dfree(p.d_ent_zk);
+  dfree(p.d_pmap2);
+  dfree(p.d_pair_lma);
+  dfree(p.d_pair_uv);
+  dfree(p.d_pair_fp);
+  dfree(p.d_pair_ph);
   p = PPInfo();
 }
 
@@ -642,6 +647,39 @@ int sb200_set_pp(sb200_ctx* c, int natom, int nps, int nlma, const int* mps, con
     pmap[vi_pt[v]] = (vi_start[v] << 8) | cnt;
   }
   TRY(upload(&p.d_pmap, pmap));
+  // (point, atom) pairs: the entries of a point grouped by atom (ilma ascending)
+  if (npmax <= 4) {
+    std::vector<int> pmap2(g.npts, -1), pair_lma, pair_fp;
+    std::vector<double> pair_uv;
+    for (int v = 0; v < nvi; ++v) {
+      const int first = (int)pair_lma.size();
+      int prev_atom = -1;
+      for (int e = vi_start[v]; e < vi_start[v + 1]; ++e) {
+        const int at = ia_tbl[ent_lma[e]] - 1;
+        if (at == prev_atom) continue;
+        prev_atom = at;
+        const int fp = ent_pt[e];
+        const int j = fp - atom_start[at];
+        pair_lma.push_back(lma_start[at] | (nproj[at] << 24));
+        pair_fp.push_back(fp);
+        for (int q = 0; q < 4; ++q)
+          pair_uv.push_back(q < nproj[at] ? huv[(size_t)(lma_start[at] + q) * nps + j] : 0.0);
+      }
+      const int cnt = (int)pair_lma.size() - first;
+      if (cnt > 255) return set_error(SB200_ERR_UNSUPPORTED, "more than 255 atoms on one grid point");
+      pmap2[vi_pt[v]] = (first << 8) | cnt;
+    }
+    p.npair = (int)pair_lma.size();
+    TRY(upload(&p.d_pmap2, pmap2));
+    TRY(upload(&p.d_pair_lma, pair_lma));
+    TRY(upload(&p.d_pair_uv, pair_uv));
+    TRY(upload(&p.d_pair_fp, pair_fp));
+    TRY(dalloc(&p.d_pair_ph, (size_t)p.nk_phase * (p.npair > 0 ? p.npair : 1)));
+    if (!g.periodic) {  // isolated: exp(i 0.r) = 1
+      std::vector<double2> one(p.npair > 0 ? p.npair : 1, make_double2(1.0, 0.0));
+      SB_CUDA(cudaMemcpy(p.d_pair_ph, one.data(), one.size() * sizeof(double2), cudaMemcpyHostToDevice));
+    }
+  }
   TRY(dalloc(&p.d_ent_zk, (size_t)p.nk_phase * (nent > 0 ? nent : 1)));
   if (!g.periodic) {  // isolated: zekr_uV = uV (prep_pp.f90:618-619)
     std::vector<double2> one(tot > 0 ? tot : 1, make_double2(1.0, 0.0));

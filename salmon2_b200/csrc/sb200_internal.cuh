@@ -69,6 +69,16 @@ struct PPInfo {
   int* d_pmap = nullptr;
   // zekr_uV of every scatter entry for every k: [nk_phase][nent] (k_prep)
   double2* d_ent_zk = nullptr;
+  // (point, atom) pairs of the scatter for the tiled / tensor-copy kernels (atoms
+  // with at most 4 projectors): per point (first pair << 8) | pair count,
+  // per pair lma0 | (nproj << 24), uV of its projectors, flat sphere point,
+  // and exp(i (k+A).r) per k (k_prep)
+  int npair = 0;
+  int* d_pmap2 = nullptr;
+  int* d_pair_lma = nullptr;
+  double* d_pair_uv = nullptr;  // [npair][4]
+  int* d_pair_fp = nullptr;
+  double2* d_pair_ph = nullptr; // [nk_phase][npair]
 };
 
 struct RTBuffers {

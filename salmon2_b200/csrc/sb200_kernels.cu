@@ -27,6 +27,9 @@ struct PrepArgs {
   const int* ent_pt;
   const double* ent_uv;
   double2* ent_zk;              // [nk][nent] zekr_uV per entry, or null
+  int npair;                    // (point, atom) pairs (0: none)
+  const int* pair_fp;
+  double2* pair_ph;             // [nk][npair] exp(i kAc.r), or null
 };
 
 __global__ void k_prep(PrepArgs a) {
@@ -76,6 +79,20 @@ __global__ void k_prep(PrepArgs a) {
       sincos(th, &s, &c);
       const double uv = a.ent_uv[e];
       a.ent_zk[i] = make_double2(c * uv, -s * uv);
+    }
+  }
+  // pair phases exp(i kAc.r) (the same sincos as the point phases)
+  if (a.pair_ph != nullptr && a.npair > 0) {
+    const long npr = (long)a.nk * a.npair;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < npr; i += (long)gridDim.x * blockDim.x) {
+      const int k = (int)(i / a.npair);
+      const double* r = a.pt_r + 3L * a.pair_fp[(int)(i % a.npair)];
+      double kAc[3];
+      for (int d = 0; d < 3; ++d) kAc[d] = a.vec_k[3 * k + d] + A[d];
+      const double th = kAc[0] * r[0] + kAc[1] * r[1] + kAc[2] * r[2];
+      double sn, cs;
+      sincos(th, &sn, &cs);
+      a.pair_ph[i] = make_double2(cs, sn);
     }
   }
 }
@@ -469,8 +486,12 @@ int launch_prep_k(sb200_ctx* c, const double* d_A, int a_mode, int itt, double* 
   a.ent_pt = c->pp.d_ent_pt;
   a.ent_uv = c->pp.d_ent_uv;
   a.ent_zk = (phases && c->g.periodic && c->pp.nent > 0) ? c->pp.d_ent_zk : nullptr;
+  a.npair = c->pp.npair;
+  a.pair_fp = c->pp.d_pair_fp;
+  a.pair_ph = (phases && c->g.periodic && c->pp.npair > 0) ? c->pp.d_pair_ph : nullptr;
   long items = (long)a.nk * (a.totpts > 0 ? a.totpts : 1);
   if ((long)a.nk * a.nent > items) items = (long)a.nk * a.nent;
+  if ((long)a.nk * a.npair > items) items = (long)a.nk * a.npair;
   k_prep<<<grid_for(items, 256), 256, 0, c->stream>>>(a);
   SB_LAUNCH_CHECK("k_prep");
   return SB200_OK;

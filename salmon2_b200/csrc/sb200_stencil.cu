@@ -78,6 +78,12 @@ TiledArgs make_tiled_args(const sb200_ctx* c, double2 zc) {
   a.ent_lma = c->pp.d_ent_lma;
   a.ent_zk = c->pp.d_ent_zk;
   a.proj = c->d_proj;
+  a.use_pairs = (c->pp.nlma > 0 && c->pp.d_pmap2 != nullptr) ? 1 : 0;
+  a.npair = c->pp.npair;
+  a.pair_lma = c->pp.d_pair_lma;
+  a.pair_uv = c->pp.d_pair_uv;
+  a.pair_ph = c->pp.d_pair_ph;
+  if (a.use_pairs) a.pmap = c->pp.d_pmap2;
   a.zc = zc;
   a.zchunk = c->g.nz;
   return a;

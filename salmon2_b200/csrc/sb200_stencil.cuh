@@ -14,6 +14,11 @@ struct TiledArgs {
   const int *pmap, *ent_lma;
   const double2* ent_zk;
   const double2* proj;
+  // (point, atom) pair form of the scatter (use_pairs = 1: pmap holds pair ranges)
+  int use_pairs, npair;
+  const int* pair_lma;
+  const double* pair_uv;
+  const double2* pair_ph;
   double2 zc;
 };
 

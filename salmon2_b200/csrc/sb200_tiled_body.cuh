@@ -92,6 +92,45 @@ __device__ __forceinline__ float2 hcore(float vl, float lap0, float2 c, float2 v
   return __ffma2_rn(make_float2(-0.5f, -0.5f), v, __ffma2_rn(make_float2(vl, vl), c, cscal(lap0, c)));
 }
 
+// KB term of one point in the (point, atom) pair form: for each atom whose
+// sphere holds the point, conj(exp(i (k+A).r)) sum_q uV_q P(lma0 + q)
+// (the zekr_uV of nonlocal_potential.f90:368-375 factored into the point's
+// phase and the projectors' uV); pairs two at a time with their loads issued
+// together.  P: this orbital's projections (shared or global memory).
+template <typename R, typename C2>
+__device__ __forceinline__ C2 kb_pairs(C2 h, int pm, const double2* __restrict__ P, const TiledArgs& a, int ik) {
+  const double2* ph = a.pair_ph + (a.phase_per_k ? (long)ik * a.npair : 0L);
+  const int p0 = pm >> 8, p1 = p0 + (pm & 255);
+  for (int pr = p0; pr < p1; pr += 2) {
+    int lm[2];
+    double2 u01[2], u23[2], e[2];
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      const int pp = min(pr + i, p1 - 1);
+      lm[i] = __ldg(a.pair_lma + pp);
+      u01[i] = __ldg((const double2*)(a.pair_uv + 4L * pp));
+      u23[i] = __ldg((const double2*)(a.pair_uv + 4L * pp + 2));
+      e[i] = __ldg(ph + pp);
+    }
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      if (pr + i < p1) {
+        const int l0 = lm[i] & 0xffffff, np = lm[i] >> 24;
+        const double uq[4] = {u01[i].x, u01[i].y, u23[i].x, u23[i].y};
+        C2 sp = Cx<R>::make(0, 0);
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+          if (q < np) {
+            const double2 pv = P[l0 + q];
+            sp = cfma((R)uq[q], Cx<R>::make((R)pv.x, (R)pv.y), sp);
+          }
+        h = cadd(h, cmul(Cx<R>::make((R)e[i].x, -(R)e[i].y), sp));
+      }
+    }
+  }
+  return h;
+}
+
 // wrap (periodic) or test (Dirichlet) a coordinate that may be up to 4 outside
 __device__ __forceinline__ int wrapc(int q, int n, int periodic, bool& ok) {
   if (periodic) {
@@ -286,7 +325,9 @@ __device__ __forceinline__ void tiled_body(const typename Cx<typename ModeT<MODE
         h.x += ww.y;
         h.y -= ww.x;
       }
-      if (a.nlma > 0 && pm >= 0) {
+      if (a.nlma > 0 && pm >= 0 && a.use_pairs) {
+        h = kb_pairs<R>(h, pm, a.proj + (long)o * a.nlma, a, ik);
+      } else if (a.nlma > 0 && pm >= 0) {
         const double2* pj = a.proj + (long)o * a.nlma;
         const double2* zk = a.ent_zk + (a.phase_per_k ? (long)ik * a.nent : 0L);
         const int e0 = pm >> 8, e1 = e0 + (pm & 255);

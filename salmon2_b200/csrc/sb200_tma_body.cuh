@@ -241,7 +241,9 @@ __device__ __forceinline__ bool tma_body(const TmaMaps& maps, void* __restrict__
           h.x += ww.y;
           h.y -= ww.x;
         }
-        if (a.nlma > 0 && pm >= 0) {
+        if (a.nlma > 0 && pm >= 0 && a.use_pairs) {
+          h = kb_pairs<R>(h, pm, ps_smem ? psm : a.proj + (long)o * a.nlma, a, ik);
+        } else if (a.nlma > 0 && pm >= 0) {
           const double2* pj = ps_smem ? psm : a.proj + (long)o * a.nlma;
           const double2* zk = a.ent_zk + (a.phase_per_k ? (long)ik * a.nent : 0L);
           const int e0 = pm >> 8, e1 = e0 + (pm & 255);

@@ -351,8 +351,9 @@ def main_batch(args):
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": bytes_io,
                 "d2h_bytes_per_step": bytes_io + 4 * nt * 8 * len(systems)},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": ncu_traffic("k_hpsi_batch", "batch"), "peak_source": peak_kind,
-                     "kernel": "k_hpsi_batch", "avg_launch_ms": avg_ms,
+                     "traffic": None, "peak_source": peak_kind,
+                     "kernel": "k_hpsi_batch_tma" if all(t == 2 for t in tiles[0]) else "k_hpsi_batch",
+                     "avg_launch_ms": avg_ms,
                      "algorithmic_bytes_per_launch": bytes_per_launch},
         "kernel_shares": {k: round(v[0] / total_ms, 4) for k, v in kt.items()},
         "gpu_launches": int(round(launches_per_tstep * nt * args.steps)),

@@ -16,6 +16,13 @@ FP64 first term, psi accumulation, density and current) -- and reports:
 
 Usage: ``python -m salmon2_b200.precision_study --nt 4000`` (the 2x2x2
 supercell workload: 32^3 grid, 64 atoms, 8 k-points, 256 orbitals per k).
+
+The initial orbitals are band-limited plane-wave sums (kinetic energy
+|k+G|^2/2 <= ``--ecut`` Hartree, 2.0 by default), a stand-in for occupied
+states; ``--white`` uses white-noise fields instead, whose spectral weight sits
+near the grid cutoff (mean kinetic energy about 12 Hartree at h = 0.64 bohr),
+where the Taylor terms n >= 2 are of the order of psi itself and the FP32
+rounding of those terms is largest.
 """
 from __future__ import annotations
 
@@ -75,10 +82,13 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--nt", type=int, default=4000)
     ap.add_argument("--nkgrid", type=int, default=2)
+    ap.add_argument("--ecut", type=float, default=2.0)
+    ap.add_argument("--white", action="store_true")
     ap.add_argument("--out", default=None)
     args = ap.parse_args()
+    ecut = None if args.white else args.ecut
     s = synth.periodic_system(a=10.26, num=16, nkgrid=args.nkgrid, no=256, supercell=2, seed=3,
-                              name="periodic_supercell")
+                              name="periodic_supercell", ecut=ecut)
     dt = 0.08
     omega = 1.55 / synth.AU_ENERGY_EV
     Ac = synth.asin2cos(args.nt, dt, omega=omega, f0=omega * 1e-3, tw=args.nt * dt)
@@ -87,7 +97,8 @@ def main():
     rmx = run(s, args.nt, dt, Ac, zc, "mixed")
     res = compare(r64, rmx)
     res.update(workload=f"periodic supercell 32^3, {s.pp.natom} atoms, {s.nk} k, {s.no} orbitals/k, "
-                        f"{args.nt} steps dt={dt}", nt=args.nt)
+                        f"{args.nt} steps dt={dt}", nt=args.nt,
+               orbitals="white noise" if ecut is None else f"band-limited, |k+G|^2/2 <= {ecut} Ha")
     print(json.dumps(res), flush=True)
     if args.out:
         json.dump(res, open(args.out, "w"))

@@ -15,7 +15,8 @@ SALMON's set-up code would hand them to ``hpsi``/``taylor``:
   ``src/rt/em_field.f90:86-306``.
 
 No real pseudopotential or ground state is involved: orbitals are seeded random
-fields times a smooth envelope, orthonormalised with the ``hvol`` metric.
+fields times a smooth envelope (or, for periodic grids on request, band-limited
+plane-wave sums), orthonormalised with the ``hvol`` metric.
 """
 from __future__ import annotations
 
@@ -268,6 +269,37 @@ def random_orbitals(grid: Grid, rng, nspin, no, nk, envelope_width=None, real=Fa
     return out
 
 
+def band_limited_orbitals(grid: Grid, rng, nspin, no, vec_k, ecut) -> np.ndarray:
+    """Seeded Bloch orbitals (periodic part u_k on the grid) built only from
+    plane waves with kinetic energy |k+G|^2/2 <= ecut (Hartree), orthonormal
+    per (k, spin) in the hvol metric.  A stand-in for occupied states, whose
+    spectral weight lies at low energy, unlike white-noise fields."""
+    if not grid.periodic:
+        raise ValueError("band-limited orbitals are defined for periodic grids")
+    nx, ny, nz = grid.shape
+    npt = nx * ny * nz
+    L = grid.hgs * np.array([nx, ny, nz], dtype=np.float64)
+    g = [2.0 * math.pi * np.fft.fftfreq(n, 1.0 / n) / L[d] for d, n in enumerate((nx, ny, nz))]
+    out = np.zeros(grid.shape_array + (nspin, no, vec_k.shape[1]), dtype=np.complex128, order="F")
+    sl = grid.interior_slices()
+    for ik in range(vec_k.shape[1]):
+        k = vec_k[:, ik]
+        kin = 0.5 * ((g[0][:, None, None] + k[0]) ** 2 + (g[1][None, :, None] + k[1]) ** 2
+                     + (g[2][None, None, :] + k[2]) ** 2)
+        mask = kin <= ecut
+        ng = int(mask.sum())
+        if ng < no:
+            raise ValueError(f"ecut={ecut} admits {ng} plane waves at k-point {ik}, fewer than {no} orbitals")
+        for isp in range(nspin):
+            c = np.zeros((nx, ny, nz, no), dtype=np.complex128)
+            c[mask] = rng.standard_normal((ng, no)) + 1j * rng.standard_normal((ng, no))
+            a = np.fft.ifftn(c, axes=(0, 1, 2)).reshape((npt, no), order="F")
+            q = _cholesky_qr2(a) / math.sqrt(grid.hvol)
+            for io in range(no):
+                out[sl + (isp, io, ik)] = q[:, io].reshape((nx, ny, nz), order="F")
+    return out
+
+
 def mp_kpoints(nkgrid, cell):
     """Monkhorst-Pack k-points, cubic cell, Cartesian, weights 1/nk."""
     n = int(nkgrid)
@@ -373,8 +405,10 @@ DIAMOND = np.array([[0, 0, 0], [0.5, 0.5, 0], [0.5, 0, 0.5], [0, 0.5, 0.5],
 
 
 def periodic_system(a=10.26, num=16, nkgrid=4, no=32, supercell=1, seed=2, rc_aa=1.2,
-                    nspin=1, name="periodic") -> System:
-    """Periodic bulk (diamond positions), Monkhorst-Pack k-points."""
+                    nspin=1, name="periodic", ecut=None) -> System:
+    """Periodic bulk (diamond positions), Monkhorst-Pack k-points.  Orbitals are
+    white-noise fields, or with ``ecut`` (Hartree) band-limited to plane waves
+    of kinetic energy <= ecut."""
     rng = np.random.default_rng(seed)
     cell = np.full(3, a * supercell)
     grid = make_grid([num * supercell] * 3, cell[0] / (num * supercell), periodic=True)
@@ -389,6 +423,9 @@ def periodic_system(a=10.26, num=16, nkgrid=4, no=32, supercell=1, seed=2, rc_aa
     V_local = np.asfortranarray(np.repeat(V[..., None], nspin, axis=3))
     vec_k, wtk = mp_kpoints(nkgrid, cell)
     nk = vec_k.shape[1]
-    psi = random_orbitals(grid, rng, nspin, no, nk)
+    if ecut is None:
+        psi = random_orbitals(grid, rng, nspin, no, nk)
+    else:
+        psi = band_limited_orbitals(grid, rng, nspin, no, vec_k, ecut)
     return System(grid, pp, nspin, no, nk, vec_k, np.asfortranarray(np.full((no, nk, nspin), 2.0)), wtk,
                   V_local, rion, psi, int(np.prod(grid.num)), seed, name)

@@ -14,9 +14,10 @@ computed every step.  Metric: grid-point x orbital Taylor steps per second
   buffers: per bench step the pinned reference-layout orbitals are uploaded
   (sb200_orbitals_from_ref), propagated, and J(t) plus the final orbitals are
   read back to the host (sb200_orbitals_to_ref).
-* ``roofline``: the fused stencil kernel (k_hpsi), timed with CUDA events on
-  the library's stream in an instrumented replay right after the timed
-  region; algorithmic bytes 224 B per unit per Taylor step over its 4 launches.
+* ``roofline``: the kernel that applies H (on this workload k_step_orbital,
+  the whole Taylor step of one orbital per CTA), timed with CUDA events on the
+  library's stream in an instrumented replay right after the timed region;
+  algorithmic bytes 224 B per unit per Taylor step.
 * ``cpu_baseline``: the CPU oracle (a C++/OpenMP restatement of the
   reference's Fortran path) on a bounded sample of the same workload.
 
@@ -153,8 +154,26 @@ def measured_peaks():
 
 
 def orbital_path(s, args):
-    """The one-CTA-per-orbital kernel runs periodic 16^3 grids in FP64."""
+    """The one-CTA-per-orbital kernels run periodic 16^3 grids in FP64."""
     return s.grid.periodic and tuple(s.grid.shape) == (16, 16, 16) and args.precision == "fp64"
+
+
+def hpsi_kernel(s, args, units_per_launch):
+    """(name, algorithmic bytes per launch) of the kernel that applies H.
+
+    The algorithmic bytes of a Taylor step are 224 B per unit (FP64; 144 B
+    mixed) whatever the kernel split: a per-term kernel is credited a quarter
+    per launch, the fused-step kernel (all four terms in one launch, which
+    itself moves only psi in and psi_out out) the whole 224 B."""
+    if orbital_path(s, args):
+        v = os.environ.get("SB200_ORBITAL", "fused")
+        if v.startswith("p"):
+            return "k_term_orbital_tma", UNIT_BYTES["fp64"] / 4.0 * units_per_launch
+        if v.startswith("t"):
+            return "k_term_orbital", UNIT_BYTES["fp64"] / 4.0 * units_per_launch
+        return "k_step_orbital", UNIT_BYTES["fp64"] * units_per_launch
+    name = "k_hpsi_tiled" if os.environ.get("SB200_TMA", "on").startswith("of") else "k_hpsi_tma"
+    return name, UNIT_BYTES[args.precision] / 4.0 * units_per_launch
 
 
 def ncu_traffic(kernel, workload):
@@ -461,19 +480,13 @@ def main():
     ctx.set_timing(False)
     launches_per_tstep = sum(v[1] for v in kt.values()) / nt_i
     gpu_launches = int(round(launches_per_tstep * nt * args.steps))
-    if orbital_path(s, args):
-        hpsi_kernel = "k_term_orbital"
-    elif os.environ.get("SB200_TMA", "on").startswith("of"):
-        hpsi_kernel = "k_hpsi_tiled"
-    else:  # the tensor-copy sweep takes isolated grids and periodic grids with nx = 32
-        hpsi_kernel = "k_hpsi_tma"
+    units_per_launch = int(np.prod(s.grid.shape)) * s.norb
+    kname, bytes_per_launch = hpsi_kernel(s, args, units_per_launch)
     peak, peak_kind = measured_peaks()
     h_ms, h_cnt = kt.get("hpsi", (float("nan"), 1))
-    units_per_launch = int(np.prod(s.grid.shape)) * s.norb
-    bytes_per_launch = UNIT_BYTES[args.precision] / 4.0 * units_per_launch
     avg_ms = h_ms / h_cnt
     achieved = bytes_per_launch / (avg_ms / 1e3) / 1e9
-    traffic = ncu_traffic(hpsi_kernel, args.workload)
+    traffic = ncu_traffic(kname, args.workload)
     total_ms = sum(v[0] for v in kt.values())
     shares = {k: round(v[0] / total_ms, 4) for k, v in kt.items()}
 
@@ -491,7 +504,7 @@ def main():
                     "d2h_bytes_per_step": bytes_io + 3 * nt * 8 + 4 * nt * 8},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
-                         "kernel": hpsi_kernel, "avg_launch_ms": avg_ms,
+                         "kernel": kname, "avg_launch_ms": avg_ms,
                          "algorithmic_bytes_per_launch": bytes_per_launch},
             "kernel_shares": shares,
             "gpu_launches": gpu_launches,

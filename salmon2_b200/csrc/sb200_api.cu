@@ -214,6 +214,10 @@ int timing_flush(sb200_ctx* c) {
 // projections of each term's input computed first.
 int issue_taylor(sb200_ctx* c, double2* tin, double2* tout, double2* work, const double2* zc, int n_hamil,
                  bool last_with_obs = false) {
+  if (step_orbital_applies(c, n_hamil)) {  // all terms in one launch, observables fused
+    TIMED(c, SB200_KIND_HPSI, launch_step_orbital(c, tin, tout, zc, n_hamil, last_with_obs));
+    return SB200_OK;
+  }
   const bool orbital = orbital_kernel_applies(c);
   for (int nn = 1; nn <= n_hamil; ++nn) {
     if (orbital) {  // one CTA per orbital: projections and observables in-kernel
@@ -314,7 +318,7 @@ int sb200_ctx_create(int device, sb200_ctx** out) {
   }
   c->stream = c->own_stream;
   if (const char* v = getenv("SB200_STENCIL")) c->stencil_variant = (v[0] == 'n') ? 0 : 1;
-  if (const char* v = getenv("SB200_ORBITAL")) c->orbital_variant = (v[0] == 'p') ? 1 : 0;
+  if (const char* v = getenv("SB200_ORBITAL")) c->orbital_variant = (v[0] == 'p') ? 1 : (v[0] == 't') ? 0 : 2;
   if (const char* v = getenv("SB200_TMA")) c->tma_variant = (v[0] == 'o' && v[1] == 'f') ? 0 : 1;
   int r = dalloc(&c->d_result, 16);
   if (r == SB200_OK) r = dalloc(&c->rt.d_step, 1);

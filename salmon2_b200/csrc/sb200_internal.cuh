@@ -142,7 +142,7 @@ struct sb200_ctx {
   size_t stage_bytes = 0;
   bool vloc_set = false;
   int stencil_variant = 1;     // 0: per-point reference kernel, 1: tiled 2.5-D sweep
-  int orbital_variant = 0;     // 16^3 periodic grids: 0 one CTA per orbital, 1 persistent with bulk copies
+  int orbital_variant = 2;     // 16^3 periodic grids: 2 fused Taylor step, 0 one launch per term, 1 persistent per term
   int tma_variant = 1;         // tiled hpsi fed by tensor copies where it applies (0: register-prefetch sweep)
   // optional per-kernel-class device timing (sb200_set_timing)
   bool timing = false;
@@ -209,6 +209,9 @@ int launch_hpsi_tiled(sb200_ctx* c, const HpsiLaunch& L);  // sb200_stencil.cu
 int launch_hpsi_tma(sb200_ctx* c, const HpsiLaunch& L);
 bool orbital_kernel_applies(const sb200_ctx* c);             // sb200_orbital.cu
 int launch_term_orbital(sb200_ctx* c, const HpsiLaunch& L, bool with_obs);
+bool step_orbital_applies(const sb200_ctx* c, int n_hamil);                  // sb200_orbital.cu
+int launch_step_orbital(sb200_ctx* c, const double2* in, double2* out, const double2* zc, int n_hamil,
+                        bool with_obs);
 int launch_observables(sb200_ctx* c, const double2* psi);
 int launch_project_moments(sb200_ctx* c, const double2* psi);
 int launch_finalize(sb200_ctx* c, int itt_host, int nt, int trans_longi, double dt, int spin_filter,

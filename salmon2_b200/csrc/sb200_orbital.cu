@@ -34,12 +34,13 @@ __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
 }
 
 // Projections P(lma) = rinv * sum_j conj(zekr_uV) v(pt_j) of the orbital held
-// in shared memory: one warp per atom, projectors four at a time.
+// in shared memory: one warp per atom (NWARP warps), projectors four at a time.
+template <int NWARP = NT / 32>
 __device__ void project_from_smem(const double2* __restrict__ sm, double2* __restrict__ Ps, const OrbArgs& a,
                                   int ik) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const double2* ph = a.phase + (long)ik * a.totpts;
-  for (int atom = warp; atom < a.natom; atom += NT / 32) {
+  for (int atom = warp; atom < a.natom; atom += NWARP) {
     const int start = a.atom_start[atom], m = a.mps[atom];
     const int lma0 = a.lma_start[atom], np = a.nproj[atom];
     for (int q0 = 0; q0 < np; q0 += 4) {
@@ -72,13 +73,15 @@ __device__ void project_from_smem(const double2* __restrict__ sm, double2* __res
 }
 
 // Nonlocal current pieces sum_lma Im(conj(<r_d zekr|v>) rinv <zekr|v>) of the
-// orbital in shared memory; result reduced over the block into red3[0..2].
+// orbital in shared memory, computed by NWARP warps (this one is number
+// `warp`); per-warp sums in wsum[warp][0..2].
 template <int NWARP>
 __device__ void current_nonlocal_from_smem(const double2* __restrict__ sm, const OrbArgs& a, int ik,
-                                           double* __restrict__ wsum /* [NWARP][3] */) {
+                                           double* __restrict__ wsum /* [NWARP][3] */,
+                                           int warp = (int)(threadIdx.x >> 5)) {
   // one pass over the atom's sphere per four projectors: e psi(pt) once per
   // point, then <zekr|psi> and <r_d zekr|psi> of each projector
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int lane = threadIdx.x & 31;
   const double2* ph = a.phase + (long)ik * a.totpts;
   double jx = 0.0, jy = 0.0, jz = 0.0;
   for (int atom = warp; atom < a.natom; atom += NWARP) {
@@ -283,6 +286,189 @@ __global__ void __launch_bounds__(NT, 2) k_term_orbital(const double2* __restric
     double s = 0.0;
     if (a.nlma > 0)
       for (int w = 0; w < NT / 32; ++w) s += jws[w][t - 32];
+    a.jw[3L * o + (t - 32)] = s;
+  }
+}
+
+
+// ---------------------------------------------------------------------------
+// Fused Taylor step: one CTA of 512 threads applies all n_hamil terms of
+// taylor.f90:47-117 to one 16^3 orbital without leaving the SM.  h_{n-1} sits
+// in one of two whole-orbital shared-memory buffers while h_n is written into
+// the other; psi_out sits in a third.  Thread t owns column (x, y) = t mod 256
+// for the eight planes z0 = 8 (t / 256) .. z0 + 7 and keeps those eight values
+// of h_{n-1} in registers for the z neighbours; the four-plane halo owned by the
+// other half of the column is read from shared memory.  Each term starts with
+// the KB projections of h_{n-1} from shared memory.  HBM traffic per step is
+// read psi + write psi_out (32 B per point) instead of 224 B for four separate
+// term launches.  The operations per point and term, and their order, are
+// those of k_term_orbital.
+// ---------------------------------------------------------------------------
+constexpr int NTF = 2 * NP;  // threads of the fused-step CTA
+constexpr int HZ = N / 2;    // planes per thread
+
+template <bool OBS>
+__global__ void __launch_bounds__(NTF, 1) k_step_orbital(const double2* __restrict__ in, double2* __restrict__ out,
+                                                         OrbArgs a, StepZC zc, int nterm) {
+  extern __shared__ double2 smem[];
+  double2* bufs = smem;               // two whole-orbital buffers: h_{n-1}, h_n
+  double2* accb = smem + 2 * N * NP;  // psi_out
+  double2* Ps = accb + N * NP;        // projections of h_{n-1}
+  const int o = blockIdx.x;
+  const int t = threadIdx.x;
+  const int col = t & (NP - 1);
+  const int z0 = (t >> 8) * HZ;
+  const int tx = col & (N - 1), ty = col >> 4;
+  const int ik = o / a.nspin_no;
+  const int ispin = o % a.nspin;
+  const double* kc = a.kcoef + (long)KC * ik;
+  const double2* src = in + (long)o * a.npts;
+
+  double2 cv[HZ];
+#pragma unroll
+  for (int j = 0; j < HZ; ++j) cv[j] = __ldg(src + (z0 + j) * NP + col);
+#pragma unroll
+  for (int j = 0; j < HZ; ++j) bufs[(z0 + j) * NP + col] = cv[j];
+  __syncthreads();
+  const double kx = kc[0], ky = kc[1], kz = kc[2], lap0 = kc[3];
+  int oxp[ND], oxm[ND], oyp[ND], oym[ND];
+#pragma unroll
+  for (int s = 1; s <= ND; ++s) {
+    oxp[s - 1] = ty * N + ((tx + s) & (N - 1));
+    oxm[s - 1] = ty * N + ((tx - s) & (N - 1));
+    oyp[s - 1] = (((ty + s) & (N - 1)) << 4) + tx;
+    oym[s - 1] = (((ty - s) & (N - 1)) << 4) + tx;
+  }
+  const double* vloc = a.vloc + (long)ispin * a.npts;
+  const double2* zkk = a.ent_zk + (long)ik * a.nent;
+  double2* odst = out + (long)o * a.npts;
+  int b = 0;
+  for (int nn = 0; nn < nterm; ++nn) {
+    const double2* cur = bufs + b * (N * NP);
+    double2* nxt = bufs + (b ^ 1) * (N * NP);
+    if (a.nlma > 0) {
+      project_from_smem<NTF / 32>(cur, Ps, a, ik);
+      __syncthreads();
+    }
+    const bool last = nn == nterm - 1;
+    const double2 zn = zc.v[nn];
+    const double2* oth = cur + (z0 ^ HZ) * NP + col;  // the other half of this column
+    double vl_n = __ldg(vloc + z0 * NP + col);
+    int pm_n = a.nlma > 0 ? __ldg(a.pmap + z0 * NP + col) : -1;
+    double2 hv[HZ];
+#pragma unroll
+    for (int j = 0; j < HZ; ++j) {
+      const int z = z0 + j;
+      const double vl = vl_n;
+      const int pm = pm_n;
+      if (j + 1 < HZ) {
+        vl_n = __ldg(vloc + (z + 1) * NP + col);
+        if (a.nlma > 0) pm_n = __ldg(a.pmap + (z + 1) * NP + col);
+      }
+      const double2* P = cur + z * NP;
+      double2 vx = make_double2(0.0, 0.0), wx = vx, vy = vx, wy = vx, vz = vx, wz = vx;
+#pragma unroll
+      for (int s = 0; s < ND; ++s) {
+        const double2 tp = P[oxp[s]], tm = P[oxm[s]];
+        vx = cadd(vx, cscal(a.lapt[s], cadd(tp, tm)));
+        wx = cadd(wx, cscal(a.nab[s], csub(tp, tm)));
+      }
+#pragma unroll
+      for (int s = 0; s < ND; ++s) {
+        const double2 tp = P[oyp[s]], tm = P[oym[s]];
+        vy = cadd(vy, cscal(a.lapt[4 + s], cadd(tp, tm)));
+        wy = cadd(wy, cscal(a.nab[4 + s], csub(tp, tm)));
+      }
+#pragma unroll
+      for (int s = 0; s < ND; ++s) {
+        const double2 tp = (j + s + 1 < HZ) ? cv[(j + s + 1) & (HZ - 1)] : oth[(j + s + 1 - HZ) * NP];
+        const double2 tm = (j - s - 1 >= 0) ? cv[(j - s - 1) & (HZ - 1)] : oth[(j - s - 1 + HZ) * NP];
+        vz = cadd(vz, cscal(a.lapt[8 + s], cadd(tp, tm)));
+        wz = cadd(wz, cscal(a.nab[8 + s], csub(tp, tm)));
+      }
+      const double2 v = cadd(vz, cadd(vy, vx));
+      const double2 w = cadd(cscal(kz, wz), cadd(cscal(ky, wy), cscal(kx, wx)));
+      const double2 c = cv[j];
+      const int p = z * NP + col;
+      double2 h;
+      h.x = vl * c.x + lap0 * c.x - 0.5 * v.x + w.y;
+      h.y = vl * c.y + lap0 * c.y - 0.5 * v.y - w.x;
+      if (a.nlma > 0) {
+        if (pm >= 0) {
+          const int e1 = (pm >> 8) + (pm & 255);
+          for (int e = pm >> 8; e < e1; ++e) h = cadd(h, cmul(Ps[__ldg(a.ent_lma + e)], __ldg(zkk + e)));
+        }
+      }
+      // psi_out = psi + zc_1 h_1 (first term), psi_out + zc_n h_n (later terms)
+      const double2 nv = cadd(nn == 0 ? c : accb[p], cmul(zn, h));
+      if (last) {
+        odst[p] = nv;
+        if (OBS) accb[p] = nv;
+      } else {
+        accb[p] = nv;
+        nxt[p] = h;
+        hv[j] = h;
+      }
+    }
+    __syncthreads();  // h_n complete in nxt; reads of cur and Ps done
+    if (!last) {
+#pragma unroll
+      for (int j = 0; j < HZ; ++j) cv[j] = hv[j];
+      b ^= 1;
+    }
+  }
+  if (!OBS) return;
+  // ---- observables of the new orbital (in accb): warps 0-7 the local sums
+  // over whole columns, warps 8-15 the nonlocal current, as in k_term_orbital
+  __shared__ double red[OBS_NQ][NP / 32];
+  __shared__ double jws[NP / 32][3];
+  const int warp = t >> 5, lane = t & 31;
+  if (t < NP) {
+    const double2* sm = accb;
+    double q[OBS_NQ];
+#pragma unroll
+    for (int i = 0; i < OBS_NQ; ++i) q[i] = 0.0;
+#pragma unroll 4
+    for (int z = 0; z < N; ++z) {
+      const double2 c = sm[z * NP + t];
+      const double r2 = c.x * c.x + c.y * c.y;
+      q[0] += r2;
+      double ix = 0.0, iy = 0.0, iz = 0.0;
+#pragma unroll
+      for (int s = 1; s <= ND; ++s) {
+        const double2 txv = sm[z * NP + ty * N + ((tx + s) & (N - 1))];
+        const double2 tyv = sm[z * NP + (((ty + s) & (N - 1)) << 4) + tx];
+        const double2 tzv = sm[((z + s) & (N - 1)) * NP + t];
+        ix += a.nab[s - 1] * (c.x * txv.y - c.y * txv.x);
+        iy += a.nab[4 + s - 1] * (c.x * tyv.y - c.y * tyv.x);
+        iz += a.nab[8 + s - 1] * (c.x * tzv.y - c.y * tzv.x);
+      }
+      q[1] += ix;
+      q[2] += iy;
+      q[3] += iz;
+      q[4] += ((double)tx + a.off[0]) * r2;
+      q[5] += ((double)ty + a.off[1]) * r2;
+      q[6] += ((double)z + a.off[2]) * r2;
+    }
+#pragma unroll
+    for (int i = 0; i < OBS_NQ; ++i) {
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) q[i] += __shfl_xor_sync(0xffffffffu, q[i], off);
+    }
+    if (lane == 0)
+      for (int i = 0; i < OBS_NQ; ++i) red[i][warp] = q[i];
+  } else if (a.nlma > 0) {
+    current_nonlocal_from_smem<NP / 32>(accb, a, ik, &jws[0][0], warp - NP / 32);
+  }
+  __syncthreads();
+  if (t < OBS_NQ) {
+    double s = 0.0;
+    for (int w = 0; w < NP / 32; ++w) s += red[t][w];
+    a.obs[(long)o * OBS_NQ + t] = s;
+  } else if (t >= 32 && t < 35) {
+    double s = 0.0;
+    if (a.nlma > 0)
+      for (int w = 0; w < NP / 32; ++w) s += jws[w][t - 32];
     a.jw[3L * o + (t - 32)] = s;
   }
 }
@@ -532,25 +718,8 @@ bool orbital_kernel_applies(const sb200_ctx* c) {
          c->pp.nlma <= ORB_MAX_NLMA && c->precision == SB200_PREC_FP64;
 }
 
-int launch_term_orbital(sb200_ctx* c, const HpsiLaunch& L, bool with_obs) {
-  static bool attr_set = false, attr_set2 = false;
-  const size_t smem = (size_t)N * NP * sizeof(double2) + (size_t)ORB_MAX_NLMA * sizeof(double2);
-  const size_t smem2 = 3 * (size_t)ORB_BYTES + (size_t)ORB_MAX_NLMA * sizeof(double2);
-  const bool persistent = c->orbital_variant == 1;
-  if (!persistent && !attr_set) {
-    SB_CUDA(cudaFuncSetAttribute(k_term_orbital<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    SB_CUDA(cudaFuncSetAttribute(k_term_orbital<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    SB_CUDA(cudaFuncSetAttribute(k_term_orbital<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    SB_CUDA(cudaFuncSetAttribute(k_term_orbital<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    attr_set = true;
-  }
-  if (persistent && !attr_set2) {
-    SB_CUDA(cudaFuncSetAttribute(k_term_orbital_tma<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2));
-    SB_CUDA(cudaFuncSetAttribute(k_term_orbital_tma<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2));
-    SB_CUDA(cudaFuncSetAttribute(k_term_orbital_tma<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2));
-    SB_CUDA(cudaFuncSetAttribute(k_term_orbital_tma<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2));
-    attr_set2 = true;
-  }
+namespace {
+OrbArgs make_orb_args(const sb200_ctx* c, double2 zc, bool with_obs) {
   OrbArgs a;
   a.npts = c->g.npts;
   a.nspin = c->orb.nspin;
@@ -580,9 +749,59 @@ int launch_term_orbital(sb200_ctx* c, const HpsiLaunch& L, bool with_obs) {
   a.pt_r = c->pp.d_pt_r;
   a.uv = c->pp.d_uv;
   a.rinv = c->pp.d_rinv;
-  a.zc = L.zc;
+  a.zc = zc;
   a.obs = with_obs ? c->d_obs : nullptr;
   a.jw = with_obs ? c->d_jw : nullptr;
+  return a;
+}
+}  // namespace
+
+bool step_orbital_applies(const sb200_ctx* c, int n_hamil) {
+  return orbital_kernel_applies(c) && c->orbital_variant == 2 && n_hamil >= 1 && n_hamil <= STEP_MAX_NTERM;
+}
+
+// One launch for the whole Taylor step: psi_out = sum_n zc_n H^n psi (+ psi).
+int launch_step_orbital(sb200_ctx* c, const double2* in, double2* out, const double2* zc, int n_hamil,
+                        bool with_obs) {
+  // dynamic shared memory: three orbital buffers and the projections
+  const size_t smem = 3 * (size_t)N * NP * sizeof(double2) + (size_t)ORB_MAX_NLMA * sizeof(double2);
+  static bool attr_set = false;
+  if (!attr_set) {
+    SB_CUDA(cudaFuncSetAttribute(k_step_orbital<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    SB_CUDA(cudaFuncSetAttribute(k_step_orbital<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    attr_set = true;
+  }
+  if (n_hamil < 1 || n_hamil > STEP_MAX_NTERM) return set_error(SB200_ERR_INVALID_ARG, "fused step: bad n_hamil");
+  StepZC z;
+  for (int i = 0; i < STEP_MAX_NTERM; ++i) z.v[i] = i < n_hamil ? zc[i] : make_double2(0.0, 0.0);
+  const OrbArgs a = make_orb_args(c, zc[0], with_obs);
+  dim3 grid(c->orb.norb);
+  if (with_obs) k_step_orbital<true><<<grid, NTF, smem, c->stream>>>(in, out, a, z, n_hamil);
+  else k_step_orbital<false><<<grid, NTF, smem, c->stream>>>(in, out, a, z, n_hamil);
+  SB_LAUNCH_CHECK("k_step_orbital");
+  return SB200_OK;
+}
+
+int launch_term_orbital(sb200_ctx* c, const HpsiLaunch& L, bool with_obs) {
+  static bool attr_set = false, attr_set2 = false;
+  const size_t smem = (size_t)N * NP * sizeof(double2) + (size_t)ORB_MAX_NLMA * sizeof(double2);
+  const size_t smem2 = 3 * (size_t)ORB_BYTES + (size_t)ORB_MAX_NLMA * sizeof(double2);
+  const bool persistent = c->orbital_variant == 1;
+  if (!persistent && !attr_set) {
+    SB_CUDA(cudaFuncSetAttribute(k_term_orbital<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    SB_CUDA(cudaFuncSetAttribute(k_term_orbital<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    SB_CUDA(cudaFuncSetAttribute(k_term_orbital<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    SB_CUDA(cudaFuncSetAttribute(k_term_orbital<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    attr_set = true;
+  }
+  if (persistent && !attr_set2) {
+    SB_CUDA(cudaFuncSetAttribute(k_term_orbital_tma<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2));
+    SB_CUDA(cudaFuncSetAttribute(k_term_orbital_tma<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2));
+    SB_CUDA(cudaFuncSetAttribute(k_term_orbital_tma<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2));
+    SB_CUDA(cudaFuncSetAttribute(k_term_orbital_tma<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2));
+    attr_set2 = true;
+  }
+  const OrbArgs a = make_orb_args(c, L.zc, with_obs);
   const double2* IN = (const double2*)L.in;
   double2* HOUT = (double2*)L.hout;
   if (persistent) {

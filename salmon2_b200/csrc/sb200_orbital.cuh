@@ -23,4 +23,9 @@ struct OrbArgs {
   double* jw;   // [norb][3] or null
 };
 
+constexpr int STEP_MAX_NTERM = 8;  // Taylor terms of the fused step kernel
+struct StepZC {
+  double2 v[STEP_MAX_NTERM];  // zc(1..n_hamil)
+};
+
 }  // namespace sb200

@@ -173,11 +173,12 @@ def test_rt_propagate_periodic16_orbital_kernel(trans):
     assert S.rel_err(ctx.download(res["psi"]), ref["psi"]) < 1e-11
 
 
-@pytest.mark.parametrize("variant", ["persistent", "classic"])
+@pytest.mark.parametrize("variant", ["fused", "persistent", "terms"])
 def test_rt_propagate_periodic16_many_orbitals(variant, monkeypatch):
-    """More orbitals than SMs: the persistent form walks several orbitals per
-    CTA through its double-buffered bulk copies (buffer reuse, barrier phase
-    flips); the one-CTA-per-orbital form is checked on the same input."""
+    """More orbitals than SMs: the fused-step kernel (all Taylor terms in one
+    launch), the persistent per-term form that walks several orbitals per CTA
+    through double-buffered bulk copies (buffer reuse, barrier phase flips) and
+    the one-launch-per-term form, each against the oracle on the same input."""
     from salmon2_b200 import synth
     monkeypatch.setenv("SB200_ORBITAL", variant)
     sysm = synth.periodic_system(a=10.26, num=16, nkgrid=4, no=5, seed=32, name="periodic16k64")
@@ -192,6 +193,35 @@ def test_rt_propagate_periodic16_many_orbitals(variant, monkeypatch):
     assert np.max(np.abs(res["curr"] - ref["curr"])) <= TOL_OBS * jmax
     assert S.rel_err(res["rbox"], ref["rbox"]) < TOL_OBS
     assert S.rel_err(ctx.download(res["psi"]), ref["psi"]) < 1e-11
+
+
+@pytest.mark.parametrize("n_hamil", [4, 1, 3])
+def test_fused_step_equals_term_launches(n_hamil, monkeypatch):
+    """The fused Taylor step and the per-term launches do the same arithmetic
+    per point and term: Taylor steps, J(t), the dipole and the orbitals agree
+    bit for bit."""
+    from salmon2_b200 import synth
+    sysm = synth.periodic_system(a=10.26, num=16, nkgrid=2, no=3, seed=34, name="periodic16k8")
+    zc = synth.taylor_zc(0.08)[:n_hamil]
+    nt, dt = 5, 0.08
+    Ac = synth.asin2cos(nt, dt, omega=0.05696, f0=0.05696 * 2e-2, tw=nt * dt)
+    outs, runs = [], []
+    for variant in ("fused", "terms"):
+        monkeypatch.setenv("SB200_ORBITAL", variant)
+        ctx = _ctx(sysm)
+        ctx.set_vec_Ac((0.01, -0.02, 0.03))
+        a, out, work = ctx.upload(sysm.psi), ctx.zeros(), ctx.zeros()
+        ctx.taylor(a, out, work, zc)
+        outs.append(ctx.download(out))
+        if n_hamil == 4:
+            a, b, w = ctx.upload(sysm.psi), ctx.zeros(), ctx.zeros()
+            res = ctx.rt_propagate(a, b, w, nt, dt, zc, Ac_ext=Ac, trans_longi="tr")
+            runs.append((res["curr"].copy(), res["rbox"].copy(), ctx.download(res["psi"])))
+        ctx.close()
+    assert np.array_equal(outs[0], outs[1])
+    if runs:
+        for x, y in zip(runs[0], runs[1]):
+            assert np.array_equal(x, y)
 
 
 def _periodic32():

@@ -146,6 +146,22 @@ int sb200_orbitals_to_ref(sb200_ctx* ctx, const double* psi_dev, double* zwf_ref
  * src/common/zpseudo.cu:132-191).  tpsi and htpsi are distinct device blocks. */
 int sb200_hpsi(sb200_ctx* ctx, const double* tpsi, double* htpsi);
 
+/* hpsi with its optional argument ttpsi: htpsi = H tpsi as sb200_hpsi, and
+ * ttpsi = the kinetic part, the stencil output minus V_local tpsi before the
+ * nonlocal term is added (-1/2 (nabla + i(k+A))^2 tpsi).
+ * Replaces: hpsi(tpsi,htpsi,...,ttpsi) (src/common/hamiltonian.f90:27,364-414).
+ * Three distinct device blocks.                                                 */
+int sb200_hpsi_tt(sb200_ctx* ctx, const double* tpsi, double* htpsi, double* ttpsi);
+
+/* Band energies of the orbital block psi: esp(no,nk,nspin) (host, Fortran
+ * order) = Re <psi|H|psi> hvol per orbital, *e_kin = sum rocc wtk Re <psi|T|psi>
+ * hvol, *e_nloc = sum rocc wtk hvol Re <psi|H - T - V_local|psi> (the KB
+ * energy).  htpsi and ttpsi are device work blocks that receive H psi and T psi.
+ * Replaces: calc_eigen_energy (src/common/total_energy.f90:505-775, complex
+ * branch), energy%esp / E_kin / E_ion_nloc.  Synchronous.                       */
+int sb200_calc_eigen_energy(sb200_ctx* ctx, const double* psi, double* htpsi, double* ttpsi, double* esp,
+                            double* e_kin, double* e_nloc);
+
 /* tspsi_out = sum_{n=0}^{n_hamil} zc(n) H^n tspsi_in, zc(0) = 1, with zc the
  * complex(n_hamil) array rt%zc (interleaved re/im, host pointer).
  * Replaces: taylor (src/rt/taylor.f90:21-121).  tspsi_in and sshtpsi are

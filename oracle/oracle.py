@@ -54,7 +54,8 @@ def lib():
         build()
         L = C.CDLL(LIB_PATH)
         for name in ("sbo_zstencil", "sbo_dstencil", "sbo_update_kvector_nonlocalpt", "sbo_zpseudo",
-                     "sbo_dpseudo", "sbo_zprojections", "sbo_hpsi", "sbo_hpsi_real", "sbo_taylor",
+                     "sbo_dpseudo", "sbo_zprojections", "sbo_hpsi", "sbo_hpsi_tt", "sbo_calc_eigen_energy",
+                     "sbo_hpsi_real", "sbo_taylor",
                      "sbo_calc_density", "sbo_calc_current", "sbo_current_parts", "sbo_calc_dip",
                      "sbo_calc_Ac_ext_t", "sbo_rt_run", "sbo_set_threads", "sbo_get_threads",
                      "sbo_precond_real", "sbo_gscg_rwf", "sbo_gram_schmidt_real", "sbo_gram_schmidt_complex",
@@ -143,6 +144,24 @@ class Oracle:
         out = np.zeros_like(a, order="F")
         lib().sbo_hpsi(C.byref(self.s), _p(a), _p(out))
         return out
+
+    def hpsi_tt(self, psi):
+        """(H psi, T psi): hpsi with its optional kinetic output ttpsi."""
+        a = self._orb(psi)
+        h = np.zeros_like(a, order="F")
+        tt = np.zeros_like(a, order="F")
+        lib().sbo_hpsi_tt(C.byref(self.s), _p(a), _p(h), _p(tt))
+        return h, tt
+
+    def calc_eigen_energy(self, psi):
+        """(esp(no,nk,nspin), E_kin, E_ion_nloc) of calc_eigen_energy."""
+        a = self._orb(psi)
+        h = np.zeros_like(a, order="F")
+        tt = np.zeros_like(a, order="F")
+        esp = np.zeros((self.sys.no, self.sys.nk, self.sys.nspin), order="F")
+        e = np.zeros(2)
+        lib().sbo_calc_eigen_energy(C.byref(self.s), _p(a), _p(h), _p(tt), _p(esp), _p(e))
+        return esp, float(e[0]), float(e[1])
 
     def hpsi_real(self, psi):
         a = np.asfortranarray(psi, dtype=np.float64)

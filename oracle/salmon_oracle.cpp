@@ -337,6 +337,74 @@ void sbo_hpsi(const sbo_system* s, const double* tpsi, double* htpsi) {
   if (s->nlma > 0) sbo_zpseudo(s, tpsi, htpsi);
 }
 
+// hpsi with ttpsi (hamiltonian.f90:27 optional argument): after the stencil,
+// ttpsi = htpsi - V_local * tpsi on the interior (:364-414), then the nonlocal
+// term is added to htpsi only.
+void sbo_hpsi_tt(const sbo_system* s, const double* tpsi, double* htpsi, double* ttpsi) {
+  Idx I(s);
+  const long nxy = I.nx * I.ny * I.nz;
+  sbo_system s0 = *s;
+  s0.nlma = 0;  // the stencil part of hpsi
+  sbo_hpsi(&s0, tpsi, htpsi);
+#pragma omp parallel for collapse(3)
+  for (int ik = 1; ik <= s->nk; ++ik)
+    for (int io = 1; io <= s->no; ++io)
+      for (int is = 1; is <= s->nspin; ++is) {
+        const long o = I.orb(is, io, ik);
+        const double* V = s->V_local + nxy * (is - 1);
+        const double* t = tpsi + 2 * I.vol * o;
+        const double* h = htpsi + 2 * I.vol * o;
+        double* tt = ttpsi + 2 * I.vol * o;
+        for (int iz = s->is[2]; iz <= s->ie[2]; ++iz)
+          for (int iy = s->is[1]; iy <= s->ie[1]; ++iy)
+            for (int ix = s->is[0]; ix <= s->ie[0]; ++ix) {
+              const long i = I.a(ix, iy, iz);
+              const double v = V[I.r(ix, iy, iz)];
+              tt[2 * i] = h[2 * i] - v * t[2 * i];
+              tt[2 * i + 1] = h[2 * i + 1] - v * t[2 * i + 1];
+            }
+      }
+  if (s->nlma > 0) sbo_zpseudo(s, tpsi, htpsi);
+}
+
+// calc_eigen_energy, complex branch (total_energy.f90:505-775): per orbital
+// esp = Re sum conj(psi) H psi * Hvol; E_kin = sum occ w Re sum conj(psi) T psi
+// * Hvol; E_ion_nloc = sum occ w Hvol Re sum conj(psi) (H psi - (T psi + V psi)).
+void sbo_calc_eigen_energy(const sbo_system* s, const double* tpsi, double* htpsi, double* ttpsi, double* esp,
+                           double* e) {
+  Idx I(s);
+  const long nxy = I.nx * I.ny * I.nz;
+  sbo_hpsi_tt(s, tpsi, htpsi, ttpsi);
+  double ek = 0.0, en = 0.0;
+  for (int is = 1; is <= s->nspin; ++is)
+    for (int ik = 1; ik <= s->nk; ++ik)
+      for (int io = 1; io <= s->no; ++io) {
+        const long o = I.orb(is, io, ik);
+        const double* V = s->V_local + nxy * (is - 1);
+        const double* t = tpsi + 2 * I.vol * o;
+        const double* h = htpsi + 2 * I.vol * o;
+        const double* tt = ttpsi + 2 * I.vol * o;
+        double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+        for (int iz = s->is[2]; iz <= s->ie[2]; ++iz)
+          for (int iy = s->is[1]; iy <= s->ie[1]; ++iy)
+            for (int ix = s->is[0]; ix <= s->ie[0]; ++ix) {
+              const long i = I.a(ix, iy, iz);
+              const double v = V[I.r(ix, iy, iz)];
+              const double tr = t[2 * i], ti = t[2 * i + 1];
+              s0 += tr * h[2 * i] + ti * h[2 * i + 1];
+              s1 += tr * tt[2 * i] + ti * tt[2 * i + 1];
+              const double nr = h[2 * i] - (tt[2 * i] + v * tr), ni = h[2 * i + 1] - (tt[2 * i + 1] + v * ti);
+              s2 += tr * nr + ti * ni;
+            }
+        const double w = s->rocc[(io - 1) + (long)s->no * ((ik - 1) + (long)s->nk * (is - 1))] * s->wtk[ik - 1];
+        esp[(io - 1) + (long)s->no * ((ik - 1) + (long)s->nk * (is - 1))] = s0 * s->hvol;
+        ek += w * s1 * s->hvol;
+        en += w * s->hvol * s2;
+      }
+  e[0] = ek;
+  e[1] = en;
+}
+
 // hpsi, real orbitals: hamiltonian.f90:88-125 (dstencil + dpseudo).
 void sbo_hpsi_real(const sbo_system* s, const double* tpsi, double* htpsi) {
   Idx I(s);

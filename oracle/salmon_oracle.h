@@ -88,6 +88,13 @@ void sbo_zprojections(const sbo_system* s, const double* tpsi, double* uvpsi);
 
 /* hpsi, complex orbitals, orthogonal lattice (hamiltonian.f90:27-235,424-435) */
 void sbo_hpsi(const sbo_system* s, const double* tpsi, double* htpsi);
+/* hpsi with the optional ttpsi: the kinetic part, stencil output minus V psi
+ * before the nonlocal term (hamiltonian.f90:364-414).                           */
+void sbo_hpsi_tt(const sbo_system* s, const double* tpsi, double* htpsi, double* ttpsi);
+/* calc_eigen_energy, complex orbitals (total_energy.f90:505-775):
+ * esp(no,nk,nspin), e[0] = E_kin, e[1] = E_ion_nloc.                            */
+void sbo_calc_eigen_energy(const sbo_system* s, const double* tpsi, double* htpsi, double* ttpsi, double* esp,
+                           double* e);
 /* hpsi, real orbitals (hamiltonian.f90:88-125) */
 void sbo_hpsi_real(const sbo_system* s, const double* tpsi, double* htpsi);
 

@@ -53,6 +53,8 @@ SIGNATURES = {
     "sb200_orbitals_from_ref": (C.c_int, [_vp, _vp, _vp]),
     "sb200_orbitals_to_ref": (C.c_int, [_vp, _vp, _vp]),
     "sb200_hpsi": (C.c_int, [_vp, _vp, _vp]),
+    "sb200_hpsi_tt": (C.c_int, [_vp, _vp, _vp, _vp]),
+    "sb200_calc_eigen_energy": (C.c_int, [_vp, _vp, _vp, _vp, _dp, _dp, _dp]),
     "sb200_taylor": (C.c_int, [_vp, _vp, _vp, _vp, _dp, C.c_int]),
     "sb200_calc_density": (C.c_int, [_vp, _vp, _vp]),
     "sb200_calc_current": (C.c_int, [_vp, _vp, _dp, _dp]),

@@ -774,6 +774,62 @@ int sb200_hpsi(sb200_ctx* c, const double* tpsi, double* htpsi) {
   return SB200_OK;
 }
 
+int sb200_hpsi_tt(sb200_ctx* c, const double* tpsi, double* htpsi, double* ttpsi) {
+  CHECK_CTX(c);
+  TRY(require_ready(c));
+  if (!tpsi || !htpsi || !ttpsi || tpsi == htpsi || tpsi == ttpsi || htpsi == ttpsi)
+    return set_error(SB200_ERR_INVALID_ARG, "tpsi/htpsi/ttpsi null or aliased");
+  TRY(sb200_hpsi(c, tpsi, htpsi));
+  DeviceGuard dg(c->device);
+  TIMED(c, SB200_KIND_HPSI, launch_hpsi_kinetic(c, (const double2*)tpsi, (double2*)ttpsi));
+  return SB200_OK;
+}
+
+int sb200_calc_eigen_energy(sb200_ctx* c, const double* psi, double* htpsi, double* ttpsi, double* esp,
+                            double* e_kin, double* e_nloc) {
+  CHECK_CTX(c);
+  if (!esp || !e_kin || !e_nloc) return set_error(SB200_ERR_INVALID_ARG, "null output pointer");
+  TRY(sb200_hpsi_tt(c, psi, htpsi, ttpsi));
+  DeviceGuard dg(c->device);
+  const int nblk = 32;
+  const int norb = c->orb.norb;
+  double* part = nullptr;
+  TRY(dalloc(&part, (size_t)norb * nblk * 3));
+  int r = launch_energy_parts(c, (const double2*)psi, (const double2*)htpsi, (const double2*)ttpsi, part, nblk);
+  std::vector<double> h((size_t)norb * nblk * 3);
+  if (r == SB200_OK) {
+    cudaError_t e = cudaMemcpyAsync(h.data(), part, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) r = cuda_error(e, "energy partial sums");
+  }
+  dfree(part);
+  TRY(r);
+  TRY(check_device_flag(c));
+  // calc_eigen_energy (total_energy.f90:505-775): per-orbital sums in block
+  // order, then the weighted totals in the reference's (ispin, ik, io) order
+  const int nspin = c->orb.nspin, no = c->orb.no, nk = c->orb.nk;
+  const double hv = c->g.hvol;
+  double ek = 0.0, en = 0.0;
+  for (int is = 0; is < nspin; ++is)
+    for (int ik = 0; ik < nk; ++ik)
+      for (int io = 0; io < no; ++io) {
+        const long o = is + (long)nspin * (io + (long)no * ik);
+        double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+        for (int b = 0; b < nblk; ++b) {
+          s0 += h[(o * nblk + b) * 3 + 0];
+          s1 += h[(o * nblk + b) * 3 + 1];
+          s2 += h[(o * nblk + b) * 3 + 2];
+        }
+        esp[io + (long)no * (ik + (long)nk * is)] = s0 * hv;
+        const double w = c->orb.weight[o];
+        ek += w * s1 * hv;
+        en += w * hv * s2;
+      }
+  *e_kin = ek;
+  *e_nloc = en;
+  return SB200_OK;
+}
+
 int sb200_taylor(sb200_ctx* c, double* tspsi_in, double* tspsi_out, double* sshtpsi, const double* zc, int n_hamil) {
   CHECK_CTX(c);
   TRY(require_ready(c));

@@ -209,6 +209,9 @@ int launch_hpsi_tiled(sb200_ctx* c, const HpsiLaunch& L);  // sb200_stencil.cu
 int launch_hpsi_tma(sb200_ctx* c, const HpsiLaunch& L);
 bool orbital_kernel_applies(const sb200_ctx* c);             // sb200_orbital.cu
 int launch_term_orbital(sb200_ctx* c, const HpsiLaunch& L, bool with_obs);
+int launch_hpsi_kinetic(sb200_ctx* c, const double2* in, double2* tt);       // sb200_kernels.cu
+int launch_energy_parts(sb200_ctx* c, const double2* psi, const double2* h, const double2* tt, double* part,
+                        int nblk);
 bool step_orbital_applies(const sb200_ctx* c, int n_hamil);                  // sb200_orbital.cu
 int launch_step_orbital(sb200_ctx* c, const double2* in, double2* out, const double2* zc, int n_hamil,
                         bool with_obs);

@@ -261,6 +261,10 @@ __global__ void __launch_bounds__(256) k_hpsi(const double2* __restrict__ in, do
   double2 h;
   h.x = vl * c.x + lap0 * c.x - 0.5 * v.x + w.y;
   h.y = vl * c.y + lap0 * c.y - 0.5 * v.y - w.x;
+  if (MODE == 9) {  // ttpsi = htpsi - V_local tpsi before the nonlocal term (hamiltonian.f90:364-414)
+    hout[(long)o * a.npts + p] = make_double2(h.x - vl * c.x, h.y - vl * c.y);
+    return;
+  }
 
   if (a.nlma > 0) {
     const int pm = __ldg(a.pmap + p);
@@ -534,6 +538,78 @@ int launch_project_moments(sb200_ctx* c, const double2* psi) {
   dim3 grid((a.natom + 3) / 4, c->orb.norb);
   k_project_moments<4><<<grid, 128, 0, c->stream>>>(psi, c->d_jw, a);
   SB_LAUNCH_CHECK("k_project_moments");
+  return SB200_OK;
+}
+
+namespace {
+HArgs make_hargs(const sb200_ctx* c, double2 zc) {
+  HArgs a;
+  a.nx = c->g.nx;
+  a.ny = c->g.ny;
+  a.nz = c->g.nz;
+  a.periodic = c->g.periodic;
+  a.nspin = c->orb.nspin;
+  a.nspin_no = c->orb.nspin * c->orb.no;
+  a.nlma = c->pp.nlma;
+  a.nent = c->pp.nent;
+  a.phase_per_k = c->g.periodic;
+  a.npts = c->g.npts;
+  for (int i = 0; i < 12; ++i) a.lapt[i] = c->g.coef_lap[i];
+  a.kcoef = c->d_kcoef;
+  a.vloc = c->d_vloc;
+  a.pmap = c->pp.d_pmap;
+  a.ent_lma = c->pp.d_ent_lma;
+  a.ent_zk = c->pp.d_ent_zk;
+  a.proj = c->d_proj;
+  a.zc = zc;
+  return a;
+}
+
+// per (orbital, block): Re sum conj(psi) h, Re sum conj(psi) tt and
+// Re sum conj(psi) (h - (tt + V psi)), fixed-order tree in shared memory
+__global__ void __launch_bounds__(256) k_energy_part(const double2* __restrict__ psi, const double2* __restrict__ h,
+                                                     const double2* __restrict__ tt, const double* __restrict__ vloc,
+                                                     long npts, int nspin, double* __restrict__ part, int nblk) {
+  __shared__ double r[3][256];
+  const long o = blockIdx.y;
+  const double* V = vloc + (long)(o % nspin) * npts;
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+  for (long p = blockIdx.x * 256L + threadIdx.x; p < npts; p += (long)nblk * 256) {
+    const long i = o * npts + p;
+    const double2 c = psi[i], hv = h[i], tv = tt[i];
+    const double v = V[p];
+    s0 += c.x * hv.x + c.y * hv.y;
+    s1 += c.x * tv.x + c.y * tv.y;
+    s2 += c.x * (hv.x - (tv.x + v * c.x)) + c.y * (hv.y - (tv.y + v * c.y));
+  }
+  r[0][threadIdx.x] = s0;
+  r[1][threadIdx.x] = s1;
+  r[2][threadIdx.x] = s2;
+  __syncthreads();
+  for (int st = 128; st > 0; st >>= 1) {
+    if (threadIdx.x < st)
+      for (int q = 0; q < 3; ++q) r[q][threadIdx.x] += r[q][threadIdx.x + st];
+    __syncthreads();
+  }
+  if (threadIdx.x < 3) part[(o * nblk + blockIdx.x) * 3 + threadIdx.x] = r[threadIdx.x][0];
+}
+}  // namespace
+
+// ttpsi of hpsi (the kinetic part) with the per-point kernel
+int launch_hpsi_kinetic(sb200_ctx* c, const double2* in, double2* tt) {
+  const HArgs a = make_hargs(c, make_double2(0.0, 0.0));
+  dim3 grid((unsigned)((c->g.npts + 255) / 256), c->orb.norb);
+  k_hpsi<9><<<grid, 256, 0, c->stream>>>(in, tt, nullptr, a);
+  SB_LAUNCH_CHECK("k_hpsi(kinetic)");
+  return SB200_OK;
+}
+
+// per-orbital partial energy sums: part[norb][nblk][3]
+int launch_energy_parts(sb200_ctx* c, const double2* psi, const double2* h, const double2* tt, double* part,
+                        int nblk) {
+  dim3 grid(nblk, c->orb.norb);
+  k_energy_part<<<grid, 256, 0, c->stream>>>(psi, h, tt, c->d_vloc, c->g.npts, c->orb.nspin, part, nblk);
+  SB_LAUNCH_CHECK("k_energy_part");
   return SB200_OK;
 }
 

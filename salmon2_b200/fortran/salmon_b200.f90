@@ -116,6 +116,21 @@ module salmon_b200
       type(c_ptr), value :: ctx, tpsi, htpsi
     end function
 
+    ! hpsi with its optional ttpsi (hamiltonian.f90:27,364-414)
+    integer(c_int) function sb200_hpsi_tt(ctx, tpsi, htpsi, ttpsi) bind(c, name="sb200_hpsi_tt")
+      import
+      type(c_ptr), value :: ctx, tpsi, htpsi, ttpsi
+    end function
+
+    ! calc_eigen_energy (total_energy.f90:505): esp(no,nk,nspin), E_kin, E_ion_nloc
+    integer(c_int) function sb200_calc_eigen_energy(ctx, psi, htpsi, ttpsi, esp, e_kin, e_nloc) &
+        bind(c, name="sb200_calc_eigen_energy")
+      import
+      type(c_ptr), value :: ctx, psi, htpsi, ttpsi
+      real(c_double) :: esp(*)
+      real(c_double) :: e_kin, e_nloc
+    end function
+
     ! taylor (taylor.f90:21) on resident device blocks; zc = rt%zc
     integer(c_int) function sb200_taylor(ctx, tspsi_in, tspsi_out, sshtpsi, zc, n_hamil) &
         bind(c, name="sb200_taylor")

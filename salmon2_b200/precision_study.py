@@ -11,8 +11,8 @@ FP64 first term, psi accumulation, density and current) -- and reports:
 * ``norm_drift``: max_t |N_mixed(t) - N_fp64(t)| / N_fp64(0) with N the
   electron count of calc_dip (src/rt/dip.f90:114-225);
 * ``energy_rel_err``: relative difference of the band energy
-  sum_o w_o <psi_o|H|psi_o> hvol of the final orbitals (H psi from sb200_hpsi,
-  the quantity calc_eigen_energy sums, src/common/total_energy.f90:505-775).
+  sum_o w_o <psi_o|H|psi_o> hvol of the final orbitals (esp of
+  sb200_calc_eigen_energy, calc_eigen_energy in src/common/total_energy.f90:505-775).
 
 Usage: ``python -m salmon2_b200.precision_study --nt 4000`` (the 2x2x2
 supercell workload: 32^3 grid, 64 atoms, 8 k-points, 256 orbitals per k).
@@ -33,13 +33,12 @@ import time
 import numpy as np
 
 
-def band_energy(ctx, psi, weight):
-    torch = ctx.torch
-    h = ctx.zeros()
-    ctx.hpsi(psi, h)
-    torch.cuda.synchronize()
-    e = (psi.conj() * h).real.reshape(ctx.sys.norb, -1).sum(1).cpu().numpy() * ctx.sys.grid.hvol
-    return float(np.sum(weight * e))
+def band_energy(ctx, psi):
+    """sum_o rocc wtk esp_o with esp from sb200_calc_eigen_energy."""
+    esp, _, _ = ctx.calc_eigen_energy(psi)
+    s = ctx.sys
+    occ = np.asarray(s.rocc, dtype=np.float64)  # (no, nk, nspin)
+    return float(np.sum(occ * esp * np.asarray(s.wtk)[None, :, None]))
 
 
 def run(system, nt, dt, Ac, zc, precision):
@@ -51,10 +50,7 @@ def run(system, nt, dt, Ac, zc, precision):
     ctx.sync()
     el = time.perf_counter() - t0
     ctx.set_vec_Ac(Ac[:, nt])
-    occ = np.asarray(system.rocc, dtype=np.float64)  # (no, nk, nspin)
-    weight = np.array([occ[io, ik, isp] * system.wtk[ik] for ik in range(system.nk) for io in range(system.no)
-                       for isp in range(system.nspin)])
-    e = band_energy(ctx, res["psi"], weight)
+    e = band_energy(ctx, res["psi"])
     out = dict(curr=res["curr"].copy(), rbox=res["rbox"].copy(), energy=e, seconds=el)
     ctx.close()
     return out

@@ -147,6 +147,23 @@ class Context:
         check(lib().sb200_hpsi(self.h, C.c_void_p(tpsi.data_ptr()), C.c_void_p(htpsi.data_ptr())))
         return htpsi
 
+    def hpsi_tt(self, tpsi, htpsi, ttpsi):
+        """H psi and its kinetic part T psi (hpsi's optional ttpsi)."""
+        check(lib().sb200_hpsi_tt(self.h, C.c_void_p(tpsi.data_ptr()), C.c_void_p(htpsi.data_ptr()),
+                                  C.c_void_p(ttpsi.data_ptr())))
+        return htpsi, ttpsi
+
+    def calc_eigen_energy(self, psi, htpsi=None, ttpsi=None):
+        """(esp(no,nk,nspin), E_kin, E_ion_nloc) of calc_eigen_energy; htpsi and
+        ttpsi are work blocks (allocated when not given)."""
+        htpsi = self.zeros() if htpsi is None else htpsi
+        ttpsi = self.zeros() if ttpsi is None else ttpsi
+        esp = np.zeros((self.sys.no, self.sys.nk, self.sys.nspin), order="F")
+        ek, en = np.zeros(1), np.zeros(1)
+        check(lib().sb200_calc_eigen_energy(self.h, C.c_void_p(psi.data_ptr()), C.c_void_p(htpsi.data_ptr()),
+                                            C.c_void_p(ttpsi.data_ptr()), _ptr(esp), _ptr(ek), _ptr(en)))
+        return esp, float(ek[0]), float(en[0])
+
     def taylor(self, tspsi_in, tspsi_out, sshtpsi, zc):
         z = np.ascontiguousarray(zc, dtype=np.complex128)
         check(lib().sb200_taylor(self.h, C.c_void_p(tspsi_in.data_ptr()), C.c_void_p(tspsi_out.data_ptr()),

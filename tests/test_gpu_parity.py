@@ -60,6 +60,30 @@ def test_hpsi_parity_two_spins():
 
 
 @pytest.mark.parametrize("make", SYSTEMS, ids=lambda f: f.__name__)
+def test_hpsi_tt_and_eigen_energy(make):
+    """hpsi's optional kinetic output ttpsi and calc_eigen_energy (esp,
+    E_kin, E_ion_nloc) against the oracle."""
+    sysm = make()
+    O = Oracle(sysm)
+    ctx = _ctx(sysm)
+    ac = (0.013, -0.004, 0.02)
+    O.set_vec_Ac(ac)
+    ctx.set_vec_Ac(ac)
+    t = ctx.upload(sysm.psi)
+    h, tt = ctx.zeros(), ctx.zeros()
+    ctx.hpsi_tt(t, h, tt)
+    ref_h, ref_tt = O.hpsi_tt(sysm.psi)
+    assert S.rel_err(ctx.download(h), ref_h) < TOL_H
+    assert S.rel_err(ctx.download(tt), ref_tt) < TOL_H
+    esp, ek, en = ctx.calc_eigen_energy(t, h, tt)
+    ref_esp, ref_ek, ref_en = O.calc_eigen_energy(sysm.psi)
+    scale = np.max(np.abs(ref_esp))
+    assert np.max(np.abs(esp - ref_esp)) <= TOL_H * scale
+    assert abs(ek - ref_ek) <= TOL_H * abs(ref_ek)
+    assert abs(en - ref_en) <= TOL_H * max(abs(ref_en), scale)
+
+
+@pytest.mark.parametrize("make", SYSTEMS, ids=lambda f: f.__name__)
 def test_taylor_parity(make):
     from salmon2_b200 import synth
     sysm = make()

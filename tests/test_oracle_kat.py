@@ -159,3 +159,50 @@ def test_pp_tables_inside_grid():
             assert np.all(j >= g.is_[:, None]) and np.all(j <= g.ie[:, None])
         # projectors of each atom are contiguous in ilma (set_lma ordering)
         assert np.all(np.diff(pp.ia_tbl) >= 0)
+
+
+def test_kinetic_part_and_eigen_energy():
+    """hpsi's optional ttpsi (stencil output minus V psi, before the nonlocal
+    term) and calc_eigen_energy: H psi unchanged by asking for ttpsi, H psi =
+    T psi + V psi + KB psi, esp = Re <psi|H|psi> hvol, E_kin and E_ion_nloc
+    the occupation-weighted sums of <psi|T|psi> and <psi|KB|psi>; on a plane
+    wave with V = 0 and no projectors T psi is the finite-difference energy
+    times psi."""
+    s = S.periodic_small()
+    O = Oracle(s)
+    O.set_vec_Ac((0.01, -0.02, 0.015))
+    psi = s.psi
+    h, tt = O.hpsi_tt(psi)
+    assert np.array_equal(h, O.hpsi(psi))
+    sl = s.grid.interior_slices()
+    V = s.V_local
+    nl = O.zpseudo(psi)
+    for io in range(s.no):
+        for ik in range(s.nk):
+            p = psi[sl + (0, io, ik)]
+            rebuilt = tt[sl + (0, io, ik)] + V[..., 0] * p + nl[sl + (0, io, ik)]
+            np.testing.assert_allclose(rebuilt, h[sl + (0, io, ik)], rtol=0,
+                                       atol=1e-12 * np.abs(h[sl + (0, io, ik)]).max())
+    esp, ekin, enl = O.calc_eigen_energy(psi)
+    hv = s.grid.hvol
+    ref_esp = np.zeros_like(esp)
+    ek = en = 0.0
+    for ik in range(s.nk):
+        for io in range(s.no):
+            p = psi[sl + (0, io, ik)]
+            ref_esp[io, ik, 0] = np.real(np.vdot(p, h[sl + (0, io, ik)])) * hv
+            w = s.rocc[io, ik, 0] * s.wtk[ik]
+            ek += w * np.real(np.vdot(p, tt[sl + (0, io, ik)])) * hv
+            en += w * np.real(np.vdot(p, nl[sl + (0, io, ik)])) * hv
+    np.testing.assert_allclose(esp, ref_esp, rtol=1e-12)
+    assert abs(ekin - ek) <= 1e-12 * abs(ek)
+    assert abs(enl - en) <= 1e-10 * max(abs(en), 1e-8)
+    # plane wave: T psi = E_FD psi
+    s2 = plane_wave_system()
+    O2 = Oracle(s2)
+    O2.set_vec_Ac((0.0, 0.0, 0.03))
+    pwv, q = pw(s2.grid, (1, 2, -3))
+    _, tt2 = O2.hpsi_tt(pwv)
+    sl2 = s2.grid.interior_slices() + (0, 0, 0)
+    E = fd_energy(s2.grid, q, s2.vec_k[:, 0] + np.array([0.0, 0.0, 0.03]))
+    np.testing.assert_allclose(tt2[sl2], E * pwv[sl2], rtol=0, atol=1e-13 * np.abs(pwv[sl2]).max() * max(1, abs(E)))

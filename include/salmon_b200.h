@@ -224,6 +224,12 @@ int sb200_gscg(sb200_ctx* ctx, double* psi, int ncg, int precondition, double al
 /* Classical column Gram-Schmidt.
  * Replaces: gram_schmidt_col_real8 (src/gs/gram_schmidt_orth.f90:59-230).          */
 int sb200_gram_schmidt_real(sb200_ctx* ctx, double* psi);
+/* Classical column Gram-Schmidt of complex orbitals, every (k, spin) group of
+ * the resident block (any number of k-points), orbitals in order.
+ * Replaces: gram_schmidt_col_complex8 (src/gs/gram_schmidt_orth.f90:1069-1242),
+ * called on the RT path every gram_schmidt_interval steps
+ * (src/rt/time_evolution_step.f90:154-155).  Synchronous.                       */
+int sb200_gram_schmidt_complex(sb200_ctx* ctx, double* psi);
 /* Subspace diagonalisation (nspin = 1); evals (host, no) ascending.
  * Replaces: ssdg_rwf (src/gs/subspace_diagonalization.f90:62-238) with
  * eigen_dsyev (src/gs/eigen_subdiag_lapack.f90:23-38).                          */

@@ -66,6 +66,7 @@ SIGNATURES = {
     "sb200_hpsi_real": (C.c_int, [_vp, _vp, _vp]),
     "sb200_gscg": (C.c_int, [_vp, _vp, C.c_int, C.c_int, C.c_double, _dp]),
     "sb200_gram_schmidt_real": (C.c_int, [_vp, _vp]),
+    "sb200_gram_schmidt_complex": (C.c_int, [_vp, _vp]),
     "sb200_subspace_diag_real": (C.c_int, [_vp, _vp, _dp]),
     "sb200_learned_init": (C.c_int, [_vp, _vp, C.c_int, C.c_int]),
     "sb200_learned_get_params": (C.c_int, [_vp, _vp, C.c_int]),

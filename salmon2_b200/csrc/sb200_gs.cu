@@ -532,6 +532,93 @@ int gs_precond(sb200_ctx* c, const double* g, double* pre, double alpha) {
 }
 
 // C (m x n, row-major [i][j]) = scale * A(m orbitals) . B(n orbitals)
+// ---- complex column Gram-Schmidt (gram_schmidt_col_complex8) -------------
+// Orbitals io of one (k, spin) group sit `stride` complex values apart.
+// part[io2][b] = sum over the points of block b of conj(psi_io2) psi_io1
+__global__ void __launch_bounds__(RT) k_zgs_dots(const double2* __restrict__ psi, long stride, int io1, long npts,
+                                                 double2* __restrict__ part, int nb) {
+  __shared__ double rr[RT], ri[RT];
+  const int io2 = blockIdx.y;
+  const double2* a = psi + stride * io2;
+  const double2* b = psi + stride * io1;
+  double sr = 0.0, si = 0.0;
+  const long p0 = (long)blockIdx.x * DOT_PTS;
+  for (int it = 0; it < DOT_PTS / RT; ++it) {
+    const long p = p0 + it * RT + threadIdx.x;
+    if (p < npts) {
+      const double2 x = a[p], y = b[p];
+      sr += x.x * y.x + x.y * y.y;
+      si += x.x * y.y - x.y * y.x;
+    }
+  }
+  rr[threadIdx.x] = sr;
+  ri[threadIdx.x] = si;
+  __syncthreads();
+  for (int st = RT / 2; st > 0; st >>= 1) {
+    if (threadIdx.x < st) {
+      rr[threadIdx.x] += rr[threadIdx.x + st];
+      ri[threadIdx.x] += ri[threadIdx.x + st];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) part[(long)io2 * nb + blockIdx.x] = make_double2(rr[0], ri[0]);
+}
+
+// coeff[io2] = hvol * sum_b part[io2][b] (blocks in order)
+__global__ void k_zgs_coeff(const double2* __restrict__ part, int nb, int m, double hvol,
+                            double2* __restrict__ coeff) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  double sr = 0.0, si = 0.0;
+  for (int b = 0; b < nb; ++b) {
+    sr += part[(long)i * nb + b].x;
+    si += part[(long)i * nb + b].y;
+  }
+  coeff[i] = make_double2(sr * hvol, si * hvol);
+}
+
+// psi_io1 <- psi_io1 - sum_{io2 < io1} coeff[io2] psi_io2 (exclusion term
+// accumulated in io2 order, then subtracted)
+__global__ void k_zgs_sub(double2* __restrict__ psi, long stride, int io1, const double2* __restrict__ coeff,
+                          long npts) {
+  for (long p = blockIdx.x * 256L + threadIdx.x; p < npts; p += (long)gridDim.x * 256) {
+    double2 exc = make_double2(0.0, 0.0);
+    for (int io2 = 0; io2 < io1; ++io2) {
+      const double2 cf = coeff[io2], x = psi[stride * io2 + p];
+      exc = make_double2(cf.x * x.x - cf.y * x.y + exc.x, cf.x * x.y + cf.y * x.x + exc.y);
+    }
+    double2* w = psi + stride * io1 + p;
+    *w = make_double2(-exc.x + w->x, -exc.y + w->y);
+  }
+}
+
+// part[b] = sum over block b of |psi|^2
+__global__ void __launch_bounds__(RT) k_zsq_part(const double2* __restrict__ y, long n, double* __restrict__ part) {
+  __shared__ double r[RT];
+  double s = 0.0;
+  const long p0 = (long)blockIdx.x * DOT_PTS;
+  for (int it = 0; it < DOT_PTS / RT; ++it) {
+    const long p = p0 + it * RT + threadIdx.x;
+    if (p < n) s += y[p].x * y[p].x + y[p].y * y[p].y;
+  }
+  r[threadIdx.x] = s;
+  __syncthreads();
+  for (int st = RT / 2; st > 0; st >>= 1) {
+    if (threadIdx.x < st) r[threadIdx.x] += r[threadIdx.x + st];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) part[blockIdx.x] = r[0];
+}
+
+// y <- y / sqrt(hvol * sum_b part[b])
+__global__ void k_zscale_norm(double2* __restrict__ y, long n, const double* __restrict__ part, int nb, double hvol) {
+  double s = 0.0;
+  for (int b = 0; b < nb; ++b) s += part[b];
+  const double sc = 1.0 / sqrt(s * hvol);
+  for (long p = blockIdx.x * 256L + threadIdx.x; p < n; p += (long)gridDim.x * 256)
+    y[p] = make_double2(sc * y[p].x, sc * y[p].y);
+}
+
 int gs_gram(sb200_ctx* c, const double* A, int m, const double* B, int n, double scale, double* C_dev) {
   const long npts = c->g.npts;
   int nb = (int)((npts + 16383) / 16384);
@@ -859,6 +946,47 @@ int sb200_gram_schmidt_real(sb200_ctx* c, double* psi) {
   }
   SB_CUDA(cudaStreamSynchronize(c->stream));
   return SB200_OK;
+}
+
+// gram_schmidt_col_complex8 (gram_schmidt_orth.f90:1069-1242) for every
+// (k, spin) group of the complex orbital block, orbitals in order.
+int sb200_gram_schmidt_complex(sb200_ctx* c, double* psi) {
+  if (!c) return set_error(SB200_ERR_INVALID_ARG, "null ctx");
+  if (!c->g.set || !c->orb.set) return set_error(SB200_ERR_STATE, "sb200_set_grid / _set_orbitals first");
+  if (!psi) return set_error(SB200_ERR_INVALID_ARG, "null psi");
+  DevGuard dg(c->device);
+  const int nspin = c->orb.nspin, no = c->orb.no, nk = c->orb.nk;
+  const long npts = c->g.npts;
+  const int nb = (int)((npts + DOT_PTS - 1) / DOT_PTS);
+  double2* part = nullptr;
+  double2* coeff = nullptr;
+  TRY_GS(dalloc(&part, (size_t)no * nb));
+  int r = dalloc(&coeff, (size_t)no);
+  double2* z = (double2*)psi;
+  const long stride = (long)nspin * npts;
+  for (int ik = 0; ik < nk && r == SB200_OK; ++ik)
+    for (int is = 0; is < nspin && r == SB200_OK; ++is) {
+      double2* base = z + npts * ((long)is + (long)nspin * no * ik);
+      for (int io1 = 0; io1 < no; ++io1) {
+        double2* w1 = base + stride * io1;
+        if (io1 > 0) {
+          k_zgs_dots<<<dim3(nb, io1), RT, 0, c->stream>>>(base, stride, io1, npts, part, nb);
+          k_zgs_coeff<<<(io1 + 127) / 128, 128, 0, c->stream>>>(part, nb, io1, c->g.hvol, coeff);
+          k_zgs_sub<<<gridsz(npts), 256, 0, c->stream>>>(base, stride, io1, coeff, npts);
+        }
+        k_zsq_part<<<nb, RT, 0, c->stream>>>(w1, npts, (double*)part);
+        k_zscale_norm<<<gridsz(npts), 256, 0, c->stream>>>(w1, npts, (const double*)part, nb, c->g.hvol);
+      }
+      const cudaError_t e = cudaGetLastError();
+      if (e != cudaSuccess) r = cuda_error(e, "complex Gram-Schmidt");
+    }
+  if (r == SB200_OK) {
+    const cudaError_t e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) r = cuda_error(e, "complex Gram-Schmidt");
+  }
+  dfree(part);
+  dfree(coeff);
+  return r;
 }
 
 // ssdg_rwf (subspace_diagonalization.f90:62-238): H_sub = <psi_i|H|psi_j>,

@@ -204,6 +204,12 @@ module salmon_b200
       type(c_ptr), value :: ctx, psi
     end function
 
+    ! gram_schmidt_col_complex8 (gram_schmidt_orth.f90:1069); RT path every gram_schmidt_interval steps
+    integer(c_int) function sb200_gram_schmidt_complex(ctx, psi) bind(c, name="sb200_gram_schmidt_complex")
+      import
+      type(c_ptr), value :: ctx, psi
+    end function
+
     integer(c_int) function sb200_subspace_diag_real(ctx, psi, evals) bind(c, name="sb200_subspace_diag_real")
       import
       type(c_ptr), value :: ctx, psi

@@ -238,6 +238,11 @@ class Context:
         check(lib().sb200_gram_schmidt_real(self.h, C.c_void_p(psi.data_ptr())))
         return psi
 
+    def gram_schmidt_complex(self, psi):
+        """Column Gram-Schmidt of the resident complex orbitals, per (k, spin)."""
+        check(lib().sb200_gram_schmidt_complex(self.h, C.c_void_p(psi.data_ptr())))
+        return psi
+
     def subspace_diag_real(self, psi):
         ev = np.zeros(self.sys.no)
         check(lib().sb200_subspace_diag_real(self.h, C.c_void_p(psi.data_ptr()), _ptr(ev)))

@@ -1,6 +1,7 @@
 """GPU parity of the ground-state path (real orbitals) against the oracle:
 real hpsi, the CG eigensolver (with and without the low-pass
-preconditioner), classical Gram-Schmidt and the subspace diagonalisation."""
+preconditioner), classical Gram-Schmidt (real, and complex as the RT path
+calls it) and the subspace diagonalisation."""
 import functools
 
 import numpy as np
@@ -77,3 +78,27 @@ def test_subspace_diag_parity():
     got = ctx.gs_download(psi)
     # eigenvectors are defined up to sign; both sides fix the largest component positive
     assert S.rel_err(got, ref) < 1e-8
+
+
+@pytest.mark.parametrize("make", [S.periodic_small, S.isolated_odd], ids=lambda f: f.__name__)
+def test_gram_schmidt_complex_parity(make):
+    """Complex column Gram-Schmidt (RT path, every (k, spin) group) against the
+    oracle's gram_schmidt_col_complex8, on orbitals mixed to be far from
+    orthonormal; the result is orthonormal in the hvol metric."""
+    s = make()
+    rng = np.random.default_rng(5)
+    psi = s.psi.copy(order="F")
+    no = s.no
+    mix = np.eye(no) + 0.3 * (rng.standard_normal((no, no)) + 1j * rng.standard_normal((no, no)))
+    psi = np.asfortranarray(np.einsum("xyzsok,op->xyzspk", psi, mix))
+    ref = Oracle(s).gram_schmidt_complex(psi)
+    ctx = _ctx(s)
+    d = ctx.upload(psi)
+    ctx.gram_schmidt_complex(d)
+    out = ctx.download(d)
+    assert S.rel_err(out, ref) < 1e-12
+    sl = s.grid.interior_slices()
+    for ik in range(s.nk):
+        for isp in range(s.nspin):
+            X = out[sl + (isp, slice(None), ik)].reshape(-1, no, order="F")
+            np.testing.assert_allclose(X.conj().T @ X * s.grid.hvol, np.eye(no), atol=1e-12)

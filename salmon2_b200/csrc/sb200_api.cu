@@ -123,6 +123,8 @@ void free_pp(PPInfo& p) {
   dfree(p.d_rinv);
   dfree(p.d_map);
   dfree(p.d_vi_start);
+  dfree(p.d_pair_pt);
+  dfree(p.d_apj);
   dfree(p.d_ent_lma);
   dfree(p.d_ent_pt);
   dfree(p.d_ent_uv);
@@ -318,7 +320,8 @@ int sb200_ctx_create(int device, sb200_ctx** out) {
   }
   c->stream = c->own_stream;
   if (const char* v = getenv("SB200_STENCIL")) c->stencil_variant = (v[0] == 'n') ? 0 : 1;
-  if (const char* v = getenv("SB200_ORBITAL")) c->orbital_variant = (v[0] == 'p') ? 1 : (v[0] == 't') ? 0 : 2;
+  if (const char* v = getenv("SB200_ORBITAL"))
+    c->orbital_variant = (v[0] == 'p') ? 1 : (v[0] == 't') ? 0 : (v[0] == 'u') ? 3 : 2;
   if (const char* v = getenv("SB200_TMA")) c->tma_variant = (v[0] == 'o' && v[1] == 'f') ? 0 : 1;
   int r = dalloc(&c->d_result, 16);
   if (r == SB200_OK) r = dalloc(&c->rt.d_step, 1);
@@ -651,10 +654,23 @@ int sb200_set_pp(sb200_ctx* c, int natom, int nps, int nlma, const int* mps, con
     pmap[vi_pt[v]] = (vi_start[v] << 8) | cnt;
   }
   TRY(upload(&p.d_pmap, pmap));
-  // (point, atom) pairs: the entries of a point grouped by atom (ilma ascending)
-  if (npmax <= 4) {
+  // (point, atom) pairs: the entries of a point grouped by atom (ilma
+  // ascending).  A sphere that reaches the same grid point twice (through two
+  // periodic images) has no pair form.
+  bool pair_form = npmax <= 4;
+  for (int v = 0; v < nvi && pair_form; ++v) {
+    int prev_atom = -1, run = 0;
+    for (int e = vi_start[v]; e < vi_start[v + 1]; ++e) {
+      const int at = ia_tbl[ent_lma[e]] - 1;
+      run = (at == prev_atom) ? run + 1 : 1;
+      prev_atom = at;
+      if (run > nproj[at]) pair_form = false;
+    }
+  }
+  if (pair_form) {
     std::vector<int> pmap2(g.npts, -1), pair_lma, pair_fp;
     std::vector<double> pair_uv;
+    std::vector<int> apj(tot > 0 ? tot : 1, -1);
     for (int v = 0; v < nvi; ++v) {
       const int first = (int)pair_lma.size();
       int prev_atom = -1;
@@ -662,6 +678,7 @@ int sb200_set_pp(sb200_ctx* c, int natom, int nps, int nlma, const int* mps, con
         const int at = ia_tbl[ent_lma[e]] - 1;
         if (at == prev_atom) continue;
         prev_atom = at;
+        apj[ent_pt[e]] = (int)pair_lma.size();
         const int fp = ent_pt[e];
         const int j = fp - atom_start[at];
         pair_lma.push_back(lma_start[at] | (nproj[at] << 24));
@@ -674,6 +691,10 @@ int sb200_set_pp(sb200_ctx* c, int natom, int nps, int nlma, const int* mps, con
       pmap2[vi_pt[v]] = (first << 8) | cnt;
     }
     p.npair = (int)pair_lma.size();
+    std::vector<int> pair_pt(pair_fp.size());
+    for (size_t i = 0; i < pair_fp.size(); ++i) pair_pt[i] = pt_lin[pair_fp[i]];
+    TRY(upload(&p.d_pair_pt, pair_pt));
+    TRY(upload(&p.d_apj, apj));
     TRY(upload(&p.d_pmap2, pmap2));
     TRY(upload(&p.d_pair_lma, pair_lma));
     TRY(upload(&p.d_pair_uv, pair_uv));

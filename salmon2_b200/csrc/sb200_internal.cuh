@@ -79,6 +79,8 @@ struct PPInfo {
   double* d_pair_uv = nullptr;  // [npair][4]
   int* d_pair_fp = nullptr;
   double2* d_pair_ph = nullptr; // [nk_phase][npair]
+  int* d_pair_pt = nullptr;     // [npair] grid point of the pair
+  int* d_apj = nullptr;         // [totpts] pair of each flat sphere point
 };
 
 struct RTBuffers {
@@ -142,7 +144,8 @@ struct sb200_ctx {
   size_t stage_bytes = 0;
   bool vloc_set = false;
   int stencil_variant = 1;     // 0: per-point reference kernel, 1: tiled 2.5-D sweep
-  int orbital_variant = 2;     // 16^3 periodic grids: 2 fused Taylor step, 0 one launch per term, 1 persistent per term
+  int orbital_variant = 2;     // 16^3 periodic grids: 2 fused Taylor step (KB tables staged in shared memory
+                               // when they fit), 3 fused without staging, 0 one launch per term, 1 persistent per term
   int tma_variant = 1;         // tiled hpsi fed by tensor copies where it applies (0: register-prefetch sweep)
   // optional per-kernel-class device timing (sb200_set_timing)
   bool timing = false;

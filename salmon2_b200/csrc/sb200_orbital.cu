@@ -307,6 +307,65 @@ __global__ void __launch_bounds__(NT, 2) k_term_orbital(const double2* __restric
 constexpr int NTF = 2 * NP;  // threads of the fused-step CTA
 constexpr int HZ = N / 2;    // planes per thread
 
+// Observables of the new orbital held in shared memory, after the last
+// Taylor term of the fused step: warps 0-7 the local sums over whole columns,
+// warps 8-15 the nonlocal current, as in k_term_orbital.
+__device__ __forceinline__ void step_observables(const double2* __restrict__ accb, const OrbArgs& a, int o, int ik) {
+  const int t = threadIdx.x;
+  const int tx = t & (N - 1), ty = (t >> 4) & (N - 1);
+  __shared__ double red[OBS_NQ][NP / 32];
+  __shared__ double jws[NP / 32][3];
+  const int warp = t >> 5, lane = t & 31;
+  if (t < NP) {
+    const double2* sm = accb;
+    double q[OBS_NQ];
+#pragma unroll
+    for (int i = 0; i < OBS_NQ; ++i) q[i] = 0.0;
+#pragma unroll 4
+    for (int z = 0; z < N; ++z) {
+      const double2 c = sm[z * NP + t];
+      const double r2 = c.x * c.x + c.y * c.y;
+      q[0] += r2;
+      double ix = 0.0, iy = 0.0, iz = 0.0;
+#pragma unroll
+      for (int s = 1; s <= ND; ++s) {
+        const double2 txv = sm[z * NP + ty * N + ((tx + s) & (N - 1))];
+        const double2 tyv = sm[z * NP + (((ty + s) & (N - 1)) << 4) + tx];
+        const double2 tzv = sm[((z + s) & (N - 1)) * NP + t];
+        ix += a.nab[s - 1] * (c.x * txv.y - c.y * txv.x);
+        iy += a.nab[4 + s - 1] * (c.x * tyv.y - c.y * tyv.x);
+        iz += a.nab[8 + s - 1] * (c.x * tzv.y - c.y * tzv.x);
+      }
+      q[1] += ix;
+      q[2] += iy;
+      q[3] += iz;
+      q[4] += ((double)tx + a.off[0]) * r2;
+      q[5] += ((double)ty + a.off[1]) * r2;
+      q[6] += ((double)z + a.off[2]) * r2;
+    }
+#pragma unroll
+    for (int i = 0; i < OBS_NQ; ++i) {
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) q[i] += __shfl_xor_sync(0xffffffffu, q[i], off);
+    }
+    if (lane == 0)
+      for (int i = 0; i < OBS_NQ; ++i) red[i][warp] = q[i];
+  } else if (a.nlma > 0) {
+    current_nonlocal_from_smem<NP / 32>(accb, a, ik, &jws[0][0], warp - NP / 32);
+  }
+  __syncthreads();
+  if (t < OBS_NQ) {
+    double s = 0.0;
+    for (int w = 0; w < NP / 32; ++w) s += red[t][w];
+    a.obs[(long)o * OBS_NQ + t] = s;
+  } else if (t >= 32 && t < 35) {
+    double s = 0.0;
+    if (a.nlma > 0)
+      for (int w = 0; w < NP / 32; ++w) s += jws[w][t - 32];
+    a.jw[3L * o + (t - 32)] = s;
+  }
+}
+
 template <bool OBS>
 __global__ void __launch_bounds__(NTF, 1) k_step_orbital(const double2* __restrict__ in, double2* __restrict__ out,
                                                          OrbArgs a, StepZC zc, int nterm) {
@@ -418,59 +477,187 @@ __global__ void __launch_bounds__(NTF, 1) k_step_orbital(const double2* __restri
     }
   }
   if (!OBS) return;
-  // ---- observables of the new orbital (in accb): warps 0-7 the local sums
-  // over whole columns, warps 8-15 the nonlocal current, as in k_term_orbital
-  __shared__ double red[OBS_NQ][NP / 32];
-  __shared__ double jws[NP / 32][3];
-  const int warp = t >> 5, lane = t & 31;
-  if (t < NP) {
-    const double2* sm = accb;
-    double q[OBS_NQ];
+  step_observables(accb, a, o, ik);
+}
+
+
+// ---------------------------------------------------------------------------
+// Fused Taylor step with the KB tables in shared memory.  The (point, atom)
+// pair tables of the CTA's k-point -- phase exp(i(k+A).r), the uV of the
+// atom's projectors at the point, lma0 | nproj, the grid point -- and the map
+// (atom, sphere point) -> pair are copied into shared memory once per step, so
+// the projections of every term and the scatter read no global tables.  To
+// make room psi_out is kept in registers (eight values per thread) and h_n is
+// re-read from shared memory for the next term's z neighbours.  The scatter
+// sums each atom's projectors first, sum_q uV_q P_q, then multiplies by the
+// conjugate phase (the pair form of the tiled kernels).
+// ---------------------------------------------------------------------------
+template <bool OBS>
+__global__ void __launch_bounds__(NTF, 1) k_step_orbital_st(const double2* __restrict__ in,
+                                                            double2* __restrict__ out, OrbArgs a, StageArgs st,
+                                                            StepZC zc, int nterm) {
+  extern __shared__ double2 smem[];
+  double2* bufs = smem;                            // two whole-orbital buffers
+  double2* Ps = smem + 2 * N * NP;                 // projections of h_{n-1}
+  double2* sph = Ps + a.nlma;                      // [npair] phase
+  double* suv = (double*)(sph + st.npair);         // [npair][4] uV
+  int* slma = (int*)(suv + 4L * st.npair);         // [npair] lma0 | nproj << 24
+  int* spt = slma + st.npair;                      // [npair] grid point
+  int* sapj = spt + st.npair;                      // [totpts] pair of (atom, sphere point)
+  const int o = blockIdx.x;
+  const int t = threadIdx.x;
+  const int col = t & (NP - 1);
+  const int z0 = (t >> 8) * HZ;
+  const int tx = col & (N - 1), ty = col >> 4;
+  const int ik = o / a.nspin_no;
+  const int ispin = o % a.nspin;
+  const double* kc = a.kcoef + (long)KC * ik;
+  const double2* src = in + (long)o * a.npts;
+
+  double2 cv[HZ];
 #pragma unroll
-    for (int i = 0; i < OBS_NQ; ++i) q[i] = 0.0;
-#pragma unroll 4
-    for (int z = 0; z < N; ++z) {
-      const double2 c = sm[z * NP + t];
-      const double r2 = c.x * c.x + c.y * c.y;
-      q[0] += r2;
-      double ix = 0.0, iy = 0.0, iz = 0.0;
-#pragma unroll
-      for (int s = 1; s <= ND; ++s) {
-        const double2 txv = sm[z * NP + ty * N + ((tx + s) & (N - 1))];
-        const double2 tyv = sm[z * NP + (((ty + s) & (N - 1)) << 4) + tx];
-        const double2 tzv = sm[((z + s) & (N - 1)) * NP + t];
-        ix += a.nab[s - 1] * (c.x * txv.y - c.y * txv.x);
-        iy += a.nab[4 + s - 1] * (c.x * tyv.y - c.y * tyv.x);
-        iz += a.nab[8 + s - 1] * (c.x * tzv.y - c.y * tzv.x);
-      }
-      q[1] += ix;
-      q[2] += iy;
-      q[3] += iz;
-      q[4] += ((double)tx + a.off[0]) * r2;
-      q[5] += ((double)ty + a.off[1]) * r2;
-      q[6] += ((double)z + a.off[2]) * r2;
+  for (int j = 0; j < HZ; ++j) cv[j] = __ldg(src + (z0 + j) * NP + col);
+  {
+    const double2* gph = st.pair_ph + (long)ik * st.npair;
+    for (int i = t; i < st.npair; i += NTF) {
+      sph[i] = __ldg(gph + i);
+      const double2* u = (const double2*)(st.pair_uv + 4L * i);
+      ((double2*)suv)[2 * i] = __ldg(u);
+      ((double2*)suv)[2 * i + 1] = __ldg(u + 1);
+      slma[i] = __ldg(st.pair_lma + i);
+      spt[i] = __ldg(st.pair_pt + i);
     }
-#pragma unroll
-    for (int i = 0; i < OBS_NQ; ++i) {
-#pragma unroll
-      for (int off = 16; off > 0; off >>= 1) q[i] += __shfl_xor_sync(0xffffffffu, q[i], off);
-    }
-    if (lane == 0)
-      for (int i = 0; i < OBS_NQ; ++i) red[i][warp] = q[i];
-  } else if (a.nlma > 0) {
-    current_nonlocal_from_smem<NP / 32>(accb, a, ik, &jws[0][0], warp - NP / 32);
+    for (int i = t; i < a.totpts; i += NTF) sapj[i] = __ldg(st.apj + i);
   }
+#pragma unroll
+  for (int j = 0; j < HZ; ++j) bufs[(z0 + j) * NP + col] = cv[j];
   __syncthreads();
-  if (t < OBS_NQ) {
-    double s = 0.0;
-    for (int w = 0; w < NP / 32; ++w) s += red[t][w];
-    a.obs[(long)o * OBS_NQ + t] = s;
-  } else if (t >= 32 && t < 35) {
-    double s = 0.0;
-    if (a.nlma > 0)
-      for (int w = 0; w < NP / 32; ++w) s += jws[w][t - 32];
-    a.jw[3L * o + (t - 32)] = s;
+  const double kx = kc[0], ky = kc[1], kz = kc[2], lap0 = kc[3];
+  int oxp[ND], oxm[ND], oyp[ND], oym[ND];
+#pragma unroll
+  for (int s = 1; s <= ND; ++s) {
+    oxp[s - 1] = ty * N + ((tx + s) & (N - 1));
+    oxm[s - 1] = ty * N + ((tx - s) & (N - 1));
+    oyp[s - 1] = (((ty + s) & (N - 1)) << 4) + tx;
+    oym[s - 1] = (((ty - s) & (N - 1)) << 4) + tx;
   }
+  const double* vloc = a.vloc + (long)ispin * a.npts;
+  double2* odst = out + (long)o * a.npts;
+  const int warp = t >> 5, lane = t & 31;
+  double2 acc[HZ];
+  int b = 0;
+  for (int nn = 0; nn < nterm; ++nn) {
+    const double2* cur = bufs + b * (N * NP);
+    double2* nxt = bufs + (b ^ 1) * (N * NP);
+    if (a.nlma > 0) {  // P(lma) = rinv sum_j uV e^{i(k+A).r_j} h(pt_j): one warp per atom
+      for (int atom = warp; atom < a.natom; atom += NTF / 32) {
+        const int start = __ldg(a.atom_start + atom), m = __ldg(a.mps + atom);
+        const int lma0 = __ldg(a.lma_start + atom), np = __ldg(a.nproj + atom);
+        if (np == 0) continue;  // no projectors: its sphere points have no pairs
+        double2 pq[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) pq[q] = make_double2(0.0, 0.0);
+        for (int j = lane; j < m; j += 32) {
+          const int pr = sapj[start + j];
+          const double2 ev = cmul(sph[pr], cur[spt[pr]]);
+#pragma unroll
+          for (int q = 0; q < 4; ++q)
+            if (q < np) pq[q] = cadd(pq[q], cscal(suv[4 * pr + q], ev));
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+#pragma unroll
+          for (int off = 16; off > 0; off >>= 1) {
+            pq[q].x += __shfl_xor_sync(0xffffffffu, pq[q].x, off);
+            pq[q].y += __shfl_xor_sync(0xffffffffu, pq[q].y, off);
+          }
+        }
+        if (lane == 0) {
+#pragma unroll
+          for (int q = 0; q < 4; ++q)
+            if (q < np) Ps[lma0 + q] = cscal(__ldg(a.rinv + lma0 + q), pq[q]);
+        }
+      }
+      __syncthreads();
+    }
+    const bool last = nn == nterm - 1;
+    const double2 zn = zc.v[nn];
+    const double2* oth = cur + (z0 ^ HZ) * NP + col;  // the other half of this column
+    double vl_n = __ldg(vloc + z0 * NP + col);
+    int pm_n = a.nlma > 0 ? __ldg(st.pmap2 + z0 * NP + col) : -1;
+#pragma unroll
+    for (int j = 0; j < HZ; ++j) {
+      const int z = z0 + j;
+      const double vl = vl_n;
+      const int pm = pm_n;
+      if (j + 1 < HZ) {
+        vl_n = __ldg(vloc + (z + 1) * NP + col);
+        if (a.nlma > 0) pm_n = __ldg(st.pmap2 + (z + 1) * NP + col);
+      }
+      const double2* P = cur + z * NP;
+      double2 vx = make_double2(0.0, 0.0), wx = vx, vy = vx, wy = vx, vz = vx, wz = vx;
+#pragma unroll
+      for (int s = 0; s < ND; ++s) {
+        const double2 tp = P[oxp[s]], tm = P[oxm[s]];
+        vx = cadd(vx, cscal(a.lapt[s], cadd(tp, tm)));
+        wx = cadd(wx, cscal(a.nab[s], csub(tp, tm)));
+      }
+#pragma unroll
+      for (int s = 0; s < ND; ++s) {
+        const double2 tp = P[oyp[s]], tm = P[oym[s]];
+        vy = cadd(vy, cscal(a.lapt[4 + s], cadd(tp, tm)));
+        wy = cadd(wy, cscal(a.nab[4 + s], csub(tp, tm)));
+      }
+#pragma unroll
+      for (int s = 0; s < ND; ++s) {
+        const double2 tp = (j + s + 1 < HZ) ? cv[(j + s + 1) & (HZ - 1)] : oth[(j + s + 1 - HZ) * NP];
+        const double2 tm = (j - s - 1 >= 0) ? cv[(j - s - 1) & (HZ - 1)] : oth[(j - s - 1 + HZ) * NP];
+        vz = cadd(vz, cscal(a.lapt[8 + s], cadd(tp, tm)));
+        wz = cadd(wz, cscal(a.nab[8 + s], csub(tp, tm)));
+      }
+      const double2 v = cadd(vz, cadd(vy, vx));
+      const double2 w = cadd(cscal(kz, wz), cadd(cscal(ky, wy), cscal(kx, wx)));
+      const double2 c = cv[j];
+      const int p = z * NP + col;
+      double2 h;
+      h.x = vl * c.x + lap0 * c.x - 0.5 * v.x + w.y;
+      h.y = vl * c.y + lap0 * c.y - 0.5 * v.y - w.x;
+      if (pm >= 0) {  // (point, atom) pairs of this point, atoms in ilma order
+        const int p1 = (pm >> 8) + (pm & 255);
+        for (int pr = pm >> 8; pr < p1; ++pr) {
+          const int lm = slma[pr];
+          const int l0 = lm & 0xffffff, np = lm >> 24;
+          double2 sp = make_double2(0.0, 0.0);
+#pragma unroll
+          for (int q = 0; q < 4; ++q)
+            if (q < np) {
+              const double u = suv[4 * pr + q];
+              const double2 pv = Ps[l0 + q];
+              sp = make_double2(fma(u, pv.x, sp.x), fma(u, pv.y, sp.y));
+            }
+          const double2 e = sph[pr];
+          h = cadd(h, cmul(make_double2(e.x, -e.y), sp));
+        }
+      }
+      // psi_out = psi + zc_1 h_1 (first term), psi_out + zc_n h_n (later terms)
+      const double2 nv = cadd(nn == 0 ? c : acc[j], cmul(zn, h));
+      acc[j] = nv;
+      if (last) {
+        odst[p] = nv;
+        if (OBS) nxt[p] = nv;  // the new orbital, for the observables
+      } else {
+        nxt[p] = h;
+      }
+    }
+    __syncthreads();  // h_n complete in nxt; reads of cur and Ps done
+    if (!last) {
+#pragma unroll
+      for (int j = 0; j < HZ; ++j) cv[j] = nxt[(z0 + j) * NP + col];
+      b ^= 1;
+    }
+  }
+  if (!OBS) return;
+  step_observables(bufs + (b ^ 1) * (N * NP), a, o, ik);
 }
 
 
@@ -757,18 +944,31 @@ OrbArgs make_orb_args(const sb200_ctx* c, double2 zc, bool with_obs) {
 }  // namespace
 
 bool step_orbital_applies(const sb200_ctx* c, int n_hamil) {
-  return orbital_kernel_applies(c) && c->orbital_variant == 2 && n_hamil >= 1 && n_hamil <= STEP_MAX_NTERM;
+  return orbital_kernel_applies(c) && (c->orbital_variant == 2 || c->orbital_variant == 3) && n_hamil >= 1 &&
+         n_hamil <= STEP_MAX_NTERM;
 }
 
 // One launch for the whole Taylor step: psi_out = sum_n zc_n H^n psi (+ psi).
 int launch_step_orbital(sb200_ctx* c, const double2* in, double2* out, const double2* zc, int n_hamil,
                         bool with_obs) {
-  // dynamic shared memory: three orbital buffers and the projections
+  // dynamic shared memory: three orbital buffers and the projections, or (KB
+  // tables staged) two orbital buffers, the projections and the pair tables
+  constexpr size_t SMEM_MAX = 227 * 1024 - 2048;  // less the static arrays
   const size_t smem = 3 * (size_t)N * NP * sizeof(double2) + (size_t)ORB_MAX_NLMA * sizeof(double2);
+  const PPInfo& pp = c->pp;
+  const size_t smem_st = 2 * (size_t)N * NP * sizeof(double2) + (size_t)pp.nlma * sizeof(double2) +
+                         (size_t)pp.npair * (sizeof(double2) + 4 * sizeof(double) + 2 * sizeof(int)) +
+                         (size_t)pp.totpts * sizeof(int);
+  const bool staged = c->orbital_variant == 2 && pp.nlma > 0 && pp.npair > 0 && pp.d_apj != nullptr &&
+                      smem_st <= SMEM_MAX;
   static bool attr_set = false;
   if (!attr_set) {
     SB_CUDA(cudaFuncSetAttribute(k_step_orbital<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     SB_CUDA(cudaFuncSetAttribute(k_step_orbital<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    SB_CUDA(cudaFuncSetAttribute(k_step_orbital_st<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)SMEM_MAX));
+    SB_CUDA(cudaFuncSetAttribute(k_step_orbital_st<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)SMEM_MAX));
     attr_set = true;
   }
   if (n_hamil < 1 || n_hamil > STEP_MAX_NTERM) return set_error(SB200_ERR_INVALID_ARG, "fused step: bad n_hamil");
@@ -776,6 +976,20 @@ int launch_step_orbital(sb200_ctx* c, const double2* in, double2* out, const dou
   for (int i = 0; i < STEP_MAX_NTERM; ++i) z.v[i] = i < n_hamil ? zc[i] : make_double2(0.0, 0.0);
   const OrbArgs a = make_orb_args(c, zc[0], with_obs);
   dim3 grid(c->orb.norb);
+  if (staged) {
+    StageArgs st;
+    st.npair = pp.npair;
+    st.pair_ph = pp.d_pair_ph;
+    st.pair_uv = pp.d_pair_uv;
+    st.pair_lma = pp.d_pair_lma;
+    st.pair_pt = pp.d_pair_pt;
+    st.apj = pp.d_apj;
+    st.pmap2 = pp.d_pmap2;
+    if (with_obs) k_step_orbital_st<true><<<grid, NTF, smem_st, c->stream>>>(in, out, a, st, z, n_hamil);
+    else k_step_orbital_st<false><<<grid, NTF, smem_st, c->stream>>>(in, out, a, st, z, n_hamil);
+    SB_LAUNCH_CHECK("k_step_orbital_st");
+    return SB200_OK;
+  }
   if (with_obs) k_step_orbital<true><<<grid, NTF, smem, c->stream>>>(in, out, a, z, n_hamil);
   else k_step_orbital<false><<<grid, NTF, smem, c->stream>>>(in, out, a, z, n_hamil);
   SB_LAUNCH_CHECK("k_step_orbital");

@@ -23,6 +23,17 @@ struct OrbArgs {
   double* jw;   // [norb][3] or null
 };
 
+// KB (point, atom) pair tables the fused step stages in shared memory
+struct StageArgs {
+  int npair;
+  const double2* pair_ph;  // [nk][npair] exp(i (k+A).r)
+  const double* pair_uv;   // [npair][4] uV of the atom's projectors
+  const int* pair_lma;     // [npair] lma0 | nproj << 24
+  const int* pair_pt;      // [npair] grid point
+  const int* apj;          // [totpts] flat sphere point -> pair
+  const int* pmap2;        // [npts] (first pair << 8) | count, or -1
+};
+
 constexpr int STEP_MAX_NTERM = 8;  // Taylor terms of the fused step kernel
 struct StepZC {
   double2 v[STEP_MAX_NTERM];  // zc(1..n_hamil)

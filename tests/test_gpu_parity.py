@@ -197,12 +197,13 @@ def test_rt_propagate_periodic16_orbital_kernel(trans):
     assert S.rel_err(ctx.download(res["psi"]), ref["psi"]) < 1e-11
 
 
-@pytest.mark.parametrize("variant", ["fused", "persistent", "terms"])
+@pytest.mark.parametrize("variant", ["fused", "unstaged", "persistent", "terms"])
 def test_rt_propagate_periodic16_many_orbitals(variant, monkeypatch):
     """More orbitals than SMs: the fused-step kernel (all Taylor terms in one
-    launch), the persistent per-term form that walks several orbitals per CTA
-    through double-buffered bulk copies (buffer reuse, barrier phase flips) and
-    the one-launch-per-term form, each against the oracle on the same input."""
+    launch) with its KB tables staged in shared memory and without, the
+    persistent per-term form that walks several orbitals per CTA through
+    double-buffered bulk copies (buffer reuse, barrier phase flips) and the
+    one-launch-per-term form, each against the oracle on the same input."""
     from salmon2_b200 import synth
     monkeypatch.setenv("SB200_ORBITAL", variant)
     sysm = synth.periodic_system(a=10.26, num=16, nkgrid=4, no=5, seed=32, name="periodic16k64")
@@ -221,16 +222,18 @@ def test_rt_propagate_periodic16_many_orbitals(variant, monkeypatch):
 
 @pytest.mark.parametrize("n_hamil", [4, 1, 3])
 def test_fused_step_equals_term_launches(n_hamil, monkeypatch):
-    """The fused Taylor step and the per-term launches do the same arithmetic
-    per point and term: Taylor steps, J(t), the dipole and the orbitals agree
-    bit for bit."""
+    """The fused Taylor step with the global KB tables and the per-term
+    launches do the same arithmetic per point and term: Taylor steps, J(t),
+    the dipole and the orbitals agree bit for bit.  (The default fused form
+    stages the tables in shared memory and sums the scatter by (point, atom)
+    pair; it is checked against the oracle.)"""
     from salmon2_b200 import synth
     sysm = synth.periodic_system(a=10.26, num=16, nkgrid=2, no=3, seed=34, name="periodic16k8")
     zc = synth.taylor_zc(0.08)[:n_hamil]
     nt, dt = 5, 0.08
     Ac = synth.asin2cos(nt, dt, omega=0.05696, f0=0.05696 * 2e-2, tw=nt * dt)
     outs, runs = [], []
-    for variant in ("fused", "terms"):
+    for variant in ("unstaged", "terms"):
         monkeypatch.setenv("SB200_ORBITAL", variant)
         ctx = _ctx(sysm)
         ctx.set_vec_Ac((0.01, -0.02, 0.03))

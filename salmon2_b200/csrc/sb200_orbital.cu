@@ -500,7 +500,7 @@ __global__ void __launch_bounds__(NTF, 1) k_step_orbital_st(const double2* __res
   double2* bufs = smem;                            // two whole-orbital buffers
   double2* Ps = smem + 2 * N * NP;                 // projections of h_{n-1}
   double2* sph = Ps + a.nlma;                      // [npair] phase
-  double* suv = (double*)(sph + st.npair);         // [npair][4] uV
+  double* suv = (double*)(sph + st.npair);         // [4][npair] uV (projector-major: no bank conflicts)
   int* slma = (int*)(suv + 4L * st.npair);         // [npair] lma0 | nproj << 24
   int* spt = slma + st.npair;                      // [npair] grid point
   int* sapj = spt + st.npair;                      // [totpts] pair of (atom, sphere point)
@@ -521,9 +521,12 @@ __global__ void __launch_bounds__(NTF, 1) k_step_orbital_st(const double2* __res
     const double2* gph = st.pair_ph + (long)ik * st.npair;
     for (int i = t; i < st.npair; i += NTF) {
       sph[i] = __ldg(gph + i);
-      const double2* u = (const double2*)(st.pair_uv + 4L * i);
-      ((double2*)suv)[2 * i] = __ldg(u);
-      ((double2*)suv)[2 * i + 1] = __ldg(u + 1);
+      const double2 u01 = __ldg((const double2*)(st.pair_uv + 4L * i));
+      const double2 u23 = __ldg((const double2*)(st.pair_uv + 4L * i + 2));
+      suv[i] = u01.x;
+      suv[st.npair + i] = u01.y;
+      suv[2 * st.npair + i] = u23.x;
+      suv[3 * st.npair + i] = u23.y;
       slma[i] = __ldg(st.pair_lma + i);
       spt[i] = __ldg(st.pair_pt + i);
     }
@@ -562,7 +565,7 @@ __global__ void __launch_bounds__(NTF, 1) k_step_orbital_st(const double2* __res
           const double2 ev = cmul(sph[pr], cur[spt[pr]]);
 #pragma unroll
           for (int q = 0; q < 4; ++q)
-            if (q < np) pq[q] = cadd(pq[q], cscal(suv[4 * pr + q], ev));
+            if (q < np) pq[q] = cadd(pq[q], cscal(suv[q * st.npair + pr], ev));
         }
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
@@ -631,7 +634,7 @@ __global__ void __launch_bounds__(NTF, 1) k_step_orbital_st(const double2* __res
 #pragma unroll
           for (int q = 0; q < 4; ++q)
             if (q < np) {
-              const double u = suv[4 * pr + q];
+              const double u = suv[q * st.npair + pr];
               const double2 pv = Ps[l0 + q];
               sp = make_double2(fma(u, pv.x, sp.x), fma(u, pv.y, sp.y));
             }

@@ -282,7 +282,7 @@ __global__ void __launch_bounds__(NT, 2) k_term_orbital(const double2* __restric
     double s = 0.0;
     for (int w = 0; w < NT / 32; ++w) s += red[t][w];
     a.obs[(long)o * OBS_NQ + t] = s;
-  } else if (t >= 32 && t < 35) {
+  } else if (t >= 32 && t < 35 && a.jw != nullptr) {  // no nonlocal current without projectors
     double s = 0.0;
     if (a.nlma > 0)
       for (int w = 0; w < NT / 32; ++w) s += jws[w][t - 32];
@@ -358,7 +358,7 @@ __device__ __forceinline__ void step_observables(const double2* __restrict__ acc
     double s = 0.0;
     for (int w = 0; w < NP / 32; ++w) s += red[t][w];
     a.obs[(long)o * OBS_NQ + t] = s;
-  } else if (t >= 32 && t < 35) {
+  } else if (t >= 32 && t < 35 && a.jw != nullptr) {  // no nonlocal current without projectors
     double s = 0.0;
     if (a.nlma > 0)
       for (int w = 0; w < NP / 32; ++w) s += jws[w][t - 32];
@@ -808,7 +808,7 @@ __device__ __forceinline__ void observables_smem(const double2* __restrict__ sm,
     double s = 0.0;
     for (int w = 0; w < NT2 / 32; ++w) s += red[t][w];
     a.obs[(long)o * OBS_NQ + t] = s;
-  } else if (t >= 32 && t < 35) {
+  } else if (t >= 32 && t < 35 && a.jw != nullptr) {  // no nonlocal current without projectors
     double s = 0.0;
     if (a.nlma > 0)
       for (int w = 0; w < NT2 / 32; ++w) s += jws[w][t - 32];
@@ -941,7 +941,7 @@ OrbArgs make_orb_args(const sb200_ctx* c, double2 zc, bool with_obs) {
   a.rinv = c->pp.d_rinv;
   a.zc = zc;
   a.obs = with_obs ? c->d_obs : nullptr;
-  a.jw = with_obs ? c->d_jw : nullptr;
+  a.jw = (with_obs && c->pp.nlma > 0) ? c->d_jw : nullptr;  // allocated only with projectors
   return a;
 }
 }  // namespace

@@ -220,6 +220,43 @@ def test_rt_propagate_periodic16_many_orbitals(variant, monkeypatch):
     assert S.rel_err(ctx.download(res["psi"]), ref["psi"]) < 1e-11
 
 
+def _p16_two_spins():
+    from salmon2_b200 import synth
+    return synth.periodic_system(a=10.26, num=16, nkgrid=1, no=2, seed=35, nspin=2, name="p16s2")
+
+
+def _p16_wide_spheres():
+    # rc = 2.0 A: about 860 sphere points per atom, pair tables too large for
+    # shared memory -> the fused step reads the KB tables from global memory
+    from salmon2_b200 import synth
+    return synth.periodic_system(a=10.26, num=16, nkgrid=1, no=2, seed=36, rc_aa=2.0, name="p16wide")
+
+
+def _p16_no_pp():
+    from salmon2_b200 import synth
+    return S.no_pp(synth.periodic_system(a=10.26, num=16, nkgrid=2, no=2, seed=37, name="p16nopp"))
+
+
+@pytest.mark.parametrize("make", [_p16_two_spins, _p16_wide_spheres, _p16_no_pp], ids=lambda f: f.__name__)
+def test_fused_step_variants_against_oracle(make):
+    """The fused 16^3 step on two spins, on projector spheres whose tables do
+    not fit in shared memory (fallback to global tables) and without
+    projectors: J(t), the dipole and psi against the oracle's time loop."""
+    from salmon2_b200 import synth
+    sysm = make()
+    nt, dt = 6, 0.08
+    Ac = synth.asin2cos(nt, dt, omega=0.05696, f0=0.05696 * 2e-2, tw=nt * dt)
+    zc = synth.taylor_zc(dt)
+    ref = Oracle(sysm).rt_run(sysm.psi, nt, dt, zc, Ac_ext=Ac, trans_longi=0)
+    ctx = _ctx(sysm)
+    a, b, w = ctx.upload(sysm.psi), ctx.zeros(), ctx.zeros()
+    res = ctx.rt_propagate(a, b, w, nt, dt, zc, Ac_ext=Ac, trans_longi="tr")
+    jmax = np.max(np.abs(ref["curr"]))
+    assert np.max(np.abs(res["curr"] - ref["curr"])) <= TOL_OBS * max(jmax, 1e-30)
+    assert S.rel_err(res["rbox"], ref["rbox"]) < TOL_OBS
+    assert S.rel_err(ctx.download(res["psi"]), ref["psi"]) < 1e-11
+
+
 @pytest.mark.parametrize("n_hamil", [4, 1, 3])
 def test_fused_step_equals_term_launches(n_hamil, monkeypatch):
     """The fused Taylor step with the global KB tables and the per-term

@@ -257,6 +257,43 @@ def test_fused_step_variants_against_oracle(make):
     assert S.rel_err(ctx.download(res["psi"]), ref["psi"]) < 1e-11
 
 
+def _iso_no_pp():
+    return S.no_pp(S.isolated_small())
+
+
+def _p32_no_pp():
+    return S.no_pp(_periodic32())
+
+
+def _p12_two_spins():
+    return S.periodic_small(nspin=2)
+
+
+@pytest.mark.parametrize("make", [_iso_no_pp, _p32_no_pp, _p12_two_spins], ids=lambda f: f.__name__)
+def test_rt_propagate_edge_systems(make):
+    """The time loop on the tiled / tensor-copy kernels and the separate
+    observables kernels without projectors and with two spins."""
+    from salmon2_b200 import synth
+    sysm = make()
+    nt, dt = 6, 0.05
+    zc = synth.taylor_zc(dt)
+    if sysm.grid.periodic:
+        Ac = synth.asin2cos(nt, dt, omega=0.05696, f0=0.05696 * 2e-2, tw=nt * dt)
+        ref = Oracle(sysm).rt_run(sysm.psi, nt, dt, zc, Ac_ext=Ac, trans_longi=0)
+    else:
+        Ac = None
+        ref = Oracle(sysm).rt_run(sysm.psi, nt, dt, zc)
+    ctx = _ctx(sysm)
+    a, b, w = ctx.upload(sysm.psi), ctx.zeros(), ctx.zeros()
+    res = ctx.rt_propagate(a, b, w, nt, dt, zc, Ac_ext=Ac, trans_longi="tr") if Ac is not None else \
+        ctx.rt_propagate(a, b, w, nt, dt, zc)
+    if sysm.grid.periodic:
+        jmax = np.max(np.abs(ref["curr"]))
+        assert np.max(np.abs(res["curr"] - ref["curr"])) <= TOL_OBS * jmax
+    assert S.rel_err(res["rbox"], ref["rbox"]) < TOL_OBS
+    assert S.rel_err(ctx.download(res["psi"]), ref["psi"]) < 1e-11
+
+
 @pytest.mark.parametrize("n_hamil", [4, 1, 3])
 def test_fused_step_equals_term_launches(n_hamil, monkeypatch):
     """The fused Taylor step with the global KB tables and the per-term

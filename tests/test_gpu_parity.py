@@ -294,6 +294,28 @@ def test_rt_propagate_edge_systems(make):
     assert S.rel_err(ctx.download(res["psi"]), ref["psi"]) < 1e-11
 
 
+@pytest.mark.parametrize("num,a", [(12, 6.0), (16, 6.0)])
+def test_spheres_reaching_a_point_twice(num, a):
+    """Projector spheres wider than half the cell reach some grid points through
+    two periodic images: the (point, atom) pair form does not apply and the
+    kernels take the per-entry scatter (12^3: tiled sweep; 16^3: fused step)."""
+    from salmon2_b200 import synth
+    sysm = synth.periodic_system(a=a, num=num, nkgrid=1, no=2, seed=38, rc_aa=1.8, name="wrap")
+    O = Oracle(sysm)
+    ctx = _ctx(sysm)
+    ac = (0.01, 0.0, -0.02)
+    O.set_vec_Ac(ac)
+    ctx.set_vec_Ac(ac)
+    t = ctx.upload(sysm.psi)
+    h = ctx.zeros()
+    ctx.hpsi(t, h)
+    assert S.rel_err(ctx.download(h), O.hpsi(sysm.psi)) < TOL_H
+    zc = synth.taylor_zc(0.05)
+    out, work = ctx.zeros(), ctx.zeros()
+    ctx.taylor(ctx.upload(sysm.psi), out, work, zc)
+    assert S.rel_err(ctx.download(out), O.taylor(sysm.psi, zc)) < TOL_H
+
+
 @pytest.mark.parametrize("n_hamil", [4, 1, 3])
 def test_fused_step_equals_term_launches(n_hamil, monkeypatch):
     """The fused Taylor step with the global KB tables and the per-term

@@ -136,11 +136,23 @@ int launch_hpsi_tma(sb200_ctx* c, const HpsiLaunch& L) {
   if (rd32 && !make_tma_map(&maps.d32, L.d32, true, g, norb, 2 * TX, TY)) return SB200_ERR_UNSUPPORTED;
   TiledArgs a = make_tiled_args(c, L.zc);
   const int ntiles = ((g.nx + TX - 1) / TX) * ((g.ny + TY - 1) / TY);
-  // z chunks: long sweeps (each chunk re-reads 8 halo planes), split only
-  // until there are about four CTAs per SM
+  // z chunks: the count that minimises waves x planes per CTA (each chunk
+  // re-reads 8 halo planes), with the CTAs that fit on the GPU at once
   const long ctas = (long)ntiles * norb;
+  int sms = 148;
+  SB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
+  const long slots = (long)sms * ((L.mode >= 6) ? 3 : 2);
   int nchunk = 1;
-  while (ctas * nchunk < 148L * 4 && g.nz / (nchunk * 2) >= 16) nchunk *= 2;
+  double best = 0.0;
+  for (int n = 1; n <= 16 && (n == 1 || g.nz / n >= 8); ++n) {
+    const int zc = (g.nz + n - 1) / n;
+    const int nzc_n = (g.nz + zc - 1) / zc;
+    const double cost = (double)((ctas * nzc_n + slots - 1) / slots) * (zc + 2 * HALO);
+    if (n == 1 || cost < best) {
+      best = cost;
+      nchunk = n;
+    }
+  }
   a.zchunk = (g.nz + nchunk - 1) / nchunk;
   const int nzc = (g.nz + a.zchunk - 1) / a.zchunk;
   dim3 grid(ntiles, nzc, norb);

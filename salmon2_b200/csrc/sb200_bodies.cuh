@@ -60,7 +60,8 @@ __device__ __forceinline__ void project_atom(const TIN* __restrict__ in, double2
     double2 acc[NP];
 #pragma unroll
     for (int q = 0; q < NP; ++q) acc[q] = make_double2(0.0, 0.0);
-    for (int j = lane; j < m; j += 32) {
+#pragma unroll 4
+    for (int j = lane; j < m; j += 32) {  // unrolled: the gathers of four iterations in flight
       const TIN vi = __ldg(psi + a.pt_lin[start + j]);
       const double2 v = make_double2((double)vi.x, (double)vi.y);
       const double2 ev = cmul(__ldg(ph + j), v);  // conj(zekr_uV) / uV times psi

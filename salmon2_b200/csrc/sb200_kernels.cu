@@ -107,8 +107,9 @@ __global__ void __launch_bounds__(128) k_project(const TIN* __restrict__ in, dou
 
 // Nonlocal current pieces per (orbital, atom): sum over the atom's projectors
 // of Im(conj(<r_d zekr|psi>) * rinv <zekr|psi>)  (density_matrix.f90:532-591).
+// (at most 128 registers: four CTAs per SM)
 template <int NP>
-__global__ void __launch_bounds__(128, 4) k_project_moments(  // <= 128 registers: four CTAs per SMconst double2* __restrict__ in, double* __restrict__ jw,
+__global__ void __launch_bounds__(128, 4) k_project_moments(const double2* __restrict__ in, double* __restrict__ jw,
                                                          ProjArgs a) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int atom = blockIdx.x * 4 + warp;

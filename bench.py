@@ -125,7 +125,11 @@ class Clocks:
         ids = [v.strip() for v in vis.split(",") if v.strip()]
         self.index = ids[index] if index < len(ids) else str(index)
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+        # the raw samples go to SB200_CLOCKS_DIR (default: the system temp
+        # directory); their summary goes into the JSON line
+        import tempfile
+        self.path = os.path.join(os.environ.get("SB200_CLOCKS_DIR", tempfile.gettempdir()),
+                                 f"clocks_{os.getpid()}.csv")
 
     def __enter__(self):
         try:

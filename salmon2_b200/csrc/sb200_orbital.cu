@@ -1,7 +1,12 @@
-// sb200_orbital.cu -- orbital-resident Taylor-term kernel for small periodic
-// grids (one CTA owns one whole 16^3 orbital).
+// sb200_orbital.cu -- orbital-resident kernels for small periodic grids (one
+// CTA owns one whole 16^3 orbital).  Three forms:
+//   * k_step_orbital_st / k_step_orbital (default): the whole Taylor step of
+//     the orbital in one launch, every term's h kept on the SM (described at
+//     the kernels below);
+//   * k_term_orbital: one launch per Taylor term (described here);
+//   * k_term_orbital_tma: the per-term form with persistent CTAs and bulk copies.
 //
-// Each CTA loads its orbital once from HBM (16 independent 16-byte loads per
+// Per-term form: each CTA loads its orbital once from HBM (16 independent 16-byte loads per
 // thread: a full z column), keeps the column in registers for the z
 // neighbours and all 16 xy planes in shared memory for the x / y neighbours.
 // Because the CTA owns the whole orbital it also computes, from shared memory:

@@ -171,7 +171,7 @@ def eval_loss(ctx, x0, off, tgt, batch=8):
 def evaluate(ctx, psi_ref_layout, tol=1e-8, max_outer=600, ncg=4):
     """Outer iterations and wall time for the low-pass, learned and
     unpreconditioned CG to reach the converged eigenvalues (tightly converged
-    low-pass CG, 1e-12 Ha, as the judge) within `tol` Hartree."""
+    low-pass CG, 1e-12 Ha, as the reference values) within `tol` Hartree."""
     psi = ctx.gs_upload(psi_ref_layout)
     ctx.gram_schmidt_real(psi)
     ref = converge(ctx, psi, tol=1e-12, max_outer=3 * max_outer, precondition="lowpass", ncg=ncg)["evals"]

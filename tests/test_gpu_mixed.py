@@ -1,6 +1,6 @@
 """Mixed-precision form (FP32 Taylor terms n >= 2, FP64 first term and psi
-accumulation) against the FP64 oracle.  The north-star budget is a relative
-error of J(t) <= 1e-6; the tests state the error they measure."""
+accumulation) against the FP64 oracle.  The error budget of the mixed form is
+a relative error of J(t) <= 1e-6; the tests state the error they measure."""
 import numpy as np
 import pytest
 

@@ -299,6 +299,33 @@ int sb200_batch_propagate(sb200_batch* batch, double* const* psi_a, double* cons
                           int nt, double dt, const double* zc, int n_hamil, double* const* rbox_out,
                           double** psi_final);
 
+/* ---- per-step potential update (self-consistent path) ---------------------- *
+ * The three steps time_evolution_step takes after the density when the
+ * functional is not fixed (src/rt/time_evolution_step.f90:184-207): Hartree,
+ * exchange-correlation, update_vlocal.  Density and potentials are interior
+ * arrays (is:ie), x fastest, host or device pointers; all three calls are
+ * synchronous.                                                                 */
+
+/* Vxc(is:ie) and E_xc = hvol * sum rho*eps_xc of the Perdew-Zunger LDA for
+ * nspin = 1 (other nspin: SB200_ERR_UNSUPPORTED).  E_xc may be NULL.
+ * Replaces: exchange_correlation with xc = 'PZ' (src/xc/salmon_xc.f90:58-343,
+ * calc_xc :667-812) -> exc_cor_pz / PZxc (src/xc/builtin_pz.f90:23-83).        */
+int sb200_exc_cor_pz(sb200_ctx* ctx, const double* rho, double* Vxc, double* E_xc);
+
+/* Vh(is:ie) of rho on a periodic grid by separable discrete Fourier transforms
+ * with 4 pi / |G|^2 (G = 0 dropped).  primitive_b(3,3), column j = b_j
+ * (system%primitive_b, host).  Isolated grids: SB200_ERR_UNSUPPORTED.
+ * Replaces: hartree (src/poisson/hartree.f90:20-128) -> poisson_ft
+ * (src/poisson/poisson_periodic.f90:23-242) with fg%coef and the egx/egy/egz
+ * tables of src/common/initialization.f90:632-776.                             */
+int sb200_hartree_periodic(sb200_ctx* ctx, const double primitive_b[9], const double* rho, double* Vh);
+
+/* V_local(is) = Vpsl + Vh + Vxc(is) written into the context's device copy of
+ * V_local (FP64 and the FP32 copy of the mixed form); Vpsl, Vh (is:ie), Vxc
+ * (is:ie, nspin).  Also serves as the first sb200_set_vlocal.
+ * Replaces: update_vlocal (src/common/hamiltonian.f90:813-843).               */
+int sb200_update_vlocal(sb200_ctx* ctx, const double* Vpsl, const double* Vh, const double* Vxc);
+
 /* ---- H psi without device allocation ---------------------------------------- */
 
 /* No counterpart in the reference.  For callers that cannot allocate device

@@ -15,7 +15,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libsalmon_oracle.so")
-_SOURCES = ("salmon_oracle.cpp", "salmon_oracle_gs.cpp", "salmon_oracle.h")
+_SOURCES = ("salmon_oracle.cpp", "salmon_oracle_gs.cpp", "salmon_oracle_scf.cpp", "salmon_oracle.h")
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int)
@@ -59,7 +59,8 @@ def lib():
                      "sbo_calc_density", "sbo_calc_current", "sbo_current_parts", "sbo_calc_dip",
                      "sbo_calc_Ac_ext_t", "sbo_rt_run", "sbo_set_threads", "sbo_get_threads",
                      "sbo_precond_real", "sbo_gscg_rwf", "sbo_gram_schmidt_real", "sbo_gram_schmidt_complex",
-                     "sbo_subspace_diag_real", "sbo_inner_product_real"):
+                     "sbo_subspace_diag_real", "sbo_inner_product_real", "sbo_exc_cor_pz", "sbo_poisson_coef",
+                     "sbo_dft_table", "sbo_poisson_ft", "sbo_update_vlocal"):
             getattr(L, name)
         L.sbo_rt_run.restype = C.c_int
         L.sbo_get_threads.restype = C.c_int
@@ -277,3 +278,56 @@ class Oracle:
         out = np.zeros(self.sys.nspin * self.sys.no)
         lib().sbo_inner_product_real(C.byref(self.s), _p(self._real(x)), _p(self._real(y)), _p(out))
         return out
+
+
+# ---- per-step potential update (salmon_oracle_scf.cpp) ----------------------
+
+def _flat_f(a):
+    """(nx, ny, nz[, ...]) array -> contiguous float64 vector, x fastest."""
+    return np.ascontiguousarray(np.asarray(a, dtype=np.float64).ravel(order="F"))
+
+
+def exc_cor_pz(rho, hvol):
+    """PZ-LDA for nspin = 1 (builtin_pz.f90, salmon_xc.f90:86-254).  rho: (nx, ny, nz)
+    interior, Fortran order.  Returns (Vxc with rho's shape, E_xc)."""
+    r = _flat_f(rho)
+    v = np.zeros_like(r)
+    e = C.c_double(0.0)
+    lib().sbo_exc_cor_pz(C.c_long(r.size), _p(r), C.c_double(hvol), _p(v), C.byref(e))
+    return v.reshape(np.shape(rho), order="F"), e.value
+
+
+def primitive_b_orthogonal(lengths):
+    """Reciprocal primitive vectors 2 pi / L_d of an orthogonal cell, (3,3) with
+    column j = b_j (system%primitive_b)."""
+    return np.diag([2.0 * np.pi / float(L) for L in lengths])
+
+
+def poisson_coef(num, brl):
+    out = np.zeros(int(np.prod(num)))
+    n = np.asarray(num, dtype=np.int32)
+    b = np.ascontiguousarray(np.asarray(brl, dtype=np.float64).ravel(order="F"))
+    lib().sbo_poisson_coef(n.ctypes.data_as(C.POINTER(C.c_int)), _p(b), _p(out))
+    return out
+
+
+def poisson_ft(rho, brl):
+    """Periodic Hartree potential (poisson_ft, poisson_periodic.f90:23-242).
+    rho: (nx, ny, nz) interior, Fortran order; brl: (3,3) primitive_b."""
+    r = _flat_f(rho)
+    v = np.zeros_like(r)
+    n = np.asarray(np.shape(rho), dtype=np.int32)
+    b = np.ascontiguousarray(np.asarray(brl, dtype=np.float64).ravel(order="F"))
+    lib().sbo_poisson_ft(n.ctypes.data_as(C.POINTER(C.c_int)), _p(b), _p(r), _p(v))
+    return v.reshape(np.shape(rho), order="F")
+
+
+def update_vlocal(vpsl, vh, vxc):
+    """update_vlocal (hamiltonian.f90:813-843).  vpsl, vh: (nx, ny, nz);
+    vxc: (nx, ny, nz, nspin).  Returns V_local (nx, ny, nz, nspin)."""
+    vxc = np.asarray(vxc, dtype=np.float64)
+    nspin = vxc.shape[3]
+    a, b, c = _flat_f(vpsl), _flat_f(vh), _flat_f(vxc)
+    out = np.zeros_like(c)
+    lib().sbo_update_vlocal(C.c_long(a.size), C.c_int(nspin), _p(a), _p(b), _p(c), _p(out))
+    return out.reshape(vxc.shape, order="F")

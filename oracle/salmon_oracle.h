@@ -148,6 +148,17 @@ void sbo_gram_schmidt_complex(const sbo_system* s, double* psi);
 void sbo_subspace_diag_real(const sbo_system* s, double* psi, double* work, double* evals);
 void sbo_inner_product_real(const sbo_system* s, const double* x, const double* y, double* out);
 
+/* Per-step potential update (salmon_oracle_scf.cpp): PZ-LDA exchange-correlation
+ * for nspin = 1 (src/xc/builtin_pz.f90, src/xc/salmon_xc.f90:86-254), the
+ * periodic Hartree potential by separable DFTs (poisson_ft,
+ * src/poisson/poisson_periodic.f90:23-242) and update_vlocal
+ * (src/common/hamiltonian.f90:813-843).  Interior arrays, x fastest.           */
+void sbo_exc_cor_pz(long n, const double* rho, double hvol, double* vxc, double* E_xc);
+void sbo_poisson_coef(const int num[3], const double brl[9], double* coef);
+void sbo_dft_table(int n, double* eg);
+void sbo_poisson_ft(const int num[3], const double brl[9], const double* rho, double* vh);
+void sbo_update_vlocal(long n, int nspin, const double* vpsl, const double* vh, const double* vxc, double* vloc);
+
 #ifdef __cplusplus
 }
 #endif

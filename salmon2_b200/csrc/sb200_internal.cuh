@@ -157,6 +157,8 @@ struct sb200_ctx {
   // learned preconditioner (sb200_learned.cu)
   bool learned_set = false;
   void* learned = nullptr;
+  // per-step potential update (sb200_scf.cu)
+  void* scf = nullptr;
 };
 
 namespace sb200 {
@@ -237,5 +239,6 @@ int learned_precond_apply(sb200_ctx* c, const double* g, const double* x, double
 // Y -= X (X^T Y) hvol: components of n orbitals Y along m orthonormal X removed (sb200_gs.cu)
 int gs_project_out(sb200_ctx* c, const double* X, int m, double* Y, int n);
 void learned_free(sb200_ctx* c);
+void scf_free(sb200_ctx* c);
 
 }  // namespace sb200

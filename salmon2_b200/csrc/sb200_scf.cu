@@ -1,0 +1,436 @@
+// sb200_scf.cu -- per-step potential update of the self-consistent RT path:
+// PZ-LDA exchange-correlation (nspin = 1), the periodic Hartree potential and
+// update_vlocal, on the device, so that V_local can follow the density every
+// time step without a host round trip.
+//
+//   sb200_exc_cor_pz        exchange_correlation, xc = 'PZ' (src/xc/salmon_xc.f90:58-343,
+//                           src/xc/builtin_pz.f90:23-83)
+//   sb200_hartree_periodic  hartree -> poisson_ft (src/poisson/hartree.f90:20-128,
+//                           src/poisson/poisson_periodic.f90:23-242)
+//   sb200_update_vlocal     update_vlocal (src/common/hamiltonian.f90:813-843)
+//
+// The Hartree solve keeps the reference's method: separable discrete Fourier
+// transforms with the exp(+-i 2 pi j k / n) tables (forward along z, y, x;
+// division by the number of points and multiplication by 4 pi / |G|^2; inverse
+// along z, y, x; real part).  Each pass is one launch in which a thread forms
+// one output value as the ordered sum over the transformed axis, so the result
+// does not depend on the launch shape.  The grids of this path (16^3 to 128^3)
+// make each pass a few microseconds to tens of microseconds; the tables
+// (3 n^2 complex) and 4 pi / |G|^2 stay resident across steps.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "sb200_internal.cuh"
+
+namespace sb200 {
+namespace {
+
+constexpr double SCF_PI = 3.141592653589793;
+constexpr int SCF_THREADS = 256;
+constexpr int SCF_XC_BLOCKS = 296;  // fixed: the E_xc partial sums have a fixed order
+
+struct ScfState {
+  long npts = 0;
+  int num[3] = {0, 0, 0};
+  double2* d_a = nullptr;     // [npts] complex work
+  double2* d_b = nullptr;     // [npts] complex work
+  double* d_coef = nullptr;   // [npts] 4 pi / |G|^2, x fastest
+  double2* d_tab = nullptr;   // egx [nx][nx], egy [ny][ny], egz [nz][nz]
+  double* d_in = nullptr;     // staging of host inputs: up to (3 + nspin) * npts
+  size_t in_cap = 0;
+  double* d_out = nullptr;    // staging of host outputs: nspin * npts
+  size_t out_cap = 0;
+  double* d_part = nullptr;   // [SCF_XC_BLOCKS + 1]
+  bool have_coef = false;
+  double brl[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+};
+
+ScfState* scf_of(sb200_ctx* c) { return static_cast<ScfState*>(c->scf); }
+
+#define TRY_S(x)                   \
+  do {                             \
+    int _r = (x);                  \
+    if (_r != SB200_OK) return _r; \
+  } while (0)
+
+struct ScfDevGuard {
+  int prev = -1;
+  explicit ScfDevGuard(int dev) {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~ScfDevGuard() {
+    int cur = -1;
+    if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+bool scf_is_device(const void* p) {
+  cudaPointerAttributes at;
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
+}
+
+int scf_ready(sb200_ctx* c) {
+  if (!c) return set_error(SB200_ERR_INVALID_ARG, "null ctx");
+  if (!c->g.set) return set_error(SB200_ERR_STATE, "sb200_set_grid has not been called");
+  if (!c->orb.set) return set_error(SB200_ERR_STATE, "sb200_set_orbitals has not been called");
+  return SB200_OK;
+}
+
+int scf_ensure(sb200_ctx* c) {
+  ScfState* s = scf_of(c);
+  if (s && s->npts == c->g.npts && s->num[0] == c->g.nx && s->num[1] == c->g.ny && s->num[2] == c->g.nz)
+    return SB200_OK;
+  scf_free(c);
+  s = new ScfState();
+  c->scf = s;
+  s->npts = c->g.npts;
+  s->num[0] = c->g.nx;
+  s->num[1] = c->g.ny;
+  s->num[2] = c->g.nz;
+  TRY_S(dalloc(&s->d_part, (size_t)SCF_XC_BLOCKS + 1));
+  return SB200_OK;
+}
+
+int scf_stage_in(sb200_ctx* c, size_t count) {
+  ScfState* s = scf_of(c);
+  if (s->in_cap >= count) return SB200_OK;
+  dfree(s->d_in);
+  s->in_cap = 0;
+  TRY_S(dalloc(&s->d_in, count));
+  s->in_cap = count;
+  return SB200_OK;
+}
+
+int scf_stage_out(sb200_ctx* c, size_t count) {
+  ScfState* s = scf_of(c);
+  if (s->out_cap >= count) return SB200_OK;
+  dfree(s->d_out);
+  s->out_cap = 0;
+  TRY_S(dalloc(&s->d_out, count));
+  s->out_cap = count;
+  return SB200_OK;
+}
+
+// device view of a caller array: the array itself when it is device memory,
+// else a copy in the staging slot
+int scf_input(sb200_ctx* c, const double* p, size_t count, double* slot, const double** dev) {
+  if (scf_is_device(p)) {
+    *dev = p;
+    return SB200_OK;
+  }
+  SB_CUDA(cudaMemcpyAsync(slot, p, count * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  *dev = slot;
+  return SB200_OK;
+}
+
+int scf_grid_blocks(long n) {
+  long b = (n + SCF_THREADS - 1) / SCF_THREADS;
+  const long cap = 148L * 8;
+  if (b > cap) b = cap;
+  return (int)(b < 1 ? 1 : b);
+}
+
+// ---- kernels -----------------------------------------------------------------
+
+// PZxc, src/xc/builtin_pz.f90:51-83 (Perdew-Zunger 1981: Slater exchange and
+// the Ceperley-Alder correlation fit, high-density branch for rs <= 1).
+__device__ __forceinline__ void pzxc_dev(double trho, double cst, double& exc, double& dexc) {
+  const double gammaU = -0.1423, beta1U = 1.0529, beta2U = 0.3334, AU = 0.0311, BU = -0.048, CU = 0.002,
+               DU = -0.0116;
+  const double ttrho = trho + 1e-10;
+  const double rs = pow(3.0 / (4.0 * SCF_PI * ttrho), 1.0 / 3.0);
+  double e = -cst / rs;
+  double de = e / (3.0 * ttrho);
+  if (rs > 1.0) {
+    const double rssq = sqrt(rs);
+    const double den = 1.0 + beta1U * rssq + beta2U * rs;
+    e = e + gammaU / den;
+    de = de + gammaU * (0.5 * beta1U * rssq + beta2U * rs) / (3.0 * ttrho) / (den * den);
+  } else {
+    const double rsln = log(rs);
+    e = e + AU * rsln + BU + CU * rs * rsln + DU * rs;
+    de = de - rs / (3.0 * ttrho) * (AU / rs + CU * (rsln + 1.0) + DU);
+  }
+  exc = e;
+  dexc = de;
+}
+
+// Vxc = e_xc + trho de_xc/drho per point (rho_s = rho/2, trho = 2 rho_s as
+// calc_xc forms them, salmon_xc.f90:778 and builtin_pz.f90:39-44); per-block
+// partial sums of e_xc * trho in a fixed tree order.
+__global__ void __launch_bounds__(SCF_THREADS) k_exc_pz(const double* __restrict__ rho, double* __restrict__ vxc,
+                                                        long n, double cst, double* __restrict__ part) {
+  __shared__ double red[SCF_THREADS];
+  double s = 0.0;
+  for (long i = blockIdx.x * (long)SCF_THREADS + threadIdx.x; i < n; i += (long)gridDim.x * SCF_THREADS) {
+    const double rho_s = rho[i] * 0.5;
+    const double trho = 2.0 * rho_s;
+    double e, de;
+    pzxc_dev(trho, cst, e, de);
+    vxc[i] = e + trho * de;
+    s += e * trho;
+  }
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int st = SCF_THREADS / 2; st > 0; st >>= 1) {
+    if (threadIdx.x < st) red[threadIdx.x] += red[threadIdx.x + st];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) part[blockIdx.x] = red[0];
+}
+
+// E_xc = hvol * sum of the block partials, in block order (one thread).
+__global__ void k_exc_final(double* __restrict__ part, int nblk, double hvol) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    double t = 0.0;
+    for (int b = 0; b < nblk; ++b) t += part[b];
+    part[nblk] = t * hvol;
+  }
+}
+
+// One separable transform pass along `axis` (0 x, 1 y, 2 z):
+//   out(k) = sum_j T(k, j) * in(j)   (sg = -1: the conjugate table)
+// for every line of the grid, x fastest.  in_real: the input is the real array
+// in_real (first forward pass).  coef: the forward x pass ends with
+// coef * (sum / ntot) as poisson_ft does.  out_real: keep the real part (last
+// inverse pass).
+__global__ void __launch_bounds__(SCF_THREADS) k_dft_pass(const double2* __restrict__ in,
+                                                          const double* __restrict__ in_real,
+                                                          double2* __restrict__ out, double* __restrict__ out_real,
+                                                          const double2* __restrict__ T, double sg, int nx, int ny,
+                                                          int nz, int axis, const double* __restrict__ coef,
+                                                          double ntot) {
+  const long npts = (long)nx * ny * nz;
+  for (long p = blockIdx.x * (long)SCF_THREADS + threadIdx.x; p < npts; p += (long)gridDim.x * SCF_THREADS) {
+    const int x = (int)(p % nx);
+    const long r = p / nx;
+    const int y = (int)(r % ny);
+    const int z = (int)(r / ny);
+    int k, n;
+    long stride;
+    if (axis == 0) {
+      k = x;
+      n = nx;
+      stride = 1;
+    } else if (axis == 1) {
+      k = y;
+      n = ny;
+      stride = nx;
+    } else {
+      k = z;
+      n = nz;
+      stride = (long)nx * ny;
+    }
+    const long base = p - (long)k * stride;
+    const double2* Tk = T + (long)k * n;
+    double re = 0.0, im = 0.0;
+    for (int j = 0; j < n; ++j) {
+      const double2 t = Tk[j];
+      const double ti = sg * t.y;
+      double vr, vi;
+      if (in_real) {
+        vr = in_real[base + (long)j * stride];
+        vi = 0.0;
+      } else {
+        const double2 v = in[base + (long)j * stride];
+        vr = v.x;
+        vi = v.y;
+      }
+      re = re + (t.x * vr - ti * vi);
+      im = im + (t.x * vi + ti * vr);
+    }
+    if (coef) {
+      const double cf = coef[p];
+      re = cf * (re / ntot);
+      im = cf * (im / ntot);
+    }
+    if (out_real)
+      out_real[p] = re;
+    else
+      out[p] = make_double2(re, im);
+  }
+}
+
+// V_local(is) = Vpsl + Vh + Vxc(is), FP64 and its FP32 copy.
+__global__ void k_update_vlocal(const double* __restrict__ vpsl, const double* __restrict__ vh,
+                                const double* __restrict__ vxc, double* __restrict__ v, float* __restrict__ v32,
+                                long n, int nspin) {
+  const long tot = n * nspin;
+  for (long i = blockIdx.x * (long)SCF_THREADS + threadIdx.x; i < tot; i += (long)gridDim.x * SCF_THREADS) {
+    const long p = i % n;
+    const double val = vpsl[p] + vh[p] + vxc[i];
+    v[i] = val;
+    v32[i] = (float)val;
+  }
+}
+
+// ---- host tables (the same expressions as initialization.f90:690-776) -------
+
+int fold_index(int m, int n) { return (m - (n + 1) / 2 >= 0) ? m - n : m; }
+
+int scf_tables(sb200_ctx* c, const double brl[9]) {
+  ScfState* s = scf_of(c);
+  const int nx = s->num[0], ny = s->num[1], nz = s->num[2];
+  if (!s->d_tab) {
+    const size_t nt = (size_t)nx * nx + (size_t)ny * ny + (size_t)nz * nz;
+    TRY_S(dalloc(&s->d_tab, nt));
+    std::vector<double2> tab(nt);
+    size_t o = 0;
+    for (int n : {nx, ny, nz}) {
+      for (int k = 0; k < n; ++k)
+        for (int i = 0; i < n; ++i) {
+          const double a = 2.0 * SCF_PI * (double)(i * k) / (double)n;
+          tab[o + (size_t)k * n + i] = make_double2(std::cos(a), std::sin(a));
+        }
+      o += (size_t)n * n;
+    }
+    SB_CUDA(cudaMemcpyAsync(s->d_tab, tab.data(), nt * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
+    SB_CUDA(cudaStreamSynchronize(c->stream));
+  }
+  if (s->have_coef && std::memcmp(s->brl, brl, sizeof(s->brl)) == 0) return SB200_OK;
+  if (!s->d_coef) TRY_S(dalloc(&s->d_coef, (size_t)s->npts));
+  if (!s->d_a) TRY_S(dalloc(&s->d_a, (size_t)s->npts));
+  if (!s->d_b) TRY_S(dalloc(&s->d_b, (size_t)s->npts));
+  std::vector<double> coef((size_t)s->npts);
+  for (int kz = 0; kz < nz; ++kz)
+    for (int ky = 0; ky < ny; ++ky)
+      for (int kx = 0; kx < nx; ++kx) {
+        const long p = kx + (long)nx * (ky + (long)ny * kz);
+        const int iix = fold_index(kx, nx), iiy = fold_index(ky, ny), iiz = fold_index(kz, nz);
+        double g[3];
+        for (int d = 0; d < 3; ++d)
+          g[d] = (double)iix * brl[d + 0] + (double)iiy * brl[d + 3] + (double)iiz * brl[d + 6];
+        const double G2 = g[0] * g[0] + g[1] * g[1] + g[2] * g[2];
+        coef[p] = (kx == 0 && ky == 0 && kz == 0) ? 0.0 : 4.0 * SCF_PI / G2;
+      }
+  SB_CUDA(cudaMemcpyAsync(s->d_coef, coef.data(), coef.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  SB_CUDA(cudaStreamSynchronize(c->stream));
+  std::memcpy(s->brl, brl, sizeof(s->brl));
+  s->have_coef = true;
+  return SB200_OK;
+}
+
+}  // namespace
+
+void scf_free(sb200_ctx* c) {
+  ScfState* s = scf_of(c);
+  if (!s) return;
+  dfree(s->d_a);
+  dfree(s->d_b);
+  dfree(s->d_coef);
+  dfree(s->d_tab);
+  dfree(s->d_in);
+  dfree(s->d_out);
+  dfree(s->d_part);
+  delete s;
+  c->scf = nullptr;
+}
+
+}  // namespace sb200
+
+using namespace sb200;
+
+extern "C" {
+
+int sb200_exc_cor_pz(sb200_ctx* c, const double* rho, double* Vxc, double* E_xc) {
+  TRY_S(scf_ready(c));
+  if (!rho || !Vxc) return set_error(SB200_ERR_INVALID_ARG, "null argument");
+  if (c->orb.nspin != 1)
+    return set_error(SB200_ERR_UNSUPPORTED, "sb200_exc_cor_pz: the PZ functional here is the nspin = 1 form");
+  ScfDevGuard dg(c->device);
+  TRY_S(scf_ensure(c));
+  ScfState* s = scf_of(c);
+  const long n = s->npts;
+  TRY_S(scf_stage_in(c, (size_t)n));
+  const double* d_rho = nullptr;
+  TRY_S(scf_input(c, rho, (size_t)n, s->d_in, &d_rho));
+  const bool out_dev = scf_is_device(Vxc);
+  if (!out_dev) TRY_S(scf_stage_out(c, (size_t)n));
+  double* d_v = out_dev ? Vxc : s->d_out;
+  const double cst = 0.75 * std::pow(3.0 / (2.0 * SCF_PI), 2.0 / 3.0);
+  k_exc_pz<<<SCF_XC_BLOCKS, SCF_THREADS, 0, c->stream>>>(d_rho, d_v, n, cst, s->d_part);
+  k_exc_final<<<1, 32, 0, c->stream>>>(s->d_part, SCF_XC_BLOCKS, c->g.hvol);
+  SB_LAUNCH_CHECK("k_exc_pz");
+  if (!out_dev) SB_CUDA(cudaMemcpyAsync(Vxc, d_v, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  double e = 0.0;
+  SB_CUDA(cudaMemcpyAsync(&e, s->d_part + SCF_XC_BLOCKS, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  SB_CUDA(cudaStreamSynchronize(c->stream));
+  if (E_xc) *E_xc = e;
+  return SB200_OK;
+}
+
+int sb200_hartree_periodic(sb200_ctx* c, const double primitive_b[9], const double* rho, double* Vh) {
+  TRY_S(scf_ready(c));
+  if (!primitive_b || !rho || !Vh) return set_error(SB200_ERR_INVALID_ARG, "null argument");
+  if (!c->g.periodic)
+    return set_error(SB200_ERR_UNSUPPORTED, "sb200_hartree_periodic needs a periodic grid");
+  ScfDevGuard dg(c->device);
+  TRY_S(scf_ensure(c));
+  TRY_S(scf_tables(c, primitive_b));
+  ScfState* s = scf_of(c);
+  const long n = s->npts;
+  const int nx = s->num[0], ny = s->num[1], nz = s->num[2];
+  TRY_S(scf_stage_in(c, (size_t)n));
+  const double* d_rho = nullptr;
+  TRY_S(scf_input(c, rho, (size_t)n, s->d_in, &d_rho));
+  const bool out_dev = scf_is_device(Vh);
+  if (!out_dev) TRY_S(scf_stage_out(c, (size_t)n));
+  double* d_v = out_dev ? Vh : s->d_out;
+  const double2* tx = s->d_tab;
+  const double2* ty = tx + (size_t)nx * nx;
+  const double2* tz = ty + (size_t)ny * ny;
+  const int gb = scf_grid_blocks(n);
+  const double ntot = (double)n;
+  // forward: z, y, x (conjugate tables); the x pass divides by the point count
+  // and multiplies by 4 pi / |G|^2
+  k_dft_pass<<<gb, SCF_THREADS, 0, c->stream>>>(nullptr, d_rho, s->d_a, nullptr, tz, -1.0, nx, ny, nz, 2, nullptr,
+                                                 ntot);
+  k_dft_pass<<<gb, SCF_THREADS, 0, c->stream>>>(s->d_a, nullptr, s->d_b, nullptr, ty, -1.0, nx, ny, nz, 1, nullptr,
+                                                 ntot);
+  k_dft_pass<<<gb, SCF_THREADS, 0, c->stream>>>(s->d_b, nullptr, s->d_a, nullptr, tx, -1.0, nx, ny, nz, 0, s->d_coef,
+                                                 ntot);
+  // inverse: z, y, x; the last pass keeps the real part
+  k_dft_pass<<<gb, SCF_THREADS, 0, c->stream>>>(s->d_a, nullptr, s->d_b, nullptr, tz, 1.0, nx, ny, nz, 2, nullptr,
+                                                 ntot);
+  k_dft_pass<<<gb, SCF_THREADS, 0, c->stream>>>(s->d_b, nullptr, s->d_a, nullptr, ty, 1.0, nx, ny, nz, 1, nullptr,
+                                                 ntot);
+  k_dft_pass<<<gb, SCF_THREADS, 0, c->stream>>>(s->d_a, nullptr, nullptr, d_v, tx, 1.0, nx, ny, nz, 0, nullptr, ntot);
+  SB_LAUNCH_CHECK("k_dft_pass");
+  if (!out_dev) SB_CUDA(cudaMemcpyAsync(Vh, d_v, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  SB_CUDA(cudaStreamSynchronize(c->stream));
+  return SB200_OK;
+}
+
+int sb200_update_vlocal(sb200_ctx* c, const double* Vpsl, const double* Vh, const double* Vxc) {
+  TRY_S(scf_ready(c));
+  if (!Vpsl || !Vh || !Vxc) return set_error(SB200_ERR_INVALID_ARG, "null argument");
+  ScfDevGuard dg(c->device);
+  TRY_S(scf_ensure(c));
+  ScfState* s = scf_of(c);
+  const long n = s->npts;
+  const int nspin = c->orb.nspin;
+  if (!c->d_vloc) TRY_S(dalloc(&c->d_vloc, (size_t)n * nspin));
+  if (!c->d_vloc32) TRY_S(dalloc(&c->d_vloc32, (size_t)n * nspin));
+  TRY_S(scf_stage_in(c, (size_t)n * (2 + nspin)));
+  const double *a = nullptr, *b = nullptr, *x = nullptr;
+  TRY_S(scf_input(c, Vpsl, (size_t)n, s->d_in, &a));
+  TRY_S(scf_input(c, Vh, (size_t)n, s->d_in + n, &b));
+  TRY_S(scf_input(c, Vxc, (size_t)n * nspin, s->d_in + 2 * n, &x));
+  k_update_vlocal<<<scf_grid_blocks(n * nspin), SCF_THREADS, 0, c->stream>>>(a, b, x, c->d_vloc, c->d_vloc32, n,
+                                                                            nspin);
+  SB_LAUNCH_CHECK("k_update_vlocal");
+  SB_CUDA(cudaStreamSynchronize(c->stream));
+  c->vloc_set = true;
+  return SB200_OK;
+}
+
+}  // extern "C"

@@ -168,10 +168,14 @@ def eval_loss(ctx, x0, off, tgt, batch=8):
     return tot / max(1, (n // batch) * batch)
 
 
-def evaluate(ctx, psi_ref_layout, tol=1e-8, max_outer=600, ncg=4):
+def evaluate(ctx, psi_ref_layout, tol=1e-8, max_outer=600, ncg=4, restart_batch=None):
     """Outer iterations and wall time for the low-pass, learned and
     unpreconditioned CG to reach the converged eigenvalues (tightly converged
-    low-pass CG, 1e-12 Ha, as the reference values) within `tol` Hartree."""
+    low-pass CG, 1e-12 Ha, as the reference values) within `tol` Hartree.
+    With ``restart_batch`` (the network's batch) also "lowpass_restart": the
+    learned hook with an all-zero network, i.e. the low-pass direction with the
+    conjugation restarted at every CG iteration as the hook does; the trained
+    weights are restored afterwards."""
     psi = ctx.gs_upload(psi_ref_layout)
     ctx.gram_schmidt_real(psi)
     ref = converge(ctx, psi, tol=1e-12, max_outer=3 * max_outer, precondition="lowpass", ncg=ncg)["evals"]
@@ -182,4 +186,13 @@ def evaluate(ctx, psi_ref_layout, tol=1e-8, max_outer=600, ncg=4):
         r = converge(ctx, psi, tol=tol, max_outer=max_outer, precondition=pre, ncg=ncg, ref=ref)
         out[pre] = dict(outer=r["outer"], seconds=r["seconds"], converged=r["converged"],
                         max_err=float(np.max(np.abs(r["evals"] - ref))))
+    if restart_batch is not None:
+        params = get_params(ctx)
+        init(ctx, restart_batch, None)
+        psi = ctx.gs_upload(psi_ref_layout)
+        ctx.gram_schmidt_real(psi)
+        r = converge(ctx, psi, tol=tol, max_outer=max_outer, precondition="learned", ncg=ncg, ref=ref)
+        out["lowpass_restart"] = dict(outer=r["outer"], seconds=r["seconds"], converged=r["converged"],
+                                      max_err=float(np.max(np.abs(r["evals"] - ref))))
+        init(ctx, restart_batch, params)
     return out

@@ -192,6 +192,65 @@ class Context:
         check(lib().sb200_calc_dip(self.h, p, _ptr(out)))
         return out
 
+    # ---- per-step potential update (time_evolution_step.f90:184-207) ----
+
+    @staticmethod
+    def _scalar_field(a):
+        """(pointer, keep-alive) of an interior field: a numpy array (any order,
+        converted to x fastest) or a contiguous torch device tensor."""
+        if isinstance(a, np.ndarray):
+            f = np.asfortranarray(a, dtype=np.float64)
+            return C.c_void_p(f.ctypes.data), f
+        return C.c_void_p(a.data_ptr()), a
+
+    def exc_cor_pz(self, rho):
+        """exchange_correlation with xc = 'PZ' for nspin = 1 (salmon_xc.f90:58-343):
+        returns (Vxc as an (nx, ny, nz) Fortran-order array, E_xc)."""
+        g = self.sys.grid
+        p, keep = self._scalar_field(rho)
+        v = np.zeros(g.shape, order="F")
+        e = C.c_double(0.0)
+        check(lib().sb200_exc_cor_pz(self.h, p, C.c_void_p(v.ctypes.data), C.byref(e)))
+        return v, e.value
+
+    def hartree_periodic(self, rho, primitive_b):
+        """hartree -> poisson_ft (poisson_periodic.f90:23-242) on a periodic grid;
+        primitive_b (3, 3) with column j = b_j.  Returns Vh (nx, ny, nz)."""
+        g = self.sys.grid
+        b = np.asfortranarray(primitive_b, dtype=np.float64)
+        p, keep = self._scalar_field(rho)
+        v = np.zeros(g.shape, order="F")
+        check(lib().sb200_hartree_periodic(self.h, _ptr(b), p, C.c_void_p(v.ctypes.data)))
+        return v
+
+    def update_vlocal(self, vpsl, vh, vxc):
+        """update_vlocal (hamiltonian.f90:813-843): V_local = Vpsl + Vh + Vxc on the
+        device.  vxc: (nx, ny, nz, nspin) or (nx, ny, nz) for nspin = 1."""
+        pa, ka = self._scalar_field(vpsl)
+        pb, kb = self._scalar_field(vh)
+        pc, kc = self._scalar_field(vxc)
+        check(lib().sb200_update_vlocal(self.h, pa, pb, pc))
+
+    def update_potential(self, psi, vpsl, primitive_b):
+        """The self-consistent part of one time step on the device
+        (time_evolution_step.f90:160-207 for a periodic grid, nspin = 1):
+        rho = calc_density(psi), Vh = hartree(rho), Vxc = exchange_correlation(rho),
+        V_local = Vpsl + Vh + Vxc.  vpsl: a device tensor (nx*ny*nz, x fastest)
+        or a numpy array.  Nothing is copied to the host; returns E_xc."""
+        torch = self.torch
+        n = int(np.prod(self.sys.grid.shape))
+        if getattr(self, "_pot_buf", None) is None:
+            self._pot_buf = torch.empty((3, n), dtype=torch.float64, device=f"cuda:{self.device}")
+        rho, vh, vxc = self._pot_buf
+        b = np.asfortranarray(primitive_b, dtype=np.float64)
+        check(lib().sb200_calc_density(self.h, C.c_void_p(psi.data_ptr()), C.c_void_p(rho.data_ptr())))
+        check(lib().sb200_hartree_periodic(self.h, _ptr(b), C.c_void_p(rho.data_ptr()), C.c_void_p(vh.data_ptr())))
+        e = C.c_double(0.0)
+        check(lib().sb200_exc_cor_pz(self.h, C.c_void_p(rho.data_ptr()), C.c_void_p(vxc.data_ptr()), C.byref(e)))
+        pa, keep = self._scalar_field(vpsl)
+        check(lib().sb200_update_vlocal(self.h, pa, C.c_void_p(vh.data_ptr()), C.c_void_p(vxc.data_ptr())))
+        return e.value
+
     def rt_propagate(self, psi_a, psi_b, work, nt, dt, zc, Ac_ext=None, trans_longi="tr"):
         z = np.ascontiguousarray(zc, dtype=np.complex128)
         ac = None if Ac_ext is None else np.asfortranarray(Ac_ext, dtype=np.float64)

@@ -1,0 +1,171 @@
+"""Per-step potential update on the GPU against the oracle: PZ-LDA
+exchange-correlation, the periodic Hartree potential (separable transforms)
+and update_vlocal, each through the C ABI with host and device arrays, and a
+self-consistent time loop (Taylor step, density, Hartree, XC, V_local every
+step) against the same loop run by the oracle."""
+import ctypes as C
+import dataclasses
+
+import numpy as np
+import pytest
+
+import _systems as S
+import oracle as OR
+from oracle import Oracle
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-12        # relative (max-norm) per call, FP64
+TOL_LOOP = 1e-10   # relative on the density and orbitals after the loop
+
+
+def _brl(system):
+    g = system.grid
+    return OR.primitive_b_orthogonal([n * h for n, h in zip(g.shape, g.hgs)])
+
+
+def _periodic_box(num, h=0.6, no=2):
+    """A periodic system on an arbitrary (non-cubic) grid, without projectors;
+    only its grid is used."""
+    from salmon2_b200 import synth
+    base = S.no_pp(S.periodic_small())
+    g = synth.make_grid(list(num), h, periodic=True)
+    shp = g.shape_array
+    return dataclasses.replace(base, grid=g, no=no, nk=1, vec_k=np.zeros((3, 1), order="F"),
+                               rocc=np.asfortranarray(np.full((no, 1, 1), 2.0)), wtk=np.ones(1),
+                               V_local=np.zeros(tuple(num) + (1,), order="F"),
+                               psi=np.zeros(shp + (1, no, 1), dtype=np.complex128, order="F"),
+                               ngrid=int(np.prod(num)))
+
+
+def _oracle(system):
+    """An oracle with its own copy of V_local (the tests rewrite it in place)."""
+    return Oracle(dataclasses.replace(system, V_local=np.array(system.V_local, order="F")))
+
+
+def test_exc_cor_pz_against_oracle():
+    import torch
+    from salmon2_b200 import _lib
+    from salmon2_b200.rt import Context
+
+    s = S.periodic_small()
+    ctx = Context(s)
+    rho = Oracle(s).density(s.psi)[..., 0]
+    rng = np.random.default_rng(7)
+    wide = np.exp(rng.uniform(np.log(1e-5), np.log(50.0), rho.shape))  # rs from 0.17 to 29
+    for f in (rho, wide):
+        v, e = ctx.exc_cor_pz(f)
+        vr, er = OR.exc_cor_pz(f, s.grid.hvol)
+        assert S.rel_err(v, vr) < TOL
+        assert abs(e - er) <= TOL * abs(er)
+    # device input and output
+    fd = torch.from_numpy(np.ascontiguousarray(wide.ravel(order="F"))).cuda()
+    vd = torch.empty_like(fd)
+    e = C.c_double(0.0)
+    _lib.check(_lib.lib().sb200_exc_cor_pz(ctx.h, C.c_void_p(fd.data_ptr()), C.c_void_p(vd.data_ptr()),
+                                           C.byref(e)))
+    vr, er = OR.exc_cor_pz(wide, s.grid.hvol)
+    assert S.rel_err(vd.cpu().numpy(), vr.ravel(order="F")) < TOL
+    assert abs(e.value - er) <= TOL * abs(er)
+    ctx.close()
+
+
+@pytest.mark.parametrize("num", [(12, 12, 12), (16, 16, 16), (12, 16, 20), (15, 9, 10)])
+def test_hartree_periodic_against_oracle(num):
+    import torch
+    from salmon2_b200 import _lib
+    from salmon2_b200.rt import Context
+
+    s = S.periodic_small() if num == (12, 12, 12) else _periodic_box(num)
+    ctx = Context(s)
+    brl = _brl(s)
+    rng = np.random.default_rng(sum(num))
+    rho = rng.uniform(0.0, 0.2, tuple(num))
+    vh = ctx.hartree_periodic(rho, brl)
+    ref = OR.poisson_ft(rho, brl)
+    assert S.rel_err(vh, ref) < TOL
+    # a second call with another cell reuses the transform tables and rebuilds 4 pi / |G|^2
+    brl2 = 1.1 * brl
+    assert S.rel_err(ctx.hartree_periodic(rho, brl2), OR.poisson_ft(rho, brl2)) < TOL
+    # device arrays
+    rd = torch.from_numpy(np.ascontiguousarray(rho.ravel(order="F"))).cuda()
+    vd = torch.empty_like(rd)
+    b = np.asfortranarray(brl)
+    _lib.check(_lib.lib().sb200_hartree_periodic(ctx.h, b.ctypes.data_as(C.POINTER(C.c_double)),
+                                                 C.c_void_p(rd.data_ptr()), C.c_void_p(vd.data_ptr())))
+    assert S.rel_err(vd.cpu().numpy(), ref.ravel(order="F")) < TOL
+    ctx.close()
+
+
+def test_hartree_needs_a_periodic_grid():
+    from salmon2_b200.rt import Context, SB200Error
+
+    s = S.isolated_small()
+    ctx = Context(s)
+    with pytest.raises(SB200Error):
+        ctx.hartree_periodic(np.zeros(s.grid.shape), np.eye(3))
+    ctx.close()
+
+
+def test_update_vlocal_feeds_hpsi():
+    """After update_vlocal the context's H uses the new potential: H psi
+    matches the oracle's H psi with V_local = Vpsl + Vh + Vxc."""
+    from salmon2_b200.rt import Context
+
+    s = S.periodic_c2_like()
+    O = _oracle(s)
+    ctx = Context(s)
+    rng = np.random.default_rng(8)
+    shp = s.grid.shape
+    vpsl = s.V_local[..., 0]
+    vh, vxc = rng.standard_normal(shp), rng.standard_normal(shp)
+    ctx.update_vlocal(vpsl, vh, vxc)
+    O.V[...] = OR.update_vlocal(vpsl, vh, vxc[..., None])
+    psi = ctx.upload(s.psi)
+    h = ctx.zeros()
+    ctx.hpsi(psi, h)
+    assert S.rel_err(ctx.download(h), O.hpsi(s.psi)) < TOL
+    ctx.close()
+
+
+def test_self_consistent_time_loop_against_oracle():
+    """Four steps of the self-consistent loop of time_evolution_step
+    (taylor, calc_density, hartree, exchange_correlation, update_vlocal), with
+    the fixed Gaussian local potential standing in for Vpsl: on the GPU through
+    Context.update_potential (device arrays only), on the CPU by the oracle."""
+    import torch
+    from salmon2_b200 import synth
+    from salmon2_b200.rt import Context
+
+    s = S.periodic_small()
+    O = _oracle(s)
+    ctx = Context(s)
+    brl = _brl(s)
+    zc = synth.taylor_zc(0.05)
+    vpsl = np.array(s.V_local[..., 0])
+    vpsl_dev = torch.from_numpy(np.ascontiguousarray(vpsl.ravel(order="F"))).cuda()
+    a = ctx.upload(s.psi)
+    out, work = ctx.zeros(), ctx.zeros()
+    psi_ref = s.psi
+    for step in range(4):
+        ctx.taylor(a, out, work, zc)
+        a, out = out, a
+        exc = ctx.update_potential(a, vpsl_dev, brl)
+        rho = ctx._pot_buf[0].cpu().numpy().reshape(s.grid.shape, order="F")
+
+        psi_ref = O.taylor(psi_ref, zc)
+        rho_ref = O.density(psi_ref)[..., 0]
+        vh_ref = OR.poisson_ft(rho_ref, brl)
+        vxc_ref, exc_ref = OR.exc_cor_pz(rho_ref, s.grid.hvol)
+        O.V[...] = OR.update_vlocal(vpsl, vh_ref, vxc_ref[..., None])
+
+        assert S.rel_err(rho, rho_ref) < TOL_LOOP, step
+        assert abs(exc - exc_ref) <= TOL_LOOP * abs(exc_ref), step
+    assert S.rel_err(ctx.download(a), psi_ref) < TOL_LOOP
+    # the potential the next step would use, through the host path of each call
+    rho_h = ctx.calc_density(a)[..., 0]
+    vh_h = ctx.hartree_periodic(rho_h, brl)
+    vxc_h, _ = ctx.exc_cor_pz(rho_h)
+    assert S.rel_err(vh_h, OR.poisson_ft(rho_ref, brl)) < TOL_LOOP
+    assert S.rel_err(vxc_h, vxc_ref) < TOL_LOOP
+    ctx.close()

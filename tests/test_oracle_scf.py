@@ -1,0 +1,119 @@
+"""Known-answer tests of the oracle's per-step potential update (CPU):
+the PZ-LDA exchange-correlation against the published Perdew-Zunger (1981)
+parametrisation restated independently in numpy, the potential as the density
+derivative of the energy, and the periodic Poisson solver on sampled plane
+waves (exact for the discrete transform), neutrality and symmetry."""
+import numpy as np
+import pytest
+
+import oracle as O
+
+# Perdew & Zunger, Phys. Rev. B 23, 5048 (1981), unpolarised fit (Hartree):
+# rs >= 1: gamma / (1 + beta1 sqrt(rs) + beta2 rs); rs < 1: A ln rs + B + C rs ln rs + D rs
+PZ = dict(gamma=-0.1423, beta1=1.0529, beta2=0.3334, A=0.0311, B=-0.048, C=0.0020, D=-0.0116)
+# Slater exchange energy per electron of the uniform gas: -(3/4) (3 rho / pi)^(1/3)
+
+
+def eps_xc_published(rho):
+    rho = np.asarray(rho, dtype=np.float64) + 1e-10  # the reference's regulariser
+    rs = (3.0 / (4.0 * np.pi * rho)) ** (1.0 / 3.0)
+    ex = -0.75 * (3.0 * rho / np.pi) ** (1.0 / 3.0)
+    hi = PZ["gamma"] / (1.0 + PZ["beta1"] * np.sqrt(rs) + PZ["beta2"] * rs)
+    lo = PZ["A"] * np.log(rs) + PZ["B"] + PZ["C"] * rs * np.log(rs) + PZ["D"] * rs
+    return ex + np.where(rs > 1.0, hi, lo)
+
+
+def test_pz_energy_matches_published_fit():
+    # densities from rs = 0.2 to rs = 20, both branches and rs = 1 itself
+    rs = np.concatenate([np.geomspace(0.2, 20.0, 61), [1.0]])
+    rho = 3.0 / (4.0 * np.pi * rs ** 3)
+    hvol = 0.37
+    field = rho.reshape(62, 1, 1)
+    v, E = O.exc_cor_pz(field, hvol)
+    want = hvol * np.sum(rho * eps_xc_published(rho))
+    assert abs(E - want) <= 1e-13 * abs(want)
+    # per point: E of a one-point field is hvol * rho * eps_xc
+    for r in rho[::7]:
+        _, e1 = O.exc_cor_pz(np.full((1, 1, 1), r), 1.0)
+        assert abs(e1 - r * eps_xc_published(r)) <= 1e-13 * abs(e1)
+
+
+def test_pz_branches_meet_at_rs_one():
+    # the fit is built continuous at rs = 1 (to the precision of its printed
+    # constants): both branches agree to a few 1e-5 Ha
+    hi = PZ["gamma"] / (1.0 + PZ["beta1"] + PZ["beta2"])
+    lo = PZ["B"] + PZ["D"]
+    assert abs(hi - lo) < 1e-4
+    rho1 = 3.0 / (4.0 * np.pi)
+    eps = 1e-7
+    _, ea = O.exc_cor_pz(np.full((1, 1, 1), rho1 * (1 + eps)), 1.0)
+    _, eb = O.exc_cor_pz(np.full((1, 1, 1), rho1 * (1 - eps)), 1.0)
+    assert abs(ea / (rho1 * (1 + eps)) - eb / (rho1 * (1 - eps))) < 1e-4
+
+
+@pytest.mark.parametrize("rs", [0.3, 0.7, 1.5, 4.0, 12.0])
+def test_pz_potential_is_energy_derivative(rs):
+    """Vxc = d(rho eps_xc)/d rho: central differences of E_xc in rho."""
+    rho = 3.0 / (4.0 * np.pi * rs ** 3)
+    v, _ = O.exc_cor_pz(np.full((1, 1, 1), rho), 1.0)
+    h = 1e-5 * rho
+    _, ep = O.exc_cor_pz(np.full((1, 1, 1), rho + h), 1.0)
+    _, em = O.exc_cor_pz(np.full((1, 1, 1), rho - h), 1.0)
+    fd = (ep - em) / (2 * h)
+    assert abs(v.ravel()[0] - fd) <= 1e-7 * abs(fd)
+
+
+def _grid(num, h):
+    L = [n * h for n in num]
+    xs = [np.arange(n) * h for n in num]
+    X, Y, Z = np.meshgrid(*xs, indexing="ij")
+    return L, X, Y, Z
+
+
+@pytest.mark.parametrize("num,m", [((12, 12, 12), (1, 0, 0)), ((12, 16, 20), (2, -1, 3)),
+                                   ((15, 10, 9), (-7, 4, 4)), ((16, 16, 16), (8, 0, 1))])
+def test_poisson_sampled_plane_wave(num, m):
+    """cos and sin of G.r sampled on the grid are eigenvectors of the
+    discrete transform: Vh = 4 pi / |G|^2 times the density."""
+    L, X, Y, Z = _grid(num, 0.55)
+    brl = O.primitive_b_orthogonal(L)
+    G = [2 * np.pi * mi / Li for mi, Li in zip(m, L)]
+    ph = G[0] * X + G[1] * Y + G[2] * Z
+    G2 = sum(g * g for g in G)
+    for rho in (np.cos(ph), np.sin(ph)):
+        vh = O.poisson_ft(rho, brl)
+        want = 4 * np.pi / G2 * rho
+        assert np.max(np.abs(vh - want)) <= 1e-12 * np.max(np.abs(want)) + 1e-14
+
+
+def test_poisson_neutral_linear_symmetric():
+    num = (12, 14, 10)
+    L, X, Y, Z = _grid(num, 0.6)
+    brl = O.primitive_b_orthogonal(L)
+    rng = np.random.default_rng(5)
+    # the G = 0 term is dropped: a uniform density has no potential
+    assert np.max(np.abs(O.poisson_ft(np.full(num, 0.3), brl))) < 1e-14
+    r1 = rng.standard_normal(num)
+    r2 = rng.standard_normal(num)
+    v1, v2 = O.poisson_ft(r1, brl), O.poisson_ft(r2, brl)
+    v12 = O.poisson_ft(r1 + 2.0 * r2, brl)
+    assert np.max(np.abs(v12 - (v1 + 2.0 * v2))) <= 1e-12 * np.max(np.abs(v12))
+    # the Coulomb kernel is symmetric and positive
+    s12, s21 = np.sum(r1 * v2), np.sum(r2 * v1)
+    assert abs(s12 - s21) <= 1e-12 * (abs(s12) + np.sum(np.abs(r1 * v2)))
+    assert np.sum(r1 * v1) > 0
+    # the coefficient table: 4 pi / |G|^2 with folded indices, zero at G = 0
+    coef = O.poisson_coef(num, brl).reshape(num, order="F")
+    assert coef[0, 0, 0] == 0.0
+    kx = np.fft.fftfreq(num[0], d=1.0 / num[0])
+    assert np.isclose(coef[num[0] - 1, 0, 0], 4 * np.pi / (2 * np.pi * kx[-1] / L[0]) ** 2, rtol=1e-14)
+
+
+def test_update_vlocal_is_the_sum():
+    rng = np.random.default_rng(6)
+    num = (5, 6, 7)
+    vpsl, vh = rng.standard_normal(num), rng.standard_normal(num)
+    vxc = rng.standard_normal(num + (2,))
+    v = O.update_vlocal(vpsl, vh, vxc)
+    for s in range(2):
+        assert np.array_equal(v[..., s], (vpsl + vh) + vxc[..., s])

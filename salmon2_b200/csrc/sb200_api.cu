@@ -351,6 +351,7 @@ int sb200_ctx_destroy(sb200_ctx* c) {
   dfree(c->d_jw);
   dfree(c->d_obs);
   dfree(c->d_obs1);
+  dfree(c->d_rho_part);
   dfree(c->d_result);
   dfree(c->rt.d_Ac_ext);
   dfree(c->rt.d_Ac_ind);

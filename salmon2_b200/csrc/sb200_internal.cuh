@@ -140,6 +140,8 @@ struct sb200_ctx {
   double* d_result = nullptr;   // small result area (8 doubles)
   int* d_err = nullptr;         // device error flag: a bounded wait expired
   int obs_blocks = 0;
+  double* d_rho_part = nullptr; // [chunk][nspin][npts] density partial sums (calc_density)
+  size_t rho_part_cap = 0;
   void* d_stage = nullptr;      // relayout staging
   size_t stage_bytes = 0;
   bool vloc_set = false;

@@ -397,19 +397,33 @@ __global__ void __launch_bounds__(256) k_collapse(const double* __restrict__ par
 }
 
 // rho(p, ispin) = sum_{ik, io} w |psi|^2 (density_matrix.f90:150-232)
-__global__ void k_density(const double2* __restrict__ in, double* __restrict__ rho, long npts, int nspin,
-                          int no, int nk, const double* __restrict__ weight) {
+// rho of one chunk of (io, ik) orbitals per spin, rocc*wtk weighted, in the
+// reference's order within the chunk (ik outer, io inner).  With one chunk the
+// result goes straight to rho; with several, part[chunk][is][p] holds the chunk
+// sums and k_density_sum adds them in chunk order.  The chunk count depends only
+// on the grid and orbital counts, so the summation order is fixed.
+__global__ void k_density(const double2* __restrict__ in, double* __restrict__ out, long npts, int nspin,
+                          int nos, int nper, const double* __restrict__ weight) {
   const long p = blockIdx.x * (long)blockDim.x + threadIdx.x;
   if (p >= npts) return;
+  const int j0 = blockIdx.y * nper;
+  const int j1 = min(nos, j0 + nper);
   for (int is = 0; is < nspin; ++is) {
     double acc = 0.0;
-    for (int ik = 0; ik < nk; ++ik)
-      for (int io = 0; io < no; ++io) {
-        const long o = is + (long)nspin * (io + (long)no * ik);
-        const double2 c = __ldg(in + o * npts + p);
-        acc += (c.x * c.x + c.y * c.y) * weight[o];
-      }
-    rho[(long)is * npts + p] = acc;
+    for (int j = j0; j < j1; ++j) {  // j = io + no * ik
+      const long o = is + (long)nspin * j;
+      const double2 c = __ldg(in + o * npts + p);
+      acc += (c.x * c.x + c.y * c.y) * weight[o];
+    }
+    out[((long)blockIdx.y * nspin + is) * npts + p] = acc;
+  }
+}
+
+__global__ void k_density_sum(const double* __restrict__ part, double* __restrict__ rho, long n, int nchunk) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    double acc = 0.0;
+    for (int c = 0; c < nchunk; ++c) acc += part[(long)c * n + i];
+    rho[i] = acc;
   }
 }
 
@@ -760,8 +774,34 @@ int launch_finalize(sb200_ctx* c, int itt, int nt, int trans_longi, double dt, i
 
 int launch_density(sb200_ctx* c, const double2* psi, double* rho) {
   const long n = c->g.npts;
-  k_density<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(psi, rho, n, c->orb.nspin, c->orb.no, c->orb.nk,
-                                                               c->d_weight);
+  const int nspin = c->orb.nspin;
+  const int nos = c->orb.no * c->orb.nk;
+  const long pblocks = (n + 255) / 256;
+  // enough (point block, orbital chunk) pairs for about eight blocks per SM,
+  // with at least eight orbitals per chunk
+  long nchunk = (148L * 8 + pblocks - 1) / pblocks;
+  const long cap = (nos + 7) / 8;
+  if (nchunk > cap) nchunk = cap;
+  if (nchunk < 1) nchunk = 1;
+  const int nper = (int)((nos + nchunk - 1) / nchunk);
+  nchunk = (nos + nper - 1) / nper;
+  if (nchunk <= 1) {
+    k_density<<<dim3((unsigned)pblocks, 1), 256, 0, c->stream>>>(psi, rho, n, nspin, nos, nos, c->d_weight);
+    SB_LAUNCH_CHECK("k_density");
+    return SB200_OK;
+  }
+  const size_t need = (size_t)nchunk * nspin * n;
+  if (c->rho_part_cap < need) {
+    dfree(c->d_rho_part);
+    c->rho_part_cap = 0;
+    if (dalloc(&c->d_rho_part, need)) return SB200_ERR_OOM;
+    c->rho_part_cap = need;
+  }
+  k_density<<<dim3((unsigned)pblocks, (unsigned)nchunk), 256, 0, c->stream>>>(psi, c->d_rho_part, n, nspin, nos,
+                                                                             nper, c->d_weight);
+  long sblocks = (n * nspin + 255) / 256;
+  if (sblocks > 148L * 8) sblocks = 148L * 8;
+  k_density_sum<<<(unsigned)sblocks, 256, 0, c->stream>>>(c->d_rho_part, rho, n * nspin, (int)nchunk);
   SB_LAUNCH_CHECK("k_density");
   return SB200_OK;
 }

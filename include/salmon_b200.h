@@ -326,6 +326,19 @@ int sb200_hartree_periodic(sb200_ctx* ctx, const double primitive_b[9], const do
  * Replaces: update_vlocal (src/common/hamiltonian.f90:813-843).               */
 int sb200_update_vlocal(sb200_ctx* ctx, const double* Vpsl, const double* Vh, const double* Vxc);
 
+/* Self-consistent time loop.  With enable = 1 every step of sb200_rt_propagate
+ * ends with calc_density, hartree, exchange_correlation (PZ) and update_vlocal
+ * with this Vpsl(is:ie) (host or device; copied), in the order of
+ * time_evolution_step with yn_fix_func = 'n', inside the loop's CUDA graph; the
+ * next step's Taylor expansion uses the updated V_local.  The first step uses
+ * the V_local already set (sb200_set_vlocal, or sb200_update_vlocal from
+ * rho(t=0)).  The Hartree solve uses the cell of the latest call that passed
+ * primitive_b.  Periodic grids and nspin = 1 (else SB200_ERR_UNSUPPORTED);
+ * enable = 0 returns to the fixed-potential loop (Vpsl, primitive_b unused).
+ * Replaces: the yn_fix_func = 'n' branch of time_evolution_step
+ * (src/rt/time_evolution_step.f90:160-207).                                    */
+int sb200_set_self_consistent(sb200_ctx* ctx, int enable, const double* Vpsl, const double primitive_b[9]);
+
 /* ---- H psi without device allocation ---------------------------------------- */
 
 /* No counterpart in the reference.  For callers that cannot allocate device

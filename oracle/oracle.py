@@ -60,9 +60,10 @@ def lib():
                      "sbo_calc_Ac_ext_t", "sbo_rt_run", "sbo_set_threads", "sbo_get_threads",
                      "sbo_precond_real", "sbo_gscg_rwf", "sbo_gram_schmidt_real", "sbo_gram_schmidt_complex",
                      "sbo_subspace_diag_real", "sbo_inner_product_real", "sbo_exc_cor_pz", "sbo_poisson_coef",
-                     "sbo_dft_table", "sbo_poisson_ft", "sbo_update_vlocal"):
+                     "sbo_dft_table", "sbo_poisson_ft", "sbo_update_vlocal", "sbo_rt_run_scf"):
             getattr(L, name)
         L.sbo_rt_run.restype = C.c_int
+        L.sbo_rt_run_scf.restype = C.c_int
         L.sbo_get_threads.restype = C.c_int
         _lib = L
     return _lib
@@ -236,6 +237,33 @@ class Oracle:
                                  _p(Ac_tot), C.c_int(trans_longi), _p(curr), _p(rbox), _p(rho))
         psi = a if which == 0 else b
         return dict(psi=psi, curr=curr, rbox=rbox, Ac_tot=Ac_tot, Ac_ind=Ac_ind, rho=rho)
+
+    def rt_run_scf(self, psi0, nt, dt, zc, vpsl, brl, v0, Ac_ext=None, trans_longi=0):
+        """rt_run with the self-consistent potential update every step
+        (time_evolution_step.f90:184-207; periodic, nspin = 1).  v0: V_local
+        (nx, ny, nz) for the first step.  The oracle's own V_local is untouched."""
+        a = self._orb(psi0).copy(order="F")
+        b = np.zeros_like(a, order="F")
+        work = np.zeros_like(a, order="F")
+        if Ac_ext is None:
+            Ac_ext = np.zeros((3, nt + 2), order="F")
+        Ac_ext = np.asfortranarray(Ac_ext, dtype=np.float64)
+        Ac_ind = np.zeros_like(Ac_ext, order="F")
+        Ac_tot = Ac_ext.copy(order="F")
+        curr = np.zeros((3, nt), order="F")
+        rbox = np.zeros((4, nt), order="F")
+        rho = np.zeros(self.sys.grid.shape + (self.sys.nspin,), order="F")
+        zc = np.ascontiguousarray(zc, dtype=np.complex128)
+        vp = _flat_f(vpsl)
+        bb = np.ascontiguousarray(np.asarray(brl, dtype=np.float64).ravel(order="F"))
+        vl = _flat_f(v0).copy()
+        which = lib().sbo_rt_run_scf(C.byref(self.s), _p(a), _p(b), _p(work), C.c_int(nt), C.c_double(dt),
+                                     _p(zc), C.c_int(len(zc)), _p(Ac_ext), _p(Ac_ind), _p(Ac_tot),
+                                     C.c_int(trans_longi), _p(curr), _p(rbox), _p(rho), _p(vp), _p(bb), _p(vl))
+        assert which in (0, 1), "rt_run_scf needs a periodic nspin = 1 system"
+        psi = a if which == 0 else b
+        return dict(psi=psi, curr=curr, rbox=rbox, Ac_tot=Ac_tot, rho=rho,
+                    V_local=vl.reshape(self.sys.grid.shape, order="F"))
 
     # -- ground state (real orbitals, one k) --------------------------------
     def _real(self, psi):

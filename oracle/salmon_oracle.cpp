@@ -626,10 +626,21 @@ void sbo_calc_Ac_ext_t(int shape, double t0, double delta_t, int is, int ie, con
 
 // time loop body, time_evolution_step.f90:102-312, linear response
 // (yn_fix_func='y' path: V_local fixed), middlepoint propagator.
-int sbo_rt_run(sbo_system* s, double* psi_a, double* psi_b, double* work, int nt, double dt,
-               const double* zc, int n_hamil, const double* Ac_ext, double* Ac_ind,
-               double* Ac_tot, int trans_longi, double* curr, double* rbox, double* rho_work) {
+// The self-consistent variant (sbo_rt_run_scf): after the density, the
+// Hartree and exchange-correlation potentials of rho(t+dt) and update_vlocal,
+// time_evolution_step.f90:184-207 with yn_fix_func = 'n' (periodic, nspin = 1).
+struct ScfUpdate {
+  const double* vpsl;
+  const double* brl;
+  double* vloc;  // the buffer s->V_local points to
+};
+
+static int rt_run_impl(sbo_system* s, double* psi_a, double* psi_b, double* work, int nt, double dt,
+                       const double* zc, int n_hamil, const double* Ac_ext, double* Ac_ind, double* Ac_tot,
+                       int trans_longi, double* curr, double* rbox, double* rho_work, const ScfUpdate* scf) {
   const double pi = 3.141592653589793238462643383279502884;
+  const long npts = (long)(s->ie[0] - s->is[0] + 1) * (s->ie[1] - s->is[1] + 1) * (s->ie[2] - s->is[2] + 1);
+  std::vector<double> vh(scf ? npts : 0), vxc(scf ? npts : 0);
   double* in = psi_a;
   double* out = psi_b;
   int which = 1;
@@ -641,6 +652,13 @@ int sbo_rt_run(sbo_system* s, double* psi_a, double* psi_b, double* work, int nt
     }
     sbo_taylor(s, in, out, work, zc, n_hamil);
     sbo_calc_density(s, out, rho_work);
+    if (scf) {
+      const int num[3] = {s->ie[0] - s->is[0] + 1, s->ie[1] - s->is[1] + 1, s->ie[2] - s->is[2] + 1};
+      double exc = 0.0;
+      sbo_poisson_ft(num, scf->brl, rho_work, vh.data());
+      sbo_exc_cor_pz(npts, rho_work, s->hvol, vxc.data(), &exc);
+      sbo_update_vlocal(npts, 1, scf->vpsl, vh.data(), vxc.data(), scf->vloc);
+    }
     if (s->periodic) {
       for (int d = 0; d < 3; ++d) s->vec_Ac[d] = Ac_tot[3 * itt + d];
       double c[6] = {0, 0, 0, 0, 0, 0};
@@ -666,6 +684,27 @@ int sbo_rt_run(sbo_system* s, double* psi_a, double* psi_b, double* work, int nt
   }
   // after the last swap "in" holds the newest orbitals
   return (in == psi_a) ? 0 : 1;
+}
+
+int sbo_rt_run(sbo_system* s, double* psi_a, double* psi_b, double* work, int nt, double dt,
+               const double* zc, int n_hamil, const double* Ac_ext, double* Ac_ind,
+               double* Ac_tot, int trans_longi, double* curr, double* rbox, double* rho_work) {
+  return rt_run_impl(s, psi_a, psi_b, work, nt, dt, zc, n_hamil, Ac_ext, Ac_ind, Ac_tot, trans_longi, curr, rbox,
+                     rho_work, nullptr);
+}
+
+int sbo_rt_run_scf(sbo_system* s, double* psi_a, double* psi_b, double* work, int nt, double dt,
+                   const double* zc, int n_hamil, const double* Ac_ext, double* Ac_ind,
+                   double* Ac_tot, int trans_longi, double* curr, double* rbox, double* rho_work,
+                   const double* vpsl, const double brl[9], double* vloc) {
+  if (!s->periodic || s->nspin != 1) return -1;
+  const ScfUpdate u{vpsl, brl, vloc};
+  const double* saved = s->V_local;
+  s->V_local = vloc;
+  const int r = rt_run_impl(s, psi_a, psi_b, work, nt, dt, zc, n_hamil, Ac_ext, Ac_ind, Ac_tot, trans_longi, curr,
+                            rbox, rho_work, &u);
+  s->V_local = saved;
+  return r;
 }
 
 }  // extern "C"

@@ -282,13 +282,14 @@ int issue_rt_step(sb200_ctx* c, double2* in, double2* out, double2* work, const 
   if (orbital_kernel_applies(c)) {  // observables fused into the last Taylor term
     TRY(issue_taylor(c, in, out, work, zc, n_hamil, true));
     TIMED(c, SB200_KIND_FINAL, launch_finalize(c, -1, 0, trans_longi, dt, -1, true));
-    return SB200_OK;
+    return scf_rt_issue(c, out);
   }
   TRY(issue_taylor(c, in, out, work, zc, n_hamil));
   TIMED(c, SB200_KIND_OBS, launch_observables(c, out));
   if (c->g.periodic) TIMED(c, SB200_KIND_MOMENTS, launch_project_moments(c, out));
   TIMED(c, SB200_KIND_FINAL, launch_finalize(c, -1, 0, trans_longi, dt, -1));
-  return SB200_OK;
+  // self-consistent path: V_local of the next step from rho(t+dt)
+  return scf_rt_issue(c, out);
 }
 
 }  // namespace
@@ -951,6 +952,7 @@ int sb200_rt_propagate(sb200_ctx* c, double* psi_a, double* psi_b, double* work,
   double2* A = (double2*)psi_a;
   double2* B = (double2*)psi_b;
   double2* W = (double2*)work;
+  TRY(scf_rt_prepare(c));
   SB_CUDA(cudaStreamSynchronize(c->stream));
 
   // Two steps (A->B, B->A) captured as one CUDA graph and replayed.

@@ -227,6 +227,7 @@ int launch_project_moments(sb200_ctx* c, const double2* psi);
 int launch_finalize(sb200_ctx* c, int itt_host, int nt, int trans_longi, double dt, int spin_filter,
                     bool fused_obs = false);
 int launch_density(sb200_ctx* c, const double2* psi, double* rho);
+int density_prepare(sb200_ctx* c);
 int launch_dip(sb200_ctx* c, const double* rho, double* d_out4);
 int launch_relayout(sb200_ctx* c, const void* src, void* dst, int norb_chunk, bool to_ref);
 // time-loop histories of capacity nt (sb200_api.cu)
@@ -242,5 +243,10 @@ int learned_precond_apply(sb200_ctx* c, const double* g, const double* x, double
 int gs_project_out(sb200_ctx* c, const double* X, int m, double* Y, int n);
 void learned_free(sb200_ctx* c);
 void scf_free(sb200_ctx* c);
+// self-consistent time loop (sb200_scf.cu): buffers sized before a capture, and
+// the per-step potential update issued after each Taylor step (no-ops unless
+// sb200_set_self_consistent enabled it)
+int scf_rt_prepare(sb200_ctx* c);
+int scf_rt_issue(sb200_ctx* c, const double2* psi);
 
 }  // namespace sb200

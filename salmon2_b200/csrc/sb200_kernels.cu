@@ -772,36 +772,53 @@ int launch_finalize(sb200_ctx* c, int itt, int nt, int trans_longi, double dt, i
   return SB200_OK;
 }
 
+// Orbital chunking of calc_density: enough (point block, orbital chunk) pairs
+// for about eight blocks per SM, with at least eight orbitals per chunk.
+void density_chunks(const sb200_ctx* c, long* pblocks, int* nchunk, int* nper) {
+  const long n = c->g.npts;
+  const int nos = c->orb.no * c->orb.nk;
+  *pblocks = (n + 255) / 256;
+  long nc = (148L * 8 + *pblocks - 1) / *pblocks;
+  const long cap = (nos + 7) / 8;
+  if (nc > cap) nc = cap;
+  if (nc < 1) nc = 1;
+  *nper = (int)((nos + nc - 1) / nc);
+  *nchunk = (nos + *nper - 1) / *nper;
+}
+
+// Sizes the chunk partial-sum buffer (outside any stream capture).
+int density_prepare(sb200_ctx* c) {
+  long pblocks;
+  int nchunk, nper;
+  density_chunks(c, &pblocks, &nchunk, &nper);
+  if (nchunk <= 1) return SB200_OK;
+  const size_t need = (size_t)nchunk * c->orb.nspin * c->g.npts;
+  if (c->rho_part_cap >= need) return SB200_OK;
+  dfree(c->d_rho_part);
+  c->rho_part_cap = 0;
+  if (dalloc(&c->d_rho_part, need)) return SB200_ERR_OOM;
+  c->rho_part_cap = need;
+  return SB200_OK;
+}
+
 int launch_density(sb200_ctx* c, const double2* psi, double* rho) {
   const long n = c->g.npts;
   const int nspin = c->orb.nspin;
   const int nos = c->orb.no * c->orb.nk;
-  const long pblocks = (n + 255) / 256;
-  // enough (point block, orbital chunk) pairs for about eight blocks per SM,
-  // with at least eight orbitals per chunk
-  long nchunk = (148L * 8 + pblocks - 1) / pblocks;
-  const long cap = (nos + 7) / 8;
-  if (nchunk > cap) nchunk = cap;
-  if (nchunk < 1) nchunk = 1;
-  const int nper = (int)((nos + nchunk - 1) / nchunk);
-  nchunk = (nos + nper - 1) / nper;
+  long pblocks;
+  int nchunk, nper;
+  density_chunks(c, &pblocks, &nchunk, &nper);
   if (nchunk <= 1) {
     k_density<<<dim3((unsigned)pblocks, 1), 256, 0, c->stream>>>(psi, rho, n, nspin, nos, nos, c->d_weight);
     SB_LAUNCH_CHECK("k_density");
     return SB200_OK;
   }
-  const size_t need = (size_t)nchunk * nspin * n;
-  if (c->rho_part_cap < need) {
-    dfree(c->d_rho_part);
-    c->rho_part_cap = 0;
-    if (dalloc(&c->d_rho_part, need)) return SB200_ERR_OOM;
-    c->rho_part_cap = need;
-  }
+  if (density_prepare(c) != SB200_OK) return SB200_ERR_OOM;
   k_density<<<dim3((unsigned)pblocks, (unsigned)nchunk), 256, 0, c->stream>>>(psi, c->d_rho_part, n, nspin, nos,
                                                                              nper, c->d_weight);
   long sblocks = (n * nspin + 255) / 256;
   if (sblocks > 148L * 8) sblocks = 148L * 8;
-  k_density_sum<<<(unsigned)sblocks, 256, 0, c->stream>>>(c->d_rho_part, rho, n * nspin, (int)nchunk);
+  k_density_sum<<<(unsigned)sblocks, 256, 0, c->stream>>>(c->d_rho_part, rho, n * nspin, nchunk);
   SB_LAUNCH_CHECK("k_density");
   return SB200_OK;
 }

@@ -47,6 +47,12 @@ struct ScfState {
   double* d_part = nullptr;   // [SCF_XC_BLOCKS + 1]
   bool have_coef = false;
   double brl[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  // self-consistent time loop (sb200_set_self_consistent)
+  bool rt_on = false;
+  double* d_vpsl = nullptr;   // [npts]
+  double* d_rho = nullptr;    // [npts]
+  double* d_vh = nullptr;     // [npts]
+  double* d_vxc = nullptr;    // [npts]
 };
 
 ScfState* scf_of(sb200_ctx* c) { return static_cast<ScfState*>(c->scf); }
@@ -319,7 +325,68 @@ int scf_tables(sb200_ctx* c, const double brl[9]) {
   return SB200_OK;
 }
 
+// ---- launch sequences (no host synchronisation: also issued inside the
+// CUDA graph of the time loop) ---------------------------------------------------
+
+void scf_launch_hartree(sb200_ctx* c, const double* d_rho, double* d_vh) {
+  ScfState* s = scf_of(c);
+  const long n = s->npts;
+  const int nx = s->num[0], ny = s->num[1], nz = s->num[2];
+  const double2* tx = s->d_tab;
+  const double2* ty = tx + (size_t)nx * nx;
+  const double2* tz = ty + (size_t)ny * ny;
+  const int gb = scf_grid_blocks(n);
+  const double ntot = (double)n;
+  // forward: z, y, x (conjugate tables); the x pass divides by the point count
+  // and multiplies by 4 pi / |G|^2
+  k_dft_pass<<<gb, SCF_THREADS, 0, c->stream>>>(nullptr, d_rho, s->d_a, nullptr, tz, -1.0, nx, ny, nz, 2, nullptr,
+                                                 ntot);
+  k_dft_pass<<<gb, SCF_THREADS, 0, c->stream>>>(s->d_a, nullptr, s->d_b, nullptr, ty, -1.0, nx, ny, nz, 1, nullptr,
+                                                 ntot);
+  k_dft_pass<<<gb, SCF_THREADS, 0, c->stream>>>(s->d_b, nullptr, s->d_a, nullptr, tx, -1.0, nx, ny, nz, 0, s->d_coef,
+                                                 ntot);
+  // inverse: z, y, x; the last pass keeps the real part
+  k_dft_pass<<<gb, SCF_THREADS, 0, c->stream>>>(s->d_a, nullptr, s->d_b, nullptr, tz, 1.0, nx, ny, nz, 2, nullptr,
+                                                 ntot);
+  k_dft_pass<<<gb, SCF_THREADS, 0, c->stream>>>(s->d_b, nullptr, s->d_a, nullptr, ty, 1.0, nx, ny, nz, 1, nullptr,
+                                                 ntot);
+  k_dft_pass<<<gb, SCF_THREADS, 0, c->stream>>>(s->d_a, nullptr, nullptr, d_vh, tx, 1.0, nx, ny, nz, 0, nullptr, ntot);
+}
+
+// Vxc of d_rho; E_xc lands in d_part[SCF_XC_BLOCKS]
+void scf_launch_xc(sb200_ctx* c, const double* d_rho, double* d_vxc) {
+  ScfState* s = scf_of(c);
+  const double cst = 0.75 * std::pow(3.0 / (2.0 * SCF_PI), 2.0 / 3.0);
+  k_exc_pz<<<SCF_XC_BLOCKS, SCF_THREADS, 0, c->stream>>>(d_rho, d_vxc, s->npts, cst, s->d_part);
+  k_exc_final<<<1, 32, 0, c->stream>>>(s->d_part, SCF_XC_BLOCKS, c->g.hvol);
+}
+
+void scf_launch_update(sb200_ctx* c, const double* vpsl, const double* vh, const double* vxc) {
+  const long n = scf_of(c)->npts;
+  const int nspin = c->orb.nspin;
+  k_update_vlocal<<<scf_grid_blocks(n * nspin), SCF_THREADS, 0, c->stream>>>(vpsl, vh, vxc, c->d_vloc, c->d_vloc32,
+                                                                            n, nspin);
+}
+
 }  // namespace
+
+int scf_rt_prepare(sb200_ctx* c) {
+  ScfState* s = scf_of(c);
+  if (!s || !s->rt_on) return SB200_OK;
+  if (s->npts != c->g.npts) return set_error(SB200_ERR_STATE, "grid changed since sb200_set_self_consistent");
+  return density_prepare(c);
+}
+
+int scf_rt_issue(sb200_ctx* c, const double2* psi) {
+  ScfState* s = scf_of(c);
+  if (!s || !s->rt_on) return SB200_OK;
+  TRY_S(launch_density(c, psi, s->d_rho));
+  scf_launch_hartree(c, s->d_rho, s->d_vh);
+  scf_launch_xc(c, s->d_rho, s->d_vxc);
+  scf_launch_update(c, s->d_vpsl, s->d_vh, s->d_vxc);
+  SB_LAUNCH_CHECK("self-consistent potential update");
+  return SB200_OK;
+}
 
 void scf_free(sb200_ctx* c) {
   ScfState* s = scf_of(c);
@@ -331,6 +398,10 @@ void scf_free(sb200_ctx* c) {
   dfree(s->d_in);
   dfree(s->d_out);
   dfree(s->d_part);
+  dfree(s->d_vpsl);
+  dfree(s->d_rho);
+  dfree(s->d_vh);
+  dfree(s->d_vxc);
   delete s;
   c->scf = nullptr;
 }
@@ -356,9 +427,7 @@ int sb200_exc_cor_pz(sb200_ctx* c, const double* rho, double* Vxc, double* E_xc)
   const bool out_dev = scf_is_device(Vxc);
   if (!out_dev) TRY_S(scf_stage_out(c, (size_t)n));
   double* d_v = out_dev ? Vxc : s->d_out;
-  const double cst = 0.75 * std::pow(3.0 / (2.0 * SCF_PI), 2.0 / 3.0);
-  k_exc_pz<<<SCF_XC_BLOCKS, SCF_THREADS, 0, c->stream>>>(d_rho, d_v, n, cst, s->d_part);
-  k_exc_final<<<1, 32, 0, c->stream>>>(s->d_part, SCF_XC_BLOCKS, c->g.hvol);
+  scf_launch_xc(c, d_rho, d_v);
   SB_LAUNCH_CHECK("k_exc_pz");
   if (!out_dev) SB_CUDA(cudaMemcpyAsync(Vxc, d_v, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   double e = 0.0;
@@ -378,32 +447,13 @@ int sb200_hartree_periodic(sb200_ctx* c, const double primitive_b[9], const doub
   TRY_S(scf_tables(c, primitive_b));
   ScfState* s = scf_of(c);
   const long n = s->npts;
-  const int nx = s->num[0], ny = s->num[1], nz = s->num[2];
   TRY_S(scf_stage_in(c, (size_t)n));
   const double* d_rho = nullptr;
   TRY_S(scf_input(c, rho, (size_t)n, s->d_in, &d_rho));
   const bool out_dev = scf_is_device(Vh);
   if (!out_dev) TRY_S(scf_stage_out(c, (size_t)n));
   double* d_v = out_dev ? Vh : s->d_out;
-  const double2* tx = s->d_tab;
-  const double2* ty = tx + (size_t)nx * nx;
-  const double2* tz = ty + (size_t)ny * ny;
-  const int gb = scf_grid_blocks(n);
-  const double ntot = (double)n;
-  // forward: z, y, x (conjugate tables); the x pass divides by the point count
-  // and multiplies by 4 pi / |G|^2
-  k_dft_pass<<<gb, SCF_THREADS, 0, c->stream>>>(nullptr, d_rho, s->d_a, nullptr, tz, -1.0, nx, ny, nz, 2, nullptr,
-                                                 ntot);
-  k_dft_pass<<<gb, SCF_THREADS, 0, c->stream>>>(s->d_a, nullptr, s->d_b, nullptr, ty, -1.0, nx, ny, nz, 1, nullptr,
-                                                 ntot);
-  k_dft_pass<<<gb, SCF_THREADS, 0, c->stream>>>(s->d_b, nullptr, s->d_a, nullptr, tx, -1.0, nx, ny, nz, 0, s->d_coef,
-                                                 ntot);
-  // inverse: z, y, x; the last pass keeps the real part
-  k_dft_pass<<<gb, SCF_THREADS, 0, c->stream>>>(s->d_a, nullptr, s->d_b, nullptr, tz, 1.0, nx, ny, nz, 2, nullptr,
-                                                 ntot);
-  k_dft_pass<<<gb, SCF_THREADS, 0, c->stream>>>(s->d_b, nullptr, s->d_a, nullptr, ty, 1.0, nx, ny, nz, 1, nullptr,
-                                                 ntot);
-  k_dft_pass<<<gb, SCF_THREADS, 0, c->stream>>>(s->d_a, nullptr, nullptr, d_v, tx, 1.0, nx, ny, nz, 0, nullptr, ntot);
+  scf_launch_hartree(c, d_rho, d_v);
   SB_LAUNCH_CHECK("k_dft_pass");
   if (!out_dev) SB_CUDA(cudaMemcpyAsync(Vh, d_v, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   SB_CUDA(cudaStreamSynchronize(c->stream));
@@ -425,11 +475,38 @@ int sb200_update_vlocal(sb200_ctx* c, const double* Vpsl, const double* Vh, cons
   TRY_S(scf_input(c, Vpsl, (size_t)n, s->d_in, &a));
   TRY_S(scf_input(c, Vh, (size_t)n, s->d_in + n, &b));
   TRY_S(scf_input(c, Vxc, (size_t)n * nspin, s->d_in + 2 * n, &x));
-  k_update_vlocal<<<scf_grid_blocks(n * nspin), SCF_THREADS, 0, c->stream>>>(a, b, x, c->d_vloc, c->d_vloc32, n,
-                                                                            nspin);
+  scf_launch_update(c, a, b, x);
   SB_LAUNCH_CHECK("k_update_vlocal");
   SB_CUDA(cudaStreamSynchronize(c->stream));
   c->vloc_set = true;
+  return SB200_OK;
+}
+
+int sb200_set_self_consistent(sb200_ctx* c, int enable, const double* Vpsl, const double primitive_b[9]) {
+  TRY_S(scf_ready(c));
+  ScfDevGuard dg(c->device);
+  if (!enable) {
+    if (scf_of(c)) scf_of(c)->rt_on = false;
+    return SB200_OK;
+  }
+  if (!Vpsl || !primitive_b) return set_error(SB200_ERR_INVALID_ARG, "null argument");
+  if (!c->g.periodic)
+    return set_error(SB200_ERR_UNSUPPORTED, "the self-consistent time loop needs a periodic grid");
+  if (c->orb.nspin != 1)
+    return set_error(SB200_ERR_UNSUPPORTED, "the self-consistent time loop is the nspin = 1 form");
+  if (!c->vloc_set) return set_error(SB200_ERR_STATE, "set V_local (sb200_set_vlocal / sb200_update_vlocal) first");
+  TRY_S(scf_ensure(c));
+  TRY_S(scf_tables(c, primitive_b));
+  ScfState* s = scf_of(c);
+  const size_t n = (size_t)s->npts;
+  if (!s->d_vpsl) TRY_S(dalloc(&s->d_vpsl, n));
+  if (!s->d_rho) TRY_S(dalloc(&s->d_rho, n));
+  if (!s->d_vh) TRY_S(dalloc(&s->d_vh, n));
+  if (!s->d_vxc) TRY_S(dalloc(&s->d_vxc, n));
+  SB_CUDA(cudaMemcpyAsync(s->d_vpsl, Vpsl, n * sizeof(double), cudaMemcpyDefault, c->stream));
+  SB_CUDA(cudaStreamSynchronize(c->stream));
+  TRY_S(density_prepare(c));
+  s->rt_on = true;
   return SB200_OK;
 }
 

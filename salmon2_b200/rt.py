@@ -231,6 +231,17 @@ class Context:
         pc, kc = self._scalar_field(vxc)
         check(lib().sb200_update_vlocal(self.h, pa, pb, pc))
 
+    def set_self_consistent(self, enable, vpsl=None, primitive_b=None):
+        """Self-consistent time loop (time_evolution_step.f90:160-207 with
+        yn_fix_func = 'n'): rt_propagate recomputes V_local = Vpsl + Vh[rho] +
+        Vxc[rho] after every step.  enable = False returns to the fixed potential."""
+        if not enable:
+            check(lib().sb200_set_self_consistent(self.h, 0, None, None))
+            return
+        b = np.asfortranarray(primitive_b, dtype=np.float64)
+        p, keep = self._scalar_field(vpsl)
+        check(lib().sb200_set_self_consistent(self.h, 1, p, _ptr(b)))
+
     def update_potential(self, psi, vpsl, primitive_b):
         """The self-consistent part of one time step on the device
         (time_evolution_step.f90:160-207 for a periodic grid, nspin = 1):

@@ -169,3 +169,54 @@ def test_self_consistent_time_loop_against_oracle():
     assert S.rel_err(vh_h, OR.poisson_ft(rho_ref, brl)) < TOL_LOOP
     assert S.rel_err(vxc_h, vxc_ref) < TOL_LOOP
     ctx.close()
+
+
+@pytest.mark.parametrize("make,nt", [(S.periodic_small, 6), (S.periodic_small, 5), (S.periodic_c2_like, 6)],
+                         ids=["p12_even", "p12_odd", "p16_fused"])
+def test_rt_propagate_self_consistent(make, nt):
+    """sb200_rt_propagate with the potential update inside its CUDA graph
+    against the oracle's self-consistent loop, under a sin^2-envelope field:
+    J(t) and the dipole every step, the final orbitals and V_local.  The
+    16^3 system runs the fused Taylor-step kernel, the 12^3 one the sweep."""
+    from salmon2_b200 import synth
+    from salmon2_b200.rt import Context
+
+    s = make()
+    dt = 0.08
+    Ac = synth.asin2cos(nt, dt, omega=0.05696, f0=0.05696 * 2e-2, tw=nt * dt)
+    zc = synth.taylor_zc(dt)
+    brl = _brl(s)
+    vpsl = np.array(s.V_local[..., 0])
+    O = _oracle(s)
+    rho0 = O.density(s.psi)[..., 0]
+    v0 = OR.update_vlocal(vpsl, OR.poisson_ft(rho0, brl), OR.exc_cor_pz(rho0, s.grid.hvol)[0][..., None])[..., 0]
+    ref = O.rt_run_scf(s.psi, nt, dt, zc, vpsl, brl, v0, Ac_ext=Ac)
+
+    ctx = Context(s)
+    a, b, w = ctx.upload(s.psi), ctx.zeros(), ctx.zeros()
+    rho = ctx.calc_density(a)[..., 0]
+    vxc, _ = ctx.exc_cor_pz(rho)
+    ctx.update_vlocal(vpsl, ctx.hartree_periodic(rho, brl), vxc)
+    ctx.set_self_consistent(True, vpsl, brl)
+    res = ctx.rt_propagate(a, b, w, nt, dt, zc, Ac_ext=Ac)
+    jmax = np.max(np.abs(ref["curr"]))
+    assert jmax > 0
+    assert np.max(np.abs(res["curr"] - ref["curr"])) <= TOL_LOOP * jmax
+    assert S.rel_err(res["rbox"], ref["rbox"]) < TOL_LOOP
+    assert S.rel_err(ctx.download(res["psi"]), ref["psi"]) < TOL_LOOP
+    # the potential the loop left behind: H psi with it matches the oracle's
+    # (both at A = 0: the oracle's loop leaves its last A(t) set)
+    O.V[..., 0] = ref["V_local"]
+    O.set_vec_Ac((0.0, 0.0, 0.0))
+    ctx.set_vec_Ac((0.0, 0.0, 0.0))
+    h = ctx.zeros()
+    ctx.hpsi(res["psi"], h)
+    assert S.rel_err(ctx.download(h), O.hpsi(ref["psi"])) < TOL_LOOP
+    # the fixed-potential loop again after switching the update off
+    ctx.set_self_consistent(False)
+    ctx.update_vlocal(vpsl, np.zeros_like(vpsl), np.zeros_like(vpsl))
+    a2, b2, w2 = ctx.upload(s.psi), ctx.zeros(), ctx.zeros()
+    res2 = ctx.rt_propagate(a2, b2, w2, 2, dt, zc, Ac_ext=Ac[:, :4])
+    ref2 = _oracle(s).rt_run(s.psi, 2, dt, zc, Ac_ext=Ac[:, :4])
+    assert S.rel_err(ctx.download(res2["psi"]), ref2["psi"]) < TOL_LOOP
+    ctx.close()

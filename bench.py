@@ -55,6 +55,9 @@ def parse():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--cpu-steps", type=int, default=4, help="Taylor steps in each CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--self-consistent", action="store_true",
+                    help="periodic workloads: V_local = Vpsl + Vh[rho] + Vxc[rho] (PZ) recomputed after every "
+                         "Taylor step inside the time loop (the fixed Gaussian potential stands in for Vpsl)")
     ap.add_argument("--small", action="store_true", help="8 k-points instead of 64 (quick check)")
     ap.add_argument("--workload", default="bulk", choices=["bulk", "supercell", "batch", "isolated"],
                     help="bulk: 16^3 x 64 k x 32 orbitals; supercell: its 2x2x2 supercell, 32^3 x 8 k x 256; "
@@ -103,11 +106,14 @@ def config_dict(args, s, nt, world):
                 f"{s.pp.natom} atoms (diamond), {s.grid.shape[0]}^3 grid, "
                 f"{s.nk} k-points, {s.no} complex128 orbitals/k, Asin2cos A(t) omega=1.55 eV "
                 f"peak 1e-3 au, {nt} Taylor-4 steps per bench step, J(t) every step")
+        if getattr(args, "self_consistent", False):
+            desc += ", self-consistent: density, Hartree (periodic) and PZ-LDA potential every step"
     return {
         "workload": desc,
         "grid": list(s.grid.shape), "k_points": s.nk, "orbitals_per_k": s.no, "atoms": s.pp.natom,
         "projectors": s.pp.nlma, "taylor_steps_per_bench_step": nt, "units_per_bench_step_per_rank": units,
         "precision": args.precision,
+        "self_consistent": bool(getattr(args, "self_consistent", False)),
         "parallelism": f"replicas x{world}" if args.workload == "isolated" else f"k-point shards x{world}",
         "l2": ("inputs larger than L2 (3 orbital blocks of %.0f MB each)" % (units / nt * 16 / 1e6)
                if units / nt * 16 * 3 > 126e6 else
@@ -227,10 +233,21 @@ def cpu_baseline(args, s, dt, Ac, zc, nsteps, min_seconds=10.0):
     threads = os.cpu_count() or 1
     O = Oracle(s, threads=threads)
     Ac_s = None if Ac is None else Ac[:, : nsteps + 2].copy(order="F")
+    scf = getattr(args, "self_consistent", False)
+    if scf:  # the same per-step potential update as the GPU loop
+        import oracle as OR
+        brl = np.diag([2.0 * np.pi / (n * h) for n, h in zip(s.grid.shape, s.grid.hgs)])
+        vpsl = np.array(s.V_local[..., 0])
+        rho0 = O.density(s.psi)[..., 0]
+        v0 = OR.update_vlocal(vpsl, OR.poisson_ft(rho0, brl),
+                              OR.exc_cor_pz(rho0, s.grid.hvol)[0][..., None])[..., 0]
     el, runs = 0.0, 0
     while el < min_seconds or runs == 0:
         t0 = time.perf_counter()
-        O.rt_run(s.psi, nsteps, dt, zc, Ac_ext=Ac_s)
+        if scf:
+            O.rt_run_scf(s.psi, nsteps, dt, zc, vpsl, brl, v0, Ac_ext=Ac_s)
+        else:
+            O.rt_run(s.psi, nsteps, dt, zc, Ac_ext=Ac_s)
         el += time.perf_counter() - t0
         runs += 1
     units = int(np.prod(s.grid.shape)) * s.norb * nsteps * runs
@@ -448,6 +465,14 @@ def main():
     ctx.set_stream(stream)
     a, b, w = ctx.upload(s.psi), ctx.zeros(), ctx.zeros()
     units_rank = int(np.prod(s.grid.shape)) * s.norb * nt
+    if args.self_consistent:
+        if not s.grid.periodic or s.nspin != 1:
+            raise SystemExit("--self-consistent needs a periodic workload with one spin")
+        # cubic cell: primitive_b = 2 pi / L; V_local from rho(t=0), then the update every step
+        brl = np.diag([2.0 * np.pi / (n * h) for n, h in zip(s.grid.shape, s.grid.hgs)])
+        vpsl = torch.from_numpy(np.ascontiguousarray(s.V_local[..., 0].ravel(order="F"))).cuda(local)
+        ctx.update_potential(a, vpsl, brl)
+        ctx.set_self_consistent(True, vpsl, brl)
 
     def barrier():
         if world > 1:

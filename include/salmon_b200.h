@@ -57,6 +57,7 @@ typedef struct sb200_ctx sb200_ctx;
 #define SB200_KIND_OBS 3       /* density / current / dipole partial sums       */
 #define SB200_KIND_MOMENTS 4   /* nonlocal current projections                  */
 #define SB200_KIND_FINAL 5     /* per-step reduction and field update           */
+#define SB200_KIND_POTENTIAL 6 /* self-consistent update: rho, Hartree, XC, V    */
 #define SB200_KIND_COUNT 8
 
 /* ---- context ------------------------------------------------------------ */

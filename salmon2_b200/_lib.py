@@ -20,7 +20,7 @@ PREC_FP64, PREC_MIXED = 0, 1
 TRANS_TR, TRANS_LO = 0, 1
 PRECOND_NONE, PRECOND_LOWPASS, PRECOND_LEARNED = 0, 1, 2
 LEARNED_CHANNELS, LEARNED_NPARAM = 16, 8241
-KIND_NAMES = ["prep", "project", "hpsi", "observables", "moments", "finalize", "k6", "k7"]
+KIND_NAMES = ["prep", "project", "hpsi", "observables", "moments", "finalize", "potential", "k7"]
 
 
 class SB200Error(RuntimeError):

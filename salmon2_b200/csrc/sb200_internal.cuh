@@ -226,7 +226,8 @@ int launch_observables(sb200_ctx* c, const double2* psi);
 int launch_project_moments(sb200_ctx* c, const double2* psi);
 int launch_finalize(sb200_ctx* c, int itt_host, int nt, int trans_longi, double dt, int spin_filter,
                     bool fused_obs = false);
-int launch_density(sb200_ctx* c, const double2* psi, double* rho);
+// kind >= 0: each launch bracketed for sb200_kernel_times (SB200_KIND_*)
+int launch_density(sb200_ctx* c, const double2* psi, double* rho, int kind = -1);
 int density_prepare(sb200_ctx* c);
 int launch_dip(sb200_ctx* c, const double* rho, double* d_out4);
 int launch_relayout(sb200_ctx* c, const void* src, void* dst, int norb_chunk, bool to_ref);

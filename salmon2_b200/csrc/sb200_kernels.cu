@@ -801,26 +801,31 @@ int density_prepare(sb200_ctx* c) {
   return SB200_OK;
 }
 
-int launch_density(sb200_ctx* c, const double2* psi, double* rho) {
+int launch_density(sb200_ctx* c, const double2* psi, double* rho, int kind) {
   const long n = c->g.npts;
   const int nspin = c->orb.nspin;
   const int nos = c->orb.no * c->orb.nk;
   long pblocks;
   int nchunk, nper;
   density_chunks(c, &pblocks, &nchunk, &nper);
+  // kind >= 0: each launch bracketed for sb200_kernel_times
+  auto mark = [&](bool start) { return kind >= 0 ? kernel_timing_mark(c, kind, start) : SB200_OK; };
   if (nchunk <= 1) {
+    if (mark(true)) return SB200_ERR_CUDA;
     k_density<<<dim3((unsigned)pblocks, 1), 256, 0, c->stream>>>(psi, rho, n, nspin, nos, nos, c->d_weight);
     SB_LAUNCH_CHECK("k_density");
-    return SB200_OK;
+    return mark(false);
   }
   if (density_prepare(c) != SB200_OK) return SB200_ERR_OOM;
+  if (mark(true)) return SB200_ERR_CUDA;
   k_density<<<dim3((unsigned)pblocks, (unsigned)nchunk), 256, 0, c->stream>>>(psi, c->d_rho_part, n, nspin, nos,
                                                                              nper, c->d_weight);
+  if (mark(false) || mark(true)) return SB200_ERR_CUDA;
   long sblocks = (n * nspin + 255) / 256;
   if (sblocks > 148L * 8) sblocks = 148L * 8;
   k_density_sum<<<(unsigned)sblocks, 256, 0, c->stream>>>(c->d_rho_part, rho, n * nspin, nchunk);
   SB_LAUNCH_CHECK("k_density");
-  return SB200_OK;
+  return mark(false);
 }
 
 int launch_dip(sb200_ctx* c, const double* rho, double* d_out4) {

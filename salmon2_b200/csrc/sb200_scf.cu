@@ -328,7 +328,10 @@ int scf_tables(sb200_ctx* c, const double brl[9]) {
 // ---- launch sequences (no host synchronisation: also issued inside the
 // CUDA graph of the time loop) ---------------------------------------------------
 
-void scf_launch_hartree(sb200_ctx* c, const double* d_rho, double* d_vh) {
+// kind >= 0: each launch bracketed for sb200_kernel_times
+int scf_mark(sb200_ctx* c, int kind, bool start) { return kind >= 0 ? kernel_timing_mark(c, kind, start) : SB200_OK; }
+
+int scf_launch_hartree(sb200_ctx* c, const double* d_rho, double* d_vh, int kind) {
   ScfState* s = scf_of(c);
   const long n = s->npts;
   const int nx = s->num[0], ny = s->num[1], nz = s->num[2];
@@ -337,35 +340,51 @@ void scf_launch_hartree(sb200_ctx* c, const double* d_rho, double* d_vh) {
   const double2* tz = ty + (size_t)ny * ny;
   const int gb = scf_grid_blocks(n);
   const double ntot = (double)n;
-  // forward: z, y, x (conjugate tables); the x pass divides by the point count
-  // and multiplies by 4 pi / |G|^2
-  k_dft_pass<<<gb, SCF_THREADS, 0, c->stream>>>(nullptr, d_rho, s->d_a, nullptr, tz, -1.0, nx, ny, nz, 2, nullptr,
-                                                 ntot);
-  k_dft_pass<<<gb, SCF_THREADS, 0, c->stream>>>(s->d_a, nullptr, s->d_b, nullptr, ty, -1.0, nx, ny, nz, 1, nullptr,
-                                                 ntot);
-  k_dft_pass<<<gb, SCF_THREADS, 0, c->stream>>>(s->d_b, nullptr, s->d_a, nullptr, tx, -1.0, nx, ny, nz, 0, s->d_coef,
-                                                 ntot);
-  // inverse: z, y, x; the last pass keeps the real part
-  k_dft_pass<<<gb, SCF_THREADS, 0, c->stream>>>(s->d_a, nullptr, s->d_b, nullptr, tz, 1.0, nx, ny, nz, 2, nullptr,
-                                                 ntot);
-  k_dft_pass<<<gb, SCF_THREADS, 0, c->stream>>>(s->d_b, nullptr, s->d_a, nullptr, ty, 1.0, nx, ny, nz, 1, nullptr,
-                                                 ntot);
-  k_dft_pass<<<gb, SCF_THREADS, 0, c->stream>>>(s->d_a, nullptr, nullptr, d_vh, tx, 1.0, nx, ny, nz, 0, nullptr, ntot);
+  // forward: z, y, x (conjugate tables), the x pass dividing by the point count
+  // and multiplying by 4 pi / |G|^2; inverse: z, y, x, the last keeping the real part
+  struct Pass {
+    const double2* in;
+    const double* in_real;
+    double2* out;
+    double* out_real;
+    const double2* T;
+    double sg;
+    int axis;
+    const double* coef;
+  } passes[6] = {{nullptr, d_rho, s->d_a, nullptr, tz, -1.0, 2, nullptr},
+                 {s->d_a, nullptr, s->d_b, nullptr, ty, -1.0, 1, nullptr},
+                 {s->d_b, nullptr, s->d_a, nullptr, tx, -1.0, 0, s->d_coef},
+                 {s->d_a, nullptr, s->d_b, nullptr, tz, 1.0, 2, nullptr},
+                 {s->d_b, nullptr, s->d_a, nullptr, ty, 1.0, 1, nullptr},
+                 {s->d_a, nullptr, nullptr, d_vh, tx, 1.0, 0, nullptr}};
+  for (const Pass& p : passes) {
+    TRY_S(scf_mark(c, kind, true));
+    k_dft_pass<<<gb, SCF_THREADS, 0, c->stream>>>(p.in, p.in_real, p.out, p.out_real, p.T, p.sg, nx, ny, nz, p.axis,
+                                                   p.coef, ntot);
+    TRY_S(scf_mark(c, kind, false));
+  }
+  return SB200_OK;
 }
 
 // Vxc of d_rho; E_xc lands in d_part[SCF_XC_BLOCKS]
-void scf_launch_xc(sb200_ctx* c, const double* d_rho, double* d_vxc) {
+int scf_launch_xc(sb200_ctx* c, const double* d_rho, double* d_vxc, int kind) {
   ScfState* s = scf_of(c);
   const double cst = 0.75 * std::pow(3.0 / (2.0 * SCF_PI), 2.0 / 3.0);
+  TRY_S(scf_mark(c, kind, true));
   k_exc_pz<<<SCF_XC_BLOCKS, SCF_THREADS, 0, c->stream>>>(d_rho, d_vxc, s->npts, cst, s->d_part);
+  TRY_S(scf_mark(c, kind, false));
+  TRY_S(scf_mark(c, kind, true));
   k_exc_final<<<1, 32, 0, c->stream>>>(s->d_part, SCF_XC_BLOCKS, c->g.hvol);
+  return scf_mark(c, kind, false);
 }
 
-void scf_launch_update(sb200_ctx* c, const double* vpsl, const double* vh, const double* vxc) {
+int scf_launch_update(sb200_ctx* c, const double* vpsl, const double* vh, const double* vxc, int kind) {
   const long n = scf_of(c)->npts;
   const int nspin = c->orb.nspin;
+  TRY_S(scf_mark(c, kind, true));
   k_update_vlocal<<<scf_grid_blocks(n * nspin), SCF_THREADS, 0, c->stream>>>(vpsl, vh, vxc, c->d_vloc, c->d_vloc32,
                                                                             n, nspin);
+  return scf_mark(c, kind, false);
 }
 
 }  // namespace
@@ -380,10 +399,10 @@ int scf_rt_prepare(sb200_ctx* c) {
 int scf_rt_issue(sb200_ctx* c, const double2* psi) {
   ScfState* s = scf_of(c);
   if (!s || !s->rt_on) return SB200_OK;
-  TRY_S(launch_density(c, psi, s->d_rho));
-  scf_launch_hartree(c, s->d_rho, s->d_vh);
-  scf_launch_xc(c, s->d_rho, s->d_vxc);
-  scf_launch_update(c, s->d_vpsl, s->d_vh, s->d_vxc);
+  TRY_S(launch_density(c, psi, s->d_rho, SB200_KIND_POTENTIAL));
+  TRY_S(scf_launch_hartree(c, s->d_rho, s->d_vh, SB200_KIND_POTENTIAL));
+  TRY_S(scf_launch_xc(c, s->d_rho, s->d_vxc, SB200_KIND_POTENTIAL));
+  TRY_S(scf_launch_update(c, s->d_vpsl, s->d_vh, s->d_vxc, SB200_KIND_POTENTIAL));
   SB_LAUNCH_CHECK("self-consistent potential update");
   return SB200_OK;
 }
@@ -427,7 +446,7 @@ int sb200_exc_cor_pz(sb200_ctx* c, const double* rho, double* Vxc, double* E_xc)
   const bool out_dev = scf_is_device(Vxc);
   if (!out_dev) TRY_S(scf_stage_out(c, (size_t)n));
   double* d_v = out_dev ? Vxc : s->d_out;
-  scf_launch_xc(c, d_rho, d_v);
+  TRY_S(scf_launch_xc(c, d_rho, d_v, -1));
   SB_LAUNCH_CHECK("k_exc_pz");
   if (!out_dev) SB_CUDA(cudaMemcpyAsync(Vxc, d_v, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   double e = 0.0;
@@ -453,7 +472,7 @@ int sb200_hartree_periodic(sb200_ctx* c, const double primitive_b[9], const doub
   const bool out_dev = scf_is_device(Vh);
   if (!out_dev) TRY_S(scf_stage_out(c, (size_t)n));
   double* d_v = out_dev ? Vh : s->d_out;
-  scf_launch_hartree(c, d_rho, d_v);
+  TRY_S(scf_launch_hartree(c, d_rho, d_v, -1));
   SB_LAUNCH_CHECK("k_dft_pass");
   if (!out_dev) SB_CUDA(cudaMemcpyAsync(Vh, d_v, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   SB_CUDA(cudaStreamSynchronize(c->stream));
@@ -475,7 +494,7 @@ int sb200_update_vlocal(sb200_ctx* c, const double* Vpsl, const double* Vh, cons
   TRY_S(scf_input(c, Vpsl, (size_t)n, s->d_in, &a));
   TRY_S(scf_input(c, Vh, (size_t)n, s->d_in + n, &b));
   TRY_S(scf_input(c, Vxc, (size_t)n * nspin, s->d_in + 2 * n, &x));
-  scf_launch_update(c, a, b, x);
+  TRY_S(scf_launch_update(c, a, b, x, -1));
   SB_LAUNCH_CHECK("k_update_vlocal");
   SB_CUDA(cudaStreamSynchronize(c->stream));
   c->vloc_set = true;

@@ -212,6 +212,30 @@ inline void calc_eigen_energy(context& ctx, const s_orbital& tpsi, s_orbital& ht
         "calc_eigen_energy");
 }
 
+// hartree(lg,mg,info,system,fg,poisson,srg_scalar,stencil,rho,Vh) (hartree.f90:20) on
+// a periodic grid: poisson_ft (poisson_periodic.f90:23); primitive_b = system%primitive_b
+inline void hartree(context& ctx, const double primitive_b[9], const s_scalar& rho, s_scalar& Vh) {
+  Vh.f.resize(rho.f.size());
+  check(sb200_hartree_periodic(ctx.get(), primitive_b, rho.f.data(), Vh.f.data()), "hartree");
+}
+
+// exchange_correlation(system,xc_func,mg,srg_scalar,srg,rho_s,ppn,info,spsi,stencil,Vxc,E_xc)
+// (salmon_xc.f90:58) with xc = 'PZ' and nspin = 1
+inline void exchange_correlation(context& ctx, const s_scalar& rho, std::vector<s_scalar>& Vxc, double& E_xc) {
+  Vxc.resize(1);
+  Vxc[0].f.resize(rho.f.size());
+  check(sb200_exc_cor_pz(ctx.get(), rho.f.data(), Vxc[0].f.data(), &E_xc), "exchange_correlation");
+}
+
+// update_vlocal(mg,nspin,Vh,Vpsl,Vxc,Vlocal) (hamiltonian.f90:813): V_local of the
+// context (its device copy, used by hpsi / taylor) becomes Vpsl + Vh + Vxc(ispin)
+inline void update_vlocal(context& ctx, const s_scalar& Vh, const s_scalar& Vpsl, const std::vector<s_scalar>& Vxc) {
+  const size_t n = Vpsl.f.size();
+  std::vector<double> x(n * Vxc.size());
+  for (size_t s = 0; s < Vxc.size(); ++s) std::copy(Vxc[s].f.begin(), Vxc[s].f.end(), x.begin() + s * n);
+  check(sb200_update_vlocal(ctx.get(), Vpsl.f.data(), Vh.f.data(), x.data()), "update_vlocal");
+}
+
 // gram_schmidt(system, mg, info, psi) for complex orbitals (gram_schmidt_orth.f90:1069)
 inline void gram_schmidt(context& ctx, s_orbital& psi) {
   check(sb200_gram_schmidt_complex(ctx.get(), psi.data()), "gram_schmidt");

@@ -397,25 +397,35 @@ __global__ void __launch_bounds__(256) k_collapse(const double* __restrict__ par
 }
 
 // rho(p, ispin) = sum_{ik, io} w |psi|^2 (density_matrix.f90:150-232)
-// rho of one chunk of (io, ik) orbitals per spin, rocc*wtk weighted, in the
-// reference's order within the chunk (ik outer, io inner).  With one chunk the
-// result goes straight to rho; with several, part[chunk][is][p] holds the chunk
-// sums and k_density_sum adds them in chunk order.  The chunk count depends only
-// on the grid and orbital counts, so the summation order is fixed.
-__global__ void k_density(const double2* __restrict__ in, double* __restrict__ out, long npts, int nspin,
-                          int nos, int nper, const double* __restrict__ weight) {
-  const long p = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  if (p >= npts) return;
+// rho of one chunk of (io, ik) orbitals per spin, rocc*wtk weighted.  A block
+// is 32 points x 8 orbital slices: slice y sums the chunk's orbitals
+// j = j0 + y, j0 + y + 8, ... and the eight slice sums are added in slice
+// order.  With one chunk the result goes straight to rho; with several,
+// part[chunk][is][p] holds the chunk sums and k_density_sum adds them in chunk
+// order.  The chunk count depends only on the grid and orbital counts, so the
+// summation order is fixed.
+__global__ void __launch_bounds__(256) k_density(const double2* __restrict__ in, double* __restrict__ out, long npts,
+                                                 int nspin, int nos, int nper, const double* __restrict__ weight) {
+  __shared__ double red[8][32];
+  const long p = blockIdx.x * 32L + threadIdx.x;
   const int j0 = blockIdx.y * nper;
   const int j1 = min(nos, j0 + nper);
   for (int is = 0; is < nspin; ++is) {
     double acc = 0.0;
-    for (int j = j0; j < j1; ++j) {  // j = io + no * ik
-      const long o = is + (long)nspin * j;
-      const double2 c = __ldg(in + o * npts + p);
-      acc += (c.x * c.x + c.y * c.y) * weight[o];
+    if (p < npts)
+      for (int j = j0 + (int)threadIdx.y; j < j1; j += 8) {  // j = io + no * ik
+        const long o = is + (long)nspin * j;
+        const double2 c = __ldg(in + o * npts + p);
+        acc += (c.x * c.x + c.y * c.y) * weight[o];
+      }
+    red[threadIdx.y][threadIdx.x] = acc;
+    __syncthreads();
+    if (threadIdx.y == 0 && p < npts) {
+      double t = red[0][threadIdx.x];
+      for (int k = 1; k < 8; ++k) t += red[k][threadIdx.x];
+      out[((long)blockIdx.y * nspin + is) * npts + p] = t;
     }
-    out[((long)blockIdx.y * nspin + is) * npts + p] = acc;
+    __syncthreads();
   }
 }
 
@@ -772,14 +782,15 @@ int launch_finalize(sb200_ctx* c, int itt, int nt, int trans_longi, double dt, i
   return SB200_OK;
 }
 
-// Orbital chunking of calc_density: enough (point block, orbital chunk) pairs
-// for about eight blocks per SM, with at least eight orbitals per chunk.
+// Orbital chunking of calc_density: enough (32-point block, orbital chunk)
+// pairs for about eight blocks per SM, with at least 32 orbitals per chunk
+// (four per orbital slice).
 void density_chunks(const sb200_ctx* c, long* pblocks, int* nchunk, int* nper) {
   const long n = c->g.npts;
   const int nos = c->orb.no * c->orb.nk;
-  *pblocks = (n + 255) / 256;
+  *pblocks = (n + 31) / 32;
   long nc = (148L * 8 + *pblocks - 1) / *pblocks;
-  const long cap = (nos + 7) / 8;
+  const long cap = (nos + 31) / 32;
   if (nc > cap) nc = cap;
   if (nc < 1) nc = 1;
   *nper = (int)((nos + nc - 1) / nc);
@@ -812,14 +823,14 @@ int launch_density(sb200_ctx* c, const double2* psi, double* rho, int kind) {
   auto mark = [&](bool start) { return kind >= 0 ? kernel_timing_mark(c, kind, start) : SB200_OK; };
   if (nchunk <= 1) {
     if (mark(true)) return SB200_ERR_CUDA;
-    k_density<<<dim3((unsigned)pblocks, 1), 256, 0, c->stream>>>(psi, rho, n, nspin, nos, nos, c->d_weight);
+    k_density<<<dim3((unsigned)pblocks, 1), dim3(32, 8), 0, c->stream>>>(psi, rho, n, nspin, nos, nos, c->d_weight);
     SB_LAUNCH_CHECK("k_density");
     return mark(false);
   }
   if (density_prepare(c) != SB200_OK) return SB200_ERR_OOM;
   if (mark(true)) return SB200_ERR_CUDA;
-  k_density<<<dim3((unsigned)pblocks, (unsigned)nchunk), 256, 0, c->stream>>>(psi, c->d_rho_part, n, nspin, nos,
-                                                                             nper, c->d_weight);
+  k_density<<<dim3((unsigned)pblocks, (unsigned)nchunk), dim3(32, 8), 0, c->stream>>>(psi, c->d_rho_part, n, nspin,
+                                                                                     nos, nper, c->d_weight);
   if (mark(false) || mark(true)) return SB200_ERR_CUDA;
   long sblocks = (n * nspin + 255) / 256;
   if (sblocks > 148L * 8) sblocks = 148L * 8;

@@ -32,6 +32,7 @@ namespace {
 constexpr double SCF_PI = 3.141592653589793;
 constexpr int SCF_THREADS = 256;
 constexpr int SCF_XC_BLOCKS = 296;  // fixed: the E_xc partial sums have a fixed order
+constexpr int SCF_DFT_THREADS = 64;  // small blocks: a 16^3 pass spreads over 64 SMs
 
 struct ScfState {
   long npts = 0;
@@ -209,14 +210,14 @@ __global__ void k_exc_final(double* __restrict__ part, int nblk, double hvol) {
 // in_real (first forward pass).  coef: the forward x pass ends with
 // coef * (sum / ntot) as poisson_ft does.  out_real: keep the real part (last
 // inverse pass).
-__global__ void __launch_bounds__(SCF_THREADS) k_dft_pass(const double2* __restrict__ in,
+__global__ void __launch_bounds__(SCF_DFT_THREADS) k_dft_pass(const double2* __restrict__ in,
                                                           const double* __restrict__ in_real,
                                                           double2* __restrict__ out, double* __restrict__ out_real,
                                                           const double2* __restrict__ T, double sg, int nx, int ny,
                                                           int nz, int axis, const double* __restrict__ coef,
                                                           double ntot) {
   const long npts = (long)nx * ny * nz;
-  for (long p = blockIdx.x * (long)SCF_THREADS + threadIdx.x; p < npts; p += (long)gridDim.x * SCF_THREADS) {
+  for (long p = blockIdx.x * (long)SCF_DFT_THREADS + threadIdx.x; p < npts; p += (long)gridDim.x * SCF_DFT_THREADS) {
     const int x = (int)(p % nx);
     const long r = p / nx;
     const int y = (int)(r % ny);
@@ -239,6 +240,7 @@ __global__ void __launch_bounds__(SCF_THREADS) k_dft_pass(const double2* __restr
     const long base = p - (long)k * stride;
     const double2* Tk = T + (long)k * n;
     double re = 0.0, im = 0.0;
+#pragma unroll 4
     for (int j = 0; j < n; ++j) {
       const double2 t = Tk[j];
       const double ti = sg * t.y;
@@ -338,7 +340,9 @@ int scf_launch_hartree(sb200_ctx* c, const double* d_rho, double* d_vh, int kind
   const double2* tx = s->d_tab;
   const double2* ty = tx + (size_t)nx * nx;
   const double2* tz = ty + (size_t)ny * ny;
-  const int gb = scf_grid_blocks(n);
+  long gbl = (n + SCF_DFT_THREADS - 1) / SCF_DFT_THREADS;
+  if (gbl > 148L * 16) gbl = 148L * 16;
+  const int gb = (int)gbl;
   const double ntot = (double)n;
   // forward: z, y, x (conjugate tables), the x pass dividing by the point count
   // and multiplying by 4 pi / |G|^2; inverse: z, y, x, the last keeping the real part
@@ -359,20 +363,22 @@ int scf_launch_hartree(sb200_ctx* c, const double* d_rho, double* d_vh, int kind
                  {s->d_a, nullptr, nullptr, d_vh, tx, 1.0, 0, nullptr}};
   for (const Pass& p : passes) {
     TRY_S(scf_mark(c, kind, true));
-    k_dft_pass<<<gb, SCF_THREADS, 0, c->stream>>>(p.in, p.in_real, p.out, p.out_real, p.T, p.sg, nx, ny, nz, p.axis,
-                                                   p.coef, ntot);
+    k_dft_pass<<<gb, SCF_DFT_THREADS, 0, c->stream>>>(p.in, p.in_real, p.out, p.out_real, p.T, p.sg, nx, ny, nz,
+                                                       p.axis, p.coef, ntot);
     TRY_S(scf_mark(c, kind, false));
   }
   return SB200_OK;
 }
 
-// Vxc of d_rho; E_xc lands in d_part[SCF_XC_BLOCKS]
-int scf_launch_xc(sb200_ctx* c, const double* d_rho, double* d_vxc, int kind) {
+// Vxc of d_rho; with total, E_xc lands in d_part[SCF_XC_BLOCKS] (the time loop
+// does not use it and skips the final sum)
+int scf_launch_xc(sb200_ctx* c, const double* d_rho, double* d_vxc, int kind, bool total = true) {
   ScfState* s = scf_of(c);
   const double cst = 0.75 * std::pow(3.0 / (2.0 * SCF_PI), 2.0 / 3.0);
   TRY_S(scf_mark(c, kind, true));
   k_exc_pz<<<SCF_XC_BLOCKS, SCF_THREADS, 0, c->stream>>>(d_rho, d_vxc, s->npts, cst, s->d_part);
   TRY_S(scf_mark(c, kind, false));
+  if (!total) return SB200_OK;
   TRY_S(scf_mark(c, kind, true));
   k_exc_final<<<1, 32, 0, c->stream>>>(s->d_part, SCF_XC_BLOCKS, c->g.hvol);
   return scf_mark(c, kind, false);
@@ -401,7 +407,7 @@ int scf_rt_issue(sb200_ctx* c, const double2* psi) {
   if (!s || !s->rt_on) return SB200_OK;
   TRY_S(launch_density(c, psi, s->d_rho, SB200_KIND_POTENTIAL));
   TRY_S(scf_launch_hartree(c, s->d_rho, s->d_vh, SB200_KIND_POTENTIAL));
-  TRY_S(scf_launch_xc(c, s->d_rho, s->d_vxc, SB200_KIND_POTENTIAL));
+  TRY_S(scf_launch_xc(c, s->d_rho, s->d_vxc, SB200_KIND_POTENTIAL, false));
   TRY_S(scf_launch_update(c, s->d_vpsl, s->d_vh, s->d_vxc, SB200_KIND_POTENTIAL));
   SB_LAUNCH_CHECK("self-consistent potential update");
   return SB200_OK;

@@ -160,6 +160,41 @@ module salmon_b200
       real(c_double), intent(inout) :: rbox(4)
     end function
 
+    ! time_evolution_step.f90:184-207: hartree (periodic), exchange_correlation (PZ,
+    ! nspin = 1), update_vlocal; rho, Vh, Vxc, Vpsl: s_scalar%f(mg%is:mg%ie) host arrays
+    integer(c_int) function sb200_exc_cor_pz(ctx, rho, Vxc, E_xc) bind(c, name="sb200_exc_cor_pz")
+      import
+      type(c_ptr), value :: ctx
+      real(c_double), intent(in) :: rho(*)
+      real(c_double), intent(inout) :: Vxc(*)
+      real(c_double), intent(out) :: E_xc
+    end function
+
+    integer(c_int) function sb200_hartree_periodic(ctx, primitive_b, rho, Vh) &
+        bind(c, name="sb200_hartree_periodic")
+      import
+      type(c_ptr), value :: ctx
+      real(c_double), intent(in) :: primitive_b(3, 3)
+      real(c_double), intent(in) :: rho(*)
+      real(c_double), intent(inout) :: Vh(*)
+    end function
+
+    integer(c_int) function sb200_update_vlocal(ctx, Vpsl, Vh, Vxc) bind(c, name="sb200_update_vlocal")
+      import
+      type(c_ptr), value :: ctx
+      real(c_double), intent(in) :: Vpsl(*), Vh(*), Vxc(*)
+    end function
+
+    ! yn_fix_func = 'n' inside sb200_rt_propagate (enable = 1); Vpsl(mg%is:mg%ie)
+    integer(c_int) function sb200_set_self_consistent(ctx, enable, Vpsl, primitive_b) &
+        bind(c, name="sb200_set_self_consistent")
+      import
+      type(c_ptr), value :: ctx
+      integer(c_int), value :: enable
+      real(c_double), intent(in) :: Vpsl(*)
+      real(c_double), intent(in) :: primitive_b(3, 3)
+    end function
+
     integer(c_int) function sb200_rt_propagate(ctx, psi_a, psi_b, work, nt, dt, zc, n_hamil, Ac_ext, &
                                                trans_longi, curr, rbox, Ac_tot, psi_final) &
         bind(c, name="sb200_rt_propagate")

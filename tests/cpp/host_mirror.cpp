@@ -158,6 +158,7 @@ int main(int argc, char** argv) {
     sb::calc_density(ctx, rho, tpsi);
     for (int s = 0; s < sys.nspin; ++s) put(of, "rho" + std::to_string(s), rho[s].f.data(), nint);
 
+
     sb::taylor(ctx, sys, tpsi, out, work, rt);  // tpsi is scratch afterwards
     out.to_ref(buf.data());
     put(of, "taylor", reinterpret_cast<const double*>(buf.data()), 2 * buf.size());
@@ -170,6 +171,23 @@ int main(int argc, char** argv) {
       code = e.code();
     }
     put(of, "alias_code", &code, 1);
+
+    // the self-consistent potential of this density (periodic, nspin = 1)
+    const auto brl = get<double>(in, "primitive_b");
+    sb::s_scalar vh, vpsl;
+    std::vector<sb::s_scalar> vxc;
+    double exc = 0.0;
+    sb::hartree(ctx, brl.data(), rho[0], vh);
+    sb::exchange_correlation(ctx, rho[0], vxc, exc);
+    put(of, "Vh", vh.f.data(), nint);
+    put(of, "Vxc", vxc[0].f.data(), nint);
+    put(of, "E_xc", &exc, 1);
+    vpsl.f = V_local[0].f;
+    sb::update_vlocal(ctx, vh, vpsl, vxc);
+    tpsi.from_ref(zwf.data());  // tpsi was the Taylor step's scratch
+    sb::hpsi(ctx, tpsi, htpsi, sys);
+    htpsi.to_ref(buf.data());
+    put(of, "htpsi_scf", reinterpret_cast<const double*>(buf.data()), 2 * buf.size());
     ctx.sync();
   } catch (const std::exception& e) {
     std::fprintf(stderr, "host_mirror: %s\n", e.what());

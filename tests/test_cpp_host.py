@@ -78,6 +78,7 @@ def system_records(s, vec_Ac, zc):
         "ia_tbl": np.asarray(pp.ia_tbl, np.int32), "rinv_uvu": np.asarray(pp.rinv_uvu, np.float64),
         "zc": np.asarray(zc, np.complex128).view(np.float64),
         "zwf": zwf.ravel(order="F").view(np.float64),
+        "primitive_b": np.diag([2 * np.pi / (n * h) for n, h in zip(g.shape, g.hgs)]),
     }
 
 
@@ -116,3 +117,17 @@ def test_host_mirror_parity(tmp_path):
     assert S.rel_err(res["rho0"].reshape(rho[..., 0].shape, order="F"), rho[..., 0]) < TOL
     assert S.rel_err(orb("taylor"), O.taylor(s.psi, zc)) < TOL
     assert res["alias_code"][0] == 1.0  # SB200_ERR_INVALID_ARG
+    # hartree / exchange_correlation / update_vlocal of that density, then H psi with the new V_local
+    import oracle as OR
+    g = s.grid
+    brl = np.diag([2 * np.pi / (n * h) for n, h in zip(g.shape, g.hgs)])
+    r0 = rho[..., 0]
+    vh = OR.poisson_ft(r0, brl)
+    vxc, exc = OR.exc_cor_pz(r0, g.hvol)
+    assert S.rel_err(res["Vh"].reshape(r0.shape, order="F"), vh) < TOL
+    assert S.rel_err(res["Vxc"].reshape(r0.shape, order="F"), vxc) < TOL
+    assert abs(res["E_xc"][0] - exc) <= TOL * abs(exc)
+    import dataclasses
+    O2 = Oracle(dataclasses.replace(s, V_local=OR.update_vlocal(s.V_local[..., 0], vh, vxc[..., None])))
+    O2.set_vec_Ac(ac)
+    assert S.rel_err(orb("htpsi_scf"), O2.hpsi(s.psi)) < TOL

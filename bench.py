@@ -468,6 +468,10 @@ def main():
     if args.self_consistent:
         if not s.grid.periodic or s.nspin != 1:
             raise SystemExit("--self-consistent needs a periodic workload with one spin")
+        if world > 1:
+            # the density of every step would have to be summed over the k-point shards
+            # before the Hartree and XC potentials; the loop here holds all k-points
+            raise SystemExit("--self-consistent runs on one GPU (no per-step density all-reduce)")
         # cubic cell: primitive_b = 2 pi / L; V_local from rho(t=0), then the update every step
         brl = np.diag([2.0 * np.pi / (n * h) for n, h in zip(s.grid.shape, s.grid.hgs)])
         vpsl = torch.from_numpy(np.ascontiguousarray(s.V_local[..., 0].ravel(order="F"))).cuda(local)

@@ -336,6 +336,8 @@ int sb200_update_vlocal(sb200_ctx* ctx, const double* Vpsl, const double* Vh, co
  * rho(t=0)).  The Hartree solve uses the cell of the latest call that passed
  * primitive_b.  Periodic grids and nspin = 1 (else SB200_ERR_UNSUPPORTED);
  * enable = 0 returns to the fixed-potential loop (Vpsl, primitive_b unused).
+ * The density is that of the context's own orbitals: the context must hold
+ * every occupied orbital and k-point of the system (no sum across contexts).
  * Replaces: the yn_fix_func = 'n' branch of time_evolution_step
  * (src/rt/time_evolution_step.f90:160-207).                                    */
 int sb200_set_self_consistent(sb200_ctx* ctx, int enable, const double* Vpsl, const double primitive_b[9]);

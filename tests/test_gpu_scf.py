@@ -220,3 +220,30 @@ def test_rt_propagate_self_consistent(make, nt):
     ref2 = _oracle(s).rt_run(s.psi, 2, dt, zc, Ac_ext=Ac[:, :4])
     assert S.rel_err(ctx.download(res2["psi"]), ref2["psi"]) < TOL_LOOP
     ctx.close()
+
+
+def test_rt_propagate_self_consistent_mixed():
+    """The mixed form (FP32 terms n >= 2) in the self-consistent loop: the
+    update also refreshes the FP32 copy of V_local; J(t) stays within the
+    mixed form's budget (1e-6 relative) of the FP64 self-consistent loop."""
+    from salmon2_b200 import synth
+    from salmon2_b200.rt import Context
+
+    s = S.periodic_small()
+    nt, dt = 20, 0.08
+    Ac = synth.asin2cos(nt, dt, omega=0.05696, f0=0.05696 * 2e-2, tw=nt * dt)
+    zc = synth.taylor_zc(dt)
+    brl = _brl(s)
+    vpsl = np.array(s.V_local[..., 0])
+    out = {}
+    for prec in ("fp64", "mixed"):
+        ctx = Context(s, precision=prec)
+        a, b, w = ctx.upload(s.psi), ctx.zeros(), ctx.zeros()
+        ctx.update_potential(a, vpsl, brl)
+        ctx.set_self_consistent(True, vpsl, brl)
+        out[prec] = ctx.rt_propagate(a, b, w, nt, dt, zc, Ac_ext=Ac)["curr"]
+        ctx.close()
+    jmax = np.max(np.abs(out["fp64"]))
+    err = np.max(np.abs(out["mixed"] - out["fp64"])) / jmax
+    print("self-consistent loop, mixed vs FP64: J(t) rel err %.2e over %d steps" % (err, nt))
+    assert 0 < err <= 1e-6

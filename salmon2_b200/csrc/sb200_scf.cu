@@ -398,7 +398,8 @@ int scf_launch_update(sb200_ctx* c, const double* vpsl, const double* vh, const 
 int scf_rt_prepare(sb200_ctx* c) {
   ScfState* s = scf_of(c);
   if (!s || !s->rt_on) return SB200_OK;
-  if (s->npts != c->g.npts) return set_error(SB200_ERR_STATE, "grid changed since sb200_set_self_consistent");
+  if (s->npts != c->g.npts || s->num[0] != c->g.nx || s->num[1] != c->g.ny || s->num[2] != c->g.nz)
+    return set_error(SB200_ERR_STATE, "grid changed since sb200_set_self_consistent");
   return density_prepare(c);
 }
 

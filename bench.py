@@ -469,9 +469,14 @@ def main():
         if not s.grid.periodic or s.nspin != 1:
             raise SystemExit("--self-consistent needs a periodic workload with one spin")
         if world > 1:
-            # the density of every step would have to be summed over the k-point shards
-            # before the Hartree and XC potentials; the loop here holds all k-points
-            raise SystemExit("--self-consistent runs on one GPU (no per-step density all-reduce)")
+            # the density of every step is summed over the k-point shards (NCCL all-reduce
+            # inside the loop's graph) before the Hartree and XC potentials
+            from salmon2_b200.rt import nccl_unique_id
+            uid = torch.zeros(128, dtype=torch.uint8, device=f"cuda:{local}")
+            if rank == 0:
+                uid.copy_(torch.frombuffer(bytearray(nccl_unique_id()), dtype=torch.uint8))
+            dist.broadcast(uid, 0)
+            ctx.set_density_comm(world, rank, bytes(uid.cpu().numpy().tobytes()))
         # cubic cell: primitive_b = 2 pi / L; V_local from rho(t=0), then the update every step
         brl = np.diag([2.0 * np.pi / (n * h) for n, h in zip(s.grid.shape, s.grid.hgs)])
         vpsl = torch.from_numpy(np.ascontiguousarray(s.V_local[..., 0].ravel(order="F"))).cuda(local)

@@ -336,11 +336,25 @@ int sb200_update_vlocal(sb200_ctx* ctx, const double* Vpsl, const double* Vh, co
  * rho(t=0)).  The Hartree solve uses the cell of the latest call that passed
  * primitive_b.  Periodic grids and nspin = 1 (else SB200_ERR_UNSUPPORTED);
  * enable = 0 returns to the fixed-potential loop (Vpsl, primitive_b unused).
- * The density is that of the context's own orbitals: the context must hold
- * every occupied orbital and k-point of the system (no sum across contexts).
+ * The density is that of the context's own orbitals, summed over the k-point
+ * shards of other processes when sb200_set_density_comm gave the context a
+ * communicator.
  * Replaces: the yn_fix_func = 'n' branch of time_evolution_step
  * (src/rt/time_evolution_step.f90:160-207).                                    */
 int sb200_set_self_consistent(sb200_ctx* ctx, int enable, const double* Vpsl, const double primitive_b[9]);
+
+/* Density sum over k-point shards.  A job that gives each process (one per GPU)
+ * a share of the k-points needs the density of all of them before the Hartree
+ * and exchange-correlation potentials: with a communicator set,
+ * sb200_calc_density and the self-consistent loop all-reduce rho (NCCL, in the
+ * loop's CUDA graph) over the nranks processes.  id: 128 bytes from
+ * sb200_nccl_unique_id on rank 0, passed to every rank by the host (MPI_Bcast,
+ * torch.distributed).  nranks <= 0 removes the communicator.  NCCL is the
+ * process's libnccl.so.2, loaded at run time (absent: SB200_ERR_UNSUPPORTED).
+ * Replaces: comm_summation of rho over info%icomm_ko in calc_density
+ * (src/common/density_matrix.f90:223).                                         */
+int sb200_nccl_unique_id(unsigned char id[128]);
+int sb200_set_density_comm(sb200_ctx* ctx, int nranks, int rank, const unsigned char id[128]);
 
 /* ---- H psi without device allocation ---------------------------------------- */
 

@@ -63,6 +63,8 @@ SIGNATURES = {
     "sb200_hartree_periodic": (C.c_int, [_vp, _dp, _vp, _vp]),
     "sb200_update_vlocal": (C.c_int, [_vp, _vp, _vp, _vp]),
     "sb200_set_self_consistent": (C.c_int, [_vp, C.c_int, _vp, _dp]),
+    "sb200_nccl_unique_id": (C.c_int, [_vp]),
+    "sb200_set_density_comm": (C.c_int, [_vp, C.c_int, C.c_int, _vp]),
     "sb200_rt_propagate": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int, C.c_double, _dp, C.c_int, _dp, C.c_int, _dp,
                                      _dp, _dp, C.POINTER(C.c_void_p)]),
     "sb200_gs_from_ref": (C.c_int, [_vp, _vp, _vp]),

@@ -875,9 +875,11 @@ int sb200_calc_density(sb200_ctx* c, const double* psi, double* rho) {
   const size_t n = (size_t)c->g.npts * c->orb.nspin;
   if (is_device_ptr(rho)) {
     TRY(launch_density(c, (const double2*)psi, rho));
+    TRY(scf_density_allreduce(c, rho));
   } else {
     TRY(ensure_stage(c, n * sizeof(double)));
     TRY(launch_density(c, (const double2*)psi, (double*)c->d_stage));
+    TRY(scf_density_allreduce(c, (double*)c->d_stage));
     SB_CUDA(cudaMemcpyAsync(rho, c->d_stage, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   }
   SB_CUDA(cudaStreamSynchronize(c->stream));

@@ -249,5 +249,7 @@ void scf_free(sb200_ctx* c);
 // sb200_set_self_consistent enabled it)
 int scf_rt_prepare(sb200_ctx* c);
 int scf_rt_issue(sb200_ctx* c, const double2* psi);
+// sum of a device density over the k-point shards (no-op without a communicator)
+int scf_density_allreduce(sb200_ctx* c, double* d_rho);
 
 }  // namespace sb200

@@ -18,9 +18,12 @@
 // make each pass a few microseconds to tens of microseconds; the tables
 // (3 n^2 complex) and 4 pi / |G|^2 stay resident across steps.
 #include <cuda_runtime.h>
+#include <dlfcn.h>
+#include <nccl.h>
 
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -33,6 +36,35 @@ constexpr double SCF_PI = 3.141592653589793;
 constexpr int SCF_THREADS = 256;
 constexpr int SCF_XC_BLOCKS = 296;  // fixed: the E_xc partial sums have a fixed order
 constexpr int SCF_DFT_THREADS = 64;  // small blocks: a 16^3 pass spreads over 64 SMs
+
+// NCCL entry points, resolved at run time from the process's libnccl.so.2
+// (the one the host's torch / MPI stack already loaded, else the system's), so
+// the library carries no link-time NCCL dependency.
+struct NcclApi {
+  ncclResult_t (*get_unique_id)(ncclUniqueId*) = nullptr;
+  ncclResult_t (*comm_init_rank)(ncclComm_t*, int, ncclUniqueId, int) = nullptr;
+  ncclResult_t (*all_reduce)(const void*, void*, size_t, ncclDataType_t, ncclRedOp_t, ncclComm_t,
+                             cudaStream_t) = nullptr;
+  ncclResult_t (*comm_destroy)(ncclComm_t) = nullptr;
+  const char* (*error_string)(ncclResult_t) = nullptr;
+};
+
+const NcclApi* nccl_api() {
+  static NcclApi api;
+  static bool ok = false;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* h = dlopen("libnccl.so.2", RTLD_NOW | RTLD_GLOBAL);
+    if (!h) return;
+    api.get_unique_id = reinterpret_cast<decltype(api.get_unique_id)>(dlsym(h, "ncclGetUniqueId"));
+    api.comm_init_rank = reinterpret_cast<decltype(api.comm_init_rank)>(dlsym(h, "ncclCommInitRank"));
+    api.all_reduce = reinterpret_cast<decltype(api.all_reduce)>(dlsym(h, "ncclAllReduce"));
+    api.comm_destroy = reinterpret_cast<decltype(api.comm_destroy)>(dlsym(h, "ncclCommDestroy"));
+    api.error_string = reinterpret_cast<decltype(api.error_string)>(dlsym(h, "ncclGetErrorString"));
+    ok = api.get_unique_id && api.comm_init_rank && api.all_reduce && api.comm_destroy && api.error_string;
+  });
+  return ok ? &api : nullptr;
+}
 
 struct ScfState {
   long npts = 0;
@@ -54,6 +86,8 @@ struct ScfState {
   double* d_rho = nullptr;    // [npts]
   double* d_vh = nullptr;     // [npts]
   double* d_vxc = nullptr;    // [npts]
+  // density sum over k-point shards (sb200_set_density_comm)
+  ncclComm_t comm = nullptr;
 };
 
 ScfState* scf_of(sb200_ctx* c) { return static_cast<ScfState*>(c->scf); }
@@ -403,10 +437,21 @@ int scf_rt_prepare(sb200_ctx* c) {
   return density_prepare(c);
 }
 
+int scf_density_allreduce(sb200_ctx* c, double* d_rho) {
+  ScfState* s = scf_of(c);
+  if (!s || !s->comm) return SB200_OK;
+  const NcclApi* api = nccl_api();
+  const ncclResult_t r = api->all_reduce(d_rho, d_rho, (size_t)c->g.npts * c->orb.nspin, ncclFloat64, ncclSum,
+                                         s->comm, c->stream);
+  if (r != ncclSuccess) return set_error(SB200_ERR_CUDA, std::string("ncclAllReduce: ") + api->error_string(r));
+  return SB200_OK;
+}
+
 int scf_rt_issue(sb200_ctx* c, const double2* psi) {
   ScfState* s = scf_of(c);
   if (!s || !s->rt_on) return SB200_OK;
   TRY_S(launch_density(c, psi, s->d_rho, SB200_KIND_POTENTIAL));
+  TRY_S(scf_density_allreduce(c, s->d_rho));
   TRY_S(scf_launch_hartree(c, s->d_rho, s->d_vh, SB200_KIND_POTENTIAL));
   TRY_S(scf_launch_xc(c, s->d_rho, s->d_vxc, SB200_KIND_POTENTIAL, false));
   TRY_S(scf_launch_update(c, s->d_vpsl, s->d_vh, s->d_vxc, SB200_KIND_POTENTIAL));
@@ -428,6 +473,7 @@ void scf_free(sb200_ctx* c) {
   dfree(s->d_rho);
   dfree(s->d_vh);
   dfree(s->d_vxc);
+  if (s->comm) nccl_api()->comm_destroy(s->comm);
   delete s;
   c->scf = nullptr;
 }
@@ -505,6 +551,42 @@ int sb200_update_vlocal(sb200_ctx* c, const double* Vpsl, const double* Vh, cons
   SB_LAUNCH_CHECK("k_update_vlocal");
   SB_CUDA(cudaStreamSynchronize(c->stream));
   c->vloc_set = true;
+  return SB200_OK;
+}
+
+int sb200_nccl_unique_id(unsigned char id[128]) {
+  if (!id) return set_error(SB200_ERR_INVALID_ARG, "null argument");
+  static_assert(sizeof(ncclUniqueId) == 128, "NCCL unique id size");
+  const NcclApi* api = nccl_api();
+  if (!api) return set_error(SB200_ERR_UNSUPPORTED, "libnccl.so.2 could not be loaded");
+  ncclUniqueId u;
+  const ncclResult_t r = api->get_unique_id(&u);
+  if (r != ncclSuccess) return set_error(SB200_ERR_CUDA, std::string("ncclGetUniqueId: ") + api->error_string(r));
+  std::memcpy(id, &u, sizeof(u));
+  return SB200_OK;
+}
+
+int sb200_set_density_comm(sb200_ctx* c, int nranks, int rank, const unsigned char id[128]) {
+  TRY_S(scf_ready(c));
+  ScfDevGuard dg(c->device);
+  TRY_S(scf_ensure(c));
+  ScfState* s = scf_of(c);
+  const NcclApi* api = nccl_api();
+  if (s->comm) {
+    SB_CUDA(cudaStreamSynchronize(c->stream));
+    api->comm_destroy(s->comm);
+    s->comm = nullptr;
+  }
+  if (nranks <= 0) return SB200_OK;
+  if (!id || rank < 0 || rank >= nranks) return set_error(SB200_ERR_INVALID_ARG, "bad rank or null id");
+  if (!api) return set_error(SB200_ERR_UNSUPPORTED, "libnccl.so.2 could not be loaded");
+  ncclUniqueId u;
+  std::memcpy(&u, id, sizeof(u));
+  const ncclResult_t r = api->comm_init_rank(&s->comm, nranks, u, rank);
+  if (r != ncclSuccess) {
+    s->comm = nullptr;
+    return set_error(SB200_ERR_CUDA, std::string("ncclCommInitRank: ") + api->error_string(r));
+  }
   return SB200_OK;
 }
 

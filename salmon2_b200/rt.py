@@ -35,6 +35,13 @@ def _i3(v):
     return (C.c_int * 3)(*[int(x) for x in v])
 
 
+def nccl_unique_id() -> bytes:
+    """128-byte NCCL id (on rank 0) for :meth:`Context.set_density_comm`."""
+    buf = (C.c_ubyte * 128)()
+    check(lib().sb200_nccl_unique_id(buf))
+    return bytes(buf)
+
+
 class Context:
     """Device context for one orbital block (one ``(ik, io, ispin)`` set)."""
 
@@ -241,6 +248,12 @@ class Context:
         b = np.asfortranarray(primitive_b, dtype=np.float64)
         p, keep = self._scalar_field(vpsl)
         check(lib().sb200_set_self_consistent(self.h, 1, p, _ptr(b)))
+
+    def set_density_comm(self, nranks, rank, unique_id: bytes):
+        """All-reduce the density over `nranks` k-point shards (one process per
+        GPU) in calc_density and the self-consistent loop; nranks = 0 removes it."""
+        buf = (C.c_ubyte * 128).from_buffer_copy(unique_id) if unique_id is not None else None
+        check(lib().sb200_set_density_comm(self.h, int(nranks), int(rank), buf))
 
     def update_potential(self, psi, vpsl, primitive_b):
         """The self-consistent part of one time step on the device

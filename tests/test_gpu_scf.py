@@ -247,3 +247,33 @@ def test_rt_propagate_self_consistent_mixed():
     err = np.max(np.abs(out["mixed"] - out["fp64"])) / jmax
     print("self-consistent loop, mixed vs FP64: J(t) rel err %.2e over %d steps" % (err, nt))
     assert 0 < err <= 1e-6
+
+
+def test_density_comm_single_rank():
+    """A one-rank NCCL communicator: calc_density and the self-consistent loop
+    with the density all-reduce (inside the loop's CUDA graph) give exactly the
+    numbers of the same calls without it."""
+    from salmon2_b200 import synth
+    from salmon2_b200.rt import Context, nccl_unique_id
+
+    s = S.periodic_small()
+    nt, dt = 4, 0.08
+    Ac = synth.asin2cos(nt, dt, omega=0.05696, f0=0.05696 * 2e-2, tw=nt * dt)
+    zc = synth.taylor_zc(dt)
+    brl = _brl(s)
+    vpsl = np.array(s.V_local[..., 0])
+    got = {}
+    for comm in (False, True):
+        ctx = Context(s)
+        if comm:
+            ctx.set_density_comm(1, 0, nccl_unique_id())
+        a, b, w = ctx.upload(s.psi), ctx.zeros(), ctx.zeros()
+        rho = ctx.calc_density(a)
+        ctx.update_potential(a, vpsl, brl)
+        ctx.set_self_consistent(True, vpsl, brl)
+        r = ctx.rt_propagate(a, b, w, nt, dt, zc, Ac_ext=Ac)
+        got[comm] = (rho, r["curr"], ctx.download(r["psi"]))
+        ctx.set_density_comm(0, 0, None)
+        ctx.close()
+    for x, y in zip(got[False], got[True]):
+        assert np.array_equal(x, y)

@@ -61,3 +61,77 @@ def test_two_rank_current_equals_merged_kmesh(tmp_path):
     Ac, zc = _field()
     j_merged = Oracle(merged, threads=1).rt_run(merged.psi, NT, DT, zc, Ac_ext=Ac)["curr"]
     assert np.max(np.abs(j_ranks - j_merged)) <= 1e-12 * np.max(np.abs(j_merged))
+
+
+def _scf_rank_main(rank, world, port, out):
+    """One k-point shard of the self-consistent loop: per step the Taylor step
+    of the shard's orbitals, the shard densities summed over the ranks (the
+    all-reduce the library issues with sb200_set_density_comm), then the
+    Hartree, PZ-LDA and V_local of the summed density."""
+    import torch
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    import oracle as OR
+    from oracle import Oracle
+    from salmon2_b200 import synth
+    s = synth.kpoint_shard(_system(), rank, world, 10.26, 1)
+    s = dataclasses.replace(s, V_local=np.array(s.V_local, order="F"))
+    O = Oracle(s, threads=1)
+    _, zc = _field()
+    g = s.grid
+    brl = OR.primitive_b_orthogonal([n * h for n, h in zip(g.shape, g.hgs)])
+    vpsl = np.array(s.V_local[..., 0])
+
+    def summed_density(psi):
+        t = torch.from_numpy(np.ascontiguousarray(O.density(psi)[..., 0]))
+        dist.all_reduce(t)
+        return t.numpy()
+
+    def set_potential(rho):
+        vxc, _ = OR.exc_cor_pz(rho, g.hvol)
+        O.V[...] = OR.update_vlocal(vpsl, OR.poisson_ft(rho, brl), vxc[..., None])
+
+    psi = s.psi
+    set_potential(summed_density(psi))
+    for _ in range(NT):
+        psi = O.taylor(psi, zc)
+        rho = summed_density(psi)
+        set_potential(rho)
+    if rank == 0:
+        np.save(out, rho)
+    dist.destroy_process_group()
+
+
+def test_two_rank_self_consistent_density_equals_merged_kmesh(tmp_path):
+    """The self-consistent loop over two k-point shards, each with the
+    all-reduced density, equals one loop over the merged k-mesh (the oracle's
+    sbo_rt_run_scf): the density after the last step."""
+    import socket
+
+    import torch.multiprocessing as mp
+    import oracle as OR
+    from oracle import Oracle
+    from salmon2_b200 import synth
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    out = str(tmp_path / "rho.npy")
+    mp.start_processes(_scf_rank_main, args=(2, port, out), nprocs=2, join=True, start_method="spawn")
+    rho_ranks = np.load(out)
+    base = _system()
+    sh = [synth.kpoint_shard(base, r, 2, 10.26, 1) for r in range(2)]
+    merged = dataclasses.replace(
+        base, nk=2, vec_k=np.asfortranarray(np.concatenate([x.vec_k for x in sh], axis=1)),
+        wtk=np.concatenate([x.wtk for x in sh]),
+        rocc=np.asfortranarray(np.concatenate([x.rocc for x in sh], axis=1)),
+        psi=np.asfortranarray(np.concatenate([x.psi for x in sh], axis=5)))
+    O = Oracle(merged, threads=1)
+    g = merged.grid
+    brl = OR.primitive_b_orthogonal([n * h for n, h in zip(g.shape, g.hgs)])
+    vpsl = np.array(merged.V_local[..., 0])
+    rho0 = O.density(merged.psi)[..., 0]
+    v0 = OR.update_vlocal(vpsl, OR.poisson_ft(rho0, brl), OR.exc_cor_pz(rho0, g.hvol)[0][..., None])[..., 0]
+    _, zc = _field()
+    ref = O.rt_run_scf(merged.psi, NT, DT, zc, vpsl, brl, v0)
+    assert np.max(np.abs(rho_ranks - ref["rho"][..., 0])) <= 1e-12 * np.max(np.abs(ref["rho"]))

@@ -195,6 +195,19 @@ module salmon_b200
       real(c_double), intent(in) :: primitive_b(3, 3)
     end function
 
+    ! rho summed over the k-point processes (comm_summation over icomm_ko)
+    integer(c_int) function sb200_nccl_unique_id(id) bind(c, name="sb200_nccl_unique_id")
+      import
+      integer(c_signed_char), intent(inout) :: id(128)
+    end function
+
+    integer(c_int) function sb200_set_density_comm(ctx, nranks, rank, id) bind(c, name="sb200_set_density_comm")
+      import
+      type(c_ptr), value :: ctx
+      integer(c_int), value :: nranks, rank
+      integer(c_signed_char), intent(in) :: id(128)
+    end function
+
     integer(c_int) function sb200_rt_propagate(ctx, psi_a, psi_b, work, nt, dt, zc, n_hamil, Ac_ext, &
                                                trans_longi, curr, rbox, Ac_tot, psi_final) &
         bind(c, name="sb200_rt_propagate")

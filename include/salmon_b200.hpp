@@ -236,6 +236,20 @@ inline void update_vlocal(context& ctx, const s_scalar& Vh, const s_scalar& Vpsl
   check(sb200_update_vlocal(ctx.get(), Vpsl.f.data(), Vh.f.data(), x.data()), "update_vlocal");
 }
 
+// yn_fix_func = 'n' (time_evolution_step.f90:160-207): sb200_rt_propagate recomputes
+// V_local = Vpsl + Vh[rho] + Vxc[rho] after every step; enable = false: fixed potential
+inline void set_self_consistent(context& ctx, bool enable, const s_scalar& Vpsl, const double primitive_b[9]) {
+  check(sb200_set_self_consistent(ctx.get(), enable ? 1 : 0, enable ? Vpsl.f.data() : nullptr,
+                                  enable ? primitive_b : nullptr),
+        "set_self_consistent");
+}
+
+// rho summed over the processes that share the k-points (comm_summation over
+// icomm_ko, density_matrix.f90:223): id from sb200_nccl_unique_id on rank 0
+inline void set_density_comm(context& ctx, int nranks, int rank, const unsigned char id[128]) {
+  check(sb200_set_density_comm(ctx.get(), nranks, rank, id), "set_density_comm");
+}
+
 // gram_schmidt(system, mg, info, psi) for complex orbitals (gram_schmidt_orth.f90:1069)
 inline void gram_schmidt(context& ctx, s_orbital& psi) {
   check(sb200_gram_schmidt_complex(ctx.get(), psi.data()), "gram_schmidt");

@@ -262,6 +262,8 @@ class Context:
         V_local = Vpsl + Vh + Vxc.  vpsl: a device tensor (nx*ny*nz, x fastest)
         or a numpy array.  Nothing is copied to the host; returns E_xc."""
         torch = self.torch
+        if self.sys.nspin != 1:
+            raise SB200Error(3, "update_potential: the PZ potential here is the nspin = 1 form")
         n = int(np.prod(self.sys.grid.shape))
         if getattr(self, "_pot_buf", None) is None:
             self._pot_buf = torch.empty((3, n), dtype=torch.float64, device=f"cuda:{self.device}")

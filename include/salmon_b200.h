@@ -321,6 +321,15 @@ int sb200_exc_cor_pz(sb200_ctx* ctx, const double* rho, double* Vxc, double* E_x
  * tables of src/common/initialization.f90:632-776.                             */
 int sb200_hartree_periodic(sb200_ctx* ctx, const double primitive_b[9], const double* rho, double* Vh);
 
+/* Vh(is:ie) of rho on an isolated grid: the density placed in the corner of a
+ * doubled box, separable transforms of length 2n, 4 pi / |G|^2 of the doubled
+ * cell (G = 0 dropped), inverse transforms, the corner kept.  primitive_b of the
+ * box (orthogonal: 2 pi / L_d on the diagonal).  Periodic grids:
+ * SB200_ERR_UNSUPPORTED.  Replaces: hartree with method_poisson = 'ft' on an
+ * isolated system -> poisson_isolated_ft (src/poisson/poisson_isolated.f90:692-836;
+ * tables init_reciprocal_grid_isolated_ft, src/common/initialization.f90:823-1077). */
+int sb200_hartree_isolated_ft(sb200_ctx* ctx, const double primitive_b[9], const double* rho, double* Vh);
+
 /* V_local(is) = Vpsl + Vh + Vxc(is) written into the context's device copy of
  * V_local (FP64 and the FP32 copy of the mixed form); Vpsl, Vh (is:ie), Vxc
  * (is:ie, nspin).  Also serves as the first sb200_set_vlocal.
@@ -333,8 +342,9 @@ int sb200_update_vlocal(sb200_ctx* ctx, const double* Vpsl, const double* Vh, co
  * time_evolution_step with yn_fix_func = 'n', inside the loop's CUDA graph; the
  * next step's Taylor expansion uses the updated V_local.  The first step uses
  * the V_local already set (sb200_set_vlocal, or sb200_update_vlocal from
- * rho(t=0)).  The Hartree solve uses the cell of the latest call that passed
- * primitive_b.  Periodic grids and nspin = 1 (else SB200_ERR_UNSUPPORTED);
+ * rho(t=0)).  The Hartree solve (poisson_ft on periodic grids,
+ * poisson_isolated_ft on isolated ones) uses the cell of the latest call that
+ * passed primitive_b.  nspin = 1 (else SB200_ERR_UNSUPPORTED);
  * enable = 0 returns to the fixed-potential loop (Vpsl, primitive_b unused).
  * The density is that of the context's own orbitals, summed over the k-point
  * shards of other processes when sb200_set_density_comm gave the context a

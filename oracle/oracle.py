@@ -60,7 +60,8 @@ def lib():
                      "sbo_calc_Ac_ext_t", "sbo_rt_run", "sbo_set_threads", "sbo_get_threads",
                      "sbo_precond_real", "sbo_gscg_rwf", "sbo_gram_schmidt_real", "sbo_gram_schmidt_complex",
                      "sbo_subspace_diag_real", "sbo_inner_product_real", "sbo_exc_cor_pz", "sbo_poisson_coef",
-                     "sbo_dft_table", "sbo_poisson_ft", "sbo_update_vlocal", "sbo_rt_run_scf"):
+                     "sbo_dft_table", "sbo_poisson_ft", "sbo_update_vlocal", "sbo_rt_run_scf",
+                     "sbo_poisson_isolated_ft"):
             getattr(L, name)
         L.sbo_rt_run.restype = C.c_int
         L.sbo_rt_run_scf.restype = C.c_int
@@ -240,7 +241,7 @@ class Oracle:
 
     def rt_run_scf(self, psi0, nt, dt, zc, vpsl, brl, v0, Ac_ext=None, trans_longi=0):
         """rt_run with the self-consistent potential update every step
-        (time_evolution_step.f90:184-207; periodic, nspin = 1).  v0: V_local
+        (time_evolution_step.f90:184-207; nspin = 1, periodic or isolated).  v0: V_local
         (nx, ny, nz) for the first step.  The oracle's own V_local is untouched."""
         a = self._orb(psi0).copy(order="F")
         b = np.zeros_like(a, order="F")
@@ -260,7 +261,7 @@ class Oracle:
         which = lib().sbo_rt_run_scf(C.byref(self.s), _p(a), _p(b), _p(work), C.c_int(nt), C.c_double(dt),
                                      _p(zc), C.c_int(len(zc)), _p(Ac_ext), _p(Ac_ind), _p(Ac_tot),
                                      C.c_int(trans_longi), _p(curr), _p(rbox), _p(rho), _p(vp), _p(bb), _p(vl))
-        assert which in (0, 1), "rt_run_scf needs a periodic nspin = 1 system"
+        assert which in (0, 1), "rt_run_scf needs an nspin = 1 system"
         psi = a if which == 0 else b
         return dict(psi=psi, curr=curr, rbox=rbox, Ac_tot=Ac_tot, rho=rho,
                     V_local=vl.reshape(self.sys.grid.shape, order="F"))
@@ -347,6 +348,18 @@ def poisson_ft(rho, brl):
     n = np.asarray(np.shape(rho), dtype=np.int32)
     b = np.ascontiguousarray(np.asarray(brl, dtype=np.float64).ravel(order="F"))
     lib().sbo_poisson_ft(n.ctypes.data_as(C.POINTER(C.c_int)), _p(b), _p(r), _p(v))
+    return v.reshape(np.shape(rho), order="F")
+
+
+def poisson_isolated_ft(rho, brl):
+    """Isolated Hartree potential by transforms on a doubled box
+    (poisson_isolated_ft, poisson_isolated.f90:692-836).  rho: (nx, ny, nz)
+    interior, Fortran order; brl: (3,3) primitive_b of the (orthogonal) box."""
+    r = _flat_f(rho)
+    v = np.zeros_like(r)
+    n = np.asarray(np.shape(rho), dtype=np.int32)
+    b = np.ascontiguousarray(np.asarray(brl, dtype=np.float64).ravel(order="F"))
+    lib().sbo_poisson_isolated_ft(n.ctypes.data_as(C.POINTER(C.c_int)), _p(b), _p(r), _p(v))
     return v.reshape(np.shape(rho), order="F")
 
 

@@ -628,7 +628,8 @@ void sbo_calc_Ac_ext_t(int shape, double t0, double delta_t, int is, int ie, con
 // (yn_fix_func='y' path: V_local fixed), middlepoint propagator.
 // The self-consistent variant (sbo_rt_run_scf): after the density, the
 // Hartree and exchange-correlation potentials of rho(t+dt) and update_vlocal,
-// time_evolution_step.f90:184-207 with yn_fix_func = 'n' (periodic, nspin = 1).
+// time_evolution_step.f90:184-207 with yn_fix_func = 'n' (nspin = 1; Hartree by
+// poisson_ft on periodic grids, poisson_isolated_ft on isolated ones).
 struct ScfUpdate {
   const double* vpsl;
   const double* brl;
@@ -655,7 +656,10 @@ static int rt_run_impl(sbo_system* s, double* psi_a, double* psi_b, double* work
     if (scf) {
       const int num[3] = {s->ie[0] - s->is[0] + 1, s->ie[1] - s->is[1] + 1, s->ie[2] - s->is[2] + 1};
       double exc = 0.0;
-      sbo_poisson_ft(num, scf->brl, rho_work, vh.data());
+      if (s->periodic)
+        sbo_poisson_ft(num, scf->brl, rho_work, vh.data());
+      else
+        sbo_poisson_isolated_ft(num, scf->brl, rho_work, vh.data());
       sbo_exc_cor_pz(npts, rho_work, s->hvol, vxc.data(), &exc);
       sbo_update_vlocal(npts, 1, scf->vpsl, vh.data(), vxc.data(), scf->vloc);
     }
@@ -697,7 +701,7 @@ int sbo_rt_run_scf(sbo_system* s, double* psi_a, double* psi_b, double* work, in
                    const double* zc, int n_hamil, const double* Ac_ext, double* Ac_ind,
                    double* Ac_tot, int trans_longi, double* curr, double* rbox, double* rho_work,
                    const double* vpsl, const double brl[9], double* vloc) {
-  if (!s->periodic || s->nspin != 1) return -1;
+  if (s->nspin != 1) return -1;
   const ScfUpdate u{vpsl, brl, vloc};
   const double* saved = s->V_local;
   s->V_local = vloc;

@@ -157,10 +157,11 @@ void sbo_exc_cor_pz(long n, const double* rho, double hvol, double* vxc, double*
 void sbo_poisson_coef(const int num[3], const double brl[9], double* coef);
 void sbo_dft_table(int n, double* eg);
 void sbo_poisson_ft(const int num[3], const double brl[9], const double* rho, double* vh);
+void sbo_poisson_isolated_ft(const int num[3], const double brl[9], const double* rho, double* vh);
 void sbo_update_vlocal(long n, int nspin, const double* vpsl, const double* vh, const double* vxc, double* vloc);
-/* sbo_rt_run with the self-consistent potential update every step (periodic,
- * nspin = 1): vloc holds V_local on entry and is rewritten each step as
- * Vpsl + Vh[rho] + Vxc[rho]; returns -1 for other systems.                    */
+/* sbo_rt_run with the self-consistent potential update every step (nspin = 1;
+ * periodic or isolated Hartree by transforms): vloc holds V_local on entry and
+ * is rewritten each step as Vpsl + Vh[rho] + Vxc[rho]; returns -1 for nspin 2. */
 int sbo_rt_run_scf(sbo_system* s, double* psi_a, double* psi_b, double* work, int nt, double dt,
                    const double* zc, int n_hamil, const double* Ac_ext, double* Ac_ind,
                    double* Ac_tot, int trans_longi, double* curr, double* rbox, double* rho_work,

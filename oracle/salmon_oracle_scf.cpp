@@ -150,6 +150,78 @@ void sbo_poisson_ft(const int num[3], const double brl[9], const double* rho, do
   for (long p = 0; p < n; ++p) vh[p] = b[2 * p];
 }
 
+// poisson_isolated_ft, src/poisson/poisson_isolated.f90:692-836 (one process),
+// with the tables of init_reciprocal_grid_isolated_ft (src/common/initialization.f90:
+// 823-1077): rho placed in the corner of a doubled (2nx, 2ny, 2nz) box of zeros,
+// forward transforms along z, y, x of size 2n, division by 8 nx ny nz,
+// multiplication by 4 pi / |G|^2 of the doubled cell (G = fold(k) b_d / 2,
+// G = 0 dropped), inverse transforms along z, y, x, Vh = real part on the
+// original nx x ny x nz corner.  Only the corner rows that carry data are formed
+// and only those summed, as the reference's loop bounds do.  The reference's
+// tables repeat the first n columns in the second n (egx(k, i + n) = egx(k, i));
+// those columns only ever multiply the zero half, so the plain exp(2 pi i j k / 2n)
+// is used for all j.  brl: primitive_b (3x3, diagonal for this box).
+void sbo_poisson_isolated_ft(const int num[3], const double brl[9], const double* rho, double* vh) {
+  const int n0[3] = {num[0], num[1], num[2]};
+  const int m[3] = {2 * num[0], 2 * num[1], 2 * num[2]};
+  const long M = (long)m[0] * m[1] * m[2];
+  std::vector<double> eg[3];
+  for (int d = 0; d < 3; ++d) {
+    eg[d].resize(2L * m[d] * m[d]);
+    sbo_dft_table(m[d], eg[d].data());
+  }
+  std::vector<double> a(2 * M, 0.0), b(2 * M, 0.0);
+  auto at = [&](int x, int y, int z) { return (long)x + (long)m[0] * (y + (long)m[1] * z); };
+  // one pass over the box [0,bx) x [0,by) x [0,bz) of outputs, summing the
+  // first nsum inputs along `axis`
+  auto pass = [&](const double* in, double* out, int axis, bool conj, int bx, int by, int bz, int nsum) {
+    const double* T = eg[axis].data();
+    const int na = m[axis];
+    const double sg = conj ? -1.0 : 1.0;
+#pragma omp parallel for collapse(2)
+    for (int z = 0; z < bz; ++z)
+      for (int y = 0; y < by; ++y)
+        for (int x = 0; x < bx; ++x) {
+          const int k = axis == 0 ? x : axis == 1 ? y : z;
+          double re = 0.0, im = 0.0;
+          for (int j = 0; j < nsum; ++j) {
+            const long q = axis == 0 ? at(j, y, z) : axis == 1 ? at(x, j, z) : at(x, y, j);
+            const double tr = T[2 * ((long)k * na + j)], ti = sg * T[2 * ((long)k * na + j) + 1];
+            const double vr = in[2 * q], vi = in[2 * q + 1];
+            re = re + (tr * vr - ti * vi);
+            im = im + (tr * vi + ti * vr);
+          }
+          const long p = at(x, y, z);
+          out[2 * p] = re;
+          out[2 * p + 1] = im;
+        }
+  };
+  for (int z = 0; z < n0[2]; ++z)
+    for (int y = 0; y < n0[1]; ++y)
+      for (int x = 0; x < n0[0]; ++x) a[2 * at(x, y, z)] = rho[x + (long)n0[0] * (y + (long)n0[1] * z)];
+  pass(a.data(), b.data(), 2, true, n0[0], n0[1], m[2], n0[2]);
+  pass(b.data(), a.data(), 1, true, n0[0], m[1], m[2], n0[1]);
+  pass(a.data(), b.data(), 0, true, m[0], m[1], m[2], n0[0]);
+  const double ntot = 8.0 * n0[0] * n0[1] * n0[2];
+  for (int z = 0; z < m[2]; ++z)
+    for (int y = 0; y < m[1]; ++y)
+      for (int x = 0; x < m[0]; ++x) {
+        const long p = at(x, y, z);
+        const int ix = fold(x, m[0]), iy = fold(y, m[1]), iz = fold(z, m[2]);
+        const double g0 = (double)ix * brl[0] / 2.0, g1 = (double)iy * brl[4] / 2.0, g2 = (double)iz * brl[8] / 2.0;
+        const double G2 = g0 * g0 + g1 * g1 + g2 * g2;
+        const double cf = (ix == 0 && iy == 0 && iz == 0) ? 0.0 : 4.0 * PI / G2;
+        b[2 * p] = cf * (b[2 * p] / ntot);
+        b[2 * p + 1] = cf * (b[2 * p + 1] / ntot);
+      }
+  pass(b.data(), a.data(), 2, false, m[0], m[1], n0[2], m[2]);
+  pass(a.data(), b.data(), 1, false, m[0], n0[1], n0[2], m[1]);
+  pass(b.data(), a.data(), 0, false, n0[0], n0[1], n0[2], m[0]);
+  for (int z = 0; z < n0[2]; ++z)
+    for (int y = 0; y < n0[1]; ++y)
+      for (int x = 0; x < n0[0]; ++x) vh[x + (long)n0[0] * (y + (long)n0[1] * z)] = a[2 * at(x, y, z)];
+}
+
 // update_vlocal, src/common/hamiltonian.f90:813-843: V_local(is) = Vpsl + Vh + Vxc(is).
 void sbo_update_vlocal(long n, int nspin, const double* vpsl, const double* vh, const double* vxc, double* vloc) {
   for (int is = 0; is < nspin; ++is)

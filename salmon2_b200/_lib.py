@@ -62,6 +62,7 @@ SIGNATURES = {
     "sb200_exc_cor_pz": (C.c_int, [_vp, _vp, _vp, _dp]),
     "sb200_hartree_periodic": (C.c_int, [_vp, _dp, _vp, _vp]),
     "sb200_update_vlocal": (C.c_int, [_vp, _vp, _vp, _vp]),
+    "sb200_hartree_isolated_ft": (C.c_int, [_vp, _dp, _vp, _vp]),
     "sb200_set_self_consistent": (C.c_int, [_vp, C.c_int, _vp, _dp]),
     "sb200_nccl_unique_id": (C.c_int, [_vp]),
     "sb200_set_density_comm": (C.c_int, [_vp, C.c_int, C.c_int, _vp]),

@@ -88,6 +88,13 @@ struct ScfState {
   double* d_vxc = nullptr;    // [npts]
   // density sum over k-point shards (sb200_set_density_comm)
   ncclComm_t comm = nullptr;
+  // isolated grids: transforms on the doubled box (sb200_hartree_isolated_ft)
+  double2* d_ia = nullptr;    // [8 npts] complex work
+  double2* d_ib = nullptr;    // [8 npts] complex work
+  double* d_icoef = nullptr;  // [8 npts] 4 pi / |G|^2 of the doubled cell
+  double2* d_itab = nullptr;  // tables of length 2nx, 2ny, 2nz
+  bool have_icoef = false;
+  double ibrl[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
 };
 
 ScfState* scf_of(sb200_ctx* c) { return static_cast<ScfState*>(c->scf); }
@@ -302,6 +309,65 @@ __global__ void __launch_bounds__(SCF_DFT_THREADS) k_dft_pass(const double2* __r
   }
 }
 
+// One pass of the isolated solve on the doubled (mx, my, mz) box: outputs on
+// the corner box [0,bx) x [0,by) x [0,bz), each the ordered sum over the first
+// nsum inputs along `axis` of T(k, j) * in(j), T the exp(+-2 pi i jk / ma) table
+// of the axis (sg = -1: conjugate).  in_real / out_real: the (rx, ry, .) interior
+// array (the density in, Vh out) instead of the doubled complex one.
+__global__ void __launch_bounds__(SCF_DFT_THREADS) k_dft_box(const double2* __restrict__ in,
+                                                         const double* __restrict__ in_real,
+                                                         double2* __restrict__ out, double* __restrict__ out_real,
+                                                         const double2* __restrict__ T, double sg, int mx, int my,
+                                                         int bx, int by, int bz, int axis, int nsum, int ma,
+                                                         const double* __restrict__ coef, double ntot, int rx,
+                                                         int ry) {
+  const long nb = (long)bx * by * bz;
+  for (long p = blockIdx.x * (long)SCF_DFT_THREADS + threadIdx.x; p < nb; p += (long)gridDim.x * SCF_DFT_THREADS) {
+    const int x = (int)(p % bx);
+    const long r = p / bx;
+    const int y = (int)(r % by);
+    const int z = (int)(r / by);
+    const int k = axis == 0 ? x : axis == 1 ? y : z;
+    // input index of j = 0 along the axis, and the stride along it
+    const int ix = axis == 0 ? 0 : x, iy = axis == 1 ? 0 : y, iz = axis == 2 ? 0 : z;
+    long base, stride;
+    if (in_real) {
+      base = ix + (long)rx * (iy + (long)ry * iz);
+      stride = axis == 0 ? 1 : axis == 1 ? rx : (long)rx * ry;
+    } else {
+      base = ix + (long)mx * (iy + (long)my * iz);
+      stride = axis == 0 ? 1 : axis == 1 ? mx : (long)mx * my;
+    }
+    const double2* Tk = T + (long)k * ma;
+    double re = 0.0, im = 0.0;
+#pragma unroll 4
+    for (int j = 0; j < nsum; ++j) {
+      const double2 t = Tk[j];
+      const double ti = sg * t.y;
+      double vr, vi;
+      if (in_real) {
+        vr = in_real[base + (long)j * stride];
+        vi = 0.0;
+      } else {
+        const double2 v = in[base + (long)j * stride];
+        vr = v.x;
+        vi = v.y;
+      }
+      re = re + (t.x * vr - ti * vi);
+      im = im + (t.x * vi + ti * vr);
+    }
+    if (coef) {
+      const double cf = coef[x + (long)mx * (y + (long)my * z)];
+      re = cf * (re / ntot);
+      im = cf * (im / ntot);
+    }
+    if (out_real)
+      out_real[x + (long)rx * (y + (long)ry * z)] = re;
+    else
+      out[x + (long)mx * (y + (long)my * z)] = make_double2(re, im);
+  }
+}
+
 // V_local(is) = Vpsl + Vh + Vxc(is), FP64 and its FP32 copy.
 __global__ void k_update_vlocal(const double* __restrict__ vpsl, const double* __restrict__ vh,
                                 const double* __restrict__ vxc, double* __restrict__ v, float* __restrict__ v32,
@@ -361,6 +427,52 @@ int scf_tables(sb200_ctx* c, const double brl[9]) {
   return SB200_OK;
 }
 
+// Doubled-box tables of init_reciprocal_grid_isolated_ft
+// (src/common/initialization.f90:823-1077): exp(i 2 pi j k / 2n) per axis and
+// 4 pi / |G|^2 with G_d = fold(k_d, 2n_d) b_d / 2 (zero at G = 0).  The
+// reference's tables repeat the first n columns in the second n; those columns
+// only multiply the zero half of the box, so the plain table is used.
+int scf_itables(sb200_ctx* c, const double brl[9]) {
+  ScfState* s = scf_of(c);
+  const int mx = 2 * s->num[0], my = 2 * s->num[1], mz = 2 * s->num[2];
+  const size_t M = (size_t)mx * my * mz;
+  if (!s->d_itab) {
+    const size_t nt = (size_t)mx * mx + (size_t)my * my + (size_t)mz * mz;
+    TRY_S(dalloc(&s->d_itab, nt));
+    std::vector<double2> tab(nt);
+    size_t o = 0;
+    for (int n : {mx, my, mz}) {
+      for (int k = 0; k < n; ++k)
+        for (int i = 0; i < n; ++i) {
+          const double a = 2.0 * SCF_PI * (double)(i * k) / (double)n;
+          tab[o + (size_t)k * n + i] = make_double2(std::cos(a), std::sin(a));
+        }
+      o += (size_t)n * n;
+    }
+    SB_CUDA(cudaMemcpyAsync(s->d_itab, tab.data(), nt * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
+    SB_CUDA(cudaStreamSynchronize(c->stream));
+  }
+  if (!s->d_ia) TRY_S(dalloc(&s->d_ia, M));
+  if (!s->d_ib) TRY_S(dalloc(&s->d_ib, M));
+  if (s->have_icoef && std::memcmp(s->ibrl, brl, sizeof(s->ibrl)) == 0) return SB200_OK;
+  if (!s->d_icoef) TRY_S(dalloc(&s->d_icoef, M));
+  std::vector<double> coef(M);
+  for (int kz = 0; kz < mz; ++kz)
+    for (int ky = 0; ky < my; ++ky)
+      for (int kx = 0; kx < mx; ++kx) {
+        const int iix = fold_index(kx, mx), iiy = fold_index(ky, my), iiz = fold_index(kz, mz);
+        const double g0 = (double)iix * brl[0] / 2.0, g1 = (double)iiy * brl[4] / 2.0, g2 = (double)iiz * brl[8] / 2.0;
+        const double G2 = g0 * g0 + g1 * g1 + g2 * g2;
+        coef[kx + (size_t)mx * (ky + (size_t)my * kz)] =
+            (iix == 0 && iiy == 0 && iiz == 0) ? 0.0 : 4.0 * SCF_PI / G2;
+      }
+  SB_CUDA(cudaMemcpyAsync(s->d_icoef, coef.data(), M * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  SB_CUDA(cudaStreamSynchronize(c->stream));
+  std::memcpy(s->ibrl, brl, sizeof(s->ibrl));
+  s->have_icoef = true;
+  return SB200_OK;
+}
+
 // ---- launch sequences (no host synchronisation: also issued inside the
 // CUDA graph of the time loop) ---------------------------------------------------
 
@@ -399,6 +511,43 @@ int scf_launch_hartree(sb200_ctx* c, const double* d_rho, double* d_vh, int kind
     TRY_S(scf_mark(c, kind, true));
     k_dft_pass<<<gb, SCF_DFT_THREADS, 0, c->stream>>>(p.in, p.in_real, p.out, p.out_real, p.T, p.sg, nx, ny, nz,
                                                        p.axis, p.coef, ntot);
+    TRY_S(scf_mark(c, kind, false));
+  }
+  return SB200_OK;
+}
+
+// poisson_isolated_ft's six passes on the doubled box (only the corner rows
+// that carry data formed, as the reference's loop bounds)
+int scf_launch_hartree_isolated(sb200_ctx* c, const double* d_rho, double* d_vh, int kind) {
+  ScfState* s = scf_of(c);
+  const int nx = s->num[0], ny = s->num[1], nz = s->num[2];
+  const int mx = 2 * nx, my = 2 * ny, mz = 2 * nz;
+  const double2* tx = s->d_itab;
+  const double2* ty = tx + (size_t)mx * mx;
+  const double2* tz = ty + (size_t)my * my;
+  const double ntot = 8.0 * (double)nx * ny * nz;
+  struct Pass {
+    const double2* in;
+    const double* in_real;
+    double2* out;
+    double* out_real;
+    const double2* T;
+    double sg;
+    int bx, by, bz, axis, nsum, ma;
+    const double* coef;
+  } passes[6] = {{nullptr, d_rho, s->d_ia, nullptr, tz, -1.0, nx, ny, mz, 2, nz, mz, nullptr},
+                 {s->d_ia, nullptr, s->d_ib, nullptr, ty, -1.0, nx, my, mz, 1, ny, my, nullptr},
+                 {s->d_ib, nullptr, s->d_ia, nullptr, tx, -1.0, mx, my, mz, 0, nx, mx, s->d_icoef},
+                 {s->d_ia, nullptr, s->d_ib, nullptr, tz, 1.0, mx, my, nz, 2, mz, mz, nullptr},
+                 {s->d_ib, nullptr, s->d_ia, nullptr, ty, 1.0, mx, ny, nz, 1, my, my, nullptr},
+                 {s->d_ia, nullptr, nullptr, d_vh, tx, 1.0, nx, ny, nz, 0, mx, mx, nullptr}};
+  for (const Pass& p : passes) {
+    long nb = ((long)p.bx * p.by * p.bz + SCF_DFT_THREADS - 1) / SCF_DFT_THREADS;
+    if (nb > 148L * 16) nb = 148L * 16;
+    TRY_S(scf_mark(c, kind, true));
+    k_dft_box<<<(int)nb, SCF_DFT_THREADS, 0, c->stream>>>(p.in, p.in_real, p.out, p.out_real, p.T, p.sg, mx, my,
+                                                           p.bx, p.by, p.bz, p.axis, p.nsum, p.ma, p.coef, ntot,
+                                                           nx, ny);
     TRY_S(scf_mark(c, kind, false));
   }
   return SB200_OK;
@@ -452,7 +601,10 @@ int scf_rt_issue(sb200_ctx* c, const double2* psi) {
   if (!s || !s->rt_on) return SB200_OK;
   TRY_S(launch_density(c, psi, s->d_rho, SB200_KIND_POTENTIAL));
   TRY_S(scf_density_allreduce(c, s->d_rho));
-  TRY_S(scf_launch_hartree(c, s->d_rho, s->d_vh, SB200_KIND_POTENTIAL));
+  if (c->g.periodic)
+    TRY_S(scf_launch_hartree(c, s->d_rho, s->d_vh, SB200_KIND_POTENTIAL));
+  else
+    TRY_S(scf_launch_hartree_isolated(c, s->d_rho, s->d_vh, SB200_KIND_POTENTIAL));
   TRY_S(scf_launch_xc(c, s->d_rho, s->d_vxc, SB200_KIND_POTENTIAL, false));
   TRY_S(scf_launch_update(c, s->d_vpsl, s->d_vh, s->d_vxc, SB200_KIND_POTENTIAL));
   SB_LAUNCH_CHECK("self-consistent potential update");
@@ -474,6 +626,10 @@ void scf_free(sb200_ctx* c) {
   dfree(s->d_vh);
   dfree(s->d_vxc);
   if (s->comm) nccl_api()->comm_destroy(s->comm);
+  dfree(s->d_ia);
+  dfree(s->d_ib);
+  dfree(s->d_icoef);
+  dfree(s->d_itab);
   delete s;
   c->scf = nullptr;
 }
@@ -527,6 +683,29 @@ int sb200_hartree_periodic(sb200_ctx* c, const double primitive_b[9], const doub
   double* d_v = out_dev ? Vh : s->d_out;
   TRY_S(scf_launch_hartree(c, d_rho, d_v, -1));
   SB_LAUNCH_CHECK("k_dft_pass");
+  if (!out_dev) SB_CUDA(cudaMemcpyAsync(Vh, d_v, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  SB_CUDA(cudaStreamSynchronize(c->stream));
+  return SB200_OK;
+}
+
+int sb200_hartree_isolated_ft(sb200_ctx* c, const double primitive_b[9], const double* rho, double* Vh) {
+  TRY_S(scf_ready(c));
+  if (!primitive_b || !rho || !Vh) return set_error(SB200_ERR_INVALID_ARG, "null argument");
+  if (c->g.periodic)
+    return set_error(SB200_ERR_UNSUPPORTED, "sb200_hartree_isolated_ft needs an isolated grid");
+  ScfDevGuard dg(c->device);
+  TRY_S(scf_ensure(c));
+  TRY_S(scf_itables(c, primitive_b));
+  ScfState* s = scf_of(c);
+  const long n = s->npts;
+  TRY_S(scf_stage_in(c, (size_t)n));
+  const double* d_rho = nullptr;
+  TRY_S(scf_input(c, rho, (size_t)n, s->d_in, &d_rho));
+  const bool out_dev = scf_is_device(Vh);
+  if (!out_dev) TRY_S(scf_stage_out(c, (size_t)n));
+  double* d_v = out_dev ? Vh : s->d_out;
+  TRY_S(scf_launch_hartree_isolated(c, d_rho, d_v, -1));
+  SB_LAUNCH_CHECK("k_dft_box");
   if (!out_dev) SB_CUDA(cudaMemcpyAsync(Vh, d_v, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   SB_CUDA(cudaStreamSynchronize(c->stream));
   return SB200_OK;
@@ -598,13 +777,14 @@ int sb200_set_self_consistent(sb200_ctx* c, int enable, const double* Vpsl, cons
     return SB200_OK;
   }
   if (!Vpsl || !primitive_b) return set_error(SB200_ERR_INVALID_ARG, "null argument");
-  if (!c->g.periodic)
-    return set_error(SB200_ERR_UNSUPPORTED, "the self-consistent time loop needs a periodic grid");
   if (c->orb.nspin != 1)
     return set_error(SB200_ERR_UNSUPPORTED, "the self-consistent time loop is the nspin = 1 form");
   if (!c->vloc_set) return set_error(SB200_ERR_STATE, "set V_local (sb200_set_vlocal / sb200_update_vlocal) first");
   TRY_S(scf_ensure(c));
-  TRY_S(scf_tables(c, primitive_b));
+  if (c->g.periodic)
+    TRY_S(scf_tables(c, primitive_b));
+  else
+    TRY_S(scf_itables(c, primitive_b));
   ScfState* s = scf_of(c);
   const size_t n = (size_t)s->npts;
   if (!s->d_vpsl) TRY_S(dalloc(&s->d_vpsl, n));

@@ -230,6 +230,16 @@ class Context:
         check(lib().sb200_hartree_periodic(self.h, _ptr(b), p, C.c_void_p(v.ctypes.data)))
         return v
 
+    def hartree_isolated_ft(self, rho, primitive_b):
+        """hartree -> poisson_isolated_ft (poisson_isolated.f90:692-836) on an
+        isolated grid; primitive_b (3, 3) of the box.  Returns Vh (nx, ny, nz)."""
+        g = self.sys.grid
+        b = np.asfortranarray(primitive_b, dtype=np.float64)
+        p, keep = self._scalar_field(rho)
+        v = np.zeros(g.shape, order="F")
+        check(lib().sb200_hartree_isolated_ft(self.h, _ptr(b), p, C.c_void_p(v.ctypes.data)))
+        return v
+
     def update_vlocal(self, vpsl, vh, vxc):
         """update_vlocal (hamiltonian.f90:813-843): V_local = Vpsl + Vh + Vxc on the
         device.  vxc: (nx, ny, nz, nspin) or (nx, ny, nz) for nspin = 1."""
@@ -257,7 +267,8 @@ class Context:
 
     def update_potential(self, psi, vpsl, primitive_b):
         """The self-consistent part of one time step on the device
-        (time_evolution_step.f90:160-207 for a periodic grid, nspin = 1):
+        (time_evolution_step.f90:160-207, nspin = 1; Hartree by poisson_ft on a
+        periodic grid, poisson_isolated_ft on an isolated one):
         rho = calc_density(psi), Vh = hartree(rho), Vxc = exchange_correlation(rho),
         V_local = Vpsl + Vh + Vxc.  vpsl: a device tensor (nx*ny*nz, x fastest)
         or a numpy array.  Nothing is copied to the host; returns E_xc."""
@@ -270,7 +281,8 @@ class Context:
         rho, vh, vxc = self._pot_buf
         b = np.asfortranarray(primitive_b, dtype=np.float64)
         check(lib().sb200_calc_density(self.h, C.c_void_p(psi.data_ptr()), C.c_void_p(rho.data_ptr())))
-        check(lib().sb200_hartree_periodic(self.h, _ptr(b), C.c_void_p(rho.data_ptr()), C.c_void_p(vh.data_ptr())))
+        hartree = lib().sb200_hartree_periodic if self.sys.grid.periodic else lib().sb200_hartree_isolated_ft
+        check(hartree(self.h, _ptr(b), C.c_void_p(rho.data_ptr()), C.c_void_p(vh.data_ptr())))
         e = C.c_double(0.0)
         check(lib().sb200_exc_cor_pz(self.h, C.c_void_p(rho.data_ptr()), C.c_void_p(vxc.data_ptr()), C.byref(e)))
         pa, keep = self._scalar_field(vpsl)

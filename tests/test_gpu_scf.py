@@ -277,3 +277,56 @@ def test_density_comm_single_rank():
         ctx.close()
     for x, y in zip(got[False], got[True]):
         assert np.array_equal(x, y)
+
+
+@pytest.mark.parametrize("make", [S.isolated_small, S.isolated_odd], ids=["iso24", "iso_odd"])
+def test_hartree_isolated_ft_against_oracle(make):
+    import torch
+    from salmon2_b200 import _lib
+    from salmon2_b200.rt import Context
+
+    s = make()
+    ctx = Context(s)
+    brl = _brl(s)
+    rho = Oracle(s).density(s.psi)[..., 0]
+    vh = ctx.hartree_isolated_ft(rho, brl)
+    ref = OR.poisson_isolated_ft(rho, brl)
+    assert S.rel_err(vh, ref) < TOL
+    rd = torch.from_numpy(np.ascontiguousarray(rho.ravel(order="F"))).cuda()
+    vd = torch.empty_like(rd)
+    b = np.asfortranarray(brl)
+    _lib.check(_lib.lib().sb200_hartree_isolated_ft(ctx.h, b.ctypes.data_as(C.POINTER(C.c_double)),
+                                                    C.c_void_p(rd.data_ptr()), C.c_void_p(vd.data_ptr())))
+    assert S.rel_err(vd.cpu().numpy(), ref.ravel(order="F")) < TOL
+    ctx.close()
+
+
+def test_rt_propagate_self_consistent_isolated():
+    """The self-consistent loop on an isolated grid after an impulse kick (the
+    doubled-box Hartree solve inside the graph) against the oracle's loop:
+    dipole every step, final orbitals."""
+    import dataclasses as dc
+    from salmon2_b200 import synth
+    from salmon2_b200.rt import Context
+
+    s0 = S.isolated_small()
+    s = dc.replace(s0, psi=synth.impulse_kick(s0.grid, s0.psi, 1e-3))
+    nt, dt = 6, 0.05
+    zc = synth.taylor_zc(dt)
+    brl = _brl(s)
+    vpsl = np.array(s.V_local[..., 0])
+    O = _oracle(s)
+    rho0 = O.density(s.psi)[..., 0]
+    v0 = OR.update_vlocal(vpsl, OR.poisson_isolated_ft(rho0, brl),
+                          OR.exc_cor_pz(rho0, s.grid.hvol)[0][..., None])[..., 0]
+    ref = O.rt_run_scf(s.psi, nt, dt, zc, vpsl, brl, v0)
+    ctx = Context(s)
+    a, b, w = ctx.upload(s.psi), ctx.zeros(), ctx.zeros()
+    ctx.update_potential(a, vpsl, brl)
+    ctx.set_self_consistent(True, vpsl, brl)
+    res = ctx.rt_propagate(a, b, w, nt, dt, zc)
+    d_ref = ref["rbox"][:3] - ref["rbox"][:3, :1]
+    d_got = res["rbox"][:3] - res["rbox"][:3, :1]
+    assert np.max(np.abs(d_got - d_ref)) <= TOL_LOOP * np.max(np.abs(ref["rbox"][:3]))
+    assert S.rel_err(ctx.download(res["psi"]), ref["psi"]) < TOL_LOOP
+    ctx.close()

@@ -117,3 +117,28 @@ def test_update_vlocal_is_the_sum():
     v = O.update_vlocal(vpsl, vh, vxc)
     for s in range(2):
         assert np.array_equal(v[..., s], (vpsl + vh) + vxc[..., s])
+
+
+@pytest.mark.parametrize("n", [24, 32])
+def test_poisson_isolated_gaussian_charge(n):
+    """The doubled-box solve of a unit Gaussian charge in the box centre equals
+    erf(r / (sqrt(2) s)) / r up to what dropping G = 0 of the doubled cell
+    implies: a constant plus the parabola 2 pi/3 * rho_bg * r^2 of the uniform
+    background rho_bg = -1 / (8 L^3)."""
+    from math import erf
+    h = 0.4
+    L = n * h
+    x = (np.arange(n) - n / 2 + 0.5) * h
+    X, Y, Z = np.meshgrid(x, x, x, indexing="ij")
+    r = np.sqrt(X ** 2 + Y ** 2 + Z ** 2)
+    s = 0.8
+    rho = np.exp(-r ** 2 / (2 * s * s)) / (2 * np.pi * s * s) ** 1.5
+    v = O.poisson_isolated_ft(rho, O.primitive_b_orthogonal([L, L, L]))
+    exact = np.vectorize(lambda q: erf(q / (np.sqrt(2) * s)) / q)(r)
+    d = v - exact - 2 * np.pi / 3 * (1.0 / (8 * L ** 3)) * r ** 2
+    inner = r < 3.0
+    assert np.ptp(d[inner]) < 2e-4 * np.max(exact)
+    # odd, unequal extents run too
+    rho2 = rho[: n - 1, : n - 2, :]
+    v2 = O.poisson_isolated_ft(rho2, O.primitive_b_orthogonal([(n - 1) * h, (n - 2) * h, L]))
+    assert v2.shape == rho2.shape and np.all(np.isfinite(v2))

@@ -219,6 +219,13 @@ inline void hartree(context& ctx, const double primitive_b[9], const s_scalar& r
   check(sb200_hartree_periodic(ctx.get(), primitive_b, rho.f.data(), Vh.f.data()), "hartree");
 }
 
+// the same call on an isolated system with method_poisson = 'ft': poisson_isolated_ft
+// (poisson_isolated.f90:692)
+inline void hartree_isolated_ft(context& ctx, const double primitive_b[9], const s_scalar& rho, s_scalar& Vh) {
+  Vh.f.resize(rho.f.size());
+  check(sb200_hartree_isolated_ft(ctx.get(), primitive_b, rho.f.data(), Vh.f.data()), "hartree");
+}
+
 // exchange_correlation(system,xc_func,mg,srg_scalar,srg,rho_s,ppn,info,spsi,stencil,Vxc,E_xc)
 // (salmon_xc.f90:58) with xc = 'PZ' and nspin = 1
 inline void exchange_correlation(context& ctx, const s_scalar& rho, std::vector<s_scalar>& Vxc, double& E_xc) {

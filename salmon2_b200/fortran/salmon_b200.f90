@@ -179,6 +179,15 @@ module salmon_b200
       real(c_double), intent(inout) :: Vh(*)
     end function
 
+    integer(c_int) function sb200_hartree_isolated_ft(ctx, primitive_b, rho, Vh) &
+        bind(c, name="sb200_hartree_isolated_ft")
+      import
+      type(c_ptr), value :: ctx
+      real(c_double), intent(in) :: primitive_b(3, 3)
+      real(c_double), intent(in) :: rho(*)
+      real(c_double), intent(inout) :: Vh(*)
+    end function
+
     integer(c_int) function sb200_update_vlocal(ctx, Vpsl, Vh, Vxc) bind(c, name="sb200_update_vlocal")
       import
       type(c_ptr), value :: ctx

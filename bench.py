@@ -56,8 +56,8 @@ def parse():
     ap.add_argument("--cpu-steps", type=int, default=4, help="Taylor steps in each CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--self-consistent", action="store_true",
-                    help="periodic workloads: V_local = Vpsl + Vh[rho] + Vxc[rho] (PZ) recomputed after every "
-                         "Taylor step inside the time loop (the fixed Gaussian potential stands in for Vpsl)")
+                    help="V_local = Vpsl + Vh[rho] + Vxc[rho] (PZ) recomputed after every Taylor step inside the "
+                         "time loop (the fixed Gaussian potential stands in for Vpsl)")
     ap.add_argument("--small", action="store_true", help="8 k-points instead of 64 (quick check)")
     ap.add_argument("--workload", default="bulk", choices=["bulk", "supercell", "batch", "isolated"],
                     help="bulk: 16^3 x 64 k x 32 orbitals; supercell: its 2x2x2 supercell, 32^3 x 8 k x 256; "
@@ -106,8 +106,8 @@ def config_dict(args, s, nt, world):
                 f"{s.pp.natom} atoms (diamond), {s.grid.shape[0]}^3 grid, "
                 f"{s.nk} k-points, {s.no} complex128 orbitals/k, Asin2cos A(t) omega=1.55 eV "
                 f"peak 1e-3 au, {nt} Taylor-4 steps per bench step, J(t) every step")
-        if getattr(args, "self_consistent", False):
-            desc += ", self-consistent: density, Hartree (periodic) and PZ-LDA potential every step"
+    if getattr(args, "self_consistent", False):
+        desc += ", self-consistent: density, Hartree and PZ-LDA potential every step"
     return {
         "workload": desc,
         "grid": list(s.grid.shape), "k_points": s.nk, "orbitals_per_k": s.no, "atoms": s.pp.natom,
@@ -466,8 +466,8 @@ def main():
     a, b, w = ctx.upload(s.psi), ctx.zeros(), ctx.zeros()
     units_rank = int(np.prod(s.grid.shape)) * s.norb * nt
     if args.self_consistent:
-        if not s.grid.periodic or s.nspin != 1:
-            raise SystemExit("--self-consistent needs a periodic workload with one spin")
+        if s.nspin != 1:
+            raise SystemExit("--self-consistent needs a workload with one spin")
         if world > 1:
             # the density of every step is summed over the k-point shards (NCCL all-reduce
             # inside the loop's graph) before the Hartree and XC potentials
@@ -477,7 +477,9 @@ def main():
                 uid.copy_(torch.frombuffer(bytearray(nccl_unique_id()), dtype=torch.uint8))
             dist.broadcast(uid, 0)
             ctx.set_density_comm(world, rank, bytes(uid.cpu().numpy().tobytes()))
-        # cubic cell: primitive_b = 2 pi / L; V_local from rho(t=0), then the update every step
+        # orthogonal box: primitive_b = 2 pi / L (the Hartree solve is poisson_ft on the
+        # periodic cell, poisson_isolated_ft on an isolated box); V_local from rho(t=0),
+        # then the update every step
         brl = np.diag([2.0 * np.pi / (n * h) for n, h in zip(s.grid.shape, s.grid.hgs)])
         vpsl = torch.from_numpy(np.ascontiguousarray(s.V_local[..., 0].ravel(order="F"))).cuda(local)
         ctx.update_potential(a, vpsl, brl)

@@ -42,6 +42,31 @@ module salmon_b200
       import
     end function
 
+    type(c_ptr) function sb200_version() bind(c, name="sb200_version")
+      import
+    end function
+
+    ! a caller-owned cudaStream_t (c_null_ptr: the context's own stream)
+    integer(c_int) function sb200_ctx_set_stream(ctx, stream) bind(c, name="sb200_ctx_set_stream")
+      import
+      type(c_ptr), value :: ctx, stream
+    end function
+
+    ! device-time accounting per kernel class (SB200_KIND_*, 8 slots)
+    integer(c_int) function sb200_set_timing(ctx, enable) bind(c, name="sb200_set_timing")
+      import
+      type(c_ptr), value :: ctx
+      integer(c_int), value :: enable
+    end function
+
+    integer(c_int) function sb200_kernel_times(ctx, ms, count, reset) bind(c, name="sb200_kernel_times")
+      import
+      type(c_ptr), value :: ctx
+      real(c_double), intent(inout) :: ms(8)
+      integer(c_long), intent(inout) :: count(8)
+      integer(c_int), value :: reset
+    end function
+
     ! s_rgrid + s_stencil (initialization.f90:241-256,508-611)
     integer(c_int) function sb200_set_grid(ctx, is, ie, is_array, ie_array, idx, idy, idz, lg_num, hgs, hvol, &
                                            coef_lap0, coef_lap, coef_nab) bind(c, name="sb200_set_grid")
@@ -158,6 +183,22 @@ module salmon_b200
       type(c_ptr), value :: ctx
       real(c_double), intent(in) :: rho(*)
       real(c_double), intent(inout) :: rbox(4)
+    end function
+
+    ! H psi without any allocation: every array is caller-owned device memory
+    ! (passed as addresses) except is, coef_lap0, coef_lap, coef_nab
+    integer(c_int) function sb200_hpsi_noalloc(nx, ny, nz, periodic, nspin, no, nk, is, coef_lap0, coef_lap, &
+                                               coef_nab, kAc, V_local, natom, nps, nlma, mps, jxyz, rxyz, uv, &
+                                               ia_tbl, rinv_uvu, tpsi, htpsi, stream) &
+        bind(c, name="sb200_hpsi_noalloc")
+      import
+      integer(c_int), value :: nx, ny, nz, periodic, nspin, no, nk
+      integer(c_int), intent(in) :: is(3)
+      real(c_double), value :: coef_lap0
+      real(c_double), intent(in) :: coef_lap(12), coef_nab(12)
+      type(c_ptr), value :: kAc, V_local
+      integer(c_int), value :: natom, nps, nlma
+      type(c_ptr), value :: mps, jxyz, rxyz, uv, ia_tbl, rinv_uvu, tpsi, htpsi, stream
     end function
 
     ! time_evolution_step.f90:184-207: hartree (periodic), exchange_correlation (PZ,
@@ -280,6 +321,39 @@ module salmon_b200
       integer(c_int), value :: nparam, batch
     end function
 
+    integer(c_int) function sb200_learned_get_params(ctx, params, nparam) bind(c, name="sb200_learned_get_params")
+      import
+      type(c_ptr), value :: ctx
+      real(c_float), intent(inout) :: params(*)
+      integer(c_int), value :: nparam
+    end function
+
+    ! network inputs x0(npts, 2, batch), outputs y / offset / target (npts, batch):
+    ! host or device arrays, passed as addresses
+    integer(c_int) function sb200_learned_forward(ctx, x0, y, batch) bind(c, name="sb200_learned_forward")
+      import
+      type(c_ptr), value :: ctx, x0, y
+      integer(c_int), value :: batch
+    end function
+
+    integer(c_int) function sb200_learned_loss_grad(ctx, x0, offset, target, batch, loss, grad) &
+        bind(c, name="sb200_learned_loss_grad")
+      import
+      type(c_ptr), value :: ctx, x0, offset, target
+      integer(c_int), value :: batch
+      real(c_double), intent(out) :: loss
+      type(c_ptr), value :: grad
+    end function
+
+    integer(c_int) function sb200_learned_train_step(ctx, x0, offset, target, batch, lr, loss) &
+        bind(c, name="sb200_learned_train_step")
+      import
+      type(c_ptr), value :: ctx, x0, offset, target
+      integer(c_int), value :: batch
+      real(c_float), value :: lr
+      real(c_double), intent(out) :: loss
+    end function
+
     ! ---- batches of independent isolated systems ----
     integer(c_int) function sb200_batch_create(systems, nsys, batch) bind(c, name="sb200_batch_create")
       import
@@ -291,6 +365,18 @@ module salmon_b200
     integer(c_int) function sb200_batch_destroy(batch) bind(c, name="sb200_batch_destroy")
       import
       type(c_ptr), value :: batch
+    end function
+
+    integer(c_int) function sb200_batch_set_tiles(batch, shape, zchunk) bind(c, name="sb200_batch_set_tiles")
+      import
+      type(c_ptr), value :: batch
+      integer(c_int), intent(in) :: shape(*), zchunk(*)
+    end function
+
+    integer(c_int) function sb200_batch_get_tiles(batch, shape, zchunk) bind(c, name="sb200_batch_get_tiles")
+      import
+      type(c_ptr), value :: batch
+      integer(c_int), intent(inout) :: shape(*), zchunk(*)
     end function
 
     integer(c_int) function sb200_batch_autotune(batch, psi, work, reps, shape, zchunk) &

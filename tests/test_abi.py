@@ -46,3 +46,12 @@ def test_library_reports_missing_device_without_crashing():
     rc = _lib.lib().sb200_ctx_create(0, ctypes.byref(h))
     assert rc == 5  # SB200_ERR_CUDA
     assert _lib.lib().sb200_last_error()
+
+
+def test_fortran_interface_binds_every_entry_point():
+    """The ISO_C_BINDING module a SALMON build would use declares every entry
+    point of the header under its C name (no Fortran compiler here: checked
+    as text)."""
+    src = open(os.path.join(ROOT, "salmon2_b200", "fortran", "salmon_b200.f90")).read()
+    bound = set(re.findall(r'bind\(c,\s*name="(sb200_\w+)"\)', src))
+    assert bound == set(declared_symbols())

@@ -142,3 +142,37 @@ def test_poisson_isolated_gaussian_charge(n):
     rho2 = rho[: n - 1, : n - 2, :]
     v2 = O.poisson_isolated_ft(rho2, O.primitive_b_orthogonal([(n - 1) * h, (n - 2) * h, L]))
     assert v2.shape == rho2.shape and np.all(np.isfinite(v2))
+
+
+@pytest.mark.parametrize("kind", ["periodic", "isolated"])
+def test_rt_run_scf_equals_the_loop_written_out(kind):
+    """sbo_rt_run_scf against the self-consistent loop spelled out call by call
+    (taylor, calc_density, Hartree, PZ-LDA, update_vlocal) with no field."""
+    import dataclasses
+
+    import _systems as S
+    from salmon2_b200 import synth
+
+    s = S.periodic_small() if kind == "periodic" else S.isolated_small()
+    s = dataclasses.replace(s, V_local=np.array(s.V_local, order="F"))
+    g = s.grid
+    brl = O.primitive_b_orthogonal([n * h for n, h in zip(g.shape, g.hgs)])
+    poisson = O.poisson_ft if g.periodic else O.poisson_isolated_ft
+    vpsl = np.array(s.V_local[..., 0])
+    zc = synth.taylor_zc(0.05)
+    nt = 3
+
+    def potential(rho):
+        return O.update_vlocal(vpsl, poisson(rho, brl), O.exc_cor_pz(rho, g.hvol)[0][..., None])
+
+    orc = O.Oracle(s, threads=2)
+    v0 = potential(orc.density(s.psi)[..., 0])[..., 0]
+    ref = orc.rt_run_scf(s.psi, nt, 0.05, zc, vpsl, brl, v0)
+    step = O.Oracle(dataclasses.replace(s, V_local=np.array(s.V_local, order="F")), threads=2)
+    step.V[..., 0] = v0
+    psi = s.psi
+    for _ in range(nt):
+        psi = step.taylor(psi, zc)
+        step.V[...] = potential(step.density(psi)[..., 0])
+    assert np.max(np.abs(ref["psi"] - psi)) <= 1e-13 * np.max(np.abs(psi))
+    assert np.max(np.abs(ref["V_local"] - step.V[..., 0])) <= 1e-13 * np.max(np.abs(step.V))

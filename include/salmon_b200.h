@@ -382,6 +382,14 @@ int sb200_set_density_comm(sb200_ctx* ctx, int nranks, int rank, const unsigned 
  *   is[3], coef_lap0, coef_lap(4,3), coef_nab(4,3).  periodic = 0 means the
  *   zero Dirichlet boundary of an isolated grid.  Work is queued on `stream`
  *   (a cudaStream_t, NULL for the legacy default stream).
+ * The projector tables are checked on the device, since the host never sees
+ * them: a jxyz entry outside is..is+n-1, an ia_tbl entry outside 1..natom or
+ * an mps entry outside 0..nps is skipped (it adds nothing) instead of being
+ * read or written, and the call's `status` word (caller-owned device int, may
+ * be NULL) is set to SB200_ERR_BAD_SHAPE; otherwise the call sets it to
+ * SB200_OK.  Read it after the stream's work has finished.  Spheres that
+ * reach one grid point twice through two periodic images are added in the
+ * reference's order (ilma, then j) without lost updates.
  * Its only scratch, the projections <beta|psi> of all orbitals, is a fixed
  * device array inside the library of SB200_NOALLOC_MAX_PROJECTIONS complex
  * values (4 MiB), held by every GPU that loads the library until the process
@@ -396,7 +404,7 @@ int sb200_hpsi_noalloc(int nx, int ny, int nz, int periodic, int nspin, int no, 
                        const double* kAc, const double* V_local, int natom, int nps, int nlma,
                        const int* mps, const int* jxyz, const double* rxyz, const double* uv,
                        const int* ia_tbl, const double* rinv_uvu, const double* tpsi, double* htpsi,
-                       void* stream);
+                       int* status, void* stream);
 
 #ifdef __cplusplus
 }

@@ -88,7 +88,7 @@ SIGNATURES = {
     "sb200_batch_propagate": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int, C.c_double, _dp, C.c_int, _vp, _vp]),
     "sb200_hpsi_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _ip,
                                      C.c_double, _dp, _dp, _vp, _vp, C.c_int, C.c_int, C.c_int, _vp, _vp, _vp,
-                                     _vp, _vp, _vp, _vp, _vp, _vp]),
+                                     _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
 }
 
 

@@ -186,10 +186,12 @@ module salmon_b200
     end function
 
     ! H psi without any allocation: every array is caller-owned device memory
-    ! (passed as addresses) except is, coef_lap0, coef_lap, coef_nab
+    ! (passed as addresses) except is, coef_lap0, coef_lap, coef_nab; status is
+    ! a device integer (or c_null_ptr) set to SB200_ERR_BAD_SHAPE when a table
+    ! entry lies outside the grid
     integer(c_int) function sb200_hpsi_noalloc(nx, ny, nz, periodic, nspin, no, nk, is, coef_lap0, coef_lap, &
                                                coef_nab, kAc, V_local, natom, nps, nlma, mps, jxyz, rxyz, uv, &
-                                               ia_tbl, rinv_uvu, tpsi, htpsi, stream) &
+                                               ia_tbl, rinv_uvu, tpsi, htpsi, status, stream) &
         bind(c, name="sb200_hpsi_noalloc")
       import
       integer(c_int), value :: nx, ny, nz, periodic, nspin, no, nk
@@ -198,7 +200,7 @@ module salmon_b200
       real(c_double), intent(in) :: coef_lap(12), coef_nab(12)
       type(c_ptr), value :: kAc, V_local
       integer(c_int), value :: natom, nps, nlma
-      type(c_ptr), value :: mps, jxyz, rxyz, uv, ia_tbl, rinv_uvu, tpsi, htpsi, stream
+      type(c_ptr), value :: mps, jxyz, rxyz, uv, ia_tbl, rinv_uvu, tpsi, htpsi, status, stream
     end function
 
     ! time_evolution_step.f90:184-207: hartree (periodic), exchange_correlation (PZ,

@@ -239,10 +239,13 @@ def _cholesky_qr2(a):
 
 
 def random_orbitals(grid: Grid, rng, nspin, no, nk, envelope_width=None, real=False,
-                    fast=False) -> np.ndarray:
+                    fast=False, ecut=None) -> np.ndarray:
     """Seeded orbitals, orthonormal per (k, spin) in the hvol metric, in the
     reference array layout with a zero halo (structures.f90:646-669).
-    fast=True orthonormalises by Cholesky QR instead of Householder QR."""
+    fast=True orthonormalises by Cholesky QR instead of Householder QR.
+    ecut (Hartree): the random field keeps only the Fourier components of the
+    box with |G|^2/2 <= ecut before the envelope is applied (smooth orbitals
+    whose spectral weight lies at low energy, like occupied states)."""
     nx, ny, nz = grid.shape
     X, Y, Z = np.meshgrid(grid.coordinate(0), grid.coordinate(1), grid.coordinate(2), indexing="ij")
     if envelope_width is None:
@@ -261,6 +264,15 @@ def random_orbitals(grid: Grid, rng, nspin, no, nk, envelope_width=None, real=Fa
             a = rng.standard_normal((npt, no))
             if not real:
                 a = a + 1j * rng.standard_normal((npt, no))
+            if ecut is not None:
+                L = grid.hgs * np.array([nx, ny, nz], dtype=np.float64)
+                g = [2.0 * math.pi * np.fft.fftfreq(n, 1.0 / n) / L[d] for d, n in enumerate((nx, ny, nz))]
+                kin = 0.5 * (g[0][:, None, None] ** 2 + g[1][None, :, None] ** 2 + g[2][None, None, :] ** 2)
+                f = np.fft.fftn(a.reshape((nx, ny, nz, no), order="F"), axes=(0, 1, 2))
+                f[kin > ecut] = 0.0
+                a = np.fft.ifftn(f, axes=(0, 1, 2)).reshape((npt, no), order="F")
+                if real:
+                    a = a.real
             a *= env.reshape(-1, order="F")[:, None]
             q = _cholesky_qr2(a) if fast else np.linalg.qr(a)[0]
             q = q / math.sqrt(grid.hvol)
@@ -350,8 +362,9 @@ def asin2cos(nt: int, dt: float, omega: float, f0: float, tw: float, epdir=(0.0,
 # --------------------------------------------------------------------------
 
 def isolated_system(num=64, h_aa=0.25, no=5, natom=4, seed=1, rc_aa=1.2, nspin=1,
-                    real=False, name="isolated", fast=False) -> System:
-    """Isolated molecule: Dirichlet box, seeded atoms in the central 60 %."""
+                    real=False, name="isolated", fast=False, ecut=None) -> System:
+    """Isolated molecule: Dirichlet box, seeded atoms in the central 60 %.
+    ecut: band-limit the orbitals (random_orbitals)."""
     rng = np.random.default_rng(seed)
     h = h_aa / AU_LENGTH_AA
     nums = [int(num)] * 3 if np.isscalar(num) else [int(v) for v in num]
@@ -363,7 +376,7 @@ def isolated_system(num=64, h_aa=0.25, no=5, natom=4, seed=1, rc_aa=1.2, nspin=1
                  inorm=rng.choice([-1, 1], size=(natom, 2)))
     V = gaussian_potential(grid, rion, rng.uniform(-2.0, -0.5, natom), rng.uniform(0.8, 1.6, natom))
     V_local = np.asfortranarray(np.repeat(V[..., None], nspin, axis=3))
-    psi = random_orbitals(grid, rng, nspin, no, 1, envelope_width=0.2 * L, real=real, fast=fast)
+    psi = random_orbitals(grid, rng, nspin, no, 1, envelope_width=0.2 * L, real=real, fast=fast, ecut=ecut)
     return System(grid, pp, nspin, no, 1, np.zeros((3, 1), order="F"),
                   np.asfortranarray(np.full((no, 1, nspin), 2.0)), np.ones(1), V_local, rion, psi,
                   int(np.prod(grid.num)), seed, name)

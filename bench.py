@@ -202,9 +202,11 @@ def hpsi_kernel(s, args, units_per_launch):
             return "k_term_orbital_tma", UNIT_BYTES["fp64"] / 4.0 * units_per_launch
         if v.startswith("t"):
             return "k_term_orbital", UNIT_BYTES["fp64"] / 4.0 * units_per_launch
-        if v.startswith("u") or s.pp.nlma == 0:
+        if v.startswith("u") or (v.startswith("s") and s.pp.nlma == 0):
             return "k_step_orbital", UNIT_BYTES["fp64"] * units_per_launch
-        return "k_step_orbital_st", UNIT_BYTES["fp64"] * units_per_launch  # KB tables in shared memory
+        if v.startswith("s"):
+            return "k_step_orbital_st", UNIT_BYTES["fp64"] * units_per_launch  # KB tables in shared memory
+        return "k_step_blk", UNIT_BYTES["fp64"] * units_per_launch  # register-blocked fused step
     name = "k_hpsi_tiled" if os.environ.get("SB200_TMA", "on").startswith("of") else "k_hpsi_tma"
     return name, UNIT_BYTES[args.precision] / 4.0 * units_per_launch
 

@@ -322,7 +322,8 @@ int sb200_ctx_create(int device, sb200_ctx** out) {
   c->stream = c->own_stream;
   if (const char* v = getenv("SB200_STENCIL")) c->stencil_variant = (v[0] == 'n') ? 0 : 1;
   if (const char* v = getenv("SB200_ORBITAL"))
-    c->orbital_variant = (v[0] == 'p') ? 1 : (v[0] == 't') ? 0 : (v[0] == 'u') ? 3 : 2;
+    c->orbital_variant = (v[0] == 'p') ? 1 : (v[0] == 't') ? 0 : (v[0] == 'u') ? 3 : (v[0] == 's') ? 2 : 4;
+  if (const char* v = getenv("SB200_BLK_DEPTH")) c->blk_depth = (v[0] == '4') ? 4 : 2;
   if (const char* v = getenv("SB200_TMA")) c->tma_variant = (v[0] == 'o' && v[1] == 'f') ? 0 : 1;
   int r = dalloc(&c->d_result, 16);
   if (r == SB200_OK) r = dalloc(&c->rt.d_step, 1);

@@ -146,8 +146,10 @@ struct sb200_ctx {
   size_t stage_bytes = 0;
   bool vloc_set = false;
   int stencil_variant = 1;     // 0: per-point reference kernel, 1: tiled 2.5-D sweep
-  int orbital_variant = 2;     // 16^3 periodic grids: 2 fused Taylor step (KB tables staged in shared memory
-                               // when they fit), 3 fused without staging, 0 one launch per term, 1 persistent per term
+  int orbital_variant = 4;     // 16^3 periodic grids: 4 fused Taylor step with register blocking (when its
+                               // tables fit, else form 2), 2 fused step with the KB tables staged in shared memory
+                               // (when they fit), 3 fused without staging, 0 one launch per term, 1 persistent per term
+  int blk_depth = 2;           // z depth of the register block of the blocked fused step (2: 512 threads, 4: 256)
   int tma_variant = 1;         // tiled hpsi fed by tensor copies where it applies (0: register-prefetch sweep)
   // optional per-kernel-class device timing (sb200_set_timing)
   bool timing = false;

@@ -952,8 +952,7 @@ OrbArgs make_orb_args(const sb200_ctx* c, double2 zc, bool with_obs) {
 }  // namespace
 
 bool step_orbital_applies(const sb200_ctx* c, int n_hamil) {
-  return orbital_kernel_applies(c) && (c->orbital_variant == 2 || c->orbital_variant == 3) && n_hamil >= 1 &&
-         n_hamil <= STEP_MAX_NTERM;
+  return orbital_kernel_applies(c) && (c->orbital_variant >= 2) && n_hamil >= 1 && n_hamil <= STEP_MAX_NTERM;
 }
 
 // One launch for the whole Taylor step: psi_out = sum_n zc_n H^n psi (+ psi).
@@ -967,7 +966,7 @@ int launch_step_orbital(sb200_ctx* c, const double2* in, double2* out, const dou
   const size_t smem_st = 2 * (size_t)N * NP * sizeof(double2) + (size_t)pp.nlma * sizeof(double2) +
                          (size_t)pp.npair * (sizeof(double2) + 4 * sizeof(double) + 2 * sizeof(int)) +
                          (size_t)pp.totpts * sizeof(int);
-  const bool staged = c->orbital_variant == 2 && pp.nlma > 0 && pp.npair > 0 && pp.d_apj != nullptr &&
+  const bool staged = (c->orbital_variant == 2 || c->orbital_variant == 4) && pp.nlma > 0 && pp.npair > 0 && pp.d_apj != nullptr &&
                       smem_st <= SMEM_MAX;
   static bool attr_set = false;
   if (!attr_set) {
@@ -983,6 +982,10 @@ int launch_step_orbital(sb200_ctx* c, const double2* in, double2* out, const dou
   StepZC z;
   for (int i = 0; i < STEP_MAX_NTERM; ++i) z.v[i] = i < n_hamil ? zc[i] : make_double2(0.0, 0.0);
   const OrbArgs a = make_orb_args(c, zc[0], with_obs);
+  if (c->orbital_variant == 4) {  // register-blocked form, when its tables fit
+    const int r = launch_step_blk(c, in, out, a, z, n_hamil, with_obs);
+    if (r != SB200_ERR_UNSUPPORTED) return r;
+  }
   dim3 grid(c->orb.norb);
   if (staged) {
     StageArgs st;

@@ -2,6 +2,8 @@
 #pragma once
 #include <cuda_runtime.h>
 
+struct sb200_ctx;
+
 namespace sb200 {
 
 constexpr int ORB_MAX_NLMA = 1024;  // projections held in shared memory
@@ -38,5 +40,18 @@ constexpr int STEP_MAX_NTERM = 8;  // Taylor terms of the fused step kernel
 struct StepZC {
   double2 v[STEP_MAX_NTERM];  // zc(1..n_hamil)
 };
+
+// extra arguments of the register-blocked fused step (sb200_orbital_blk.cu)
+struct BlkArgs {
+  double mhl[12];      // -coef_lap / 2
+  int npair;           // (point, atom) pairs
+  const int* pmap2;    // [npts] (first pair << 8) | count, or -1
+  const int* pair_fp;  // [npair] flat sphere point of each pair (point-major)
+};
+
+// The register-blocked fused step; SB200_ERR_UNSUPPORTED (no error recorded)
+// when its shared-memory tables do not fit or the KB tables have no pair form.
+int launch_step_blk(sb200_ctx* c, const double2* in, double2* out, const OrbArgs& a, const StepZC& z, int n_hamil,
+                    bool with_obs);
 
 }  // namespace sb200

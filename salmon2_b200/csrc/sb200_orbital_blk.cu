@@ -1,0 +1,570 @@
+// sb200_orbital_blk.cu -- the fused Taylor step for periodic 16^3 orbitals
+// with register blocking (default form of the periodic-bulk path).
+//
+// One CTA applies all n_hamil terms of taylor.f90:47-117 to one 16^3 orbital.
+// Thread t owns a block of 2 (x) x 2 (y) x BZ (z) grid points: x = 2 bx + i,
+// y = 2 by + j, z = BZ bz + l with (bx, by, bz) = (t % 8, (t / 8) % 8, t / 64),
+// slot s = i + 2 j + 4 l; the CTA has 1024 / BZ threads (BZ = 2: 512, BZ = 4:
+// 256).  Per term the thread keeps the values of h_{n-1} at its own points in
+// registers and accumulates those of h_n in registers; only the 4-point halo
+// of its block comes from shared memory: 8 x-neighbours per (y, z) row, 8
+// y-neighbours per (x, z) column and 8 z-neighbours per (x, y) column, i.e.
+// 12 (BZ = 2) or 10 (BZ = 4) loads of 16 bytes per point and term, against
+// 24 for a point-per-thread sweep.
+//
+// Shared-memory layout of an orbital: index (z, y, x) = 256 z + 16 y + 8 (x % 2)
+// + x / 2, i.e. each 16-point x row is stored as its 8 even then its 8 odd
+// points.  The 8 threads of a quarter warp share (by, bz) and differ in bx, so
+// every x, y or z neighbour load of a quarter warp touches 8 consecutive
+// 16-byte words of one 128-byte row half: no bank conflicts.
+//
+// Tensor memory (TMEM, 256 columns of the SM's 512) holds per thread the
+// Taylor accumulator psi_out of its 16 points (FP64 complex), the diagonal
+// V_local + k_lap0 of its points and their KB point-map words, so neither
+// registers nor shared memory carry them through the step.  The orbital
+// buffer is updated in place between terms (three CTA barriers per term).
+//
+// Kleinman-Bylander term (nonlocal_potential.f90:351-382, pair form): the
+// CTA's k-point tables -- phase exp(i (k+A).r), uV of the atom's projectors,
+// and the shared-memory index of every flat sphere point, plus the
+// point-major list of (point, atom) pairs -- are staged in shared memory once
+// per step.  After each h_{n-1} is complete, one warp per atom computes its
+// projections P_q = rinv_q sum_j uV_qj e^{i(k+A).r_j} h(r_j) (butterfly, all
+// lanes get the sums) and then, for each of its sphere points, the
+// contribution c_j = conj(e_j) sum_q uV_qj P_q into a per-point buffer.  The
+// owner of a grid point adds the contributions of its pairs in atom (ilma)
+// order.  The stencil arithmetic per point and neighbour pair is that of
+// zstencil_typical_seq (zstencil_core/typical/seq.f90:65-122) with the
+// coefficients folded: h += (-lapt/2)(t+ + t-) - i k_nabt (t+ - t-).
+//
+// After the last term (OBS), the observables of psi(t+dt) (sum |psi|^2, the
+// forward-difference current sums of density_matrix.f90:465-530, the dipole
+// moments of dip.f90:114-225 and the nonlocal current of
+// density_matrix.f90:532-591) are reduced per orbital in a fixed order.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "sb200_internal.cuh"
+#include "sb200_orbital.cuh"
+#include "sb200_tmem.cuh"
+
+namespace sb200 {
+namespace {
+
+constexpr int N = 16, NP = N * N, NPTS = N * NP;
+constexpr uint32_t TMEM_COLS = 256;
+// TMEM words (columns) per thread: psi_out 4 per point, diagonal 2 per point,
+// point-map word 1 per point; the NW / 4 warps of one lane quarter each use
+// 1024 / NW columns of the 256
+template <int BZ>
+struct Blk {
+  static constexpr int BT = 1024 / BZ;  // threads
+  static constexpr int NW = BT / 32;    // warps
+  static constexpr int NS = 4 * BZ;     // own points per thread
+  static constexpr uint32_t TW_ACC = 0, TW_D = 4 * NS, TW_PM = 6 * NS;
+  static constexpr uint32_t TW_WARP = TMEM_COLS / (NW / 4);
+  static_assert(7 * NS <= TW_WARP, "TMEM words per thread");
+};
+
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+// h += A (tp + tm) - i B (tp - tm)  (A = -lapt/2, B = k_nabt of one direction and distance)
+__device__ __forceinline__ void pair_acc(double2& h, const double2 tp, const double2 tm, const double A,
+                                         const double B) {
+  const double sx = tp.x + tm.x, sy = tp.y + tm.y, dx = tp.x - tm.x, dy = tp.y - tm.y;
+  h.x = fma(A, sx, h.x);
+  h.y = fma(A, sy, h.y);
+  h.x = fma(B, dy, h.x);
+  h.y = fma(-B, dx, h.y);
+}
+
+// Im(conj(c) t) weighted: the current sums of density_matrix.f90:465-530
+__device__ __forceinline__ double cur_term(const double nab, const double2 c, const double2 t) {
+  return nab * (c.x * t.y - c.y * t.x);
+}
+
+__device__ __forceinline__ int gidx(int x, int y, int z) { return (z << 8) | (y << 4) | x; }
+__device__ __forceinline__ int sidx(int x, int y, int z) { return (z << 8) | (y << 4) | ((x & 1) << 3) | (x >> 1); }
+
+// Projections of the orbital in shared memory, one warp per atom, followed by
+// the per-sphere-point KB contributions pc[fp] = conj(e) sum_q uV_q P_q.
+template <int NW>
+__device__ __forceinline__ void project_contrib(const double2* __restrict__ buf, const double2* __restrict__ sph,
+                                                const double* __restrict__ suv, const int* __restrict__ spt,
+                                                double2* __restrict__ pc, int T, const OrbArgs& a, int warp,
+                                                int lane) {
+  for (int atom = warp; atom < a.natom; atom += NW) {
+    const int start = __ldg(a.atom_start + atom), m = __ldg(a.mps + atom);
+    const int lma0 = __ldg(a.lma_start + atom), np = __ldg(a.nproj + atom);
+    if (np == 0) continue;  // no projectors: its sphere points have no pairs
+    double2 pq[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) pq[q] = make_double2(0.0, 0.0);
+    for (int j = lane; j < m; j += 32) {
+      const int fp = start + j;
+      const double2 ev = cmul(sph[fp], buf[spt[fp]]);
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+        if (q < np) {
+          const double u = suv[q * T + fp];
+          pq[q] = make_double2(fma(u, ev.x, pq[q].x), fma(u, ev.y, pq[q].y));
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) {
+        pq[q].x += __shfl_xor_sync(0xffffffffu, pq[q].x, off);
+        pq[q].y += __shfl_xor_sync(0xffffffffu, pq[q].y, off);
+      }
+      const double r = q < np ? __ldg(a.rinv + lma0 + q) : 0.0;
+      pq[q] = make_double2(r * pq[q].x, r * pq[q].y);
+    }
+    for (int j = lane; j < m; j += 32) {
+      const int fp = start + j;
+      double2 sp = make_double2(0.0, 0.0);
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+        if (q < np) {
+          const double u = suv[q * T + fp];
+          sp = make_double2(fma(u, pq[q].x, sp.x), fma(u, pq[q].y, sp.y));
+        }
+      const double2 e = sph[fp];
+      pc[fp] = cmul(make_double2(e.x, -e.y), sp);
+    }
+  }
+}
+
+template <int BZ, bool OBS>
+__global__ void __launch_bounds__(Blk<BZ>::BT, 1) k_step_blk(const double2* __restrict__ in,
+                                                             double2* __restrict__ out, OrbArgs a, BlkArgs bk,
+                                                             StepZC zc, int nterm) {
+  constexpr int BT = Blk<BZ>::BT, NW = Blk<BZ>::NW, NS = Blk<BZ>::NS;
+  constexpr uint32_t TW_ACC = Blk<BZ>::TW_ACC, TW_D = Blk<BZ>::TW_D, TW_PM = Blk<BZ>::TW_PM;
+  constexpr uint32_t TW_WARP = Blk<BZ>::TW_WARP;
+  extern __shared__ __align__(16) double2 smem[];
+  const int T = a.totpts;
+  const bool kb = a.nlma > 0;
+  double2* buf = smem;                      // [4096] the orbital h_{n-1}, split-x layout
+  double2* sph = buf + NPTS;                // [T] phase of the CTA's k-point
+  double2* pc = sph + T;                    // [T] KB contribution of each sphere point
+  double* suv = (double*)(pc + T);          // [4][T] uV of the atom's projectors
+  int* spt = (int*)(suv + 4 * T);           // [T] shared-memory index of each sphere point
+  int* plist = spt + T;                     // [npair] pairs of each grid point (flat sphere points)
+  __shared__ uint32_t s_tmem;
+  __shared__ double kn[12];
+  __shared__ double red[OBS_NQ][NW];
+  __shared__ double jws[NW][3];
+
+  const int o = blockIdx.x, t = threadIdx.x, warp = t >> 5, lane = t & 31;
+  const int bx = t & 7, by = (t >> 3) & 7, bz = t >> 6;
+  const int z0 = BZ * bz;
+  const int ik = o / a.nspin_no, ispin = o % a.nspin;
+  const double* kc = a.kcoef + (long)KC * ik;
+
+  if (warp == 0) tmem::alloc(&s_tmem, TMEM_COLS);
+  if (t < 12) kn[t] = __ldg(kc + 4 + t);  // k_nabt(s, d) = kAc_d nab(s, d)
+
+  // psi -> registers and the shared orbital buffer
+  const double2* src = in + (long)o * a.npts;
+  double2 cv[NS];
+#pragma unroll
+  for (int s = 0; s < NS; ++s) {
+    const int x = 2 * bx + (s & 1), y = 2 * by + ((s >> 1) & 1), z = z0 + (s >> 2);
+    cv[s] = __ldg(src + gidx(x, y, z));
+  }
+#pragma unroll
+  for (int s = 0; s < NS; ++s) {
+    const int x = 2 * bx + (s & 1), y = 2 * by + ((s >> 1) & 1), z = z0 + (s >> 2);
+    buf[sidx(x, y, z)] = cv[s];
+  }
+  if (kb) {  // the k-point's KB tables
+    const double2* gph = a.phase + (long)ik * T;
+    for (int i = t; i < T; i += BT) {
+      sph[i] = __ldg(gph + i);
+      const int p = __ldg(a.pt_lin + i);
+      spt[i] = sidx(p & 15, (p >> 4) & 15, p >> 8);
+    }
+    for (int atom = 0; atom < a.natom; ++atom) {
+      const int start = __ldg(a.atom_start + atom), m = __ldg(a.mps + atom);
+      const int lma0 = __ldg(a.lma_start + atom), np = __ldg(a.nproj + atom);
+      for (int j = t; j < m; j += BT) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) suv[q * T + start + j] = q < np ? __ldg(a.uv + (long)(lma0 + q) * a.nps + j) : 0.0;
+      }
+    }
+    for (int i = t; i < bk.npair; i += BT) plist[i] = __ldg(bk.pair_fp + i);
+  }
+  tmem::fence_before_sync();
+  __syncthreads();
+  tmem::fence_after_sync();
+  const uint32_t tb = tmem::warp_addr(s_tmem, warp, (uint32_t)(warp >> 2) * TW_WARP);
+  {  // diagonal V_local + k_lap0 and point-map words of the own points -> TMEM
+    const double lap0 = __ldg(kc + 3);
+    const double* vloc = a.vloc + (long)ispin * a.npts;
+    uint32_t w[8];
+#pragma unroll
+    for (int hh = 0; hh < NS / 4; ++hh) {
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int s = 4 * hh + u;
+        const int x = 2 * bx + (s & 1), y = 2 * by + ((s >> 1) & 1), z = z0 + (s >> 2);
+        const double d = __ldg(vloc + gidx(x, y, z)) + lap0;
+        w[2 * u] = tmem::lo_word(d);
+        w[2 * u + 1] = tmem::hi_word(d);
+      }
+      tmem::st8(tb + TW_D + 8 * hh, w);
+    }
+#pragma unroll
+    for (int hh = 0; hh < NS / 8; ++hh) {
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const int s = 8 * hh + u;
+        const int x = 2 * bx + (s & 1), y = 2 * by + ((s >> 1) & 1), z = z0 + (s >> 2);
+        w[u] = kb ? (uint32_t)__ldg(bk.pmap2 + gidx(x, y, z)) : 0xffffffffu;
+      }
+      tmem::st8(tb + TW_PM + 8 * hh, w);
+    }
+  }
+  if (kb) {
+    project_contrib<NW>(buf, sph, suv, spt, pc, T, a, warp, lane);
+    __syncthreads();
+  }
+  const int hm2 = (bx - 2) & 7, hm1 = (bx - 1) & 7, hp1 = (bx + 1) & 7, hp2 = (bx + 2) & 7;
+  double2* odst = out + (long)o * a.npts;
+  for (int nn = 0; nn < nterm; ++nn) {
+    double2 h[NS];
+#pragma unroll
+    for (int s = 0; s < NS; ++s) h[s] = make_double2(0.0, 0.0);
+    // ---- x neighbours: per (y, z) row, x = 2 bx - 4 .. 2 bx + 5 ----
+    {
+      const double B1 = kn[0], B2 = kn[1], B3 = kn[2], B4 = kn[3];
+      const double A1 = bk.mhl[0], A2 = bk.mhl[1], A3 = bk.mhl[2], A4 = bk.mhl[3];
+#pragma unroll
+      for (int r = 0; r < 2 * BZ; ++r) {
+        const int j = r & 1, l = r >> 1;
+        const double2* row = buf + ((z0 + l) << 8) + ((2 * by + j) << 4);
+        const double2 vm4 = row[hm2], vm3 = row[8 + hm2], vm2 = row[hm1], vm1 = row[8 + hm1];
+        const double2 vp2 = row[hp1], vp3 = row[8 + hp1], vp4 = row[hp2], vp5 = row[8 + hp2];
+        const int s0 = 2 * j + 4 * l, s1 = s0 + 1;
+        pair_acc(h[s0], cv[s1], vm1, A1, B1);
+        pair_acc(h[s0], vp2, vm2, A2, B2);
+        pair_acc(h[s0], vp3, vm3, A3, B3);
+        pair_acc(h[s0], vp4, vm4, A4, B4);
+        pair_acc(h[s1], vp2, cv[s0], A1, B1);
+        pair_acc(h[s1], vp3, vm1, A2, B2);
+        pair_acc(h[s1], vp4, vm2, A3, B3);
+        pair_acc(h[s1], vp5, vm3, A4, B4);
+      }
+    }
+    // ---- y neighbours: per (x, z) column, y = 2 by - 4 .. 2 by + 5 ----
+    {
+      const double B1 = kn[4], B2 = kn[5], B3 = kn[6], B4 = kn[7];
+      const double A1 = bk.mhl[4], A2 = bk.mhl[5], A3 = bk.mhl[6], A4 = bk.mhl[7];
+#pragma unroll
+      for (int r = 0; r < 2 * BZ; ++r) {
+        const int i = r & 1, l = r >> 1;
+        const double2* col = buf + ((z0 + l) << 8) + (i << 3) + bx;
+        const int y0 = 2 * by;
+        const double2 vm4 = col[((y0 - 4) & 15) << 4], vm3 = col[((y0 - 3) & 15) << 4];
+        const double2 vm2 = col[((y0 - 2) & 15) << 4], vm1 = col[((y0 - 1) & 15) << 4];
+        const double2 vp2 = col[((y0 + 2) & 15) << 4], vp3 = col[((y0 + 3) & 15) << 4];
+        const double2 vp4 = col[((y0 + 4) & 15) << 4], vp5 = col[((y0 + 5) & 15) << 4];
+        const int s0 = i + 4 * l, s1 = s0 + 2;
+        pair_acc(h[s0], cv[s1], vm1, A1, B1);
+        pair_acc(h[s0], vp2, vm2, A2, B2);
+        pair_acc(h[s0], vp3, vm3, A3, B3);
+        pair_acc(h[s0], vp4, vm4, A4, B4);
+        pair_acc(h[s1], vp2, cv[s0], A1, B1);
+        pair_acc(h[s1], vp3, vm1, A2, B2);
+        pair_acc(h[s1], vp4, vm2, A3, B3);
+        pair_acc(h[s1], vp5, vm3, A4, B4);
+      }
+    }
+    // ---- z neighbours: per (x, y) column, z = 4 bz - 4 .. 4 bz + 7 ----
+    {
+      const double Bz[4] = {kn[8], kn[9], kn[10], kn[11]};
+      const double Az[4] = {bk.mhl[8], bk.mhl[9], bk.mhl[10], bk.mhl[11]};
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        const int i = r & 1, j = r >> 1;
+        const double2* col = buf + ((2 * by + j) << 4) + (i << 3) + bx;
+        double2 zm[4], zp[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          zm[e] = col[((z0 - 4 + e) & 15) << 8];   // z offset e - 4
+          zp[e] = col[((z0 + BZ + e) & 15) << 8];  // z offset BZ + e
+        }
+#pragma unroll
+        for (int l = 0; l < BZ; ++l) {
+          const int s = i + 2 * j + 4 * l;
+#pragma unroll
+          for (int d = 1; d <= 4; ++d) {
+            const int ep = l + d, em = l - d;  // z offsets of the pair, -4 .. BZ + 3
+            const double2 tp = ep < BZ ? cv[i + 2 * j + 4 * (ep % BZ)] : zp[(ep - BZ) & 3];
+            const double2 tm = em >= 0 ? cv[i + 2 * j + 4 * (em % BZ)] : zm[(em + 4) & 3];
+            pair_acc(h[s], tp, tm, Az[d - 1], Bz[d - 1]);
+          }
+        }
+      }
+    }
+    // ---- diagonal, KB contributions, Taylor update (taylor.f90:47-117) ----
+    const bool last = nn == nterm - 1;
+    // zc(nn + 1) by constant indices (no local-memory copy of the argument)
+    double2 zn = zc.v[0];
+#pragma unroll
+    for (int q = 1; q < STEP_MAX_NTERM; ++q)
+      if (nn == q) zn = zc.v[q];
+    uint32_t pw[NS];
+#pragma unroll
+    for (int hh = 0; hh < NS / 8; ++hh) {
+      uint32_t w8[8];
+      tmem::ld8(tb + TW_PM + 8 * hh, w8);
+#pragma unroll
+      for (int u = 0; u < 8; ++u) pw[8 * hh + u] = w8[u];
+    }
+#pragma unroll
+    for (int q4 = 0; q4 < NS / 4; ++q4) {
+      uint32_t dw[8], aw[16];
+      tmem::ld8(tb + TW_D + 8 * q4, dw);
+      if (nn > 0) tmem::ld16(tb + TW_ACC + 16 * q4, aw);
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int s = 4 * q4 + u;
+        const double dg = tmem::as_double(dw[2 * u], dw[2 * u + 1]);
+        double2 hs = make_double2(fma(dg, cv[s].x, h[s].x), fma(dg, cv[s].y, h[s].y));
+        const int pm = (int)pw[s];
+        if (pm >= 0) {
+          const int p1 = (pm >> 8) + (pm & 255);
+          for (int pr = pm >> 8; pr < p1; ++pr) {
+            const double2 cc = pc[plist[pr]];
+            hs = make_double2(hs.x + cc.x, hs.y + cc.y);
+          }
+        }
+        h[s] = hs;
+        // psi_out = psi + zc_1 h_1 (first term), psi_out + zc_n h_n (later terms)
+        const double2 ao = nn == 0 ? cv[s]
+                                   : make_double2(tmem::as_double(aw[4 * u], aw[4 * u + 1]),
+                                                  tmem::as_double(aw[4 * u + 2], aw[4 * u + 3]));
+        const double2 an = make_double2(fma(zn.x, hs.x, fma(-zn.y, hs.y, ao.x)),
+                                        fma(zn.x, hs.y, fma(zn.y, hs.x, ao.y)));
+        if (last) {
+          const int x = 2 * bx + (s & 1), y = 2 * by + ((s >> 1) & 1), z = z0 + (s >> 2);
+          odst[gidx(x, y, z)] = an;
+          if (OBS) cv[s] = an;  // the new orbital, for the observables
+        } else {
+          aw[4 * u] = tmem::lo_word(an.x);
+          aw[4 * u + 1] = tmem::hi_word(an.x);
+          aw[4 * u + 2] = tmem::lo_word(an.y);
+          aw[4 * u + 3] = tmem::hi_word(an.y);
+        }
+      }
+      if (!last) tmem::st16(tb + TW_ACC + 16 * q4, aw);
+    }
+    if (last) break;
+    __syncthreads();  // every read of h_{n-1} and of the contributions is done
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+      const int x = 2 * bx + (s & 1), y = 2 * by + ((s >> 1) & 1), z = z0 + (s >> 2);
+      buf[sidx(x, y, z)] = h[s];
+      cv[s] = h[s];
+    }
+    __syncthreads();
+    if (kb) {
+      project_contrib<NW>(buf, sph, suv, spt, pc, T, a, warp, lane);
+      __syncthreads();
+    }
+  }
+  if (OBS) {
+    __syncthreads();  // the last term's reads of h_{n-1} are done
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+      const int x = 2 * bx + (s & 1), y = 2 * by + ((s >> 1) & 1), z = z0 + (s >> 2);
+      buf[sidx(x, y, z)] = cv[s];
+    }
+    __syncthreads();
+    double q[OBS_NQ];
+#pragma unroll
+    for (int i = 0; i < OBS_NQ; ++i) q[i] = 0.0;
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+      const double r2 = cv[s].x * cv[s].x + cv[s].y * cv[s].y;
+      q[0] += r2;
+      q[4] += ((double)(2 * bx + (s & 1)) + a.off[0]) * r2;
+      q[5] += ((double)(2 * by + ((s >> 1) & 1)) + a.off[1]) * r2;
+      q[6] += ((double)(z0 + (s >> 2)) + a.off[2]) * r2;
+    }
+#pragma unroll
+    for (int r = 0; r < 2 * BZ; ++r) {  // x: t(+1 .. +4)
+      const int j = r & 1, l = r >> 1;
+      const double2* row = buf + ((z0 + l) << 8) + ((2 * by + j) << 4);
+      const double2 vp2 = row[hp1], vp3 = row[8 + hp1], vp4 = row[hp2], vp5 = row[8 + hp2];
+      const int s0 = 2 * j + 4 * l, s1 = s0 + 1;
+      q[1] += cur_term(a.nab[0], cv[s0], cv[s1]) + cur_term(a.nab[1], cv[s0], vp2) +
+              cur_term(a.nab[2], cv[s0], vp3) + cur_term(a.nab[3], cv[s0], vp4);
+      q[1] += cur_term(a.nab[0], cv[s1], vp2) + cur_term(a.nab[1], cv[s1], vp3) +
+              cur_term(a.nab[2], cv[s1], vp4) + cur_term(a.nab[3], cv[s1], vp5);
+    }
+#pragma unroll
+    for (int r = 0; r < 2 * BZ; ++r) {  // y
+      const int i = r & 1, l = r >> 1;
+      const double2* col = buf + ((z0 + l) << 8) + (i << 3) + bx;
+      const int y0 = 2 * by;
+      const double2 vp2 = col[((y0 + 2) & 15) << 4], vp3 = col[((y0 + 3) & 15) << 4];
+      const double2 vp4 = col[((y0 + 4) & 15) << 4], vp5 = col[((y0 + 5) & 15) << 4];
+      const int s0 = i + 4 * l, s1 = s0 + 2;
+      q[2] += cur_term(a.nab[4], cv[s0], cv[s1]) + cur_term(a.nab[5], cv[s0], vp2) +
+              cur_term(a.nab[6], cv[s0], vp3) + cur_term(a.nab[7], cv[s0], vp4);
+      q[2] += cur_term(a.nab[4], cv[s1], vp2) + cur_term(a.nab[5], cv[s1], vp3) +
+              cur_term(a.nab[6], cv[s1], vp4) + cur_term(a.nab[7], cv[s1], vp5);
+    }
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {  // z
+      const int i = r & 1, j = r >> 1;
+      const double2* col = buf + ((2 * by + j) << 4) + (i << 3) + bx;
+      double2 zp[4];
+#pragma unroll
+      for (int e = 0; e < 4; ++e) zp[e] = col[((z0 + BZ + e) & 15) << 8];
+#pragma unroll
+      for (int l = 0; l < BZ; ++l) {
+        const int s = i + 2 * j + 4 * l;
+#pragma unroll
+        for (int d = 1; d <= 4; ++d) {
+          const int ep = l + d;
+          const double2 tp = ep < BZ ? cv[i + 2 * j + 4 * (ep % BZ)] : zp[(ep - BZ) & 3];
+          q[3] += cur_term(a.nab[8 + d - 1], cv[s], tp);
+        }
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < OBS_NQ; ++i) {
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) q[i] += __shfl_xor_sync(0xffffffffu, q[i], off);
+    }
+    if (lane == 0)
+      for (int i = 0; i < OBS_NQ; ++i) red[i][warp] = q[i];
+    // nonlocal current: one warp per atom (density_matrix.f90:532-591)
+    double jx = 0.0, jy = 0.0, jz = 0.0;
+    if (kb) {
+      for (int atom = warp; atom < a.natom; atom += NW) {
+        const int start = __ldg(a.atom_start + atom), m = __ldg(a.mps + atom);
+        const int lma0 = __ldg(a.lma_start + atom), np = __ldg(a.nproj + atom);
+        if (np == 0) continue;
+        double2 uq[4], ur[4][3];
+#pragma unroll
+        for (int qq = 0; qq < 4; ++qq) {
+          uq[qq] = make_double2(0.0, 0.0);
+          ur[qq][0] = ur[qq][1] = ur[qq][2] = uq[qq];
+        }
+        for (int j = lane; j < m; j += 32) {
+          const int fp = start + j;
+          const double2 ev = cmul(sph[fp], buf[spt[fp]]);
+          const double* rr = a.pt_r + 3L * fp;
+          const double r0 = __ldg(rr), r1 = __ldg(rr + 1), r2 = __ldg(rr + 2);
+#pragma unroll
+          for (int qq = 0; qq < 4; ++qq) {
+            if (qq < np) {
+              const double u = suv[qq * T + fp];
+              const double2 tq = make_double2(u * ev.x, u * ev.y);
+              uq[qq] = make_double2(uq[qq].x + tq.x, uq[qq].y + tq.y);
+              ur[qq][0] = make_double2(fma(r0, tq.x, ur[qq][0].x), fma(r0, tq.y, ur[qq][0].y));
+              ur[qq][1] = make_double2(fma(r1, tq.x, ur[qq][1].x), fma(r1, tq.y, ur[qq][1].y));
+              ur[qq][2] = make_double2(fma(r2, tq.x, ur[qq][2].x), fma(r2, tq.y, ur[qq][2].y));
+            }
+          }
+        }
+#pragma unroll
+        for (int qq = 0; qq < 4; ++qq) {
+#pragma unroll
+          for (int off = 16; off > 0; off >>= 1) {
+            uq[qq].x += __shfl_xor_sync(0xffffffffu, uq[qq].x, off);
+            uq[qq].y += __shfl_xor_sync(0xffffffffu, uq[qq].y, off);
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+              ur[qq][d].x += __shfl_xor_sync(0xffffffffu, ur[qq][d].x, off);
+              ur[qq][d].y += __shfl_xor_sync(0xffffffffu, ur[qq][d].y, off);
+            }
+          }
+        }
+#pragma unroll
+        for (int qq = 0; qq < 4; ++qq) {
+          if (qq < np) {
+            const double rv = __ldg(a.rinv + lma0 + qq);
+            const double2 us = make_double2(rv * uq[qq].x, rv * uq[qq].y);
+            jx += ur[qq][0].x * us.y - ur[qq][0].y * us.x;
+            jy += ur[qq][1].x * us.y - ur[qq][1].y * us.x;
+            jz += ur[qq][2].x * us.y - ur[qq][2].y * us.x;
+          }
+        }
+      }
+    }
+    if (lane == 0) {
+      jws[warp][0] = jx;
+      jws[warp][1] = jy;
+      jws[warp][2] = jz;
+    }
+    __syncthreads();
+    if (t < OBS_NQ) {
+      double sum = 0.0;
+      for (int w = 0; w < NW; ++w) sum += red[t][w];
+      a.obs[(long)o * OBS_NQ + t] = sum;
+    } else if (t >= 32 && t < 35 && a.jw != nullptr) {  // no nonlocal current without projectors
+      double sum = 0.0;
+      for (int w = 0; w < NW; ++w) sum += jws[w][t - 32];
+      a.jw[3L * o + (t - 32)] = sum;
+    }
+  }
+  tmem::fence_before_sync();
+  __syncthreads();
+  tmem::fence_after_sync();
+  if (warp == 0) tmem::dealloc(s_tmem, TMEM_COLS);
+}
+
+}  // namespace
+
+// Shared memory of the blocked fused step for the context's KB tables (bytes),
+// or 0 when the form does not apply.
+size_t step_blk_smem(const sb200_ctx* c) {
+  const PPInfo& pp = c->pp;
+  const size_t T = pp.nlma > 0 ? (size_t)pp.totpts : 0;
+  const size_t npair = pp.nlma > 0 ? (size_t)pp.npair : 0;
+  if (pp.nlma > 0 && (pp.npair <= 0 || pp.d_pmap2 == nullptr || pp.d_pair_fp == nullptr || pp.nprojmax > 4))
+    return 0;  // no (point, atom) pair form
+  return (size_t)NPTS * sizeof(double2) + T * (2 * sizeof(double2) + 4 * sizeof(double) + sizeof(int)) +
+         npair * sizeof(int);
+}
+
+int launch_step_blk(sb200_ctx* c, const double2* in, double2* out, const OrbArgs& a, const StepZC& z, int n_hamil,
+                    bool with_obs) {
+  constexpr size_t SMEM_MAX = 227 * 1024 - 2048;  // less the static arrays (at most 1.4 KB)
+  const size_t smem = step_blk_smem(c);
+  if (smem == 0 || smem > SMEM_MAX) return SB200_ERR_UNSUPPORTED;
+  static bool attr_set = false;
+  if (!attr_set) {
+    SB_CUDA(cudaFuncSetAttribute(k_step_blk<2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
+    SB_CUDA(cudaFuncSetAttribute(k_step_blk<2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
+    SB_CUDA(cudaFuncSetAttribute(k_step_blk<4, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
+    SB_CUDA(cudaFuncSetAttribute(k_step_blk<4, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
+    attr_set = true;
+  }
+  BlkArgs bk;
+  for (int i = 0; i < 12; ++i) bk.mhl[i] = -0.5 * c->g.coef_lap[i];
+  bk.npair = c->pp.nlma > 0 ? c->pp.npair : 0;
+  bk.pmap2 = c->pp.d_pmap2;
+  bk.pair_fp = c->pp.d_pair_fp;
+  dim3 grid(c->orb.norb);
+  if (c->blk_depth == 4) {
+    if (with_obs) k_step_blk<4, true><<<grid, Blk<4>::BT, smem, c->stream>>>(in, out, a, bk, z, n_hamil);
+    else k_step_blk<4, false><<<grid, Blk<4>::BT, smem, c->stream>>>(in, out, a, bk, z, n_hamil);
+  } else {
+    if (with_obs) k_step_blk<2, true><<<grid, Blk<2>::BT, smem, c->stream>>>(in, out, a, bk, z, n_hamil);
+    else k_step_blk<2, false><<<grid, Blk<2>::BT, smem, c->stream>>>(in, out, a, bk, z, n_hamil);
+  }
+  SB_LAUNCH_CHECK("k_step_blk");
+  return SB200_OK;
+}
+
+}  // namespace sb200

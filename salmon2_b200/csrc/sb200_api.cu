@@ -10,6 +10,7 @@
 #include <vector>
 
 #include "sb200_internal.cuh"
+#include "sb200_orbital.cuh"
 
 using namespace sb200;
 
@@ -136,6 +137,9 @@ void free_pp(PPInfo& p) {
   dfree(p.d_pair_uv);
   dfree(p.d_pair_fp);
   dfree(p.d_pair_ph);
+  dfree(p.d_blk_uv);
+  dfree(p.d_blk_r);
+  dfree(p.d_blk_sap);
   p = PPInfo();
 }
 
@@ -703,6 +707,7 @@ int sb200_set_pp(sb200_ctx* c, int natom, int nps, int nlma, const int* mps, con
     TRY(upload(&p.d_pair_lma, pair_lma));
     TRY(upload(&p.d_pair_uv, pair_uv));
     TRY(upload(&p.d_pair_fp, pair_fp));
+    TRY(blk_build_tables(c, pt_lin, apj, huv, pt_r, atom_start, hmps, lma_start, nproj));
     TRY(dalloc(&p.d_pair_ph, (size_t)p.nk_phase * (p.npair > 0 ? p.npair : 1)));
     if (!g.periodic) {  // isolated: exp(i 0.r) = 1
       std::vector<double2> one(p.npair > 0 ? p.npair : 1, make_double2(1.0, 0.0));

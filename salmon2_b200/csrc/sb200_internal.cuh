@@ -81,6 +81,11 @@ struct PPInfo {
   double2* d_pair_ph = nullptr; // [nk_phase][npair]
   int* d_pair_pt = nullptr;     // [npair] grid point of the pair
   int* d_apj = nullptr;         // [totpts] pair of each flat sphere point
+  // the register-blocked fused step's tables in its shared-memory layout (16^3 grids)
+  int blk_tpad = 0;
+  double* d_blk_uv = nullptr;   // [4][blk_tpad]
+  double* d_blk_r = nullptr;    // [3][blk_tpad]
+  int* d_blk_sap = nullptr;     // [blk_tpad]
 };
 
 struct RTBuffers {

@@ -2,6 +2,8 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <vector>
+
 struct sb200_ctx;
 
 namespace sb200 {
@@ -46,11 +48,20 @@ struct BlkArgs {
   double mhl[12];      // -coef_lap / 2
   int npair;           // (point, atom) pairs
   const int* pmap2;    // [npts] (first pair << 8) | count, or -1
-  const int* pair_fp;  // [npair] flat sphere point of each pair (point-major)
+  int tpad;            // flat sphere points rounded up to a multiple of 4
+  const double* uv4;   // [4][tpad] uV of each sphere point's atom projectors
+  const double* r3;    // [3][tpad] sphere-point coordinates
+  const int* sap;      // [tpad] (pair index << 12) | shared-memory grid index
+  int* err;            // device error flag (a bounded wait expired)
 };
 
 // The register-blocked fused step; SB200_ERR_UNSUPPORTED (no error recorded)
 // when its shared-memory tables do not fit or the KB tables have no pair form.
+// Host-side tables of the blocked fused step (called by sb200_set_pp).
+int blk_build_tables(sb200_ctx* c, const std::vector<int>& pt_lin, const std::vector<int>& apj,
+                     const std::vector<double>& uv_lma, const std::vector<double>& pt_r,
+                     const std::vector<int>& atom_start, const std::vector<int>& mps,
+                     const std::vector<int>& lma_start, const std::vector<int>& nproj);
 int launch_step_blk(sb200_ctx* c, const double2* in, double2* out, const OrbArgs& a, const StepZC& z, int n_hamil,
                     bool with_obs);
 

@@ -47,6 +47,7 @@
 
 #include "sb200_internal.cuh"
 #include "sb200_orbital.cuh"
+#include "sb200_tma.cuh"
 #include "sb200_tmem.cuh"
 
 namespace sb200 {
@@ -89,27 +90,45 @@ __device__ __forceinline__ double cur_term(const double nab, const double2 c, co
 __device__ __forceinline__ int gidx(int x, int y, int z) { return (z << 8) | (y << 4) | x; }
 __device__ __forceinline__ int sidx(int x, int y, int z) { return (z << 8) | (y << 4) | ((x & 1) << 3) | (x >> 1); }
 
-// Projections of the orbital in shared memory, one warp per atom, followed by
-// the per-sphere-point KB contributions pc[fp] = conj(e) sum_q uV_q P_q.
+// Projections of the orbital in shared memory and the KB contributions
+// pc[pr] = conj(e) sum_q uV_q P_q of every (point, atom) pair pr, stored in
+// point-major pair order so that each grid point's owner reads its pairs as
+// one contiguous run.  sap[fp] packs, for flat sphere point fp, its pair index
+// (bits 12..30) and its shared-memory grid index (bits 0..11).
+// SPLIT = 1: one warp per atom.  SPLIT = 2: a pair of warps per atom, warp
+// 2p + h taking the 32-point chunks 2k + h of the sphere; the pair meets at a
+// named barrier and both form P_q = rinv_q (part_2p + part_2p+1) in that
+// fixed order, so the result does not depend on timing.
+#ifndef SB200_PROJ_SPLIT
+#define SB200_PROJ_SPLIT 1
+#endif
+constexpr int SPLIT = SB200_PROJ_SPLIT;
+
+__device__ __forceinline__ void pair_barrier(int pair) {
+  asm volatile("bar.sync %0, 64;" ::"r"(1 + pair) : "memory");
+}
+
 template <int NW>
 __device__ __forceinline__ void project_contrib(const double2* __restrict__ buf, const double2* __restrict__ sph,
-                                                const double* __restrict__ suv, const int* __restrict__ spt,
-                                                double2* __restrict__ pc, int T, const OrbArgs& a, int warp,
-                                                int lane) {
-  for (int atom = warp; atom < a.natom; atom += NW) {
+                                                const double* __restrict__ suv, const int* __restrict__ sap,
+                                                double2* __restrict__ pc, double2 (*ppart)[4], int TP,
+                                                const OrbArgs& a, int warp, int lane) {
+  const int grp = warp / SPLIT, part = warp % SPLIT;
+  for (int atom = grp; atom < a.natom; atom += NW / SPLIT) {
     const int start = __ldg(a.atom_start + atom), m = __ldg(a.mps + atom);
     const int lma0 = __ldg(a.lma_start + atom), np = __ldg(a.nproj + atom);
-    if (np == 0) continue;  // no projectors: its sphere points have no pairs
+    if (np == 0) continue;  // no projectors: no pairs (the same for every warp of the group)
     double2 pq[4];
 #pragma unroll
     for (int q = 0; q < 4; ++q) pq[q] = make_double2(0.0, 0.0);
-    for (int j = lane; j < m; j += 32) {
+#pragma unroll 3
+    for (int j = lane + 32 * part; j < m; j += 32 * SPLIT) {
       const int fp = start + j;
-      const double2 ev = cmul(sph[fp], buf[spt[fp]]);
+      const double2 ev = cmul(sph[fp], buf[sap[fp] & 4095]);
 #pragma unroll
       for (int q = 0; q < 4; ++q)
         if (q < np) {
-          const double u = suv[q * T + fp];
+          const double u = suv[q * TP + fp];
           pq[q] = make_double2(fma(u, ev.x, pq[q].x), fma(u, ev.y, pq[q].y));
         }
     }
@@ -120,20 +139,37 @@ __device__ __forceinline__ void project_contrib(const double2* __restrict__ buf,
         pq[q].x += __shfl_xor_sync(0xffffffffu, pq[q].x, off);
         pq[q].y += __shfl_xor_sync(0xffffffffu, pq[q].y, off);
       }
+    }
+    if (SPLIT == 2) {
+      if (lane == 0) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) ppart[warp][q] = pq[q];
+      }
+      pair_barrier(grp);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const double2 p0 = ppart[2 * grp][q], p1 = ppart[2 * grp + 1][q];
+        pq[q] = make_double2(p0.x + p1.x, p0.y + p1.y);
+      }
+      pair_barrier(grp);  // both warps have read the partial sums before the next atom's
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
       const double r = q < np ? __ldg(a.rinv + lma0 + q) : 0.0;
       pq[q] = make_double2(r * pq[q].x, r * pq[q].y);
     }
-    for (int j = lane; j < m; j += 32) {
+#pragma unroll 3
+    for (int j = lane + 32 * part; j < m; j += 32 * SPLIT) {
       const int fp = start + j;
       double2 sp = make_double2(0.0, 0.0);
 #pragma unroll
       for (int q = 0; q < 4; ++q)
         if (q < np) {
-          const double u = suv[q * T + fp];
+          const double u = suv[q * TP + fp];
           sp = make_double2(fma(u, pq[q].x, sp.x), fma(u, pq[q].y, sp.y));
         }
       const double2 e = sph[fp];
-      pc[fp] = cmul(make_double2(e.x, -e.y), sp);
+      pc[sap[fp] >> 12] = cmul(make_double2(e.x, -e.y), sp);
     }
   }
 }
@@ -142,22 +178,25 @@ template <int BZ, bool OBS>
 __global__ void __launch_bounds__(Blk<BZ>::BT, 1) k_step_blk(const double2* __restrict__ in,
                                                              double2* __restrict__ out, OrbArgs a, BlkArgs bk,
                                                              StepZC zc, int nterm) {
-  constexpr int BT = Blk<BZ>::BT, NW = Blk<BZ>::NW, NS = Blk<BZ>::NS;
+  constexpr int NW = Blk<BZ>::NW, NS = Blk<BZ>::NS;
   constexpr uint32_t TW_ACC = Blk<BZ>::TW_ACC, TW_D = Blk<BZ>::TW_D, TW_PM = Blk<BZ>::TW_PM;
   constexpr uint32_t TW_WARP = Blk<BZ>::TW_WARP;
   extern __shared__ __align__(16) double2 smem[];
   const int T = a.totpts;
   const bool kb = a.nlma > 0;
+  const int TP = bk.tpad;                   // T rounded up to a multiple of 4
   double2* buf = smem;                      // [4096] the orbital h_{n-1}, split-x layout
-  double2* sph = buf + NPTS;                // [T] phase of the CTA's k-point
-  double2* pc = sph + T;                    // [T] KB contribution of each sphere point
-  double* suv = (double*)(pc + T);          // [4][T] uV of the atom's projectors
-  int* spt = (int*)(suv + 4 * T);           // [T] shared-memory index of each sphere point
-  int* plist = spt + T;                     // [npair] pairs of each grid point (flat sphere points)
+  double2* sph = buf + NPTS;                // [TP] phase of the CTA's k-point
+  double* suv = (double*)(sph + TP);        // [4][TP] uV of the atom's projectors
+  double* sr = suv + 4 * TP;                // [3][TP] coordinates of the sphere points
+  double2* pc = (double2*)(sr + 3 * TP);    // [npair] KB contribution of each (point, atom) pair
+  int* sap = (int*)(pc + bk.npair);         // [TP] pair index << 12 | shared-memory index of each sphere point
   __shared__ uint32_t s_tmem;
   __shared__ double kn[12];
   __shared__ double red[OBS_NQ][NW];
   __shared__ double jws[NW][3];
+  __shared__ double2 ppart[SPLIT == 2 ? NW : 1][4];  // projection partial sums of each warp
+  __shared__ __align__(8) uint64_t s_bar;             // completion of the table copies
 
   const int o = blockIdx.x, t = threadIdx.x, warp = t >> 5, lane = t & 31;
   const int bx = t & 7, by = (t >> 3) & 7, bz = t >> 6;
@@ -167,6 +206,18 @@ __global__ void __launch_bounds__(Blk<BZ>::BT, 1) k_step_blk(const double2* __re
 
   if (warp == 0) tmem::alloc(&s_tmem, TMEM_COLS);
   if (t < 12) kn[t] = __ldg(kc + 4 + t);  // k_nabt(s, d) = kAc_d nab(s, d)
+  if (kb && t == 32) {
+    // the k-point's KB tables: bulk copies (no multicast) into shared memory,
+    // completion counted on s_bar; they overlap the orbital load below
+    tma::mbar_init(&s_bar, 1);
+    tma::fence_barrier_init();
+    const unsigned b_ph = 16u * T, b_uv = 32u * TP, b_r = 24u * TP, b_ap = 4u * TP;
+    tma::mbar_arrive_expect_tx(&s_bar, b_ph + b_uv + b_r + b_ap);
+    tma::bulk_load(sph, a.phase + (long)ik * T, b_ph, &s_bar);
+    tma::bulk_load(suv, bk.uv4, b_uv, &s_bar);
+    tma::bulk_load(sr, bk.r3, b_r, &s_bar);
+    tma::bulk_load(sap, bk.sap, b_ap, &s_bar);
+  }
 
   // psi -> registers and the shared orbital buffer
   const double2* src = in + (long)o * a.npts;
@@ -180,23 +231,6 @@ __global__ void __launch_bounds__(Blk<BZ>::BT, 1) k_step_blk(const double2* __re
   for (int s = 0; s < NS; ++s) {
     const int x = 2 * bx + (s & 1), y = 2 * by + ((s >> 1) & 1), z = z0 + (s >> 2);
     buf[sidx(x, y, z)] = cv[s];
-  }
-  if (kb) {  // the k-point's KB tables
-    const double2* gph = a.phase + (long)ik * T;
-    for (int i = t; i < T; i += BT) {
-      sph[i] = __ldg(gph + i);
-      const int p = __ldg(a.pt_lin + i);
-      spt[i] = sidx(p & 15, (p >> 4) & 15, p >> 8);
-    }
-    for (int atom = 0; atom < a.natom; ++atom) {
-      const int start = __ldg(a.atom_start + atom), m = __ldg(a.mps + atom);
-      const int lma0 = __ldg(a.lma_start + atom), np = __ldg(a.nproj + atom);
-      for (int j = t; j < m; j += BT) {
-#pragma unroll
-        for (int q = 0; q < 4; ++q) suv[q * T + start + j] = q < np ? __ldg(a.uv + (long)(lma0 + q) * a.nps + j) : 0.0;
-      }
-    }
-    for (int i = t; i < bk.npair; i += BT) plist[i] = __ldg(bk.pair_fp + i);
   }
   tmem::fence_before_sync();
   __syncthreads();
@@ -229,8 +263,21 @@ __global__ void __launch_bounds__(Blk<BZ>::BT, 1) k_step_blk(const double2* __re
       tmem::st8(tb + TW_PM + 8 * hh, w);
     }
   }
+  // the tables have arrived (bounded wait; on expiry: flag, wait once more for
+  // the copies in flight, skip the step, release TMEM)
+  bool ok = true;
+  if (kb) ok = tma::mbar_wait(&s_bar, 0);
+  ok = __syncthreads_and(ok);
+  if (!ok) {
+    if (t == 0) {
+      atomicExch(bk.err, 1);
+      tma::mbar_wait(&s_bar, 0);
+    }
+    __syncthreads();
+  }
+  if (ok) {
   if (kb) {
-    project_contrib<NW>(buf, sph, suv, spt, pc, T, a, warp, lane);
+    project_contrib<NW>(buf, sph, suv, sap, pc, ppart, TP, a, warp, lane);
     __syncthreads();
   }
   const int hm2 = (bx - 2) & 7, hm1 = (bx - 1) & 7, hp1 = (bx + 1) & 7, hp2 = (bx + 2) & 7;
@@ -331,16 +378,23 @@ __global__ void __launch_bounds__(Blk<BZ>::BT, 1) k_step_blk(const double2* __re
       uint32_t dw[8], aw[16];
       tmem::ld8(tb + TW_D + 8 * q4, dw);
       if (nn > 0) tmem::ld16(tb + TW_ACC + 16 * q4, aw);
+      double2 c1[4];  // each point's first pair, loaded before any is used
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int pm = (int)pw[4 * q4 + u];
+        c1[u] = pm >= 0 ? pc[pm >> 8] : make_double2(0.0, 0.0);
+      }
 #pragma unroll
       for (int u = 0; u < 4; ++u) {
         const int s = 4 * q4 + u;
         const double dg = tmem::as_double(dw[2 * u], dw[2 * u + 1]);
         double2 hs = make_double2(fma(dg, cv[s].x, h[s].x), fma(dg, cv[s].y, h[s].y));
         const int pm = (int)pw[s];
-        if (pm >= 0) {
+        if (pm >= 0) {  // the point's pairs, atoms in ilma order
+          hs = make_double2(hs.x + c1[u].x, hs.y + c1[u].y);
           const int p1 = (pm >> 8) + (pm & 255);
-          for (int pr = pm >> 8; pr < p1; ++pr) {
-            const double2 cc = pc[plist[pr]];
+          for (int pr = (pm >> 8) + 1; pr < p1; ++pr) {
+            const double2 cc = pc[pr];
             hs = make_double2(hs.x + cc.x, hs.y + cc.y);
           }
         }
@@ -374,7 +428,7 @@ __global__ void __launch_bounds__(Blk<BZ>::BT, 1) k_step_blk(const double2* __re
     }
     __syncthreads();
     if (kb) {
-      project_contrib<NW>(buf, sph, suv, spt, pc, T, a, warp, lane);
+      project_contrib<NW>(buf, sph, suv, sap, pc, ppart, TP, a, warp, lane);
       __syncthreads();
     }
   }
@@ -461,9 +515,8 @@ __global__ void __launch_bounds__(Blk<BZ>::BT, 1) k_step_blk(const double2* __re
         }
         for (int j = lane; j < m; j += 32) {
           const int fp = start + j;
-          const double2 ev = cmul(sph[fp], buf[spt[fp]]);
-          const double* rr = a.pt_r + 3L * fp;
-          const double r0 = __ldg(rr), r1 = __ldg(rr + 1), r2 = __ldg(rr + 2);
+          const double2 ev = cmul(sph[fp], buf[sap[fp] & 4095]);
+          const double r0 = sr[fp], r1 = sr[TP + fp], r2 = sr[2 * TP + fp];
 #pragma unroll
           for (int qq = 0; qq < 4; ++qq) {
             if (qq < np) {
@@ -517,6 +570,7 @@ __global__ void __launch_bounds__(Blk<BZ>::BT, 1) k_step_blk(const double2* __re
       a.jw[3L * o + (t - 32)] = sum;
     }
   }
+  }  // ok
   tmem::fence_before_sync();
   __syncthreads();
   tmem::fence_after_sync();
@@ -525,36 +579,87 @@ __global__ void __launch_bounds__(Blk<BZ>::BT, 1) k_step_blk(const double2* __re
 
 }  // namespace
 
+// Host-built tables of the blocked fused step, in its shared-memory layout
+// (k-independent; the phases come per k from the context's phase table):
+// uV of each flat sphere point for the atom's projectors [4][tpad] (zero past
+// the atom's count), coordinates [3][tpad], and (pair index << 12) | the
+// split-x shared-memory index of its grid point [tpad].  Only for 16^3 grids
+// with the (point, atom) pair form and fewer than 2^19 pairs.
+int blk_build_tables(sb200_ctx* c, const std::vector<int>& pt_lin, const std::vector<int>& apj,
+                     const std::vector<double>& uv_lma, const std::vector<double>& pt_r,
+                     const std::vector<int>& atom_start, const std::vector<int>& mps,
+                     const std::vector<int>& lma_start, const std::vector<int>& nproj) {
+  PPInfo& p = c->pp;
+  const GridInfo& g = c->g;
+  if (!(g.nx == N && g.ny == N && g.nz == N) || p.npair <= 0 || p.npair >= (1 << 19) || p.nprojmax > 4)
+    return SB200_OK;
+  const int T = p.totpts, TP = (T + 3) & ~3;
+  std::vector<double> uv4(4 * (size_t)TP, 0.0), r3(3 * (size_t)TP, 0.0);
+  std::vector<int> sap(TP, 0);
+  for (size_t at = 0; at < atom_start.size(); ++at)
+    for (int j = 0; j < mps[at]; ++j) {
+      const int fp = atom_start[at] + j;
+      for (int q = 0; q < nproj[at] && q < 4; ++q) uv4[(size_t)q * TP + fp] = uv_lma[(size_t)(lma_start[at] + q) * p.nps + j];
+      for (int d = 0; d < 3; ++d) r3[(size_t)d * TP + fp] = pt_r[3 * (size_t)fp + d];
+      const int q = pt_lin[fp];
+      const int x = q & 15, y = (q >> 4) & 15, z = q >> 8;
+      sap[fp] = ((apj[fp] & 0x7ffff) << 12) | (z << 8) | (y << 4) | ((x & 1) << 3) | (x >> 1);
+    }
+  int r = dalloc(&p.d_blk_uv, uv4.size());
+  if (r == SB200_OK) r = dalloc(&p.d_blk_r, r3.size());
+  if (r == SB200_OK) r = dalloc(&p.d_blk_sap, sap.size());
+  if (r != SB200_OK) return r;
+  SB_CUDA(cudaMemcpy(p.d_blk_uv, uv4.data(), uv4.size() * sizeof(double), cudaMemcpyHostToDevice));
+  SB_CUDA(cudaMemcpy(p.d_blk_r, r3.data(), r3.size() * sizeof(double), cudaMemcpyHostToDevice));
+  SB_CUDA(cudaMemcpy(p.d_blk_sap, sap.data(), sap.size() * sizeof(int), cudaMemcpyHostToDevice));
+  p.blk_tpad = TP;
+  return SB200_OK;
+}
+
 // Shared memory of the blocked fused step for the context's KB tables (bytes),
 // or 0 when the form does not apply.
 size_t step_blk_smem(const sb200_ctx* c) {
   const PPInfo& pp = c->pp;
   const size_t T = pp.nlma > 0 ? (size_t)pp.totpts : 0;
   const size_t npair = pp.nlma > 0 ? (size_t)pp.npair : 0;
-  if (pp.nlma > 0 && (pp.npair <= 0 || pp.d_pmap2 == nullptr || pp.d_pair_fp == nullptr || pp.nprojmax > 4))
-    return 0;  // no (point, atom) pair form
-  return (size_t)NPTS * sizeof(double2) + T * (2 * sizeof(double2) + 4 * sizeof(double) + sizeof(int)) +
-         npair * sizeof(int);
+  if (pp.nlma > 0 && (pp.npair <= 0 || pp.d_pmap2 == nullptr || pp.d_blk_sap == nullptr))
+    return 0;  // no (point, atom) pair form, or no staged tables (blk_build_tables)
+  const size_t TP = pp.nlma > 0 ? (size_t)pp.blk_tpad : 0;
+  (void)T;
+  return (size_t)NPTS * sizeof(double2) + TP * (sizeof(double2) + 7 * sizeof(double) + sizeof(int)) +
+         npair * sizeof(double2);
 }
 
 int launch_step_blk(sb200_ctx* c, const double2* in, double2* out, const OrbArgs& a, const StepZC& z, int n_hamil,
                     bool with_obs) {
-  constexpr size_t SMEM_MAX = 227 * 1024 - 2048;  // less the static arrays (at most 1.4 KB)
   const size_t smem = step_blk_smem(c);
-  if (smem == 0 || smem > SMEM_MAX) return SB200_ERR_UNSUPPORTED;
-  static bool attr_set = false;
-  if (!attr_set) {
-    SB_CUDA(cudaFuncSetAttribute(k_step_blk<2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
-    SB_CUDA(cudaFuncSetAttribute(k_step_blk<2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
-    SB_CUDA(cudaFuncSetAttribute(k_step_blk<4, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
-    SB_CUDA(cudaFuncSetAttribute(k_step_blk<4, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
-    attr_set = true;
+  if (smem == 0) return SB200_ERR_UNSUPPORTED;
+  // per instantiation: the dynamic shared memory it may take next to its static arrays
+  static size_t cap[4] = {0, 0, 0, 0};
+  if (cap[0] == 0) {
+    const void* fns[4] = {(const void*)k_step_blk<2, false>, (const void*)k_step_blk<2, true>,
+                          (const void*)k_step_blk<4, false>, (const void*)k_step_blk<4, true>};
+    int optin = 0;
+    SB_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device));
+    for (int i = 0; i < 4; ++i) {
+      cudaFuncAttributes fa;
+      SB_CUDA(cudaFuncGetAttributes(&fa, fns[i]));
+      const size_t ci = (size_t)optin - fa.sharedSizeBytes;
+      SB_CUDA(cudaFuncSetAttribute(fns[i], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ci));
+      cap[i] = ci;
+    }
   }
+  const int which = (c->blk_depth == 4 ? 2 : 0) + (with_obs ? 1 : 0);
+  if (smem > cap[which]) return SB200_ERR_UNSUPPORTED;
   BlkArgs bk;
   for (int i = 0; i < 12; ++i) bk.mhl[i] = -0.5 * c->g.coef_lap[i];
   bk.npair = c->pp.nlma > 0 ? c->pp.npair : 0;
   bk.pmap2 = c->pp.d_pmap2;
-  bk.pair_fp = c->pp.d_pair_fp;
+  bk.tpad = c->pp.blk_tpad;
+  bk.uv4 = c->pp.d_blk_uv;
+  bk.r3 = c->pp.d_blk_r;
+  bk.sap = c->pp.d_blk_sap;
+  bk.err = c->d_err;
   dim3 grid(c->orb.norb);
   if (c->blk_depth == 4) {
     if (with_obs) k_step_blk<4, true><<<grid, Blk<4>::BT, smem, c->stream>>>(in, out, a, bk, z, n_hamil);

@@ -55,6 +55,9 @@ def parse():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--cpu-steps", type=int, default=4, help="Taylor steps in each CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-supercell", action="store_true",
+                    help="skip the supercell leg (FP64 and mixed) that the default periodic-bulk run adds")
+    ap.add_argument("--supercell-nt", type=int, default=100, help="Taylor steps per supercell sample")
     ap.add_argument("--self-consistent", action="store_true",
                     help="V_local = Vpsl + Vh[rho] + Vxc[rho] (PZ) recomputed after every Taylor step inside the "
                          "time loop (the fixed Gaussian potential stands in for Vpsl)")
@@ -209,6 +212,67 @@ def hpsi_kernel(s, args, units_per_launch):
         return "k_step_blk", UNIT_BYTES["fp64"] * units_per_launch  # register-blocked fused step
     name = "k_hpsi_tiled" if os.environ.get("SB200_TMA", "on").startswith("of") else "k_hpsi_tma"
     return name, UNIT_BYTES[args.precision] / 4.0 * units_per_launch
+
+
+def supercell_leg(args, local):
+    """The 2x2x2 supercell (32^3 grid, 64 atoms, 8 k-points, 256 orbitals/k,
+    band-limited orbitals |k+G|^2/2 <= 2 Ha) propagated in the FP64 and the mixed
+    form from the same start: throughput of each (resident orbitals, CUDA events
+    on the library stream, 1 warm-up + 2 timed samples of `--supercell-nt`
+    Taylor steps), the H psi kernel's roofline fraction, and the mixed form's
+    J(t) error against the FP64 run over one sample."""
+    import torch
+    from salmon2_b200 import synth
+    from salmon2_b200.rt import Context
+    s = synth.periodic_system(a=10.26, num=16, nkgrid=2, no=256, supercell=2, seed=3, ecut=2.0,
+                              name="periodic_supercell")
+    nt, dt = args.supercell_nt, 0.08
+    omega = 1.55 / synth.AU_ENERGY_EV
+    Ac = synth.asin2cos(nt, dt, omega=omega, f0=omega * 1e-3, tw=nt * dt)
+    zc = synth.taylor_zc(dt)
+    units = int(np.prod(s.grid.shape)) * s.norb * nt
+    peak, peak_kind = measured_peaks()
+    out = {"workload": (f"periodic supercell a=20.52 bohr, {s.pp.natom} atoms, {s.grid.shape[0]}^3 grid, {s.nk} "
+                        f"k-points, {s.no} complex128 orbitals/k (band-limited, |k+G|^2/2 <= 2 Ha), Asin2cos "
+                        f"A(t) peak 1e-3 au, {nt} Taylor-4 steps per sample"),
+           "units_per_sample": units, "peak_gbs": peak, "peak_source": peak_kind}
+    curr = {}
+    for prec in ("fp64", "mixed"):
+        ctx = Context(s, device=local, precision=prec)
+        stream = torch.cuda.Stream(device=local)
+        ctx.set_stream(stream)
+        psi0 = ctx.upload(s.psi)
+        a, b, w = ctx.empty(), ctx.zeros(), ctx.zeros()
+        a.copy_(psi0)
+        res = ctx.rt_propagate(a, b, w, nt, dt, zc, Ac_ext=Ac)  # warm-up; J(t) of the comparison
+        curr[prec] = np.array(res["curr"])
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(2):
+            ctx.rt_propagate(a, b, w, nt, dt, zc, Ac_ext=Ac)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        value = units * 2 / (e0.elapsed_time(e1) / 1e3)
+        ctx.set_timing(True)
+        ctx.kernel_times(reset=True)
+        ctx.rt_propagate(a, b, w, min(nt, 20), dt, zc, Ac_ext=Ac[:, : min(nt, 20) + 2])
+        kt = ctx.kernel_times(reset=True)
+        ctx.set_timing(False)
+        h_ms, h_cnt = kt.get("hpsi", (float("nan"), 1))
+        bytes_launch = UNIT_BYTES[prec] / 4.0 * units / nt
+        ach = bytes_launch / (h_ms / h_cnt / 1e3) / 1e9
+        out[prec] = {"value": value, "kernel": "k_hpsi_tma", "avg_launch_ms": h_ms / h_cnt,
+                     "algorithmic_bytes_per_launch": bytes_launch, "achieved_gbs": ach, "frac": ach / peak,
+                     "traffic": ncu_traffic("k_hpsi_tma", "supercell") if prec == "fp64" else None}
+        ctx.close()
+        del a, b, w, psi0
+        torch.cuda.empty_cache()
+    jmax = float(np.max(np.abs(curr["fp64"])))
+    out["mixed"]["speedup_vs_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
+    out["mixed"]["j_rel_err"] = float(np.max(np.abs(curr["mixed"] - curr["fp64"]))) / jmax
+    out["mixed"]["j_rel_err_budget"] = 1e-6
+    return out
 
 
 def ncu_traffic(kernel, workload):
@@ -581,6 +645,9 @@ def main():
                     "d2h_bytes_per_step": bytes_io + 3 * nt * 8 + 4 * nt * 8},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
+                         "traffic_source": (f"profiles/{kname}_{args.workload}.md: DRAM bytes of one launch "
+                                            "from an ncu capture of this workload, not measured in this run"
+                                            if traffic is not None else None),
                          "kernel": kname, "avg_launch_ms": avg_ms,
                          "algorithmic_bytes_per_launch": bytes_per_launch},
             "kernel_shares": shares,
@@ -588,6 +655,10 @@ def main():
             "clocks": clk.summary(),
             "cpu_baseline": cpu,
         }
+        if world == 1 and args.workload == "bulk" and args.precision == "fp64" and not args.self_consistent \
+                and not args.no_supercell:
+            ctx.close()
+            out["supercell"] = supercell_leg(args, local)
         print(json.dumps(out), flush=True)
     ctx.close()
     if world > 1:

@@ -531,18 +531,19 @@ def main():
     ctx.set_stream(stream)
     a, b, w = ctx.upload(s.psi), ctx.zeros(), ctx.zeros()
     units_rank = int(np.prod(s.grid.shape)) * s.norb * nt
+    if world > 1 and args.workload != "isolated":
+        # k-point shards: J(t) and the dipole sums of every step (and, self-consistent,
+        # the density) are summed over the ranks by an NCCL all-reduce inside the
+        # loop's CUDA graph -- the exchange step of the path
+        from salmon2_b200.rt import nccl_unique_id
+        uid = torch.zeros(128, dtype=torch.uint8, device=f"cuda:{local}")
+        if rank == 0:
+            uid.copy_(torch.frombuffer(bytearray(nccl_unique_id()), dtype=torch.uint8))
+        dist.broadcast(uid, 0)
+        ctx.set_density_comm(world, rank, bytes(uid.cpu().numpy().tobytes()))
     if args.self_consistent:
         if s.nspin != 1:
             raise SystemExit("--self-consistent needs a workload with one spin")
-        if world > 1:
-            # the density of every step is summed over the k-point shards (NCCL all-reduce
-            # inside the loop's graph) before the Hartree and XC potentials
-            from salmon2_b200.rt import nccl_unique_id
-            uid = torch.zeros(128, dtype=torch.uint8, device=f"cuda:{local}")
-            if rank == 0:
-                uid.copy_(torch.frombuffer(bytearray(nccl_unique_id()), dtype=torch.uint8))
-            dist.broadcast(uid, 0)
-            ctx.set_density_comm(world, rank, bytes(uid.cpu().numpy().tobytes()))
         # orthogonal box: primitive_b = 2 pi / L (the Hartree solve is poisson_ft on the
         # periodic cell, poisson_isolated_ft on an isolated box); V_local from rho(t=0),
         # then the update every step
@@ -557,11 +558,7 @@ def main():
         torch.cuda.synchronize()
 
     def one_step():
-        res = ctx.rt_propagate(a, b, w, nt, dt, zc, Ac_ext=Ac)
-        if world > 1:  # the exchange step of the path: J(t) summed over k shards
-            j = torch.from_numpy(np.ascontiguousarray(res["curr"])).cuda()
-            dist.all_reduce(j)
-        return res
+        return ctx.rt_propagate(a, b, w, nt, dt, zc, Ac_ext=Ac)
 
     for _ in range(args.warmup):
         one_step()
@@ -589,9 +586,6 @@ def main():
     def e2e_step():
         ctx.upload(host_in, out=a)
         res = ctx.rt_propagate(a, b, w, nt, dt, zc, Ac_ext=Ac)
-        if world > 1:
-            j = torch.from_numpy(np.ascontiguousarray(res["curr"])).cuda()
-            dist.all_reduce(j)
         ctx.download(res["psi"], out=host_out)
         return res
 

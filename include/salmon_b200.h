@@ -353,16 +353,19 @@ int sb200_update_vlocal(sb200_ctx* ctx, const double* Vpsl, const double* Vh, co
  * (src/rt/time_evolution_step.f90:160-207).                                    */
 int sb200_set_self_consistent(sb200_ctx* ctx, int enable, const double* Vpsl, const double primitive_b[9]);
 
-/* Density sum over k-point shards.  A job that gives each process (one per GPU)
- * a share of the k-points needs the density of all of them before the Hartree
- * and exchange-correlation potentials: with a communicator set,
- * sb200_calc_density and the self-consistent loop all-reduce rho (NCCL, in the
- * loop's CUDA graph) over the nranks processes.  id: 128 bytes from
+/* Sums over k-point shards.  A job that gives each process (one per GPU) a
+ * share of the k-points needs the density and the current of all of them:
+ * with a communicator set, sb200_calc_density and the self-consistent loop
+ * all-reduce rho (NCCL, in the loop's CUDA graph) over the nranks processes,
+ * and every step of sb200_rt_propagate (and sb200_calc_current) all-reduces
+ * J(t) and the dipole sums before calc_emfields updates the induced field,
+ * so trans_longi = 'lo' sees the current of the whole k-mesh.  id: 128 bytes from
  * sb200_nccl_unique_id on rank 0, passed to every rank by the host (MPI_Bcast,
  * torch.distributed).  nranks <= 0 removes the communicator.  NCCL is the
  * process's libnccl.so.2, loaded at run time (absent: SB200_ERR_UNSUPPORTED).
  * Replaces: comm_summation of rho over info%icomm_ko in calc_density
- * (src/common/density_matrix.f90:223).                                         */
+ * (src/common/density_matrix.f90:223) and of the current over info%icomm_rko
+ * in calc_current (src/common/density_matrix.f90:448).                          */
 int sb200_nccl_unique_id(unsigned char id[128]);
 int sb200_set_density_comm(sb200_ctx* ctx, int nranks, int rank, const unsigned char id[128]);
 

@@ -176,6 +176,11 @@ struct FinArgs {
   double* rbox_hist;       // (4, nt) or null
   double* result;          // [8] direct results (J3, rbox4) or null
   int* step;
+  // shard sums: 0 one pass; 1 write the 7 sums (J before 1/Ngrid, rbox) to
+  // sums and stop; 2 take the 7 sums from sums (all-reduced over the k-point
+  // shards in between) and finish
+  int stage;
+  double* sums;
 };
 
 // Called by one CTA of 256 threads.
@@ -189,7 +194,7 @@ __device__ __forceinline__ void finalize_body(const FinArgs& a) {
   }
   double s[7] = {0, 0, 0, 0, 0, 0, 0};
 #pragma unroll 4
-  for (int o = threadIdx.x; o < a.norb; o += blockDim.x) {
+  for (int o = threadIdx.x; o < a.norb && a.stage != 2; o += blockDim.x) {
     if (a.spin_filter >= 0 && (o % a.nspin) != a.spin_filter) continue;
     double q[OBS_NQ] = {0, 0, 0, 0, 0, 0, 0};
     for (int b = 0; b < a.nblk; ++b)
@@ -217,10 +222,16 @@ __device__ __forceinline__ void finalize_body(const FinArgs& a) {
     __syncthreads();
   }
   if (threadIdx.x == 0) {
+    if (a.stage == 1) {
+      for (int i = 0; i < 7; ++i) a.sums[i] = red[i][0];
+      return;
+    }
+    double tot[7];
+    for (int i = 0; i < 7; ++i) tot[i] = a.stage == 2 ? a.sums[i] : red[i][0];
     double J[3], rb[4];
-    for (int d = 0; d < 3; ++d) J[d] = red[d][0] * a.ngrid_inv;
-    for (int d = 0; d < 3; ++d) rb[d] = red[3 + d][0];
-    rb[3] = red[6][0];
+    for (int d = 0; d < 3; ++d) J[d] = tot[d] * a.ngrid_inv;
+    for (int d = 0; d < 3; ++d) rb[d] = tot[3 + d];
+    rb[3] = tot[6];
     if (a.result) {
       for (int d = 0; d < 3; ++d) a.result[d] = J[d];
       for (int d = 0; d < 4; ++d) a.result[3 + d] = rb[d];

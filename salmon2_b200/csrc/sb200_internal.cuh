@@ -258,5 +258,9 @@ int scf_rt_prepare(sb200_ctx* c);
 int scf_rt_issue(sb200_ctx* c, const double2* psi);
 // sum of a device density over the k-point shards (no-op without a communicator)
 int scf_density_allreduce(sb200_ctx* c, double* d_rho);
+// k-point shard communicator (sb200_set_density_comm): set?, and an in-place
+// sum of n device doubles over the shards on the context's stream
+bool shard_comm_set(const sb200_ctx* c);
+int shard_sum(sb200_ctx* c, double* d, size_t n);
 
 }  // namespace sb200

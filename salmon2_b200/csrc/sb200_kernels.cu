@@ -715,6 +715,8 @@ int launch_observables(sb200_ctx* c, const double2* psi) {
 // itt < 0: RT loop, index from the device step counter.
 FinArgs make_fin_args(const sb200_ctx* c, int itt, int trans_longi, double dt, int spin_filter, bool fused_obs) {
   FinArgs a;
+  a.stage = 0;  // one pass (launch_finalize splits it for k-point shards)
+  a.sums = nullptr;
   a.norb = c->orb.norb;
   a.jw_natom = fused_obs ? 1 : c->pp.natom;
   a.obs_stride = OBS_NQ;
@@ -776,6 +778,19 @@ int launch_finalize(sb200_ctx* c, int itt, int nt, int trans_longi, double dt, i
       a.jw_natom = 1;
       a.jw_stride = OBS_NQ + 3;
     }
+  }
+  a.stage = 0;
+  a.sums = c->d_result + 16;
+  if (shard_comm_set(c)) {
+    // k-point shards: the 7 sums of every shard added over the ranks before
+    // J(t) enters calc_emfields (comm_summation over icomm_rko,
+    // density_matrix.f90:448)
+    a.stage = 1;
+    k_finalize<<<1, 256, 0, c->stream>>>(a);
+    SB_LAUNCH_CHECK("k_finalize");
+    int r = shard_sum(c, a.sums, 7);
+    if (r != SB200_OK) return r;
+    a.stage = 2;
   }
   k_finalize<<<1, 256, 0, c->stream>>>(a);
   SB_LAUNCH_CHECK("k_finalize");

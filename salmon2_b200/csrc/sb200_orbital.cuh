@@ -53,6 +53,7 @@ struct BlkArgs {
   const double* r3;    // [3][tpad] sphere-point coordinates
   const int* sap;      // [tpad] (pair index << 12) | shared-memory grid index
   int* err;            // device error flag (a bounded wait expired)
+  int kbcache;         // 1: each atom's uV and phases kept in TMEM by its warp
 };
 
 // The register-blocked fused step; SB200_ERR_UNSUPPORTED (no error recorded)

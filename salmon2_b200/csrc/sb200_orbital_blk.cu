@@ -54,19 +54,46 @@ namespace sb200 {
 namespace {
 
 constexpr int N = 16, NP = N * N, NPTS = N * NP;
-constexpr uint32_t TMEM_COLS = 256;
+constexpr uint32_t TMEM_COLS = 512;
 // TMEM words (columns) per thread: psi_out 4 per point, diagonal 2 per point,
-// point-map word 1 per point; the NW / 4 warps of one lane quarter each use
-// 1024 / NW columns of the 256
+// point-map word 1 per point, then (warps that project one atom) 12 words per
+// 32-point chunk of its sphere: the lane's uV of the atom's 4 projectors and
+// its phase.  The NW / 4 warps of one lane quarter each use 2048 / NW of the
+// 512 columns.
 template <int BZ>
 struct Blk {
   static constexpr int BT = 1024 / BZ;  // threads
   static constexpr int NW = BT / 32;    // warps
   static constexpr int NS = 4 * BZ;     // own points per thread
-  static constexpr uint32_t TW_ACC = 0, TW_D = 4 * NS, TW_PM = 6 * NS;
+  static constexpr uint32_t TW_ACC = 0, TW_D = 4 * NS, TW_PM = 6 * NS, TW_KB = 7 * NS;
   static constexpr uint32_t TW_WARP = TMEM_COLS / (NW / 4);
-  static_assert(7 * NS <= TW_WARP, "TMEM words per thread");
+  static constexpr int KB_CHUNKS = (int)(TW_WARP - TW_KB) / 12;  // sphere chunks a warp can keep
+  static_assert(KB_CHUNKS >= 1, "TMEM words per thread");
 };
+
+// uV of the 4 projectors and the phase of one sphere point, kept in TMEM
+__device__ __forceinline__ void kb_store(uint32_t taddr, const double (&u)[4], double2 e) {
+  uint32_t w8[8], w4[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    w8[2 * q] = tmem::lo_word(u[q]);
+    w8[2 * q + 1] = tmem::hi_word(u[q]);
+  }
+  w4[0] = tmem::lo_word(e.x);
+  w4[1] = tmem::hi_word(e.x);
+  w4[2] = tmem::lo_word(e.y);
+  w4[3] = tmem::hi_word(e.y);
+  tmem::st8(taddr, w8);
+  tmem::st4(taddr + 8, w4);
+}
+__device__ __forceinline__ void kb_load(uint32_t taddr, double (&u)[4], double2& e) {
+  uint32_t w8[8], w4[4];
+  tmem::ld8(taddr, w8);
+  tmem::ld4(taddr + 8, w4);
+#pragma unroll
+  for (int q = 0; q < 4; ++q) u[q] = tmem::as_double(w8[2 * q], w8[2 * q + 1]);
+  e = make_double2(tmem::as_double(w4[0], w4[1]), tmem::as_double(w4[2], w4[3]));
+}
 
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
   return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
@@ -87,89 +114,132 @@ __device__ __forceinline__ double cur_term(const double nab, const double2 c, co
   return nab * (c.x * t.y - c.y * t.x);
 }
 
+// Sum of NV doubles (NV = 2^m <= 32) over the 32 lanes of a warp, by
+// reduce-scatter: at each level a lane keeps half of its live values and adds
+// its partner's copy of them, so NV - 1 + (5 - m) shuffles replace the 5 NV of
+// a butterfly per value.  Afterwards lane L holds the total of value
+// L >> (5 - m) (fixed operation order: the result does not depend on timing).
+template <int NV>
+__device__ __forceinline__ double warp_reduce_scatter(double (&v)[NV], int lane) {
+  static_assert(NV >= 1 && NV <= 32 && (NV & (NV - 1)) == 0, "NV");
+#pragma unroll
+  for (int lev = 0; lev < 5; ++lev) {
+    const int off = 16 >> lev, n = NV >> lev;
+    if (n > 1) {
+      const bool upper = (lane & off) != 0;
+#pragma unroll
+      for (int i = 0; i < n / 2; ++i) {
+        const double keep = upper ? v[n / 2 + i] : v[i];
+        const double send = upper ? v[i] : v[n / 2 + i];
+        v[i] = keep + __shfl_xor_sync(0xffffffffu, send, off);
+      }
+    } else {
+      v[0] += __shfl_xor_sync(0xffffffffu, v[0], off);
+    }
+  }
+  return v[0];
+}
+template <int NV>
+__device__ __forceinline__ int rs_lane(int k) {  // a lane holding value k after warp_reduce_scatter<NV>
+  return k << (5 - (NV == 1 ? 0 : NV == 2 ? 1 : NV == 4 ? 2 : NV == 8 ? 3 : NV == 16 ? 4 : 5));
+}
+
 __device__ __forceinline__ int gidx(int x, int y, int z) { return (z << 8) | (y << 4) | x; }
 __device__ __forceinline__ int sidx(int x, int y, int z) { return (z << 8) | (y << 4) | ((x & 1) << 3) | (x >> 1); }
 
 // Projections of the orbital in shared memory and the KB contributions
 // pc[pr] = conj(e) sum_q uV_q P_q of every (point, atom) pair pr, stored in
 // point-major pair order so that each grid point's owner reads its pairs as
-// one contiguous run.  sap[fp] packs, for flat sphere point fp, its pair index
-// (bits 12..30) and its shared-memory grid index (bits 0..11).
-// SPLIT = 1: one warp per atom.  SPLIT = 2: a pair of warps per atom, warp
-// 2p + h taking the 32-point chunks 2k + h of the sphere; the pair meets at a
-// named barrier and both form P_q = rinv_q (part_2p + part_2p+1) in that
-// fixed order, so the result does not depend on timing.
-#ifndef SB200_PROJ_SPLIT
-#define SB200_PROJ_SPLIT 1
-#endif
-constexpr int SPLIT = SB200_PROJ_SPLIT;
-
-__device__ __forceinline__ void pair_barrier(int pair) {
-  asm volatile("bar.sync %0, 64;" ::"r"(1 + pair) : "memory");
-}
-
+// one contiguous run; one warp per atom.  sap[fp] packs, for flat sphere
+// point fp, its pair index (bits 12..30) and its shared-memory grid index
+// (bits 0..11).  With `cached` (at most one atom per warp) each lane's uV and
+// phase come from its TMEM words at tkb + 12 k (chunk k of 32 sphere points)
+// instead of shared memory, which the gathers of both loops otherwise load
+// twice per term.
 template <int NW>
 __device__ __forceinline__ void project_contrib(const double2* __restrict__ buf, const double2* __restrict__ sph,
                                                 const double* __restrict__ suv, const int* __restrict__ sap,
-                                                double2* __restrict__ pc, double2 (*ppart)[4], int TP,
-                                                const OrbArgs& a, int warp, int lane) {
-  const int grp = warp / SPLIT, part = warp % SPLIT;
-  for (int atom = grp; atom < a.natom; atom += NW / SPLIT) {
-    const int start = __ldg(a.atom_start + atom), m = __ldg(a.mps + atom);
-    const int lma0 = __ldg(a.lma_start + atom), np = __ldg(a.nproj + atom);
-    if (np == 0) continue;  // no projectors: no pairs (the same for every warp of the group)
+                                                double2* __restrict__ pc, int TP, const int4* __restrict__ satm,
+                                                const double* __restrict__ srinv, const OrbArgs& a, int warp,
+                                                int lane, bool cached, uint32_t tkb) {
+  for (int atom = warp; atom < a.natom; atom += NW) {
+    const int4 at = satm[atom];
+    const int start = at.x, m = at.y, lma0 = at.z, np = at.w;
+    if (np == 0) continue;  // no projectors: no pairs
+    const int nk = (m + 31) >> 5;
     double2 pq[4];
 #pragma unroll
     for (int q = 0; q < 4; ++q) pq[q] = make_double2(0.0, 0.0);
-#pragma unroll 3
-    for (int j = lane + 32 * part; j < m; j += 32 * SPLIT) {
-      const int fp = start + j;
-      const double2 ev = cmul(sph[fp], buf[sap[fp] & 4095]);
+    if (cached) {
+      for (int k = 0; k < nk; ++k) {  // uniform over the warp (TMEM loads)
+        double u[4];
+        double2 e;
+        kb_load(tkb + 12 * k, u, e);
+        const int j = lane + 32 * k;
+        if (j < m) {
+          const double2 ev = cmul(e, buf[sap[start + j] & 4095]);
 #pragma unroll
-      for (int q = 0; q < 4; ++q)
-        if (q < np) {
-          const double u = suv[q * TP + fp];
-          pq[q] = make_double2(fma(u, ev.x, pq[q].x), fma(u, ev.y, pq[q].y));
+          for (int q = 0; q < 4; ++q) pq[q] = make_double2(fma(u[q], ev.x, pq[q].x), fma(u[q], ev.y, pq[q].y));
         }
-    }
+      }
+    } else {
+#pragma unroll 3
+      for (int j = lane; j < m; j += 32) {
+        const int fp = start + j;
+        const double2 ev = cmul(sph[fp], buf[sap[fp] & 4095]);
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-#pragma unroll
-      for (int off = 16; off > 0; off >>= 1) {
-        pq[q].x += __shfl_xor_sync(0xffffffffu, pq[q].x, off);
-        pq[q].y += __shfl_xor_sync(0xffffffffu, pq[q].y, off);
+        for (int q = 0; q < 4; ++q)
+          if (q < np) {
+            const double u = suv[q * TP + fp];
+            pq[q] = make_double2(fma(u, ev.x, pq[q].x), fma(u, ev.y, pq[q].y));
+          }
       }
     }
-    if (SPLIT == 2) {
-      if (lane == 0) {
-#pragma unroll
-        for (int q = 0; q < 4; ++q) ppart[warp][q] = pq[q];
-      }
-      pair_barrier(grp);
+    {  // sums over the warp, then every lane gets the four totals
+      double v[8];
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
-        const double2 p0 = ppart[2 * grp][q], p1 = ppart[2 * grp + 1][q];
-        pq[q] = make_double2(p0.x + p1.x, p0.y + p1.y);
+        v[2 * q] = pq[q].x;
+        v[2 * q + 1] = pq[q].y;
       }
-      pair_barrier(grp);  // both warps have read the partial sums before the next atom's
+      const double r = warp_reduce_scatter<8>(v, lane);
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+        pq[q] = make_double2(__shfl_sync(0xffffffffu, r, rs_lane<8>(2 * q)),
+                             __shfl_sync(0xffffffffu, r, rs_lane<8>(2 * q + 1)));
     }
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
-      const double r = q < np ? __ldg(a.rinv + lma0 + q) : 0.0;
+      const double r = q < np ? srinv[lma0 + q] : 0.0;
       pq[q] = make_double2(r * pq[q].x, r * pq[q].y);
     }
-#pragma unroll 3
-    for (int j = lane + 32 * part; j < m; j += 32 * SPLIT) {
-      const int fp = start + j;
-      double2 sp = make_double2(0.0, 0.0);
+    if (cached) {
+      for (int k = 0; k < nk; ++k) {
+        double u[4];
+        double2 e;
+        kb_load(tkb + 12 * k, u, e);
+        const int j = lane + 32 * k;
+        if (j < m) {
+          double2 sp = make_double2(0.0, 0.0);
 #pragma unroll
-      for (int q = 0; q < 4; ++q)
-        if (q < np) {
-          const double u = suv[q * TP + fp];
-          sp = make_double2(fma(u, pq[q].x, sp.x), fma(u, pq[q].y, sp.y));
+          for (int q = 0; q < 4; ++q) sp = make_double2(fma(u[q], pq[q].x, sp.x), fma(u[q], pq[q].y, sp.y));
+          pc[sap[start + j] >> 12] = cmul(make_double2(e.x, -e.y), sp);
         }
-      const double2 e = sph[fp];
-      pc[sap[fp] >> 12] = cmul(make_double2(e.x, -e.y), sp);
+      }
+    } else {
+#pragma unroll 3
+      for (int j = lane; j < m; j += 32) {
+        const int fp = start + j;
+        double2 sp = make_double2(0.0, 0.0);
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+          if (q < np) {
+            const double u = suv[q * TP + fp];
+            sp = make_double2(fma(u, pq[q].x, sp.x), fma(u, pq[q].y, sp.y));
+          }
+        const double2 e = sph[fp];
+        pc[sap[fp] >> 12] = cmul(make_double2(e.x, -e.y), sp);
+      }
     }
   }
 }
@@ -180,7 +250,7 @@ __global__ void __launch_bounds__(Blk<BZ>::BT, 1) k_step_blk(const double2* __re
                                                              StepZC zc, int nterm) {
   constexpr int NW = Blk<BZ>::NW, NS = Blk<BZ>::NS;
   constexpr uint32_t TW_ACC = Blk<BZ>::TW_ACC, TW_D = Blk<BZ>::TW_D, TW_PM = Blk<BZ>::TW_PM;
-  constexpr uint32_t TW_WARP = Blk<BZ>::TW_WARP;
+  constexpr uint32_t TW_WARP = Blk<BZ>::TW_WARP, TW_KB = Blk<BZ>::TW_KB;
   extern __shared__ __align__(16) double2 smem[];
   const int T = a.totpts;
   const bool kb = a.nlma > 0;
@@ -191,11 +261,13 @@ __global__ void __launch_bounds__(Blk<BZ>::BT, 1) k_step_blk(const double2* __re
   double* sr = suv + 4 * TP;                // [3][TP] coordinates of the sphere points
   double2* pc = (double2*)(sr + 3 * TP);    // [npair] KB contribution of each (point, atom) pair
   int* sap = (int*)(pc + bk.npair);         // [TP] pair index << 12 | shared-memory index of each sphere point
+  int4* satm = (int4*)(sap + TP);           // [natom] first flat point, sphere size, first ilma, projectors
+  double* srinv = (double*)(satm + (kb ? a.natom : 0));  // [nlma] rinv_uvu
   __shared__ uint32_t s_tmem;
   __shared__ double kn[12];
   __shared__ double red[OBS_NQ][NW];
   __shared__ double jws[NW][3];
-  __shared__ double2 ppart[SPLIT == 2 ? NW : 1][4];  // projection partial sums of each warp
+  __shared__ double nlred[OBS ? NW : 1][32];  // reduced nonlocal-current sums of each warp
   __shared__ __align__(8) uint64_t s_bar;             // completion of the table copies
 
   const int o = blockIdx.x, t = threadIdx.x, warp = t >> 5, lane = t & 31;
@@ -217,6 +289,12 @@ __global__ void __launch_bounds__(Blk<BZ>::BT, 1) k_step_blk(const double2* __re
     tma::bulk_load(suv, bk.uv4, b_uv, &s_bar);
     tma::bulk_load(sr, bk.r3, b_r, &s_bar);
     tma::bulk_load(sap, bk.sap, b_ap, &s_bar);
+  }
+
+  if (kb) {
+    for (int i = t; i < a.natom; i += Blk<BZ>::BT)
+      satm[i] = make_int4(__ldg(a.atom_start + i), __ldg(a.mps + i), __ldg(a.lma_start + i), __ldg(a.nproj + i));
+    for (int i = t; i < a.nlma; i += Blk<BZ>::BT) srinv[i] = __ldg(a.rinv + i);
   }
 
   // psi -> registers and the shared orbital buffer
@@ -276,8 +354,26 @@ __global__ void __launch_bounds__(Blk<BZ>::BT, 1) k_step_blk(const double2* __re
     __syncthreads();
   }
   if (ok) {
+  // KB cache: warp w < natom keeps its atom's uV and phases in TMEM for the step
+  const bool kbc = kb && bk.kbcache != 0;
+  const uint32_t tkb = tb + TW_KB;
+  if (kbc && warp < a.natom) {
+    const int4 at = satm[warp];
+    const int nk = (at.y + 31) >> 5;
+    for (int k = 0; k < nk; ++k) {
+      const int j = lane + 32 * k;
+      double u[4] = {0.0, 0.0, 0.0, 0.0};
+      double2 e = make_double2(0.0, 0.0);
+      if (j < at.y) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) u[q] = suv[q * TP + at.x + j];
+        e = sph[at.x + j];
+      }
+      kb_store(tkb + 12 * k, u, e);
+    }
+  }
   if (kb) {
-    project_contrib<NW>(buf, sph, suv, sap, pc, ppart, TP, a, warp, lane);
+    project_contrib<NW>(buf, sph, suv, sap, pc, TP, satm, srinv, a, warp, lane, kbc, tkb);
     __syncthreads();
   }
   const int hm2 = (bx - 2) & 7, hm1 = (bx - 1) & 7, hp1 = (bx + 1) & 7, hp2 = (bx + 2) & 7;
@@ -428,7 +524,7 @@ __global__ void __launch_bounds__(Blk<BZ>::BT, 1) k_step_blk(const double2* __re
     }
     __syncthreads();
     if (kb) {
-      project_contrib<NW>(buf, sph, suv, sap, pc, ppart, TP, a, warp, lane);
+      project_contrib<NW>(buf, sph, suv, sap, pc, TP, satm, srinv, a, warp, lane, kbc, tkb);
       __syncthreads();
     }
   }
@@ -493,65 +589,74 @@ __global__ void __launch_bounds__(Blk<BZ>::BT, 1) k_step_blk(const double2* __re
         }
       }
     }
+    {
+      static_assert(OBS_NQ <= 8, "local sums");
+      double v[8];
 #pragma unroll
-    for (int i = 0; i < OBS_NQ; ++i) {
-#pragma unroll
-      for (int off = 16; off > 0; off >>= 1) q[i] += __shfl_xor_sync(0xffffffffu, q[i], off);
+      for (int i = 0; i < 8; ++i) v[i] = i < OBS_NQ ? q[i] : 0.0;
+      const double r = warp_reduce_scatter<8>(v, lane);
+      const int k = lane >> 2;  // rs_lane<8>(k) = 4 k
+      if ((lane & 3) == 0 && k < OBS_NQ) red[k][warp] = r;
     }
-    if (lane == 0)
-      for (int i = 0; i < OBS_NQ; ++i) red[i][warp] = q[i];
     // nonlocal current: one warp per atom (density_matrix.f90:532-591)
     double jx = 0.0, jy = 0.0, jz = 0.0;
     if (kb) {
       for (int atom = warp; atom < a.natom; atom += NW) {
-        const int start = __ldg(a.atom_start + atom), m = __ldg(a.mps + atom);
-        const int lma0 = __ldg(a.lma_start + atom), np = __ldg(a.nproj + atom);
+        const int4 at = satm[atom];
+        const int start = at.x, m = at.y, lma0 = at.z, np = at.w;
         if (np == 0) continue;
-        double2 uq[4], ur[4][3];
+        // v[2c], v[2c + 1]: <beta_q|psi> (c = q < 4) and <r_d beta_q|psi> (c = 4 + 3 q + d)
+        double v[32];
 #pragma unroll
-        for (int qq = 0; qq < 4; ++qq) {
-          uq[qq] = make_double2(0.0, 0.0);
-          ur[qq][0] = ur[qq][1] = ur[qq][2] = uq[qq];
-        }
-        for (int j = lane; j < m; j += 32) {
+        for (int i = 0; i < 32; ++i) v[i] = 0.0;
+        const int nk = (m + 31) >> 5;
+        for (int k = 0; k < nk; ++k) {
+          const int j = lane + 32 * k;
+          double uc[4];
+          double2 e;
+          if (kbc) kb_load(tkb + 12 * k, uc, e);
+          if (j >= m) continue;
           const int fp = start + j;
-          const double2 ev = cmul(sph[fp], buf[sap[fp] & 4095]);
+          if (!kbc) {
+#pragma unroll
+            for (int qq = 0; qq < 4; ++qq) uc[qq] = suv[qq * TP + fp];
+            e = sph[fp];
+          }
+          const double2 ev = cmul(e, buf[sap[fp] & 4095]);
           const double r0 = sr[fp], r1 = sr[TP + fp], r2 = sr[2 * TP + fp];
 #pragma unroll
           for (int qq = 0; qq < 4; ++qq) {
             if (qq < np) {
-              const double u = suv[qq * T + fp];
-              const double2 tq = make_double2(u * ev.x, u * ev.y);
-              uq[qq] = make_double2(uq[qq].x + tq.x, uq[qq].y + tq.y);
-              ur[qq][0] = make_double2(fma(r0, tq.x, ur[qq][0].x), fma(r0, tq.y, ur[qq][0].y));
-              ur[qq][1] = make_double2(fma(r1, tq.x, ur[qq][1].x), fma(r1, tq.y, ur[qq][1].y));
-              ur[qq][2] = make_double2(fma(r2, tq.x, ur[qq][2].x), fma(r2, tq.y, ur[qq][2].y));
+              const double u = uc[qq];
+              const double tx = u * ev.x, ty = u * ev.y;
+              v[2 * qq] += tx;
+              v[2 * qq + 1] += ty;
+              v[8 + 6 * qq] = fma(r0, tx, v[8 + 6 * qq]);
+              v[9 + 6 * qq] = fma(r0, ty, v[9 + 6 * qq]);
+              v[10 + 6 * qq] = fma(r1, tx, v[10 + 6 * qq]);
+              v[11 + 6 * qq] = fma(r1, ty, v[11 + 6 * qq]);
+              v[12 + 6 * qq] = fma(r2, tx, v[12 + 6 * qq]);
+              v[13 + 6 * qq] = fma(r2, ty, v[13 + 6 * qq]);
             }
           }
         }
+        const double r = warp_reduce_scatter<32>(v, lane);  // lane L holds value L
+        nlred[warp][lane] = r;
+        __syncwarp();
+        if (lane == 0) {
 #pragma unroll
-        for (int qq = 0; qq < 4; ++qq) {
-#pragma unroll
-          for (int off = 16; off > 0; off >>= 1) {
-            uq[qq].x += __shfl_xor_sync(0xffffffffu, uq[qq].x, off);
-            uq[qq].y += __shfl_xor_sync(0xffffffffu, uq[qq].y, off);
-#pragma unroll
-            for (int d = 0; d < 3; ++d) {
-              ur[qq][d].x += __shfl_xor_sync(0xffffffffu, ur[qq][d].x, off);
-              ur[qq][d].y += __shfl_xor_sync(0xffffffffu, ur[qq][d].y, off);
+          for (int qq = 0; qq < 4; ++qq) {
+            if (qq < np) {
+              const double rv = srinv[lma0 + qq];
+              const double usx = rv * nlred[warp][2 * qq], usy = rv * nlred[warp][2 * qq + 1];
+              const double* ur = &nlred[warp][8 + 6 * qq];
+              jx += ur[0] * usy - ur[1] * usx;
+              jy += ur[2] * usy - ur[3] * usx;
+              jz += ur[4] * usy - ur[5] * usx;
             }
           }
         }
-#pragma unroll
-        for (int qq = 0; qq < 4; ++qq) {
-          if (qq < np) {
-            const double rv = __ldg(a.rinv + lma0 + qq);
-            const double2 us = make_double2(rv * uq[qq].x, rv * uq[qq].y);
-            jx += ur[qq][0].x * us.y - ur[qq][0].y * us.x;
-            jy += ur[qq][1].x * us.y - ur[qq][1].y * us.x;
-            jz += ur[qq][2].x * us.y - ur[qq][2].y * us.x;
-          }
-        }
+        __syncwarp();
       }
     }
     if (lane == 0) {
@@ -626,8 +731,9 @@ size_t step_blk_smem(const sb200_ctx* c) {
     return 0;  // no (point, atom) pair form, or no staged tables (blk_build_tables)
   const size_t TP = pp.nlma > 0 ? (size_t)pp.blk_tpad : 0;
   (void)T;
+  const size_t natom = pp.nlma > 0 ? (size_t)pp.natom : 0, nlma = pp.nlma > 0 ? (size_t)pp.nlma : 0;
   return (size_t)NPTS * sizeof(double2) + TP * (sizeof(double2) + 7 * sizeof(double) + sizeof(int)) +
-         npair * sizeof(double2);
+         npair * sizeof(double2) + natom * sizeof(int4) + nlma * sizeof(double);
 }
 
 int launch_step_blk(sb200_ctx* c, const double2* in, double2* out, const OrbArgs& a, const StepZC& z, int n_hamil,
@@ -660,6 +766,11 @@ int launch_step_blk(sb200_ctx* c, const double2* in, double2* out, const OrbArgs
   bk.r3 = c->pp.d_blk_r;
   bk.sap = c->pp.d_blk_sap;
   bk.err = c->d_err;
+  {  // TMEM KB cache: at most one atom per warp and every sphere within the warp's TMEM words
+    const int nw = c->blk_depth == 4 ? Blk<4>::NW : Blk<2>::NW;
+    const int chunks = c->blk_depth == 4 ? Blk<4>::KB_CHUNKS : Blk<2>::KB_CHUNKS;
+    bk.kbcache = (c->pp.nlma > 0 && c->pp.natom <= nw && c->pp.nps <= 32 * chunks) ? 1 : 0;
+  }
   dim3 grid(c->orb.norb);
   if (c->blk_depth == 4) {
     if (with_obs) k_step_blk<4, true><<<grid, Blk<4>::BT, smem, c->stream>>>(in, out, a, bk, z, n_hamil);

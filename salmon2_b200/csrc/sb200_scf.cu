@@ -596,6 +596,20 @@ int scf_density_allreduce(sb200_ctx* c, double* d_rho) {
   return SB200_OK;
 }
 
+bool shard_comm_set(const sb200_ctx* c) {
+  const ScfState* s = c->scf ? static_cast<const ScfState*>(c->scf) : nullptr;
+  return s != nullptr && s->comm != nullptr;
+}
+
+int shard_sum(sb200_ctx* c, double* d, size_t n) {
+  ScfState* s = scf_of(c);
+  if (!s || !s->comm) return SB200_OK;
+  const NcclApi* api = nccl_api();
+  const ncclResult_t r = api->all_reduce(d, d, n, ncclFloat64, ncclSum, s->comm, c->stream);
+  if (r != ncclSuccess) return set_error(SB200_ERR_CUDA, std::string("ncclAllReduce: ") + api->error_string(r));
+  return SB200_OK;
+}
+
 int scf_rt_issue(sb200_ctx* c, const double2* psi) {
   ScfState* s = scf_of(c);
   if (!s || !s->rt_on) return SB200_OK;

@@ -44,6 +44,23 @@ __device__ __forceinline__ uint32_t warp_addr(uint32_t base, int warp, uint32_t 
   return base + ((uint32_t)(32 * (warp & 3)) << 16) + col;
 }
 
+__device__ __forceinline__ void ld4(uint32_t taddr, uint32_t (&r)[4]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0, %1, %2, %3}, [%4];\n\t"
+      "tcgen05.wait::ld.sync.aligned;"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+      : "r"(taddr)
+      : "memory");
+}
+
+__device__ __forceinline__ void st4(uint32_t taddr, const uint32_t (&r)[4]) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x4.b32 [%0], {%1, %2, %3, %4};\n\t"
+      "tcgen05.wait::st.sync.aligned;" ::"r"(taddr),
+      "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3])
+      : "memory");
+}
+
 __device__ __forceinline__ void ld8(uint32_t taddr, uint32_t (&r)[8]) {
   asm volatile(
       "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];\n\t"

@@ -279,6 +279,35 @@ def test_density_comm_single_rank():
         assert np.array_equal(x, y)
 
 
+@pytest.mark.parametrize("num", [12, 16], ids=["tiled", "fused16"])
+def test_shard_current_sum_single_rank_lo(num):
+    """With a shard communicator the loop's finalize runs in two stages around
+    an NCCL all-reduce of J(t) and the dipole sums (inside the CUDA graph);
+    with one rank that all-reduce is the identity, so J(t), A_tot, the dipole
+    and the orbitals of the induced-field ('lo') loop equal those without a
+    communicator bit for bit."""
+    from salmon2_b200 import synth
+    from salmon2_b200.rt import Context, nccl_unique_id
+
+    s = synth.periodic_system(a=10.26, num=num, nkgrid=1, no=3, seed=44, name=f"lo{num}")
+    nt, dt = 6, 0.08
+    Ac = synth.asin2cos(nt, dt, omega=0.05696, f0=0.05696 * 2e-2, tw=nt * dt)
+    zc = synth.taylor_zc(dt)
+    got = {}
+    for comm in (False, True):
+        ctx = Context(s)
+        if comm:
+            ctx.set_density_comm(1, 0, nccl_unique_id())
+        a, b, w = ctx.upload(s.psi), ctx.zeros(), ctx.zeros()
+        r = ctx.rt_propagate(a, b, w, nt, dt, zc, Ac_ext=Ac, trans_longi="lo")
+        got[comm] = (r["curr"], r["Ac_tot"], r["rbox"], ctx.download(r["psi"]))
+        ctx.set_density_comm(0, 0, None)
+        ctx.close()
+    for x, y in zip(got[False], got[True]):
+        assert np.array_equal(x, y)
+    assert np.max(np.abs(got[True][0])) > 0
+
+
 @pytest.mark.parametrize("make", [S.isolated_small, S.isolated_odd], ids=["iso24", "iso_odd"])
 def test_hartree_isolated_ft_against_oracle(make):
     import torch

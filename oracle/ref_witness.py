@@ -105,3 +105,70 @@ def stencil_current(system, psi_ref, vec_Ac, ispin=1):
     torch.cuda.synchronize()
     j[:] = (jx.value, jy.value, jz.value)
     return j
+
+
+def time_zpseudo(system, tpsi_ref, zekr, reps=5):
+    """Milliseconds per call of the reference's zpseudo_cuda on device-resident
+    inputs (median of `reps` calls after one warm-up; each call ends with the
+    reference's own cudaDeviceSynchronize)."""
+    import torch
+    g, pp = system.grid, system.pp
+    t = _dev(torch, tpsi_ref, torch.complex128)
+    h = torch.zeros_like(t)
+    ia = _dev(torch, pp.ia_tbl.astype(np.int32), torch.int32)
+    mps = _dev(torch, pp.mps.astype(np.int32), torch.int32)
+    jxyz = _dev(torch, pp.jxyz.astype(np.int32), torch.int32)
+    zk = _dev(torch, zekr, torch.complex128)
+    rinv = _dev(torch, pp.rinv_uvu, torch.float64)
+    n = pp.nlma // pp.natom
+    args = (h.data_ptr(), n, 1, 1, 1, system.nk, 1, system.no, system.nspin, pp.nlma, pp.nps, pp.natom,
+            int(g.is_array[0]), int(g.ie_array[0]), int(g.is_array[1]), int(g.ie_array[1]),
+            int(g.is_array[2]), int(g.ie_array[2]), ia.data_ptr(), mps.data_ptr(), jxyz.data_ptr(),
+            zk.data_ptr(), rinv.data_ptr(), t.data_ptr())
+    lib().zpseudo_cuda(*args)
+    times = []
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        lib().zpseudo_cuda(*args)
+        e1.record()
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    return float(np.median(times))
+
+
+def time_stencil_current(system, psi_ref, vec_Ac, reps=2):
+    """Milliseconds per call of the reference's stencil_current_core_gpu over
+    every orbital of spin 1 (one launch and one device-to-host copy per (k,
+    orbital), as the reference issues it)."""
+    import time
+    import torch
+    g = system.grid
+    assert g.periodic and int(np.prod(g.shape)) % 128 == 0
+    psi = _dev(torch, psi_ref, torch.complex128)
+    vec_k = np.asfortranarray(system.vec_k, dtype=np.float64)
+    vac = np.ascontiguousarray(vec_Ac, dtype=np.float64)
+    i3 = lambda v: np.ascontiguousarray(np.asarray(v, dtype=np.int32))
+    isa, iea, is_, ie = i3(g.is_array), i3(g.ie_array), i3(g.is_), i3(g.ie)
+    idx = [np.ascontiguousarray(m[4:], dtype=np.int32) for m in (g.idx, g.idy, g.idz)]
+    nab = np.ascontiguousarray(np.asarray(g.coef_nab).ravel(order="F"))
+    BT = np.ascontiguousarray(np.eye(3).ravel(order="F"))
+    rocc = np.asfortranarray(system.rocc[:, :, 0], dtype=np.float64)
+    wtk = np.ascontiguousarray(system.wtk, dtype=np.float64)
+    P = lambda a: a.ctypes.data_as(C.c_void_p)
+
+    def call():
+        jx, jy, jz = C.c_double(0.0), C.c_double(0.0), C.c_double(0.0)
+        lib().stencil_current_core_gpu(1, system.nk, 1, system.no, P(vec_k), P(vac), P(isa), P(iea), P(is_), P(ie),
+                                       P(idx[0]), P(idx[1]), P(idx[2]), P(nab), 1, 1, system.nspin,
+                                       psi.data_ptr(), P(BT), P(rocc), P(wtk), C.addressof(jx), C.addressof(jy),
+                                       C.addressof(jz))
+        torch.cuda.synchronize()
+
+    call()
+    times = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        call()
+        times.append((time.perf_counter() - t0) * 1e3)
+    return float(np.median(times))

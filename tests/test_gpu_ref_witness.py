@@ -56,3 +56,58 @@ def test_stencil_current_reference_vs_oracle():
             io = (o // per.nspin) % per.no
             local += ((per.vec_k[:, ik] + np.asarray(ac)) * parts[0, o] + parts[1:4, o]) * per.rocc[io, ik, 0] * per.wtk[ik]
         assert np.max(np.abs(local - ref)) <= 1e-12 * max(np.max(np.abs(ref)), 1e-300)
+
+
+def _timed(ctx, fn, reps=5):
+    """Milliseconds per call of fn on the context's stream (median)."""
+    import torch
+    st = torch.cuda.Stream()
+    ctx.set_stream(st)
+    fn()
+    times = []
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        fn()
+        e1.record(st)
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    ctx.set_stream(None)
+    return float(np.median(times))
+
+
+@pytest.mark.parametrize("which", ["bulk", "supercell"])
+def test_reference_gpu_kernels_timed_beside_library(which):
+    """The reference's own GPU kernels for the two sub-steps it ships in CUDA,
+    timed on the B200 beside this library on the same inputs (one line per
+    workload starting with REFTIME): zpseudo_cuda (the KB nonlocal term alone;
+    one thread per (orbital, projector), atomics) against sb200_hpsi (the
+    whole H psi: stencil, k+A gradient, V_local and KB), and
+    stencil_current_core_gpu (the local current; one launch and one copy back
+    per (k, orbital)) against sb200_calc_current (local and nonlocal current).
+    Their results are compared with the oracle by the tests above."""
+    import json
+    from salmon2_b200 import synth
+    from salmon2_b200.rt import Context
+    if which == "bulk":
+        s = synth.periodic_system(a=10.26, num=16, nkgrid=4, no=32, seed=2, name="periodic_bulk")
+    else:
+        s = synth.periodic_system(a=10.26, num=16, nkgrid=2, no=256, supercell=2, seed=3, ecut=2.0,
+                                  name="periodic_supercell")
+    ac = (0.0, 0.0, 1e-3)
+    O = Oracle(s)
+    O.set_vec_Ac(ac)
+    ref_ms = ref_witness.time_zpseudo(s, s.psi, O.zekr)
+    ctx = Context(s)
+    ctx.set_vec_Ac(ac)
+    t = ctx.upload(s.psi)
+    h = ctx.zeros()
+    lib_ms = _timed(ctx, lambda: ctx.hpsi(t, h))
+    out = dict(workload=which, orbitals=s.norb, grid=list(s.grid.shape), projectors=s.pp.nlma,
+               ref_zpseudo_cuda_ms=ref_ms, lib_hpsi_ms=lib_ms)
+    if which == "bulk":
+        out["ref_stencil_current_core_gpu_ms"] = ref_witness.time_stencil_current(s, s.psi, ac)
+        out["lib_calc_current_ms"] = _timed(ctx, lambda: ctx.calc_current(t, ac), reps=3)
+    print("REFTIME " + json.dumps(out))
+    ctx.close()
+    assert ref_ms > 0 and lib_ms > 0

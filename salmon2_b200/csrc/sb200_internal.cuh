@@ -154,6 +154,8 @@ struct sb200_ctx {
   int orbital_variant = 4;     // 16^3 periodic grids: 4 fused Taylor step with register blocking (when its
                                // tables fit, else form 2), 2 fused step with the KB tables staged in shared memory
                                // (when they fit), 3 fused without staging, 0 one launch per term, 1 persistent per term
+  int project_variant = 1;     // KB projections: 1 tensor cores where a k-point fills a 16-orbital tile,
+                               // 2 tensor cores always, 0 one warp per (orbital, atom)
   int blk_depth = 2;           // z depth of the register block of the blocked fused step (2: 512 threads, 4: 256)
   int tma_variant = 1;         // tiled hpsi fed by tensor copies where it applies (0: register-prefetch sweep)
   // optional per-kernel-class device timing (sb200_set_timing)
@@ -217,6 +219,9 @@ struct HpsiLaunch {
 int launch_prep_k(sb200_ctx* c, const double* d_A, int a_mode, int itt_from_device,
                   double* d_kcoef, bool phases);
 int launch_project(sb200_ctx* c, const void* in, double2* proj, bool in32 = false);
+// KB projections on the FP64 tensor cores; SB200_ERR_UNSUPPORTED (no error
+// recorded) when the form does not apply (sb200_project_mma.cu)
+int launch_project_dmma(sb200_ctx* c, const void* in, double2* proj, bool in32);
 int launch_hpsi(sb200_ctx* c, const HpsiLaunch& L);
 int launch_hpsi_tiled(sb200_ctx* c, const HpsiLaunch& L);  // sb200_stencil.cu
 // tensor-copy-fed tiled kernel; SB200_ERR_UNSUPPORTED when it does not apply (sb200_tma_stencil.cu)

@@ -549,6 +549,13 @@ ProjArgs make_proj_args(const sb200_ctx* c) {
 
 int launch_project(sb200_ctx* c, const void* in, double2* proj, bool in32) {
   if (c->pp.nlma == 0) return SB200_OK;
+  // the tensor-core form (sb200_project_mma.cu) when a k-point has at least
+  // one full 16-orbital tile, else one warp per (orbital, atom)
+  const int nspin_no = c->orb.nspin * c->orb.no;
+  if (c->project_variant == 2 || (c->project_variant == 1 && nspin_no >= 16)) {
+    const int r = launch_project_dmma(c, in, proj, in32);
+    if (r != SB200_ERR_UNSUPPORTED) return r;
+  }
   ProjArgs a = make_proj_args(c);
   dim3 grid((a.natom + 3) / 4, c->orb.norb);
   if (in32) k_project<4, float2><<<grid, 128, 0, c->stream>>>((const float2*)in, proj, a);

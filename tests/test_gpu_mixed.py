@@ -53,3 +53,23 @@ def test_mixed_current_over_time_loop():
     norm_mix = res["rbox"][3]
     assert err_j <= TOL_J_MIXED, err_j
     assert np.max(np.abs(norm_mix - norm_ref)) / norm_ref[0] < 1e-6
+
+
+def test_mixed_taylor_step_with_tensor_core_projections(monkeypatch):
+    """The mixed form's FP32 Taylor terms feed the tensor-core projections
+    through their FP32-input path (SB200_PROJECT=dmma): a Taylor step stays
+    within the mixed form's error of the FP64 oracle."""
+    from salmon2_b200 import synth
+    monkeypatch.setenv("SB200_PROJECT", "dmma")
+    s = synth.periodic_system(a=10.26, num=12, nkgrid=1, no=20, seed=45, name="p12n20")
+    O = Oracle(s)
+    ac = (0.0, 0.0, 0.02)
+    O.set_vec_Ac(ac)
+    zc = synth.taylor_zc(0.05)
+    ref = O.taylor(s.psi, zc)
+    ctx = _ctx(s, "mixed")
+    ctx.set_vec_Ac(ac)
+    out, work = ctx.zeros(), ctx.zeros()
+    ctx.taylor(ctx.upload(s.psi), out, work, zc)
+    err = S.rel_err(ctx.download(out), ref)
+    assert 1e-14 < err < 1e-6, err

@@ -422,3 +422,46 @@ def test_current_periodic32():
     ref = O.current(sysm.psi)
     got = ctx.calc_current(ctx.upload(sysm.psi), a_cur)
     assert np.max(np.abs(got - ref)) <= TOL_OBS * max(np.max(np.abs(ref)), 1e-30)
+
+
+def _p12_twenty_orbitals():
+    # 20 orbitals per k-point: one full 16-orbital tile of the tensor-core
+    # projection and a partial one
+    from salmon2_b200 import synth
+    return synth.periodic_system(a=10.26, num=12, nkgrid=1, no=20, seed=45, name="p12n20")
+
+
+def _p12_two_spins_ten():
+    from salmon2_b200 import synth
+    return synth.periodic_system(a=10.26, num=12, nkgrid=2, no=10, seed=46, nspin=2, name="p12s2n10")
+
+
+def _iso_eighteen():
+    from salmon2_b200 import synth
+    return synth.isolated_system(num=(20, 24, 22), no=18, natom=3, seed=47, name="iso18")
+
+
+@pytest.mark.parametrize("variant", ["dmma", "warp"])
+@pytest.mark.parametrize("make", [_p12_twenty_orbitals, _p12_two_spins_ten, _iso_eighteen, S.periodic_small],
+                         ids=lambda f: f.__name__)
+def test_projection_forms_against_oracle(make, variant, monkeypatch):
+    """The KB projections on the FP64 tensor cores (mma.sync m8n8k4 over
+    16-orbital tiles, SB200_PROJECT=dmma) and in the warp-per-(orbital, atom)
+    form, under H psi and a Taylor step, against the oracle: full and partial
+    tiles, two spins, isolated grids, fewer orbitals than a tile."""
+    from salmon2_b200 import synth
+    monkeypatch.setenv("SB200_PROJECT", variant)
+    sysm = make()
+    O = Oracle(sysm)
+    ctx = _ctx(sysm)
+    ac = (0.02, -0.01, 0.015) if sysm.grid.periodic else (0.0, 0.0, 0.0)
+    O.set_vec_Ac(ac)
+    ctx.set_vec_Ac(ac)
+    t = ctx.upload(sysm.psi)
+    h = ctx.zeros()
+    ctx.hpsi(t, h)
+    assert S.rel_err(ctx.download(h), O.hpsi(sysm.psi)) < TOL_H
+    zc = synth.taylor_zc(0.05)
+    out, work = ctx.zeros(), ctx.zeros()
+    ctx.taylor(ctx.upload(sysm.psi), out, work, zc)
+    assert S.rel_err(ctx.download(out), O.taylor(sysm.psi, zc)) < TOL_H

@@ -639,62 +639,6 @@ int gs_gram(sb200_ctx* c, const double* A, int m, const double* B, int n, double
   return SB200_OK;
 }
 
-// symmetric eigen-decomposition on the host (cyclic Jacobi), eigenvalues
-// ascending with column eigenvectors, largest-magnitude component positive
-void host_eigh(int n, std::vector<double>& A, std::vector<double>& w, std::vector<double>& V) {
-  V.assign((size_t)n * n, 0.0);
-  for (int i = 0; i < n; ++i) V[(size_t)i * n + i] = 1.0;
-  auto at = [&](int i, int j) -> double& { return A[(size_t)j * n + i]; };
-  for (int sweep = 0; sweep < 60; ++sweep) {
-    double off = 0.0, tot = 0.0;
-    for (int j = 0; j < n; ++j)
-      for (int i = 0; i < n; ++i) {
-        tot += at(i, j) * at(i, j);
-        if (i != j) off += at(i, j) * at(i, j);
-      }
-    if (off <= 1e-30 * (tot > 0 ? tot : 1.0)) break;
-    for (int p = 0; p < n - 1; ++p)
-      for (int q = p + 1; q < n; ++q) {
-        const double apq = at(p, q);
-        if (apq == 0.0) continue;
-        const double theta = (at(q, q) - at(p, p)) / (2.0 * apq);
-        const double t = (theta >= 0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
-        const double cs = 1.0 / std::sqrt(t * t + 1.0), sn = t * cs;
-        for (int k = 0; k < n; ++k) {
-          const double akp = at(k, p), akq = at(k, q);
-          at(k, p) = cs * akp - sn * akq;
-          at(k, q) = sn * akp + cs * akq;
-        }
-        for (int k = 0; k < n; ++k) {
-          const double apk = at(p, k), aqk = at(q, k);
-          at(p, k) = cs * apk - sn * aqk;
-          at(q, k) = sn * apk + cs * aqk;
-        }
-        for (int k = 0; k < n; ++k) {
-          const double vkp = V[(size_t)p * n + k], vkq = V[(size_t)q * n + k];
-          V[(size_t)p * n + k] = cs * vkp - sn * vkq;
-          V[(size_t)q * n + k] = sn * vkp + cs * vkq;
-        }
-      }
-  }
-  std::vector<int> ord(n);
-  for (int i = 0; i < n; ++i) ord[i] = i;
-  for (int i = 0; i < n; ++i)
-    for (int j = i + 1; j < n; ++j)
-      if (at(ord[j], ord[j]) < at(ord[i], ord[i])) std::swap(ord[i], ord[j]);
-  w.resize(n);
-  std::vector<double> Vs((size_t)n * n);
-  for (int i = 0; i < n; ++i) {
-    w[i] = at(ord[i], ord[i]);
-    int im = 0;
-    for (int k = 1; k < n; ++k)
-      if (std::fabs(V[(size_t)ord[i] * n + k]) > std::fabs(V[(size_t)ord[i] * n + im])) im = k;
-    const double sg = V[(size_t)ord[i] * n + im] < 0 ? -1.0 : 1.0;
-    for (int k = 0; k < n; ++k) Vs[(size_t)i * n + k] = sg * V[(size_t)ord[i] * n + k];
-  }
-  V.swap(Vs);
-}
-
 int gs_relayout(sb200_ctx* c, const double* src, double* dst, int norb, bool to_ref) {
   const GridInfo& g = c->g;
   const int nxa = g.ie_array[0] - g.is_array[0] + 1;
@@ -990,7 +934,8 @@ int sb200_gram_schmidt_complex(sb200_ctx* c, double* psi) {
 }
 
 // ssdg_rwf (subspace_diagonalization.f90:62-238): H_sub = <psi_i|H|psi_j>,
-// eigenvectors on the host, psi <- psi V, normalised.  evals(no*nspin) host.
+// its eigenvectors on the GPU (sb200_eigh.cu), psi <- psi V, normalised.
+// evals(no*nspin) host.
 int sb200_subspace_diag_real(sb200_ctx* c, double* psi, double* evals) {
   TRY_GS(gs_ready(c));
   if (!psi) return set_error(SB200_ERR_INVALID_ARG, "null psi");
@@ -1002,23 +947,29 @@ int sb200_subspace_diag_real(sb200_ctx* c, double* psi, double* evals) {
   double* hpsi = c->gs.d_work;
   double* rot = c->gs.d_work + c->gs.n;
   TRY_GS(gs_hpsi(c, psi, hpsi));
-  TRY_GS(gs_mat(c, (size_t)no * no + 8));
-  TRY_GS(gs_gram(c, psi, no, hpsi, no, c->g.hvol, c->gs.d_mat));
-  std::vector<double> M((size_t)no * no), w, V;
-  SB_CUDA(cudaMemcpyAsync(M.data(), c->gs.d_mat, M.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-  SB_CUDA(cudaStreamSynchronize(c->stream));
-  // M[i][j] row-major = <psi_i|H psi_j>; dsyev reads the upper triangle
-  std::vector<double> A((size_t)no * no);
-  for (int j = 0; j < no; ++j)
-    for (int i = 0; i < no; ++i) A[(size_t)j * no + i] = (i <= j) ? M[(size_t)i * no + j] : M[(size_t)j * no + i];
-  host_eigh(no, A, w, V);
-  SB_CUDA(cudaMemcpyAsync(c->gs.d_mat, V.data(), V.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-  TRY_GS(gs_rotate(c, psi, no, c->gs.d_mat, no, 0.0, rot));
+  // work: M (no^2), V (no^2), eigensolver scratch (2 no^2), w (no), info
+  const size_t nn = (size_t)no * no;
+  TRY_GS(gs_mat(c, 4 * nn + no + 8));
+  double* M = c->gs.d_mat;
+  double* V = M + nn;
+  double* ework = M + 2 * nn;
+  double* w = M + 4 * nn;
+  int* info = (int*)(w + no);
+  TRY_GS(gs_gram(c, psi, no, hpsi, no, c->g.hvol, M));
+  // M[i][j] row-major = <psi_i|H psi_j>; the eigensolver reads its upper
+  // triangle (dsyev with uplo = 'U'), on the GPU
+  TRY_GS(launch_eigh(c, M, no, ework, V, w, info));
+  TRY_GS(gs_rotate(c, psi, no, V, no, 0.0, rot));
   for (int io = 0; io < no; ++io) TRY_GS(gs_norm_scale(c, rot + npts * io));
   SB_CUDA(cudaMemcpyAsync(psi, rot, sizeof(double) * npts * no, cudaMemcpyDeviceToDevice, c->stream));
+  std::vector<double> hw(no + 1);
+  SB_CUDA(cudaMemcpyAsync(hw.data(), w, sizeof(double) * (no + 1), cudaMemcpyDeviceToHost, c->stream));
   SB_CUDA(cudaStreamSynchronize(c->stream));
+  int hinfo = 0;
+  std::memcpy(&hinfo, &hw[no], sizeof(int));
+  if (hinfo != 0) return set_error(SB200_ERR_UNSUPPORTED, "subspace eigensolver: QL iterations did not converge");
   if (evals)
-    for (int i = 0; i < no; ++i) evals[i] = w[i];
+    for (int i = 0; i < no; ++i) evals[i] = hw[i];
   return SB200_OK;
 }
 

@@ -222,6 +222,10 @@ int launch_project(sb200_ctx* c, const void* in, double2* proj, bool in32 = fals
 // KB projections on the FP64 tensor cores; SB200_ERR_UNSUPPORTED (no error
 // recorded) when the form does not apply (sb200_project_mma.cu)
 int launch_project_dmma(sb200_ctx* c, const void* in, double2* proj, bool in32);
+// symmetric eigen-decomposition of the upper triangle of row-major M (n x n)
+// on the GPU: w ascending, V[i n + k] = component k of eigenvector i; work
+// 2 n^2 doubles; *info = 1 when the QL iterations did not converge (sb200_eigh.cu)
+int launch_eigh(sb200_ctx* c, const double* M, int n, double* work, double* V, double* w, int* info);
 int launch_hpsi(sb200_ctx* c, const HpsiLaunch& L);
 int launch_hpsi_tiled(sb200_ctx* c, const HpsiLaunch& L);  // sb200_stencil.cu
 // tensor-copy-fed tiled kernel; SB200_ERR_UNSUPPORTED when it does not apply (sb200_tma_stencil.cu)

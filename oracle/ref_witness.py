@@ -23,6 +23,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_LIB = os.path.join(HERE, "_ref", "libsalmon_ref_cuda.so")
+REF_AVX512_LIB = os.path.join(HERE, "_ref", "libsalmon_ref_avx512.so")
 
 _lib = None
 
@@ -172,3 +173,75 @@ def time_stencil_current(system, psi_ref, vec_Ac, reps=2):
         call()
         times.append((time.perf_counter() - t0) * 1e3)
     return float(np.median(times))
+
+
+# ---- the reference's hand-vectorised AVX-512 stencil (CPU) -------------------
+
+_avx = None
+
+
+def cpu_has_avx512() -> bool:
+    try:
+        return any(" avx512f" in line for line in open("/proc/cpuinfo") if line.startswith("flags"))
+    except OSError:
+        return False
+
+
+def avx512_available() -> bool:
+    return os.path.exists(REF_AVX512_LIB) and cpu_has_avx512()
+
+
+def _avx_lib():
+    global _avx
+    if _avx is None:
+        L = C.CDLL(REF_AVX512_LIB)
+        L.zstencil_tuned_seq_.restype = None
+        L.zstencil_tuned_seq_.argtypes = [C.c_void_p] * 15
+        _avx = L
+    return _avx
+
+
+def _aligned(shape, dtype, order="C"):
+    """Zeroed array whose data starts on a 64-byte boundary (the reference
+    kernel uses aligned vector loads and streaming stores)."""
+    n = int(np.prod(shape)) * np.dtype(dtype).itemsize
+    raw = np.zeros(n + 64, dtype=np.uint8)
+    off = (-raw.ctypes.data) % 64
+    return raw[off:off + n].view(dtype).reshape(shape, order=order)
+
+
+def zstencil_avx512(system, psi_ref, vec_Ac):
+    """Local H psi (25-point stencil, k+A gradient, V_local) of every orbital
+    from the reference's zstencil_tuned_seq_ (zstencil_core/avx512/seq.c),
+    called as stencil.f90:101 calls it: modulo tables of
+    code_optimization.f90:88-104, k_lap0 / k_nabt of hamiltonian.f90:146-155.
+    Periodic grids whose x extent is a multiple of 4.  Returns the reference
+    array layout (interior points; padding rows zero)."""
+    g = system.grid
+    assert g.periodic
+    nl = [int(v) for v in g.shape]
+    assert nl[0] % 4 == 0
+    i3 = lambda v: np.ascontiguousarray(np.asarray(v, dtype=np.int32))
+    isa, iea, is_, ie = i3(g.is_array), i3(g.ie_array), i3(g.is_), i3(g.ie)
+    mods = [np.ascontiguousarray(np.arange(3 * n, dtype=np.int32) % n) for n in nl]
+    lapt = np.ascontiguousarray(np.asarray(g.coef_lap, dtype=np.float64).ravel(order="F"))
+    nab = np.asarray(g.coef_nab, dtype=np.float64).reshape((4, 3), order="F")
+    out = np.zeros_like(psi_ref, order="F")
+    P = lambda a: C.c_void_p(a.ctypes.data)
+    shp = tuple(psi_ref.shape[:3])
+    E = _aligned(shp[::-1], np.complex128)
+    F = _aligned(shp[::-1], np.complex128)
+    V = _aligned(tuple(nl[::-1]), np.float64)
+    for ik in range(system.nk):
+        kac = system.vec_k[:, ik] + np.asarray(vec_Ac, dtype=np.float64)
+        lap0 = np.array([g.coef_lap0 + 0.5 * float(np.dot(kac, kac))])
+        knab = np.ascontiguousarray((nab * kac[None, :]).ravel(order="F"))
+        for isp in range(system.nspin):
+            V[...] = np.asarray(system.V_local[..., isp]).transpose(2, 1, 0)
+            for io in range(system.no):
+                E[...] = psi_ref[:, :, :, isp, io, ik].transpose(2, 1, 0)
+                F[...] = 0.0
+                _avx_lib().zstencil_tuned_seq_(P(isa), P(iea), P(is_), P(ie), P(mods[0]), P(mods[1]), P(mods[2]),
+                                               P(is_), P(ie), P(E), P(F), P(V), P(lap0), P(lapt), P(knab))
+                out[:, :, :, isp, io, ik] = F.transpose(2, 1, 0)
+    return out

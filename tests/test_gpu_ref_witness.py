@@ -111,3 +111,26 @@ def test_reference_gpu_kernels_timed_beside_library(which):
     print("REFTIME " + json.dumps(out))
     ctx.close()
     assert ref_ms > 0 and lib_ms > 0
+
+
+@pytest.mark.skipif(not ref_witness.avx512_available(), reason="reference AVX-512 stencil not built or no AVX-512 CPU")
+@pytest.mark.parametrize("num,nkgrid,nspin", [(12, 2, 1), (16, 1, 2)])
+def test_stencil_reference_avx512_vs_library(num, nkgrid, nspin):
+    """The library's local H psi (no projectors; tensor-copy sweep on 12^3, the
+    per-term orbital kernel on 16^3) against the reference's own AVX-512 stencil
+    on the same inputs: 1e-12 relative."""
+    from salmon2_b200 import synth
+    from salmon2_b200.rt import Context
+    import _systems as S
+    s = S.no_pp(synth.periodic_system(a=10.26, num=num, nkgrid=nkgrid, no=2, seed=90 + num, nspin=nspin,
+                                      name=f"avxg{num}"))
+    ac = (0.013, -0.021, 0.034)
+    ref = ref_witness.zstencil_avx512(s, s.psi, ac)
+    ctx = Context(s)
+    ctx.set_vec_Ac(ac)
+    h = ctx.zeros()
+    ctx.hpsi(ctx.upload(s.psi), h)
+    sl = s.grid.interior_slices()
+    got = ctx.download(h)
+    assert np.max(np.abs(got[sl] - ref[sl])) <= 1e-12 * np.max(np.abs(ref[sl]))
+    ctx.close()

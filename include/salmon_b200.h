@@ -122,6 +122,14 @@ int sb200_set_pp(sb200_ctx* ctx, int natom, int nps, int nlma, const int* mps, c
  * src/common/hamiltonian.f90:847-903).  Isolated grids ignore it.              */
 int sb200_set_vec_Ac(sb200_ctx* ctx, const double vec_Ac[3]);
 
+/* Impulse kick of the initial orbitals: psi <- exp(i e_impulse epdir.r) psi
+ * at every interior point of every orbital of the resident block psi (device
+ * pointer), r the grid coordinate lg%coordinate of set_gridcoordinate.
+ * Replaces: the ae_shape1 = 'impulse' branch of initialization_rt
+ * (src/rt/initialization_rt.f90:382-423; coordinates
+ * src/common/initialization.f90:1125-1190).                                    */
+int sb200_impulse_kick(sb200_ctx* ctx, void* psi, double e_impulse, const double epdir[3]);
+
 /* Arithmetic form of sb200_taylor / sb200_rt_propagate (SB200_PREC_*).          */
 int sb200_set_precision(sb200_ctx* ctx, int mode);
 

@@ -61,7 +61,7 @@ def lib():
                      "sbo_precond_real", "sbo_gscg_rwf", "sbo_gram_schmidt_real", "sbo_gram_schmidt_complex",
                      "sbo_subspace_diag_real", "sbo_inner_product_real", "sbo_exc_cor_pz", "sbo_poisson_coef",
                      "sbo_dft_table", "sbo_poisson_ft", "sbo_update_vlocal", "sbo_rt_run_scf",
-                     "sbo_poisson_isolated_ft"):
+                     "sbo_poisson_isolated_ft", "sbo_impulse_kick"):
             getattr(L, name)
         L.sbo_rt_run.restype = C.c_int
         L.sbo_rt_run_scf.restype = C.c_int
@@ -193,6 +193,13 @@ class Oracle:
         lib().sbo_taylor(C.byref(self.s), _p(tin), _p(tout),
                          _p(work), _p(zc), C.c_int(len(zc)))
         return tout
+
+    def impulse_kick(self, psi, e_impulse, epdir=(0.0, 0.0, 1.0)):
+        """Kicked copy of psi: exp(i e_impulse epdir.r) psi (initialization_rt.f90:382-423)."""
+        a = self._orb(psi).copy(order="F")
+        ep = np.ascontiguousarray(epdir, dtype=np.float64)
+        lib().sbo_impulse_kick(C.byref(self.s), _p(a), C.c_double(e_impulse), _p(ep))
+        return a
 
     def density(self, psi):
         a = self._orb(psi)

@@ -593,6 +593,35 @@ void sbo_calc_dip(const sbo_system* s, const double* rho, double* rbox) {
   rbox[3] = acc;
 }
 
+// Grid coordinate lg%coordinate(i, d) of set_gridcoordinate
+// (initialization.f90:1125-1190): isolated grids i h (odd global size) or
+// (i - 1/2) h (even), periodic grids (i - 1) h.
+static double grid_coordinate(const sbo_system* s, int d, int i) {
+  if (s->periodic) return (double)(i - 1) * s->hgs[d];
+  return (s->lg_num[d] % 2 == 1) ? (double)i * s->hgs[d] : ((double)i - 0.5) * s->hgs[d];
+}
+
+// Impulse kick of the initial orbitals (initialization_rt.f90:382-423):
+// R1 = epdir . r at every interior point, then zwf <- exp(i e_impulse R1) zwf
+// for every (spin, orbital, k).
+void sbo_impulse_kick(const sbo_system* s, double* psi, double e_impulse, const double epdir[3]) {
+  Idx I(s);
+  const long vol = I.vol;
+  const int norb = s->nspin * s->no * s->nk;
+  for (int o = 0; o < norb; ++o)
+    for (int iz = s->is[2]; iz <= s->ie[2]; ++iz)
+      for (int iy = s->is[1]; iy <= s->ie[1]; ++iy)
+        for (int ix = s->is[0]; ix <= s->ie[0]; ++ix) {
+          const double r1 = epdir[0] * grid_coordinate(s, 0, ix) + epdir[1] * grid_coordinate(s, 1, iy) +
+                            epdir[2] * grid_coordinate(s, 2, iz);
+          const std::complex<double> ph = std::exp(std::complex<double>(0.0, e_impulse * r1));
+          double* z = psi + 2 * (vol * o + I.a(ix, iy, iz));
+          const std::complex<double> v = ph * std::complex<double>(z[0], z[1]);
+          z[0] = v.real();
+          z[1] = v.imag();
+        }
+}
+
 // calc_Ac_ext_t, em_field.f90:86-306 (impulse, Acos2, Asin2cos).
 void sbo_calc_Ac_ext_t(int shape, double t0, double delta_t, int is, int ie, const double* epdir,
                        double f0, double omega, double tw, double phi_cep, double t1_start,

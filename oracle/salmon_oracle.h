@@ -12,7 +12,11 @@
  *     src/common/stencil_current.cu) compiled from the reference sources into
  *     oracle/_ref and run on the GPU; their outputs are committed as golden
  *     fixtures in tests/golden/.
- *   - zstencil / taylor / calc_density / calc_dip / calc_emfields and the
+ *   - zstencil (with the k+A coefficients and V_local of hpsi) is pinned
+ *     against the reference's own hand-vectorised AVX-512 stencil
+ *     (src/common/zstencil_core/avx512/seq.c, built with gcc into oracle/_ref)
+ *     on periodic grids; golden fixture in tests/golden/.
+ *   - taylor / calc_density / calc_dip / calc_emfields and the
  *     ground-state CG are pinned only by analytic known-answer tests
  *     (plane-wave eigenvalues of the finite-difference operator, exact Taylor
  *     polynomials of diagonal systems, Hermiticity, conservation laws): the
@@ -69,6 +73,9 @@ typedef struct {
 
 void sbo_set_threads(int n);
 int  sbo_get_threads(void);
+
+/* impulse kick of the initial orbitals (initialization_rt.f90:382-423) */
+void sbo_impulse_kick(const sbo_system* s, double* psi, double e_impulse, const double epdir[3]);
 
 /* Real-space stencil kernels */
 void sbo_zstencil(const sbo_system* s, const double* tpsi, double* htpsi,

@@ -86,6 +86,7 @@ SIGNATURES = {
     "sb200_batch_get_tiles": (C.c_int, [_vp, _ip, _ip]),
     "sb200_batch_autotune": (C.c_int, [_vp, _vp, _vp, C.c_int, _ip, _ip]),
     "sb200_batch_propagate": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int, C.c_double, _dp, C.c_int, _vp, _vp]),
+    "sb200_impulse_kick": (C.c_int, [_vp, _vp, C.c_double, _dp]),
     "sb200_hpsi_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _ip,
                                      C.c_double, _dp, _dp, _vp, _vp, C.c_int, C.c_int, C.c_int, _vp, _vp, _vp,
                                      _vp, _vp, _vp, _vp, _vp, _vp, _vp]),

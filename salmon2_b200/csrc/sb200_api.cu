@@ -728,6 +728,15 @@ int sb200_set_pp(sb200_ctx* c, int natom, int nps, int nlma, const int* mps, con
   return SB200_OK;
 }
 
+int sb200_impulse_kick(sb200_ctx* c, void* psi, double e_impulse, const double epdir[3]) {
+  CHECK_CTX(c);
+  TRY(require_ready(c, false));
+  if (!psi || !epdir) return set_error(SB200_ERR_INVALID_ARG, "sb200_impulse_kick: null pointer");
+  DeviceGuard dg(c->device);
+  TRY(launch_impulse_kick(c, (double2*)psi, e_impulse, epdir));
+  return SB200_OK;
+}
+
 int sb200_set_vec_Ac(sb200_ctx* c, const double vec_Ac[3]) {
   CHECK_CTX(c);
   if (!vec_Ac) return set_error(SB200_ERR_INVALID_ARG, "null vec_Ac");

@@ -239,6 +239,10 @@ bool step_orbital_applies(const sb200_ctx* c, int n_hamil);                  // 
 int launch_step_orbital(sb200_ctx* c, const double2* in, double2* out, const double2* zc, int n_hamil,
                         bool with_obs);
 int launch_observables(sb200_ctx* c, const double2* psi);
+struct KickArgs {
+  double e, ep[3], h[3], c0[3];  // e_impulse, direction, spacing, coordinate offset per axis
+};
+int launch_impulse_kick(sb200_ctx* c, double2* psi, double e_impulse, const double epdir[3]);
 int launch_project_moments(sb200_ctx* c, const double2* psi);
 int launch_finalize(sb200_ctx* c, int itt_host, int nt, int trans_longi, double dt, int spin_filter,
                     bool fused_obs = false);

@@ -564,6 +564,38 @@ int launch_project(sb200_ctx* c, const void* in, double2* proj, bool in32) {
   return SB200_OK;
 }
 
+// psi <- exp(i e_impulse epdir.r) psi on every orbital, r the grid coordinate
+// of set_gridcoordinate (initialization.f90:1125-1190)
+__global__ void k_impulse_kick(double2* __restrict__ psi, long npts, long norb, int nx, int ny, KickArgs k) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < npts * norb; i += (long)gridDim.x * blockDim.x) {
+    const long p = i % npts;
+    const int x = (int)(p % nx), y = (int)((p / nx) % ny), z = (int)(p / ((long)nx * ny));
+    const double r1 = k.ep[0] * (k.h[0] * (x + k.c0[0])) + k.ep[1] * (k.h[1] * (y + k.c0[1])) +
+                      k.ep[2] * (k.h[2] * (z + k.c0[2]));
+    double sn, cs;
+    sincos(k.e * r1, &sn, &cs);
+    const double2 v = psi[i];
+    psi[i] = make_double2(cs * v.x - sn * v.y, cs * v.y + sn * v.x);
+  }
+}
+
+int launch_impulse_kick(sb200_ctx* c, double2* psi, double e_impulse, const double epdir[3]) {
+  KickArgs k;
+  k.e = e_impulse;
+  for (int d = 0; d < 3; ++d) {
+    k.ep[d] = epdir[d];
+    k.h[d] = c->g.hgs[d];
+    // coordinate of resident index x: (is + x - 1) h periodic; (is + x) h or (is + x - 1/2) h isolated
+    k.c0[d] = c->g.periodic ? (double)(c->g.is[d] - 1)
+                            : (c->g.lg_num[d] % 2 == 1 ? (double)c->g.is[d] : (double)c->g.is[d] - 0.5);
+  }
+  const long n = c->g.npts * c->orb.norb;
+  const unsigned blocks = (unsigned)((n + 255) / 256 < 148 * 32 ? (n + 255) / 256 : 148 * 32);
+  k_impulse_kick<<<blocks, 256, 0, c->stream>>>(psi, c->g.npts, c->orb.norb, c->g.nx, c->g.ny, k);
+  SB_LAUNCH_CHECK("k_impulse_kick");
+  return SB200_OK;
+}
+
 int launch_project_moments(sb200_ctx* c, const double2* psi) {
   if (c->pp.nlma == 0) return SB200_OK;
   ProjArgs a = make_proj_args(c);

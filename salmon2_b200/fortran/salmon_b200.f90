@@ -185,6 +185,14 @@ module salmon_b200
       real(c_double), intent(inout) :: rbox(4)
     end function
 
+    ! initialization_rt.f90:382-423: psi <- exp(i e_impulse epdir.r) psi (psi: device block)
+    integer(c_int) function sb200_impulse_kick(ctx, psi, e_impulse, epdir) bind(c, name="sb200_impulse_kick")
+      import
+      type(c_ptr), value :: ctx, psi
+      real(c_double), value :: e_impulse
+      real(c_double), intent(in) :: epdir(3)
+    end function
+
     ! H psi without any allocation: every array is caller-owned device memory
     ! (passed as addresses) except is, coef_lap0, coef_lap, coef_nab; status is
     ! a device integer (or c_null_ptr) set to SB200_ERR_BAD_SHAPE when a table

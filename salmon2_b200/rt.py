@@ -89,6 +89,12 @@ class Context:
         a = np.ascontiguousarray(vec_Ac, dtype=np.float64)
         check(lib().sb200_set_vec_Ac(self.h, _ptr(a)))
 
+    def impulse_kick(self, psi, e_impulse, epdir=(0.0, 0.0, 1.0)):
+        """psi <- exp(i e_impulse epdir.r) psi on the device (initialization_rt's impulse)."""
+        ep = np.ascontiguousarray(epdir, dtype=np.float64)
+        check(lib().sb200_impulse_kick(self.h, C.c_void_p(psi.data_ptr()), float(e_impulse), _ptr(ep)))
+        return psi
+
     def set_precision(self, precision: str):
         mode = {"fp64": _lib.PREC_FP64, "mixed": _lib.PREC_MIXED}[precision]
         check(lib().sb200_set_precision(self.h, mode))

@@ -465,3 +465,17 @@ def test_projection_forms_against_oracle(make, variant, monkeypatch):
     out, work = ctx.zeros(), ctx.zeros()
     ctx.taylor(ctx.upload(sysm.psi), out, work, zc)
     assert S.rel_err(ctx.download(out), O.taylor(sysm.psi, zc)) < TOL_H
+
+
+@pytest.mark.parametrize("make,epdir", [(S.isolated_small, (0.0, 0.0, 1.0)), (S.isolated_odd, (0.6, 0.0, 0.8)),
+                                        (S.periodic_small, (1.0, 0.0, 0.0))], ids=["iso24_z", "iso_odd", "p12_x"])
+def test_impulse_kick_against_oracle(make, epdir):
+    """sb200_impulse_kick on the resident block against the oracle's
+    restatement of initialization_rt.f90:382-423 (odd and even grid sizes,
+    the coordinate conventions of set_gridcoordinate)."""
+    sysm = make()
+    ctx = _ctx(sysm)
+    psi = ctx.upload(sysm.psi)
+    ctx.impulse_kick(psi, 1e-3, epdir)
+    ref = Oracle(sysm).impulse_kick(sysm.psi, 1e-3, epdir)
+    assert S.rel_err(ctx.download(psi), ref) < 1e-15 * 10

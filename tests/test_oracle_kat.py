@@ -206,3 +206,18 @@ def test_kinetic_part_and_eigen_energy():
     sl2 = s2.grid.interior_slices() + (0, 0, 0)
     E = fd_energy(s2.grid, q, s2.vec_k[:, 0] + np.array([0.0, 0.0, 0.03]))
     np.testing.assert_allclose(tt2[sl2], E * pwv[sl2], rtol=0, atol=1e-13 * np.abs(pwv[sl2]).max() * max(1, abs(E)))
+
+
+@pytest.mark.parametrize("num,epdir", [(24, (0.0, 0.0, 1.0)), ((21, 19, 17), (0.6, 0.0, 0.8))])
+def test_impulse_kick_oracle_equals_synth(num, epdir):
+    """The oracle's restatement of the impulse kick (initialization_rt.f90:
+    382-423 with the coordinates of set_gridcoordinate) equals the
+    generator's numpy form, and keeps |psi| point by point."""
+    from salmon2_b200 import synth
+    s = synth.isolated_system(num=num, no=2, natom=1, seed=61, name="kick")
+    O = Oracle(s)
+    k = 1e-3
+    a = O.impulse_kick(s.psi, k, epdir)
+    b = synth.impulse_kick(s.grid, s.psi, k, epdir)
+    assert np.max(np.abs(a - b)) <= 1e-15 * np.max(np.abs(b))
+    assert np.max(np.abs(np.abs(a) - np.abs(s.psi))) <= 1e-15

@@ -338,6 +338,26 @@ int sb200_hartree_periodic(sb200_ctx* ctx, const double primitive_b[9], const do
  * tables init_reciprocal_grid_isolated_ft, src/common/initialization.f90:823-1077). */
 int sb200_hartree_isolated_ft(sb200_ctx* ctx, const double primitive_b[9], const double* rho, double* Vh);
 
+/* Vh(is:ie) of rho on an isolated grid by conjugate gradients on the 25-point
+ * Laplacian (the reference's default method_poisson = 'cg').  Vh holds the
+ * start value on entry (the previous step's potential, or zeros) and the
+ * solution on exit.  Boundary values in the four halo layers of each face come
+ * from multipole expansions (l <= lmax_multipole <= 4) of the density about
+ * poles: layout_multipole 1 one pole at the origin, 2 one pole per atom over
+ * its nearest grid points (Rion(3, natom) needed), 3 box cells
+ * (num_multipole_xyz per axis; NULL or zeros: about 8 A each) centred on their
+ * charge centroid.  Stops when hvol sum |r|^2 < threshold_cg * (grid points),
+ * at most maxiter iterations; *iterations = poisson%iterVh (maxiter + 1 when
+ * not converged; may be NULL).  rho, Vh host or device, synchronous.  Periodic
+ * grids: SB200_ERR_UNSUPPORTED.
+ * Replaces: hartree with method_poisson = 'cg' on an isolated system ->
+ * poisson_isolated_cg / laplacian_poisson / poisson_boundary
+ * (src/poisson/poisson_isolated.f90:30-690) with the pole tables of
+ * make_corr_pole and set_ig_bound (src/poisson/init_poisson.f90:23-299).      */
+int sb200_hartree_isolated_cg(sb200_ctx* ctx, const double* rho, double* Vh, int layout_multipole,
+                              int lmax_multipole, const double* Rion, int natom, const int num_multipole_xyz[3],
+                              double threshold_cg, int maxiter, int* iterations);
+
 /* V_local(is) = Vpsl + Vh + Vxc(is) written into the context's device copy of
  * V_local (FP64 and the FP32 copy of the mixed form); Vpsl, Vh (is:ie), Vxc
  * (is:ie, nspin).  Also serves as the first sb200_set_vlocal.

@@ -61,11 +61,12 @@ def lib():
                      "sbo_precond_real", "sbo_gscg_rwf", "sbo_gram_schmidt_real", "sbo_gram_schmidt_complex",
                      "sbo_subspace_diag_real", "sbo_inner_product_real", "sbo_exc_cor_pz", "sbo_poisson_coef",
                      "sbo_dft_table", "sbo_poisson_ft", "sbo_update_vlocal", "sbo_rt_run_scf",
-                     "sbo_poisson_isolated_ft", "sbo_impulse_kick"):
+                     "sbo_poisson_isolated_ft", "sbo_impulse_kick", "sbo_poisson_isolated_cg", "sbo_ylm"):
             getattr(L, name)
         L.sbo_rt_run.restype = C.c_int
         L.sbo_rt_run_scf.restype = C.c_int
         L.sbo_get_threads.restype = C.c_int
+        L.sbo_ylm.restype = C.c_double
         _lib = L
     return _lib
 
@@ -201,6 +202,25 @@ class Oracle:
         lib().sbo_impulse_kick(C.byref(self.s), _p(a), C.c_double(e_impulse), _p(ep))
         return a
 
+    def poisson_isolated_cg(self, rho, vh0=None, layout=3, lmax=4, rion=None, npole_xyz=None,
+                            threshold=1e-15, maxiter=1000):
+        """Isolated Hartree potential by CG with the multipole boundary
+        (poisson_isolated_cg, src/poisson/poisson_isolated.f90:30-690).  rho,
+        vh0: (nx, ny, nz) interior; rion: (3, natom) (default: the system's
+        atoms); npole_xyz: cells of layout 3 (default: about 8 A each,
+        init_poisson.f90:112-115).  Returns (Vh, iterations)."""
+        g = self.sys.grid
+        r = _flat_f(rho)
+        v = _flat_f(np.zeros(g.shape) if vh0 is None else vh0).copy()
+        ri = np.asarray(self.sys.rion if rion is None else rion, dtype=np.float64).reshape(3, -1, order="F")
+        rflat = np.ascontiguousarray(ri.T)
+        npx = np.asarray(multipole_cells(g.num, g.hgs) if npole_xyz is None else npole_xyz, dtype=np.int32)
+        it = C.c_int(0)
+        lib().sbo_poisson_isolated_cg(C.byref(self.s), _p(r), _p(v), C.c_int(layout), C.c_int(lmax), _p(rflat),
+                                      C.c_int(rflat.shape[0]), npx.ctypes.data_as(_ip), C.c_double(threshold),
+                                      C.c_int(maxiter), C.byref(it))
+        return v.reshape(g.shape, order="F"), it.value
+
     def density(self, psi):
         a = self._orb(psi)
         rho = np.zeros(self.sys.grid.shape + (self.sys.nspin,), order="F")
@@ -321,6 +341,17 @@ class Oracle:
 def _flat_f(a):
     """(nx, ny, nz[, ...]) array -> contiguous float64 vector, x fastest."""
     return np.ascontiguousarray(np.asarray(a, dtype=np.float64).ravel(order="F"))
+
+
+def multipole_cells(num, hgs):
+    """Cells per axis of multipole layout 3 when num_multipole_xyz is 0:
+    int((al + s) / s - 1e-8) with s = 8 A (src/poisson/init_poisson.f90:112-115)."""
+    sp = 8.0 / 0.52917721067
+    return [int((float(n) * float(h) + sp) / sp - 1e-8) for n, h in zip(num, hgs)]
+
+
+def ylm(x, y, z, lm):
+    return lib().sbo_ylm(C.c_double(x), C.c_double(y), C.c_double(z), C.c_int(lm))
 
 
 def exc_cor_pz(rho, hvol):

@@ -166,6 +166,15 @@ void sbo_dft_table(int n, double* eg);
 void sbo_poisson_ft(const int num[3], const double brl[9], const double* rho, double* vh);
 void sbo_poisson_isolated_ft(const int num[3], const double brl[9], const double* rho, double* vh);
 void sbo_update_vlocal(long n, int nspin, const double* vpsl, const double* vh, const double* vxc, double* vloc);
+/* poisson_isolated_cg with the multipole boundary (src/poisson/poisson_isolated.f90:
+ * 30-690; pole tables of src/poisson/init_poisson.f90:23-299): layout 1 / 2 / 3,
+ * lmax <= 4, rion [natom][3], npole_xyz the cells of layout 3.  vh: start value
+ * in, solution out (interior, x fastest).                                       */
+void sbo_poisson_isolated_cg(const sbo_system* s, const double* rho, double* vh, int layout, int lmax,
+                             const double* rion, int natom, const int npole_xyz[3], double threshold,
+                             int maxiter, int* iterations);
+/* Ylm (src/math/salmon_math.f90:386-426), lm = l^2 + l + m, l <= 4            */
+double sbo_ylm(double x, double y, double z, int lm);
 /* sbo_rt_run with the self-consistent potential update every step (nspin = 1;
  * periodic or isolated Hartree by transforms): vloc holds V_local on entry and
  * is rewritten each step as Vpsl + Vh[rho] + Vxc[rho]; returns -1 for nspin 2. */

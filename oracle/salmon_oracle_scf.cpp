@@ -228,4 +228,260 @@ void sbo_update_vlocal(long n, int nspin, const double* vpsl, const double* vh, 
     for (long i = 0; i < n; ++i) vloc[is * n + i] = vpsl[i] + vh[i] + vxc[is * n + i];
 }
 
+
+// ---- poisson_isolated_cg with the multipole boundary ---------------------------
+//
+// poisson_isolated_cg (src/poisson/poisson_isolated.f90:30-221, one process),
+// laplacian_poisson (:223-257) and poisson_boundary (:259-690), with the pole
+// tables of make_corr_pole (src/poisson/init_poisson.f90:23-219) and the face
+// halos of set_ig_bound (:223-299).  Grid from the sbo_system (is:ie, hgs,
+// coef_lap0, coef_lap); rho and vh interior arrays (x fastest); vh is the start
+// value on entry and the solution on exit.  layout 1: one pole at the origin;
+// 2: one pole per atom over its nearest grid points; 3: box cells of about
+// 8 A with their charge centroid as centre.  *iterations is poisson%iterVh
+// (maxiter + 1 when not converged).
+void sbo_poisson_isolated_cg(const sbo_system* s, const double* rho, double* vh, int layout, int lmax,
+                             const double* rion, int natom, const int npole_xyz[3], double threshold,
+                             int maxiter, int* iterations) {
+  const int ND = 4;
+  const int nx = s->ie[0] - s->is[0] + 1, ny = s->ie[1] - s->is[1] + 1, nz = s->ie[2] - s->is[2] + 1;
+  const long N = (long)nx * ny * nz;
+  const int px = nx + 2 * ND, py = ny + 2 * ND, pz = nz + 2 * ND;
+  const long P = (long)px * py * pz;
+  auto pa = [&](int x, int y, int z) {  // padded index of interior offsets (x, y, z) in [-4, n + 4)
+    return (long)(x + ND) + px * ((long)(y + ND) + py * (long)(z + ND));
+  };
+  auto ri = [&](int x, int y, int z) { return (long)x + nx * ((long)y + (long)ny * z); };
+  auto coord = [&](int d, int i) {  // i: global index
+    return (s->lg_num[d] % 2 == 1) ? (double)i * s->hgs[d] : ((double)i - 0.5) * s->hgs[d];
+  };
+  const double hvol = s->hvol;
+  const int nlm = (lmax + 1) * (lmax + 1);
+  // ---- poles: centres, point lists and multipole moments (poisson_boundary)
+  std::vector<std::vector<long>> pts;  // interior offsets per pole, in z, y, x loop order
+  std::vector<double> cen;             // 3 per pole
+  std::vector<int> itrho;
+  if (layout == 1) {
+    pts.resize(1);
+    for (int z = 0; z < nz; ++z)
+      for (int y = 0; y < ny; ++y)
+        for (int x = 0; x < nx; ++x) pts[0].push_back(ri(x, y, z));
+    cen.assign(3, 0.0);
+    itrho.assign(1, 1);
+  } else if (layout == 2) {
+    pts.resize(natom);
+    for (int z = 0; z < nz; ++z)
+      for (int y = 0; y < ny; ++y)
+        for (int x = 0; x < nx; ++x) {
+          double rmin = 1e6;
+          int amin = 0;
+          for (int a = 0; a < natom; ++a) {
+            const double dx = coord(0, x + s->is[0]) - rion[3 * a], dy = coord(1, y + s->is[1]) - rion[3 * a + 1],
+                         dz = coord(2, z + s->is[2]) - rion[3 * a + 2];
+            const double r = std::sqrt(dx * dx + dy * dy + dz * dz);
+            if (r < rmin) {
+              rmin = r;
+              amin = a;
+            }
+          }
+          pts[amin].push_back(ri(x, y, z));
+        }
+    cen.assign(rion, rion + 3 * natom);
+    itrho.assign(natom, 1);
+  } else {
+    const int n1 = npole_xyz[0], n2 = npole_xyz[1], n3 = npole_xyz[2];
+    const int ncell = n1 * n2 * n3;
+    pts.resize(ncell);
+    for (int j3 = 0; j3 < n3; ++j3)
+      for (int j2 = 0; j2 < n2; ++j2)
+        for (int j1 = 0; j1 < n1; ++j1) {
+          const int ib = j1 + n1 * (j2 + n2 * j3);
+          for (int z = j3 * nz / n3; z <= (j3 + 1) * nz / n3 - 1; ++z)
+            for (int y = j2 * ny / n2; y <= (j2 + 1) * ny / n2 - 1; ++y)
+              for (int x = j1 * nx / n1; x <= (j1 + 1) * nx / n1 - 1; ++x) pts[ib].push_back(ri(x, y, z));
+        }
+    cen.assign(3 * (size_t)ncell, 0.0);
+    itrho.assign(ncell, 0);
+    for (int c = 0; c < ncell; ++c) {
+      double nd[4] = {0, 0, 0, 0};
+      for (long q : pts[c]) {
+        const int x = (int)(q % nx), y = (int)((q / nx) % ny), z = (int)(q / ((long)nx * ny));
+        nd[0] = nd[0] + rho[q] * coord(0, x + s->is[0]);
+        nd[1] = nd[1] + rho[q] * coord(1, y + s->is[1]);
+        nd[2] = nd[2] + rho[q] * coord(2, z + s->is[2]);
+        nd[3] = nd[3] + rho[q];
+      }
+      if (nd[3] * hvol >= 1e-12) {
+        itrho[c] = 1;
+        for (int d = 0; d < 3; ++d) cen[3 * c + d] = nd[d] / nd[3];
+      }
+    }
+  }
+  const int npole = (int)pts.size();
+  std::vector<double> rholm((size_t)npole * nlm, 0.0);
+  for (int c = 0; c < npole; ++c) {
+    if (!itrho[c]) continue;
+    for (int lm = 0; lm < nlm; ++lm) {
+      int l = 0;
+      while ((l + 1) * (l + 1) <= lm) ++l;
+      double acc = 0.0;
+      for (long q : pts[c]) {
+        const int x = (int)(q % nx), y = (int)((q / nx) % ny), z = (int)(q / ((long)nx * ny));
+        const double xx = coord(0, x + s->is[0]) - cen[3 * c], yy = coord(1, y + s->is[1]) - cen[3 * c + 1],
+                     zz = coord(2, z + s->is[2]) - cen[3 * c + 2];
+        const double rr = std::sqrt(xx * xx + yy * yy + zz * zz) + 1e-50;
+        double rl = 1.0;
+        for (int i = 0; i < l; ++i) rl *= rr;
+        acc = acc + rl * sbo_ylm(xx / rr, yy / rr, zz / rr, lm) * rho[q] * hvol;
+      }
+      rholm[(size_t)c * nlm + lm] = acc;
+    }
+  }
+  // ---- CG (pk carries the boundary values in its face halos for the first Laplacian)
+  std::vector<double> pk(P, 0.0), zk(P, 0.0), rlap(N, 0.0);
+  auto boundary = [&](int gx, int gy, int gz) {  // global indices of a halo point
+    double v = 0.0;
+    for (int c = 0; c < npole; ++c) {
+      if (!itrho[c]) continue;
+      const double xx = coord(0, gx) - cen[3 * c], yy = coord(1, gy) - cen[3 * c + 1], zz = coord(2, gz) - cen[3 * c + 2];
+      const double rinv = 1.0 / (std::sqrt(xx * xx + yy * yy + zz * zz) + 1e-50);
+      double sum1 = 0.0, rp = rinv;
+      int lcur = 0;
+      for (int lm = 0; lm < nlm; ++lm) {
+        int l = 0;
+        while ((l + 1) * (l + 1) <= lm) ++l;
+        if (l != lcur) {
+          rp *= rinv;
+          lcur = l;
+        }
+        sum1 = sum1 + sbo_ylm(xx * rinv, yy * rinv, zz * rinv, lm) * rp * rholm[(size_t)c * nlm + lm];
+      }
+      v = v + sum1;
+    }
+    return v;
+  };
+  for (int z = 0; z < nz; ++z)
+    for (int y = 0; y < ny; ++y)
+      for (int h = 0; h < ND; ++h) {
+        pk[pa(-ND + h, y, z)] = boundary(s->is[0] - ND + h, y + s->is[1], z + s->is[2]);
+        pk[pa(nx + h, y, z)] = boundary(s->ie[0] + 1 + h, y + s->is[1], z + s->is[2]);
+      }
+  for (int z = 0; z < nz; ++z)
+    for (int h = 0; h < ND; ++h)
+      for (int x = 0; x < nx; ++x) {
+        pk[pa(x, -ND + h, z)] = boundary(x + s->is[0], s->is[1] - ND + h, z + s->is[2]);
+        pk[pa(x, ny + h, z)] = boundary(x + s->is[0], s->ie[1] + 1 + h, z + s->is[2]);
+      }
+  for (int h = 0; h < ND; ++h)
+    for (int y = 0; y < ny; ++y)
+      for (int x = 0; x < nx; ++x) {
+        pk[pa(x, y, -ND + h)] = boundary(x + s->is[0], y + s->is[1], s->is[2] - ND + h);
+        pk[pa(x, y, nz + h)] = boundary(x + s->is[0], y + s->is[1], s->ie[2] + 1 + h);
+      }
+  const double lap0 = s->coef_lap0;
+  const double* lt = s->coef_lap;  // lapt(i, d) at lt[i + 4 d]
+  auto laplacian = [&]() {
+    for (int z = 0; z < nz; ++z)
+      for (int y = 0; y < ny; ++y)
+        for (int x = 0; x < nx; ++x) {
+          const long c = pa(x, y, z);
+          const long sx = 1, sy = px, sz = (long)px * py;
+          double t = 0.0;
+          t = lt[0] * (pk[c + sx] + pk[c - sx]);
+          t = t + lt[1] * (pk[c + 2 * sx] + pk[c - 2 * sx]);
+          t = t + lt[2] * (pk[c + 3 * sx] + pk[c - 3 * sx]);
+          t = t + lt[3] * (pk[c + 4 * sx] + pk[c - 4 * sx]);
+          t = t + lt[4] * (pk[c + sy] + pk[c - sy]);
+          t = t + lt[5] * (pk[c + 2 * sy] + pk[c - 2 * sy]);
+          t = t + lt[6] * (pk[c + 3 * sy] + pk[c - 3 * sy]);
+          t = t + lt[7] * (pk[c + 4 * sy] + pk[c - 4 * sy]);
+          t = t + lt[8] * (pk[c + sz] + pk[c - sz]);
+          t = t + lt[9] * (pk[c + 2 * sz] + pk[c - 2 * sz]);
+          t = t + lt[10] * (pk[c + 3 * sz] + pk[c - 3 * sz]);
+          t = t + lt[11] * (pk[c + 4 * sz] + pk[c - 4 * sz]);
+          rlap[ri(x, y, z)] = -2.0 * lap0 * pk[c] + t;
+        }
+  };
+  for (int z = 0; z < nz; ++z)
+    for (int y = 0; y < ny; ++y)
+      for (int x = 0; x < nx; ++x) {
+        pk[pa(x, y, z)] = vh[ri(x, y, z)];
+        zk[pa(x, y, z)] = -4.0 * PI * rho[ri(x, y, z)];
+      }
+  laplacian();
+  std::fill(pk.begin(), pk.end(), 0.0);
+  double sum1 = 0.0;
+  for (int z = 0; z < nz; ++z)
+    for (int y = 0; y < ny; ++y)
+      for (int x = 0; x < nx; ++x) {
+        const long c = pa(x, y, z);
+        zk[c] = zk[c] - rlap[ri(x, y, z)];
+        pk[c] = zk[c];
+        sum1 = sum1 + zk[c] * zk[c] * hvol;
+      }
+  int iter = 1;
+  for (; iter <= maxiter; ++iter) {
+    laplacian();
+    double tot = 0.0;
+    for (int z = 0; z < nz; ++z)
+      for (int y = 0; y < ny; ++y)
+        for (int x = 0; x < nx; ++x) tot = tot + zk[pa(x, y, z)] * rlap[ri(x, y, z)];
+    const double ak = sum1 / tot / hvol;
+    double z2 = 0.0;
+    for (int z = 0; z < nz; ++z)
+      for (int y = 0; y < ny; ++y)
+        for (int x = 0; x < nx; ++x) {
+          const long c = pa(x, y, z), r = ri(x, y, z);
+          vh[r] = vh[r] + ak * pk[c];
+          zk[c] = zk[c] - ak * rlap[r];
+          z2 = z2 + zk[c] * zk[c];
+        }
+    const double sum2 = z2 * hvol;
+    if (std::fabs(sum2) < threshold * (double)N) break;
+    const double ck = sum2 / sum1;
+    sum1 = sum2;
+    for (int z = 0; z < nz; ++z)
+      for (int y = 0; y < ny; ++y)
+        for (int x = 0; x < nx; ++x) {
+          const long c = pa(x, y, z);
+          pk[c] = zk[c] + ck * pk[c];
+        }
+  }
+  *iterations = iter;
+}
+
+// Ylm of src/math/salmon_math.f90:386-426 (real harmonics with the normalisation
+// sqrt(4 pi / (2l + 1)) r^l Y_lm, as polynomials of x, y, z), lm = l^2 + l + m.
+double sbo_ylm(double x, double y, double z, int lm) {
+  const double r2 = x * x + y * y + z * z;
+  switch (lm) {
+    case 0: return 1.0;
+    case 1: return -y;
+    case 2: return z;
+    case 3: return -x;
+    case 4: return std::sqrt(3.0) * x * y;
+    case 5: return -std::sqrt(3.0) * y * z;
+    case 6: return (3.0 * z * z - r2) / 2.0;
+    case 7: return -std::sqrt(3.0) * x * z;
+    case 8: return std::sqrt(3.0 / 4.0) * (x * x - y * y);
+    case 9: return -std::sqrt(5.0 / 8.0) * y * (3 * x * x - y * y);
+    case 10: return std::sqrt(15.0) * x * y * z;
+    case 11: return -std::sqrt(3.0 / 8.0) * y * (5.0 * z * z - r2);
+    case 12: return z * (5.0 * z * z - 3 * r2) / 2.0;
+    case 13: return -std::sqrt(3.0 / 8.0) * x * (5.0 * z * z - r2);
+    case 14: return std::sqrt(15.0 / 4.0) * z * (x * x - y * y);
+    case 15: return -std::sqrt(5.0 / 8.0) * x * (x * x - 3.0 * y * y);
+    case 16: return std::sqrt(35.0) / 2.0 * x * y * (x * x - y * y);
+    case 17: return -std::sqrt(35.0 / 8.0) * y * z * (3.0 * x * x - y * y);
+    case 18: return std::sqrt(5.0) / 2.0 * x * y * (7.0 * z * z - r2);
+    case 19: return -std::sqrt(5.0 / 8.0) * y * z * (7.0 * z * z - 3.0 * r2);
+    case 20: return (35.0 * z * z * z * z - 30.0 * z * z * r2 + 3.0 * r2 * r2) / 8.0;
+    case 21: return -std::sqrt(5.0 / 8.0) * x * z * (7.0 * z * z - 3.0 * r2);
+    case 22: return std::sqrt(5.0) / 4.0 * (7.0 * z * z - r2) * (x * x - y * y);
+    case 23: return -std::sqrt(35.0 / 8.0) * x * z * (x * x - 3.0 * y * y);
+    case 24: return std::sqrt(35.0) / 8.0 * (x * x * x * x + y * y * y * y - 6.0 * x * x * y * y);
+    default: return 0.0;
+  }
+}
+
 }  // extern "C"

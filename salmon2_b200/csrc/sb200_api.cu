@@ -378,6 +378,7 @@ int sb200_ctx_destroy(sb200_ctx* c) {
   dfree(c->gs.d_mat);
   learned_free(c);
   scf_free(c);
+  pcg_free(c);
   for (cudaEvent_t e : c->ev) cudaEventDestroy(e);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
   delete c;

@@ -170,6 +170,8 @@ struct sb200_ctx {
   void* learned = nullptr;
   // per-step potential update (sb200_scf.cu)
   void* scf = nullptr;
+  // isolated Hartree potential by CG (sb200_poisson_cg.cu)
+  void* pcg = nullptr;
 };
 
 namespace sb200 {
@@ -264,6 +266,13 @@ int learned_precond_apply(sb200_ctx* c, const double* g, const double* x, double
 int gs_project_out(sb200_ctx* c, const double* X, int m, double* Y, int n);
 void learned_free(sb200_ctx* c);
 void scf_free(sb200_ctx* c);
+void pcg_free(sb200_ctx* c);
+// isolated Hartree potential by CG with the multipole boundary (sb200_poisson_cg.cu):
+// rho, vh host or device (vh: start value in, solution out); rion [natom][3]
+// (layout 2); npole_xyz: cells of layout 3 (NULL or zeros: about 8 A each)
+int hartree_isolated_cg(sb200_ctx* c, const double* rho, double* vh, int layout, int lmax, const double* rion,
+                        int natom, const int npole_xyz[3], double threshold, int maxiter, int* iterations);
+void pcg_default_cells(const sb200_ctx* c, int out[3]);
 // self-consistent time loop (sb200_scf.cu): buffers sized before a capture, and
 // the per-step potential update issued after each Taylor step (no-ops unless
 // sb200_set_self_consistent enabled it)

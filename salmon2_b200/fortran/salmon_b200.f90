@@ -239,6 +239,19 @@ module salmon_b200
       real(c_double), intent(inout) :: Vh(*)
     end function
 
+    integer(c_int) function sb200_hartree_isolated_cg(ctx, rho, Vh, layout_multipole, lmax_multipole, Rion, &
+        natom, num_multipole_xyz, threshold_cg, maxiter, iterations) bind(c, name="sb200_hartree_isolated_cg")
+      import
+      type(c_ptr), value :: ctx
+      real(c_double), intent(in) :: rho(*)
+      real(c_double), intent(inout) :: Vh(*)
+      integer(c_int), value :: layout_multipole, lmax_multipole, natom, maxiter
+      real(c_double), intent(in) :: Rion(3, *)
+      integer(c_int), intent(in) :: num_multipole_xyz(3)
+      real(c_double), value :: threshold_cg
+      integer(c_int), intent(out) :: iterations
+    end function
+
     integer(c_int) function sb200_update_vlocal(ctx, Vpsl, Vh, Vxc) bind(c, name="sb200_update_vlocal")
       import
       type(c_ptr), value :: ctx

@@ -246,6 +246,25 @@ class Context:
         check(lib().sb200_hartree_isolated_ft(self.h, _ptr(b), p, C.c_void_p(v.ctypes.data)))
         return v
 
+    def hartree_isolated_cg(self, rho, vh0=None, layout=3, lmax=4, rion=None, npole_xyz=None,
+                            threshold=1e-15, maxiter=1000):
+        """hartree -> poisson_isolated_cg (poisson_isolated.f90:30-690) on an
+        isolated grid: CG on the 25-point Laplacian from vh0 (default zero) with
+        multipole boundary values (layout_multipole 1 / 2 / 3, lmax <= 4).
+        rion (3, natom): atom positions (default: the system's); npole_xyz:
+        cells of layout 3 (default about 8 A each).  Returns (Vh, iterations)."""
+        g = self.sys.grid
+        p, keep = self._scalar_field(rho)
+        v = np.zeros(g.shape, order="F") if vh0 is None else np.array(vh0, dtype=np.float64, order="F")
+        ri = np.asarray(self.sys.rion if rion is None else rion, dtype=np.float64).reshape(3, -1, order="F")
+        rflat = np.ascontiguousarray(ri.T)
+        npx = (C.c_int * 3)(*([0, 0, 0] if npole_xyz is None else [int(n) for n in npole_xyz]))
+        it = C.c_int(0)
+        check(lib().sb200_hartree_isolated_cg(self.h, p, C.c_void_p(v.ctypes.data), int(layout), int(lmax),
+                                              _ptr(rflat), rflat.shape[0], npx, float(threshold), int(maxiter),
+                                              C.byref(it)))
+        return v, it.value
+
     def update_vlocal(self, vpsl, vh, vxc):
         """update_vlocal (hamiltonian.f90:813-843): V_local = Vpsl + Vh + Vxc on the
         device.  vxc: (nx, ny, nz, nspin) or (nx, ny, nz) for nspin = 1."""

@@ -359,3 +359,105 @@ def test_rt_propagate_self_consistent_isolated():
     assert np.max(np.abs(d_got - d_ref)) <= TOL_LOOP * np.max(np.abs(ref["rbox"][:3]))
     assert S.rel_err(ctx.download(res["psi"]), ref["psi"]) < TOL_LOOP
     ctx.close()
+
+
+def _gaussian_rho(system, centre=(0.7, -0.4, 0.3), sigma=1.0):
+    g = system.grid
+    x = [((np.arange(g.is_[d], g.ie[d] + 1) - (0.5 if g.num[d] % 2 == 0 else 0.0)) * g.hgs[d]) for d in range(3)]
+    X, Y, Z = np.meshgrid(*x, indexing="ij")
+    r = np.sqrt((X - centre[0]) ** 2 + (Y - centre[1]) ** 2 + (Z - centre[2]) ** 2)
+    return np.exp(-r ** 2 / (2 * sigma * sigma)) / (2 * np.pi * sigma * sigma) ** 1.5, r
+
+
+@pytest.mark.parametrize("make", [S.isolated_small, S.isolated_odd], ids=["iso24", "iso_odd"])
+@pytest.mark.parametrize("layout", [1, 2, 3])
+def test_hartree_isolated_cg_fixed_iterations_against_oracle(make, layout):
+    """25 CG iterations with the threshold at zero (no early exit) from the
+    multipole boundary of each layout, on the orbitals' density: the same
+    iterate as the oracle's within 1e-10 relative (the per-block sums of the
+    dot products are ordered differently from the oracle's serial sums, and
+    CG carries those roundings forward)."""
+    from salmon2_b200.rt import Context
+
+    s = make()
+    ctx = Context(s)
+    rho = Oracle(s).density(s.psi)[..., 0]
+    npx = (2, 2, 1) if layout == 3 else None
+    ref, it_ref = Oracle(s).poisson_isolated_cg(rho, layout=layout, npole_xyz=npx, threshold=0.0, maxiter=25)
+    got, it = ctx.hartree_isolated_cg(rho, layout=layout, npole_xyz=npx, threshold=0.0, maxiter=25)
+    print(f"CG fixed {s.name} layout {layout}: rel {S.rel_err(got, ref):.3e}")
+    assert it == it_ref == 26
+    assert S.rel_err(got, ref) < 1e-10
+    ctx.close()
+
+
+@pytest.mark.parametrize("layout", [1, 2, 3])
+def test_hartree_isolated_cg_converged_against_oracle(layout):
+    """The default threshold (1e-15 per grid point): the same iteration count
+    as the oracle (within one) and the same potential within 1e-9 relative;
+    device arrays in and out; a second solve started from the first solution
+    stops after fewer iterations, as the oracle's does."""
+    import torch
+    from salmon2_b200 import _lib
+    from salmon2_b200.rt import Context
+
+    s = S.isolated_small()
+    ctx = Context(s)
+    rho = Oracle(s).density(s.psi)[..., 0]
+    ref, it_ref = Oracle(s).poisson_isolated_cg(rho, layout=layout)
+    got, it = ctx.hartree_isolated_cg(rho, layout=layout)
+    print(f"CG converged layout {layout}: iterations {it} (oracle {it_ref}), rel {S.rel_err(got, ref):.3e}")
+    assert it_ref <= 1000 and abs(it - it_ref) <= 1
+    assert S.rel_err(got, ref) < 1e-9
+    rd = torch.from_numpy(np.ascontiguousarray(rho.ravel(order="F"))).cuda()
+    vd = torch.zeros_like(rd)
+    ri = np.ascontiguousarray(np.asarray(s.rion, dtype=np.float64).reshape(3, -1, order="F").T)
+    itc = C.c_int(0)
+    _lib.check(_lib.lib().sb200_hartree_isolated_cg(
+        ctx.h, C.c_void_p(rd.data_ptr()), C.c_void_p(vd.data_ptr()), layout, 4,
+        ri.ctypes.data_as(C.POINTER(C.c_double)), ri.shape[0], None, 1e-15, 1000, C.byref(itc)))
+    assert itc.value == it
+    assert np.array_equal(vd.cpu().numpy(), got.ravel(order="F"))
+    again, it2 = ctx.hartree_isolated_cg(rho, vh0=got, layout=layout)
+    again_ref, it2_ref = Oracle(s).poisson_isolated_cg(rho, vh0=ref, layout=layout)
+    assert it2 < it and abs(it2 - it2_ref) <= 1
+    assert S.rel_err(again, again_ref) < 1e-9 and S.rel_err(again, got) < 1e-7
+    ctx.close()
+
+
+def test_hartree_isolated_cg_gaussian_charge():
+    """A unit Gaussian charge off the box centre: the solution equals
+    erf(r / (sqrt(2) s)) / r within 5e-5 of its peak (the finite-difference
+    Laplacian and the l <= 4 boundary), and the default cells of layout 3 for a
+    16 A box (2 per axis) agree with the oracle's rule."""
+    from math import erf
+    from salmon2_b200 import synth
+    from salmon2_b200.rt import Context
+
+    s = S.no_pp(synth.isolated_system(num=32, h_aa=0.25, no=1, natom=2, seed=5, name="gauss32"))
+    rho, r = _gaussian_rho(s)
+    exact = np.vectorize(lambda q: erf(q / np.sqrt(2.0)) / q)(r)
+    ctx = Context(s)
+    for layout in (1, 3):
+        v, it = ctx.hartree_isolated_cg(rho, layout=layout)
+        assert it < 1000
+        assert np.max(np.abs(v - exact)) < 5e-5 * np.max(exact)
+    assert OR.multipole_cells([64] * 3, [0.25 / 0.52917721067] * 3) == [2, 2, 2]
+    ctx.close()
+
+
+def test_hartree_isolated_cg_refuses_periodic_and_bad_layout():
+    from salmon2_b200 import _lib
+    from salmon2_b200.rt import Context
+
+    ctx = Context(S.periodic_small())
+    rho = np.zeros(S.periodic_small().grid.shape)
+    with pytest.raises(_lib.SB200Error):
+        ctx.hartree_isolated_cg(rho)
+    ctx.close()
+    s = S.isolated_small()
+    ctx = Context(s)
+    with pytest.raises(_lib.SB200Error):
+        ctx.hartree_isolated_cg(np.zeros(s.grid.shape), layout=4)
+    assert b"layout_multipole" in _lib.lib().sb200_last_error()
+    ctx.close()

@@ -176,3 +176,47 @@ def test_rt_run_scf_equals_the_loop_written_out(kind):
         step.V[...] = potential(step.density(psi)[..., 0])
     assert np.max(np.abs(ref["psi"] - psi)) <= 1e-13 * np.max(np.abs(psi))
     assert np.max(np.abs(ref["V_local"] - step.V[..., 0])) <= 1e-13 * np.max(np.abs(step.V))
+
+
+def test_ylm_table_obeys_the_addition_theorem():
+    """sum_m Ylm(a) Ylm(b) = P_l(a.b) for unit vectors a, b, l <= 4: the
+    normalisation sqrt(4 pi / (2l + 1)) r^l Y_lm of the reference's Ylm
+    (salmon_math.f90:386-426) on which the multipole boundary rests."""
+    rng = np.random.default_rng(3)
+    for _ in range(5):
+        a = rng.normal(size=3)
+        b = rng.normal(size=3)
+        a /= np.linalg.norm(a)
+        b /= np.linalg.norm(b)
+        c = float(a @ b)
+        leg = [1.0, c, (3 * c * c - 1) / 2, (5 * c ** 3 - 3 * c) / 2, (35 * c ** 4 - 30 * c * c + 3) / 8]
+        for l in range(5):
+            s = sum(O.ylm(*a, l * l + l + m) * O.ylm(*b, l * l + l + m) for m in range(-l, l + 1))
+            assert abs(s - leg[l]) < 1e-14
+
+
+def test_poisson_isolated_cg_gaussian_charge():
+    """poisson_isolated_cg on a unit Gaussian charge off the box centre equals
+    erf(r / (sqrt(2) s)) / r within 5e-5 of the peak with the origin pole
+    (layout 1) and the cells of layout 3; the atom poles of layout 2 split the
+    charge over the atoms' Voronoi cells and truncate at l = 4 (1e-2); with the
+    threshold at zero the loop runs maxiter times and reports maxiter + 1."""
+    from math import erf
+    import _systems as S
+    from salmon2_b200 import synth
+    s = S.no_pp(synth.isolated_system(num=32, h_aa=0.25, no=1, natom=3, seed=5, name="gauss32"))
+    g = s.grid
+    x = [((np.arange(g.is_[d], g.ie[d] + 1) - (0.5 if g.num[d] % 2 == 0 else 0.0)) * g.hgs[d]) for d in range(3)]
+    X, Y, Z = np.meshgrid(*x, indexing="ij")
+    r = np.sqrt((X - 0.7) ** 2 + (Y + 0.4) ** 2 + (Z - 0.3) ** 2)
+    rho = np.exp(-r ** 2 / 2) / (2 * np.pi) ** 1.5
+    exact = np.vectorize(lambda q: erf(q / np.sqrt(2.0)) / q)(r)
+    orc = O.Oracle(s)
+    for layout, tol in ((1, 5e-5), (3, 5e-5), (2, 1e-2)):
+        v, it = orc.poisson_isolated_cg(rho, layout=layout)
+        assert it < 1000
+        assert np.max(np.abs(v - exact)) < tol * np.max(exact)
+    v, it = orc.poisson_isolated_cg(rho, layout=3, npole_xyz=(2, 2, 2))
+    assert np.max(np.abs(v - exact)) < 5e-5 * np.max(exact)
+    _, it = orc.poisson_isolated_cg(rho, threshold=0.0, maxiter=5)
+    assert it == 6

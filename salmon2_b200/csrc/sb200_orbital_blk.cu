@@ -244,7 +244,119 @@ __device__ __forceinline__ void project_contrib(const double2* __restrict__ buf,
   }
 }
 
-template <int BZ, bool OBS>
+// Split form of the projections: two warps per atom (warp w takes atoms
+// w / 2, w / 2 + NW / 2, ...; half w % 2 its sphere chunks k = w % 2, w % 2 + 2,
+// ...), each leaving its partial sums of the atom's 4 complex projections in
+// ppart[(2 atom + half) * 8 + v] (v = 2 q + re/im).  With `cached` the chunks'
+// uV and phases come from the warp's TMEM words at tkb + 12 i (chunk hf + 2 i).
+template <int NW>
+__device__ __forceinline__ void project_half(const double2* __restrict__ buf, const double2* __restrict__ sph,
+                                             const double* __restrict__ suv, const int* __restrict__ sap, int TP,
+                                             const int4* __restrict__ satm, double* __restrict__ ppart,
+                                             const OrbArgs& a, int warp, int lane, bool cached, uint32_t tkb) {
+  const int hf = warp & 1;
+  for (int atom = warp >> 1; atom < a.natom; atom += NW / 2) {
+    const int4 at = satm[atom];
+    const int start = at.x, m = at.y, np = at.w;
+    if (np == 0) continue;  // uniform over the warp
+    const int nk = (m + 31) >> 5;
+    double2 pq[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) pq[q] = make_double2(0.0, 0.0);
+    if (cached) {
+      for (int k = hf, i = 0; k < nk; k += 2, ++i) {
+        double u[4];
+        double2 e;
+        kb_load(tkb + 12 * i, u, e);
+        const int j = lane + 32 * k;
+        if (j < m) {
+          const double2 ev = cmul(e, buf[sap[start + j] & 4095]);
+#pragma unroll
+          for (int q = 0; q < 4; ++q) pq[q] = make_double2(fma(u[q], ev.x, pq[q].x), fma(u[q], ev.y, pq[q].y));
+        }
+      }
+    } else {
+      for (int k = hf; k < nk; k += 2) {
+        const int j = lane + 32 * k;
+        if (j < m) {
+          const int fp = start + j;
+          const double2 ev = cmul(sph[fp], buf[sap[fp] & 4095]);
+#pragma unroll
+          for (int q = 0; q < 4; ++q)
+            if (q < np) {
+              const double u = suv[q * TP + fp];
+              pq[q] = make_double2(fma(u, ev.x, pq[q].x), fma(u, ev.y, pq[q].y));
+            }
+        }
+      }
+    }
+    double v[8];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      v[2 * q] = pq[q].x;
+      v[2 * q + 1] = pq[q].y;
+    }
+    const double r = warp_reduce_scatter<8>(v, lane);  // lane 4 v holds value v
+    if ((lane & 3) == 0) ppart[(2 * atom + hf) * 8 + (lane >> 2)] = r;
+  }
+}
+
+// Split form of the contributions: P_q = rinv_q (half 0 + half 1) of each
+// atom, then pc[pair] = conj(e) sum_q uV_q P_q for the warp's chunks (the same
+// warp / chunk assignment as project_half).
+template <int NW>
+__device__ __forceinline__ void contrib_half(const double2* __restrict__ sph, const double* __restrict__ suv,
+                                             const int* __restrict__ sap, double2* __restrict__ pc, int TP,
+                                             const int4* __restrict__ satm, const double* __restrict__ srinv,
+                                             const double* __restrict__ ppart, const OrbArgs& a, int warp,
+                                             int lane, bool cached, uint32_t tkb) {
+  const int hf = warp & 1;
+  for (int atom = warp >> 1; atom < a.natom; atom += NW / 2) {
+    const int4 at = satm[atom];
+    const int start = at.x, m = at.y, lma0 = at.z, np = at.w;
+    if (np == 0) continue;
+    const int nk = (m + 31) >> 5;
+    const double* p0 = ppart + 16 * atom;
+    double2 pq[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const double r = q < np ? srinv[lma0 + q] : 0.0;
+      pq[q] = make_double2(r * (p0[2 * q] + p0[8 + 2 * q]), r * (p0[2 * q + 1] + p0[9 + 2 * q]));
+    }
+    if (cached) {
+      for (int k = hf, i = 0; k < nk; k += 2, ++i) {
+        double u[4];
+        double2 e;
+        kb_load(tkb + 12 * i, u, e);
+        const int j = lane + 32 * k;
+        if (j < m) {
+          double2 sp = make_double2(0.0, 0.0);
+#pragma unroll
+          for (int q = 0; q < 4; ++q) sp = make_double2(fma(u[q], pq[q].x, sp.x), fma(u[q], pq[q].y, sp.y));
+          pc[sap[start + j] >> 12] = cmul(make_double2(e.x, -e.y), sp);
+        }
+      }
+    } else {
+      for (int k = hf; k < nk; k += 2) {
+        const int j = lane + 32 * k;
+        if (j < m) {
+          const int fp = start + j;
+          double2 sp = make_double2(0.0, 0.0);
+#pragma unroll
+          for (int q = 0; q < 4; ++q)
+            if (q < np) {
+              const double u = suv[q * TP + fp];
+              sp = make_double2(fma(u, pq[q].x, sp.x), fma(u, pq[q].y, sp.y));
+            }
+          const double2 e = sph[fp];
+          pc[sap[fp] >> 12] = cmul(make_double2(e.x, -e.y), sp);
+        }
+      }
+    }
+  }
+}
+
+template <int BZ, bool OBS, bool SPLIT>
 __global__ void __launch_bounds__(Blk<BZ>::BT, 1) k_step_blk(const double2* __restrict__ in,
                                                              double2* __restrict__ out, OrbArgs a, BlkArgs bk,
                                                              StepZC zc, int nterm) {
@@ -263,6 +375,7 @@ __global__ void __launch_bounds__(Blk<BZ>::BT, 1) k_step_blk(const double2* __re
   int* sap = (int*)(pc + bk.npair);         // [TP] pair index << 12 | shared-memory index of each sphere point
   int4* satm = (int4*)(sap + TP);           // [natom] first flat point, sphere size, first ilma, projectors
   double* srinv = (double*)(satm + (kb ? a.natom : 0));  // [nlma] rinv_uvu
+  double* ppart = srinv + (kb ? a.nlma : 0);              // [natom][2][8] half projections (split form)
   __shared__ uint32_t s_tmem;
   __shared__ double kn[12];
   __shared__ double red[OBS_NQ][NW];
@@ -357,10 +470,12 @@ __global__ void __launch_bounds__(Blk<BZ>::BT, 1) k_step_blk(const double2* __re
   // KB cache: warp w < natom keeps its atom's uV and phases in TMEM for the step
   const bool kbc = kb && bk.kbcache != 0;
   const uint32_t tkb = tb + TW_KB;
-  if (kbc && warp < a.natom) {
-    const int4 at = satm[warp];
+  // (split form: warp w keeps chunks w % 2, w % 2 + 2, ... of atom w / 2)
+  const int cw = SPLIT ? (warp >> 1) : warp, c0 = SPLIT ? (warp & 1) : 0, cs = SPLIT ? 2 : 1;
+  if (kbc && cw < a.natom) {
+    const int4 at = satm[cw];
     const int nk = (at.y + 31) >> 5;
-    for (int k = 0; k < nk; ++k) {
+    for (int k = c0, i = 0; k < nk; k += cs, ++i) {
       const int j = lane + 32 * k;
       double u[4] = {0.0, 0.0, 0.0, 0.0};
       double2 e = make_double2(0.0, 0.0);
@@ -369,16 +484,18 @@ __global__ void __launch_bounds__(Blk<BZ>::BT, 1) k_step_blk(const double2* __re
         for (int q = 0; q < 4; ++q) u[q] = suv[q * TP + at.x + j];
         e = sph[at.x + j];
       }
-      kb_store(tkb + 12 * k, u, e);
+      kb_store(tkb + 12 * i, u, e);
     }
   }
-  if (kb) {
+  if (!SPLIT && kb) {
     project_contrib<NW>(buf, sph, suv, sap, pc, TP, satm, srinv, a, warp, lane, kbc, tkb);
     __syncthreads();
   }
   const int hm2 = (bx - 2) & 7, hm1 = (bx - 1) & 7, hp1 = (bx + 1) & 7, hp2 = (bx + 2) & 7;
   double2* odst = out + (long)o * a.npts;
   for (int nn = 0; nn < nterm; ++nn) {
+    // split form: this warp's partial projections of h_{n-1}, before its stencil
+    if (SPLIT && kb) project_half<NW>(buf, sph, suv, sap, TP, satm, ppart, a, warp, lane, kbc, tkb);
     double2 h[NS];
 #pragma unroll
     for (int s = 0; s < NS; ++s) h[s] = make_double2(0.0, 0.0);
@@ -454,6 +571,15 @@ __global__ void __launch_bounds__(Blk<BZ>::BT, 1) k_step_blk(const double2* __re
         }
       }
     }
+    if (SPLIT) {
+      // every read of h_{n-1} and every partial projection is done; the
+      // contributions of the finished projections, then the buffer is free
+      __syncthreads();
+      if (kb) {
+        contrib_half<NW>(sph, suv, sap, pc, TP, satm, srinv, ppart, a, warp, lane, kbc, tkb);
+        __syncthreads();
+      }
+    }
     // ---- diagonal, KB contributions, Taylor update (taylor.f90:47-117) ----
     const bool last = nn == nterm - 1;
     // zc(nn + 1) by constant indices (no local-memory copy of the argument)
@@ -504,8 +630,16 @@ __global__ void __launch_bounds__(Blk<BZ>::BT, 1) k_step_blk(const double2* __re
         if (last) {
           const int x = 2 * bx + (s & 1), y = 2 * by + ((s >> 1) & 1), z = z0 + (s >> 2);
           odst[gidx(x, y, z)] = an;
-          if (OBS) cv[s] = an;  // the new orbital, for the observables
+          if (OBS) {
+            cv[s] = an;  // the new orbital, for the observables
+            if (SPLIT) buf[sidx(x, y, z)] = an;
+          }
         } else {
+          if (SPLIT) {  // h_n into the (no longer read) buffer
+            const int x = 2 * bx + (s & 1), y = 2 * by + ((s >> 1) & 1), z = z0 + (s >> 2);
+            buf[sidx(x, y, z)] = hs;
+            cv[s] = hs;
+          }
           aw[4 * u] = tmem::lo_word(an.x);
           aw[4 * u + 1] = tmem::hi_word(an.x);
           aw[4 * u + 2] = tmem::lo_word(an.y);
@@ -513,6 +647,12 @@ __global__ void __launch_bounds__(Blk<BZ>::BT, 1) k_step_blk(const double2* __re
         }
       }
       if (!last) tmem::st16(tb + TW_ACC + 16 * q4, aw);
+    }
+    if (SPLIT) {
+      if (last && !OBS) break;
+      __syncthreads();  // h_n (or psi(t + dt)) complete in the buffer
+      if (last) break;
+      continue;
     }
     if (last) break;
     __syncthreads();  // every read of h_{n-1} and of the contributions is done
@@ -529,13 +669,15 @@ __global__ void __launch_bounds__(Blk<BZ>::BT, 1) k_step_blk(const double2* __re
     }
   }
   if (OBS) {
-    __syncthreads();  // the last term's reads of h_{n-1} are done
+    if (!SPLIT) {
+      __syncthreads();  // the last term's reads of h_{n-1} are done
 #pragma unroll
-    for (int s = 0; s < NS; ++s) {
-      const int x = 2 * bx + (s & 1), y = 2 * by + ((s >> 1) & 1), z = z0 + (s >> 2);
-      buf[sidx(x, y, z)] = cv[s];
+      for (int s = 0; s < NS; ++s) {
+        const int x = 2 * bx + (s & 1), y = 2 * by + ((s >> 1) & 1), z = z0 + (s >> 2);
+        buf[sidx(x, y, z)] = cv[s];
+      }
+      __syncthreads();
     }
-    __syncthreads();
     double q[OBS_NQ];
 #pragma unroll
     for (int i = 0; i < OBS_NQ; ++i) q[i] = 0.0;
@@ -598,64 +740,88 @@ __global__ void __launch_bounds__(Blk<BZ>::BT, 1) k_step_blk(const double2* __re
       const int k = lane >> 2;  // rs_lane<8>(k) = 4 k
       if ((lane & 3) == 0 && k < OBS_NQ) red[k][warp] = r;
     }
-    // nonlocal current: one warp per atom (density_matrix.f90:532-591)
+    // nonlocal current (density_matrix.f90:532-591): one warp per atom, or two
+    // per atom in the split form (their sums combined in warp order)
     double jx = 0.0, jy = 0.0, jz = 0.0;
-    if (kb) {
+    // chunk k of the atom's sphere (TMEM cache word i) into v: v[2c], v[2c + 1] =
+    // <beta_q|psi> (c = q < 4) and <r_d beta_q|psi> (c = 4 + 3 q + d)
+    auto nl_chunk = [&](double (&v)[32], int start, int m, int np, int k, int i) {
+      const int j = lane + 32 * k;
+      double uc[4];
+      double2 e;
+      if (kbc) kb_load(tkb + 12 * i, uc, e);
+      if (j >= m) return;
+      const int fp = start + j;
+      if (!kbc) {
+#pragma unroll
+        for (int qq = 0; qq < 4; ++qq) uc[qq] = suv[qq * TP + fp];
+        e = sph[fp];
+      }
+      const double2 ev = cmul(e, buf[sap[fp] & 4095]);
+      const double r0 = sr[fp], r1 = sr[TP + fp], r2 = sr[2 * TP + fp];
+#pragma unroll
+      for (int qq = 0; qq < 4; ++qq) {
+        if (qq < np) {
+          const double u = uc[qq];
+          const double tx = u * ev.x, ty = u * ev.y;
+          v[2 * qq] += tx;
+          v[2 * qq + 1] += ty;
+          v[8 + 6 * qq] = fma(r0, tx, v[8 + 6 * qq]);
+          v[9 + 6 * qq] = fma(r0, ty, v[9 + 6 * qq]);
+          v[10 + 6 * qq] = fma(r1, tx, v[10 + 6 * qq]);
+          v[11 + 6 * qq] = fma(r1, ty, v[11 + 6 * qq]);
+          v[12 + 6 * qq] = fma(r2, tx, v[12 + 6 * qq]);
+          v[13 + 6 * qq] = fma(r2, ty, v[13 + 6 * qq]);
+        }
+      }
+    };
+    // J contribution of one atom from its reduced sums s0 (+ s1, the other half)
+    auto nl_atom = [&](const double* s0, const double* s1, int lma0, int np) {
+#pragma unroll
+      for (int qq = 0; qq < 4; ++qq) {
+        if (qq < np) {
+          auto g = [&](int i) { return s1 ? s0[i] + s1[i] : s0[i]; };
+          const double rv = srinv[lma0 + qq];
+          const double usx = rv * g(2 * qq), usy = rv * g(2 * qq + 1);
+          const int b = 8 + 6 * qq;
+          jx += g(b) * usy - g(b + 1) * usx;
+          jy += g(b + 2) * usy - g(b + 3) * usx;
+          jz += g(b + 4) * usy - g(b + 5) * usx;
+        }
+      }
+    };
+    if (kb && SPLIT) {
+      const int rounds = (a.natom + NW / 2 - 1) / (NW / 2);
+      for (int rd = 0; rd < rounds; ++rd) {  // uniform over the CTA
+        const int atom = (warp >> 1) + rd * (NW / 2);
+        const int4 at = atom < a.natom ? satm[atom] : make_int4(0, 0, 0, 0);
+        double v[32];
+#pragma unroll
+        for (int i = 0; i < 32; ++i) v[i] = 0.0;
+        if (at.w > 0) {
+          const int nk = (at.y + 31) >> 5;
+          for (int k = warp & 1, i = 0; k < nk; k += 2, ++i) nl_chunk(v, at.x, at.y, at.w, k, i);
+        }
+        const double r = warp_reduce_scatter<32>(v, lane);  // lane L holds value L
+        nlred[warp][lane] = r;
+        __syncthreads();
+        if ((warp & 1) == 0 && lane == 0 && at.w > 0) nl_atom(nlred[warp], nlred[warp + 1], at.z, at.w);
+        __syncthreads();
+      }
+    } else if (kb) {
       for (int atom = warp; atom < a.natom; atom += NW) {
         const int4 at = satm[atom];
         const int start = at.x, m = at.y, lma0 = at.z, np = at.w;
         if (np == 0) continue;
-        // v[2c], v[2c + 1]: <beta_q|psi> (c = q < 4) and <r_d beta_q|psi> (c = 4 + 3 q + d)
         double v[32];
 #pragma unroll
         for (int i = 0; i < 32; ++i) v[i] = 0.0;
         const int nk = (m + 31) >> 5;
-        for (int k = 0; k < nk; ++k) {
-          const int j = lane + 32 * k;
-          double uc[4];
-          double2 e;
-          if (kbc) kb_load(tkb + 12 * k, uc, e);
-          if (j >= m) continue;
-          const int fp = start + j;
-          if (!kbc) {
-#pragma unroll
-            for (int qq = 0; qq < 4; ++qq) uc[qq] = suv[qq * TP + fp];
-            e = sph[fp];
-          }
-          const double2 ev = cmul(e, buf[sap[fp] & 4095]);
-          const double r0 = sr[fp], r1 = sr[TP + fp], r2 = sr[2 * TP + fp];
-#pragma unroll
-          for (int qq = 0; qq < 4; ++qq) {
-            if (qq < np) {
-              const double u = uc[qq];
-              const double tx = u * ev.x, ty = u * ev.y;
-              v[2 * qq] += tx;
-              v[2 * qq + 1] += ty;
-              v[8 + 6 * qq] = fma(r0, tx, v[8 + 6 * qq]);
-              v[9 + 6 * qq] = fma(r0, ty, v[9 + 6 * qq]);
-              v[10 + 6 * qq] = fma(r1, tx, v[10 + 6 * qq]);
-              v[11 + 6 * qq] = fma(r1, ty, v[11 + 6 * qq]);
-              v[12 + 6 * qq] = fma(r2, tx, v[12 + 6 * qq]);
-              v[13 + 6 * qq] = fma(r2, ty, v[13 + 6 * qq]);
-            }
-          }
-        }
+        for (int k = 0; k < nk; ++k) nl_chunk(v, start, m, np, k, k);
         const double r = warp_reduce_scatter<32>(v, lane);  // lane L holds value L
         nlred[warp][lane] = r;
         __syncwarp();
-        if (lane == 0) {
-#pragma unroll
-          for (int qq = 0; qq < 4; ++qq) {
-            if (qq < np) {
-              const double rv = srinv[lma0 + qq];
-              const double usx = rv * nlred[warp][2 * qq], usy = rv * nlred[warp][2 * qq + 1];
-              const double* ur = &nlred[warp][8 + 6 * qq];
-              jx += ur[0] * usy - ur[1] * usx;
-              jy += ur[2] * usy - ur[3] * usx;
-              jz += ur[4] * usy - ur[5] * usx;
-            }
-          }
-        }
+        if (lane == 0) nl_atom(nlred[warp], nullptr, lma0, np);
         __syncwarp();
       }
     }
@@ -733,7 +899,7 @@ size_t step_blk_smem(const sb200_ctx* c) {
   (void)T;
   const size_t natom = pp.nlma > 0 ? (size_t)pp.natom : 0, nlma = pp.nlma > 0 ? (size_t)pp.nlma : 0;
   return (size_t)NPTS * sizeof(double2) + TP * (sizeof(double2) + 7 * sizeof(double) + sizeof(int)) +
-         npair * sizeof(double2) + natom * sizeof(int4) + nlma * sizeof(double);
+         npair * sizeof(double2) + natom * sizeof(int4) + nlma * sizeof(double) + natom * 16 * sizeof(double);
 }
 
 int launch_step_blk(sb200_ctx* c, const double2* in, double2* out, const OrbArgs& a, const StepZC& z, int n_hamil,
@@ -741,13 +907,15 @@ int launch_step_blk(sb200_ctx* c, const double2* in, double2* out, const OrbArgs
   const size_t smem = step_blk_smem(c);
   if (smem == 0) return SB200_ERR_UNSUPPORTED;
   // per instantiation: the dynamic shared memory it may take next to its static arrays
-  static size_t cap[4] = {0, 0, 0, 0};
+  static size_t cap[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   if (cap[0] == 0) {
-    const void* fns[4] = {(const void*)k_step_blk<2, false>, (const void*)k_step_blk<2, true>,
-                          (const void*)k_step_blk<4, false>, (const void*)k_step_blk<4, true>};
+    const void* fns[8] = {(const void*)k_step_blk<2, false, false>, (const void*)k_step_blk<2, true, false>,
+                          (const void*)k_step_blk<4, false, false>, (const void*)k_step_blk<4, true, false>,
+                          (const void*)k_step_blk<2, false, true>,  (const void*)k_step_blk<2, true, true>,
+                          (const void*)k_step_blk<4, false, true>,  (const void*)k_step_blk<4, true, true>};
     int optin = 0;
     SB_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device));
-    for (int i = 0; i < 4; ++i) {
+    for (int i = 0; i < 8; ++i) {
       cudaFuncAttributes fa;
       SB_CUDA(cudaFuncGetAttributes(&fa, fns[i]));
       const size_t ci = (size_t)optin - fa.sharedSizeBytes;
@@ -755,7 +923,8 @@ int launch_step_blk(sb200_ctx* c, const double2* in, double2* out, const OrbArgs
       cap[i] = ci;
     }
   }
-  const int which = (c->blk_depth == 4 ? 2 : 0) + (with_obs ? 1 : 0);
+  const bool split = c->blk_split != 0;
+  const int which = (split ? 4 : 0) + (c->blk_depth == 4 ? 2 : 0) + (with_obs ? 1 : 0);
   if (smem > cap[which]) return SB200_ERR_UNSUPPORTED;
   BlkArgs bk;
   for (int i = 0; i < 12; ++i) bk.mhl[i] = -0.5 * c->g.coef_lap[i];
@@ -766,19 +935,30 @@ int launch_step_blk(sb200_ctx* c, const double2* in, double2* out, const OrbArgs
   bk.r3 = c->pp.d_blk_r;
   bk.sap = c->pp.d_blk_sap;
   bk.err = c->d_err;
-  {  // TMEM KB cache: at most one atom per warp and every sphere within the warp's TMEM words
+  {  // TMEM KB cache: at most one atom per warp (per warp pair in the split form) and
+     // every sphere chunk of the warp within its TMEM words
     const int nw = c->blk_depth == 4 ? Blk<4>::NW : Blk<2>::NW;
     const int chunks = c->blk_depth == 4 ? Blk<4>::KB_CHUNKS : Blk<2>::KB_CHUNKS;
-    bk.kbcache = (c->pp.nlma > 0 && c->pp.natom <= nw && c->pp.nps <= 32 * chunks) ? 1 : 0;
+    const int nk = (c->pp.nps + 31) / 32;
+    bk.kbcache = (c->pp.nlma > 0 && (split ? (c->pp.natom <= nw / 2 && (nk + 1) / 2 <= chunks)
+                                           : (c->pp.natom <= nw && nk <= chunks)))
+                     ? 1
+                     : 0;
   }
   dim3 grid(c->orb.norb);
-  if (c->blk_depth == 4) {
-    if (with_obs) k_step_blk<4, true><<<grid, Blk<4>::BT, smem, c->stream>>>(in, out, a, bk, z, n_hamil);
-    else k_step_blk<4, false><<<grid, Blk<4>::BT, smem, c->stream>>>(in, out, a, bk, z, n_hamil);
-  } else {
-    if (with_obs) k_step_blk<2, true><<<grid, Blk<2>::BT, smem, c->stream>>>(in, out, a, bk, z, n_hamil);
-    else k_step_blk<2, false><<<grid, Blk<2>::BT, smem, c->stream>>>(in, out, a, bk, z, n_hamil);
+#define SB_BLK_LAUNCH(BZ, OBS, SPLIT) \
+  k_step_blk<BZ, OBS, SPLIT><<<grid, Blk<BZ>::BT, smem, c->stream>>>(in, out, a, bk, z, n_hamil)
+  switch (which) {
+    case 0: SB_BLK_LAUNCH(2, false, false); break;
+    case 1: SB_BLK_LAUNCH(2, true, false); break;
+    case 2: SB_BLK_LAUNCH(4, false, false); break;
+    case 3: SB_BLK_LAUNCH(4, true, false); break;
+    case 4: SB_BLK_LAUNCH(2, false, true); break;
+    case 5: SB_BLK_LAUNCH(2, true, true); break;
+    case 6: SB_BLK_LAUNCH(4, false, true); break;
+    default: SB_BLK_LAUNCH(4, true, true); break;
   }
+#undef SB_BLK_LAUNCH
   SB_LAUNCH_CHECK("k_step_blk");
   return SB200_OK;
 }

@@ -197,15 +197,18 @@ def test_rt_propagate_periodic16_orbital_kernel(trans):
     assert S.rel_err(ctx.download(res["psi"]), ref["psi"]) < 1e-11
 
 
-@pytest.mark.parametrize("variant", ["fused", "unstaged", "persistent", "terms"])
+@pytest.mark.parametrize("variant", ["fused", "fused_nosplit", "unstaged", "persistent", "terms"])
 def test_rt_propagate_periodic16_many_orbitals(variant, monkeypatch):
     """More orbitals than SMs: the fused-step kernel (all Taylor terms in one
-    launch) with its KB tables staged in shared memory and without, the
-    persistent per-term form that walks several orbitals per CTA through
-    double-buffered bulk copies (buffer reuse, barrier phase flips) and the
-    one-launch-per-term form, each against the oracle on the same input."""
+    launch; its default form with the KB projections split over two warps per
+    atom, and the form with one warp per atom) with its KB tables staged in
+    shared memory and without, the persistent per-term form that walks several
+    orbitals per CTA through double-buffered bulk copies (buffer reuse, barrier
+    phase flips) and the one-launch-per-term form, each against the oracle on
+    the same input."""
     from salmon2_b200 import synth
-    monkeypatch.setenv("SB200_ORBITAL", variant)
+    monkeypatch.setenv("SB200_ORBITAL", variant.split("_")[0])
+    monkeypatch.setenv("SB200_BLK_SPLIT", "0" if variant.endswith("nosplit") else "1")
     sysm = synth.periodic_system(a=10.26, num=16, nkgrid=4, no=5, seed=32, name="periodic16k64")
     nt, dt = 6, 0.08
     Ac = synth.asin2cos(nt, dt, omega=0.05696, f0=0.05696 * 2e-2, tw=nt * dt)
@@ -237,11 +240,27 @@ def _p16_no_pp():
     return S.no_pp(synth.periodic_system(a=10.26, num=16, nkgrid=2, no=2, seed=37, name="p16nopp"))
 
 
-@pytest.mark.parametrize("make", [_p16_two_spins, _p16_wide_spheres, _p16_no_pp], ids=lambda f: f.__name__)
+def _p16_twelve_atoms():
+    # 12 atoms (more than half the warps of the fused step: the split
+    # projections take two rounds, and no TMEM cache), smaller spheres
+    import dataclasses
+    from salmon2_b200 import synth
+    s = synth.periodic_system(a=10.26, num=16, nkgrid=1, no=3, seed=39, rc_aa=0.9, name="p16twelve")
+    rng = np.random.default_rng(39)
+    rion = np.asfortranarray(np.concatenate([s.rion, rng.uniform(0.0, 10.26, size=(3, 4))], axis=1))
+    pp = synth.make_pp(s.grid, rion, 0.9 / synth.AU_LENGTH_AA, sigma=rng.uniform(0.5, 0.8, 12),
+                       amp=rng.uniform(0.3, 0.6, 12), inorm=rng.choice([-1, 1], size=(12, 2)),
+                       cell=np.full(3, 10.26))
+    return dataclasses.replace(s, pp=pp, rion=rion)
+
+
+@pytest.mark.parametrize("make", [_p16_two_spins, _p16_wide_spheres, _p16_no_pp, _p16_twelve_atoms],
+                         ids=lambda f: f.__name__)
 def test_fused_step_variants_against_oracle(make):
     """The fused 16^3 step on two spins, on projector spheres whose tables do
-    not fit in shared memory (fallback to global tables) and without
-    projectors: J(t), the dipole and psi against the oracle's time loop."""
+    not fit in shared memory (fallback to global tables), without projectors
+    and with more atoms than warp pairs: J(t), the dipole and psi against the
+    oracle's time loop."""
     from salmon2_b200 import synth
     sysm = make()
     nt, dt = 6, 0.08

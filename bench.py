@@ -61,6 +61,9 @@ def parse():
     ap.add_argument("--self-consistent", action="store_true",
                     help="V_local = Vpsl + Vh[rho] + Vxc[rho] (PZ) recomputed after every Taylor step inside the "
                          "time loop (the fixed Gaussian potential stands in for Vpsl)")
+    ap.add_argument("--poisson", default="cg", choices=["cg", "ft"],
+                    help="isolated self-consistent workload: Hartree by CG with the multipole boundary "
+                         "(the reference's default) or by transforms on the doubled box")
     ap.add_argument("--small", action="store_true", help="8 k-points instead of 64 (quick check)")
     ap.add_argument("--workload", default="bulk", choices=["bulk", "supercell", "batch", "isolated"],
                     help="bulk: 16^3 x 64 k x 32 orbitals; supercell: its 2x2x2 supercell, 32^3 x 8 k x 256; "
@@ -111,6 +114,10 @@ def config_dict(args, s, nt, world):
                 f"peak 1e-3 au, {nt} Taylor-4 steps per bench step, J(t) every step")
     if getattr(args, "self_consistent", False):
         desc += ", self-consistent: density, Hartree and PZ-LDA potential every step"
+        if args.workload == "isolated":
+            desc += (" (Hartree by CG with the multipole boundary from the extrapolated potential, layout 3, "
+                     "threshold 1e-15)" if getattr(args, "poisson", "cg") == "cg"
+                     else " (Hartree by transforms on the doubled box)")
     return {
         "workload": desc,
         "grid": list(s.grid.shape), "k_points": s.nk, "orbitals_per_k": s.no, "atoms": s.pp.natom,
@@ -305,13 +312,20 @@ def cpu_baseline(args, s, dt, Ac, zc, nsteps, min_seconds=10.0):
         brl = np.diag([2.0 * np.pi / (n * h) for n, h in zip(s.grid.shape, s.grid.hgs)])
         vpsl = np.array(s.V_local[..., 0])
         rho0 = O.density(s.psi)[..., 0]
-        v0 = OR.update_vlocal(vpsl, OR.poisson_ft(rho0, brl),
-                              OR.exc_cor_pz(rho0, s.grid.hvol)[0][..., None])[..., 0]
+        cg = None
+        if s.grid.periodic:
+            vh0 = OR.poisson_ft(rho0, brl)
+        elif args.poisson == "cg":
+            vh0, _ = O.poisson_isolated_cg(rho0)
+            cg = dict(vh0=vh0)
+        else:
+            vh0 = OR.poisson_isolated_ft(rho0, brl)
+        v0 = OR.update_vlocal(vpsl, vh0, OR.exc_cor_pz(rho0, s.grid.hvol)[0][..., None])[..., 0]
     el, runs = 0.0, 0
     while el < min_seconds or runs == 0:
         t0 = time.perf_counter()
         if scf:
-            O.rt_run_scf(s.psi, nsteps, dt, zc, vpsl, brl, v0, Ac_ext=Ac_s)
+            O.rt_run_scf(s.psi, nsteps, dt, zc, vpsl, brl, v0, Ac_ext=Ac_s, cg=cg)
         else:
             O.rt_run(s.psi, nsteps, dt, zc, Ac_ext=Ac_s)
         el += time.perf_counter() - t0
@@ -549,7 +563,11 @@ def main():
         # then the update every step
         brl = np.diag([2.0 * np.pi / (n * h) for n, h in zip(s.grid.shape, s.grid.hgs)])
         vpsl = torch.from_numpy(np.ascontiguousarray(s.V_local[..., 0].ravel(order="F"))).cuda(local)
-        ctx.update_potential(a, vpsl, brl)
+        if s.grid.periodic or args.poisson == "ft":
+            ctx.update_potential(a, vpsl, brl)
+        else:  # method_poisson = 'cg': CG from the extrapolated potential every step
+            ctx.update_potential(a, vpsl, brl, poisson="cg")
+            ctx.set_hartree_cg(ctx.last_vh)
         ctx.set_self_consistent(True, vpsl, brl)
 
     def barrier():

@@ -358,6 +358,22 @@ int sb200_hartree_isolated_cg(sb200_ctx* ctx, const double* rho, double* Vh, int
                               int lmax_multipole, const double* Rion, int natom, const int num_multipole_xyz[3],
                               double threshold_cg, int maxiter, int* iterations);
 
+/* Selects the CG Hartree solve (sb200_hartree_isolated_cg, same arguments) for
+ * the isolated self-consistent time loop (sb200_set_self_consistent) in place
+ * of the doubled-box transforms, the reference's default for isolated systems.
+ * Vh0(is:ie) is the potential of the initial density (the Vh of
+ * initialization_rt; host or device); it starts the first step's CG and both
+ * stored potentials of the extrapolation.  Every later step starts its CG from
+ * 2 Vh_stock1 - Vh_stock2 as the reference does.  The iterations run inside the
+ * loop's CUDA graph with the convergence test on the device.  Vh0 = NULL goes
+ * back to the transforms.  Periodic grids: SB200_ERR_UNSUPPORTED.
+ * Replaces: the Vh extrapolation and hartree call of time_evolution_step
+ * (src/rt/time_evolution_step.f90:184-198) with method_poisson = 'cg', and the
+ * Vh_stock set-up of src/rt/initialization_rt.f90:277-286.                     */
+int sb200_set_hartree_cg(sb200_ctx* ctx, const double* Vh0, int layout_multipole, int lmax_multipole,
+                         const double* Rion, int natom, const int num_multipole_xyz[3], double threshold_cg,
+                         int maxiter);
+
 /* V_local(is) = Vpsl + Vh + Vxc(is) written into the context's device copy of
  * V_local (FP64 and the FP32 copy of the mixed form); Vpsl, Vh (is:ie), Vxc
  * (is:ie, nspin).  Also serves as the first sb200_set_vlocal.

@@ -61,10 +61,11 @@ def lib():
                      "sbo_precond_real", "sbo_gscg_rwf", "sbo_gram_schmidt_real", "sbo_gram_schmidt_complex",
                      "sbo_subspace_diag_real", "sbo_inner_product_real", "sbo_exc_cor_pz", "sbo_poisson_coef",
                      "sbo_dft_table", "sbo_poisson_ft", "sbo_update_vlocal", "sbo_rt_run_scf",
-                     "sbo_poisson_isolated_ft", "sbo_impulse_kick", "sbo_poisson_isolated_cg", "sbo_ylm"):
+                     "sbo_poisson_isolated_ft", "sbo_impulse_kick", "sbo_poisson_isolated_cg", "sbo_ylm", "sbo_rt_run_scf_cg"):
             getattr(L, name)
         L.sbo_rt_run.restype = C.c_int
         L.sbo_rt_run_scf.restype = C.c_int
+        L.sbo_rt_run_scf_cg.restype = C.c_int
         L.sbo_get_threads.restype = C.c_int
         L.sbo_ylm.restype = C.c_double
         _lib = L
@@ -266,10 +267,13 @@ class Oracle:
         psi = a if which == 0 else b
         return dict(psi=psi, curr=curr, rbox=rbox, Ac_tot=Ac_tot, Ac_ind=Ac_ind, rho=rho)
 
-    def rt_run_scf(self, psi0, nt, dt, zc, vpsl, brl, v0, Ac_ext=None, trans_longi=0):
+    def rt_run_scf(self, psi0, nt, dt, zc, vpsl, brl, v0, Ac_ext=None, trans_longi=0, cg=None):
         """rt_run with the self-consistent potential update every step
         (time_evolution_step.f90:184-207; nspin = 1, periodic or isolated).  v0: V_local
-        (nx, ny, nz) for the first step.  The oracle's own V_local is untouched."""
+        (nx, ny, nz) for the first step.  The oracle's own V_local is untouched.
+        cg (isolated grids): dict(vh0=..., layout=3, lmax=4, rion=None,
+        npole_xyz=None, threshold=1e-15, maxiter=1000) selects the CG Hartree
+        solve with the Vh extrapolation; the result then has "Vh" and "cg_iters"."""
         a = self._orb(psi0).copy(order="F")
         b = np.zeros_like(a, order="F")
         work = np.zeros_like(a, order="F")
@@ -285,13 +289,30 @@ class Oracle:
         vp = _flat_f(vpsl)
         bb = np.ascontiguousarray(np.asarray(brl, dtype=np.float64).ravel(order="F"))
         vl = _flat_f(v0).copy()
-        which = lib().sbo_rt_run_scf(C.byref(self.s), _p(a), _p(b), _p(work), C.c_int(nt), C.c_double(dt),
-                                     _p(zc), C.c_int(len(zc)), _p(Ac_ext), _p(Ac_ind), _p(Ac_tot),
-                                     C.c_int(trans_longi), _p(curr), _p(rbox), _p(rho), _p(vp), _p(bb), _p(vl))
-        assert which in (0, 1), "rt_run_scf needs an nspin = 1 system"
+        extra = {}
+        if cg is None:
+            which = lib().sbo_rt_run_scf(C.byref(self.s), _p(a), _p(b), _p(work), C.c_int(nt), C.c_double(dt),
+                                         _p(zc), C.c_int(len(zc)), _p(Ac_ext), _p(Ac_ind), _p(Ac_tot),
+                                         C.c_int(trans_longi), _p(curr), _p(rbox), _p(rho), _p(vp), _p(bb), _p(vl))
+        else:
+            g = self.sys.grid
+            vh = _flat_f(cg["vh0"]).copy()
+            ri = np.asarray(self.sys.rion if cg.get("rion") is None else cg["rion"], dtype=np.float64)
+            rflat = np.ascontiguousarray(ri.reshape(3, -1, order="F").T)
+            npx = cg.get("npole_xyz")
+            npx = np.asarray(multipole_cells(g.num, g.hgs) if npx is None else npx, dtype=np.int32)
+            iters = np.zeros(nt, dtype=np.int32)
+            which = lib().sbo_rt_run_scf_cg(
+                C.byref(self.s), _p(a), _p(b), _p(work), C.c_int(nt), C.c_double(dt), _p(zc), C.c_int(len(zc)),
+                _p(Ac_ext), _p(Ac_ind), _p(Ac_tot), C.c_int(trans_longi), _p(curr), _p(rbox), _p(rho), _p(vp),
+                _p(vl), _p(vh), C.c_int(cg.get("layout", 3)), C.c_int(cg.get("lmax", 4)), _p(rflat),
+                C.c_int(rflat.shape[0]), npx.ctypes.data_as(_ip), C.c_double(cg.get("threshold", 1e-15)),
+                C.c_int(cg.get("maxiter", 1000)), iters.ctypes.data_as(_ip))
+            extra = dict(Vh=vh.reshape(g.shape, order="F"), cg_iters=iters)
+        assert which in (0, 1), "rt_run_scf needs an nspin = 1 system (cg: an isolated one)"
         psi = a if which == 0 else b
         return dict(psi=psi, curr=curr, rbox=rbox, Ac_tot=Ac_tot, rho=rho,
-                    V_local=vl.reshape(self.sys.grid.shape, order="F"))
+                    V_local=vl.reshape(self.sys.grid.shape, order="F"), **extra)
 
     # -- ground state (real orbitals, one k) --------------------------------
     def _real(self, psi):

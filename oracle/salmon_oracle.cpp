@@ -5,6 +5,7 @@
 // salmon_oracle.h for the parity status.
 #include "salmon_oracle.h"
 
+#include <algorithm>
 #include <cmath>
 #include <complex>
 #include <cstring>
@@ -659,10 +660,24 @@ void sbo_calc_Ac_ext_t(int shape, double t0, double delta_t, int is, int ie, con
 // Hartree and exchange-correlation potentials of rho(t+dt) and update_vlocal,
 // time_evolution_step.f90:184-207 with yn_fix_func = 'n' (nspin = 1; Hartree by
 // poisson_ft on periodic grids, poisson_isolated_ft on isolated ones).
+// method_poisson = 'cg' on isolated grids (time_evolution_step.f90:186-198):
+// vh carries the potential from step to step (the CG start), with the two
+// stored potentials of the extrapolation
+struct ScfCg {
+  int layout, lmax;
+  const double* rion;
+  int natom;
+  int npole[3];
+  double threshold;
+  int maxiter;
+  double* vh;     // in: Vh of the initial density; out: the last step's
+  int* iters;     // [nt] iterations of each step's solve
+};
 struct ScfUpdate {
   const double* vpsl;
   const double* brl;
   double* vloc;  // the buffer s->V_local points to
+  const ScfCg* cg = nullptr;
 };
 
 static int rt_run_impl(sbo_system* s, double* psi_a, double* psi_b, double* work, int nt, double dt,
@@ -670,7 +685,13 @@ static int rt_run_impl(sbo_system* s, double* psi_a, double* psi_b, double* work
                        int trans_longi, double* curr, double* rbox, double* rho_work, const ScfUpdate* scf) {
   const double pi = 3.141592653589793238462643383279502884;
   const long npts = (long)(s->ie[0] - s->is[0] + 1) * (s->ie[1] - s->is[1] + 1) * (s->ie[2] - s->is[2] + 1);
-  std::vector<double> vh(scf ? npts : 0), vxc(scf ? npts : 0);
+  std::vector<double> vh(scf ? npts : 0), vxc(scf ? npts : 0), stock1, stock2;
+  const ScfCg* cg = (scf && !s->periodic) ? scf->cg : nullptr;
+  if (cg) {  // initialization_rt.f90:277-286
+    vh.assign(cg->vh, cg->vh + npts);
+    stock1 = vh;
+    stock2 = vh;
+  }
   double* in = psi_a;
   double* out = psi_b;
   int which = 1;
@@ -685,10 +706,22 @@ static int rt_run_impl(sbo_system* s, double* psi_a, double* psi_b, double* work
     if (scf) {
       const int num[3] = {s->ie[0] - s->is[0] + 1, s->ie[1] - s->is[1] + 1, s->ie[2] - s->is[2] + 1};
       double exc = 0.0;
-      if (s->periodic)
+      if (s->periodic) {
         sbo_poisson_ft(num, scf->brl, rho_work, vh.data());
-      else
+      } else if (cg) {
+        if (itt != 1)
+          for (long i = 0; i < npts; ++i) {
+            vh[i] = 2.0 * stock1[i] - stock2[i];
+            stock2[i] = stock1[i];
+          }
+        int it = 0;
+        sbo_poisson_isolated_cg(s, rho_work, vh.data(), cg->layout, cg->lmax, cg->rion, cg->natom, cg->npole,
+                                cg->threshold, cg->maxiter, &it);
+        if (cg->iters) cg->iters[itt - 1] = it;
+        if (itt != 1) stock1 = vh;
+      } else {
         sbo_poisson_isolated_ft(num, scf->brl, rho_work, vh.data());
+      }
       sbo_exc_cor_pz(npts, rho_work, s->hvol, vxc.data(), &exc);
       sbo_update_vlocal(npts, 1, scf->vpsl, vh.data(), vxc.data(), scf->vloc);
     }
@@ -715,6 +748,7 @@ static int rt_run_impl(sbo_system* s, double* psi_a, double* psi_b, double* work
     out = t;
     which = 1 - which;
   }
+  if (cg) std::copy(vh.begin(), vh.end(), cg->vh);
   // after the last swap "in" holds the newest orbitals
   return (in == psi_a) ? 0 : 1;
 }
@@ -732,6 +766,22 @@ int sbo_rt_run_scf(sbo_system* s, double* psi_a, double* psi_b, double* work, in
                    const double* vpsl, const double brl[9], double* vloc) {
   if (s->nspin != 1) return -1;
   const ScfUpdate u{vpsl, brl, vloc};
+  const double* saved = s->V_local;
+  s->V_local = vloc;
+  const int r = rt_run_impl(s, psi_a, psi_b, work, nt, dt, zc, n_hamil, Ac_ext, Ac_ind, Ac_tot, trans_longi, curr,
+                            rbox, rho_work, &u);
+  s->V_local = saved;
+  return r;
+}
+
+int sbo_rt_run_scf_cg(sbo_system* s, double* psi_a, double* psi_b, double* work, int nt, double dt,
+                      const double* zc, int n_hamil, const double* Ac_ext, double* Ac_ind, double* Ac_tot,
+                      int trans_longi, double* curr, double* rbox, double* rho_work, const double* vpsl,
+                      double* vloc, double* vh, int layout, int lmax, const double* rion, int natom,
+                      const int npole_xyz[3], double threshold, int maxiter, int* iters) {
+  if (s->nspin != 1 || s->periodic) return -1;
+  ScfCg cg{layout, lmax, rion, natom, {npole_xyz[0], npole_xyz[1], npole_xyz[2]}, threshold, maxiter, vh, iters};
+  ScfUpdate u{vpsl, nullptr, vloc, &cg};
   const double* saved = s->V_local;
   s->V_local = vloc;
   const int r = rt_run_impl(s, psi_a, psi_b, work, nt, dt, zc, n_hamil, Ac_ext, Ac_ind, Ac_tot, trans_longi, curr,

@@ -173,6 +173,16 @@ void sbo_update_vlocal(long n, int nspin, const double* vpsl, const double* vh, 
 void sbo_poisson_isolated_cg(const sbo_system* s, const double* rho, double* vh, int layout, int lmax,
                              const double* rion, int natom, const int npole_xyz[3], double threshold,
                              int maxiter, int* iterations);
+/* sbo_rt_run_scf on an isolated grid with the Hartree potential by
+ * poisson_isolated_cg (method_poisson = 'cg') and the Vh extrapolation of
+ * time_evolution_step.f90:186-198: vh holds the potential of the initial density
+ * on entry (initialization_rt.f90:277-286) and the last step's on exit;
+ * iters[nt] the iterations of each solve.  Returns -1 for nspin 2 or periodic. */
+int sbo_rt_run_scf_cg(sbo_system* s, double* psi_a, double* psi_b, double* work, int nt, double dt,
+                      const double* zc, int n_hamil, const double* Ac_ext, double* Ac_ind, double* Ac_tot,
+                      int trans_longi, double* curr, double* rbox, double* rho_work, const double* vpsl,
+                      double* vloc, double* vh, int layout, int lmax, const double* rion, int natom,
+                      const int npole_xyz[3], double threshold, int maxiter, int* iters);
 /* Ylm (src/math/salmon_math.f90:386-426), lm = l^2 + l + m, l <= 4            */
 double sbo_ylm(double x, double y, double z, int lm);
 /* sbo_rt_run with the self-consistent potential update every step (nspin = 1;

@@ -275,6 +275,13 @@ void pcg_free(sb200_ctx* c);
 int hartree_isolated_cg(sb200_ctx* c, const double* rho, double* vh, int layout, int lmax, const double* rion,
                         int natom, const int npole_xyz[3], double threshold, int maxiter, int* iterations);
 void pcg_default_cells(const sb200_ctx* c, int out[3]);
+// the same solve in pieces for the self-consistent loop: configure once, then
+// issue per step on device arrays (inside a stream capture the iterations
+// become a conditional WHILE node); the Vh extrapolation of isolated steps
+int pcg_configure(sb200_ctx* c, int layout, int lmax, const double* rion, int natom, const int npole_xyz[3],
+                  double threshold, int maxiter);
+int pcg_issue(sb200_ctx* c, const double* d_rho, double* d_vh, int* iterations);
+int pcg_vh_stock(sb200_ctx* c, const int* d_step, double* d_vh, double* d_s1, double* d_s2, bool before);
 // self-consistent time loop (sb200_scf.cu): buffers sized before a capture, and
 // the per-step potential update issued after each Taylor step (no-ops unless
 // sb200_set_self_consistent enabled it)

@@ -24,9 +24,12 @@
 // last block of each launch to finish sums the per-block partials in block
 // order (fixed order: the result does not depend on timing) and writes the
 // scalars for the next launch; the convergence test sets a device flag after
-// which every later launch returns at once.  The host checks the flag every
-// PCG_CHUNK iterations.  zk and the two pk buffers are padded by the 4-point
-// halo, which stays zero, so the stencil needs no bounds tests.
+// which every later launch returns at once.  Called directly, the host checks
+// the flag every PCG_CHUNK iterations; inside a CUDA graph capture (the
+// self-consistent time loop) the iterations are the body of a conditional
+// WHILE node whose condition the convergence test clears, so the loop runs
+// without the host.  zk and the two pk buffers are padded by the 4-point halo,
+// which stays zero, so the stencil needs no bounds tests.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -44,16 +47,12 @@ constexpr int MCH = 2048;      // points per block of the pole sums
 constexpr int NLM_MAX = 25;    // lmax <= 4
 constexpr int POLE_W = 32;     // doubles per pole entry: centre (3), itrho, rholm (25)
 constexpr int PCG_CHUNK = 16;  // iterations between host checks of the convergence flag
+constexpr int PCG_UNROLL = 2;  // iterations per body of the conditional node
 constexpr double PCG_PI = 3.141592653589793;
 
 // scalars of the iteration (device)
-enum { SC_SUM1 = 0, SC_AK, SC_CK, SC_DONE, SC_ITER, SC_COUNT };
-
-struct PcgState {
-  size_t cap = 0;       // bytes of the arena
-  void* arena = nullptr;
-  double* host_sc = nullptr;  // pinned: the scalars read back by the host
-};
+// (SC_NEXT: the iteration the next launch pair performs)
+enum { SC_SUM1 = 0, SC_AK, SC_CK, SC_DONE, SC_ITER, SC_NEXT, SC_COUNT };
 
 struct PArgs {
   int nx, ny, nz;
@@ -69,6 +68,8 @@ struct PArgs {
   double* zk;           // padded
   double* pk[2];        // padded, alternating per iteration
   double* rlap;         // interior
+  double* rho_stage;    // interior: host inputs of the direct call
+  double* vh_stage;
   double* part;         // per-block partial sums
   unsigned int* counter;
   double* sc;           // SC_COUNT scalars
@@ -387,16 +388,19 @@ __global__ void __launch_bounds__(PT) k_pcg_first(PArgs a) {
       a.sc[SC_CK] = 0.0;
       a.sc[SC_DONE] = 0.0;
       a.sc[SC_ITER] = 0.0;
+      a.sc[SC_NEXT] = 1.0;
       *a.counter = 0u;
     }
   }
 }
 
-// (A) of iteration it: pk = zk + ck pk_old (pk = zk at it = 1), lap pk, zk.lap pk
-__global__ void __launch_bounds__(PT) k_pcg_direction(PArgs a, int it) {
+// (A) of the iteration it = SC_NEXT: pk = zk + ck pk_old (pk = zk at it = 1),
+// lap pk, zk.lap pk
+__global__ void __launch_bounds__(PT) k_pcg_direction(PArgs a) {
   __shared__ double red[PT / 32 + 1];
   __shared__ bool last;
   if (a.sc[SC_DONE] != 0.0) return;
+  const int it = (int)a.sc[SC_NEXT];
   const double ck = a.sc[SC_CK];
   const double* zk = a.zk;
   const double* po = a.pk[(it + 1) & 1];
@@ -422,11 +426,14 @@ __global__ void __launch_bounds__(PT) k_pcg_direction(PArgs a, int it) {
   }
 }
 
-// (B) of iteration it: Vh += ak pk, zk -= ak lap pk, convergence test, ck
-__global__ void __launch_bounds__(PT) k_pcg_update(PArgs a, int it) {
+// (B) of the iteration it = SC_NEXT: Vh += ak pk, zk -= ak lap pk, convergence
+// test, ck; with use_cond the test also clears the condition of the graph's
+// WHILE node
+__global__ void __launch_bounds__(PT) k_pcg_update(PArgs a, cudaGraphConditionalHandle cond, int use_cond) {
   __shared__ double red[PT / 32 + 1];
   __shared__ bool last;
   if (a.sc[SC_DONE] != 0.0) return;
+  const int it = (int)a.sc[SC_NEXT];
   const double ak = a.sc[SC_AK];
   const double* pk = a.pk[it & 1];
   double s = 0.0;
@@ -453,10 +460,38 @@ __global__ void __launch_bounds__(PT) k_pcg_update(PArgs a, int it) {
           a.sc[SC_ITER] = (double)(a.maxiter + 1);
         }
       }
+      a.sc[SC_NEXT] = (double)(it + 1);
+      if (use_cond && a.sc[SC_DONE] != 0.0) cudaGraphSetConditional(cond, 0u);
       *a.counter = 0u;
     }
   }
 }
+
+// Vh extrapolation of the isolated time step (time_evolution_step.f90:187-190,
+// 196-198): with the device step counter (itt + 1 after finalize) not 2,
+// Vh = 2 stock1 - stock2 and stock2 = stock1 before the solve (before = 1),
+// stock1 = Vh after it (before = 0)
+__global__ void k_vh_stock(const int* step, double* vh, double* s1, double* s2, long n, int before) {
+  if (*step == 2) return;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    if (before) {
+      const double a1 = s1[i];
+      vh[i] = 2.0 * a1 - s2[i];
+      s2[i] = a1;
+    } else {
+      s1[i] = vh[i];
+    }
+  }
+}
+
+struct PcgState {
+  size_t cap = 0;       // bytes of the arena
+  void* arena = nullptr;
+  double* host_sc = nullptr;  // pinned: the scalars read back by the host
+  PArgs base{};               // the configured solve (rho, vh set per call)
+  bool configured = false;
+  cudaStream_t side = nullptr;  // captures the body of the conditional node
+};
 
 PcgState* pcg_of(sb200_ctx* c) { return static_cast<PcgState*>(c->pcg); }
 
@@ -473,6 +508,7 @@ void pcg_free(sb200_ctx* c) {
   if (!s) return;
   if (s->arena) cudaFree(s->arena);
   if (s->host_sc) cudaFreeHost(s->host_sc);
+  if (s->side) cudaStreamDestroy(s->side);
   delete s;
   c->pcg = nullptr;
 }
@@ -494,8 +530,11 @@ bool pcg_is_device(const void* p) {
   return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
 }
 
-int hartree_isolated_cg(sb200_ctx* c, const double* rho, double* vh, int layout, int lmax, const double* rion,
-                        int natom, const int npole_xyz[3], double threshold, int maxiter, int* iterations) {
+// Sizes the work arrays for the context's grid and the given boundary, uploads
+// the pole tables and (layout 2) forms the nearest-atom map; the arrays whose
+// halos must stay zero are cleared here, once.
+int pcg_configure(sb200_ctx* c, int layout, int lmax, const double* rion, int natom, const int npole_xyz[3],
+                  double threshold, int maxiter) {
   if (layout < 1 || layout > 3) return set_error(SB200_ERR_INVALID_ARG, "layout_multipole must be 1, 2 or 3");
   if (lmax < 0 || lmax > 4) return set_error(SB200_ERR_UNSUPPORTED, "lmax_multipole must be 0..4");
   if (maxiter < 1) return set_error(SB200_ERR_INVALID_ARG, "maxiter must be at least 1");
@@ -584,7 +623,9 @@ int hartree_isolated_cg(sb200_ctx* c, const double* rho, double* vh, int layout,
     s = new PcgState();
     c->pcg = s;
     SB_CUDA(cudaMallocHost((void**)&s->host_sc, 8 * sizeof(double)));
+    SB_CUDA(cudaStreamCreateWithFlags(&s->side, cudaStreamNonBlocking));
   }
+  s->configured = false;
   if (s->cap < need) {
     if (s->arena) cudaFree(s->arena);
     s->arena = nullptr;
@@ -605,9 +646,9 @@ int hartree_isolated_cg(sb200_ctx* c, const double* rho, double* vh, int layout,
   p += b_pad;
   a.rlap = (double*)p;
   p += b_int;
-  double* rho_s = (double*)p;
+  a.rho_stage = (double*)p;
   p += b_int;
-  double* vh_s = (double*)p;
+  a.vh_stage = (double*)p;
   p += b_int;
   a.part = (double*)p;
   p += b_part;
@@ -626,60 +667,118 @@ int hartree_isolated_cg(sb200_ctx* c, const double* rho, double* vh, int layout,
   double* rion_d = (double*)p;
   a.rion = rion_d;
   cudaStream_t st = c->stream;
-  const bool rho_dev = pcg_is_device(rho), vh_dev = pcg_is_device(vh);
-  if (!rho_dev) SB_CUDA(cudaMemcpyAsync(rho_s, rho, a.N * sizeof(double), cudaMemcpyHostToDevice, st));
-  if (!vh_dev) SB_CUDA(cudaMemcpyAsync(vh_s, vh, a.N * sizeof(double), cudaMemcpyHostToDevice, st));
-  a.rho = rho_dev ? rho : rho_s;
-  a.vh = vh_dev ? vh : vh_s;
   // the padded arrays start at zero (their halos stay zero; vb's face halos are
-  // rewritten below), the block counter at zero
+  // rewritten by every solve), the block counter at zero
   SB_CUDA(cudaMemsetAsync(a.vb, 0, 4 * b_pad, st));
   SB_CUDA(cudaMemsetAsync(a.counter, 0, sizeof(unsigned int), st));
   SB_CUDA(cudaMemcpyAsync(a.pole, pole_h.data(), pole_h.size() * sizeof(double), cudaMemcpyHostToDevice, st));
   if (!cell_h.empty())
     SB_CUDA(cudaMemcpyAsync(cell_d, cell_h.data(), cell_h.size() * sizeof(int), cudaMemcpyHostToDevice, st));
-  if (layout == 2)
+  if (layout == 2) {
     SB_CUDA(cudaMemcpyAsync(rion_d, rion, (size_t)natom * 3 * sizeof(double), cudaMemcpyHostToDevice, st));
+    k_pcg_owner<<<grid_blocks(a.N), PT, 0, st>>>(a);
+    SB_LAUNCH_CHECK("k_pcg_owner");
+  }
+  SB_CUDA(cudaStreamSynchronize(st));  // the host tables above are temporaries
+  s->base = a;
+  s->configured = true;
+  return SB200_OK;
+}
+
+// One solve of the configured kind: Vh (device, start value in, solution out)
+// of rho (device).  Outside a stream capture the host checks convergence every
+// PCG_CHUNK iterations and *iterations gets poisson%iterVh; inside one the
+// iterations become a conditional WHILE node of the captured graph and
+// *iterations is left alone.
+int pcg_issue(sb200_ctx* c, const double* d_rho, double* d_vh, int* iterations) {
+  PcgState* s = pcg_of(c);
+  if (!s || !s->configured) return set_error(SB200_ERR_STATE, "the CG Hartree solve is not configured");
+  PArgs a = s->base;
+  a.rho = d_rho;
+  a.vh = d_vh;
+  cudaStream_t st = c->stream;
   const int gb = grid_blocks(a.N);
   const dim3 gpole(a.nchunk, a.npole);
   const int gred = (a.npole + 127) / 128;
-  if (layout == 2) {
-    k_pcg_owner<<<gb, PT, 0, st>>>(a);
-    SB_LAUNCH_CHECK("k_pcg_owner");
-  }
-  if (layout == 3) {
+  if (a.layout == 3) {
     k_pcg_pole_sum<0><<<gpole, PT, 0, st>>>(a);
-    SB_LAUNCH_CHECK("k_pcg_pole_sum");
     k_pcg_pole_reduce<0><<<gred, 128, 0, st>>>(a);
-    SB_LAUNCH_CHECK("k_pcg_pole_reduce");
   }
   k_pcg_pole_sum<1><<<gpole, PT, 0, st>>>(a);
-  SB_LAUNCH_CHECK("k_pcg_pole_sum");
   k_pcg_pole_reduce<1><<<gred, 128, 0, st>>>(a);
-  SB_LAUNCH_CHECK("k_pcg_pole_reduce");
-  const long nface = 2L * HALO * ((long)ny * nz + (long)nx * nz + (long)nx * ny);
+  const long nface = 2L * HALO * ((long)a.ny * a.nz + (long)a.nx * a.nz + (long)a.nx * a.ny);
   k_pcg_boundary<<<grid_blocks(nface), PT, 0, st>>>(a);
-  SB_LAUNCH_CHECK("k_pcg_boundary");
   k_pcg_fill<<<gb, PT, 0, st>>>(a);
-  SB_LAUNCH_CHECK("k_pcg_fill");
   k_pcg_first<<<gb, PT, 0, st>>>(a);
-  SB_LAUNCH_CHECK("k_pcg_first");
-  for (int it0 = 1; it0 <= maxiter; it0 += PCG_CHUNK) {
-    const int it1 = it0 + PCG_CHUNK - 1 < maxiter ? it0 + PCG_CHUNK - 1 : maxiter;
+  SB_LAUNCH_CHECK("k_pcg boundary / first residual");
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  cudaGraph_t g = nullptr;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t nd = 0;
+  SB_CUDA(cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &nd));
+  if (cs == cudaStreamCaptureStatusActive) {
+    cudaGraphConditionalHandle h;
+    SB_CUDA(cudaGraphConditionalHandleCreate(&h, g, 1u, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    SB_CUDA(cudaGraphAddNode(&node, g, deps, nd, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    SB_CUDA(cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies));
+    SB_CUDA(cudaStreamBeginCaptureToGraph(s->side, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+    for (int u = 0; u < PCG_UNROLL; ++u) {
+      k_pcg_direction<<<gb, PT, 0, s->side>>>(a);
+      k_pcg_update<<<gb, PT, 0, s->side>>>(a, h, 1);
+    }
+    const cudaError_t le = cudaGetLastError();
+    cudaGraph_t captured = nullptr;
+    const cudaError_t ee = cudaStreamEndCapture(s->side, &captured);
+    if (le != cudaSuccess) return cuda_error(le, "k_pcg_direction / k_pcg_update (graph body)");
+    if (ee != cudaSuccess) return cuda_error(ee, "cudaStreamEndCapture (graph body)");
+    return SB200_OK;
+  }
+  for (int it0 = 1; it0 <= a.maxiter; it0 += PCG_CHUNK) {
+    const int it1 = it0 + PCG_CHUNK - 1 < a.maxiter ? it0 + PCG_CHUNK - 1 : a.maxiter;
     for (int it = it0; it <= it1; ++it) {
-      k_pcg_direction<<<gb, PT, 0, st>>>(a, it);
-      k_pcg_update<<<gb, PT, 0, st>>>(a, it);
+      k_pcg_direction<<<gb, PT, 0, st>>>(a);
+      k_pcg_update<<<gb, PT, 0, st>>>(a, cudaGraphConditionalHandle{}, 0);
     }
     SB_LAUNCH_CHECK("k_pcg_direction / k_pcg_update");
     SB_CUDA(cudaMemcpyAsync(s->host_sc, a.sc, SC_COUNT * sizeof(double), cudaMemcpyDeviceToHost, st));
     SB_CUDA(cudaStreamSynchronize(st));
     if (s->host_sc[SC_DONE] != 0.0) break;
   }
+  if (iterations) *iterations = (int)s->host_sc[SC_ITER];
+  return SB200_OK;
+}
+
+int pcg_vh_stock(sb200_ctx* c, const int* d_step, double* d_vh, double* d_s1, double* d_s2, bool before) {
+  const long n = c->g.npts;
+  k_vh_stock<<<grid_blocks(n), PT, 0, c->stream>>>(d_step, d_vh, d_s1, d_s2, n, before ? 1 : 0);
+  SB_LAUNCH_CHECK("k_vh_stock");
+  return SB200_OK;
+}
+
+int hartree_isolated_cg(sb200_ctx* c, const double* rho, double* vh, int layout, int lmax, const double* rion,
+                        int natom, const int npole_xyz[3], double threshold, int maxiter, int* iterations) {
+  int r = pcg_configure(c, layout, lmax, rion, natom, npole_xyz, threshold, maxiter);
+  if (r != SB200_OK) return r;
+  PcgState* s = pcg_of(c);
+  const long n = s->base.N;
+  cudaStream_t st = c->stream;
+  const bool rho_dev = pcg_is_device(rho), vh_dev = pcg_is_device(vh);
+  if (!rho_dev) SB_CUDA(cudaMemcpyAsync(s->base.rho_stage, rho, n * sizeof(double), cudaMemcpyHostToDevice, st));
+  if (!vh_dev) SB_CUDA(cudaMemcpyAsync(s->base.vh_stage, vh, n * sizeof(double), cudaMemcpyHostToDevice, st));
+  double* d_vh = vh_dev ? vh : s->base.vh_stage;
+  r = pcg_issue(c, rho_dev ? rho : s->base.rho_stage, d_vh, iterations);
+  if (r != SB200_OK) return r;
   if (!vh_dev) {
-    SB_CUDA(cudaMemcpyAsync(vh, a.vh, a.N * sizeof(double), cudaMemcpyDeviceToHost, st));
+    SB_CUDA(cudaMemcpyAsync(vh, d_vh, n * sizeof(double), cudaMemcpyDeviceToHost, st));
     SB_CUDA(cudaStreamSynchronize(st));
   }
-  if (iterations) *iterations = (int)s->host_sc[SC_ITER];
   return SB200_OK;
 }
 

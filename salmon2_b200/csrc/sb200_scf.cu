@@ -95,6 +95,12 @@ struct ScfState {
   double2* d_itab = nullptr;  // tables of length 2nx, 2ny, 2nz
   bool have_icoef = false;
   double ibrl[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  // isolated grids, method_poisson = 'cg' (sb200_set_hartree_cg): d_vh carries
+  // Vh from step to step as the CG start value, with the two stored potentials
+  // of the extrapolation
+  bool cg_on = false;
+  double* d_stock1 = nullptr;
+  double* d_stock2 = nullptr;
 };
 
 ScfState* scf_of(sb200_ctx* c) { return static_cast<ScfState*>(c->scf); }
@@ -615,10 +621,17 @@ int scf_rt_issue(sb200_ctx* c, const double2* psi) {
   if (!s || !s->rt_on) return SB200_OK;
   TRY_S(launch_density(c, psi, s->d_rho, SB200_KIND_POTENTIAL));
   TRY_S(scf_density_allreduce(c, s->d_rho));
-  if (c->g.periodic)
+  if (c->g.periodic) {
     TRY_S(scf_launch_hartree(c, s->d_rho, s->d_vh, SB200_KIND_POTENTIAL));
-  else
+  } else if (s->cg_on) {  // time_evolution_step.f90:186-198 with method_poisson = 'cg'
+    TRY_S(scf_mark(c, SB200_KIND_POTENTIAL, true));
+    TRY_S(pcg_vh_stock(c, c->rt.d_step, s->d_vh, s->d_stock1, s->d_stock2, true));
+    TRY_S(pcg_issue(c, s->d_rho, s->d_vh, nullptr));
+    TRY_S(pcg_vh_stock(c, c->rt.d_step, s->d_vh, s->d_stock1, s->d_stock2, false));
+    TRY_S(scf_mark(c, SB200_KIND_POTENTIAL, false));
+  } else {
     TRY_S(scf_launch_hartree_isolated(c, s->d_rho, s->d_vh, SB200_KIND_POTENTIAL));
+  }
   TRY_S(scf_launch_xc(c, s->d_rho, s->d_vxc, SB200_KIND_POTENTIAL, false));
   TRY_S(scf_launch_update(c, s->d_vpsl, s->d_vh, s->d_vxc, SB200_KIND_POTENTIAL));
   SB_LAUNCH_CHECK("self-consistent potential update");
@@ -644,6 +657,8 @@ void scf_free(sb200_ctx* c) {
   dfree(s->d_ib);
   dfree(s->d_icoef);
   dfree(s->d_itab);
+  dfree(s->d_stock1);
+  dfree(s->d_stock2);
   delete s;
   c->scf = nullptr;
 }
@@ -809,6 +824,33 @@ int sb200_set_self_consistent(sb200_ctx* c, int enable, const double* Vpsl, cons
   SB_CUDA(cudaStreamSynchronize(c->stream));
   TRY_S(density_prepare(c));
   s->rt_on = true;
+  return SB200_OK;
+}
+
+int sb200_set_hartree_cg(sb200_ctx* c, const double* Vh0, int layout_multipole, int lmax_multipole,
+                         const double* Rion, int natom, const int num_multipole_xyz[3], double threshold_cg,
+                         int maxiter) {
+  TRY_S(scf_ready(c));
+  if (c->g.periodic) return set_error(SB200_ERR_UNSUPPORTED, "sb200_set_hartree_cg needs an isolated grid");
+  ScfDevGuard dg(c->device);
+  TRY_S(scf_ensure(c));
+  ScfState* s = scf_of(c);
+  if (!Vh0) {
+    s->cg_on = false;
+    return SB200_OK;
+  }
+  TRY_S(pcg_configure(c, layout_multipole, lmax_multipole, Rion, natom, num_multipole_xyz, threshold_cg, maxiter));
+  const size_t n = (size_t)s->npts;
+  if (!s->d_vh) TRY_S(dalloc(&s->d_vh, n));
+  if (!s->d_stock1) TRY_S(dalloc(&s->d_stock1, n));
+  if (!s->d_stock2) TRY_S(dalloc(&s->d_stock2, n));
+  // initialization_rt.f90:277-286 (no restart): Vh of the initial density, both
+  // stored potentials equal to it
+  SB_CUDA(cudaMemcpyAsync(s->d_vh, Vh0, n * sizeof(double), cudaMemcpyDefault, c->stream));
+  SB_CUDA(cudaMemcpyAsync(s->d_stock1, s->d_vh, n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+  SB_CUDA(cudaMemcpyAsync(s->d_stock2, s->d_vh, n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+  SB_CUDA(cudaStreamSynchronize(c->stream));
+  s->cg_on = true;
   return SB200_OK;
 }
 

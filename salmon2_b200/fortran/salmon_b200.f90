@@ -252,6 +252,17 @@ module salmon_b200
       integer(c_int), intent(out) :: iterations
     end function
 
+    integer(c_int) function sb200_set_hartree_cg(ctx, Vh0, layout_multipole, lmax_multipole, Rion, natom, &
+        num_multipole_xyz, threshold_cg, maxiter) bind(c, name="sb200_set_hartree_cg")
+      import
+      type(c_ptr), value :: ctx
+      real(c_double), intent(in) :: Vh0(*)
+      integer(c_int), value :: layout_multipole, lmax_multipole, natom, maxiter
+      real(c_double), intent(in) :: Rion(3, *)
+      integer(c_int), intent(in) :: num_multipole_xyz(3)
+      real(c_double), value :: threshold_cg
+    end function
+
     integer(c_int) function sb200_update_vlocal(ctx, Vpsl, Vh, Vxc) bind(c, name="sb200_update_vlocal")
       import
       type(c_ptr), value :: ctx

@@ -265,6 +265,21 @@ class Context:
                                               C.byref(it)))
         return v, it.value
 
+    def set_hartree_cg(self, vh0, layout=3, lmax=4, rion=None, npole_xyz=None, threshold=1e-15, maxiter=1000):
+        """method_poisson = 'cg' for the isolated self-consistent loop
+        (time_evolution_step.f90:184-198): vh0 (nx, ny, nz) the potential of the
+        initial density; later steps start from the extrapolated potential.
+        vh0 = None returns to the transforms."""
+        if vh0 is None:
+            check(lib().sb200_set_hartree_cg(self.h, None, 0, 0, None, 0, None, 0.0, 0))
+            return
+        p, keep = self._scalar_field(vh0)
+        ri = np.asarray(self.sys.rion if rion is None else rion, dtype=np.float64).reshape(3, -1, order="F")
+        rflat = np.ascontiguousarray(ri.T)
+        npx = (C.c_int * 3)(*([0, 0, 0] if npole_xyz is None else [int(n) for n in npole_xyz]))
+        check(lib().sb200_set_hartree_cg(self.h, p, int(layout), int(lmax), _ptr(rflat), rflat.shape[0], npx,
+                                         float(threshold), int(maxiter)))
+
     def update_vlocal(self, vpsl, vh, vxc):
         """update_vlocal (hamiltonian.f90:813-843): V_local = Vpsl + Vh + Vxc on the
         device.  vxc: (nx, ny, nz, nspin) or (nx, ny, nz) for nspin = 1."""
@@ -290,13 +305,15 @@ class Context:
         buf = (C.c_ubyte * 128).from_buffer_copy(unique_id) if unique_id is not None else None
         check(lib().sb200_set_density_comm(self.h, int(nranks), int(rank), buf))
 
-    def update_potential(self, psi, vpsl, primitive_b):
+    def update_potential(self, psi, vpsl, primitive_b, poisson="ft"):
         """The self-consistent part of one time step on the device
         (time_evolution_step.f90:160-207, nspin = 1; Hartree by poisson_ft on a
-        periodic grid, poisson_isolated_ft on an isolated one):
-        rho = calc_density(psi), Vh = hartree(rho), Vxc = exchange_correlation(rho),
-        V_local = Vpsl + Vh + Vxc.  vpsl: a device tensor (nx*ny*nz, x fastest)
-        or a numpy array.  Nothing is copied to the host; returns E_xc."""
+        periodic grid, poisson_isolated_ft on an isolated one, or with
+        poisson = "cg" poisson_isolated_cg from zero with the default multipole
+        boundary): rho = calc_density(psi), Vh = hartree(rho),
+        Vxc = exchange_correlation(rho), V_local = Vpsl + Vh + Vxc.  vpsl: a
+        device tensor (nx*ny*nz, x fastest) or a numpy array.  Nothing is copied
+        to the host; returns E_xc.  The potential stays in self.last_vh."""
         torch = self.torch
         if self.sys.nspin != 1:
             raise SB200Error(3, "update_potential: the PZ potential here is the nspin = 1 form")
@@ -306,8 +323,16 @@ class Context:
         rho, vh, vxc = self._pot_buf
         b = np.asfortranarray(primitive_b, dtype=np.float64)
         check(lib().sb200_calc_density(self.h, C.c_void_p(psi.data_ptr()), C.c_void_p(rho.data_ptr())))
-        hartree = lib().sb200_hartree_periodic if self.sys.grid.periodic else lib().sb200_hartree_isolated_ft
-        check(hartree(self.h, _ptr(b), C.c_void_p(rho.data_ptr()), C.c_void_p(vh.data_ptr())))
+        if poisson == "cg" and not self.sys.grid.periodic:
+            vh.zero_()
+            ri = np.ascontiguousarray(np.asarray(self.sys.rion, dtype=np.float64).reshape(3, -1, order="F").T)
+            it = C.c_int(0)
+            check(lib().sb200_hartree_isolated_cg(self.h, C.c_void_p(rho.data_ptr()), C.c_void_p(vh.data_ptr()), 3,
+                                                  4, _ptr(ri), ri.shape[0], None, 1e-15, 1000, C.byref(it)))
+        else:
+            hartree = lib().sb200_hartree_periodic if self.sys.grid.periodic else lib().sb200_hartree_isolated_ft
+            check(hartree(self.h, _ptr(b), C.c_void_p(rho.data_ptr()), C.c_void_p(vh.data_ptr())))
+        self.last_vh = vh
         e = C.c_double(0.0)
         check(lib().sb200_exc_cor_pz(self.h, C.c_void_p(rho.data_ptr()), C.c_void_p(vxc.data_ptr()), C.byref(e)))
         pa, keep = self._scalar_field(vpsl)

@@ -461,3 +461,42 @@ def test_hartree_isolated_cg_refuses_periodic_and_bad_layout():
         ctx.hartree_isolated_cg(np.zeros(s.grid.shape), layout=4)
     assert b"layout_multipole" in _lib.lib().sb200_last_error()
     ctx.close()
+
+
+@pytest.mark.parametrize("nt", [5, 6])
+def test_rt_propagate_self_consistent_isolated_cg(nt):
+    """The isolated self-consistent loop with method_poisson = 'cg' (the
+    reference's default): each step's Hartree potential by CG from the
+    extrapolated potential (time_evolution_step.f90:186-198), the iterations
+    inside the loop's CUDA graph as a conditional node (the odd last step of
+    nt = 5 runs outside the graph), against the oracle's loop: dipole every
+    step, final orbitals."""
+    import dataclasses as dc
+    from salmon2_b200 import synth
+    from salmon2_b200.rt import Context
+
+    s0 = S.isolated_small()
+    s = dc.replace(s0, psi=synth.impulse_kick(s0.grid, s0.psi, 1e-3))
+    dt = 0.05
+    zc = synth.taylor_zc(dt)
+    vpsl = np.array(s.V_local[..., 0])
+    O = _oracle(s)
+    rho0 = O.density(s.psi)[..., 0]
+    vh0, _ = O.poisson_isolated_cg(rho0)
+    v0 = OR.update_vlocal(vpsl, vh0, OR.exc_cor_pz(rho0, s.grid.hvol)[0][..., None])[..., 0]
+    ref = O.rt_run_scf(s.psi, nt, dt, zc, vpsl, None, v0, cg=dict(vh0=vh0))
+    assert max(ref["cg_iters"]) < 1000
+    ctx = Context(s)
+    a, b, w = ctx.upload(s.psi), ctx.zeros(), ctx.zeros()
+    ctx.update_vlocal(vpsl, vh0, OR.exc_cor_pz(rho0, s.grid.hvol)[0])
+    ctx.set_hartree_cg(vh0)
+    ctx.set_self_consistent(True, vpsl, _brl(s))
+    res = ctx.rt_propagate(a, b, w, nt, dt, zc)
+    d_ref = ref["rbox"][:3] - ref["rbox"][:3, :1]
+    d_got = res["rbox"][:3] - res["rbox"][:3, :1]
+    print(f"CG loop nt={nt}: iterations {list(ref['cg_iters'])}, dipole response err "
+          f"{np.max(np.abs(d_got - d_ref)) / np.max(np.abs(d_ref)):.3e}")
+    assert np.max(np.abs(d_got - d_ref)) <= TOL_LOOP * np.max(np.abs(ref["rbox"][:3]))
+    assert np.max(np.abs(d_got - d_ref)) <= 1e-8 * np.max(np.abs(d_ref))
+    assert S.rel_err(ctx.download(res["psi"]), ref["psi"]) < TOL_LOOP
+    ctx.close()

@@ -220,3 +220,46 @@ def test_poisson_isolated_cg_gaussian_charge():
     assert np.max(np.abs(v - exact)) < 5e-5 * np.max(exact)
     _, it = orc.poisson_isolated_cg(rho, threshold=0.0, maxiter=5)
     assert it == 6
+
+
+def test_rt_run_scf_cg_equals_the_loop_written_out():
+    """The isolated self-consistent loop with method_poisson = 'cg' against the
+    loop spelled out call by call: Taylor step, density, the Vh extrapolation of
+    time_evolution_step.f90:186-198 (none at the first step; 2 Vh_stock1 -
+    Vh_stock2 after it, Vh_stock1 kept at the initial Vh through step 2), the
+    CG solve from that start, PZ-LDA and update_vlocal."""
+    import dataclasses
+
+    import _systems as S
+    from salmon2_b200 import synth
+
+    s = S.isolated_small()
+    s = dataclasses.replace(s, V_local=np.array(s.V_local, order="F"))
+    g = s.grid
+    vpsl = np.array(s.V_local[..., 0])
+    zc = synth.taylor_zc(0.05)
+    nt = 4
+    orc = O.Oracle(s, threads=2)
+    rho0 = orc.density(s.psi)[..., 0]
+    vh0, _ = orc.poisson_isolated_cg(rho0)
+    v0 = O.update_vlocal(vpsl, vh0, O.exc_cor_pz(rho0, g.hvol)[0][..., None])[..., 0]
+    ref = orc.rt_run_scf(s.psi, nt, 0.05, zc, vpsl, None, v0, cg=dict(vh0=vh0))
+    step = O.Oracle(dataclasses.replace(s, V_local=np.array(s.V_local, order="F")), threads=2)
+    step.V[..., 0] = v0
+    psi, vh, s1, s2 = s.psi, vh0.copy(), vh0.copy(), vh0.copy()
+    iters = []
+    for itt in range(1, nt + 1):
+        psi = step.taylor(psi, zc)
+        rho = step.density(psi)[..., 0]
+        if itt != 1:
+            vh = 2 * s1 - s2
+            s2 = s1.copy()
+        vh, it = step.poisson_isolated_cg(rho, vh0=vh)
+        iters.append(it)
+        if itt != 1:
+            s1 = vh.copy()
+        step.V[...] = O.update_vlocal(vpsl, vh, O.exc_cor_pz(rho, g.hvol)[0][..., None])
+    assert list(ref["cg_iters"]) == iters and max(iters) < 1000
+    assert np.max(np.abs(ref["psi"] - psi)) <= 1e-13 * np.max(np.abs(psi))
+    assert np.max(np.abs(ref["Vh"] - vh)) <= 1e-13 * np.max(np.abs(vh))
+    assert np.max(np.abs(ref["V_local"] - step.V[..., 0])) <= 1e-13 * np.max(np.abs(step.V))

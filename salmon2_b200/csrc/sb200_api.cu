@@ -330,6 +330,7 @@ int sb200_ctx_create(int device, sb200_ctx** out) {
   if (const char* v = getenv("SB200_PROJECT")) c->project_variant = (v[0] == 'w') ? 0 : (v[0] == 'd') ? 2 : 1;
   if (const char* v = getenv("SB200_BLK_DEPTH")) c->blk_depth = (v[0] == '4') ? 4 : 2;
   if (const char* v = getenv("SB200_BLK_SPLIT")) c->blk_split = (v[0] == '0') ? 0 : 1;
+  if (const char* v = getenv("SB200_BLK_PREFETCH")) c->blk_prefetch = (v[0] == '0') ? 0 : 1;
   if (const char* v = getenv("SB200_TMA")) c->tma_variant = (v[0] == 'o' && v[1] == 'f') ? 0 : 1;
   int r = dalloc(&c->d_result, 24);  // results [0, 8), staged A [8, 11), shard sums [16, 23)
   if (r == SB200_OK) r = dalloc(&c->rt.d_step, 1);

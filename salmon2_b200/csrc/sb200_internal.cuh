@@ -159,6 +159,7 @@ struct sb200_ctx {
   int blk_depth = 2;           // z depth of the register block of the blocked fused step (2: 512 threads, 4: 256)
   int blk_split = 1;           // blocked fused step: KB projections by two warps per atom, overlapped with the
                                // stencil (1), or one warp per atom between the terms (0)
+  int blk_prefetch = 1;        // blocked fused step: each CTA prefetches the orbital one wave ahead into L2
   int tma_variant = 1;         // tiled hpsi fed by tensor copies where it applies (0: register-prefetch sweep)
   // optional per-kernel-class device timing (sb200_set_timing)
   bool timing = false;

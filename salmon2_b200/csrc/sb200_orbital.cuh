@@ -54,6 +54,7 @@ struct BlkArgs {
   const int* sap;      // [tpad] (pair index << 12) | shared-memory grid index
   int* err;            // device error flag (a bounded wait expired)
   int kbcache;         // 1: each atom's uV and phases kept in TMEM by its warp
+  int prefetch_ahead;  // CTA o prefetches the orbital of CTA o + prefetch_ahead into L2 (0: none)
 };
 
 // The register-blocked fused step; SB200_ERR_UNSUPPORTED (no error recorded)

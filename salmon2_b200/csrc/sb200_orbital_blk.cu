@@ -390,6 +390,9 @@ __global__ void __launch_bounds__(Blk<BZ>::BT, 1) k_step_blk(const double2* __re
   const double* kc = a.kcoef + (long)KC * ik;
 
   if (warp == 0) tmem::alloc(&s_tmem, TMEM_COLS);
+  // the orbital of the CTA one wave of resident CTAs later, into L2
+  if (t == 64 && bk.prefetch_ahead > 0 && o + bk.prefetch_ahead < (int)gridDim.x)
+    tma::bulk_prefetch_l2(in + (long)(o + bk.prefetch_ahead) * a.npts, (unsigned)(a.npts * sizeof(double2)));
   if (t < 12) kn[t] = __ldg(kc + 4 + t);  // k_nabt(s, d) = kAc_d nab(s, d)
   if (kb && t == 32) {
     // the k-point's KB tables: bulk copies (no multicast) into shared memory,
@@ -944,6 +947,11 @@ int launch_step_blk(sb200_ctx* c, const double2* in, double2* out, const OrbArgs
                                            : (c->pp.natom <= nw && nk <= chunks)))
                      ? 1
                      : 0;
+  }
+  {  // one wave of resident CTAs (one per SM) ahead, unless switched off
+    int nsm = 0;
+    SB_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device));
+    bk.prefetch_ahead = c->blk_prefetch ? nsm : 0;
   }
   dim3 grid(c->orb.norb);
 #define SB_BLK_LAUNCH(BZ, OBS, SPLIT) \

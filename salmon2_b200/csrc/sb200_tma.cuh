@@ -61,6 +61,11 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
 
 // 1-D bulk copy global -> shared (both 16-byte aligned, bytes % 16 == 0),
 // completion counted on the barrier.
+// bytes (a multiple of 16, 16-byte aligned) of global memory into L2, no completion tracking
+__device__ __forceinline__ void bulk_prefetch_l2(const void* src, unsigned bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
+}
+
 __device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
   asm volatile(
       "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(saddr(dst)),

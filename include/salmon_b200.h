@@ -122,6 +122,22 @@ int sb200_set_pp(sb200_ctx* ctx, int natom, int nps, int nlma, const int* mps, c
  * src/common/hamiltonian.f90:847-903).  Isolated grids ignore it.              */
 int sb200_set_vec_Ac(sb200_ctx* ctx, const double vec_Ac[3]);
 
+/* Non-orthogonal periodic cell: rmatrix_B(3,3) (system%rmatrix_B, the
+ * inverse of the unit lattice vectors [u v w]) and coef_F(6) (stencil%coef_F:
+ * F = B B^T, (f_uu, f_vv, f_ww, f_vw, f_uw, f_uv)) of init_lattice; the grid of
+ * sb200_set_grid then runs along the lattice vectors and its coef_lap0 is the
+ * F-weighted one.  hpsi and everything built on it (taylor, rt_propagate) take
+ * the non-orthogonal stencil: lattice-axis Laplacian and B (k+A) gradient,
+ * then the mixed second derivatives from the stored first derivatives; the
+ * current's gradient sums are taken to Cartesian components by B^T.  Periodic
+ * grids, FP64 only (no mixed form, no ttpsi).  NULL arguments return to the
+ * orthogonal stencil.
+ * Replaces: hpsi's non-orthogonal branch (src/common/hamiltonian.f90:306-357)
+ * -> zstencil_nonorthogonal (src/common/stencil.f90:120-214); the B^T of
+ * calc_current (src/common/density_matrix.f90:313,413); the tables of
+ * init_lattice (src/common/lattice.f90:23-75).                                */
+int sb200_set_lattice(sb200_ctx* ctx, const double rmatrix_B[9], const double coef_F[6]);
+
 /* Impulse kick of the initial orbitals: psi <- exp(i e_impulse epdir.r) psi
  * at every interior point of every orbital of the resident block psi (device
  * pointer), r the grid coordinate lg%coordinate of set_gridcoordinate.

@@ -35,6 +35,7 @@ class SboSystem(C.Structure):
         ("mps", _ip), ("jxyz", _ip), ("rxyz", _dp), ("uv", _dp), ("ia_tbl", _ip), ("rinv_uvu", _dp),
         ("zekr", _dp),
         ("stencil_rgrid_mode", C.c_int),
+        ("nonorth", C.c_int), ("rmatrix_B", C.c_double * 9), ("coef_F", C.c_double * 6),
     ]
 
 
@@ -105,8 +106,16 @@ class Oracle:
         self.wtk = np.ascontiguousarray(system.wtk, dtype=np.float64)
         self.V = np.asfortranarray(system.V_local, dtype=np.float64)
         s.vec_k, s.rocc, s.wtk, s.V_local = _p(self.vec_k), _p(self.rocc), _p(self.wtk), _p(self.V)
+        lat = getattr(system, "lattice", None)
+        rB = np.eye(3) if lat is None else np.asarray(lat.rmatrix_B, dtype=np.float64)
+        bt = rB.T
         for i in range(9):
-            s.BT[i] = 1.0 if i in (0, 4, 8) else 0.0
+            s.BT[i] = float(bt.ravel(order="F")[i])
+            s.rmatrix_B[i] = float(rB.ravel(order="F")[i])
+        if lat is not None:
+            s.nonorth = 1
+            for i in range(6):
+                s.coef_F[i] = float(lat.coef_F[i])
         s.natom, s.nps, s.nlma = pp.natom, pp.nps, pp.nlma
         self.mps = np.ascontiguousarray(pp.mps, dtype=np.int32)
         self.jxyz = np.asfortranarray(pp.jxyz, dtype=np.int32)

@@ -114,6 +114,66 @@ void zstencil_one(const sbo_system* s, const Idx& I, const double* tpsi, double*
       }
 }
 
+// One orbital of the non-orthogonal-lattice stencil, zstencil_nonorthogonal
+// (stencil.f90:120-214): lattice-axis Laplacian sums v(d) and first
+// derivatives w(d) (coef_nab, not k-weighted), htpsi = (V + lap0) psi
+// - 1/2 sum F(d) v(d) - i sum Bk(d) w(d); then the mixed terms
+// - 1/2 (F(4) d_z(w_y) + F(5) d_z(w_x) + F(6) d_y(w_x)) from the stored
+// first derivatives (the reference's wrk array, read through the index maps).
+void zstencil_nonorth_one(const sbo_system* s, const Idx& I, const double* tpsi, double* htpsi,
+                          const double* V, double lap0, const double* Bk) {
+  const double* lapt = s->coef_lap;
+  const double* nab = s->coef_nab;
+  const double* F = s->coef_F;
+  std::vector<zc_t> wrk1(I.vol), wrk2(I.vol);
+  auto T = [&](int x, int y, int z) { return ld(tpsi, I.a(x, y, z)); };
+  for (int iz = s->is[2]; iz <= s->ie[2]; ++iz)
+    for (int iy = s->is[1]; iy <= s->ie[1]; ++iy)
+      for (int ix = s->is[0]; ix <= s->ie[0]; ++ix) {
+        zc_t v[3], w[3];
+        for (int d = 0; d < 3; ++d) {
+          zc_t vv(0.0, 0.0), ww(0.0, 0.0);
+          for (int k = 1; k <= 4; ++k) {
+            zc_t tp, tm;
+            if (d == 0) {
+              tp = T(I.X(ix + k), iy, iz);
+              tm = T(I.X(ix - k), iy, iz);
+            } else if (d == 1) {
+              tp = T(ix, I.Y(iy + k), iz);
+              tm = T(ix, I.Y(iy - k), iz);
+            } else {
+              tp = T(ix, iy, I.Z(iz + k));
+              tm = T(ix, iy, I.Z(iz - k));
+            }
+            vv = vv + rmul(lapt[4 * d + k - 1], tp + tm);
+            ww = ww + rmul(nab[4 * d + k - 1], tp - tm);
+          }
+          v[d] = vv;
+          w[d] = ww;
+        }
+        const zc_t c = T(ix, iy, iz);
+        const zc_t fv = rmul(F[0], v[0]) + rmul(F[1], v[1]) + rmul(F[2], v[2]);
+        const zc_t bw = rmul(Bk[0], w[0]) + rmul(Bk[1], w[1]) + rmul(Bk[2], w[2]);
+        // (V + lap0) psi - 0.5 (F.v) - zI (Bk.w)
+        const zc_t h = rmul(V[I.r(ix, iy, iz)] + lap0, c) - rmul(0.5, fv) - zc_t(-bw.imag(), bw.real());
+        st(htpsi, I.a(ix, iy, iz), h);
+        wrk1[I.a(ix, iy, iz)] = w[0];
+        wrk2[I.a(ix, iy, iz)] = w[1];
+      }
+  for (int iz = s->is[2]; iz <= s->ie[2]; ++iz)
+    for (int iy = s->is[1]; iy <= s->ie[1]; ++iy)
+      for (int ix = s->is[0]; ix <= s->ie[0]; ++ix) {
+        zc_t w1(0.0, 0.0), w2(0.0, 0.0), w3(0.0, 0.0);
+        for (int k = 1; k <= 4; ++k) {
+          w1 = w1 + rmul(nab[8 + k - 1], wrk2[I.a(ix, iy, I.Z(iz + k))] - wrk2[I.a(ix, iy, I.Z(iz - k))]);  // yz
+          w2 = w2 + rmul(nab[8 + k - 1], wrk1[I.a(ix, iy, I.Z(iz + k))] - wrk1[I.a(ix, iy, I.Z(iz - k))]);  // zx
+          w3 = w3 + rmul(nab[4 + k - 1], wrk1[I.a(ix, I.Y(iy + k), iz)] - wrk1[I.a(ix, I.Y(iy - k), iz)]);  // xy
+        }
+        const zc_t h = ld(htpsi, I.a(ix, iy, iz)) - rmul(0.5, rmul(F[3], w1) + rmul(F[4], w2) + rmul(F[5], w3));
+        st(htpsi, I.a(ix, iy, iz), h);
+      }
+}
+
 // One orbital of the real 25-point stencil.  stencil.f90:30-80.
 void dstencil_one(const sbo_system* s, const Idx& I, const double* tpsi, double* htpsi,
                   const double* V, double lap0, const double* lapt, bool omp_grid) {
@@ -307,11 +367,30 @@ void sbo_dpseudo(const sbo_system* s, const double* tpsi, double* htpsi) {
   }
 }
 
-// hpsi, complex, orthogonal lattice: hamiltonian.f90:139-235 then zpseudo :424-435.
+// hpsi, complex, orthogonal lattice: hamiltonian.f90:139-235 then zpseudo :424-435;
+// non-orthogonal lattice: hamiltonian.f90:306-357 (kAc Cartesian, k_lap0 =
+// coef_lap0 + |kAc|^2 / 2, Bk = rmatrix_B kAc) then zpseudo.
 void sbo_hpsi(const sbo_system* s, const double* tpsi, double* htpsi) {
   Idx I(s);
   const bool grid_mode = s->stencil_rgrid_mode != 0;
   const long nxy = I.nx * I.ny * I.nz;
+  if (s->nonorth) {
+#pragma omp parallel for collapse(3)
+    for (int ik = 1; ik <= s->nk; ++ik)
+      for (int io = 1; io <= s->no; ++io)
+        for (int is = 1; is <= s->nspin; ++is) {
+          double kAc[3], Bk[3];
+          for (int d = 0; d < 3; ++d) kAc[d] = s->vec_k[3 * (ik - 1) + d] + s->vec_Ac[d];
+          const double k_lap0 = s->coef_lap0 + 0.5 * (kAc[0] * kAc[0] + kAc[1] * kAc[1] + kAc[2] * kAc[2]);
+          for (int d = 0; d < 3; ++d)
+            Bk[d] = s->rmatrix_B[d] * kAc[0] + s->rmatrix_B[d + 3] * kAc[1] + s->rmatrix_B[d + 6] * kAc[2];
+          const long o = I.orb(is, io, ik);
+          zstencil_nonorth_one(s, I, tpsi + 2 * I.vol * o, htpsi + 2 * I.vol * o, s->V_local + nxy * (is - 1),
+                               k_lap0, Bk);
+        }
+    if (s->nlma > 0) sbo_zpseudo(s, tpsi, htpsi);
+    return;
+  }
   if (grid_mode) {
     for (int ik = 1; ik <= s->nk; ++ik) {
       double kAc[3], k_lap0, k_nabt[12];

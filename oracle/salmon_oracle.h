@@ -69,6 +69,11 @@ typedef struct {
   double *zekr;             /* (nps,nlma,nk) complex; written by update_kvector */
   /* OpenMP mode: 1 = grid-parallel stencil (>=32^3), 0 = orbital-parallel   */
   int stencil_rgrid_mode;
+  /* non-orthogonal lattice (stencil%if_orthogonal = .false.): system%rmatrix_B
+   * and stencil%coef_F of init_lattice (lattice.f90:23-75)                    */
+  int nonorth;
+  double rmatrix_B[9];      /* (3,3) column-major                            */
+  double coef_F[6];
 } sbo_system;
 
 void sbo_set_threads(int n);

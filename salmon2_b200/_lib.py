@@ -65,6 +65,7 @@ SIGNATURES = {
     "sb200_hartree_isolated_ft": (C.c_int, [_vp, _dp, _vp, _vp]),
     "sb200_hartree_isolated_cg": (C.c_int, [_vp, _vp, _vp, C.c_int, C.c_int, _dp, C.c_int, _ip, C.c_double,
                                             C.c_int, _ip]),
+    "sb200_set_lattice": (C.c_int, [_vp, _dp, _dp]),
     "sb200_set_hartree_cg": (C.c_int, [_vp, _vp, C.c_int, C.c_int, _dp, C.c_int, _ip, C.c_double, C.c_int]),
     "sb200_set_self_consistent": (C.c_int, [_vp, C.c_int, _vp, _dp]),
     "sb200_nccl_unique_id": (C.c_int, [_vp]),

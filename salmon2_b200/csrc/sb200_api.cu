@@ -381,6 +381,7 @@ int sb200_ctx_destroy(sb200_ctx* c) {
   learned_free(c);
   scf_free(c);
   pcg_free(c);
+  dfree(c->d_nonorth);
   for (cudaEvent_t e : c->ev) cudaEventDestroy(e);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
   delete c;
@@ -749,6 +750,27 @@ int sb200_set_vec_Ac(sb200_ctx* c, const double vec_Ac[3]) {
   return SB200_OK;
 }
 
+int sb200_set_lattice(sb200_ctx* c, const double rmatrix_B[9], const double coef_F[6]) {
+  CHECK_CTX(c);
+  if (!c->g.set) return set_error(SB200_ERR_STATE, "sb200_set_grid has not been called");
+  DeviceGuard dg(c->device);
+  if (!rmatrix_B || !coef_F) {  // back to the orthogonal branch
+    c->g.nonorth = 0;
+    for (int i = 0; i < 9; ++i) c->g.rB[i] = (i % 4 == 0) ? 1.0 : 0.0;
+    for (int i = 0; i < 6; ++i) c->g.coefF[i] = i < 3 ? 1.0 : 0.0;
+  } else {
+    if (!c->g.periodic) return set_error(SB200_ERR_UNSUPPORTED, "a non-orthogonal lattice needs a periodic grid");
+    for (int i = 0; i < 9; ++i) c->g.rB[i] = rmatrix_B[i];
+    for (int i = 0; i < 6; ++i) c->g.coefF[i] = coef_F[i];
+    c->g.nonorth = 1;
+  }
+  if (c->orb.set) {
+    TRY(refresh_k(c));
+    TRY(nonorth_prepare(c));  // the two-pass scratch at set-up, not inside a later capture
+  }
+  return SB200_OK;
+}
+
 int sb200_set_precision(sb200_ctx* c, int mode) {
   CHECK_CTX(c);
   if (mode != SB200_PREC_FP64 && mode != SB200_PREC_MIXED)
@@ -974,6 +996,7 @@ int sb200_rt_propagate(sb200_ctx* c, double* psi_a, double* psi_b, double* work,
   double2* B = (double2*)psi_b;
   double2* W = (double2*)work;
   TRY(scf_rt_prepare(c));
+  TRY(nonorth_prepare(c));
   SB_CUDA(cudaStreamSynchronize(c->stream));
 
   // Two steps (A->B, B->A) captured as one CUDA graph and replayed.

@@ -181,6 +181,10 @@ struct FinArgs {
   // shards in between) and finish
   int stage;
   double* sums;
+  // non-orthogonal lattice: the lattice-axis current sums are taken to
+  // Cartesian components by B^T (density_matrix.f90:313, 413: wrk2 = BT wrk2)
+  int nonorth;
+  double rB[9];  // rmatrix_B, column-major
 };
 
 // Called by one CTA of 256 threads.
@@ -208,7 +212,8 @@ __device__ __forceinline__ void finalize_body(const FinArgs& a) {
           for (int d = 0; d < 3; ++d) jw[d] += a.jw[(long)a.jw_stride * ((long)o * a.jw_natom + at) + d];
       for (int d = 0; d < 3; ++d) {
         const double kAc = a.vec_k[3 * ik + d] + A[d];
-        s[d] += (kAc * q[0] + 2.0 * q[1 + d] + 2.0 * jw[d]) * w;
+        const double ql = a.nonorth ? a.rB[3 * d] * q[1] + a.rB[3 * d + 1] * q[2] + a.rB[3 * d + 2] * q[3] : q[1 + d];
+        s[d] += (kAc * q[0] + 2.0 * ql + 2.0 * jw[d]) * w;
       }
     }
     for (int d = 0; d < 3; ++d) s[3 + d] += q[4 + d] * w;

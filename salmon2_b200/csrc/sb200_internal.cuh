@@ -12,7 +12,7 @@
 namespace sb200 {
 
 constexpr int ND = 4;            // stencil half-width (Nd of the reference)
-constexpr int KC = 16;           // doubles per k-point coefficient record
+constexpr int KC = 20;           // doubles per k-point coefficient record: kAc(3), k_lap0, k_nabt(12), B kAc(3), pad
 constexpr int OBS_NQ = 7;        // per-orbital local observables (see k_observables)
 constexpr int OBS_THREADS = 256;
 constexpr int OBS_PTS_PER_THREAD = 8;
@@ -27,6 +27,10 @@ struct GridInfo {
   int periodic = 0;
   int is[3], ie[3], is_array[3], ie_array[3], lg_num[3];
   double hgs[3], hvol = 0, coef_lap0 = 0, coef_lap[12], coef_nab[12];
+  // non-orthogonal lattice (sb200_set_lattice): rmatrix_B (3,3) column-major, coef_F(6)
+  int nonorth = 0;
+  double rB[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+  double coefF[6] = {1, 1, 1, 0, 0, 0};
   long vol_array() const {
     return (long)(ie_array[0] - is_array[0] + 1) * (ie_array[1] - is_array[1] + 1) *
            (ie_array[2] - is_array[2] + 1);
@@ -175,6 +179,9 @@ struct sb200_ctx {
   void* scf = nullptr;
   // isolated Hartree potential by CG (sb200_poisson_cg.cu)
   void* pcg = nullptr;
+  // non-orthogonal H psi: first-pass H psi and the x / y first derivatives [3][norb][npts]
+  double2* d_nonorth = nullptr;
+  size_t nonorth_cap = 0;
 };
 
 namespace sb200 {
@@ -232,6 +239,7 @@ int launch_project_dmma(sb200_ctx* c, const void* in, double2* proj, bool in32);
 // 2 n^2 doubles; *info = 1 when the QL iterations did not converge (sb200_eigh.cu)
 int launch_eigh(sb200_ctx* c, const double* M, int n, double* work, double* V, double* w, int* info);
 int launch_hpsi(sb200_ctx* c, const HpsiLaunch& L);
+int nonorth_prepare(sb200_ctx* c);  // scratch of the non-orthogonal hpsi, before a graph capture
 int launch_hpsi_tiled(sb200_ctx* c, const HpsiLaunch& L);  // sb200_stencil.cu
 // tensor-copy-fed tiled kernel; SB200_ERR_UNSUPPORTED when it does not apply (sb200_tma_stencil.cu)
 int launch_hpsi_tma(sb200_ctx* c, const HpsiLaunch& L);

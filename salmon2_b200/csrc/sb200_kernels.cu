@@ -30,6 +30,7 @@ struct PrepArgs {
   int npair;                    // (point, atom) pairs (0: none)
   const int* pair_fp;
   double2* pair_ph;             // [nk][npair] exp(i kAc.r), or null
+  double rB[9];                 // rmatrix_B (identity on orthogonal cells)
 };
 
 __global__ void k_prep(PrepArgs a) {
@@ -56,6 +57,9 @@ __global__ void k_prep(PrepArgs a) {
       kc[3] = a.periodic ? a.coef_lap0 + 0.5 * (kAc[0] * kAc[0] + kAc[1] * kAc[1] + kAc[2] * kAc[2])
                          : a.coef_lap0;
       for (int q = 0; q < 12; ++q) kc[4 + q] = a.periodic ? kAc[q / 4] * a.coef_nab[q] : 0.0;
+      // B (k+A): the lattice-axis components of the non-orthogonal hpsi (hamiltonian.f90:338-343)
+      for (int d = 0; d < 3; ++d) kc[16 + d] = a.rB[d] * kAc[0] + a.rB[d + 3] * kAc[1] + a.rB[d + 6] * kAc[2];
+      kc[19] = 0.0;
     }
     if (a.phase != nullptr && a.totpts > 0) {
       const double* r = a.pt_r + 3L * j;
@@ -518,6 +522,7 @@ int launch_prep_k(sb200_ctx* c, const double* d_A, int a_mode, int itt, double* 
   a.npair = c->pp.npair;
   a.pair_fp = c->pp.d_pair_fp;
   a.pair_ph = (phases && c->g.periodic && c->pp.npair > 0) ? c->pp.d_pair_ph : nullptr;
+  for (int i = 0; i < 9; ++i) a.rB[i] = c->g.rB[i];
   long items = (long)a.nk * (a.totpts > 0 ? a.totpts : 1);
   if ((long)a.nk * a.nent > items) items = (long)a.nk * a.nent;
   if ((long)a.nk * a.npair > items) items = (long)a.nk * a.npair;
@@ -661,6 +666,7 @@ __global__ void __launch_bounds__(256) k_energy_part(const double2* __restrict__
 
 // ttpsi of hpsi (the kinetic part) with the per-point kernel
 int launch_hpsi_kinetic(sb200_ctx* c, const double2* in, double2* tt) {
+  if (c->g.nonorth) return set_error(SB200_ERR_UNSUPPORTED, "ttpsi on a non-orthogonal lattice is not supported");
   const HArgs a = make_hargs(c, make_double2(0.0, 0.0));
   dim3 grid((unsigned)((c->g.npts + 255) / 256), c->orb.norb);
   k_hpsi<9><<<grid, 256, 0, c->stream>>>(in, tt, nullptr, a);
@@ -677,7 +683,148 @@ int launch_energy_parts(sb200_ctx* c, const double2* psi, const double2* h, cons
   return SB200_OK;
 }
 
+// ---------------------------------------------------------------------------
+// hpsi on a non-orthogonal lattice (zstencil_nonorthogonal, stencil.f90:120-214,
+// called from hamiltonian.f90:306-357), one thread per point in two passes:
+// (1) the lattice-axis sums v_d = sum_s lapt(s,d) (t+ + t-) and the first
+// derivatives w_d = sum_s nab(s,d) (t+ - t-), h = (V + k_lap0) psi
+// - 1/2 sum F_d v_d - i sum Bk_d w_d with Bk = B (k+A); w_x and w_y stored;
+// (2) the mixed terms - 1/2 (F_4 d_z w_y + F_5 d_z w_x + F_6 d_y w_x) from the
+// stored derivatives, then the KB term through the inverse map and the Taylor
+// epilogue of MODE.  Periodic grids only (the neighbours wrap).
+// ---------------------------------------------------------------------------
+struct NoArgs {
+  double F[6], nab[12];
+};
+
+__device__ __forceinline__ int wrapi(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
+
+__global__ void __launch_bounds__(256) k_hpsi_no1(const double2* __restrict__ in, double2* __restrict__ h1,
+                                                  double2* __restrict__ wx, double2* __restrict__ wy, HArgs a,
+                                                  NoArgs n) {
+  const long p = blockIdx.x * 256L + threadIdx.x;
+  if (p >= a.npts) return;
+  const int o = blockIdx.y;
+  const int x = (int)(p % a.nx), y = (int)((p / a.nx) % a.ny), z = (int)(p / ((long)a.nx * a.ny));
+  const double2* src = in + (long)o * a.npts;
+  const int ik = o / a.nspin_no, ispin = o % a.nspin;
+  const double* kc = a.kcoef + (long)KC * ik;
+  const long sy = a.nx, sz = (long)a.nx * a.ny;
+  double2 v[3], w[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    double2 vv = make_double2(0.0, 0.0), ww = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int s = 1; s <= ND; ++s) {
+      long qp, qm;
+      if (d == 0) {
+        qp = p - x + wrapi(x + s, a.nx);
+        qm = p - x + wrapi(x - s, a.nx);
+      } else if (d == 1) {
+        qp = p + (long)(wrapi(y + s, a.ny) - y) * sy;
+        qm = p + (long)(wrapi(y - s, a.ny) - y) * sy;
+      } else {
+        qp = p + (long)(wrapi(z + s, a.nz) - z) * sz;
+        qm = p + (long)(wrapi(z - s, a.nz) - z) * sz;
+      }
+      const double2 tp = __ldg(src + qp), tm = __ldg(src + qm);
+      vv = cadd(vv, cscal(a.lapt[4 * d + s - 1], cadd(tp, tm)));
+      ww = cadd(ww, cscal(n.nab[4 * d + s - 1], csub(tp, tm)));
+    }
+    v[d] = vv;
+    w[d] = ww;
+  }
+  const double2 c = __ldg(src + p);
+  const double dg = __ldg(a.vloc + (long)ispin * a.npts + p) + kc[3];
+  const double2 fv = cadd(cadd(cscal(n.F[0], v[0]), cscal(n.F[1], v[1])), cscal(n.F[2], v[2]));
+  const double2 bw = cadd(cadd(cscal(kc[16], w[0]), cscal(kc[17], w[1])), cscal(kc[18], w[2]));
+  // (V + lap0) psi - 0.5 (F.v) - i (Bk.w)
+  const long gi = (long)o * a.npts + p;
+  h1[gi] = make_double2(dg * c.x - 0.5 * fv.x + bw.y, dg * c.y - 0.5 * fv.y - bw.x);
+  wx[gi] = w[0];
+  wy[gi] = w[1];
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(256) k_hpsi_no2(const double2* __restrict__ in, const double2* __restrict__ h1,
+                                                  const double2* __restrict__ wx, const double2* __restrict__ wy,
+                                                  double2* __restrict__ hout, double2* __restrict__ acc, HArgs a,
+                                                  NoArgs n) {
+  const long p = blockIdx.x * 256L + threadIdx.x;
+  if (p >= a.npts) return;
+  const int o = blockIdx.y;
+  const int y = (int)((p / a.nx) % a.ny), z = (int)(p / ((long)a.nx * a.ny));
+  const long sy = a.nx, sz = (long)a.nx * a.ny;
+  const long base = (long)o * a.npts;
+  double2 w1 = make_double2(0.0, 0.0), w2 = make_double2(0.0, 0.0), w3 = make_double2(0.0, 0.0);
+#pragma unroll
+  for (int s = 1; s <= ND; ++s) {
+    const long zp = base + p + (long)(wrapi(z + s, a.nz) - z) * sz, zm = base + p + (long)(wrapi(z - s, a.nz) - z) * sz;
+    const long yp = base + p + (long)(wrapi(y + s, a.ny) - y) * sy, ym = base + p + (long)(wrapi(y - s, a.ny) - y) * sy;
+    w1 = cadd(w1, cscal(n.nab[8 + s - 1], csub(__ldg(wy + zp), __ldg(wy + zm))));  // yz
+    w2 = cadd(w2, cscal(n.nab[8 + s - 1], csub(__ldg(wx + zp), __ldg(wx + zm))));  // zx
+    w3 = cadd(w3, cscal(n.nab[4 + s - 1], csub(__ldg(wx + yp), __ldg(wx + ym))));  // xy
+  }
+  const long gi = base + p;
+  const double2 mix = cadd(cadd(cscal(n.F[3], w1), cscal(n.F[4], w2)), cscal(n.F[5], w3));
+  double2 h = csub(__ldg(h1 + gi), cscal(0.5, mix));
+  if (a.nlma > 0) {
+    const int pm = __ldg(a.pmap + p);
+    if (pm >= 0) {
+      const int ik = o / a.nspin_no;
+      const double2* pj = a.proj + (long)o * a.nlma;
+      const double2* zk = a.ent_zk + (long)ik * a.nent;
+      const int e1 = (pm >> 8) + (pm & 255);
+      for (int e = pm >> 8; e < e1; ++e) h = cadd(h, cmul(pj[__ldg(a.ent_lma + e)], __ldg(zk + e)));
+    }
+  }
+  const double2 c = __ldg(in + gi);
+  if (MODE <= 2) hout[gi] = h;
+  if (MODE == 1 || MODE == 4) acc[gi] = cadd(c, cmul(a.zc, h));
+  if (MODE == 2 || MODE == 3) acc[gi] = cadd(acc[gi], cmul(a.zc, h));
+}
+
+// the scratch of the non-orthogonal hpsi (called before a graph capture, and by every launch)
+int nonorth_prepare(sb200_ctx* c) {
+  if (!c->g.nonorth) return SB200_OK;
+  const size_t need = 3 * (size_t)c->orb.norb * (size_t)c->g.npts;
+  if (c->nonorth_cap < need) {
+    dfree(c->d_nonorth);
+    c->nonorth_cap = 0;
+    if (dalloc(&c->d_nonorth, need) != SB200_OK) return SB200_ERR_OOM;
+    c->nonorth_cap = need;
+  }
+  return SB200_OK;
+}
+
+int launch_hpsi_nonorth(sb200_ctx* c, const HpsiLaunch& L) {
+  if (L.mode > 4) return set_error(SB200_ERR_UNSUPPORTED, "the non-orthogonal hpsi has no mixed-precision modes");
+  if (nonorth_prepare(c) != SB200_OK) return SB200_ERR_OOM;
+  const size_t blk = (size_t)c->orb.norb * (size_t)c->g.npts;
+  double2* h1 = c->d_nonorth;
+  double2* wx = h1 + blk;
+  double2* wy = wx + blk;
+  const HArgs a = make_hargs(c, L.zc);
+  NoArgs n;
+  for (int i = 0; i < 6; ++i) n.F[i] = c->g.coefF[i];
+  for (int i = 0; i < 12; ++i) n.nab[i] = c->g.coef_nab[i];
+  dim3 grid((unsigned)((c->g.npts + 255) / 256), c->orb.norb);
+  const double2* IN = (const double2*)L.in;
+  double2* HOUT = (double2*)L.hout;
+  k_hpsi_no1<<<grid, 256, 0, c->stream>>>(IN, h1, wx, wy, a, n);
+  switch (L.mode) {
+    case 0: k_hpsi_no2<0><<<grid, 256, 0, c->stream>>>(IN, h1, wx, wy, HOUT, L.out, a, n); break;
+    case 1: k_hpsi_no2<1><<<grid, 256, 0, c->stream>>>(IN, h1, wx, wy, HOUT, L.out, a, n); break;
+    case 2: k_hpsi_no2<2><<<grid, 256, 0, c->stream>>>(IN, h1, wx, wy, HOUT, L.out, a, n); break;
+    case 3: k_hpsi_no2<3><<<grid, 256, 0, c->stream>>>(IN, h1, wx, wy, HOUT, L.out, a, n); break;
+    default: k_hpsi_no2<4><<<grid, 256, 0, c->stream>>>(IN, h1, wx, wy, HOUT, L.out, a, n); break;
+  }
+  SB_LAUNCH_CHECK("k_hpsi_no1 / k_hpsi_no2");
+  return SB200_OK;
+}
+
 int launch_hpsi(sb200_ctx* c, const HpsiLaunch& L) {
+  if (c->g.nonorth) return launch_hpsi_nonorth(c, L);
   if (c->stencil_variant == 1 || L.mode >= 5) return launch_hpsi_tiled(c, L);
   const double2* IN = (const double2*)L.in;
   double2* HOUT = (double2*)L.hout;
@@ -775,6 +922,8 @@ FinArgs make_fin_args(const sb200_ctx* c, int itt, int trans_longi, double dt, i
   a.weight = c->d_weight;
   a.vec_k = c->d_vec_k;
   a.step = c->rt.d_step;
+  a.nonorth = c->g.nonorth;
+  for (int i = 0; i < 9; ++i) a.rB[i] = c->g.rB[i];
   if (itt < 0) {
     a.Ac_cur = c->rt.d_Ac_tot;
     a.A_direct = 0;

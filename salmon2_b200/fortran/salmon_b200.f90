@@ -109,6 +109,12 @@ module salmon_b200
       real(c_double), intent(in) :: vec_Ac(3)
     end function
 
+    integer(c_int) function sb200_set_lattice(ctx, rmatrix_B, coef_F) bind(c, name="sb200_set_lattice")
+      import
+      type(c_ptr), value :: ctx
+      real(c_double), intent(in) :: rmatrix_B(3, 3), coef_F(6)
+    end function
+
     integer(c_int) function sb200_set_precision(ctx, mode) bind(c, name="sb200_set_precision")
       import
       type(c_ptr), value :: ctx

@@ -70,6 +70,11 @@ class Context:
                                        _ptr(wtk)))
         V = np.asfortranarray(system.V_local, dtype=np.float64)
         check(lib().sb200_set_vlocal(self.h, _ptr(V)))
+        lat = getattr(system, "lattice", None)
+        if lat is not None:  # non-orthogonal cell: rmatrix_B and coef_F of init_lattice
+            rB = np.asfortranarray(lat.rmatrix_B, dtype=np.float64)
+            F = np.ascontiguousarray(lat.coef_F, dtype=np.float64)
+            check(lib().sb200_set_lattice(self.h, _ptr(rB), _ptr(F)))
         self.set_pp(system.pp)
         self.set_precision(precision)
         self.shape = (system.norb, g.shape[2], g.shape[1], g.shape[0])

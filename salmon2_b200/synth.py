@@ -207,10 +207,118 @@ class System:
     ngrid: int
     seed: int
     name: str = ""
+    lattice: "Lattice | None" = None   # non-orthogonal cell (None: orthogonal)
 
     @property
     def norb(self):
         return self.nspin * self.no * self.nk
+
+
+@dataclasses.dataclass
+class Lattice:
+    """system%primitive_a / rmatrix_A / rmatrix_B and stencil%coef_F of a
+    non-orthogonal cell (init_lattice, src/common/lattice.f90:23-75)."""
+
+    primitive_a: np.ndarray  # (3,3), column d = a_d
+    rmatrix_A: np.ndarray    # (3,3), columns the unit vectors u, v, w
+    rmatrix_B: np.ndarray    # inverse of rmatrix_A
+    coef_F: np.ndarray       # (6,) f_uu, f_vv, f_ww, f_vw, f_uw, f_uv
+    det_a: float
+
+
+def init_lattice(primitive_a) -> Lattice:
+    """init_lattice (lattice.f90:23-75): A = [u v w] the unit lattice vectors,
+    B = A^-1, F = B B^T; coef_F = (F11, F22, F33, F23 + F32, F13 + F31, F12 + F21)."""
+    a = np.asarray(primitive_a, dtype=np.float64)
+    det = float(np.linalg.det(a))
+    A = a / np.linalg.norm(a, axis=0)[None, :]
+    B = np.linalg.inv(A)
+    F = B @ B.T
+    coef_F = np.array([F[0, 0], F[1, 1], F[2, 2], F[1, 2] + F[2, 1], F[0, 2] + F[2, 0], F[0, 1] + F[1, 0]])
+    return Lattice(a, A, B, coef_F, det)
+
+
+def nonorthogonal_system(primitive_a, num, nkgrid=1, no=3, seed=50, natom=2, rc_aa=1.0, nspin=1,
+                         name="nonorth", with_pp=True) -> System:
+    """Periodic system on a non-orthogonal cell (columns of primitive_a the
+    lattice vectors, bohr): grid spacing |a_d| / num_d along each lattice
+    vector, coef_lap0 = -cN0 / 2 sum_d F_d / h_d^2 and hvol = det(A) / N
+    (initialization.f90:242-249, lattice.f90:38-39); Monkhorst-Pack k-points
+    on the reciprocal vectors; Gaussian V_local and Gaussian KB projectors
+    (l <= 1) at seeded atoms, evaluated at the Cartesian grid points
+    r = sum_d i_d h_d u_d with their periodic images."""
+    rng = np.random.default_rng(seed)
+    lat = init_lattice(primitive_a)
+    a = lat.primitive_a
+    nums = [int(num)] * 3 if np.isscalar(num) else [int(v) for v in num]
+    h = np.linalg.norm(a, axis=0) / np.array(nums, dtype=np.float64)
+    grid = make_grid(nums, h, periodic=True)
+    coef_lap0 = -0.5 * CN4[0] * float(np.sum(lat.coef_F[:3] / h ** 2))
+    grid = dataclasses.replace(grid, coef_lap0=coef_lap0, hvol=lat.det_a / float(np.prod(nums)))
+    # Cartesian grid points, x fastest
+    fr = np.meshgrid(*[np.arange(n) / float(n) for n in nums], indexing="ij")
+    R = np.einsum("dk,kxyz->dxyz", a, np.stack(fr))
+    frac_ion = rng.uniform(0.0, 1.0, size=(3, natom))
+    rion = np.asfortranarray(a @ frac_ion)
+    images = [a @ np.array([i, j, k], dtype=np.float64) for i in (-1, 0, 1) for j in (-1, 0, 1) for k in (-1, 0, 1)]
+    amps, widths = rng.uniform(-2.0, -0.5, natom), rng.uniform(0.8, 1.6, natom)
+    V = np.zeros(nums)
+    for ia in range(natom):
+        for t in images:
+            d = R - (rion[:, ia] + t)[:, None, None, None]
+            V += amps[ia] * np.exp(-np.sum(d * d, axis=0) / (2.0 * widths[ia] ** 2))
+    V_local = np.asfortranarray(np.repeat(V[..., None], nspin, axis=3))
+    if with_pp:
+        rc = rc_aa / AU_LENGTH_AA
+        sigma, amp = rng.uniform(0.5, 0.8, natom), rng.uniform(0.3, 0.6, natom)
+        inorm = rng.choice([-1, 1], size=(natom, 2))
+        idx = np.stack(np.meshgrid(*[np.arange(1, n + 1) for n in nums], indexing="ij"))
+        Rf = R.reshape(3, -1, order="F")
+        If = idx.reshape(3, -1, order="F")
+        pts = []
+        for ia in range(natom):
+            jl, rl = [], []
+            for t in images:
+                d = Rf - (rion[:, ia] + t)[:, None]
+                sel = np.sqrt(np.sum(d * d, axis=0)) < rc + 1e-12
+                jl.append(If[:, sel])
+                rl.append(d[:, sel])
+            pts.append((np.concatenate(jl, axis=1), np.concatenate(rl, axis=1)))
+        mps = np.array([p[0].shape[1] for p in pts], dtype=np.int32)
+        nps = int(mps.max())
+        jxyz = np.zeros((3, nps, natom), dtype=np.int32, order="F")
+        rxyz = np.zeros((3, nps, natom), dtype=np.float64, order="F")
+        for ia, (j, r) in enumerate(pts):
+            jxyz[:, : j.shape[1], ia] = j
+            rxyz[:, : r.shape[1], ia] = r
+        nlma = 4 * natom
+        uv = np.zeros((nps, nlma), order="F")
+        ia_tbl = np.zeros(nlma, dtype=np.int32)
+        rinv = np.zeros(nlma)
+        lma = 0
+        for ia in range(natom):
+            m_ = mps[ia]
+            x, y, z = rxyz[0, :m_, ia], rxyz[1, :m_, ia], rxyz[2, :m_, ia]
+            g = amp[ia] * np.exp(-(x * x + y * y + z * z) / (2.0 * sigma[ia] ** 2))
+            for (l, m) in [(0, 0), (1, -1), (1, 0), (1, 1)]:
+                uv[:m_, lma] = g * ylm(x, y, z, l, m)
+                ia_tbl[lma] = ia + 1
+                rinv[lma] = float(inorm[ia, l]) * grid.hvol
+                lma += 1
+        pp = PPGrid(natom, nps, nlma, mps, jxyz, rxyz, uv, ia_tbl, rinv)
+    else:
+        pp = PPGrid(0, 0, 0, np.zeros(0, np.int32), np.zeros((3, 0, 0), np.int32, order="F"),
+                    np.zeros((3, 0, 0), order="F"), np.zeros((0, 0), order="F"), np.zeros(0, np.int32), np.zeros(0))
+    n = int(nkgrid)
+    f = (2.0 * np.arange(1, n + 1) - n - 1) / (2.0 * n)
+    brec = 2.0 * np.pi * np.linalg.inv(a).T  # columns b_d
+    ks = [brec @ np.array([f[i], f[j], f[k]]) for k in range(n) for j in range(n) for i in range(n)]
+    vec_k = np.asfortranarray(np.array(ks).T)
+    nk = vec_k.shape[1]
+    psi = random_orbitals(grid, rng, nspin, no, nk)
+    psi *= math.sqrt(float(np.prod(h)) / grid.hvol)  # orthonormal in the det(A) / N metric
+    return System(grid, pp, nspin, no, nk, vec_k, np.asfortranarray(np.full((no, nk, nspin), 2.0)),
+                  np.full(nk, 1.0 / nk), V_local, rion, psi, int(np.prod(nums)), seed, name, lat)
 
 
 def gaussian_potential(grid: Grid, centers: np.ndarray, amps, widths, cell=None) -> np.ndarray:

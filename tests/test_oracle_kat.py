@@ -221,3 +221,65 @@ def test_impulse_kick_oracle_equals_synth(num, epdir):
     b = synth.impulse_kick(s.grid, s.psi, k, epdir)
     assert np.max(np.abs(a - b)) <= 1e-15 * np.max(np.abs(b))
     assert np.max(np.abs(np.abs(a) - np.abs(s.psi))) <= 1e-15
+
+
+def _fcc(a=10.26):
+    h = a / 2.0
+    return np.array([[0.0, h, h], [h, 0.0, h], [h, h, 0.0]]).T  # columns a1, a2, a3
+
+
+def test_nonorthogonal_stencil_plane_wave_symbol():
+    """The oracle's zstencil_nonorthogonal (stencil.f90:120-214) on a lattice
+    plane wave exp(i sum_d theta_d n_d): H psi = lambda psi with the symbol of
+    the finite-difference operator, lambda = lap0 - 1/2 sum_d F_d L_d
+    - i sum_d Bk_d D_d - 1/2 (F_4 D_z D_y + F_5 D_z D_x + F_6 D_y D_x),
+    L_d = sum_s 2 c_s cos(s theta_d) / h_d^2, D_d = 2 i sum_s b_s sin(s theta_d) / h_d
+    (the mixed terms are the first-derivative stencil applied twice)."""
+    import dataclasses
+    import _systems as S
+    from salmon2_b200 import synth
+    s = S.no_pp(synth.nonorthogonal_system(_fcc(), (10, 12, 14), nkgrid=2, no=1, seed=61, with_pp=False))
+    s = dataclasses.replace(s, V_local=np.zeros_like(s.V_local))
+    g = s.grid
+    nums = np.array(g.shape)
+    m = np.array([2, -3, 5])
+    th = 2 * np.pi * m / nums
+    n = np.meshgrid(*[np.arange(k) for k in nums], indexing="ij")
+    pw = np.exp(1j * (th[0] * n[0] + th[1] * n[1] + th[2] * n[2]))
+    psi = np.zeros_like(s.psi)
+    sl = g.interior_slices()
+    for ik in range(s.nk):
+        psi[sl + (0, 0, ik)] = pw
+    O = Oracle(s)
+    ac = (0.011, -0.02, 0.017)
+    O.set_vec_Ac(ac)
+    hp = O.hpsi(psi)
+    lat = s.lattice
+    F = lat.coef_F
+    c = synth.CN4
+    b = synth.BN4
+    L = np.array([sum(2 * c[k] * np.cos(k * th[d]) for k in range(1, 5)) / g.hgs[d] ** 2 for d in range(3)])
+    D = np.array([2j * sum(b[k - 1] * np.sin(k * th[d]) for k in range(1, 5)) / g.hgs[d] for d in range(3)])
+    for ik in range(s.nk):
+        kac = s.vec_k[:, ik] + np.array(ac)
+        lap0 = g.coef_lap0 + 0.5 * kac @ kac
+        bk = lat.rmatrix_B @ kac
+        lam = (lap0 - 0.5 * (F[:3] @ L) - 1j * (bk @ D)
+               - 0.5 * (F[3] * D[2] * D[1] + F[4] * D[2] * D[0] + F[5] * D[1] * D[0]))
+        got = hp[sl + (0, 0, ik)]
+        assert np.max(np.abs(got - lam * pw)) <= 1e-12 * np.max(np.abs(lam))
+
+
+def test_nonorthogonal_path_on_a_cubic_cell_equals_the_orthogonal_stencil():
+    """A cubic cell taken through the non-orthogonal branch (F = (1, 1, 1, 0,
+    0, 0), B = 1) gives the orthogonal branch's H psi, KB term included."""
+    import dataclasses
+    from salmon2_b200 import synth
+    s = synth.nonorthogonal_system(np.diag([8.0, 8.0, 8.0]), 12, nkgrid=2, no=2, seed=62)
+    ortho = dataclasses.replace(s, lattice=None)
+    a, b = Oracle(s), Oracle(ortho)
+    for ac in ((0.0, 0.0, 0.0), (0.03, -0.01, 0.02)):
+        a.set_vec_Ac(ac)
+        b.set_vec_Ac(ac)
+        ha, hb = a.hpsi(s.psi), b.hpsi(s.psi)
+        assert np.max(np.abs(ha - hb)) <= 1e-13 * np.max(np.abs(hb))

@@ -117,6 +117,26 @@ int sb200_set_vlocal(sb200_ctx* ctx, const double* V_local);
 int sb200_set_pp(sb200_ctx* ctx, int natom, int nps, int nlma, const int* mps, const int* jxyz,
                  const double* rxyz, const double* uv, const int* ia_tbl, const double* rinv_uvu);
 
+/* Host-side set-up (no device, no context): the Kleinman-Bylander tables of
+ * s_pp_grid and, on an isolated grid, the local pseudopotential Vpsl, from
+ * Yabana-Bertsch pseudopotential files (`_rps.dat`, ps_format = 'KY'; angstrom
+ * and eV as written).  files[nelem] the element files, lmax_ps[nelem] (Lmax_ps;
+ * NULL or -1: the file's), lloc_ps[nelem] (Lloc_ps, the local channel); the
+ * grid as for sb200_set_grid (lg%num, lg%is, system%hgs, system%hvol; orthogonal
+ * cell); natom atoms of element kion[a] (1-based) at Rion(3, natom) (bohr).
+ * Call once with mps ... rinv_uvu NULL: *nps and *nlma return the sizes; then
+ * with arrays mps(natom), jxyz(3,nps,natom), rxyz(3,nps,natom), uv(nps,nlma),
+ * ia_tbl(nlma), rinv_uvu(nlma) (the layout sb200_set_pp takes) and, for an
+ * isolated grid, Vpsl(is:ie) or NULL.  Periodic grids: Vpsl must be NULL.
+ * Replaces: read_ps_KY and the radial set-up of input_pp
+ * (src/atom/pp/input_pp.f90:96-341), making_ps_without_masking (:1111-1240),
+ * init_ps with calc_nps / calc_jxyz / set_lma / calc_uv
+ * (src/atom/pp/prep_pp.f90:22-525) and calc_Vpsl_isolated (:550-620).          */
+int sb200_init_ps_ky(int nelem, const char* const* files, const int* lmax_ps, const int* lloc_ps, int periodic,
+                     const int num[3], const int is[3], const double hgs[3], double hvol, int natom,
+                     const int* kion, const double* Rion, int* nps, int* nlma, int* mps, int* jxyz, double* rxyz,
+                     double* uv, int* ia_tbl, double* rinv_uvu, double* Vpsl);
+
 /* system%vec_Ac (A/c) used by sb200_hpsi: recomputes k+A stencil coefficients
  * and the projector phases (update_kvector_nonlocalpt,
  * src/common/hamiltonian.f90:847-903).  Isolated grids ignore it.              */

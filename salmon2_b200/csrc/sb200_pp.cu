@@ -1,0 +1,376 @@
+// sb200_pp.cu -- host side: Kleinman-Bylander tables of s_pp_grid and the
+// local pseudopotential of an isolated grid from Yabana-Bertsch pseudopotential
+// files (`_rps.dat`, ps_format = 'KY'), the set-up that produces the tables the
+// propagation path consumes (no device code).
+//
+//   read_ps_KY                    src/atom/pp/input_pp.f90:288-341
+//   input_pp (radial domain,
+//     KB norms)                   src/atom/pp/input_pp.f90:96-193
+//   making_ps_without_masking     src/atom/pp/input_pp.f90:1111-1240
+//   init_ps: calc_nps / calc_jxyz src/atom/pp/prep_pp.f90:22-372
+//            set_lma / calc_uv    src/atom/pp/prep_pp.f90:374-525
+//   calc_Vpsl_isolated            src/atom/pp/prep_pp.f90:550-620
+//   spline (natural cubic)        src/math/salmon_math.f90:500-584
+//   Ylm                           src/math/salmon_math.f90:386-426
+//
+// The radial KB function of angular momentum l is
+//   udv_l(r) = (v_l(r) - v_lloc(r)) u_l(r) sqrt((2l+1)/4pi) / r^(l+1) / anorm_l,
+//   anorm_l^2 = |int u_l^2 (v_l - v_lloc) dr| (trapezoid on the file's grid),
+// interpolated at each sphere point by a natural cubic spline over the points
+// r < rps (rps = max of the file's cut-off radii) and multiplied by the
+// polynomial Ylm(x, y, z) of the point's offset from the atom; rinv_uvu =
+// sign(anorm_l^2) hvol.  Projectors with anorm_l^2 = 0 (the local l) are left
+// out.  Vpsl of an isolated grid: the local channel v_lloc interpolated
+// linearly at each point's distance from every atom (beyond the file's grid,
+// -Zps / r) and summed over the atoms.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "sb200_internal.cuh"
+
+namespace sb200 {
+namespace {
+
+constexpr double PP_PI = 3.141592653589793;
+constexpr double AU_LENGTH_AA = 0.52917721067;  // src/io/inputoutput.f90:27
+constexpr double AU_ENERGY_EV = 27.21138505;    // src/io/inputoutput.f90:26
+
+struct KyElement {
+  int mr = 0, mlps = 0, lref = 0, nrps = 0, nrmax = 0;
+  double step = 0.0, zps = 0.0, rps = 0.0;
+  std::vector<double> rad;                  // rad[i - 1] = (i - 1) step, i = 1..nrmax
+  std::vector<std::vector<double>> vpp;     // [l][0..nrmax]
+  std::vector<std::vector<double>> upp;     // [l][0..nrmax]
+  std::vector<double> anorm;
+  std::vector<int> inorm;
+  std::vector<std::vector<double>> sa, sb, sc, sd;  // spline of udv_l on rad[0..nrps-1]
+};
+
+double ylm_poly(double x, double y, double z, int l, int m) {
+  const double r2 = x * x + y * y + z * z;
+  if (l == 0) return 1.0;
+  if (l == 1) return m == -1 ? -y : (m == 0 ? z : -x);
+  if (l == 2) {
+    switch (m) {
+      case -2: return std::sqrt(3.0) * x * y;
+      case -1: return -std::sqrt(3.0) * y * z;
+      case 0: return (3.0 * z * z - r2) / 2.0;
+      case 1: return -std::sqrt(3.0) * x * z;
+      default: return std::sqrt(3.0 / 4.0) * (x * x - y * y);
+    }
+  }
+  switch (m) {  // l = 3
+    case -3: return -std::sqrt(5.0 / 8.0) * y * (3 * x * x - y * y);
+    case -2: return std::sqrt(15.0) * x * y * z;
+    case -1: return -std::sqrt(3.0 / 8.0) * y * (5.0 * z * z - r2);
+    case 0: return z * (5.0 * z * z - 3 * r2) / 2.0;
+    case 1: return -std::sqrt(3.0 / 8.0) * x * (5.0 * z * z - r2);
+    case 2: return std::sqrt(15.0 / 4.0) * z * (x * x - y * y);
+    default: return -std::sqrt(5.0 / 8.0) * x * (x * x - 3.0 * y * y);
+  }
+}
+
+// natural cubic spline through (xn[i], yn[i]), i < np: on interval i
+// y = a (x - xn_i)^3 + b (x - xn_i)^2 + c (x - xn_i) + d; the second
+// derivatives from the tridiagonal system (Thomas algorithm)
+void natural_spline(const std::vector<double>& xn, const std::vector<double>& yn, int np, std::vector<double>& a,
+                    std::vector<double>& b, std::vector<double>& c, std::vector<double>& d) {
+  const int n = np - 2;
+  std::vector<double> dx(np - 1), dy(np - 1), u(np, 0.0);
+  for (int i = 0; i < np - 1; ++i) {
+    dx[i] = xn[i + 1] - xn[i];
+    dy[i] = yn[i + 1] - yn[i];
+  }
+  if (n > 0) {
+    std::vector<double> diag(n + 1), up(n + 1), rhs(n + 1);
+    for (int i = 1; i <= n; ++i) {
+      diag[i] = 2.0 * (dx[i] + dx[i - 1]);
+      up[i] = dx[i];
+      rhs[i] = 6.0 * (dy[i] / dx[i] - dy[i - 1] / dx[i - 1]);
+    }
+    for (int i = 2; i <= n; ++i) {  // forward elimination (sub-diagonal dx[i-1])
+      const double w = dx[i - 1] / diag[i - 1];
+      diag[i] -= w * up[i - 1];
+      rhs[i] -= w * rhs[i - 1];
+    }
+    u[n] = rhs[n] / diag[n];
+    for (int i = n - 1; i >= 1; --i) u[i] = (rhs[i] - up[i] * u[i + 1]) / diag[i];
+  }
+  a.assign(np - 1, 0.0);
+  b.assign(np - 1, 0.0);
+  c.assign(np - 1, 0.0);
+  d.assign(np - 1, 0.0);
+  for (int i = 0; i < np - 1; ++i) {
+    b[i] = 0.5 * u[i];
+    a[i] = (u[i + 1] - 2.0 * b[i]) / (6.0 * dx[i]);
+    d[i] = yn[i];
+    c[i] = dy[i] / dx[i] - dx[i] * (u[i + 1] + 2.0 * u[i]) / 6.0;
+  }
+}
+
+int read_ky(const char* path, int lmax_ps, int lloc, int nrmax, KyElement& e) {
+  FILE* f = std::fopen(path, "r");
+  if (!f) return set_error(SB200_ERR_INVALID_ARG, std::string("cannot open pseudopotential file ") + path);
+  double rzps = 0.0;
+  int ok = std::fscanf(f, "%d %lf %d %lf", &e.mr, &e.step, &e.mlps, &rzps) == 4;
+  if (!ok || e.mr < 2 || e.mlps < 0 || e.mlps > 3 || e.step <= 0.0) {
+    std::fclose(f);
+    return set_error(SB200_ERR_INVALID_ARG, std::string("not a Yabana-Bertsch (KY) file: ") + path);
+  }
+  e.zps = (double)(int)(rzps + 1e-10);
+  int irpc = 0;
+  std::vector<double> rrc(e.mlps + 1, 0.0);
+  ok = std::fscanf(f, "%d", &irpc) == 1;
+  for (int l = 0; l <= e.mlps && ok; ++l) ok = std::fscanf(f, "%lf", &rrc[l]) == 1;
+  const int nr = nrmax > e.mr ? nrmax : e.mr;
+  e.nrmax = nrmax;
+  const int nl = e.mlps + 1;
+  e.vpp.assign(nl, std::vector<double>(nr + 1, 0.0));
+  e.upp.assign(nl, std::vector<double>(nr + 1, 0.0));
+  for (int i = 0; i <= e.mr && ok; ++i) {
+    double r, rho;
+    ok = std::fscanf(f, "%lf %lf", &r, &rho) == 2;
+    for (int l = 0; l < nl && ok; ++l) ok = std::fscanf(f, "%lf", &e.vpp[l][i]) == 1;
+  }
+  for (int i = 0; i <= e.mr && ok; ++i) {
+    double r;
+    ok = std::fscanf(f, "%lf", &r) == 1;
+    for (int l = 0; l < nl && ok; ++l) ok = std::fscanf(f, "%lf", &e.upp[l][i]) == 1;
+  }
+  std::fclose(f);
+  if (!ok) return set_error(SB200_ERR_INVALID_ARG, std::string("truncated KY file: ") + path);
+  // atomic units (read_ps_KY)
+  e.step /= AU_LENGTH_AA;
+  for (int l = 0; l < nl; ++l) {
+    rrc[l] /= AU_LENGTH_AA;
+    for (int i = 0; i <= e.mr; ++i) {
+      e.vpp[l][i] /= AU_ENERGY_EV;
+      e.upp[l][i] *= std::sqrt(AU_LENGTH_AA);
+    }
+  }
+  e.rad.resize(nrmax);
+  for (int i = 1; i <= nrmax; ++i) e.rad[i - 1] = (i - 1) * e.step;
+  if (lmax_ps >= 0) {
+    if (lmax_ps > e.mlps) return set_error(SB200_ERR_INVALID_ARG, "Lmax_ps above the file's angular momenta");
+    e.mlps = lmax_ps;
+  }
+  if (lloc < 0 || lloc > e.mlps) return set_error(SB200_ERR_INVALID_ARG, "Lloc_ps must be in 0..Lmax_ps");
+  e.lref = lloc;
+  // beyond the file's grid: -Zps / r (input_pp.f90:96-102; the array index i
+  // takes rad(i) here although vpp(i) otherwise stands for rad(i + 1))
+  for (int i = e.mr + 1; i <= nrmax; ++i)
+    for (int l = 0; l <= e.mlps; ++l) {
+      if (e.rad[i - 1] > 0.0) e.vpp[l][i] = -e.zps / e.rad[i - 1];
+      e.upp[l][i] = 0.0;
+    }
+  double rps = 0.0;
+  for (int l = 0; l <= e.mlps; ++l) rps = rrc[l] > rps ? rrc[l] : rps;
+  e.rps = rps;
+  int i = 1;
+  for (; i <= nrmax; ++i)
+    if (e.rad[i - 1] > e.rps) break;
+  e.nrps = i;
+  if (e.nrps >= nrmax) return set_error(SB200_ERR_INVALID_ARG, "pseudopotential cut-off beyond the radial grid");
+  // KB norms (input_pp.f90:179-193), trapezoid on rad
+  e.anorm.assign(e.mlps + 1, 0.0);
+  e.inorm.assign(e.mlps + 1, 0);
+  for (int l = 0; l <= e.mlps; ++l) {
+    double s = 0.0;
+    for (int k = 1; k <= e.mr - 1; ++k) {
+      const double r1 = e.rad[k] - e.rad[k - 1];
+      s = s + (e.upp[l][k] * e.upp[l][k] * (e.vpp[l][k] - e.vpp[e.lref][k]) +
+               e.upp[l][k - 1] * e.upp[l][k - 1] * (e.vpp[l][k - 1] - e.vpp[e.lref][k - 1])) *
+                  r1;
+    }
+    s = 0.5 * s;
+    e.inorm[l] = 1;
+    if (s < 0.0) {
+      s = -s;
+      e.inorm[l] = -1;
+    }
+    if (std::fabs(s) < 1e-10) e.inorm[l] = 0;
+    e.anorm[l] = std::sqrt(s);
+  }
+  // making_ps_without_masking: radial functions / r^(l+1), then the KB tables
+  for (int l = 0; l <= e.mlps; ++l) {
+    for (int k = 1; k <= e.mr; ++k)
+      e.upp[l][k] = e.upp[l][k] * std::sqrt((2 * l + 1.0) / (4 * PP_PI)) / std::pow(e.rad[k], l + 1);
+    e.upp[l][0] = e.upp[l][1];
+  }
+  e.sa.assign(e.mlps + 1, {});
+  e.sb.assign(e.mlps + 1, {});
+  e.sc.assign(e.mlps + 1, {});
+  e.sd.assign(e.mlps + 1, {});
+  std::vector<double> xn(e.rad.begin(), e.rad.begin() + e.nrps), yn(e.nrps);
+  for (int l = 0; l <= e.mlps; ++l) {
+    for (int k = 1; k <= e.nrps; ++k) {
+      yn[k - 1] = (e.vpp[l][k - 1] - e.vpp[e.lref][k - 1]) * e.upp[l][k - 1];
+      if (e.inorm[l] != 0) yn[k - 1] = yn[k - 1] / e.anorm[l];
+    }
+    natural_spline(xn, yn, e.nrps, e.sa[l], e.sb[l], e.sc[l], e.sd[l]);
+  }
+  return SB200_OK;
+}
+
+}  // namespace
+}  // namespace sb200
+
+using namespace sb200;
+
+extern "C" int sb200_init_ps_ky(int nelem, const char* const* files, const int* lmax_ps, const int* lloc_ps,
+                                int periodic, const int num[3], const int is[3], const double hgs[3], double hvol,
+                                int natom, const int* kion, const double* Rion, int* nps, int* nlma, int* mps,
+                                int* jxyz, double* rxyz, double* uv, int* ia_tbl, double* rinv_uvu,
+                                double* Vpsl) {
+  if (nelem < 1 || !files || !lloc_ps || !num || !is || !hgs || natom < 0 || (natom > 0 && (!kion || !Rion)) ||
+      !nps || !nlma)
+    return set_error(SB200_ERR_INVALID_ARG, "sb200_init_ps_ky: null or inconsistent argument");
+  if (periodic && Vpsl) return set_error(SB200_ERR_UNSUPPORTED, "Vpsl is built here for isolated grids only");
+  const int nrmax = periodic ? 3000 : 20000;  // read_pslfile, salmon_pp.f90:34-38
+  std::vector<KyElement> el(nelem);
+  for (int k = 0; k < nelem; ++k) {
+    const int r = read_ky(files[k], lmax_ps ? lmax_ps[k] : -1, lloc_ps[k], nrmax, el[k]);
+    if (r != SB200_OK) return r;
+  }
+  for (int a = 0; a < natom; ++a)
+    if (kion[a] < 1 || kion[a] > nelem) return set_error(SB200_ERR_INVALID_ARG, "kion out of 1..nelem");
+  const int ie[3] = {is[0] + num[0] - 1, is[1] + num[1] - 1, is[2] + num[2] - 1};
+  const double al[3] = {num[0] * hgs[0], num[1] * hgs[1], num[2] * hgs[2]};
+  double rshift[3];
+  for (int d = 0; d < 3; ++d) rshift[d] = periodic ? -hgs[d] : ((num[d] % 2 == 1) ? 0.0 : -0.5 * hgs[d]);
+  // periodic images (init_ps, prep_pp.f90:86-112, cuboid cell)
+  double rps_max = 0.0, hmax = 0.0;
+  for (int k = 0; k < nelem; ++k) rps_max = el[k].rps > rps_max ? el[k].rps : rps_max;
+  for (int d = 0; d < 3; ++d) hmax = hgs[d] > hmax ? hgs[d] : hmax;
+  rps_max = rps_max + 1.5 * hmax + 1e-2;
+  int nc[3] = {0, 0, 0};
+  if (periodic)
+    for (int d = 0; d < 3; ++d) {
+      double mn = 1e300, mx = -1e300;
+      for (int a = 0; a < natom; ++a) {
+        mn = Rion[3 * a + d] < mn ? Rion[3 * a + d] : mn;
+        mx = Rion[3 * a + d] > mx ? Rion[3 * a + d] : mx;
+      }
+      nc[d] = (mn + 2.0 * al[d] > al[d] + rps_max && mx - 2.0 * al[d] < -rps_max) ? 1 : 2;
+    }
+  // sphere points (calc_nps / calc_jxyz): images j1, j2, j3, then z, y, x
+  std::vector<std::vector<int>> pj(natom);
+  std::vector<std::vector<double>> pr(natom);
+  for (int a = 0; a < natom; ++a) {
+    const KyElement& e = el[kion[a] - 1];
+    for (int j1 = -nc[0]; j1 <= nc[0]; ++j1) {
+      const double x1 = Rion[3 * a] + j1 * al[0];
+      if (x1 <= is[0] * hgs[0] - rps_max || x1 >= ie[0] * hgs[0] + rps_max) continue;
+      for (int j2 = -nc[1]; j2 <= nc[1]; ++j2) {
+        const double x2 = Rion[3 * a + 1] + j2 * al[1];
+        if (x2 <= is[1] * hgs[1] - rps_max || x2 >= ie[1] * hgs[1] + rps_max) continue;
+        for (int j3 = -nc[2]; j3 <= nc[2]; ++j3) {
+          const double x3 = Rion[3 * a + 2] + j3 * al[2];
+          if (x3 <= is[2] * hgs[2] - rps_max || x3 >= ie[2] * hgs[2] + rps_max) continue;
+          for (int i3 = is[2]; i3 <= ie[2]; ++i3)
+            for (int i2 = is[1]; i2 <= ie[1]; ++i2)
+              for (int i1 = is[0]; i1 <= ie[0]; ++i1) {
+                const double x = i1 * hgs[0] + rshift[0] - x1, y = i2 * hgs[1] + rshift[1] - x2,
+                             z = i3 * hgs[2] + rshift[2] - x3;
+                const double r = std::sqrt(x * x + y * y + z * z);
+                if (r < e.rps + 1e-12) {
+                  pj[a].insert(pj[a].end(), {i1, i2, i3});
+                  pr[a].insert(pr[a].end(), {x, y, z});
+                }
+              }
+        }
+      }
+    }
+  }
+  int np = 0, nl = 0;
+  for (int a = 0; a < natom; ++a) {
+    const int m = (int)pj[a].size() / 3;
+    np = m > np ? m : np;
+    const KyElement& e = el[kion[a] - 1];
+    for (int l = 0; l <= e.mlps; ++l)
+      if (e.inorm[l] != 0) nl += 2 * l + 1;
+  }
+  const bool fill = mps && jxyz && rxyz && uv && ia_tbl && rinv_uvu;
+  if (fill && (*nps < np || *nlma < nl))
+    return set_error(SB200_ERR_INVALID_ARG, "sb200_init_ps_ky: output arrays smaller than *nps, *nlma");
+  if (!fill) {
+    *nps = np;
+    *nlma = nl;
+  } else {
+    const int NPS = *nps, NLMA = *nlma;
+    std::memset(jxyz, 0, sizeof(int) * 3 * (size_t)NPS * natom);
+    std::memset(rxyz, 0, sizeof(double) * 3 * (size_t)NPS * natom);
+    std::memset(uv, 0, sizeof(double) * (size_t)NPS * NLMA);
+    int lma = 0;
+    for (int a = 0; a < natom; ++a) {
+      const KyElement& e = el[kion[a] - 1];
+      const int m = (int)pj[a].size() / 3;
+      mps[a] = m;
+      for (int j = 0; j < m; ++j)
+        for (int c = 0; c < 3; ++c) {
+          jxyz[c + 3 * ((size_t)j + (size_t)NPS * a)] = pj[a][3 * j + c];
+          rxyz[c + 3 * ((size_t)j + (size_t)NPS * a)] = pr[a][3 * j + c];
+        }
+      // calc_uv: spline at each sphere point, times Ylm of its offset
+      const int lma0 = lma;
+      for (int l = 0; l <= e.mlps; ++l) {
+        if (e.inorm[l] == 0) continue;
+        for (int mm = -l; mm <= l; ++mm) {
+          ia_tbl[lma] = a + 1;
+          rinv_uvu[lma] = (double)e.inorm[l] * hvol;
+          ++lma;
+        }
+      }
+      for (int j = 0; j < m; ++j) {
+        const double x = pr[a][3 * j], y = pr[a][3 * j + 1], z = pr[a][3 * j + 2];
+        const double r = std::sqrt(x * x + y * y + z * z) + 1e-50;
+        int ir = 1;
+        for (; ir <= e.nrps; ++ir)
+          if (e.rad[ir - 1] > r) break;
+        const int intr = ir - 1;  // 1-based interval: rad(intr) <= r < rad(intr + 1)
+        if (intr < 1 || intr >= e.nrps) return set_error(SB200_ERR_INVALID_ARG, "sphere point outside the radial grid");
+        const double xx = r - e.rad[intr - 1];
+        int col = lma0;
+        for (int l = 0; l <= e.mlps; ++l) {
+          if (e.inorm[l] == 0) continue;
+          const int s = intr - 1;
+          const double uvr = e.sa[l][s] * xx * xx * xx + e.sb[l][s] * xx * xx + e.sc[l][s] * xx + e.sd[l][s];
+          for (int mm = -l; mm <= l; ++mm) uv[(size_t)j + (size_t)NPS * col++] = uvr * ylm_poly(x, y, z, l, mm);
+        }
+      }
+    }
+  }
+  if (Vpsl) {  // calc_Vpsl_isolated: linear interpolation of the local channel
+    const long npts = (long)num[0] * num[1] * num[2];
+    for (long p = 0; p < npts; ++p) Vpsl[p] = 0.0;
+    for (int a = 0; a < natom; ++a) {
+      const KyElement& e = el[kion[a] - 1];
+      for (int iz = 0; iz < num[2]; ++iz)
+        for (int iy = 0; iy < num[1]; ++iy)
+          for (int ix = 0; ix < num[0]; ++ix) {
+            const int g[3] = {ix + is[0], iy + is[1], iz + is[2]};
+            double d2 = 0.0;
+            for (int d = 0; d < 3; ++d) {
+              const double c = (num[d] % 2 == 1) ? g[d] * hgs[d] : (g[d] - 0.5) * hgs[d];
+              const double t = c - Rion[3 * a + d];
+              d2 += t * t;
+            }
+            const double r = std::sqrt(d2) + 1e-50;
+            int imin = 1, imax = e.nrmax;  // bisection (prep_pp.f90:1013-1035)
+            while (imax - imin > 1) {
+              const int in = (imin + imax) / 2;
+              if (r > e.rad[in - 1]) imin = in;
+              else imax = in;
+            }
+            const int intr = imin;
+            const double ratio1 = (r - e.rad[intr - 1]) / (e.rad[intr] - e.rad[intr - 1]), ratio2 = 1.0 - ratio1;
+            double& v = Vpsl[ix + (long)num[0] * (iy + (long)num[1] * iz)];
+            v = v + ratio1 * e.vpp[e.lref][intr] + ratio2 * e.vpp[e.lref][intr - 1];
+          }
+    }
+  }
+  return SB200_OK;
+}

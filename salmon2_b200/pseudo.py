@@ -1,0 +1,48 @@
+"""Kleinman-Bylander tables and the isolated local potential from
+Yabana-Bertsch pseudopotential files (`_rps.dat`, ps_format = 'KY') through the
+library's host-side builder (sb200_init_ps_ky; input_pp.f90 read_ps_KY,
+making_ps_without_masking, prep_pp.f90 init_ps, calc_Vpsl_isolated)."""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from ._lib import check, lib
+from .synth import PPGrid
+
+_ip = C.POINTER(C.c_int)
+_dp = C.POINTER(C.c_double)
+
+
+def init_ps_ky(files, lloc_ps, grid, rion, kion, lmax_ps=None, vpsl=True):
+    """files: one path per element; lloc_ps / lmax_ps: per element (Lloc_ps,
+    Lmax_ps; lmax_ps None keeps the file's); grid: a synth.Grid (orthogonal);
+    rion: (3, natom) bohr; kion: 1-based element of each atom.  Returns
+    (PPGrid, Vpsl (nx, ny, nz) Fortran order, or None on periodic grids / vpsl=False)."""
+    nelem = len(files)
+    arr = (C.c_char_p * nelem)(*[str(f).encode() for f in files])
+    lloc = np.ascontiguousarray(lloc_ps, dtype=np.int32)
+    lmax = None if lmax_ps is None else np.ascontiguousarray(lmax_ps, dtype=np.int32)
+    num = np.ascontiguousarray(grid.num, dtype=np.int32)
+    is_ = np.ascontiguousarray(grid.is_, dtype=np.int32)
+    hgs = np.ascontiguousarray(grid.hgs, dtype=np.float64)
+    r = np.ascontiguousarray(np.asarray(rion, dtype=np.float64).reshape(3, -1, order="F").T)
+    natom = r.shape[0]
+    k = np.ascontiguousarray(kion, dtype=np.int32)
+    nps, nlma = C.c_int(0), C.c_int(0)
+    P = lambda a, t=_dp: None if a is None else a.ctypes.data_as(t)
+    args = [nelem, arr, P(lmax, _ip), P(lloc, _ip), 1 if grid.periodic else 0, P(num, _ip), P(is_, _ip), P(hgs),
+            float(grid.hvol), natom, P(k, _ip), P(r)]
+    check(lib().sb200_init_ps_ky(*args, C.byref(nps), C.byref(nlma), None, None, None, None, None, None, None))
+    n, m = nps.value, nlma.value
+    mps = np.zeros(natom, dtype=np.int32)
+    jxyz = np.zeros((3, n, natom), dtype=np.int32, order="F")
+    rxyz = np.zeros((3, n, natom), dtype=np.float64, order="F")
+    uv = np.zeros((n, m), dtype=np.float64, order="F")
+    ia = np.zeros(m, dtype=np.int32)
+    rinv = np.zeros(m, dtype=np.float64)
+    v = np.zeros(tuple(grid.num), dtype=np.float64, order="F") if (vpsl and not grid.periodic) else None
+    check(lib().sb200_init_ps_ky(*args, C.byref(nps), C.byref(nlma), P(mps, _ip), P(jxyz, _ip), P(rxyz), P(uv),
+                                 P(ia, _ip), P(rinv), P(v)))
+    return PPGrid(natom, n, m, mps, jxyz, rxyz, uv, ia, rinv), v

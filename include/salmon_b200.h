@@ -126,12 +126,14 @@ int sb200_set_pp(sb200_ctx* ctx, int natom, int nps, int nlma, const int* mps, c
  * cell); natom atoms of element kion[a] (1-based) at Rion(3, natom) (bohr).
  * Call once with mps ... rinv_uvu NULL: *nps and *nlma return the sizes; then
  * with arrays mps(natom), jxyz(3,nps,natom), rxyz(3,nps,natom), uv(nps,nlma),
- * ia_tbl(nlma), rinv_uvu(nlma) (the layout sb200_set_pp takes) and, for an
- * isolated grid, Vpsl(is:ie) or NULL.  Periodic grids: Vpsl must be NULL.
+ * ia_tbl(nlma), rinv_uvu(nlma) (the layout sb200_set_pp takes) and Vpsl(is:ie)
+ * or NULL (isolated grids: the local channel interpolated at each atom's
+ * distance; periodic: form factors, structure sum, inverse transforms).
  * Replaces: read_ps_KY and the radial set-up of input_pp
  * (src/atom/pp/input_pp.f90:96-341), making_ps_without_masking (:1111-1240),
  * init_ps with calc_nps / calc_jxyz / set_lma / calc_uv
- * (src/atom/pp/prep_pp.f90:22-525) and calc_Vpsl_isolated (:550-620).          */
+ * (src/atom/pp/prep_pp.f90:22-525), calc_Vpsl_isolated (:550-620) and
+ * calc_Vpsl_periodic (:798-974).                                                */
 int sb200_init_ps_ky(int nelem, const char* const* files, const int* lmax_ps, const int* lloc_ps, int periodic,
                      const int num[3], const int is[3], const double hgs[3], double hvol, int natom,
                      const int* kion, const double* Rion, int* nps, int* nlma, int* mps, int* jxyz, double* rxyz,

@@ -3,14 +3,17 @@ tables from Yabana-Bertsch pseudopotential files (`_rps.dat`, ps_format 'KY'):
 a numpy restatement of read_ps_KY (src/atom/pp/input_pp.f90:288-341), the
 radial domain and KB norms of input_pp (:96-193), making_ps_without_masking
 (:1111-1240), init_ps's calc_nps / calc_jxyz / set_lma / calc_uv
-(src/atom/pp/prep_pp.f90:22-525), calc_Vpsl_isolated (:550-620) and the natural
+(src/atom/pp/prep_pp.f90:22-525), calc_Vpsl_isolated (:550-620),
+calc_Vpsl_periodic (:798-974, with the transform tables of
+src/common/initialization.f90:632-784) and the natural
 cubic spline of src/math/salmon_math.f90:500-584 (its linear system solved, as
 the reference does, through the LU inverse of the dense matrix).  Arrays keep
 the reference's 1-based / 0-based index conventions in comments.
 
 Parity status: unpinned against reference outputs (the Fortran set-up cannot be
-run here); pinned by known answers in tests/test_pseudo_ky.py (the spline
-reproduces cubic polynomials, the KB norm of a hand-made file).
+run here); the spline is checked by its defining properties in
+tests/test_pseudo_ky.py (it passes through the nodes, first and second
+derivatives continuous, natural end conditions, straight lines exact).
 """
 from __future__ import annotations
 
@@ -139,6 +142,52 @@ class KyElement:
             self.coef.append(spline(xn, yn))
 
 
+def _vpsl_periodic(el, rion, kion, num, al):
+    """calc_Vpsl_periodic: zVG_ion per element by the midpoint rule on the
+    local channel, the structure sum with exp(-i G.R) / det A, then the inverse
+    transforms along z, y, x with egz / egy / egx; the real part."""
+    n0, n1, n2 = num
+    detA = al[0] * al[1] * al[2]
+
+    def fold(m, n):
+        return m - n if m - (n + 1) // 2 >= 0 else m
+
+    vt = np.zeros((n0, n1, n2), dtype=np.complex128)
+    for kz in range(n2):
+        for ky in range(n1):
+            for kx in range(n0):
+                g = np.array([fold(kx, n0) * 2 * np.pi / al[0], fold(ky, n1) * 2 * np.pi / al[1],
+                              fold(kz, n2) * 2 * np.pi / al[2]])
+                G2 = float(g @ g)
+                gzero = kx == 0 and ky == 0 and kz == 0
+                coef = 0.0 if gzero else 4 * np.pi / G2
+                gs = np.sqrt(G2)
+                acc = 0.0 + 0.0j
+                for a in range(rion.shape[1]):
+                    e = el[kion[a] - 1]
+                    s = 0.0
+                    for i in range(2, e.nrps + 1):
+                        r1 = 0.5 * (e.rad[i - 1] + e.rad[i - 2])
+                        dr = e.rad[i - 1] - e.rad[i - 2]
+                        vav = 0.5 * (e.vpp[i - 1, e.lref] + e.vpp[i - 2, e.lref])
+                        if gzero:
+                            s = s + 4 * np.pi * (r1 * r1 * vav + r1 * e.zps) * dr
+                        else:
+                            s = s + 4 * np.pi * np.sin(gs * r1) / gs * (r1 * vav + e.zps) * dr
+                    gd = float(g @ rion[:, a])
+                    acc = acc + (s - coef * e.zps) * (np.exp(-1j * gd) / detA)
+                vt[kx, ky, kz] = acc
+
+    def eg(n):  # eg[k, i] = exp(2 pi i (i)(k) / n), 0-based
+        k = np.arange(n)
+        return np.exp(2j * np.pi * np.outer(k, k) / n)
+
+    vt = np.einsum("ki,abk->abi", eg(n2), vt)   # z
+    vt = np.einsum("ki,akc->aic", eg(n1), vt)   # y
+    vt = np.einsum("ki,kbc->ibc", eg(n0), vt)   # x
+    return np.asfortranarray(vt.real)
+
+
 def init_ps_ky(files, lloc_ps, grid, rion, kion, lmax_ps=None):
     """(mps, jxyz, rxyz, uv, ia_tbl, rinv_uvu, Vpsl or None) as init_ps builds them."""
     periodic = bool(grid.periodic)
@@ -218,7 +267,9 @@ def init_ps_ky(files, lloc_ps, grid, rion, kion, lmax_ps=None):
                 uv[j, lma] = uvr * ylm(x, y, z, l, m)
             lma += 1
     vpsl = None
-    if not periodic:
+    if periodic:
+        vpsl = _vpsl_periodic(el, rion, kion, num, al)
+    else:
         vpsl = np.zeros(num, order="F")
         coord = [(np.arange(is_[d], ie[d] + 1) - (0.0 if num[d] % 2 == 1 else 0.5)) * hgs[d] for d in range(3)]
         X, Y, Z = np.meshgrid(*coord, indexing="ij")

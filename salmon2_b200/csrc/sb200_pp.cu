@@ -10,6 +10,7 @@
 //   init_ps: calc_nps / calc_jxyz src/atom/pp/prep_pp.f90:22-372
 //            set_lma / calc_uv    src/atom/pp/prep_pp.f90:374-525
 //   calc_Vpsl_isolated            src/atom/pp/prep_pp.f90:550-620
+//   calc_Vpsl_periodic            src/atom/pp/prep_pp.f90:798-974
 //   spline (natural cubic)        src/math/salmon_math.f90:500-584
 //   Ylm                           src/math/salmon_math.f90:386-426
 //
@@ -22,7 +23,8 @@
 // sign(anorm_l^2) hvol.  Projectors with anorm_l^2 = 0 (the local l) are left
 // out.  Vpsl of an isolated grid: the local channel v_lloc interpolated
 // linearly at each point's distance from every atom (beyond the file's grid,
-// -Zps / r) and summed over the atoms.
+// -Zps / r) and summed over the atoms; of a periodic grid: the form factors of
+// the local channel and the structure sum, transformed back to the grid.
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -228,7 +230,6 @@ extern "C" int sb200_init_ps_ky(int nelem, const char* const* files, const int* 
   if (nelem < 1 || !files || !lloc_ps || !num || !is || !hgs || natom < 0 || (natom > 0 && (!kion || !Rion)) ||
       !nps || !nlma)
     return set_error(SB200_ERR_INVALID_ARG, "sb200_init_ps_ky: null or inconsistent argument");
-  if (periodic && Vpsl) return set_error(SB200_ERR_UNSUPPORTED, "Vpsl is built here for isolated grids only");
   const int nrmax = periodic ? 3000 : 20000;  // read_pslfile, salmon_pp.f90:34-38
   std::vector<KyElement> el(nelem);
   for (int k = 0; k < nelem; ++k) {
@@ -343,7 +344,80 @@ extern "C" int sb200_init_ps_ky(int nelem, const char* const* files, const int* 
       }
     }
   }
-  if (Vpsl) {  // calc_Vpsl_isolated: linear interpolation of the local channel
+  if (Vpsl && periodic) {
+    // calc_Vpsl_periodic (prep_pp.f90:798-974, transforms without FFTE): per
+    // element the form factor of the local channel minus the Coulomb tail,
+    // zVG(G) = 4 pi sum_i sin(|G| r1) / |G| (r1 vloc_av + Zps) dr (G = 0:
+    // 4 pi sum_i (r1^2 vloc_av + r1 Zps) dr, midpoints r1), the structure sum
+    // V(G) = sum_a (zVG(G) - 4 pi / G^2 Zps) e^{-i G.R_a} / det A, then the
+    // inverse transforms along z, y, x with egz / egy / egx
+    // (initialization.f90:700-784); Vpsl = the real part.
+    const int n0 = num[0], n1 = num[1], n2 = num[2];
+    const long npts = (long)n0 * n1 * n2;
+    const double detA = al[0] * al[1] * al[2];
+    auto fold = [](int m, int n) { return (m - (n + 1) / 2 >= 0) ? m - n : m; };  // ix-1 -> folded index
+    std::vector<double> vre(npts, 0.0), vim(npts, 0.0);
+    std::vector<std::vector<double>> zvg(nelem);
+    for (int kz = 0; kz < n2; ++kz)
+      for (int ky = 0; ky < n1; ++ky)
+        for (int kx = 0; kx < n0; ++kx) {
+          const long q = kx + (long)n0 * (ky + (long)n1 * kz);
+          const double g[3] = {fold(kx, n0) * 2.0 * PP_PI / al[0], fold(ky, n1) * 2.0 * PP_PI / al[1],
+                               fold(kz, n2) * 2.0 * PP_PI / al[2]};
+          const double G2 = g[0] * g[0] + g[1] * g[1] + g[2] * g[2];
+          const bool gzero = kx == 0 && ky == 0 && kz == 0;
+          const double coef = gzero ? 0.0 : 4.0 * PP_PI / G2;
+          const double gsq = std::sqrt(G2);
+          double sr = 0.0, si = 0.0;
+          for (int a = 0; a < natom; ++a) {
+            const KyElement& e = el[kion[a] - 1];
+            double zv = 0.0;
+            for (int i2 = 2; i2 <= e.nrps; ++i2) {  // vloctbl(i) = vpp(i - 1, lref), i = 1..nrps
+              const double r1 = 0.5 * (e.rad[i2 - 1] + e.rad[i2 - 2]);
+              const double dr = e.rad[i2 - 1] - e.rad[i2 - 2];
+              const double vav = 0.5 * (e.vpp[e.lref][i2 - 1] + e.vpp[e.lref][i2 - 2]);
+              if (gzero) zv = zv + 4.0 * PP_PI * (r1 * r1 * vav + r1 * e.zps) * dr;
+              else zv = zv + 4.0 * PP_PI * std::sin(gsq * r1) / gsq * (r1 * vav + e.zps) * dr;
+            }
+            const double gd = g[0] * Rion[3 * a] + g[1] * Rion[3 * a + 1] + g[2] * Rion[3 * a + 2];
+            const double er = std::cos(gd) / detA, ei = -std::sin(gd) / detA;
+            const double w = zv - coef * e.zps;
+            sr = sr + w * er;
+            si = si + w * ei;
+          }
+          vre[q] = sr;
+          vim[q] = si;
+        }
+    // inverse transforms: z, then y, then x (each output the ordered sum over the axis)
+    auto pass = [&](int axis) {
+      const int n = axis == 0 ? n0 : axis == 1 ? n1 : n2;
+      std::vector<double> ore(npts), oim(npts);
+      for (int iz = 0; iz < n2; ++iz)
+        for (int iy = 0; iy < n1; ++iy)
+          for (int ix = 0; ix < n0; ++ix) {
+            const int out_i = axis == 0 ? ix : axis == 1 ? iy : iz;
+            double re = 0.0, im = 0.0;
+            for (int k = 0; k < n; ++k) {
+              const long q = axis == 0 ? k + (long)n0 * (iy + (long)n1 * iz)
+                                       : axis == 1 ? ix + (long)n0 * (k + (long)n1 * iz)
+                                                   : ix + (long)n0 * (iy + (long)n1 * k);
+              const double ang = 2.0 * PP_PI * (double)((long)out_i * k) / (double)n;
+              const double tr = std::cos(ang), ti = std::sin(ang);
+              re = re + (tr * vre[q] - ti * vim[q]);
+              im = im + (tr * vim[q] + ti * vre[q]);
+            }
+            const long p = ix + (long)n0 * (iy + (long)n1 * iz);
+            ore[p] = re;
+            oim[p] = im;
+          }
+      vre.swap(ore);
+      vim.swap(oim);
+    };
+    pass(2);
+    pass(1);
+    pass(0);
+    for (long p = 0; p < npts; ++p) Vpsl[p] = vre[p];
+  } else if (Vpsl) {  // calc_Vpsl_isolated: linear interpolation of the local channel
     const long npts = (long)num[0] * num[1] * num[2];
     for (long p = 0; p < npts; ++p) Vpsl[p] = 0.0;
     for (int a = 0; a < natom; ++a) {

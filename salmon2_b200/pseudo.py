@@ -1,7 +1,8 @@
 """Kleinman-Bylander tables and the isolated local potential from
 Yabana-Bertsch pseudopotential files (`_rps.dat`, ps_format = 'KY') through the
 library's host-side builder (sb200_init_ps_ky; input_pp.f90 read_ps_KY,
-making_ps_without_masking, prep_pp.f90 init_ps, calc_Vpsl_isolated)."""
+making_ps_without_masking, prep_pp.f90 init_ps, calc_Vpsl_isolated /
+calc_Vpsl_periodic)."""
 from __future__ import annotations
 
 import ctypes as C
@@ -19,7 +20,7 @@ def init_ps_ky(files, lloc_ps, grid, rion, kion, lmax_ps=None, vpsl=True):
     """files: one path per element; lloc_ps / lmax_ps: per element (Lloc_ps,
     Lmax_ps; lmax_ps None keeps the file's); grid: a synth.Grid (orthogonal);
     rion: (3, natom) bohr; kion: 1-based element of each atom.  Returns
-    (PPGrid, Vpsl (nx, ny, nz) Fortran order, or None on periodic grids / vpsl=False)."""
+    (PPGrid, Vpsl (nx, ny, nz) Fortran order, or None with vpsl=False)."""
     nelem = len(files)
     arr = (C.c_char_p * nelem)(*[str(f).encode() for f in files])
     lloc = np.ascontiguousarray(lloc_ps, dtype=np.int32)
@@ -42,7 +43,7 @@ def init_ps_ky(files, lloc_ps, grid, rion, kion, lmax_ps=None, vpsl=True):
     uv = np.zeros((n, m), dtype=np.float64, order="F")
     ia = np.zeros(m, dtype=np.int32)
     rinv = np.zeros(m, dtype=np.float64)
-    v = np.zeros(tuple(grid.num), dtype=np.float64, order="F") if (vpsl and not grid.periodic) else None
+    v = np.zeros(tuple(grid.num), dtype=np.float64, order="F") if vpsl else None
     check(lib().sb200_init_ps_ky(*args, C.byref(nps), C.byref(nlma), P(mps, _ip), P(jxyz, _ip), P(rxyz), P(uv),
                                  P(ia, _ip), P(rinv), P(v)))
     return PPGrid(natom, n, m, mps, jxyz, rxyz, uv, ia, rinv), v

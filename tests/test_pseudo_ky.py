@@ -2,7 +2,8 @@
 pseudopotential files (sb200_init_ps_ky; read_ps_KY, input_pp,
 making_ps_without_masking, init_ps, calc_Vpsl_isolated) against the oracle's
 numpy restatement (oracle/pseudo_ky.py), on CPU (the builder has no device
-code): the sphere tables bit for bit, uV, rinv_uvu and Vpsl to 1e-12, on
+code): the sphere tables bit for bit, uV and rinv_uvu to 1e-12, Vpsl (isolated
+by interpolation, periodic by form factors and transforms) to 1e-11, on
 isolated grids of odd and even extent and on a periodic cell whose spheres
 cross the boundary; the reference's own C and H files when the reference tree
 is present; known answers of the spline."""
@@ -30,7 +31,7 @@ def _compare(files, lloc, grid, rion, kion, lmax=None):
     if uv.size:
         assert np.max(np.abs(pp.uv - uv)) <= 1e-12 * np.max(np.abs(uv))
     if vref is not None:
-        assert np.max(np.abs(v - vref)) <= 1e-12 * np.max(np.abs(vref))
+        assert np.max(np.abs(v - vref)) <= 1e-11 * np.max(np.abs(vref))
     return pp, v
 
 
@@ -53,8 +54,9 @@ def test_periodic_tables_equal_oracle(tmp_path):
     g = synth.make_grid([12, 12, 12], 6.0 / 12, periodic=True)
     rion = np.array([[0.2, 5.9, 3.0], [3.1, 0.1, 5.8]]).T
     pp, v = _compare([fa], [1], g, rion, [1, 1])
-    assert v is None and pp.nlma == 2
+    assert pp.nlma == 2
     assert pp.mps.min() > 0
+    assert np.all(np.isfinite(v)) and abs(np.mean(v)) < np.max(np.abs(v))
 
 
 @pytest.mark.skipif(not os.path.exists(os.path.join(REF_PSEUDO, "C_rps.dat")),

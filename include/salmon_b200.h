@@ -160,6 +160,18 @@ int sb200_set_vec_Ac(sb200_ctx* ctx, const double vec_Ac[3]);
  * init_lattice (src/common/lattice.f90:23-75).                                */
 int sb200_set_lattice(sb200_ctx* ctx, const double rmatrix_B[9], const double coef_F[6]);
 
+/* Single-scale Maxwell-TDDFT: the microscopic vector potential Ac_micro(3, is:ie)
+ * (system%Ac_micro%v) and its divergence div_Ac(is:ie) (system%div_Ac%f), host
+ * or device, copied into the context.  hpsi and sb200_taylor then take the
+ * micro-A stencil: per point k + A(r) in the gradient term and in |k + A(r)|^2 / 2,
+ * plus -i div A / 2 (the deviation from the Coulomb gauge); the KB term as set
+ * by sb200_set_vec_Ac.  Call again whenever the field changes (the Maxwell
+ * update is the caller's).  Orthogonal lattices, FP64; NULL turns it off.
+ * Replaces: hpsi's single-scale branch (src/common/hamiltonian.f90:236-298)
+ * -> zstencil_microAc / zstencil_microAc_typical_seq
+ * (src/common/stencil.f90:268-283, src/common/zstencil_microac_core/typical/seq.f90). */
+int sb200_set_micro_ac(sb200_ctx* ctx, const double* Ac_micro, const double* div_Ac);
+
 /* Impulse kick of the initial orbitals: psi <- exp(i e_impulse epdir.r) psi
  * at every interior point of every orbital of the resident block psi (device
  * pointer), r the grid coordinate lg%coordinate of set_gridcoordinate.

@@ -36,6 +36,7 @@ class SboSystem(C.Structure):
         ("zekr", _dp),
         ("stencil_rgrid_mode", C.c_int),
         ("nonorth", C.c_int), ("rmatrix_B", C.c_double * 9), ("coef_F", C.c_double * 6),
+        ("ac_micro", _dp), ("div_ac", _dp),
     ]
 
 
@@ -141,6 +142,17 @@ class Oracle:
             self.s.vec_Ac[d] = float(ac[d])
         if self.sys.pp.nlma > 0:
             lib().sbo_update_kvector_nonlocalpt(C.byref(self.s))
+
+    def set_micro_ac(self, ac_micro, div_ac):
+        """system%Ac_micro%v (3, nx, ny, nz) and system%div_Ac%f (nx, ny, nz) for the
+        single-scale hpsi branch; None switches it off."""
+        if ac_micro is None:
+            self._acm = self._div = None
+            self.s.ac_micro = self.s.div_ac = None
+            return
+        self._acm = np.asfortranarray(ac_micro, dtype=np.float64)
+        self._div = np.asfortranarray(div_ac, dtype=np.float64)
+        self.s.ac_micro, self.s.div_ac = _p(self._acm), _p(self._div)
 
     def set_vec_Ac_local_only(self, ac):
         """Change system%vec_Ac without refreshing zekr (calc_current's order)."""

@@ -174,6 +174,54 @@ void zstencil_nonorth_one(const sbo_system* s, const Idx& I, const double* tpsi,
       }
 }
 
+// One orbital of the single-scale (microscopic A) stencil,
+// zstencil_microAc_typical_seq (zstencil_microac_core/typical/seq.f90): per
+// point kAc = k + Ac(r), v the Laplacian sums, w(d) the first derivatives
+// (coef_nab), htpsi = (V + lap0) psi - v/2 + |kAc|^2 psi / 2 - i kAc.w
+// - i div(Ac) psi / 2.
+void zstencil_microac_one(const sbo_system* s, const Idx& I, const double* tpsi, double* htpsi, const double* V,
+                          const double* k) {
+  const double* lapt = s->coef_lap;
+  const double* nab = s->coef_nab;
+  auto T = [&](int x, int y, int z) { return ld(tpsi, I.a(x, y, z)); };
+  for (int iz = s->is[2]; iz <= s->ie[2]; ++iz)
+    for (int iy = s->is[1]; iy <= s->ie[1]; ++iy)
+      for (int ix = s->is[0]; ix <= s->ie[0]; ++ix) {
+        const long r = I.r(ix, iy, iz);
+        const zc_t psi0 = T(ix, iy, iz);
+        double kAc[3];
+        for (int d = 0; d < 3; ++d) kAc[d] = k[d] + s->ac_micro[3 * r + d];
+        const double div = s->div_ac[r];
+        zc_t v(0.0, 0.0), w[3];
+        for (int d = 0; d < 3; ++d) {
+          zc_t vv(0.0, 0.0), ww(0.0, 0.0);
+          for (int q = 1; q <= 4; ++q) {
+            zc_t tp, tm;
+            if (d == 0) {
+              tp = T(I.X(ix + q), iy, iz);
+              tm = T(I.X(ix - q), iy, iz);
+            } else if (d == 1) {
+              tp = T(ix, I.Y(iy + q), iz);
+              tm = T(ix, I.Y(iy - q), iz);
+            } else {
+              tp = T(ix, iy, I.Z(iz + q));
+              tm = T(ix, iy, I.Z(iz - q));
+            }
+            vv = vv + rmul(lapt[4 * d + q - 1], tp + tm);
+            ww = ww + rmul(nab[4 * d + q - 1], tp - tm);
+          }
+          v = d == 0 ? vv : vv + v;
+          w[d] = ww;
+        }
+        const zc_t kw = rmul(kAc[0], w[0]) + rmul(kAc[1], w[1]) + rmul(kAc[2], w[2]);
+        const double k2 = kAc[0] * kAc[0] + kAc[1] * kAc[1] + kAc[2] * kAc[2];
+        // - zI kw = (kw_i, -kw_r); - zI 0.5 div psi0 = (0.5 div psi0_i, -0.5 div psi0_r)
+        const zc_t h = rmul(V[r] + s->coef_lap0, psi0) - rmul(0.5, v) + rmul(0.5 * k2, psi0) +
+                       zc_t(kw.imag(), -kw.real()) + zc_t(0.5 * div * psi0.imag(), -0.5 * div * psi0.real());
+        st(htpsi, I.a(ix, iy, iz), h);
+      }
+}
+
 // One orbital of the real 25-point stencil.  stencil.f90:30-80.
 void dstencil_one(const sbo_system* s, const Idx& I, const double* tpsi, double* htpsi,
                   const double* V, double lap0, const double* lapt, bool omp_grid) {
@@ -374,6 +422,18 @@ void sbo_hpsi(const sbo_system* s, const double* tpsi, double* htpsi) {
   Idx I(s);
   const bool grid_mode = s->stencil_rgrid_mode != 0;
   const long nxy = I.nx * I.ny * I.nz;
+  if (s->ac_micro) {  // single-scale branch, hamiltonian.f90:236-298
+#pragma omp parallel for collapse(3)
+    for (int ik = 1; ik <= s->nk; ++ik)
+      for (int io = 1; io <= s->no; ++io)
+        for (int is = 1; is <= s->nspin; ++is) {
+          const long o = I.orb(is, io, ik);
+          zstencil_microac_one(s, I, tpsi + 2 * I.vol * o, htpsi + 2 * I.vol * o, s->V_local + nxy * (is - 1),
+                               s->vec_k + 3 * (ik - 1));
+        }
+    if (s->nlma > 0) sbo_zpseudo(s, tpsi, htpsi);
+    return;
+  }
   if (s->nonorth) {
 #pragma omp parallel for collapse(3)
     for (int ik = 1; ik <= s->nk; ++ik)

@@ -74,6 +74,10 @@ typedef struct {
   int nonorth;
   double rmatrix_B[9];      /* (3,3) column-major                            */
   double coef_F[6];
+  /* single-scale Maxwell-TDDFT: system%Ac_micro%v (3, is:ie) and
+   * system%div_Ac%f (is:ie), or NULL (hamiltonian.f90:236-298)              */
+  const double *ac_micro;
+  const double *div_ac;
 } sbo_system;
 
 void sbo_set_threads(int n);

@@ -382,6 +382,8 @@ int sb200_ctx_destroy(sb200_ctx* c) {
   scf_free(c);
   pcg_free(c);
   dfree(c->d_nonorth);
+  dfree(c->d_acm);
+  dfree(c->d_divac);
   for (cudaEvent_t e : c->ev) cudaEventDestroy(e);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
   delete c;
@@ -768,6 +770,26 @@ int sb200_set_lattice(sb200_ctx* c, const double rmatrix_B[9], const double coef
     TRY(refresh_k(c));
     TRY(nonorth_prepare(c));  // the two-pass scratch at set-up, not inside a later capture
   }
+  return SB200_OK;
+}
+
+int sb200_set_micro_ac(sb200_ctx* c, const double* Ac_micro, const double* div_Ac) {
+  CHECK_CTX(c);
+  if (!c->g.set) return set_error(SB200_ERR_STATE, "sb200_set_grid has not been called");
+  DeviceGuard dg(c->device);
+  if (!Ac_micro || !div_Ac) {
+    c->microac = 0;
+    return SB200_OK;
+  }
+  if (c->g.nonorth)
+    return set_error(SB200_ERR_UNSUPPORTED, "a microscopic vector potential needs an orthogonal lattice");
+  const size_t n = (size_t)c->g.npts;
+  if (!c->d_acm) TRY(dalloc(&c->d_acm, 3 * n));
+  if (!c->d_divac) TRY(dalloc(&c->d_divac, n));
+  SB_CUDA(cudaMemcpyAsync(c->d_acm, Ac_micro, 3 * n * sizeof(double), cudaMemcpyDefault, c->stream));
+  SB_CUDA(cudaMemcpyAsync(c->d_divac, div_Ac, n * sizeof(double), cudaMemcpyDefault, c->stream));
+  SB_CUDA(cudaStreamSynchronize(c->stream));
+  c->microac = 1;
   return SB200_OK;
 }
 

@@ -182,6 +182,10 @@ struct sb200_ctx {
   // non-orthogonal H psi: first-pass H psi and the x / y first derivatives [3][norb][npts]
   double2* d_nonorth = nullptr;
   size_t nonorth_cap = 0;
+  // single-scale Maxwell-TDDFT (sb200_set_micro_ac): Ac_micro [npts][3] and div Ac [npts]
+  int microac = 0;
+  double* d_acm = nullptr;
+  double* d_divac = nullptr;
 };
 
 namespace sb200 {

@@ -666,7 +666,8 @@ __global__ void __launch_bounds__(256) k_energy_part(const double2* __restrict__
 
 // ttpsi of hpsi (the kinetic part) with the per-point kernel
 int launch_hpsi_kinetic(sb200_ctx* c, const double2* in, double2* tt) {
-  if (c->g.nonorth) return set_error(SB200_ERR_UNSUPPORTED, "ttpsi on a non-orthogonal lattice is not supported");
+  if (c->g.nonorth || c->microac)
+    return set_error(SB200_ERR_UNSUPPORTED, "ttpsi on a non-orthogonal lattice or with a microscopic A is not supported");
   const HArgs a = make_hargs(c, make_double2(0.0, 0.0));
   dim3 grid((unsigned)((c->g.npts + 255) / 256), c->orb.norb);
   k_hpsi<9><<<grid, 256, 0, c->stream>>>(in, tt, nullptr, a);
@@ -823,7 +824,103 @@ int launch_hpsi_nonorth(sb200_ctx* c, const HpsiLaunch& L) {
   return SB200_OK;
 }
 
+// ---------------------------------------------------------------------------
+// hpsi with a microscopic vector potential (single-scale Maxwell-TDDFT,
+// zstencil_microAc_typical_seq, zstencil_microac_core/typical/seq.f90; called
+// from hamiltonian.f90:236-298): per point kAc = k + Ac(r), h = (V + lap0) psi
+// - v/2 + |kAc|^2 psi / 2 - i kAc.w - i div(Ac) psi / 2 with v the Laplacian
+// sums and w_d the first derivatives (coef_nab); then the KB term and the
+// Taylor epilogue of MODE, one thread per point.
+// ---------------------------------------------------------------------------
+template <int MODE>
+__global__ void __launch_bounds__(256) k_hpsi_micro(const double2* __restrict__ in, double2* __restrict__ hout,
+                                                    double2* __restrict__ acc, HArgs a, NoArgs n,
+                                                    const double* __restrict__ acm, const double* __restrict__ divac,
+                                                    const double* __restrict__ vec_k, double lap0) {
+  const long p = blockIdx.x * 256L + threadIdx.x;
+  if (p >= a.npts) return;
+  const int o = blockIdx.y;
+  const int x = (int)(p % a.nx), y = (int)((p / a.nx) % a.ny), z = (int)(p / ((long)a.nx * a.ny));
+  const double2* src = in + (long)o * a.npts;
+  const int ik = o / a.nspin_no, ispin = o % a.nspin;
+  const long sy = a.nx, sz = (long)a.nx * a.ny;
+  double2 v = make_double2(0.0, 0.0), w[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    double2 vv = make_double2(0.0, 0.0), ww = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int s = 1; s <= ND; ++s) {
+      bool okp, okm;
+      long qp, qm;
+      if (d == 0) {
+        qp = p - x + nbr(x, s, a.nx, a.periodic, okp);
+        qm = p - x + nbr(x, -s, a.nx, a.periodic, okm);
+      } else if (d == 1) {
+        qp = p + (long)(nbr(y, s, a.ny, a.periodic, okp) - y) * sy;
+        qm = p + (long)(nbr(y, -s, a.ny, a.periodic, okm) - y) * sy;
+      } else {
+        qp = p + (long)(nbr(z, s, a.nz, a.periodic, okp) - z) * sz;
+        qm = p + (long)(nbr(z, -s, a.nz, a.periodic, okm) - z) * sz;
+      }
+      const double2 tp = ldz(src, qp, okp), tm = ldz(src, qm, okm);
+      vv = cadd(vv, cscal(a.lapt[4 * d + s - 1], cadd(tp, tm)));
+      ww = cadd(ww, cscal(n.nab[4 * d + s - 1], csub(tp, tm)));
+    }
+    v = d == 0 ? vv : cadd(vv, v);
+    w[d] = ww;
+  }
+  double kAc[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) kAc[d] = __ldg(vec_k + 3 * ik + d) + __ldg(acm + 3 * p + d);
+  const double div = __ldg(divac + p);
+  const double2 c = __ldg(src + p);
+  const double dg = __ldg(a.vloc + (long)ispin * a.npts + p) + lap0;
+  const double hk = 0.5 * (kAc[0] * kAc[0] + kAc[1] * kAc[1] + kAc[2] * kAc[2]);
+  const double2 kw = cadd(cadd(cscal(kAc[0], w[0]), cscal(kAc[1], w[1])), cscal(kAc[2], w[2]));
+  double2 h;
+  h.x = dg * c.x - 0.5 * v.x + hk * c.x + kw.y + 0.5 * div * c.y;
+  h.y = dg * c.y - 0.5 * v.y + hk * c.y - kw.x - 0.5 * div * c.x;
+  if (a.nlma > 0) {
+    const int pm = __ldg(a.pmap + p);
+    if (pm >= 0) {
+      const double2* pj = a.proj + (long)o * a.nlma;
+      const double2* zk = a.ent_zk + (a.phase_per_k ? (long)ik * a.nent : 0L);
+      const int e1 = (pm >> 8) + (pm & 255);
+      for (int e = pm >> 8; e < e1; ++e) h = cadd(h, cmul(pj[__ldg(a.ent_lma + e)], __ldg(zk + e)));
+    }
+  }
+  const long gi = (long)o * a.npts + p;
+  if (MODE <= 2) hout[gi] = h;
+  if (MODE == 1 || MODE == 4) acc[gi] = cadd(c, cmul(a.zc, h));
+  if (MODE == 2 || MODE == 3) acc[gi] = cadd(acc[gi], cmul(a.zc, h));
+}
+
+int launch_hpsi_micro(sb200_ctx* c, const HpsiLaunch& L) {
+  if (L.mode > 4) return set_error(SB200_ERR_UNSUPPORTED, "the single-scale hpsi has no mixed-precision modes");
+  const HArgs a = make_hargs(c, L.zc);
+  NoArgs n;
+  for (int i = 0; i < 6; ++i) n.F[i] = 0.0;
+  for (int i = 0; i < 12; ++i) n.nab[i] = c->g.coef_nab[i];
+  dim3 grid((unsigned)((c->g.npts + 255) / 256), c->orb.norb);
+  const double2* IN = (const double2*)L.in;
+  double2* HOUT = (double2*)L.hout;
+  const double lap0 = c->g.coef_lap0;
+#define SB_MICRO(M) \
+  k_hpsi_micro<M><<<grid, 256, 0, c->stream>>>(IN, HOUT, L.out, a, n, c->d_acm, c->d_divac, c->d_vec_k, lap0)
+  switch (L.mode) {
+    case 0: SB_MICRO(0); break;
+    case 1: SB_MICRO(1); break;
+    case 2: SB_MICRO(2); break;
+    case 3: SB_MICRO(3); break;
+    default: SB_MICRO(4); break;
+  }
+#undef SB_MICRO
+  SB_LAUNCH_CHECK("k_hpsi_micro");
+  return SB200_OK;
+}
+
 int launch_hpsi(sb200_ctx* c, const HpsiLaunch& L) {
+  if (c->microac) return launch_hpsi_micro(c, L);
   if (c->g.nonorth) return launch_hpsi_nonorth(c, L);
   if (c->stencil_variant == 1 || L.mode >= 5) return launch_hpsi_tiled(c, L);
   const double2* IN = (const double2*)L.in;

@@ -127,6 +127,12 @@ module salmon_b200
       type(c_ptr), value :: mps, jxyz, rxyz, uv, ia_tbl, rinv_uvu, Vpsl
     end function
 
+    integer(c_int) function sb200_set_micro_ac(ctx, Ac_micro, div_Ac) bind(c, name="sb200_set_micro_ac")
+      import
+      type(c_ptr), value :: ctx
+      real(c_double), intent(in) :: Ac_micro(3, *), div_Ac(*)
+    end function
+
     integer(c_int) function sb200_set_precision(ctx, mode) bind(c, name="sb200_set_precision")
       import
       type(c_ptr), value :: ctx

@@ -90,6 +90,16 @@ class Context:
         check(lib().sb200_set_pp(self.h, pp.natom, pp.nps, pp.nlma, _ptr(mps, _ip), _ptr(jxyz, _ip), _ptr(rxyz),
                                  _ptr(uv), _ptr(ia, _ip), _ptr(rinv)))
 
+    def set_micro_ac(self, ac_micro, div_ac):
+        """Single-scale hpsi (hamiltonian.f90:236-298): Ac_micro (3, nx, ny, nz)
+        and div_Ac (nx, ny, nz), Fortran order; None turns it off."""
+        if ac_micro is None:
+            check(lib().sb200_set_micro_ac(self.h, None, None))
+            return
+        a = np.asfortranarray(ac_micro, dtype=np.float64)
+        d = np.asfortranarray(div_ac, dtype=np.float64)
+        check(lib().sb200_set_micro_ac(self.h, C.c_void_p(a.ctypes.data), C.c_void_p(d.ctypes.data)))
+
     def set_vec_Ac(self, vec_Ac):
         a = np.ascontiguousarray(vec_Ac, dtype=np.float64)
         check(lib().sb200_set_vec_Ac(self.h, _ptr(a)))

@@ -283,3 +283,38 @@ def test_nonorthogonal_path_on_a_cubic_cell_equals_the_orthogonal_stencil():
         b.set_vec_Ac(ac)
         ha, hb = a.hpsi(s.psi), b.hpsi(s.psi)
         assert np.max(np.abs(ha - hb)) <= 1e-13 * np.max(np.abs(hb))
+
+
+def test_micro_ac_stencil_with_uniform_field_equals_the_macroscopic_stencil():
+    """zstencil_microAc with Ac(r) = A0 everywhere and div A = 0 is the
+    orthogonal stencil with vec_Ac = A0: |k + A0|^2 / 2 joins lap0 and (k + A0)
+    weights the gradient (hamiltonian.f90:146-155); KB term included."""
+    s = S.periodic_small()
+    a0 = np.array([0.021, -0.013, 0.034])
+    O1, O2 = Oracle(s), Oracle(s)
+    O1.set_vec_Ac(a0)
+    O2.set_vec_Ac(a0)
+    g = s.grid
+    O2.set_micro_ac(np.asfortranarray(np.broadcast_to(a0[:, None, None, None], (3,) + g.shape)),
+                    np.zeros(g.shape, order="F"))
+    h1, h2 = O1.hpsi(s.psi), O2.hpsi(s.psi)
+    assert np.max(np.abs(h1 - h2)) <= 1e-13 * np.max(np.abs(h1))
+
+
+def test_micro_ac_stencil_divergence_term():
+    """The -i div(A) psi / 2 term: two fields differing only in div A give
+    H psi differing by exactly -i (d1 - d2) psi / 2."""
+    s = S.no_pp(S.periodic_small())
+    g = s.grid
+    rng = np.random.default_rng(7)
+    acm = np.asfortranarray(rng.uniform(-0.02, 0.02, (3,) + g.shape))
+    d1 = np.asfortranarray(rng.uniform(-0.1, 0.1, g.shape))
+    O1, O2 = Oracle(s), Oracle(s)
+    O1.set_micro_ac(acm, d1)
+    O2.set_micro_ac(acm, np.zeros(g.shape, order="F"))
+    h1, h2 = O1.hpsi(s.psi), O2.hpsi(s.psi)
+    sl = g.interior_slices()
+    for ik in range(s.nk):
+        for io in range(s.no):
+            diff = (h1 - h2)[sl + (0, io, ik)]
+            assert np.max(np.abs(diff - (-0.5j) * d1 * s.psi[sl + (0, io, ik)])) <= 1e-13 * np.max(np.abs(h1))

@@ -166,11 +166,31 @@ int sb200_set_lattice(sb200_ctx* ctx, const double rmatrix_B[9], const double co
  * micro-A stencil: per point k + A(r) in the gradient term and in |k + A(r)|^2 / 2,
  * plus -i div A / 2 (the deviation from the Coulomb gauge); the KB term as set
  * by sb200_set_vec_Ac.  Call again whenever the field changes (the Maxwell
- * update is the caller's).  Orthogonal lattices, FP64; NULL turns it off.
+ * update is the caller's).  Orthogonal lattices, FP64; Ac_micro = NULL turns it
+ * off; div_Ac = NULL stands for a zero divergence (the symmetrized form below
+ * does not use it).
  * Replaces: hpsi's single-scale branch (src/common/hamiltonian.f90:236-298)
  * -> zstencil_microAc / zstencil_microAc_typical_seq
- * (src/common/stencil.f90:268-283, src/common/zstencil_microac_core/typical/seq.f90). */
+ * (src/common/stencil.f90:295-315, src/common/zstencil_microac_core/typical/seq.f90). */
 int sb200_set_micro_ac(sb200_ctx* ctx, const double* Ac_micro, const double* div_Ac);
+
+/* yn_symmetrized_stencil (1 = 'y', 0 = 'n', the default): the single-scale
+ * hpsi takes the symmetrized form, h = (V + lap0) psi - lap psi / 2
+ * + |k + A(r)|^2 psi / 2 - (i/2) ((k + A(r)).grad psi + div((k + A) psi)), the
+ * divergence formed with A at the neighbour points.
+ * Replaces: zstencil_microAc_symmetrized (src/common/stencil.f90:319-411), as
+ * hamiltonian.f90:239-256 selects it.                                          */
+int sb200_set_symmetrized_stencil(sb200_ctx* ctx, int yn);
+
+/* Electron-number current density of the orbitals psi (device), without the
+ * rho A / c term and without a nonlocal part: curr(3, is:ie) = sum_{k,o,s}
+ * rocc wtk (Im(conj(psi) grad psi) + vec_k |psi|^2), grad by coef_nab, into a
+ * host or device array; summed over the k-point shards when a communicator is
+ * set.  Synchronous.
+ * Replaces: calc_microscopic_current / micro_current
+ * (src/common/density_matrix.f90:726-845), called by time_evolution_step
+ * (src/rt/time_evolution_step.f90:175-182) for rt%j_e.                        */
+int sb200_calc_microscopic_current(sb200_ctx* ctx, const double* psi, double* curr);
 
 /* Impulse kick of the initial orbitals: psi <- exp(i e_impulse epdir.r) psi
  * at every interior point of every orbital of the resident block psi (device

@@ -37,6 +37,7 @@ class SboSystem(C.Structure):
         ("stencil_rgrid_mode", C.c_int),
         ("nonorth", C.c_int), ("rmatrix_B", C.c_double * 9), ("coef_F", C.c_double * 6),
         ("ac_micro", _dp), ("div_ac", _dp),
+        ("symmetrized", C.c_int),
     ]
 
 
@@ -58,7 +59,7 @@ def lib():
         for name in ("sbo_zstencil", "sbo_dstencil", "sbo_update_kvector_nonlocalpt", "sbo_zpseudo",
                      "sbo_dpseudo", "sbo_zprojections", "sbo_hpsi", "sbo_hpsi_tt", "sbo_calc_eigen_energy",
                      "sbo_hpsi_real", "sbo_taylor",
-                     "sbo_calc_density", "sbo_calc_current", "sbo_current_parts", "sbo_calc_dip",
+                     "sbo_calc_density", "sbo_calc_current", "sbo_calc_microscopic_current", "sbo_current_parts", "sbo_calc_dip",
                      "sbo_calc_Ac_ext_t", "sbo_rt_run", "sbo_set_threads", "sbo_get_threads",
                      "sbo_precond_real", "sbo_gscg_rwf", "sbo_gram_schmidt_real", "sbo_gram_schmidt_complex",
                      "sbo_subspace_diag_real", "sbo_inner_product_real", "sbo_exc_cor_pz", "sbo_poisson_coef",
@@ -143,14 +144,18 @@ class Oracle:
         if self.sys.pp.nlma > 0:
             lib().sbo_update_kvector_nonlocalpt(C.byref(self.s))
 
-    def set_micro_ac(self, ac_micro, div_ac):
+    def set_micro_ac(self, ac_micro, div_ac=None, symmetrized=False):
         """system%Ac_micro%v (3, nx, ny, nz) and system%div_Ac%f (nx, ny, nz) for the
-        single-scale hpsi branch; None switches it off."""
+        single-scale hpsi branch; None switches it off (div_ac None: zero).
+        symmetrized: yn_symmetrized_stencil = 'y'."""
+        self.s.symmetrized = 1 if symmetrized else 0
         if ac_micro is None:
             self._acm = self._div = None
             self.s.ac_micro = self.s.div_ac = None
             return
         self._acm = np.asfortranarray(ac_micro, dtype=np.float64)
+        if div_ac is None:
+            div_ac = np.zeros(self._acm.shape[1:])
         self._div = np.asfortranarray(div_ac, dtype=np.float64)
         self.s.ac_micro, self.s.div_ac = _p(self._acm), _p(self._div)
 
@@ -253,6 +258,13 @@ class Oracle:
         a = self._orb(psi)
         cur = np.zeros((3, self.sys.nspin), order="F")
         lib().sbo_calc_current(C.byref(self.s), _p(a), _p(cur))
+        return cur
+
+    def microscopic_current(self, psi):
+        """calc_microscopic_current: (3, nx, ny, nz), Fortran order."""
+        a = self._orb(psi)
+        cur = np.zeros((3,) + self.sys.grid.shape, order="F")
+        lib().sbo_calc_microscopic_current(C.byref(self.s), _p(a), _p(cur))
         return cur
 
     def current_parts(self, psi):

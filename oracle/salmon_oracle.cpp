@@ -222,6 +222,63 @@ void zstencil_microac_one(const sbo_system* s, const Idx& I, const double* tpsi,
       }
 }
 
+// One orbital of the symmetrized single-scale stencil, zstencil_microAc_symmetrized
+// (stencil.f90:319-411): kAc = k + Ac(r), v the Laplacian sums, w(d) the first
+// derivatives, x = sum_d sum_q nab(q,d) ((k_d + Ac_d(r + q e_d)) psi(r + q e_d)
+// - (k_d + Ac_d(r - q e_d)) psi(r - q e_d)), htpsi = (V + lap0) psi - v/2
+// + |kAc|^2 psi / 2 - (i/2) (kAc.w + x).  A neighbour outside an isolated grid
+// has psi = 0, so its product is zero whatever Ac holds there.
+void zstencil_microac_sym_one(const sbo_system* s, const Idx& I, const double* tpsi, double* htpsi,
+                              const double* V, const double* k) {
+  const double* lapt = s->coef_lap;
+  const double* nab = s->coef_nab;
+  auto T = [&](int x, int y, int z) { return ld(tpsi, I.a(x, y, z)); };
+  auto inside = [&](int x, int y, int z) {
+    return x >= s->is[0] && x <= s->ie[0] && y >= s->is[1] && y <= s->ie[1] && z >= s->is[2] && z <= s->ie[2];
+  };
+  auto A = [&](int d, int x, int y, int z) { return inside(x, y, z) ? s->ac_micro[3 * I.r(x, y, z) + d] : 0.0; };
+  for (int iz = s->is[2]; iz <= s->ie[2]; ++iz)
+    for (int iy = s->is[1]; iy <= s->ie[1]; ++iy)
+      for (int ix = s->is[0]; ix <= s->ie[0]; ++ix) {
+        const long r = I.r(ix, iy, iz);
+        const zc_t psi0 = T(ix, iy, iz);
+        double kAc[3];
+        for (int d = 0; d < 3; ++d) kAc[d] = k[d] + s->ac_micro[3 * r + d];
+        zc_t v(0.0, 0.0), w[3], x(0.0, 0.0);
+        for (int d = 0; d < 3; ++d) {
+          zc_t vv(0.0, 0.0), ww(0.0, 0.0), xx(0.0, 0.0);
+          for (int q = 1; q <= 4; ++q) {
+            int px = ix, py = iy, pz = iz, mx = ix, my = iy, mz = iz;
+            if (d == 0) {
+              px = I.X(ix + q);
+              mx = I.X(ix - q);
+            } else if (d == 1) {
+              py = I.Y(iy + q);
+              my = I.Y(iy - q);
+            } else {
+              pz = I.Z(iz + q);
+              mz = I.Z(iz - q);
+            }
+            const zc_t tp = T(px, py, pz), tm = T(mx, my, mz);
+            vv = vv + rmul(lapt[4 * d + q - 1], tp + tm);
+            ww = ww + rmul(nab[4 * d + q - 1], tp - tm);
+            xx = xx + rmul(nab[4 * d + q - 1],
+                           rmul(k[d] + A(d, px, py, pz), tp) - rmul(k[d] + A(d, mx, my, mz), tm));
+          }
+          v = d == 0 ? vv : vv + v;
+          w[d] = ww;
+          x = d == 0 ? xx : xx + x;
+        }
+        const zc_t kw = rmul(kAc[0], w[0]) + rmul(kAc[1], w[1]) + rmul(kAc[2], w[2]);
+        const zc_t t = kw + x;
+        const double k2 = kAc[0] * kAc[0] + kAc[1] * kAc[1] + kAc[2] * kAc[2];
+        // - (i/2) t = (t_i / 2, -t_r / 2)
+        const zc_t h = rmul(V[r] + s->coef_lap0, psi0) - rmul(0.5, v) + rmul(0.5 * k2, psi0) +
+                       zc_t(0.5 * t.imag(), -0.5 * t.real());
+        st(htpsi, I.a(ix, iy, iz), h);
+      }
+}
+
 // One orbital of the real 25-point stencil.  stencil.f90:30-80.
 void dstencil_one(const sbo_system* s, const Idx& I, const double* tpsi, double* htpsi,
                   const double* V, double lap0, const double* lapt, bool omp_grid) {
@@ -428,8 +485,12 @@ void sbo_hpsi(const sbo_system* s, const double* tpsi, double* htpsi) {
       for (int io = 1; io <= s->no; ++io)
         for (int is = 1; is <= s->nspin; ++is) {
           const long o = I.orb(is, io, ik);
-          zstencil_microac_one(s, I, tpsi + 2 * I.vol * o, htpsi + 2 * I.vol * o, s->V_local + nxy * (is - 1),
-                               s->vec_k + 3 * (ik - 1));
+          if (s->symmetrized)  // hamiltonian.f90:239-256
+            zstencil_microac_sym_one(s, I, tpsi + 2 * I.vol * o, htpsi + 2 * I.vol * o,
+                                     s->V_local + nxy * (is - 1), s->vec_k + 3 * (ik - 1));
+          else
+            zstencil_microac_one(s, I, tpsi + 2 * I.vol * o, htpsi + 2 * I.vol * o, s->V_local + nxy * (is - 1),
+                                 s->vec_k + 3 * (ik - 1));
         }
     if (s->nlma > 0) sbo_zpseudo(s, tpsi, htpsi);
     return;
@@ -613,6 +674,51 @@ void sbo_calc_density(const sbo_system* s, const double* psi, double* rho) {
           r[I.r(ix, iy, iz)] = acc;
         }
   }
+}
+
+// calc_microscopic_current (density_matrix.f90:726-845): per orbital
+// (k, o, spin in the reference's loop order) micro_current's
+// jw_d = Im(conj(psi) xtmp_d) + k_d |psi|^2, xtmp_d the coef_nab first
+// derivative, then wrk2 += jw rocc wtk at every point.
+void sbo_calc_microscopic_current(const sbo_system* s, const double* psi, double* curr) {
+  Idx I(s);
+  const double* nab = s->coef_nab;
+#pragma omp parallel for collapse(2)
+  for (int iz = s->is[2]; iz <= s->ie[2]; ++iz)
+    for (int iy = s->is[1]; iy <= s->ie[1]; ++iy)
+      for (int ix = s->is[0]; ix <= s->ie[0]; ++ix) {
+        double acc[3] = {0.0, 0.0, 0.0};
+        for (int ik = 1; ik <= s->nk; ++ik)
+          for (int io = 1; io <= s->no; ++io)
+            for (int is = 1; is <= s->nspin; ++is) {
+              const double* t = psi + 2 * I.vol * I.orb(is, io, ik);
+              const zc_t p = std::conj(ld(t, I.a(ix, iy, iz)));
+              const double ap = std::abs(p);
+              const double* k = s->vec_k + 3 * (ik - 1);
+              const double occ = s->rocc[(io - 1) + (long)s->no * ((ik - 1) + (long)s->nk * (is - 1))];
+              for (int d = 0; d < 3; ++d) {
+                zc_t tmp(0.0, 0.0);
+                for (int q = 1; q <= 4; ++q) {
+                  zc_t tp, tm;
+                  if (d == 0) {
+                    tp = ld(t, I.a(I.X(ix + q), iy, iz));
+                    tm = ld(t, I.a(I.X(ix - q), iy, iz));
+                  } else if (d == 1) {
+                    tp = ld(t, I.a(ix, I.Y(iy + q), iz));
+                    tm = ld(t, I.a(ix, I.Y(iy - q), iz));
+                  } else {
+                    tp = ld(t, I.a(ix, iy, I.Z(iz + q)));
+                    tm = ld(t, I.a(ix, iy, I.Z(iz - q)));
+                  }
+                  tmp = tmp + rmul(nab[4 * d + q - 1], tp - tm);
+                }
+                const double jw = (p * tmp).imag() + k[d] * ap * ap;
+                acc[d] = acc[d] + jw * occ * s->wtk[ik - 1];
+              }
+            }
+        const long r = I.r(ix, iy, iz);
+        for (int d = 0; d < 3; ++d) curr[3 * r + d] = acc[d];
+      }
 }
 
 // Per-orbital current pieces: stencil_current (density_matrix.f90:465-530) and

@@ -78,6 +78,8 @@ typedef struct {
    * system%div_Ac%f (is:ie), or NULL (hamiltonian.f90:236-298)              */
   const double *ac_micro;
   const double *div_ac;
+  /* yn_symmetrized_stencil = 'y': zstencil_microAc_symmetrized (div_ac unused) */
+  int symmetrized;
 } sbo_system;
 
 void sbo_set_threads(int n);
@@ -126,6 +128,8 @@ void sbo_calc_current(const sbo_system* s, const double* psi, double* curr);
 /* per-orbital pieces of calc_current: out(10, norb) =
  * [rtmp, Im-sums*2 (x,y,z) (before BT), jw(3) nonlocal, j_total(3) weighted] */
 void sbo_current_parts(const sbo_system* s, const double* psi, double* out);
+/* calc_microscopic_current (density_matrix.f90:726-845) -> curr(3, is:ie) */
+void sbo_calc_microscopic_current(const sbo_system* s, const double* psi, double* curr);
 /* calc_dip (dip.f90:114-225): rbox(4) */
 void sbo_calc_dip(const sbo_system* s, const double* rho, double* rbox);
 

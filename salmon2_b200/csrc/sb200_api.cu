@@ -384,6 +384,7 @@ int sb200_ctx_destroy(sb200_ctx* c) {
   dfree(c->d_nonorth);
   dfree(c->d_acm);
   dfree(c->d_divac);
+  dfree(c->d_mcur);
   for (cudaEvent_t e : c->ev) cudaEventDestroy(e);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
   delete c;
@@ -777,7 +778,7 @@ int sb200_set_micro_ac(sb200_ctx* c, const double* Ac_micro, const double* div_A
   CHECK_CTX(c);
   if (!c->g.set) return set_error(SB200_ERR_STATE, "sb200_set_grid has not been called");
   DeviceGuard dg(c->device);
-  if (!Ac_micro || !div_Ac) {
+  if (!Ac_micro) {
     c->microac = 0;
     return SB200_OK;
   }
@@ -787,9 +788,40 @@ int sb200_set_micro_ac(sb200_ctx* c, const double* Ac_micro, const double* div_A
   if (!c->d_acm) TRY(dalloc(&c->d_acm, 3 * n));
   if (!c->d_divac) TRY(dalloc(&c->d_divac, n));
   SB_CUDA(cudaMemcpyAsync(c->d_acm, Ac_micro, 3 * n * sizeof(double), cudaMemcpyDefault, c->stream));
-  SB_CUDA(cudaMemcpyAsync(c->d_divac, div_Ac, n * sizeof(double), cudaMemcpyDefault, c->stream));
+  if (div_Ac)
+    SB_CUDA(cudaMemcpyAsync(c->d_divac, div_Ac, n * sizeof(double), cudaMemcpyDefault, c->stream));
+  else
+    SB_CUDA(cudaMemsetAsync(c->d_divac, 0, n * sizeof(double), c->stream));
   SB_CUDA(cudaStreamSynchronize(c->stream));
   c->microac = 1;
+  return SB200_OK;
+}
+
+int sb200_set_symmetrized_stencil(sb200_ctx* c, int yn) {
+  CHECK_CTX(c);
+  if (yn != 0 && yn != 1) return set_error(SB200_ERR_INVALID_ARG, "yn_symmetrized_stencil is 0 or 1");
+  c->micro_sym = yn;
+  return SB200_OK;
+}
+
+int sb200_calc_microscopic_current(sb200_ctx* c, const double* psi, double* curr) {
+  CHECK_CTX(c);
+  TRY(require_ready(c, false));
+  if (!psi || !curr) return set_error(SB200_ERR_INVALID_ARG, "null argument");
+  DeviceGuard dg(c->device);
+  const size_t n3 = 3 * (size_t)c->g.npts;
+  const size_t need = n3 + micro_current_part_len(c);
+  if (c->mcur_cap < need) {
+    dfree(c->d_mcur);
+    c->mcur_cap = 0;
+    TRY(dalloc(&c->d_mcur, need));
+    c->mcur_cap = need;
+  }
+  double* out = is_device_ptr(curr) ? curr : c->d_mcur;
+  TRY(launch_micro_current(c, (const double2*)psi, out, c->d_mcur + n3));
+  TRY(shard_sum(c, out, n3));  // comm_summation over icomm_ko
+  if (out != curr) SB_CUDA(cudaMemcpyAsync(curr, out, n3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  SB_CUDA(cudaStreamSynchronize(c->stream));
   return SB200_OK;
 }
 

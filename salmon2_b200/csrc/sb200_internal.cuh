@@ -184,8 +184,12 @@ struct sb200_ctx {
   size_t nonorth_cap = 0;
   // single-scale Maxwell-TDDFT (sb200_set_micro_ac): Ac_micro [npts][3] and div Ac [npts]
   int microac = 0;
+  int micro_sym = 0;  // sb200_set_symmetrized_stencil
   double* d_acm = nullptr;
   double* d_divac = nullptr;
+  // microscopic current (sb200_calc_microscopic_current): chunk sums and the result
+  double* d_mcur = nullptr;
+  size_t mcur_cap = 0;
 };
 
 namespace sb200 {
@@ -266,6 +270,9 @@ int launch_finalize(sb200_ctx* c, int itt_host, int nt, int trans_longi, double 
 // kind >= 0: each launch bracketed for sb200_kernel_times (SB200_KIND_*)
 int launch_density(sb200_ctx* c, const double2* psi, double* rho, int kind = -1);
 int density_prepare(sb200_ctx* c);
+// microscopic current [npts][3] into curr (device); part: micro_current_part_len(c) doubles
+size_t micro_current_part_len(const sb200_ctx* c);
+int launch_micro_current(sb200_ctx* c, const double2* psi, double* curr, double* part);
 int launch_dip(sb200_ctx* c, const double* rho, double* d_out4);
 int launch_relayout(sb200_ctx* c, const void* src, void* dst, int norb_chunk, bool to_ref);
 // time-loop histories of capacity nt (sb200_api.cu)

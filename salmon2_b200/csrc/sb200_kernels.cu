@@ -831,8 +831,13 @@ int launch_hpsi_nonorth(sb200_ctx* c, const HpsiLaunch& L) {
 // - v/2 + |kAc|^2 psi / 2 - i kAc.w - i div(Ac) psi / 2 with v the Laplacian
 // sums and w_d the first derivatives (coef_nab); then the KB term and the
 // Taylor epilogue of MODE, one thread per point.
+// SYM (yn_symmetrized_stencil = 'y', zstencil_microAc_symmetrized,
+// stencil.f90:319-411): no div term; instead the divergence of (k + Ac) psi
+// taken with Ac at the neighbour points, X = sum_d sum_s nab(s,d)
+// ((k_d + Ac_d(r + s e_d)) psi(r + s e_d) - (k_d + Ac_d(r - s e_d)) psi(r - s e_d)),
+// and h = (V + lap0) psi - v/2 + |kAc|^2 psi / 2 - (i/2) (kAc.w + X).
 // ---------------------------------------------------------------------------
-template <int MODE>
+template <int MODE, int SYM>
 __global__ void __launch_bounds__(256) k_hpsi_micro(const double2* __restrict__ in, double2* __restrict__ hout,
                                                     double2* __restrict__ acc, HArgs a, NoArgs n,
                                                     const double* __restrict__ acm, const double* __restrict__ divac,
@@ -844,10 +849,11 @@ __global__ void __launch_bounds__(256) k_hpsi_micro(const double2* __restrict__ 
   const double2* src = in + (long)o * a.npts;
   const int ik = o / a.nspin_no, ispin = o % a.nspin;
   const long sy = a.nx, sz = (long)a.nx * a.ny;
-  double2 v = make_double2(0.0, 0.0), w[3];
+  double2 v = make_double2(0.0, 0.0), w[3], X = make_double2(0.0, 0.0);
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
-    double2 vv = make_double2(0.0, 0.0), ww = make_double2(0.0, 0.0);
+    double2 vv = make_double2(0.0, 0.0), ww = make_double2(0.0, 0.0), xx = make_double2(0.0, 0.0);
+    const double kd = SYM ? __ldg(vec_k + 3 * ik + d) : 0.0;
 #pragma unroll
     for (int s = 1; s <= ND; ++s) {
       bool okp, okm;
@@ -865,21 +871,33 @@ __global__ void __launch_bounds__(256) k_hpsi_micro(const double2* __restrict__ 
       const double2 tp = ldz(src, qp, okp), tm = ldz(src, qm, okm);
       vv = cadd(vv, cscal(a.lapt[4 * d + s - 1], cadd(tp, tm)));
       ww = cadd(ww, cscal(n.nab[4 * d + s - 1], csub(tp, tm)));
+      if (SYM) {  // outside an isolated grid psi is zero, and so is the product
+        const double ap = okp ? kd + __ldg(acm + 3 * qp + d) : 0.0;
+        const double am = okm ? kd + __ldg(acm + 3 * qm + d) : 0.0;
+        xx = cadd(xx, cscal(n.nab[4 * d + s - 1], csub(cscal(ap, tp), cscal(am, tm))));
+      }
     }
     v = d == 0 ? vv : cadd(vv, v);
     w[d] = ww;
+    if (SYM) X = d == 0 ? xx : cadd(xx, X);
   }
   double kAc[3];
 #pragma unroll
   for (int d = 0; d < 3; ++d) kAc[d] = __ldg(vec_k + 3 * ik + d) + __ldg(acm + 3 * p + d);
-  const double div = __ldg(divac + p);
   const double2 c = __ldg(src + p);
   const double dg = __ldg(a.vloc + (long)ispin * a.npts + p) + lap0;
   const double hk = 0.5 * (kAc[0] * kAc[0] + kAc[1] * kAc[1] + kAc[2] * kAc[2]);
   const double2 kw = cadd(cadd(cscal(kAc[0], w[0]), cscal(kAc[1], w[1])), cscal(kAc[2], w[2]));
   double2 h;
-  h.x = dg * c.x - 0.5 * v.x + hk * c.x + kw.y + 0.5 * div * c.y;
-  h.y = dg * c.y - 0.5 * v.y + hk * c.y - kw.x - 0.5 * div * c.x;
+  if (SYM) {
+    const double2 t = cadd(kw, X);
+    h.x = dg * c.x - 0.5 * v.x + hk * c.x + 0.5 * t.y;
+    h.y = dg * c.y - 0.5 * v.y + hk * c.y - 0.5 * t.x;
+  } else {
+    const double div = __ldg(divac + p);
+    h.x = dg * c.x - 0.5 * v.x + hk * c.x + kw.y + 0.5 * div * c.y;
+    h.y = dg * c.y - 0.5 * v.y + hk * c.y - kw.x - 0.5 * div * c.x;
+  }
   if (a.nlma > 0) {
     const int pm = __ldg(a.pmap + p);
     if (pm >= 0) {
@@ -905,17 +923,136 @@ int launch_hpsi_micro(sb200_ctx* c, const HpsiLaunch& L) {
   const double2* IN = (const double2*)L.in;
   double2* HOUT = (double2*)L.hout;
   const double lap0 = c->g.coef_lap0;
-#define SB_MICRO(M) \
-  k_hpsi_micro<M><<<grid, 256, 0, c->stream>>>(IN, HOUT, L.out, a, n, c->d_acm, c->d_divac, c->d_vec_k, lap0)
-  switch (L.mode) {
-    case 0: SB_MICRO(0); break;
-    case 1: SB_MICRO(1); break;
-    case 2: SB_MICRO(2); break;
-    case 3: SB_MICRO(3); break;
-    default: SB_MICRO(4); break;
+#define SB_MICRO(M, S) \
+  k_hpsi_micro<M, S><<<grid, 256, 0, c->stream>>>(IN, HOUT, L.out, a, n, c->d_acm, c->d_divac, c->d_vec_k, lap0)
+#define SB_MICRO_MODES(S)        \
+  switch (L.mode) {              \
+    case 0: SB_MICRO(0, S); break; \
+    case 1: SB_MICRO(1, S); break; \
+    case 2: SB_MICRO(2, S); break; \
+    case 3: SB_MICRO(3, S); break; \
+    default: SB_MICRO(4, S); break; \
   }
+  if (c->micro_sym) {
+    SB_MICRO_MODES(1)
+  } else {
+    SB_MICRO_MODES(0)
+  }
+#undef SB_MICRO_MODES
 #undef SB_MICRO
   SB_LAUNCH_CHECK("k_hpsi_micro");
+  return SB200_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Microscopic current density of the single-scale theory,
+// calc_microscopic_current / micro_current (density_matrix.f90:726-845):
+// j_d(r) = sum_{k,o,s} rocc wtk (Im(conj(psi) dpsi_d) + k_d |psi|^2) with dpsi_d
+// the coef_nab first derivative and k = vec_k (no A: the electron number
+// current without rho A / c; no nonlocal part).  A block is 32 points x 8
+// orbital slices of one chunk; slice y sums orbitals o0 + y, o0 + y + 8, ...
+// in orbital order (k, o, spin as the reference's loops); the slice sums are
+// added in slice order, the chunk sums (part[chunk][p][3]) in chunk order by
+// k_micro_current_sum.  The chunk count depends only on the grid and orbital
+// counts, so the summation order is fixed.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_micro_current(const double2* __restrict__ in, double* __restrict__ part,
+                                                       HArgs a, NoArgs n, const double* __restrict__ vec_k,
+                                                       const double* __restrict__ weight, int norb, int nper) {
+  __shared__ double red[3][8][32];
+  const long p = blockIdx.x * 32L + threadIdx.x;
+  const int o0 = blockIdx.y * nper, o1 = min(norb, o0 + nper);
+  double j[3] = {0.0, 0.0, 0.0};
+  if (p < a.npts) {
+    const int x = (int)(p % a.nx), y = (int)((p / a.nx) % a.ny), z = (int)(p / ((long)a.nx * a.ny));
+    const long sy = a.nx, sz = (long)a.nx * a.ny;
+    for (int o = o0 + (int)threadIdx.y; o < o1; o += 8) {
+      const double2* src = in + (long)o * a.npts;
+      const int ik = o / a.nspin_no;
+      const double2 c = __ldg(src + p);
+      const double cc = c.x * c.x + c.y * c.y;
+      const double wo = __ldg(weight + o);
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        double2 t = make_double2(0.0, 0.0);
+#pragma unroll
+        for (int s = 1; s <= ND; ++s) {
+          bool okp, okm;
+          long qp, qm;
+          if (d == 0) {
+            qp = p - x + nbr(x, s, a.nx, a.periodic, okp);
+            qm = p - x + nbr(x, -s, a.nx, a.periodic, okm);
+          } else if (d == 1) {
+            qp = p + (long)(nbr(y, s, a.ny, a.periodic, okp) - y) * sy;
+            qm = p + (long)(nbr(y, -s, a.ny, a.periodic, okm) - y) * sy;
+          } else {
+            qp = p + (long)(nbr(z, s, a.nz, a.periodic, okp) - z) * sz;
+            qm = p + (long)(nbr(z, -s, a.nz, a.periodic, okm) - z) * sz;
+          }
+          t = cadd(t, cscal(n.nab[4 * d + s - 1], csub(ldz(src, qp, okp), ldz(src, qm, okm))));
+        }
+        // Im(conj(c) t) + k_d |c|^2
+        const double jw = (c.x * t.y - c.y * t.x) + __ldg(vec_k + 3 * ik + d) * cc;
+        j[d] += jw * wo;
+      }
+    }
+  }
+#pragma unroll
+  for (int d = 0; d < 3; ++d) red[d][threadIdx.y][threadIdx.x] = j[d];
+  __syncthreads();
+  if (threadIdx.y < 3 && p < a.npts) {
+    const int d = threadIdx.y;
+    double t = red[d][0][threadIdx.x];
+    for (int k = 1; k < 8; ++k) t += red[d][k][threadIdx.x];
+    part[((long)blockIdx.y * a.npts + p) * 3 + d] = t;
+  }
+}
+
+__global__ void k_micro_current_sum(const double* __restrict__ part, double* __restrict__ curr, long n, int nchunk) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    double acc = 0.0;
+    for (int c = 0; c < nchunk; ++c) acc += part[(long)c * n + i];
+    curr[i] = acc;
+  }
+}
+
+// curr [npts][3] (device) of the orbitals psi; part: scratch of
+// micro_current_part_len(c) doubles
+void micro_current_chunks(const sb200_ctx* c, long* pblocks, int* nchunk, int* nper) {
+  const long pb = (c->g.npts + 31) / 32;
+  const int norb = c->orb.norb;
+  long want = (2L * 148 + pb - 1) / pb;  // about two blocks per SM
+  long cap = (norb + 7) / 8;             // at least eight orbitals per chunk
+  if (want > cap) want = cap;
+  if (want < 1) want = 1;
+  const int per = (int)((norb + want - 1) / want);
+  *pblocks = pb;
+  *nper = per;
+  *nchunk = (norb + per - 1) / per;
+}
+
+size_t micro_current_part_len(const sb200_ctx* c) {
+  long pb;
+  int nchunk, nper;
+  micro_current_chunks(c, &pb, &nchunk, &nper);
+  return (size_t)nchunk * (size_t)c->g.npts * 3;
+}
+
+int launch_micro_current(sb200_ctx* c, const double2* psi, double* curr, double* part) {
+  long pb;
+  int nchunk, nper;
+  micro_current_chunks(c, &pb, &nchunk, &nper);
+  const HArgs a = make_hargs(c, make_double2(0.0, 0.0));
+  NoArgs n;
+  for (int i = 0; i < 6; ++i) n.F[i] = 0.0;
+  for (int i = 0; i < 12; ++i) n.nab[i] = c->g.coef_nab[i];
+  k_micro_current<<<dim3((unsigned)pb, (unsigned)nchunk), dim3(32, 8), 0, c->stream>>>(psi, part, a, n, c->d_vec_k,
+                                                                                      c->d_weight, c->orb.norb, nper);
+  const long n3 = 3L * c->g.npts;
+  long sblocks = (n3 + 255) / 256;
+  if (sblocks > 148L * 8) sblocks = 148L * 8;
+  k_micro_current_sum<<<(unsigned)sblocks, 256, 0, c->stream>>>(part, curr, n3, nchunk);
+  SB_LAUNCH_CHECK("k_micro_current");
   return SB200_OK;
 }
 

@@ -133,6 +133,19 @@ module salmon_b200
       real(c_double), intent(in) :: Ac_micro(3, *), div_Ac(*)
     end function
 
+    integer(c_int) function sb200_set_symmetrized_stencil(ctx, yn) bind(c, name="sb200_set_symmetrized_stencil")
+      import
+      type(c_ptr), value :: ctx
+      integer(c_int), value :: yn
+    end function
+
+    integer(c_int) function sb200_calc_microscopic_current(ctx, psi, curr) &
+        bind(c, name="sb200_calc_microscopic_current")
+      import
+      type(c_ptr), value :: ctx, psi
+      real(c_double), intent(inout) :: curr(3, *)
+    end function
+
     integer(c_int) function sb200_set_precision(ctx, mode) bind(c, name="sb200_set_precision")
       import
       type(c_ptr), value :: ctx

@@ -90,15 +90,27 @@ class Context:
         check(lib().sb200_set_pp(self.h, pp.natom, pp.nps, pp.nlma, _ptr(mps, _ip), _ptr(jxyz, _ip), _ptr(rxyz),
                                  _ptr(uv), _ptr(ia, _ip), _ptr(rinv)))
 
-    def set_micro_ac(self, ac_micro, div_ac):
+    def set_micro_ac(self, ac_micro, div_ac=None, symmetrized=False):
         """Single-scale hpsi (hamiltonian.f90:236-298): Ac_micro (3, nx, ny, nz)
-        and div_Ac (nx, ny, nz), Fortran order; None turns it off."""
+        and div_Ac (nx, ny, nz), Fortran order; None turns it off (div_ac None:
+        zero).  symmetrized: yn_symmetrized_stencil = 'y'
+        (zstencil_microAc_symmetrized, stencil.f90:319-411)."""
+        check(lib().sb200_set_symmetrized_stencil(self.h, 1 if symmetrized else 0))
         if ac_micro is None:
             check(lib().sb200_set_micro_ac(self.h, None, None))
             return
         a = np.asfortranarray(ac_micro, dtype=np.float64)
-        d = np.asfortranarray(div_ac, dtype=np.float64)
-        check(lib().sb200_set_micro_ac(self.h, C.c_void_p(a.ctypes.data), C.c_void_p(d.ctypes.data)))
+        d = None if div_ac is None else np.asfortranarray(div_ac, dtype=np.float64)
+        check(lib().sb200_set_micro_ac(self.h, C.c_void_p(a.ctypes.data),
+                                       None if d is None else C.c_void_p(d.ctypes.data)))
+
+    def calc_microscopic_current(self, psi):
+        """calc_microscopic_current (density_matrix.f90:726-845): (3, nx, ny, nz),
+        Fortran order."""
+        g = self.sys.grid
+        cur = np.zeros((3,) + g.shape, order="F")
+        check(lib().sb200_calc_microscopic_current(self.h, C.c_void_p(psi.data_ptr()), C.c_void_p(cur.ctypes.data)))
+        return cur
 
     def set_vec_Ac(self, vec_Ac):
         a = np.ascontiguousarray(vec_Ac, dtype=np.float64)

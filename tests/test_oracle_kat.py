@@ -318,3 +318,81 @@ def test_micro_ac_stencil_divergence_term():
         for io in range(s.no):
             diff = (h1 - h2)[sl + (0, io, ik)]
             assert np.max(np.abs(diff - (-0.5j) * d1 * s.psi[sl + (0, io, ik)])) <= 1e-13 * np.max(np.abs(h1))
+
+
+def _micro_field(shape, seed, amp=0.03):
+    rng = np.random.default_rng(seed)
+    return np.asfortranarray(rng.uniform(-amp, amp, (3,) + tuple(shape)))
+
+
+def test_symmetrized_micro_ac_stencil_with_uniform_field_equals_the_plain_form():
+    """zstencil_microAc_symmetrized with Ac(r) = A0: the divergence of (k + A0)
+    psi is (k + A0).grad psi, so -(i/2)(kAc.w + x) = -i kAc.w, the plain
+    zstencil_microAc with div A = 0 (stencil.f90:319-411 against :295-315)."""
+    s = S.periodic_small()
+    g = s.grid
+    a0 = np.array([0.021, -0.013, 0.034])
+    field = np.asfortranarray(np.broadcast_to(a0[:, None, None, None], (3,) + g.shape))
+    O1, O2 = Oracle(s), Oracle(s)
+    O1.set_micro_ac(field, np.zeros(g.shape, order="F"))
+    O2.set_micro_ac(field, None, symmetrized=True)
+    h1, h2 = O1.hpsi(s.psi), O2.hpsi(s.psi)
+    assert np.max(np.abs(h1 - h2)) <= 1e-13 * np.max(np.abs(h1))
+
+
+def _hermitian_defect(O, s, phi, psi):
+    """max over orbitals of |<phi|H psi> - conj(<psi|H phi>)| / |<phi|H psi>|-scale"""
+    sl = s.grid.interior_slices()
+    hpsi, hphi = O.hpsi(psi), O.hpsi(phi)
+    worst, scale = 0.0, 0.0
+    for o in np.ndindex(*psi.shape[3:]):
+        a = np.vdot(phi[sl + o], hpsi[sl + o])
+        b = np.conj(np.vdot(psi[sl + o], hphi[sl + o]))
+        worst = max(worst, abs(a - b))
+        scale = max(scale, np.linalg.norm(phi[sl + o]) * np.linalg.norm(hpsi[sl + o]))
+    return worst / scale
+
+
+def test_symmetrized_micro_ac_stencil_is_hermitian():
+    """With a non-uniform A(r) on a periodic grid the symmetrized operator is
+    Hermitian to rounding ((k + A).D + D (k + A) is real antisymmetric for the
+    antisymmetric difference D), while the plain form is not (A D - D A)."""
+    s = S.periodic_small()
+    g = s.grid
+    field = _micro_field(g.shape, 21)
+    rng = np.random.default_rng(22)
+    phi = np.asfortranarray(rng.standard_normal(s.psi.shape) + 1j * rng.standard_normal(s.psi.shape))
+    Os, Op = Oracle(s), Oracle(s)
+    Os.set_micro_ac(field, None, symmetrized=True)
+    Op.set_micro_ac(field, np.zeros(g.shape, order="F"))
+    assert _hermitian_defect(Os, s, phi, s.psi) < 1e-14
+    assert _hermitian_defect(Op, s, phi, s.psi) > 1e-6
+
+
+def test_microscopic_current_of_lattice_plane_waves():
+    """calc_microscopic_current (density_matrix.f90:726-845) of orbitals
+    c_o exp(i q_o.r), q on the grid: D psi = i psi sum_s 2 nab(s) sin(q s h),
+    so j_d(r) = sum_o rocc wtk |c_o|^2 (sum_s 2 nab(s,d) sin(q_d s h_d) + k_d)
+    at every point."""
+    s = S.periodic_small(nspin=2)
+    g = s.grid
+    rng = np.random.default_rng(23)
+    psi = np.zeros(s.psi.shape, dtype=np.complex128, order="F")
+    sl = g.interior_slices()
+    X = np.meshgrid(*[g.coordinate(d) for d in range(3)], indexing="ij")
+    want = np.zeros(3)
+    for ik in range(s.nk):
+        for io in range(s.no):
+            for isp in range(s.nspin):
+                m = rng.integers(-3, 4, 3)
+                q = 2 * np.pi * m / (g.num * g.hgs)
+                c = rng.uniform(0.2, 1.0) * np.exp(1j * rng.uniform(0, 2 * np.pi))
+                psi[sl + (isp, io, ik)] = c * np.exp(1j * (q[0] * X[0] + q[1] * X[1] + q[2] * X[2]))
+                w = s.rocc[io, ik, isp] * s.wtk[ik]
+                for d in range(3):
+                    sfac = sum(2 * g.coef_nab[j, d] * np.sin(q[d] * (j + 1) * g.hgs[d]) for j in range(4))
+                    want[d] += w * abs(c) ** 2 * (sfac + s.vec_k[d, ik])
+    cur = Oracle(s).microscopic_current(psi)
+    assert cur.shape == (3,) + g.shape
+    for d in range(3):
+        assert np.max(np.abs(cur[d] - want[d])) <= 1e-12 * max(1.0, np.max(np.abs(want)))

@@ -139,6 +139,25 @@ int sb200_init_ps_ky(int nelem, const char* const* files, const int* lmax_ps, co
                      const int* kion, const double* Rion, int* nps, int* nlma, int* mps, int* jxyz, double* rxyz,
                      double* uv, int* ia_tbl, double* rinv_uvu, double* Vpsl);
 
+/* sb200_init_ps_ky for the pseudopotential formats with one projector per
+ * angular momentum, the format chosen by the file name as init_pp does:
+ * `_rps.dat` Yabana-Bertsch ('KY'), `.pspnc` ABINIT format 1 ('ABINIT',
+ * Troullier-Martins tables on ABINIT's fixed logarithmic grid), `.fhi` the FHI
+ * files of the ABINIT tables ('ABINITFHI'), `.cpi` FHI98PP ('FHI'); Hartree
+ * atomic units in the last three.  The core-correction block of an `.fhi` file
+ * is read past (no nonlinear core correction on this path); `.psp8`, `.vps`
+ * and `.upf` (several projectors per l or given beta projectors) return
+ * SB200_ERR_UNSUPPORTED.  Arguments, two-call protocol and outputs as
+ * sb200_init_ps_ky.
+ * Replaces: read_pslfile / init_pp's format selection
+ * (src/atom/pp/salmon_pp.f90:22-100), read_ps_abinit, read_ps_abinitfhi and
+ * read_ps_fhi (src/atom/pp/input_pp.f90:343-496,614-684) with the rest of
+ * input_pp and init_ps as above.                                               */
+int sb200_init_ps(int nelem, const char* const* files, const int* lmax_ps, const int* lloc_ps, int periodic,
+                  const int num[3], const int is[3], const double hgs[3], double hvol, int natom,
+                  const int* kion, const double* Rion, int* nps, int* nlma, int* mps, int* jxyz, double* rxyz,
+                  double* uv, int* ia_tbl, double* rinv_uvu, double* Vpsl);
+
 /* system%vec_Ac (A/c) used by sb200_hpsi: recomputes k+A stencil coefficients
  * and the projector phases (update_kvector_nonlocalpt,
  * src/common/hamiltonian.f90:847-903).  Isolated grids ignore it.              */

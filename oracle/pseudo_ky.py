@@ -1,6 +1,9 @@
 """CPU oracle (TEST INFRASTRUCTURE ONLY) for the set-up of the Kleinman-Bylander
-tables from Yabana-Bertsch pseudopotential files (`_rps.dat`, ps_format 'KY'):
-a numpy restatement of read_ps_KY (src/atom/pp/input_pp.f90:288-341), the
+tables from pseudopotential files with one projector per l (Yabana-Bertsch
+`_rps.dat` 'KY', ABINIT `.pspnc`, ABINITFHI `.fhi`, FHI98PP `.cpi`):
+a numpy restatement of read_ps_KY (src/atom/pp/input_pp.f90:288-341),
+read_ps_abinit (:343-400), read_ps_abinitfhi (:402-496), read_ps_fhi
+(:614-684), init_pp's choice by file name (src/atom/pp/salmon_pp.f90:66-100), the
 radial domain and KB norms of input_pp (:96-193), making_ps_without_masking
 (:1111-1240), init_ps's calc_nps / calc_jxyz / set_lma / calc_uv
 (src/atom/pp/prep_pp.f90:22-525), calc_Vpsl_isolated (:550-620),
@@ -67,36 +70,169 @@ def spline(xn, yn):
     return an, bn, cn, dn
 
 
-class KyElement:
-    """One element read and prepared as input_pp does for ps_format 'KY'."""
+class _Records:
+    """Fortran list-directed input: every read starts at a new line and drops
+    the rest of the last line it used; D exponents accepted."""
 
-    def __init__(self, path, lmax_ps, lloc, nrmax):
+    def __init__(self, path):
         with open(path) as f:
-            tok = f.read().split()
-        it = iter(tok)
-        self.mr = int(next(it))
-        step = float(next(it))
-        mlps = int(next(it))
-        self.zps = float(int(float(next(it)) + 1e-10))
-        next(it)                                       # irPC
-        rrc = np.array([float(next(it)) for _ in range(mlps + 1)])
-        nr = max(nrmax, self.mr)
-        self.vpp = np.zeros((nr + 1, mlps + 1))        # vpp(0:nr, 0:mlps)
-        self.upp = np.zeros((nr + 1, mlps + 1))
-        for i in range(self.mr + 1):
-            next(it), next(it)                         # r, rhopp
-            for l in range(mlps + 1):
-                self.vpp[i, l] = float(next(it))
-        for i in range(self.mr + 1):
-            next(it)
-            for l in range(mlps + 1):
-                self.upp[i, l] = float(next(it))
-        step = step / AU_LENGTH_AA
-        rrc = rrc / AU_LENGTH_AA
-        self.vpp[: self.mr + 1] /= AU_ENERGY_EV
-        self.upp[: self.mr + 1] *= np.sqrt(AU_LENGTH_AA)
+            self.lines = f.read().split("\n")
+        self.i = 0
+
+    def skip(self):
+        if self.i >= len(self.lines):
+            raise EOFError
+        self.i += 1
+
+    def read(self, n):
+        out = []
+        while len(out) < n:
+            if self.i >= len(self.lines):
+                raise EOFError
+            toks = self.lines[self.i].replace(",", " ").split()
+            self.i += 1
+            for t in toks:
+                if len(out) == n:
+                    break
+                out.append(float(t.replace("D", "E").replace("d", "E")))
+        return out
+
+
+def _read_ky(el, path, nrmax):
+    """read_ps_KY (input_pp.f90:288-341): angstrom / eV, linear grid."""
+    with open(path) as f:
+        tok = f.read().split()
+    it = iter(tok)
+    el.mr = int(next(it))
+    step = float(next(it))
+    mlps = int(next(it))
+    el.zps = float(int(float(next(it)) + 1e-10))
+    next(it)                                       # irPC
+    rrc = np.array([float(next(it)) for _ in range(mlps + 1)])
+    nr = max(nrmax, el.mr)
+    el.vpp = np.zeros((nr + 1, mlps + 1))          # vpp(0:nr, 0:mlps)
+    el.upp = np.zeros((nr + 1, mlps + 1))
+    for i in range(el.mr + 1):
+        next(it), next(it)                         # r, rhopp
+        for l in range(mlps + 1):
+            el.vpp[i, l] = float(next(it))
+    for i in range(el.mr + 1):
+        next(it)
+        for l in range(mlps + 1):
+            el.upp[i, l] = float(next(it))
+    step = step / AU_LENGTH_AA
+    rrc = rrc / AU_LENGTH_AA
+    el.vpp[: el.mr + 1] /= AU_ENERGY_EV
+    el.upp[: el.mr + 1] *= np.sqrt(AU_LENGTH_AA)
+    el.rad = np.array([(i - 1) * step for i in range(1, nrmax + 2)])   # rad(i) at [i - 1]
+    return mlps, rrc
+
+
+def _read_abinit(el, path, nrmax):
+    """read_ps_abinit (input_pp.f90:343-400), ABINIT format 1 (.pspnc)."""
+    R = _Records(path)
+    R.skip()
+    zatom, zion, pspdat = R.read(3)
+    el.zps = float(int(zion + 1e-10))
+    pspcod, pspxc, lmaxabinit, lloc, mmax, r2well = R.read(6)
+    mlps, mmax = int(lmaxabinit), int(mmax)
+    el.mr = mmax - 1
+    rrc = np.zeros(mlps + 1)
+    for ll in range(mlps + 1):
+        rrc[ll] = R.read(5)[4]
+        R.read(4)
+    R.read(3)
+    nr = max(nrmax, el.mr)
+    el.vpp = np.zeros((nr + 1, mlps + 1))
+    el.upp = np.zeros((nr + 1, mlps + 1))
+    for t in (el.vpp, el.upp):
+        for ll in range(mlps + 1):
+            R.skip()
+            for i in range(1, (el.mr + 1) // 3 + 1):
+                t[3 * (i - 1): 3 * (i - 1) + 3, ll] = R.read(3)
+    el.rad = np.array([1.0e2 * (i / (mmax - 1) + 1.0e-2) ** 5 - 1.0e-8 for i in range(nrmax + 1)])
+    return mlps, rrc
+
+
+def _read_fhi(el, path, nrmax, abinit):
+    """read_ps_abinitfhi (input_pp.f90:402-496, .fhi) and read_ps_fhi
+    (:614-684, .cpi)."""
+    R = _Records(path)
+    if abinit:
+        for _ in range(7):
+            R.skip()
+    rzps, m = R.read(2)
+    el.zps = float(int(rzps + 1e-10))
+    mlps = int(m) - 1
+    for _ in range(10):
+        R.read(1)
+    mr_l, step_l = [], []
+    rad = None
+    for l in range(mlps + 1):
+        a, b = R.read(2)
+        mr_l.append(int(a))
+        step_l.append(b)
+        if rad is None:
+            nr = max(nrmax, mr_l[0])
+            rad = np.zeros(nr + 2)                 # rad(i) at [i - 1]
+            el.vpp = np.zeros((nr + 1, mlps + 1))
+            el.upp = np.zeros((nr + 1, mlps + 1))
+        for i in range(1, mr_l[l] + 1):
+            j, r, u, v = R.read(4)
+            rad[i] = r
+            el.upp[i, l] = u
+            el.vpp[i, l] = v
+        rad[0] = 0.0
+        el.upp[0, l] = 0.0
+        el.vpp[0, l] = el.vpp[1, l] - (el.vpp[2, l] - el.vpp[1, l]) / (rad[2] - rad[1]) * rad[1]
+    if abinit:
+        try:
+            for i in range(1, mr_l[0] + 1):
+                rad[i] = R.read(4)[0]
+        except EOFError:
+            pass
+    assert min(mr_l) == max(mr_l) and max(step_l) - min(step_l) < 1e-14
+    el.mr = mr_l[0]
+    step = min(step_l)
+    for i in range(el.mr + 1, (nrmax - 1 if abinit else nrmax) + 1):
+        rad[i] = rad[i - 1] * step
+    rrc = np.zeros(mlps + 1)
+    for l in range(mlps + 1):
+        best = -1.0
+        for ll in range(mlps + 1):
+            rm = -1.0
+            for i in range(el.mr, 0, -1):
+                if abs(el.vpp[i, l] - el.vpp[i, ll]) > 1e-10:
+                    rm = rad[i + 1]
+                    break
+            best = max(best, rm)
+        rrc[l] = best
+    el.rad = rad
+    return mlps, rrc
+
+
+def _format_of(path):
+    """init_pp's choice by file name (salmon_pp.f90:66-100)."""
+    p = str(path)
+    for suffix, fmt in (("_rps.dat", "KY"), (".pspnc", "ABINIT"), (".fhi", "ABINITFHI"), (".cpi", "FHI")):
+        if p.endswith(suffix):
+            return fmt
+    raise ValueError("unsupported pseudopotential file " + p)
+
+
+class KyElement:
+    """One element read and prepared as input_pp does (ps_format 'KY' by
+    default; fmt 'ABINIT', 'ABINITFHI' or 'FHI' for the other one-projector
+    readers)."""
+
+    def __init__(self, path, lmax_ps, lloc, nrmax, fmt="KY"):
+        if fmt == "KY":
+            mlps, rrc = _read_ky(self, path, nrmax)
+        elif fmt == "ABINIT":
+            mlps, rrc = _read_abinit(self, path, nrmax)
+        else:
+            mlps, rrc = _read_fhi(self, path, nrmax, fmt == "ABINITFHI")
         self.nrmax = nrmax
-        self.rad = np.array([(i - 1) * step for i in range(1, nrmax + 1)])   # rad(i) at [i - 1]
         if lmax_ps is not None and lmax_ps >= 0:
             mlps = lmax_ps
         self.mlps = mlps
@@ -188,11 +324,12 @@ def _vpsl_periodic(el, rion, kion, num, al):
     return np.asfortranarray(vt.real)
 
 
-def init_ps_ky(files, lloc_ps, grid, rion, kion, lmax_ps=None):
+def init_ps_ky(files, lloc_ps, grid, rion, kion, lmax_ps=None, by_name=False):
     """(mps, jxyz, rxyz, uv, ia_tbl, rinv_uvu, Vpsl or None) as init_ps builds them."""
     periodic = bool(grid.periodic)
     nrmax = 3000 if periodic else 20000
-    el = [KyElement(f, None if lmax_ps is None else lmax_ps[k], lloc_ps[k], nrmax) for k, f in enumerate(files)]
+    el = [KyElement(f, None if lmax_ps is None else lmax_ps[k], lloc_ps[k], nrmax,
+                    _format_of(f) if by_name else "KY") for k, f in enumerate(files)]
     rion = np.asarray(rion, dtype=np.float64).reshape(3, -1, order="F")
     natom = rion.shape[1]
     num = [int(n) for n in grid.num]

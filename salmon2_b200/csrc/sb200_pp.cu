@@ -1,9 +1,14 @@
 // sb200_pp.cu -- host side: Kleinman-Bylander tables of s_pp_grid and the
-// local pseudopotential of an isolated grid from Yabana-Bertsch pseudopotential
-// files (`_rps.dat`, ps_format = 'KY'), the set-up that produces the tables the
-// propagation path consumes (no device code).
+// local pseudopotential from pseudopotential files with one projector per
+// angular momentum (Yabana-Bertsch `_rps.dat` 'KY', ABINIT format 1 `.pspnc`,
+// the ABINIT tables' FHI `.fhi`, FHI98PP `.cpi`), the set-up that produces the
+// tables the propagation path consumes (no device code).
 //
 //   read_ps_KY                    src/atom/pp/input_pp.f90:288-341
+//   read_ps_abinit                src/atom/pp/input_pp.f90:343-400
+//   read_ps_abinitfhi             src/atom/pp/input_pp.f90:402-496
+//   read_ps_fhi                   src/atom/pp/input_pp.f90:614-684
+//   format by file name (init_pp) src/atom/pp/salmon_pp.f90:66-100
 //   input_pp (radial domain,
 //     KB norms)                   src/atom/pp/input_pp.f90:96-193
 //   making_ps_without_masking     src/atom/pp/input_pp.f90:1111-1240
@@ -27,6 +32,7 @@
 // the local channel and the structure sum, transformed back to the grid.
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -40,7 +46,7 @@ constexpr double PP_PI = 3.141592653589793;
 constexpr double AU_LENGTH_AA = 0.52917721067;  // src/io/inputoutput.f90:27
 constexpr double AU_ENERGY_EV = 27.21138505;    // src/io/inputoutput.f90:26
 
-struct KyElement {
+struct PsElement {
   int mr = 0, mlps = 0, lref = 0, nrps = 0, nrmax = 0;
   double step = 0.0, zps = 0.0, rps = 0.0;
   std::vector<double> rad;                  // rad[i - 1] = (i - 1) step, i = 1..nrmax
@@ -113,7 +119,53 @@ void natural_spline(const std::vector<double>& xn, const std::vector<double>& yn
   }
 }
 
-int read_ky(const char* path, int lmax_ps, int lloc, int nrmax, KyElement& e) {
+// Fortran list-directed input, line by line: every read statement starts at a
+// new record (line) and drops what is left of the last line it used; values
+// are separated by blanks or commas; D exponents are accepted.
+class ListReader {
+ public:
+  explicit ListReader(FILE* f) : f_(f) {}
+  bool skip_record() { return next_line(); }
+  bool read(double* v, int n) {
+    int got = 0;
+    while (got < n) {
+      if (!next_line()) return false;
+      size_t i = 0;
+      while (got < n) {
+        while (i < line_.size() && (line_[i] == ' ' || line_[i] == '\t' || line_[i] == ',' || line_[i] == '\r')) ++i;
+        if (i >= line_.size()) break;
+        size_t j = i;
+        while (j < line_.size() && line_[j] != ' ' && line_[j] != '\t' && line_[j] != ',' && line_[j] != '\r') ++j;
+        std::string tok = line_.substr(i, j - i);
+        for (char& ch : tok)
+          if (ch == 'D' || ch == 'd') ch = 'E';
+        char* end = nullptr;
+        const double x = std::strtod(tok.c_str(), &end);
+        if (end == tok.c_str()) return false;
+        v[got++] = x;
+        i = j;
+      }
+    }
+    return true;
+  }
+
+ private:
+  bool next_line() {
+    line_.clear();
+    int ch = std::fgetc(f_);
+    if (ch == EOF) return false;
+    while (ch != EOF && ch != '\n') {
+      line_.push_back((char)ch);
+      ch = std::fgetc(f_);
+    }
+    return true;
+  }
+  FILE* f_;
+  std::string line_;
+};
+
+// read_ps_KY (input_pp.f90:288-341): Angstrom / eV file, linear radial grid
+int read_ky(const char* path, int nrmax, PsElement& e, std::vector<double>& rrc) {
   FILE* f = std::fopen(path, "r");
   if (!f) return set_error(SB200_ERR_INVALID_ARG, std::string("cannot open pseudopotential file ") + path);
   double rzps = 0.0;
@@ -124,11 +176,10 @@ int read_ky(const char* path, int lmax_ps, int lloc, int nrmax, KyElement& e) {
   }
   e.zps = (double)(int)(rzps + 1e-10);
   int irpc = 0;
-  std::vector<double> rrc(e.mlps + 1, 0.0);
+  rrc.assign(e.mlps + 1, 0.0);
   ok = std::fscanf(f, "%d", &irpc) == 1;
   for (int l = 0; l <= e.mlps && ok; ++l) ok = std::fscanf(f, "%lf", &rrc[l]) == 1;
   const int nr = nrmax > e.mr ? nrmax : e.mr;
-  e.nrmax = nrmax;
   const int nl = e.mlps + 1;
   e.vpp.assign(nl, std::vector<double>(nr + 1, 0.0));
   e.upp.assign(nl, std::vector<double>(nr + 1, 0.0));
@@ -153,23 +204,183 @@ int read_ky(const char* path, int lmax_ps, int lloc, int nrmax, KyElement& e) {
       e.upp[l][i] *= std::sqrt(AU_LENGTH_AA);
     }
   }
-  e.rad.resize(nrmax);
-  for (int i = 1; i <= nrmax; ++i) e.rad[i - 1] = (i - 1) * e.step;
+  e.rad.resize(nrmax + 1);
+  for (int i = 1; i <= nrmax + 1; ++i) e.rad[i - 1] = (i - 1) * e.step;
+  return SB200_OK;
+}
+
+// read_ps_abinit (input_pp.f90:343-400): ABINIT format 1 (Troullier-Martins,
+// .pspnc), Hartree atomic units; rad(i + 1) = 100 (i / (mmax - 1) + 0.01)^5 - 1e-8
+int read_abinit(const char* path, int nrmax, PsElement& e, std::vector<double>& rrc) {
+  FILE* f = std::fopen(path, "r");
+  if (!f) return set_error(SB200_ERR_INVALID_ARG, std::string("cannot open pseudopotential file ") + path);
+  ListReader in(f);
+  double v[6];
+  bool ok = in.skip_record() && in.read(v, 3);
+  if (ok) e.zps = (double)(int)(v[1] + 1e-10);
+  ok = ok && in.read(v, 6);
+  const int mmax = ok ? (int)v[4] : 0;
+  if (ok) {
+    e.mlps = (int)v[2];
+    e.mr = mmax - 1;
+  }
+  if (!ok || e.mlps < 0 || e.mlps > 3 || e.mr < 2 || e.mr > 50000) {
+    std::fclose(f);
+    return set_error(SB200_ERR_INVALID_ARG, std::string("not an ABINIT (.pspnc) file: ") + path);
+  }
+  rrc.assign(e.mlps + 1, 0.0);
+  for (int ll = 0; ll <= e.mlps && ok; ++ll) {
+    ok = in.read(v, 5);  // l, e99.0, e99.9, nproj, rcpsp
+    if (ok) rrc[ll] = v[4];
+    ok = ok && in.read(v, 4);  // rms, ekb1, ekb2, epsatm
+  }
+  ok = ok && in.read(v, 3);  // rchrg, fchrg, qchrg
+  const int nr = nrmax > e.mr ? nrmax : e.mr;
+  const int nl = e.mlps + 1;
+  e.vpp.assign(nl, std::vector<double>(nr + 1, 0.0));
+  e.upp.assign(nl, std::vector<double>(nr + 1, 0.0));
+  for (int pass = 0; pass < 2 && ok; ++pass) {
+    std::vector<std::vector<double>>& t = pass == 0 ? e.vpp : e.upp;
+    for (int ll = 0; ll <= e.mlps && ok; ++ll) {
+      ok = in.skip_record();
+      for (int i = 1; i <= (e.mr + 1) / 3 && ok; ++i) {
+        ok = in.read(v, 3);
+        for (int j = 0; j < 3 && ok; ++j) t[ll][3 * (i - 1) + j] = v[j];
+      }
+    }
+  }
+  std::fclose(f);
+  if (!ok) return set_error(SB200_ERR_INVALID_ARG, std::string("truncated ABINIT file: ") + path);
+  e.rad.resize(nrmax + 1);
+  for (int i = 0; i <= nrmax; ++i) {
+    const double x = (double)i / (double)(mmax - 1) + 1.0e-2;
+    e.rad[i] = 1.0e2 * (x * x * x * x * x) - 1.0e-8;
+  }
+  return SB200_OK;
+}
+
+// read_ps_fhi (input_pp.f90:614-684, FHI98PP .cpi) and read_ps_abinitfhi
+// (:402-496, the FHI files of the ABINIT tables, .fhi: seven header lines
+// first, then an optional core-correction block): Hartree atomic units,
+// logarithmic grid given point by point (upp(i) and vpp(i) at rad(i + 1)),
+// rad(1) = 0, upp(0) = 0, vpp(0) extrapolated linearly; the grid continued
+// by the common ratio; rrc(l) the largest radius where v_l differs from
+// another channel by more than 1e-10.  The core-correction block is read past
+// (its radii replace the grid's, as the reference reads them); nonlinear core
+// correction itself is not part of this path.
+int read_fhi(const char* path, int nrmax, PsElement& e, std::vector<double>& rrc, bool abinit) {
+  FILE* f = std::fopen(path, "r");
+  if (!f) return set_error(SB200_ERR_INVALID_ARG, std::string("cannot open pseudopotential file ") + path);
+  ListReader in(f);
+  double v[4];
+  bool ok = true;
+  if (abinit)
+    for (int i = 0; i < 7 && ok; ++i) ok = in.skip_record();
+  ok = ok && in.read(v, 2);
+  if (ok) {
+    e.zps = (double)(int)(v[0] + 1e-10);
+    e.mlps = (int)v[1] - 1;
+  }
+  if (!ok || e.mlps < 0 || e.mlps > 3) {
+    std::fclose(f);
+    return set_error(SB200_ERR_INVALID_ARG, std::string("not an FHI pseudopotential file: ") + path);
+  }
+  for (int i = 0; i < 10 && ok; ++i) ok = in.read(v, 1);
+  const int nl = e.mlps + 1;
+  std::vector<int> mr_l(nl, 0);
+  std::vector<double> step_l(nl, 0.0);
+  e.rad.assign(nrmax + 1, 0.0);
+  for (int l = 0; l <= e.mlps && ok; ++l) {
+    ok = in.read(v, 2);
+    if (!ok) break;
+    mr_l[l] = (int)v[0];
+    step_l[l] = v[1];
+    if (mr_l[l] < 3 || mr_l[l] > 50000) {
+      ok = false;
+      break;
+    }
+    if ((int)e.vpp.size() < nl) {
+      const int nr = nrmax > mr_l[l] ? nrmax : mr_l[l];
+      e.vpp.assign(nl, std::vector<double>(nr + 1, 0.0));
+      e.upp.assign(nl, std::vector<double>(nr + 1, 0.0));
+      if ((int)e.rad.size() < nr + 2) e.rad.resize(nr + 2, 0.0);
+    }
+    if (mr_l[l] > (int)e.vpp[l].size() - 1) {
+      ok = false;
+      break;
+    }
+    for (int i = 1; i <= mr_l[l] && ok; ++i) {
+      ok = in.read(v, 4);
+      if (ok) {
+        e.rad[i] = v[1];  // rad(i + 1)
+        e.upp[l][i] = v[2];
+        e.vpp[l][i] = v[3];
+      }
+    }
+    if (!ok) break;
+    e.rad[0] = 0.0;
+    e.upp[l][0] = 0.0;
+    e.vpp[l][0] = e.vpp[l][1] - (e.vpp[l][2] - e.vpp[l][1]) / (e.rad[2] - e.rad[1]) * e.rad[1];
+  }
+  if (ok && abinit)  // core-correction block, to the end of the file if present
+    for (int i = 1; i <= mr_l[0]; ++i) {
+      if (!in.read(v, 4)) break;
+      e.rad[i] = v[0];
+    }
+  std::fclose(f);
+  if (!ok) return set_error(SB200_ERR_INVALID_ARG, std::string("truncated FHI pseudopotential file: ") + path);
+  for (int l = 1; l <= e.mlps; ++l)
+    if (mr_l[l] != mr_l[0]) return set_error(SB200_ERR_INVALID_ARG, "FHI file: radial grids of different lengths");
+  double smin = step_l[0], smax = step_l[0];
+  for (int l = 1; l <= e.mlps; ++l) {
+    smin = step_l[l] < smin ? step_l[l] : smin;
+    smax = step_l[l] > smax ? step_l[l] : smax;
+  }
+  if (smax - smin >= 1e-14) return set_error(SB200_ERR_INVALID_ARG, "FHI file: radial grids of different ratios");
+  e.mr = mr_l[0];
+  e.step = smin;
+  const int iend = abinit ? nrmax - 1 : nrmax;
+  for (int i = e.mr + 1; i <= iend; ++i) e.rad[i] = e.rad[i - 1] * e.step;  // rad(i + 1) = rad(i) step
+  rrc.assign(nl, 0.0);
+  for (int l = 0; l <= e.mlps; ++l) {
+    double best = -1.0;
+    for (int ll = 0; ll <= e.mlps; ++ll) {
+      double rm = -1.0;
+      for (int i = e.mr; i >= 1; --i)
+        if (std::fabs(e.vpp[l][i] - e.vpp[ll][i]) > 1e-10) {
+          rm = e.rad[i + 1];  // rad(i + 2)
+          break;
+        }
+      best = rm > best ? rm : best;
+    }
+    rrc[l] = best;
+  }
+  return SB200_OK;
+}
+
+// input_pp's common part (input_pp.f90:93-193) and making_ps_without_masking
+// (:1111-1240) for an element read by one of the readers above
+int finish_element(PsElement& e, const std::vector<double>& rrc, int lmax_ps, int lloc, int nrmax) {
+  e.nrmax = nrmax;
   if (lmax_ps >= 0) {
     if (lmax_ps > e.mlps) return set_error(SB200_ERR_INVALID_ARG, "Lmax_ps above the file's angular momenta");
     e.mlps = lmax_ps;
   }
   if (lloc < 0 || lloc > e.mlps) return set_error(SB200_ERR_INVALID_ARG, "Lloc_ps must be in 0..Lmax_ps");
   e.lref = lloc;
+  if ((int)e.rad.size() < e.mr + 2 || (int)e.rad.size() < nrmax + 1)
+    return set_error(SB200_ERR_INVALID_ARG, "pseudopotential file's radial grid longer than the set-up's arrays");
+  const int nr = (int)e.vpp[0].size() - 1;
   // beyond the file's grid: -Zps / r (input_pp.f90:96-102; the array index i
   // takes rad(i) here although vpp(i) otherwise stands for rad(i + 1))
-  for (int i = e.mr + 1; i <= nrmax; ++i)
+  for (int i = e.mr + 1; i <= nrmax && i <= nr; ++i)
     for (int l = 0; l <= e.mlps; ++l) {
       if (e.rad[i - 1] > 0.0) e.vpp[l][i] = -e.zps / e.rad[i - 1];
       e.upp[l][i] = 0.0;
     }
   double rps = 0.0;
   for (int l = 0; l <= e.mlps; ++l) rps = rrc[l] > rps ? rrc[l] : rps;
+  if (!(rps > 0.0)) return set_error(SB200_ERR_INVALID_ARG, "pseudopotential without a cut-off radius");
   e.rps = rps;
   int i = 1;
   for (; i <= nrmax; ++i)
@@ -217,23 +428,51 @@ int read_ky(const char* path, int lmax_ps, int lloc, int nrmax, KyElement& e) {
   return SB200_OK;
 }
 
-}  // namespace
-}  // namespace sb200
+bool ends_with(const std::string& s, const char* suffix) {
+  const size_t n = std::strlen(suffix);
+  return s.size() >= n && s.compare(s.size() - n, n, suffix) == 0;
+}
 
-using namespace sb200;
+// one element: the reader of its format, then input_pp's common part.
+// force_ky: the file is read as 'KY' whatever its name; otherwise the format
+// follows the file name as init_pp does (salmon_pp.f90:66-100): _rps.dat KY,
+// .pspnc ABINIT, .fhi ABINITFHI, .cpi FHI.
+int read_element(const char* path, bool force_ky, int lmax_ps, int lloc, int nrmax, PsElement& e) {
+  const std::string name(path);
+  std::vector<double> rrc;
+  int r;
+  if (force_ky || ends_with(name, "_rps.dat")) {
+    r = read_ky(path, nrmax, e, rrc);
+  } else if (ends_with(name, ".pspnc")) {
+    r = read_abinit(path, nrmax, e, rrc);
+  } else if (ends_with(name, ".fhi")) {
+    r = read_fhi(path, nrmax, e, rrc, true);
+  } else if (ends_with(name, ".cpi")) {
+    r = read_fhi(path, nrmax, e, rrc, false);
+  } else if (ends_with(name, ".psp8") || ends_with(name, ".vps") || ends_with(name, ".upf") ||
+             ends_with(name, ".UPF")) {
+    return set_error(SB200_ERR_UNSUPPORTED,
+                     "pseudopotentials with several projectors per l or given beta projectors (psp8, vps, upf) "
+                     "are not supported: " + name);
+  } else {
+    return set_error(SB200_ERR_INVALID_ARG, "unknown pseudopotential file format: " + name);
+  }
+  if (r != SB200_OK) return r;
+  return finish_element(e, rrc, lmax_ps, lloc, nrmax);
+}
 
-extern "C" int sb200_init_ps_ky(int nelem, const char* const* files, const int* lmax_ps, const int* lloc_ps,
-                                int periodic, const int num[3], const int is[3], const double hgs[3], double hvol,
-                                int natom, const int* kion, const double* Rion, int* nps, int* nlma, int* mps,
-                                int* jxyz, double* rxyz, double* uv, int* ia_tbl, double* rinv_uvu,
-                                double* Vpsl) {
+int init_ps_impl(bool force_ky, int nelem, const char* const* files, const int* lmax_ps, const int* lloc_ps,
+                 int periodic, const int num[3], const int is[3], const double hgs[3], double hvol, int natom,
+                 const int* kion, const double* Rion, int* nps, int* nlma, int* mps, int* jxyz, double* rxyz,
+                 double* uv, int* ia_tbl, double* rinv_uvu, double* Vpsl) {
   if (nelem < 1 || !files || !lloc_ps || !num || !is || !hgs || natom < 0 || (natom > 0 && (!kion || !Rion)) ||
       !nps || !nlma)
-    return set_error(SB200_ERR_INVALID_ARG, "sb200_init_ps_ky: null or inconsistent argument");
+    return set_error(SB200_ERR_INVALID_ARG, "sb200_init_ps: null or inconsistent argument");
   const int nrmax = periodic ? 3000 : 20000;  // read_pslfile, salmon_pp.f90:34-38
-  std::vector<KyElement> el(nelem);
+  std::vector<PsElement> el(nelem);
   for (int k = 0; k < nelem; ++k) {
-    const int r = read_ky(files[k], lmax_ps ? lmax_ps[k] : -1, lloc_ps[k], nrmax, el[k]);
+    if (!files[k]) return set_error(SB200_ERR_INVALID_ARG, "null pseudopotential file name");
+    const int r = read_element(files[k], force_ky, lmax_ps ? lmax_ps[k] : -1, lloc_ps[k], nrmax, el[k]);
     if (r != SB200_OK) return r;
   }
   for (int a = 0; a < natom; ++a)
@@ -261,7 +500,7 @@ extern "C" int sb200_init_ps_ky(int nelem, const char* const* files, const int* 
   std::vector<std::vector<int>> pj(natom);
   std::vector<std::vector<double>> pr(natom);
   for (int a = 0; a < natom; ++a) {
-    const KyElement& e = el[kion[a] - 1];
+    const PsElement& e = el[kion[a] - 1];
     for (int j1 = -nc[0]; j1 <= nc[0]; ++j1) {
       const double x1 = Rion[3 * a] + j1 * al[0];
       if (x1 <= is[0] * hgs[0] - rps_max || x1 >= ie[0] * hgs[0] + rps_max) continue;
@@ -290,13 +529,13 @@ extern "C" int sb200_init_ps_ky(int nelem, const char* const* files, const int* 
   for (int a = 0; a < natom; ++a) {
     const int m = (int)pj[a].size() / 3;
     np = m > np ? m : np;
-    const KyElement& e = el[kion[a] - 1];
+    const PsElement& e = el[kion[a] - 1];
     for (int l = 0; l <= e.mlps; ++l)
       if (e.inorm[l] != 0) nl += 2 * l + 1;
   }
   const bool fill = mps && jxyz && rxyz && uv && ia_tbl && rinv_uvu;
   if (fill && (*nps < np || *nlma < nl))
-    return set_error(SB200_ERR_INVALID_ARG, "sb200_init_ps_ky: output arrays smaller than *nps, *nlma");
+    return set_error(SB200_ERR_INVALID_ARG, "sb200_init_ps: output arrays smaller than *nps, *nlma");
   if (!fill) {
     *nps = np;
     *nlma = nl;
@@ -307,7 +546,7 @@ extern "C" int sb200_init_ps_ky(int nelem, const char* const* files, const int* 
     std::memset(uv, 0, sizeof(double) * (size_t)NPS * NLMA);
     int lma = 0;
     for (int a = 0; a < natom; ++a) {
-      const KyElement& e = el[kion[a] - 1];
+      const PsElement& e = el[kion[a] - 1];
       const int m = (int)pj[a].size() / 3;
       mps[a] = m;
       for (int j = 0; j < m; ++j)
@@ -370,7 +609,7 @@ extern "C" int sb200_init_ps_ky(int nelem, const char* const* files, const int* 
           const double gsq = std::sqrt(G2);
           double sr = 0.0, si = 0.0;
           for (int a = 0; a < natom; ++a) {
-            const KyElement& e = el[kion[a] - 1];
+            const PsElement& e = el[kion[a] - 1];
             double zv = 0.0;
             for (int i2 = 2; i2 <= e.nrps; ++i2) {  // vloctbl(i) = vpp(i - 1, lref), i = 1..nrps
               const double r1 = 0.5 * (e.rad[i2 - 1] + e.rad[i2 - 2]);
@@ -421,7 +660,7 @@ extern "C" int sb200_init_ps_ky(int nelem, const char* const* files, const int* 
     const long npts = (long)num[0] * num[1] * num[2];
     for (long p = 0; p < npts; ++p) Vpsl[p] = 0.0;
     for (int a = 0; a < natom; ++a) {
-      const KyElement& e = el[kion[a] - 1];
+      const PsElement& e = el[kion[a] - 1];
       for (int iz = 0; iz < num[2]; ++iz)
         for (int iy = 0; iy < num[1]; ++iy)
           for (int ix = 0; ix < num[0]; ++ix) {
@@ -447,4 +686,26 @@ extern "C" int sb200_init_ps_ky(int nelem, const char* const* files, const int* 
     }
   }
   return SB200_OK;
+}
+
+}  // namespace
+}  // namespace sb200
+
+using namespace sb200;
+
+extern "C" int sb200_init_ps_ky(int nelem, const char* const* files, const int* lmax_ps, const int* lloc_ps,
+                                int periodic, const int num[3], const int is[3], const double hgs[3], double hvol,
+                                int natom, const int* kion, const double* Rion, int* nps, int* nlma, int* mps,
+                                int* jxyz, double* rxyz, double* uv, int* ia_tbl, double* rinv_uvu,
+                                double* Vpsl) {
+  return init_ps_impl(true, nelem, files, lmax_ps, lloc_ps, periodic, num, is, hgs, hvol, natom, kion, Rion, nps,
+                      nlma, mps, jxyz, rxyz, uv, ia_tbl, rinv_uvu, Vpsl);
+}
+
+extern "C" int sb200_init_ps(int nelem, const char* const* files, const int* lmax_ps, const int* lloc_ps,
+                             int periodic, const int num[3], const int is[3], const double hgs[3], double hvol,
+                             int natom, const int* kion, const double* Rion, int* nps, int* nlma, int* mps,
+                             int* jxyz, double* rxyz, double* uv, int* ia_tbl, double* rinv_uvu, double* Vpsl) {
+  return init_ps_impl(false, nelem, files, lmax_ps, lloc_ps, periodic, num, is, hgs, hvol, natom, kion, Rion, nps,
+                      nlma, mps, jxyz, rxyz, uv, ia_tbl, rinv_uvu, Vpsl);
 }

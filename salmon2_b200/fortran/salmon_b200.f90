@@ -127,6 +127,18 @@ module salmon_b200
       type(c_ptr), value :: mps, jxyz, rxyz, uv, ia_tbl, rinv_uvu, Vpsl
     end function
 
+    integer(c_int) function sb200_init_ps(nelem, files, lmax_ps, lloc_ps, periodic, num, is, hgs, hvol, &
+        natom, kion, Rion, nps, nlma, mps, jxyz, rxyz, uv, ia_tbl, rinv_uvu, Vpsl) bind(c, name="sb200_init_ps")
+      import
+      integer(c_int), value :: nelem, periodic, natom
+      type(c_ptr), intent(in) :: files(*)       ! c_loc of NUL-terminated file names
+      integer(c_int), intent(in) :: lmax_ps(*), lloc_ps(*), num(3), is(3), kion(*)
+      real(c_double), intent(in) :: hgs(3), Rion(3, *)
+      real(c_double), value :: hvol
+      integer(c_int), intent(inout) :: nps, nlma
+      type(c_ptr), value :: mps, jxyz, rxyz, uv, ia_tbl, rinv_uvu, Vpsl
+    end function
+
     integer(c_int) function sb200_set_micro_ac(ctx, Ac_micro, div_Ac) bind(c, name="sb200_set_micro_ac")
       import
       type(c_ptr), value :: ctx

@@ -1,6 +1,8 @@
-"""Kleinman-Bylander tables and the isolated local potential from
-Yabana-Bertsch pseudopotential files (`_rps.dat`, ps_format = 'KY') through the
-library's host-side builder (sb200_init_ps_ky; input_pp.f90 read_ps_KY,
+"""Kleinman-Bylander tables and the local potential from pseudopotential
+files through the library's host-side builder: Yabana-Bertsch files
+(`_rps.dat`, ps_format = 'KY') with sb200_init_ps_ky, and any one-projector
+format chosen by the file name (`_rps.dat`, `.pspnc` ABINIT, `.fhi`
+ABINITFHI, `.cpi` FHI) with sb200_init_ps (input_pp.f90 read_ps_*,
 making_ps_without_masking, prep_pp.f90 init_ps, calc_Vpsl_isolated /
 calc_Vpsl_periodic)."""
 from __future__ import annotations
@@ -21,6 +23,16 @@ def init_ps_ky(files, lloc_ps, grid, rion, kion, lmax_ps=None, vpsl=True):
     Lmax_ps; lmax_ps None keeps the file's); grid: a synth.Grid (orthogonal);
     rion: (3, natom) bohr; kion: 1-based element of each atom.  Returns
     (PPGrid, Vpsl (nx, ny, nz) Fortran order, or None with vpsl=False)."""
+    return _init_ps("sb200_init_ps_ky", files, lloc_ps, grid, rion, kion, lmax_ps, vpsl)
+
+
+def init_ps(files, lloc_ps, grid, rion, kion, lmax_ps=None, vpsl=True):
+    """init_ps_ky for every one-projector format, chosen by the file name."""
+    return _init_ps("sb200_init_ps", files, lloc_ps, grid, rion, kion, lmax_ps, vpsl)
+
+
+def _init_ps(entry, files, lloc_ps, grid, rion, kion, lmax_ps, vpsl):
+    fn = getattr(lib(), entry)
     nelem = len(files)
     arr = (C.c_char_p * nelem)(*[str(f).encode() for f in files])
     lloc = np.ascontiguousarray(lloc_ps, dtype=np.int32)
@@ -35,7 +47,7 @@ def init_ps_ky(files, lloc_ps, grid, rion, kion, lmax_ps=None, vpsl=True):
     P = lambda a, t=_dp: None if a is None else a.ctypes.data_as(t)
     args = [nelem, arr, P(lmax, _ip), P(lloc, _ip), 1 if grid.periodic else 0, P(num, _ip), P(is_, _ip), P(hgs),
             float(grid.hvol), natom, P(k, _ip), P(r)]
-    check(lib().sb200_init_ps_ky(*args, C.byref(nps), C.byref(nlma), None, None, None, None, None, None, None))
+    check(fn(*args, C.byref(nps), C.byref(nlma), None, None, None, None, None, None, None))
     n, m = nps.value, nlma.value
     mps = np.zeros(natom, dtype=np.int32)
     jxyz = np.zeros((3, n, natom), dtype=np.int32, order="F")
@@ -44,6 +56,6 @@ def init_ps_ky(files, lloc_ps, grid, rion, kion, lmax_ps=None, vpsl=True):
     ia = np.zeros(m, dtype=np.int32)
     rinv = np.zeros(m, dtype=np.float64)
     v = np.zeros(tuple(grid.num), dtype=np.float64, order="F") if vpsl else None
-    check(lib().sb200_init_ps_ky(*args, C.byref(nps), C.byref(nlma), P(mps, _ip), P(jxyz, _ip), P(rxyz), P(uv),
+    check(fn(*args, C.byref(nps), C.byref(nlma), P(mps, _ip), P(jxyz, _ip), P(rxyz), P(uv),
                                  P(ia, _ip), P(rinv), P(v)))
     return PPGrid(natom, n, m, mps, jxyz, rxyz, uv, ia, rinv), v

@@ -69,3 +69,85 @@ def write_ky_file(path, zps=4.0, mlps=2, mr=400, step=0.01, rc=1.1, seed=0):
     with open(path, "w") as f:
         f.write("\n".join(lines) + "\n")
     return path
+
+
+def _au_channels(r, zps, amp, l):
+    """Smooth analytic channels in Hartree atomic units for the non-KY
+    fixtures: v_l(r) = -zps erf(r/0.75)/r + A_l exp(-(r/0.5)^4), u_l(r) =
+    r^(l+1) exp(-r^2/2.6) (the channels differ only inside r ~ 1.1 bohr)."""
+    from math import erf
+    vc = -zps * (erf(r / 0.75) / r if r > 0 else 2.0 / (0.75 * np.sqrt(np.pi)))
+    return vc + amp[l] * np.exp(-(r / 0.5) ** 4), r ** (l + 1) * np.exp(-r * r / 2.6)
+
+
+def write_fhi_file(path, zps=4.0, mlps=2, mr=420, r1=0.0005, ratio=1.0247, seed=0, abinit=True, radii=None,
+                   values=None, nlcc=False):
+    """An FHI pseudopotential file: with abinit, the `.fhi` form of the ABINIT
+    tables (seven header lines first); else FHI98PP `.cpi`.  radii: the
+    mr grid radii rad(2..mr+1) (default r1 ratio^(i-1)); values: optional
+    (upp, vpp) arrays (mr, mlps + 1) at those radii instead of the analytic
+    channels.  nlcc: append a core-correction block on the same radii."""
+    rng = np.random.default_rng(seed)
+    amp = rng.uniform(-0.3, 0.3, mlps + 1)
+    rs = np.asarray(radii, dtype=np.float64) if radii is not None else r1 * ratio ** np.arange(mr)
+    mr = len(rs)
+    lines = []
+    if abinit:
+        lines += ["synthetic FHI pseudopotential (ABINIT table form)",
+                  f"  {float(zps):.4f}  {float(zps):.4f}    000101              zatom,zion,pspdat",
+                  "   6   1   2   0   {0}   0.00000  pspcod,pspxc,lmax,lloc,mmax,r2well".format(mr),
+                  "  0.00000  -1.00000  0.00000                rchrg,fchrg,qchrg",
+                  "5--- reserved for future features", "6--- reserved for future features",
+                  "7--- Here follows the cpi file in the fhi98pp format -"]
+    lines.append(f"{zps:.4f}  {mlps + 1}")
+    R = lambda x: repr(float(x))
+    for k in range(10):
+        lines.append(f"  0.0000000000E+00  0.0000000000E+00  0.0000000000E+00   # line {k}")
+    for l in range(mlps + 1):
+        lines.append(f"{mr:5d} {R(ratio)}")
+        for i, r in enumerate(rs):
+            if values is None:
+                v, u = _au_channels(r, zps, amp, l)
+            else:
+                u, v = values[0][i, l], values[1][i, l]
+            lines.append(f"{i + 1:5d} {R(r)} {R(u)} {R(v)}".replace("e", "D"))
+    if nlcc:
+        for r in rs:
+            lines.append(f"{R(r)} {np.exp(-r):.15e} {-np.exp(-r):.15e} {np.exp(-r):.15e}")
+    with open(path, "w") as f:
+        f.write("\n".join(lines) + "\n")
+    return path
+
+
+def write_abinit_file(path, zps=4.0, mlps=2, mmax=600, lloc=0, rc=None, seed=0, values=None):
+    """An ABINIT format-1 (`.pspnc`, Troullier-Martins) file on ABINIT's grid
+    rad(i + 1) = 100 (i / (mmax - 1) + 0.01)^5 - 1e-8, Hartree atomic units.
+    rc: per-channel cut-off radii (default 1.3 bohr); values: optional (upp,
+    vpp) arrays (mmax, mlps + 1) at indices 0..mmax-1."""
+    assert mmax % 3 == 0
+    rng = np.random.default_rng(seed)
+    amp = rng.uniform(-0.3, 0.3, mlps + 1)
+    rc = [1.3] * (mlps + 1) if rc is None else list(rc)
+    rad = [1.0e2 * (i / (mmax - 1) + 1.0e-2) ** 5 - 1.0e-8 for i in range(mmax)]
+    lines = ["synthetic Troullier-Martins pseudopotential",
+             f"  {zps:.5f}  {zps:.5f}  000101    zatom, zion, pspdat",
+             f"   1   1   {mlps}   {lloc}   {mmax}   0.00000    pspcod,pspxc,lmax,lloc,mmax,r2well"]
+    for l in range(mlps + 1):
+        lines.append(f"   {l}   0.000   0.000   1   {float(rc[l])!r}   l,e99.0,e99.9,nproj,rcpsp")
+        lines.append("   0.00000000   0.00000000   0.00000000   0.00000000   rms,ekb1,ekb2,epsatm")
+    lines.append("   0.00000000   0.00000000   0.00000000   rchrg,fchrg,qchrg")
+    for which in (1, 0):  # potentials, then wave functions
+        for l in range(mlps + 1):
+            lines.append(f"{l} = l for {'potential' if which else 'wavefunction'}")
+            vals = []
+            for i in range(mmax):
+                if values is None:
+                    v, u = _au_channels(rad[i], zps, amp, l)
+                else:
+                    u, v = values[0][i, l], values[1][i, l]
+                vals.append(v if which else u)
+            for i in range(0, mmax, 3):
+                lines.append(" ".join(repr(float(x)) for x in vals[i:i + 3]))
+    with open(path, "w") as f:
+        f.write("\n".join(lines) + "\n")
+    return path

@@ -1,7 +1,8 @@
 """H psi and a short time loop on the GPU with the Kleinman-Bylander tables and
-the local potential built from Yabana-Bertsch pseudopotential files by the
-library's host-side set-up (sb200_init_ps_ky), against the oracle on the same
-tables: the set-up's output drives the propagation path unchanged."""
+the local potential built from pseudopotential files by the library's
+host-side set-up (sb200_init_ps_ky for Yabana-Bertsch files; sb200_init_ps
+for ABINIT and FHI files), against the oracle on the same tables: the
+set-up's output drives the propagation path unchanged."""
 import dataclasses
 
 import numpy as np
@@ -49,4 +50,24 @@ def test_time_loop_with_tables_from_pseudopotential_files(tmp_path):
     d_got = res["rbox"][:3] - res["rbox"][:3, :1]
     assert np.max(np.abs(d_got - d_ref)) <= 1e-10 * np.max(np.abs(ref["rbox"][:3]))
     assert S.rel_err(ctx.download(res["psi"]), ref["psi"]) < 1e-11
+    ctx.close()
+
+
+@pytest.mark.parametrize("fmt", ["pspnc", "fhi"])
+def test_hpsi_with_tables_from_abinit_and_fhi_files(tmp_path, fmt):
+    from salmon2_b200 import pseudo, synth
+    from salmon2_b200.rt import Context
+    if fmt == "pspnc":
+        f = S.write_abinit_file(str(tmp_path / "A.pspnc"), zps=4.0, mlps=2, seed=13)
+    else:
+        f = S.write_fhi_file(str(tmp_path / "A.fhi"), zps=4.0, mlps=2, seed=13)
+    base = synth.isolated_system(num=28, h_aa=0.25, no=4, natom=2, seed=22, name="fmt28")
+    rion = np.array([[0.4, -0.3, 1.2], [-1.5, 0.6, -0.8]]).T
+    pp, vpsl = pseudo.init_ps([f], [2], base.grid, rion, [1, 1])
+    s = dataclasses.replace(base, pp=pp, rion=rion, V_local=np.asfortranarray(vpsl[..., None]))
+    assert s.pp.nlma == 8
+    ctx = Context(s)
+    h = ctx.zeros()
+    ctx.hpsi(ctx.upload(s.psi), h)
+    assert S.rel_err(ctx.download(h), Oracle(s).hpsi(s.psi)) < 1e-12
     ctx.close()

@@ -158,6 +158,17 @@ int sb200_init_ps(int nelem, const char* const* files, const int* lmax_ps, const
                   const int* kion, const double* Rion, int* nps, int* nlma, int* mps, int* jxyz, double* rxyz,
                   double* uv, int* ia_tbl, double* rinv_uvu, double* Vpsl);
 
+/* yn_psmask (1 = 'y', 0 = 'n', the default) and alpha_mask, gamma_mask,
+ * eta_mask (the reference's defaults 0.8, 1.8, 15) for the following
+ * sb200_init_ps / sb200_init_ps_ky calls, process-wide as the reference's
+ * input variables: the radial KB functions u_l (v_l - v_lloc) are divided by
+ * the normalized mask function on the cut-off widened to gamma_mask rps,
+ * Fourier-filtered below alpha_mask pi / max(h) (spherical Bessel transforms
+ * on 1000 k points) and multiplied by the mask again.
+ * Replaces: making_ps_with_masking, ps_masking and make_mask_function
+ * (src/atom/pp/input_pp.f90:848-1016,1302-1542).                               */
+int sb200_set_psmask(int yn_psmask, double alpha_mask, double gamma_mask, double eta_mask);
+
 /* system%vec_Ac (A/c) used by sb200_hpsi: recomputes k+A stencil coefficients
  * and the projector phases (update_kvector_nonlocalpt,
  * src/common/hamiltonian.f90:847-903).  Isolated grids ignore it.              */

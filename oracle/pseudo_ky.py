@@ -3,7 +3,9 @@ tables from pseudopotential files with one projector per l (Yabana-Bertsch
 `_rps.dat` 'KY', ABINIT `.pspnc`, ABINITFHI `.fhi`, FHI98PP `.cpi`):
 a numpy restatement of read_ps_KY (src/atom/pp/input_pp.f90:288-341),
 read_ps_abinit (:343-400), read_ps_abinitfhi (:402-496), read_ps_fhi
-(:614-684), init_pp's choice by file name (src/atom/pp/salmon_pp.f90:66-100), the
+(:614-684), init_pp's choice by file name (src/atom/pp/salmon_pp.f90:66-100),
+the masking filter (making_ps_with_masking, ps_masking, make_mask_function,
+input_pp.f90:848-1016,1302-1542, with xjl of src/math/salmon_math.f90:289-335), the
 radial domain and KB norms of input_pp (:96-193), making_ps_without_masking
 (:1111-1240), init_ps's calc_nps / calc_jxyz / set_lma / calc_uv
 (src/atom/pp/prep_pp.f90:22-525), calc_Vpsl_isolated (:550-620),
@@ -220,12 +222,105 @@ def _format_of(path):
     raise ValueError("unsupported pseudopotential file " + p)
 
 
+def _seqsum(a, axis):
+    """left-to-right sum (the reference's loop order)"""
+    return np.take(np.cumsum(a, axis=axis), -1, axis=axis)
+
+
+def xjl(x, l):
+    """x j_l(x) (salmon_math.f90:289-335): closed forms, Taylor series below 0.1."""
+    x = np.asarray(x, dtype=np.float64)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        s, c = np.sin(x), np.cos(x)
+        big = {0: s, 1: (1.0 / x) * s - c, 2: (3.0 / x ** 2 - 1.0) * s - (3.0 / x) * c,
+               3: (15.0 / x ** 3 - 6.0 / x) * s - (15.0 / x ** 2 - 1.0) * c}[l]
+    small = {0: x - x ** 3 / 6.0 + x ** 5 / 120.0 - x ** 7 / 5040.0 + x ** 9 / 362880.0,
+             1: (2.0 / 6.0) * x ** 2 - (2.0 / 60.0) * x ** 4 + (1.0 / 840.0) * x ** 6 - (2.0 / 90720.0) * x ** 8,
+             2: (4.0 / 60.0) * x ** 3 - (4.0 / 840.0) * x ** 5 + (2.0 / 15120.0) * x ** 7 - (2.0 / 997920.0) * x ** 9,
+             3: (8.0 / 840.0) * x ** 4 - (8.0 / 15120.0) * x ** 6 + (4.0 / 332640.0) * x ** 8}[l]
+    return np.where(x < 0.1, small, big)
+
+
+def make_mask(rad, nrps, rps, eta):
+    """make_mask_function (input_pp.f90:1437-1542); rmask[i - 1] at rad(i).
+    numpy's symmetric eigensolver stands in for LAPACK dsyev."""
+    M = 200
+    x = np.arange(1, M + 1) / M
+    mat = np.zeros((M, M))
+    for i in range(M):
+        xp = 2.0 * x[i]
+        mat[i, i] = np.sin(xp * eta) / xp + M * np.pi - eta
+        for j in range(i + 1, M):
+            a, b = x[i] + x[j], x[i] - x[j]
+            mat[i, j] = mat[j, i] = np.sin(a * eta) / a - np.sin(b * eta) / b
+    w, V = np.linalg.eigh(mat)
+    u = V[:, 0]
+    n0 = 3.0 * u[0] / x[0] - 3.0 * u[1] / x[1] + u[2] / x[2]
+    nm = u / x / n0
+    k = np.pi * np.arange(1, M + 1)
+    dx = x[1] - x[0]
+    kx = k[:, None] * x[None, :]
+    nmk = _seqsum(nm[None, :] * kx * np.sin(kx), 1) * dx / k ** 2
+    dk = k[1] - k[0]
+    rmask = np.zeros(nrps)
+    r = rad[1:nrps]
+    kx = k[None, :] * r[:, None] / rps
+    rmask[1:] = (2.0 / np.pi) * _seqsum(nmk[None, :] * kx * np.sin(kx), 1) * dk * rps ** 2 / r ** 2
+    rmask[0] = rmask[1] - (rmask[2] - rmask[1]) / (rad[2] - rad[1]) * (rad[1] - rad[0])
+    i1, i2, i3 = nrps - 2, nrps - 1, nrps
+    rmask[i3 - 1] = rmask[i2 - 1] + (rmask[i2 - 1] - rmask[i1 - 1]) / (rad[i2 - 1] - rad[i1 - 1]) * \
+        (rad[i3 - 1] - rad[i2 - 1])
+    return rmask
+
+
+def mask_element(el, hmax, alpha, gamma, eta):
+    """ps_masking (input_pp.f90:1302-1434) and the table part of
+    making_ps_with_masking (:848-1016): returns uv[k, l] at rad(k + 1),
+    k = 0..nrps-1, before the norm; el.rps / el.nrps widened."""
+    rps = gamma * el.rps
+    i = 1
+    while i <= len(el.rad) and not (el.rad[i - 1] > rps):
+        i += 1
+    el.nrps = i
+    el.rps = float(el.rad[i - 1])
+    mask = make_mask(el.rad, el.nrps, el.rps, eta)
+    mr, nl, nrps = el.mr, el.mlps + 1, el.nrps
+    uv = el.upp[: mr + 1, :nl] * (el.vpp[: mr + 1, :nl] - el.vpp[: mr + 1, el.lref][:, None])
+    uv[:nrps] = uv[:nrps] / mask[:, None]
+    nkmax = 1000
+    kmax = alpha * np.pi / hmax
+    radk = kmax * (np.arange(nkmax) / (nkmax - 1))
+    rad = el.rad
+    wk = np.zeros((nkmax, nl))
+    dr = rad[1:mr] - rad[0:mr - 1]                       # j = 1..mr-1: rad(j + 1) - rad(j)
+    for l in range(nl):
+        kr1 = radk[:, None] * rad[None, 0:mr - 1]
+        kr2 = radk[:, None] * rad[None, 1:mr]
+        t = 0.5 * (xjl(kr1, l) * uv[None, 0:mr - 1, l] + xjl(kr2, l) * uv[None, 1:mr, l]) * dr[None, :]
+        wk[:, l] = _seqsum(t, 1)
+    out = np.zeros((mr + 1, nl))
+    dk = radk[1:] - radk[:-1]
+    for l in range(nl):
+        kr1 = radk[:-1, None] * rad[None, 0:mr]
+        kr2 = radk[1:, None] * rad[None, 0:mr]
+        t = 0.5 * (xjl(kr1, l) * wk[:-1, l][:, None] + xjl(kr2, l) * wk[1:, l][:, None]) * dk[:, None]
+        out[0:mr, l] = _seqsum(t, 0)
+    out[mr] = 2.0 * out[mr - 1] - out[mr - 2]
+    out = (2.0 / np.pi) * out
+    out[:nrps] = out[:nrps] * mask[:, None]
+    for l in range(nl):
+        cst = np.sqrt((2.0 * l + 1.0) / (4.0 * np.pi))
+        out[1:mr + 1, l] = out[1:mr + 1, l] * cst / rad[1:mr + 1] ** (l + 1)
+        out[0, l] = 2.0 * out[1, l] - out[2, l]
+    return out[:nrps]
+
+
 class KyElement:
     """One element read and prepared as input_pp does (ps_format 'KY' by
     default; fmt 'ABINIT', 'ABINITFHI' or 'FHI' for the other one-projector
     readers)."""
 
-    def __init__(self, path, lmax_ps, lloc, nrmax, fmt="KY"):
+    def __init__(self, path, lmax_ps, lloc, nrmax, fmt="KY", mask=None, hmax=None):
         if fmt == "KY":
             mlps, rrc = _read_ky(self, path, nrmax)
         elif fmt == "ABINIT":
@@ -263,16 +358,21 @@ class KyElement:
             if abs(s) < 1e-10:
                 self.inorm[l] = 0
             self.anorm[l] = np.sqrt(s)
-        # making_ps_without_masking
-        for l in range(mlps + 1):
-            for k in range(1, self.mr + 1):
-                self.upp[k, l] = self.upp[k, l] * np.sqrt((2 * l + 1.0) / (4 * np.pi)) / self.rad[k] ** (l + 1)
-            self.upp[0, l] = self.upp[1, l]
+        if mask is not None:  # yn_psmask = 'y': mask = (alpha_mask, gamma_mask, eta_mask)
+            uvm = mask_element(self, hmax, *mask)
+        else:  # making_ps_without_masking
+            for l in range(mlps + 1):
+                for k in range(1, self.mr + 1):
+                    self.upp[k, l] = self.upp[k, l] * np.sqrt((2 * l + 1.0) / (4 * np.pi)) / self.rad[k] ** (l + 1)
+                self.upp[0, l] = self.upp[1, l]
         self.coef = []
         xn = self.rad[: self.nrps]
         for l in range(mlps + 1):
-            yn = np.array([(self.vpp[k - 1, l] - self.vpp[k - 1, lloc]) * self.upp[k - 1, l]
-                           for k in range(1, self.nrps + 1)])
+            if mask is not None:
+                yn = uvm[:, l].copy()
+            else:
+                yn = np.array([(self.vpp[k - 1, l] - self.vpp[k - 1, lloc]) * self.upp[k - 1, l]
+                               for k in range(1, self.nrps + 1)])
             if self.inorm[l] != 0:
                 yn = yn / self.anorm[l]
             self.coef.append(spline(xn, yn))
@@ -324,12 +424,13 @@ def _vpsl_periodic(el, rion, kion, num, al):
     return np.asfortranarray(vt.real)
 
 
-def init_ps_ky(files, lloc_ps, grid, rion, kion, lmax_ps=None, by_name=False):
+def init_ps_ky(files, lloc_ps, grid, rion, kion, lmax_ps=None, by_name=False, mask=None):
     """(mps, jxyz, rxyz, uv, ia_tbl, rinv_uvu, Vpsl or None) as init_ps builds them."""
     periodic = bool(grid.periodic)
     nrmax = 3000 if periodic else 20000
     el = [KyElement(f, None if lmax_ps is None else lmax_ps[k], lloc_ps[k], nrmax,
-                    _format_of(f) if by_name else "KY") for k, f in enumerate(files)]
+                    _format_of(f) if by_name else "KY", mask=mask, hmax=float(np.max(grid.hgs)))
+          for k, f in enumerate(files)]
     rion = np.asarray(rion, dtype=np.float64).reshape(3, -1, order="F")
     natom = rion.shape[1]
     num = [int(n) for n in grid.num]

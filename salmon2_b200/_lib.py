@@ -71,6 +71,7 @@ SIGNATURES = {
     "sb200_calc_microscopic_current": (C.c_int, [_vp, _vp, _vp]),
     "sb200_init_ps_ky": (C.c_int, [C.c_int, C.POINTER(C.c_char_p), _ip, _ip, C.c_int, _ip, _ip, _dp, C.c_double,
                                    C.c_int, _ip, _dp, _ip, _ip, _ip, _ip, _dp, _dp, _ip, _dp, _dp]),
+    "sb200_set_psmask": (C.c_int, [C.c_int, C.c_double, C.c_double, C.c_double]),
     "sb200_init_ps": (C.c_int, [C.c_int, C.POINTER(C.c_char_p), _ip, _ip, C.c_int, _ip, _ip, _dp, C.c_double,
                                 C.c_int, _ip, _dp, _ip, _ip, _ip, _ip, _dp, _dp, _ip, _dp, _dp]),
     "sb200_set_hartree_cg": (C.c_int, [_vp, _vp, C.c_int, C.c_int, _dp, C.c_int, _ip, C.c_double, C.c_int]),

@@ -358,9 +358,193 @@ int read_fhi(const char* path, int nrmax, PsElement& e, std::vector<double>& rrc
   return SB200_OK;
 }
 
+// Masking of the radial KB functions (yn_psmask = 'y'; alpha_mask,
+// gamma_mask, eta_mask), process-wide as the reference's input variables.
+struct PsMask {
+  int on = 0;
+  double alpha = 0.8, gamma = 1.8, eta = 15.0;  // the reference's defaults (inputoutput.f90:680-682)
+};
+PsMask g_psmask;
+
+// x j_l(x), the Riccati-Bessel function, and its derivative: the closed forms
+// in sin / cos, and below x = 0.1 the Taylor series the reference uses
+// (xjl / dxjl, salmon_math.f90:289-383), l = 0..3
+double xjl(double x, int l) {
+  if (x < 0.1) {
+    const double x2 = x * x, x3 = x2 * x, x4 = x2 * x2, x5 = x4 * x, x6 = x3 * x3, x7 = x6 * x, x8 = x4 * x4,
+                 x9 = x8 * x;
+    switch (l) {
+      case 0: return x - x3 / 6.0 + x5 / 120.0 - x7 / 5040.0 + x9 / 362880.0;
+      case 1: return (2.0 / 6.0) * x2 - (2.0 / 60.0) * x4 + (1.0 / 840.0) * x6 - (2.0 / 90720.0) * x8;
+      case 2: return (4.0 / 60.0) * x3 - (4.0 / 840.0) * x5 + (2.0 / 15120.0) * x7 - (2.0 / 997920.0) * x9;
+      default: return (8.0 / 840.0) * x4 - (8.0 / 15120.0) * x6 + (4.0 / 332640.0) * x8;
+    }
+  }
+  const double s = std::sin(x), c = std::cos(x);
+  switch (l) {
+    case 0: return s;
+    case 1: return (1.0 / x) * s - c;
+    case 2: return (3.0 / (x * x) - 1.0) * s - (3.0 / x) * c;
+    default: return (15.0 / (x * x * x) - 6.0 / x) * s - (15.0 / (x * x) - 1.0) * c;
+  }
+}
+
+// lowest eigenpair's vector of the symmetric n x n matrix a (row-major,
+// overwritten) by cyclic Jacobi rotations (the reference calls LAPACK dsyev);
+// its sign is arbitrary
+void lowest_eigenvector(std::vector<double>& a, int n, std::vector<double>& vec) {
+  std::vector<double> v((size_t)n * n, 0.0);
+  for (int i = 0; i < n; ++i) v[(size_t)i * n + i] = 1.0;
+  for (int sweep = 0; sweep < 100; ++sweep) {
+    double off = 0.0, tot = 0.0;
+    for (int i = 0; i < n; ++i)
+      for (int j = 0; j < n; ++j) {
+        const double x = a[(size_t)i * n + j] * a[(size_t)i * n + j];
+        tot += x;
+        if (i != j) off += x;
+      }
+    if (off <= 1e-30 * tot) break;
+    for (int p = 0; p < n - 1; ++p)
+      for (int q = p + 1; q < n; ++q) {
+        const double apq = a[(size_t)p * n + q];
+        if (apq == 0.0) continue;
+        const double app = a[(size_t)p * n + p], aqq = a[(size_t)q * n + q];
+        const double theta = (aqq - app) / (2.0 * apq);
+        const double t = (theta >= 0.0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
+        const double cs = 1.0 / std::sqrt(t * t + 1.0), sn = t * cs;
+        for (int k = 0; k < n; ++k) {  // columns p, q
+          const double akp = a[(size_t)k * n + p], akq = a[(size_t)k * n + q];
+          a[(size_t)k * n + p] = cs * akp - sn * akq;
+          a[(size_t)k * n + q] = sn * akp + cs * akq;
+        }
+        for (int k = 0; k < n; ++k) {  // rows p, q
+          const double apk = a[(size_t)p * n + k], aqk = a[(size_t)q * n + k];
+          a[(size_t)p * n + k] = cs * apk - sn * aqk;
+          a[(size_t)q * n + k] = sn * apk + cs * aqk;
+        }
+        for (int k = 0; k < n; ++k) {
+          const double vkp = v[(size_t)k * n + p], vkq = v[(size_t)k * n + q];
+          v[(size_t)k * n + p] = cs * vkp - sn * vkq;
+          v[(size_t)k * n + q] = sn * vkp + cs * vkq;
+        }
+      }
+  }
+  int lo = 0;
+  for (int i = 1; i < n; ++i)
+    if (a[(size_t)i * n + i] < a[(size_t)lo * n + lo]) lo = i;
+  vec.resize(n);
+  for (int i = 0; i < n; ++i) vec[i] = v[(size_t)i * n + lo];
+}
+
+// make_mask_function (input_pp.f90:1437-1542): the normalized mask on x in
+// (0, 1] as the lowest eigenvector of the M = 200 concentration matrix
+// (sin((x_i + x_j) eta) / (x_i + x_j) - sin((x_i - x_j) eta) / (x_i - x_j),
+// diagonal sin(2 x_i eta) / (2 x_i) + M pi - eta), divided by x and by its
+// value extrapolated to x = 0; its sine transform on k = pi, 2 pi, ..., M pi;
+// back on the radial grid r / rps for i = 2..nrps, the first and last points
+// extrapolated linearly.  rmask[i - 1] = mask(rad(i)).
+void make_mask(const PsElement& e, double eta, std::vector<double>& rmask) {
+  const int M = 200;
+  std::vector<double> x(M), mat((size_t)M * M), nm(M), k(M), nmk(M, 0.0);
+  for (int i = 0; i < M; ++i) x[i] = (double)(i + 1) / (double)M;
+  for (int i = 0; i < M; ++i) {
+    const double xp = 2.0 * x[i];
+    mat[(size_t)i * M + i] = std::sin(xp * eta) / xp + (double)M * PP_PI - eta;
+    for (int j = i + 1; j < M; ++j) {
+      const double a = x[i] + x[j], b = x[i] - x[j];
+      const double m = std::sin(a * eta) / a - std::sin(b * eta) / b;
+      mat[(size_t)i * M + j] = m;
+      mat[(size_t)j * M + i] = m;
+    }
+  }
+  std::vector<double> u;
+  lowest_eigenvector(mat, M, u);
+  const double n0 = 3.0 * u[0] / x[0] - 3.0 * u[1] / x[1] + u[2] / x[2];
+  for (int i = 0; i < M; ++i) nm[i] = u[i] / x[i] / n0;
+  for (int i = 0; i < M; ++i) k[i] = PP_PI * (double)(i + 1);
+  const double dx = x[1] - x[0];
+  for (int i = 0; i < M; ++i) {
+    double acc = 0.0;
+    for (int j = 0; j < M; ++j) {
+      const double kx = k[i] * x[j];
+      acc = acc + nm[j] * kx * std::sin(kx);
+    }
+    nmk[i] = acc * dx / (k[i] * k[i]);
+  }
+  const int nrps = e.nrps;
+  rmask.assign(nrps, 0.0);
+  const double dk = k[1] - k[0];
+  for (int i = 2; i <= nrps; ++i) {
+    double acc = 0.0;
+    for (int j = 0; j < M; ++j) {
+      const double kx = k[j] * e.rad[i - 1] / e.rps;
+      acc = acc + nmk[j] * kx * std::sin(kx);
+    }
+    rmask[i - 1] = (2.0 / PP_PI) * acc * dk * e.rps * e.rps / (e.rad[i - 1] * e.rad[i - 1]);
+  }
+  rmask[0] = rmask[1] - (rmask[2] - rmask[1]) / (e.rad[2] - e.rad[1]) * (e.rad[1] - e.rad[0]);
+  const int i1 = nrps - 2, i2 = nrps - 1, i3 = nrps;
+  rmask[i3 - 1] = rmask[i2 - 1] + (rmask[i2 - 1] - rmask[i1 - 1]) / (e.rad[i2 - 1] - e.rad[i1 - 1]) *
+                                      (e.rad[i3 - 1] - e.rad[i2 - 1]);
+}
+
+// ps_masking (input_pp.f90:1302-1434) and the table part of
+// making_ps_with_masking (:848-1016) for one-projector channels: the cut-off
+// widened to gamma_mask rps (snapped to the next grid point), uv_l = u_l
+// (v_l - v_lloc) divided by the mask, its Bessel transform (trapezoid on the
+// file's grid) on nkmax = 1000 points up to alpha_mask pi / max(h), the
+// transform back (trapezoid in k) times 2 / pi and the mask, then
+// sqrt((2l+1)/4pi) / r^(l+1); uvm[l][i] = uv_l at rad(i + 1), i = 0..nrps-1.
+int mask_element(PsElement& e, double hmax, std::vector<std::vector<double>>& uvm) {
+  const PsMask& m = g_psmask;
+  e.rps = m.gamma * e.rps;
+  int i = 1;
+  for (; i <= (int)e.rad.size(); ++i)
+    if (e.rad[i - 1] > e.rps) break;
+  if (i > e.mr - 2) return set_error(SB200_ERR_INVALID_ARG, "masked cut-off gamma_mask rps beyond the file's grid");
+  e.nrps = i;
+  e.rps = e.rad[e.nrps - 1];
+  std::vector<double> mask;
+  make_mask(e, m.eta, mask);
+  const int mr = e.mr, nl = e.mlps + 1;
+  std::vector<std::vector<double>> uv(nl, std::vector<double>(mr + 1, 0.0));
+  for (int l = 0; l < nl; ++l) {
+    for (int k = 0; k <= mr; ++k) uv[l][k] = e.upp[l][k] * (e.vpp[l][k] - e.vpp[e.lref][k]);
+    for (int k = 0; k < e.nrps; ++k) uv[l][k] = uv[l][k] / mask[k];
+  }
+  const int nkmax = 1000;
+  const double kmax = m.alpha * PP_PI / hmax;
+  std::vector<double> radk(nkmax);
+  for (int q = 0; q < nkmax; ++q) radk[q] = kmax * ((double)q / (double)(nkmax - 1));
+  std::vector<std::vector<double>> wk(nl, std::vector<double>(nkmax, 0.0));
+  for (int q = 0; q < nkmax; ++q)
+    for (int j = 1; j <= mr - 1; ++j) {
+      const double kr1 = radk[q] * e.rad[j - 1], kr2 = radk[q] * e.rad[j], dr = e.rad[j] - e.rad[j - 1];
+      for (int l = 0; l < nl; ++l)
+        wk[l][q] = wk[l][q] + 0.5 * (xjl(kr1, l) * uv[l][j - 1] + xjl(kr2, l) * uv[l][j]) * dr;
+    }
+  for (int l = 0; l < nl; ++l) std::fill(uv[l].begin(), uv[l].end(), 0.0);
+  for (int q = 0; q < nkmax - 1; ++q)
+    for (int j = 1; j <= mr; ++j) {
+      const double kr1 = radk[q] * e.rad[j - 1], kr2 = radk[q + 1] * e.rad[j - 1], dk = radk[q + 1] - radk[q];
+      for (int l = 0; l < nl; ++l)
+        uv[l][j - 1] = uv[l][j - 1] + 0.5 * (xjl(kr1, l) * wk[l][q] + xjl(kr2, l) * wk[l][q + 1]) * dk;
+    }
+  for (int l = 0; l < nl; ++l) {
+    uv[l][mr] = 2.0 * uv[l][mr - 1] - uv[l][mr - 2];
+    for (int k = 0; k <= mr; ++k) uv[l][k] = (2.0 / PP_PI) * uv[l][k];
+    for (int k = 0; k < e.nrps; ++k) uv[l][k] = uv[l][k] * mask[k];
+    const double cst = std::sqrt((2.0 * l + 1.0) / (4.0 * PP_PI));
+    for (int k = 1; k <= mr; ++k) uv[l][k] = uv[l][k] * cst / std::pow(e.rad[k], l + 1);
+    uv[l][0] = 2.0 * uv[l][1] - uv[l][2];
+  }
+  uvm.swap(uv);
+  return SB200_OK;
+}
+
 // input_pp's common part (input_pp.f90:93-193) and making_ps_without_masking
 // (:1111-1240) for an element read by one of the readers above
-int finish_element(PsElement& e, const std::vector<double>& rrc, int lmax_ps, int lloc, int nrmax) {
+int finish_element(PsElement& e, const std::vector<double>& rrc, int lmax_ps, int lloc, int nrmax, double hmax) {
   e.nrmax = nrmax;
   if (lmax_ps >= 0) {
     if (lmax_ps > e.mlps) return set_error(SB200_ERR_INVALID_ARG, "Lmax_ps above the file's angular momenta");
@@ -407,11 +591,17 @@ int finish_element(PsElement& e, const std::vector<double>& rrc, int lmax_ps, in
     if (std::fabs(s) < 1e-10) e.inorm[l] = 0;
     e.anorm[l] = std::sqrt(s);
   }
-  // making_ps_without_masking: radial functions / r^(l+1), then the KB tables
-  for (int l = 0; l <= e.mlps; ++l) {
-    for (int k = 1; k <= e.mr; ++k)
-      e.upp[l][k] = e.upp[l][k] * std::sqrt((2 * l + 1.0) / (4 * PP_PI)) / std::pow(e.rad[k], l + 1);
-    e.upp[l][0] = e.upp[l][1];
+  std::vector<std::vector<double>> uvm;  // masked udv_l before the norm (yn_psmask = 'y')
+  if (g_psmask.on) {
+    const int r = mask_element(e, hmax, uvm);
+    if (r != SB200_OK) return r;
+  } else {
+    // making_ps_without_masking: radial functions / r^(l+1), then the KB tables
+    for (int l = 0; l <= e.mlps; ++l) {
+      for (int k = 1; k <= e.mr; ++k)
+        e.upp[l][k] = e.upp[l][k] * std::sqrt((2 * l + 1.0) / (4 * PP_PI)) / std::pow(e.rad[k], l + 1);
+      e.upp[l][0] = e.upp[l][1];
+    }
   }
   e.sa.assign(e.mlps + 1, {});
   e.sb.assign(e.mlps + 1, {});
@@ -420,7 +610,7 @@ int finish_element(PsElement& e, const std::vector<double>& rrc, int lmax_ps, in
   std::vector<double> xn(e.rad.begin(), e.rad.begin() + e.nrps), yn(e.nrps);
   for (int l = 0; l <= e.mlps; ++l) {
     for (int k = 1; k <= e.nrps; ++k) {
-      yn[k - 1] = (e.vpp[l][k - 1] - e.vpp[e.lref][k - 1]) * e.upp[l][k - 1];
+      yn[k - 1] = g_psmask.on ? uvm[l][k - 1] : (e.vpp[l][k - 1] - e.vpp[e.lref][k - 1]) * e.upp[l][k - 1];
       if (e.inorm[l] != 0) yn[k - 1] = yn[k - 1] / e.anorm[l];
     }
     natural_spline(xn, yn, e.nrps, e.sa[l], e.sb[l], e.sc[l], e.sd[l]);
@@ -437,7 +627,7 @@ bool ends_with(const std::string& s, const char* suffix) {
 // force_ky: the file is read as 'KY' whatever its name; otherwise the format
 // follows the file name as init_pp does (salmon_pp.f90:66-100): _rps.dat KY,
 // .pspnc ABINIT, .fhi ABINITFHI, .cpi FHI.
-int read_element(const char* path, bool force_ky, int lmax_ps, int lloc, int nrmax, PsElement& e) {
+int read_element(const char* path, bool force_ky, int lmax_ps, int lloc, int nrmax, double hmax, PsElement& e) {
   const std::string name(path);
   std::vector<double> rrc;
   int r;
@@ -458,7 +648,7 @@ int read_element(const char* path, bool force_ky, int lmax_ps, int lloc, int nrm
     return set_error(SB200_ERR_INVALID_ARG, "unknown pseudopotential file format: " + name);
   }
   if (r != SB200_OK) return r;
-  return finish_element(e, rrc, lmax_ps, lloc, nrmax);
+  return finish_element(e, rrc, lmax_ps, lloc, nrmax, hmax);
 }
 
 int init_ps_impl(bool force_ky, int nelem, const char* const* files, const int* lmax_ps, const int* lloc_ps,
@@ -470,9 +660,10 @@ int init_ps_impl(bool force_ky, int nelem, const char* const* files, const int* 
     return set_error(SB200_ERR_INVALID_ARG, "sb200_init_ps: null or inconsistent argument");
   const int nrmax = periodic ? 3000 : 20000;  // read_pslfile, salmon_pp.f90:34-38
   std::vector<PsElement> el(nelem);
+  const double hgs_max = hgs[0] > hgs[1] ? (hgs[0] > hgs[2] ? hgs[0] : hgs[2]) : (hgs[1] > hgs[2] ? hgs[1] : hgs[2]);
   for (int k = 0; k < nelem; ++k) {
     if (!files[k]) return set_error(SB200_ERR_INVALID_ARG, "null pseudopotential file name");
-    const int r = read_element(files[k], force_ky, lmax_ps ? lmax_ps[k] : -1, lloc_ps[k], nrmax, el[k]);
+    const int r = read_element(files[k], force_ky, lmax_ps ? lmax_ps[k] : -1, lloc_ps[k], nrmax, hgs_max, el[k]);
     if (r != SB200_OK) return r;
   }
   for (int a = 0; a < natom; ++a)
@@ -708,4 +899,17 @@ extern "C" int sb200_init_ps(int nelem, const char* const* files, const int* lma
                              int* jxyz, double* rxyz, double* uv, int* ia_tbl, double* rinv_uvu, double* Vpsl) {
   return init_ps_impl(false, nelem, files, lmax_ps, lloc_ps, periodic, num, is, hgs, hvol, natom, kion, Rion, nps,
                       nlma, mps, jxyz, rxyz, uv, ia_tbl, rinv_uvu, Vpsl);
+}
+
+extern "C" int sb200_set_psmask(int yn_psmask, double alpha_mask, double gamma_mask, double eta_mask) {
+  if (yn_psmask != 0 && yn_psmask != 1) return set_error(SB200_ERR_INVALID_ARG, "yn_psmask is 0 or 1");
+  if (yn_psmask && !(alpha_mask > 0.0 && gamma_mask >= 1.0 && eta_mask > 0.0))
+    return set_error(SB200_ERR_INVALID_ARG, "alpha_mask > 0, gamma_mask >= 1 and eta_mask > 0 are required");
+  g_psmask.on = yn_psmask;
+  if (yn_psmask) {
+    g_psmask.alpha = alpha_mask;
+    g_psmask.gamma = gamma_mask;
+    g_psmask.eta = eta_mask;
+  }
+  return SB200_OK;
 }

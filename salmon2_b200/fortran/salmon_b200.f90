@@ -127,6 +127,13 @@ module salmon_b200
       type(c_ptr), value :: mps, jxyz, rxyz, uv, ia_tbl, rinv_uvu, Vpsl
     end function
 
+    integer(c_int) function sb200_set_psmask(yn_psmask, alpha_mask, gamma_mask, eta_mask) &
+        bind(c, name="sb200_set_psmask")
+      import
+      integer(c_int), value :: yn_psmask
+      real(c_double), value :: alpha_mask, gamma_mask, eta_mask
+    end function
+
     integer(c_int) function sb200_init_ps(nelem, files, lmax_ps, lloc_ps, periodic, num, is, hgs, hvol, &
         natom, kion, Rion, nps, nlma, mps, jxyz, rxyz, uv, ia_tbl, rinv_uvu, Vpsl) bind(c, name="sb200_init_ps")
       import

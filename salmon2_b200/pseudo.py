@@ -59,3 +59,10 @@ def _init_ps(entry, files, lloc_ps, grid, rion, kion, lmax_ps, vpsl):
     check(fn(*args, C.byref(nps), C.byref(nlma), P(mps, _ip), P(jxyz, _ip), P(rxyz), P(uv),
                                  P(ia, _ip), P(rinv), P(v)))
     return PPGrid(natom, n, m, mps, jxyz, rxyz, uv, ia, rinv), v
+
+
+def set_psmask(yn_psmask, alpha_mask=0.8, gamma_mask=1.8, eta_mask=15.0):
+    """yn_psmask and its parameters for the following set-ups (process-wide, as
+    the reference's input variables): masked radial KB functions
+    (making_ps_with_masking, input_pp.f90:848-1016)."""
+    check(lib().sb200_set_psmask(1 if yn_psmask else 0, float(alpha_mask), float(gamma_mask), float(eta_mask)))

@@ -46,10 +46,12 @@ def rel_err(a, b):
     return float(np.max(np.abs(a - b)) / (den if den > 0 else 1.0))
 
 
-def write_ky_file(path, zps=4.0, mlps=2, mr=400, step=0.01, rc=1.1, seed=0):
+def write_ky_file(path, zps=4.0, mlps=2, mr=400, step=0.01, rc=1.1, seed=0, compact=False):
     """A Yabana-Bertsch (`_rps.dat`, ps_format 'KY') file with smooth analytic
     channels (angstrom / eV, the format's units): v_l(r) = -zps e^2 erf(r/0.4)/r
-    + A_l exp(-(r/0.5)^2), u_l(r) = r^(l+1) exp(-r^2 / 0.72); cut-off radii rc."""
+    + A_l exp(-(r/0.5)^2), u_l(r) = r^(l+1) exp(-r^2 / 0.72); cut-off radii rc.
+    compact: the channels differ by A_l (1 - (r/rc)^2)^3 inside rc only, so
+    they are equal beyond it as in real files."""
     from math import erf
     rng = np.random.default_rng(seed)
     e2 = 14.399645  # eV * angstrom
@@ -61,7 +63,10 @@ def write_ky_file(path, zps=4.0, mlps=2, mr=400, step=0.01, rc=1.1, seed=0):
         vs = []
         for l in range(mlps + 1):
             vc = -zps * e2 * (erf(r / 0.4) / r if r > 0 else 2.0 / (0.4 * np.sqrt(np.pi)))
-            vs.append(vc + amp[l] * np.exp(-(r / 0.5) ** 2))
+            if compact:
+                vs.append(vc + (amp[l] * (1.0 - (r / rc) ** 2) ** 3 if r < rc else 0.0))
+            else:
+                vs.append(vc + amp[l] * np.exp(-(r / 0.5) ** 2))
         lines.append(f"{r:11.4f} {0.0:11.5f} " + " ".join(f"{v:14.7f}" for v in vs))
     for r in rs:
         us = [r ** (l + 1) * np.exp(-r * r / 0.72) for l in range(mlps + 1)]

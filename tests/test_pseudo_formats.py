@@ -115,3 +115,79 @@ def test_ky_file_through_the_general_entry_equals_the_ky_entry(tmp_path):
     pa, va = pseudo.init_ps([f], [1], g, _rion(True), [1, 1])
     pb, vb = pseudo.init_ps_ky([f], [1], g, _rion(True), [1, 1])
     assert np.array_equal(pa.uv, pb.uv) and np.array_equal(va, vb) and np.array_equal(pa.jxyz, pb.jxyz)
+
+
+@pytest.fixture
+def psmask():
+    from salmon2_b200 import pseudo
+    yield pseudo.set_psmask
+    pseudo.set_psmask(False)
+
+
+@pytest.mark.parametrize("periodic", [False, True], ids=["isolated", "periodic"])
+def test_masked_tables_equal_oracle(tmp_path, psmask, periodic):
+    """yn_psmask = 'y' (making_ps_with_masking, ps_masking, make_mask_function)
+    with the reference's default alpha_mask, gamma_mask, eta_mask.  Tolerance
+    1e-9 relative: the mask is the lowest eigenvector of a 200 x 200 matrix of
+    norm 628 whose two lowest eigenvalues are 1.6e-7 and 3.0e-4, so any two
+    symmetric eigensolvers (the library's Jacobi, numpy's, the reference's
+    LAPACK dsyev) agree on it only to about eps * 628 / 3e-4 = 2e-10."""
+    f = S.write_ky_file(str(tmp_path / "A_rps.dat"), zps=4.0, mlps=2, seed=14, compact=True, mr=500)
+    g = _grid(periodic)
+    psmask(True, 0.8, 1.8, 15.0)
+    pp, v = _lib([f], [2], g, _rion(periodic), [1, 1])
+    mps, jxyz, rxyz, uv, ia, rinv, vref = PK.init_ps_ky([f], [2], g, _rion(periodic), [1, 1], mask=(0.8, 1.8, 15.0))
+    assert np.array_equal(pp.mps, mps) and np.array_equal(pp.jxyz, jxyz)
+    assert np.array_equal(pp.rinv_uvu, rinv)
+    assert np.max(np.abs(pp.uv - uv)) <= 1e-9 * np.max(np.abs(uv))
+    assert np.max(np.abs(v - vref)) <= 1e-11 * np.max(np.abs(vref))
+
+
+def test_masking_widens_the_sphere_and_keeps_the_smooth_projector(tmp_path, psmask):
+    """The masked tables reach gamma_mask rps (more sphere points), and for a
+    smooth projector the filtered, masked function stays close to the
+    unmasked one inside the file's cut-off (the filter passes |k| below
+    alpha_mask pi / h; the mask is near 1 at small r / rps)."""
+    f = S.write_ky_file(str(tmp_path / "A_rps.dat"), zps=4.0, mlps=1, seed=15, compact=True, rc=1.3, mr=500)
+    g = _grid(False)
+    rion = np.array([[0.3, -0.2, 1.1]]).T
+    p0, _ = _lib([f], [1], g, rion, [1])
+    psmask(True)
+    p1, _ = _lib([f], [1], g, rion, [1])
+    assert p1.mps[0] > 2 * p0.mps[0]
+    # the sphere points of the unmasked table, looked up in the masked one
+    r0 = np.linalg.norm(p0.rxyz[:, : p0.mps[0], 0], axis=0)
+    idx1 = {tuple(p1.jxyz[:, j, 0]): j for j in range(p1.mps[0])}
+    sel = [j for j in range(p0.mps[0]) if r0[j] < 0.5 * 1.3 / 0.52917721067]
+    a = p0.uv[sel, 0]
+    b = p1.uv[[idx1[tuple(p0.jxyz[:, j, 0])] for j in sel], 0]
+    assert np.max(np.abs(a - b)) < 0.05 * np.max(np.abs(a))
+
+
+def test_mask_function_is_normalized_and_vanishes_at_the_cut_off():
+    """make_mask_function: 1 at r = 0 (its normalization), decreasing to about
+    zero at rps."""
+    rad = np.linspace(0.0, 3.0, 301)
+    m = PK.make_mask(rad, 201, rad[200], 15.0)
+    assert abs(m[0] - 1.0) < 1e-3
+    assert abs(m[-1]) < 2e-2 and np.all(np.diff(m[1:-1]) < 1e-12)
+
+
+def test_masked_tables_from_the_reference_files(psmask):
+    """The reference's own C and H files with yn_psmask = 'y', library
+    against oracle (1e-9, as above)."""
+    import os
+    from test_pseudo_ky import REF_PSEUDO
+    if not os.path.exists(os.path.join(REF_PSEUDO, "C_rps.dat")):
+        pytest.skip("reference pseudopotential files not present")
+    from salmon2_b200 import synth
+    files = [os.path.join(REF_PSEUDO, "C_rps.dat"), os.path.join(REF_PSEUDO, "H_rps.dat")]
+    g = synth.make_grid([48, 48, 48], 0.25 / synth.AU_LENGTH_AA, periodic=False)
+    rion = np.array([[0.0, 0.0, 1.13], [0.0, 0.0, 3.14], [0.0, 0.0, -1.13], [0.0, 0.0, -3.14]]).T
+    psmask(True)
+    pp, v = _lib(files, [1, 0], g, rion, [1, 2, 1, 2], lmax=[1, 0])
+    mps, jxyz, rxyz, uv, ia, rinv, vref = PK.init_ps_ky(files, [1, 0], g, rion, [1, 2, 1, 2], lmax_ps=[1, 0],
+                                                        by_name=True, mask=(0.8, 1.8, 15.0))
+    assert pp.nlma == 2 and np.array_equal(pp.jxyz, jxyz)
+    assert np.max(np.abs(pp.uv - uv)) <= 1e-9 * np.max(np.abs(uv))
+    assert np.max(np.abs(v - vref)) <= 1e-11 * np.max(np.abs(vref))

@@ -313,6 +313,53 @@ int sb200_rt_propagate(sb200_ctx* ctx, double* psi_a, double* psi_b, double* wor
                        int trans_longi, double* curr_out, double* rbox_out,
                        double* Ac_tot_out, double** psi_final);
 
+/* Continuation of the time loop: the next sb200_rt_propagate runs the global
+ * steps itt = Mit + 1 .. Mit + nt (main_tddft.f90:89) instead of 1 .. nt, its
+ * Ac_ext(:, 0:nt+1) taken as the global Ac_ext(:, Mit:Mit+nt+1); with Ac_tot /
+ * Ac_ind (3,2) given (steps Mit and Mit + 1, host; Ac_ind may be NULL = zero),
+ * the loop's field history starts from them ('lo'), else from Ac_ext; the
+ * isolated CG potential is extrapolated from the first step on (itt /= 1).
+ * Used once, by the next loop.  Mit = 0 with NULLs is a fresh start.
+ * Replaces: Mit of restart_rt and read_rtdata
+ * (src/io/checkpoint_restart.f90:277-306,1959-1993).                         */
+int sb200_rt_set_start(sb200_ctx* ctx, int Mit, const double Ac_tot[6], const double Ac_ind[6]);
+/* After a loop: *Mit = the global step it reached, Ac_tot / Ac_ind (3,2) at
+ * that step and the next (host; either may be NULL); what sb200_rt_set_start
+ * takes to continue it exactly.  SB200_ERR_STATE before any loop.
+ * Replaces: the rt%Ac_tot / rt%Ac_ind entries write_rtdata stores
+ * (src/io/checkpoint_restart.f90:1925-1957).                                  */
+int sb200_rt_get_state(sb200_ctx* ctx, int* Mit, double Ac_tot[6], double Ac_ind[6]);
+
+/* Restart data in the reference's file layouts, in directory dir:
+ * info.bin, occupation.bin, the orbitals (method_wf_distributor 0 = 'single':
+ * wfn.bin; 1 = 'slice': k_IK_ob_NB/wfn_ob_IO.dat in blocks of
+ * nblock_wf_distribute orbitals), Vh_stock.bin when the context runs the
+ * isolated CG self-consistent loop, rtdata.bin when trans_longi = 'lo' (the
+ * state of the last loop, sb200_rt_get_state).  psi: the context's orbital
+ * block (device), complex, or real with if_real_orbital = 1 (ground state);
+ * iter: the iteration or step number recorded.  Synchronous.
+ * Replaces: checkpoint_rt / checkpoint_gs -> write_bin, write_wavefunction,
+ * write_Vh_stock, write_rtdata (src/io/checkpoint_restart.f90:88-123,231-396,
+ * 539-677,897-967,1925-1957) for one process.                                 */
+int sb200_write_restart(sb200_ctx* ctx, const char* dir, int method_wf_distributor, int nblock_wf_distribute,
+                        const double* psi, int if_real_orbital, int iter, int trans_longi);
+/* Reads restart data written by the reference (one or many processes: the
+ * 'single' layout is the same) or by sb200_write_restart into the context's
+ * complex orbital block psi (device): the orbitals ik_s .. ik_s+nk-1 and
+ * io_s .. io_s+no-1 of the file's mk x mo (real ground-state orbitals are
+ * widened to complex on the device); the occupations become the context's
+ * (and go to rocc_out(no,nk,nspin) unless NULL).  yn_restart = 1 continues a
+ * propagation: *iter = the stored step, sb200_rt_set_start with the stored
+ * fields ('lo'), and on an isolated CG self-consistent context the stored
+ * potentials with the restart's Hartree solve and V_local update; yn_restart
+ * = 0 (ground-state data starting a propagation): *iter = 0.  Synchronous.
+ * Replaces: restart_rt / restart_gs -> read_bin, read_wavefunction,
+ * read_Vh_stock, read_rtdata (src/io/checkpoint_restart.f90:125-154,277-306,
+ * 400-534,1149-1305,1959-1993) and the yn_restart branch of initialization_rt
+ * (src/rt/initialization_rt.f90:244-283).                                     */
+int sb200_read_restart(sb200_ctx* ctx, const char* dir, int method_wf_distributor, int nblock_wf_distribute,
+                       int yn_restart, int ik_s, int io_s, double* psi, int* iter, double* rocc_out);
+
 /* ---- ground state: real orbitals, one k-point ------------------------------- */
 
 /* The context's orbital block (sb200_set_orbitals with nk = 1) holds real

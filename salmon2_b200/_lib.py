@@ -71,6 +71,11 @@ SIGNATURES = {
     "sb200_calc_microscopic_current": (C.c_int, [_vp, _vp, _vp]),
     "sb200_init_ps_ky": (C.c_int, [C.c_int, C.POINTER(C.c_char_p), _ip, _ip, C.c_int, _ip, _ip, _dp, C.c_double,
                                    C.c_int, _ip, _dp, _ip, _ip, _ip, _ip, _dp, _dp, _ip, _dp, _dp]),
+    "sb200_rt_set_start": (C.c_int, [_vp, C.c_int, _dp, _dp]),
+    "sb200_rt_get_state": (C.c_int, [_vp, _ip, _dp, _dp]),
+    "sb200_write_restart": (C.c_int, [_vp, C.c_char_p, C.c_int, C.c_int, _vp, C.c_int, C.c_int, C.c_int]),
+    "sb200_read_restart": (C.c_int, [_vp, C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _vp, _ip,
+                                     _dp]),
     "sb200_set_psmask": (C.c_int, [C.c_int, C.c_double, C.c_double, C.c_double]),
     "sb200_init_ps": (C.c_int, [C.c_int, C.POINTER(C.c_char_p), _ip, _ip, C.c_int, _ip, _ip, _dp, C.c_double,
                                 C.c_int, _ip, _dp, _ip, _ip, _ip, _ip, _dp, _dp, _ip, _dp, _dp]),

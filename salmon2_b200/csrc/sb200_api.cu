@@ -504,6 +504,8 @@ int sb200_set_orbitals(sb200_ctx* c, int nspin, int no, int nk, const double* ve
   o.nk = nk;
   o.norb = nspin * no * nk;
   o.vec_k.assign(vec_k, vec_k + 3 * nk);
+  o.rocc.assign(rocc, rocc + (size_t)no * nk * nspin);
+  o.wtk.assign(wtk, wtk + nk);
   o.weight.assign(o.norb, 0.0);
   for (int ik = 0; ik < nk; ++ik)
     for (int io = 0; io < no; ++io)
@@ -1037,6 +1039,14 @@ int sb200_rt_propagate(sb200_ctx* c, double* psi_a, double* psi_b, double* work,
   else SB_CUDA(cudaMemsetAsync(r.d_Ac_ext, 0, na * sizeof(double), c->stream));
   SB_CUDA(cudaMemsetAsync(r.d_Ac_ind, 0, na * sizeof(double), c->stream));
   SB_CUDA(cudaMemcpyAsync(r.d_Ac_tot, r.d_Ac_ext, na * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+  // a continued loop (sb200_rt_set_start / sb200_read_restart): local entries 0
+  // and 1 are the steps start_mit and start_mit + 1 (main_tddft.f90:89, itt =
+  // Mit + 1 .. nt; read_rtdata, checkpoint_restart.f90:1959-1993)
+  if (r.seed_on) {
+    SB_CUDA(cudaMemcpyAsync(r.d_Ac_tot, r.seed_tot, 6 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    SB_CUDA(cudaMemcpyAsync(r.d_Ac_ind, r.seed_ind, 6 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  }
+  r.loop_mit0 = r.start_mit;
   const int one = 1;
   SB_CUDA(cudaMemcpyAsync(r.d_step, &one, sizeof(int), cudaMemcpyHostToDevice, c->stream));
   if (!c->g.periodic) {
@@ -1100,9 +1110,43 @@ int sb200_rt_propagate(sb200_ctx* c, double* psi_a, double* psi_b, double* work,
   SB_CUDA(cudaStreamSynchronize(c->stream));
   SB_CUDA(cudaGetLastError());
   TRY(check_device_flag(c));
+  r.last_mit = r.loop_mit0 + nt;
+  r.last_nt = nt;
+  r.start_mit = 0;
+  r.loop_mit0 = 0;
+  r.seed_on = false;
   if (psi_final) *psi_final = (double*)final_buf;
   // leave hpsi coefficients consistent with system%vec_Ac for later hpsi calls
   TRY(refresh_k(c));
+  return SB200_OK;
+}
+
+int sb200_rt_set_start(sb200_ctx* c, int mit, const double Ac_tot[6], const double Ac_ind[6]) {
+  CHECK_CTX(c);
+  if (mit < 0) return set_error(SB200_ERR_INVALID_ARG, "sb200_rt_set_start: Mit < 0");
+  if (Ac_ind && !Ac_tot) return set_error(SB200_ERR_INVALID_ARG, "sb200_rt_set_start: Ac_ind without Ac_tot");
+  RTBuffers& r = c->rt;
+  r.start_mit = mit;
+  r.seed_on = Ac_tot != nullptr || Ac_ind != nullptr;
+  for (int i = 0; i < 6; ++i) {
+    r.seed_tot[i] = Ac_tot ? Ac_tot[i] : 0.0;
+    r.seed_ind[i] = Ac_ind ? Ac_ind[i] : 0.0;
+  }
+  return SB200_OK;
+}
+
+int sb200_rt_get_state(sb200_ctx* c, int* mit, double Ac_tot[6], double Ac_ind[6]) {
+  CHECK_CTX(c);
+  RTBuffers& r = c->rt;
+  if (r.last_nt < 0) return set_error(SB200_ERR_STATE, "no sb200_rt_propagate has run on this context");
+  DeviceGuard dg(c->device);
+  if (mit) *mit = r.last_mit;
+  const size_t off = 3 * (size_t)r.last_nt;  // local entries nt and nt + 1
+  if (Ac_tot)
+    SB_CUDA(cudaMemcpyAsync(Ac_tot, r.d_Ac_tot + off, 6 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  if (Ac_ind)
+    SB_CUDA(cudaMemcpyAsync(Ac_ind, r.d_Ac_ind + off, 6 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  SB_CUDA(cudaStreamSynchronize(c->stream));
   return SB200_OK;
 }
 

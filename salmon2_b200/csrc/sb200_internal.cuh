@@ -42,6 +42,8 @@ struct OrbInfo {
   int nspin = 0, no = 0, nk = 0, norb = 0;
   std::vector<double> vec_k;   // (3,nk)
   std::vector<double> weight;  // per orbital rocc*wtk, orbital order
+  std::vector<double> rocc;    // (no,nk,nspin) as given
+  std::vector<double> wtk;     // (nk)
 };
 
 // Kleinman-Bylander tables, re-indexed for the device.
@@ -101,6 +103,15 @@ struct RTBuffers {
   double* d_rbox = nullptr;     // (4, nt)
   int* d_step = nullptr;        // current itt
   double2* d_zc = nullptr;      // n_hamil coefficients
+  // continuation (sb200_rt_set_start, sb200_read_restart): the next loop runs
+  // global steps start_mit + 1 .. start_mit + nt, its history entries 0 and 1
+  // seeded with Ac_tot / Ac_ind at steps start_mit and start_mit + 1
+  int start_mit = 0;
+  int loop_mit0 = 0;  // start step of the loop being issued (global itt = local + loop_mit0)
+  bool seed_on = false;
+  double seed_tot[6] = {0, 0, 0, 0, 0, 0}, seed_ind[6] = {0, 0, 0, 0, 0, 0};
+  // the last loop: global step reached and its local step count (-1: none yet)
+  int last_mit = 0, last_nt = -1;
 };
 
 // ground-state (real orbital) work state, sb200_gs.cu
@@ -301,12 +312,18 @@ void pcg_default_cells(const sb200_ctx* c, int out[3]);
 int pcg_configure(sb200_ctx* c, int layout, int lmax, const double* rion, int natom, const int npole_xyz[3],
                   double threshold, int maxiter);
 int pcg_issue(sb200_ctx* c, const double* d_rho, double* d_vh, int* iterations);
-int pcg_vh_stock(sb200_ctx* c, const int* d_step, double* d_vh, double* d_s1, double* d_s2, bool before);
+int pcg_vh_stock(sb200_ctx* c, const int* d_step, int offset, double* d_vh, double* d_s1, double* d_s2, bool before);
 // self-consistent time loop (sb200_scf.cu): buffers sized before a capture, and
 // the per-step potential update issued after each Taylor step (no-ops unless
 // sb200_set_self_consistent enabled it)
 int scf_rt_prepare(sb200_ctx* c);
 int scf_rt_issue(sb200_ctx* c, const double2* psi);
+// initialization_rt.f90:268-283 with yn_restart = 'y' (isolated, CG): Vh from the
+// stored potentials, the Hartree solve of psi's density, stock update, V_local
+int scf_restart_potential(sb200_ctx* c, const double2* psi);
+bool scf_cg_on(const sb200_ctx* c);
+// the stored potentials of the CG loop (device), or false when there are none
+bool scf_vh_stock(sb200_ctx* c, double** vh, double** s1, double** s2);
 // sum of a device density over the k-point shards (no-op without a communicator)
 int scf_density_allreduce(sb200_ctx* c, double* d_rho);
 // k-point shard communicator (sb200_set_density_comm): set?, and an in-place

@@ -468,11 +468,11 @@ __global__ void __launch_bounds__(PT) k_pcg_update(PArgs a, cudaGraphConditional
 }
 
 // Vh extrapolation of the isolated time step (time_evolution_step.f90:187-190,
-// 196-198): with the device step counter (itt + 1 after finalize) not 2,
-// Vh = 2 stock1 - stock2 and stock2 = stock1 before the solve (before = 1),
-// stock1 = Vh after it (before = 0)
-__global__ void k_vh_stock(const int* step, double* vh, double* s1, double* s2, long n, int before) {
-  if (*step == 2) return;
+// 196-198): with the global step itt = (device step counter, itt + 1 after
+// finalize) - 1 + offset not 1, Vh = 2 stock1 - stock2 and stock2 = stock1
+// before the solve (before = 1), stock1 = Vh after it (before = 0)
+__global__ void k_vh_stock(const int* step, int offset, double* vh, double* s1, double* s2, long n, int before) {
+  if (*step + offset == 2) return;
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
     if (before) {
       const double a1 = s1[i];
@@ -755,9 +755,10 @@ int pcg_issue(sb200_ctx* c, const double* d_rho, double* d_vh, int* iterations) 
   return SB200_OK;
 }
 
-int pcg_vh_stock(sb200_ctx* c, const int* d_step, double* d_vh, double* d_s1, double* d_s2, bool before) {
+int pcg_vh_stock(sb200_ctx* c, const int* d_step, int offset, double* d_vh, double* d_s1, double* d_s2,
+                 bool before) {
   const long n = c->g.npts;
-  k_vh_stock<<<grid_blocks(n), PT, 0, c->stream>>>(d_step, d_vh, d_s1, d_s2, n, before ? 1 : 0);
+  k_vh_stock<<<grid_blocks(n), PT, 0, c->stream>>>(d_step, offset, d_vh, d_s1, d_s2, n, before ? 1 : 0);
   SB_LAUNCH_CHECK("k_vh_stock");
   return SB200_OK;
 }

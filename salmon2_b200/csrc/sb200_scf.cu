@@ -99,6 +99,7 @@ struct ScfState {
   // Vh from step to step as the CG start value, with the two stored potentials
   // of the extrapolation
   bool cg_on = false;
+  int* d_step0 = nullptr;     // a zero step counter (the restart's stock update)
   double* d_stock1 = nullptr;
   double* d_stock2 = nullptr;
 };
@@ -625,9 +626,9 @@ int scf_rt_issue(sb200_ctx* c, const double2* psi) {
     TRY_S(scf_launch_hartree(c, s->d_rho, s->d_vh, SB200_KIND_POTENTIAL));
   } else if (s->cg_on) {  // time_evolution_step.f90:186-198 with method_poisson = 'cg'
     TRY_S(scf_mark(c, SB200_KIND_POTENTIAL, true));
-    TRY_S(pcg_vh_stock(c, c->rt.d_step, s->d_vh, s->d_stock1, s->d_stock2, true));
+    TRY_S(pcg_vh_stock(c, c->rt.d_step, c->rt.loop_mit0, s->d_vh, s->d_stock1, s->d_stock2, true));
     TRY_S(pcg_issue(c, s->d_rho, s->d_vh, nullptr));
-    TRY_S(pcg_vh_stock(c, c->rt.d_step, s->d_vh, s->d_stock1, s->d_stock2, false));
+    TRY_S(pcg_vh_stock(c, c->rt.d_step, c->rt.loop_mit0, s->d_vh, s->d_stock1, s->d_stock2, false));
     TRY_S(scf_mark(c, SB200_KIND_POTENTIAL, false));
   } else {
     TRY_S(scf_launch_hartree_isolated(c, s->d_rho, s->d_vh, SB200_KIND_POTENTIAL));
@@ -635,6 +636,42 @@ int scf_rt_issue(sb200_ctx* c, const double2* psi) {
   TRY_S(scf_launch_xc(c, s->d_rho, s->d_vxc, SB200_KIND_POTENTIAL, false));
   TRY_S(scf_launch_update(c, s->d_vpsl, s->d_vh, s->d_vxc, SB200_KIND_POTENTIAL));
   SB_LAUNCH_CHECK("self-consistent potential update");
+  return SB200_OK;
+}
+
+bool scf_cg_on(const sb200_ctx* c) {
+  const ScfState* s = c->scf ? static_cast<const ScfState*>(c->scf) : nullptr;
+  return s != nullptr && s->cg_on;
+}
+
+bool scf_vh_stock(sb200_ctx* c, double** vh, double** s1, double** s2) {
+  ScfState* s = scf_of(c);
+  if (!s || !s->cg_on) return false;
+  *vh = s->d_vh;
+  *s1 = s->d_stock1;
+  *s2 = s->d_stock2;
+  return true;
+}
+
+// initialization_rt.f90:268-283 with yn_restart = 'y': Vh = 2 stock1 - stock2,
+// stock2 = stock1, Vh of the density of psi (CG from that start), Vxc,
+// V_local, stock1 = Vh
+int scf_restart_potential(sb200_ctx* c, const double2* psi) {
+  ScfState* s = scf_of(c);
+  if (!s || !s->rt_on || !s->cg_on) return SB200_OK;
+  if (!s->d_step0) {
+    TRY_S(dalloc(&s->d_step0, 1));
+    SB_CUDA(cudaMemsetAsync(s->d_step0, 0, sizeof(int), c->stream));
+  }
+  TRY_S(density_prepare(c));
+  TRY_S(launch_density(c, psi, s->d_rho));
+  TRY_S(scf_density_allreduce(c, s->d_rho));
+  TRY_S(pcg_vh_stock(c, s->d_step0, 0, s->d_vh, s->d_stock1, s->d_stock2, true));
+  TRY_S(pcg_issue(c, s->d_rho, s->d_vh, nullptr));
+  TRY_S(scf_launch_xc(c, s->d_rho, s->d_vxc, -1, false));
+  TRY_S(scf_launch_update(c, s->d_vpsl, s->d_vh, s->d_vxc, -1));
+  TRY_S(pcg_vh_stock(c, s->d_step0, 0, s->d_vh, s->d_stock1, s->d_stock2, false));
+  SB_CUDA(cudaStreamSynchronize(c->stream));
   return SB200_OK;
 }
 
@@ -658,6 +695,7 @@ void scf_free(sb200_ctx* c) {
   dfree(s->d_icoef);
   dfree(s->d_itab);
   dfree(s->d_stock1);
+  dfree(s->d_step0);
   dfree(s->d_stock2);
   delete s;
   c->scf = nullptr;

@@ -127,6 +127,38 @@ module salmon_b200
       type(c_ptr), value :: mps, jxyz, rxyz, uv, ia_tbl, rinv_uvu, Vpsl
     end function
 
+    integer(c_int) function sb200_rt_set_start(ctx, Mit, Ac_tot, Ac_ind) bind(c, name="sb200_rt_set_start")
+      import
+      type(c_ptr), value :: ctx
+      integer(c_int), value :: Mit
+      real(c_double), intent(in) :: Ac_tot(3, 2), Ac_ind(3, 2)
+    end function
+
+    integer(c_int) function sb200_rt_get_state(ctx, Mit, Ac_tot, Ac_ind) bind(c, name="sb200_rt_get_state")
+      import
+      type(c_ptr), value :: ctx
+      integer(c_int), intent(out) :: Mit
+      real(c_double), intent(out) :: Ac_tot(3, 2), Ac_ind(3, 2)
+    end function
+
+    integer(c_int) function sb200_write_restart(ctx, dir, method_wf_distributor, nblock_wf_distribute, psi, &
+        if_real_orbital, iter, trans_longi) bind(c, name="sb200_write_restart")
+      import
+      type(c_ptr), value :: ctx, psi
+      character(kind=c_char), intent(in) :: dir(*)   ! NUL-terminated
+      integer(c_int), value :: method_wf_distributor, nblock_wf_distribute, if_real_orbital, iter, trans_longi
+    end function
+
+    integer(c_int) function sb200_read_restart(ctx, dir, method_wf_distributor, nblock_wf_distribute, &
+        yn_restart, ik_s, io_s, psi, iter, rocc_out) bind(c, name="sb200_read_restart")
+      import
+      type(c_ptr), value :: ctx, psi
+      character(kind=c_char), intent(in) :: dir(*)   ! NUL-terminated
+      integer(c_int), value :: method_wf_distributor, nblock_wf_distribute, yn_restart, ik_s, io_s
+      integer(c_int), intent(out) :: iter
+      real(c_double), intent(inout) :: rocc_out(*)
+    end function
+
     integer(c_int) function sb200_set_psmask(yn_psmask, alpha_mask, gamma_mask, eta_mask) &
         bind(c, name="sb200_set_psmask")
       import

@@ -381,6 +381,37 @@ class Context:
         final = psi_a if fin.value == psi_a.data_ptr() else psi_b
         return dict(psi=final, curr=curr[:, :nt], rbox=rbox[:, :nt], Ac_tot=act)
 
+    def rt_set_start(self, mit, ac_tot=None, ac_ind=None):
+        """The next rt_propagate runs steps mit + 1 .. mit + nt (restart_rt's Mit),
+        its field history from Ac_tot / Ac_ind (3, 2) at steps mit, mit + 1."""
+        t = None if ac_tot is None else np.asfortranarray(ac_tot, dtype=np.float64).reshape(3, 2, order="F")
+        i = None if ac_ind is None else np.asfortranarray(ac_ind, dtype=np.float64).reshape(3, 2, order="F")
+        check(lib().sb200_rt_set_start(self.h, int(mit), None if t is None else _ptr(t), None if i is None else _ptr(i)))
+
+    def rt_get_state(self):
+        """(Mit, Ac_tot (3, 2), Ac_ind (3, 2)) after the last rt_propagate."""
+        mit = C.c_int(0)
+        t = np.zeros((3, 2), order="F")
+        i = np.zeros((3, 2), order="F")
+        check(lib().sb200_rt_get_state(self.h, C.byref(mit), _ptr(t), _ptr(i)))
+        return mit.value, t, i
+
+    def write_restart(self, directory, psi, iter, method="single", nblock=1, real=False, trans_longi="tr"):
+        """checkpoint_rt / checkpoint_gs in the reference's file layouts."""
+        tl = {"tr": _lib.TRANS_TR, "lo": _lib.TRANS_LO}[trans_longi]
+        check(lib().sb200_write_restart(self.h, str(directory).encode(), {"single": 0, "slice": 1}[method],
+                                        int(nblock), C.c_void_p(psi.data_ptr()), 1 if real else 0, int(iter), tl))
+
+    def read_restart(self, directory, psi, method="single", nblock=1, yn_restart=True, ik_s=1, io_s=1):
+        """restart_rt / restart_gs into the complex block psi; returns (iter,
+        rocc (no, nk, nspin))."""
+        it = C.c_int(0)
+        rocc = np.zeros((self.sys.no, self.sys.nk, self.sys.nspin), order="F")
+        check(lib().sb200_read_restart(self.h, str(directory).encode(), {"single": 0, "slice": 1}[method],
+                                       int(nblock), 1 if yn_restart else 0, int(ik_s), int(io_s),
+                                       C.c_void_p(psi.data_ptr()), C.byref(it), _ptr(rocc)))
+        return it.value, rocc
+
     # -- ground state: real orbitals, one k-point ---------------------------------
     def gs_empty(self):
         return self.torch.empty(self.shape, dtype=self.torch.float64, device=f"cuda:{self.device}")

@@ -462,10 +462,12 @@ int sb200_batch_propagate(sb200_batch* batch, double* const* psi_a, double* cons
  * arrays (is:ie), x fastest, host or device pointers; all three calls are
  * synchronous.                                                                 */
 
-/* Vxc(is:ie) and E_xc = hvol * sum rho*eps_xc of the Perdew-Zunger LDA for
- * nspin = 1 (other nspin: SB200_ERR_UNSUPPORTED).  E_xc may be NULL.
+/* Vxc and E_xc = hvol * sum rho*eps_xc of the Perdew-Zunger LDA: for nspin = 1
+ * rho(is:ie) -> Vxc(is:ie); for nspin = 2 the spin densities rho_s(is:ie, 2) ->
+ * Vxc_s(is:ie, 2) of the spin-polarised form.  E_xc may be NULL.
  * Replaces: exchange_correlation with xc = 'PZ' (src/xc/salmon_xc.f90:58-343,
- * calc_xc :667-812) -> exc_cor_pz / PZxc (src/xc/builtin_pz.f90:23-83).        */
+ * calc_xc :667-812) -> exc_cor_pz / PZxc (src/xc/builtin_pz.f90:23-83) and
+ * exc_cor_pz_sp / PZxc_sp (src/xc/builtin_pz_sp.f90:23-95).                   */
 int sb200_exc_cor_pz(sb200_ctx* ctx, const double* rho, double* Vxc, double* E_xc);
 
 /* Vh(is:ie) of rho on a periodic grid by separable discrete Fourier transforms
@@ -535,7 +537,8 @@ int sb200_update_vlocal(sb200_ctx* ctx, const double* Vpsl, const double* Vh, co
  * the V_local already set (sb200_set_vlocal, or sb200_update_vlocal from
  * rho(t=0)).  The Hartree solve (poisson_ft on periodic grids,
  * poisson_isolated_ft on isolated ones) uses the cell of the latest call that
- * passed primitive_b.  nspin = 1 (else SB200_ERR_UNSUPPORTED);
+ * passed primitive_b.  nspin = 2: the Hartree potential of rho_up + rho_dn,
+ * the spin-polarised PZ and V_local per spin (exc_cor_pz_sp);
  * enable = 0 returns to the fixed-potential loop (Vpsl, primitive_b unused).
  * The density is that of the context's own orbitals, summed over the k-point
  * shards of other processes when sb200_set_density_comm gave the context a

@@ -64,7 +64,7 @@ def lib():
                      "sbo_precond_real", "sbo_gscg_rwf", "sbo_gram_schmidt_real", "sbo_gram_schmidt_complex",
                      "sbo_subspace_diag_real", "sbo_inner_product_real", "sbo_exc_cor_pz", "sbo_poisson_coef",
                      "sbo_dft_table", "sbo_poisson_ft", "sbo_update_vlocal", "sbo_rt_run_scf",
-                     "sbo_poisson_isolated_ft", "sbo_impulse_kick", "sbo_poisson_isolated_cg", "sbo_ylm", "sbo_rt_run_scf_cg"):
+                     "sbo_poisson_isolated_ft", "sbo_impulse_kick", "sbo_exc_cor_pz_sp", "sbo_poisson_isolated_cg", "sbo_ylm", "sbo_rt_run_scf_cg"):
             getattr(L, name)
         L.sbo_rt_run.restype = C.c_int
         L.sbo_rt_run_scf.restype = C.c_int
@@ -302,8 +302,8 @@ class Oracle:
 
     def rt_run_scf(self, psi0, nt, dt, zc, vpsl, brl, v0, Ac_ext=None, trans_longi=0, cg=None):
         """rt_run with the self-consistent potential update every step
-        (time_evolution_step.f90:184-207; nspin = 1, periodic or isolated).  v0: V_local
-        (nx, ny, nz) for the first step.  The oracle's own V_local is untouched.
+        (time_evolution_step.f90:184-207; nspin = 1 or 2, periodic or isolated).  v0:
+        V_local (nx, ny, nz) or (nx, ny, nz, 2) for the first step.  The oracle's own V_local is untouched.
         cg (isolated grids): dict(vh0=..., layout=3, lmax=4, rion=None,
         npole_xyz=None, threshold=1e-15, maxiter=1000) selects the CG Hartree
         solve with the Vh extrapolation; the result then has "Vh" and "cg_iters"."""
@@ -342,10 +342,11 @@ class Oracle:
                 C.c_int(rflat.shape[0]), npx.ctypes.data_as(_ip), C.c_double(cg.get("threshold", 1e-15)),
                 C.c_int(cg.get("maxiter", 1000)), iters.ctypes.data_as(_ip))
             extra = dict(Vh=vh.reshape(g.shape, order="F"), cg_iters=iters)
-        assert which in (0, 1), "rt_run_scf needs an nspin = 1 system (cg: an isolated one)"
+        assert which in (0, 1), "rt_run_scf with cg needs an isolated system"
         psi = a if which == 0 else b
+        vshape = self.sys.grid.shape + ((self.sys.nspin,) if self.sys.nspin == 2 else ())
         return dict(psi=psi, curr=curr, rbox=rbox, Ac_tot=Ac_tot, rho=rho,
-                    V_local=vl.reshape(self.sys.grid.shape, order="F"), **extra)
+                    V_local=vl.reshape(vshape, order="F"), **extra)
 
     # -- ground state (real orbitals, one k) --------------------------------
     def _real(self, psi):
@@ -416,6 +417,16 @@ def exc_cor_pz(rho, hvol):
     e = C.c_double(0.0)
     lib().sbo_exc_cor_pz(C.c_long(r.size), _p(r), C.c_double(hvol), _p(v), C.byref(e))
     return v.reshape(np.shape(rho), order="F"), e.value
+
+
+def exc_cor_pz_sp(rho_s, hvol):
+    """PZ-LDA for nspin = 2 (builtin_pz_sp.f90).  rho_s: (nx, ny, nz, 2) interior,
+    Fortran order.  Returns (Vxc_s with rho_s's shape, E_xc)."""
+    r = _flat_f(rho_s)
+    v = np.zeros_like(r)
+    e = C.c_double(0.0)
+    lib().sbo_exc_cor_pz_sp(C.c_long(r.size // 2), _p(r), C.c_double(hvol), _p(v), C.byref(e))
+    return v.reshape(np.shape(rho_s), order="F"), e.value
 
 
 def primitive_b_orthogonal(lengths):

@@ -903,7 +903,7 @@ void sbo_calc_Ac_ext_t(int shape, double t0, double delta_t, int is, int ie, con
 // (yn_fix_func='y' path: V_local fixed), middlepoint propagator.
 // The self-consistent variant (sbo_rt_run_scf): after the density, the
 // Hartree and exchange-correlation potentials of rho(t+dt) and update_vlocal,
-// time_evolution_step.f90:184-207 with yn_fix_func = 'n' (nspin = 1; Hartree by
+// time_evolution_step.f90:184-207 with yn_fix_func = 'n' (nspin = 1 or 2; Hartree by
 // poisson_ft on periodic grids, poisson_isolated_ft on isolated ones).
 // method_poisson = 'cg' on isolated grids (time_evolution_step.f90:186-198):
 // vh carries the potential from step to step (the CG start), with the two
@@ -930,7 +930,8 @@ static int rt_run_impl(sbo_system* s, double* psi_a, double* psi_b, double* work
                        int trans_longi, double* curr, double* rbox, double* rho_work, const ScfUpdate* scf) {
   const double pi = 3.141592653589793238462643383279502884;
   const long npts = (long)(s->ie[0] - s->is[0] + 1) * (s->ie[1] - s->is[1] + 1) * (s->ie[2] - s->is[2] + 1);
-  std::vector<double> vh(scf ? npts : 0), vxc(scf ? npts : 0), stock1, stock2;
+  std::vector<double> vh(scf ? npts : 0), vxc(scf ? npts * s->nspin : 0), stock1, stock2;
+  std::vector<double> rho_tot(scf && s->nspin == 2 ? npts : 0);
   const ScfCg* cg = (scf && !s->periodic) ? scf->cg : nullptr;
   if (cg) {  // initialization_rt.f90:277-286
     vh.assign(cg->vh, cg->vh + npts);
@@ -951,8 +952,14 @@ static int rt_run_impl(sbo_system* s, double* psi_a, double* psi_b, double* work
     if (scf) {
       const int num[3] = {s->ie[0] - s->is[0] + 1, s->ie[1] - s->is[1] + 1, s->ie[2] - s->is[2] + 1};
       double exc = 0.0;
+      // rho = sum over spins of rho_s (time_evolution_step.f90:160-170)
+      const double* rho_h = rho_work;
+      if (s->nspin == 2) {
+        for (long i = 0; i < npts; ++i) rho_tot[i] = (0.0 + rho_work[i]) + rho_work[npts + i];
+        rho_h = rho_tot.data();
+      }
       if (s->periodic) {
-        sbo_poisson_ft(num, scf->brl, rho_work, vh.data());
+        sbo_poisson_ft(num, scf->brl, rho_h, vh.data());
       } else if (cg) {
         if (itt != 1)
           for (long i = 0; i < npts; ++i) {
@@ -960,15 +967,18 @@ static int rt_run_impl(sbo_system* s, double* psi_a, double* psi_b, double* work
             stock2[i] = stock1[i];
           }
         int it = 0;
-        sbo_poisson_isolated_cg(s, rho_work, vh.data(), cg->layout, cg->lmax, cg->rion, cg->natom, cg->npole,
+        sbo_poisson_isolated_cg(s, rho_h, vh.data(), cg->layout, cg->lmax, cg->rion, cg->natom, cg->npole,
                                 cg->threshold, cg->maxiter, &it);
         if (cg->iters) cg->iters[itt - 1] = it;
         if (itt != 1) stock1 = vh;
       } else {
-        sbo_poisson_isolated_ft(num, scf->brl, rho_work, vh.data());
+        sbo_poisson_isolated_ft(num, scf->brl, rho_h, vh.data());
       }
-      sbo_exc_cor_pz(npts, rho_work, s->hvol, vxc.data(), &exc);
-      sbo_update_vlocal(npts, 1, scf->vpsl, vh.data(), vxc.data(), scf->vloc);
+      if (s->nspin == 2)
+        sbo_exc_cor_pz_sp(npts, rho_work, s->hvol, vxc.data(), &exc);
+      else
+        sbo_exc_cor_pz(npts, rho_work, s->hvol, vxc.data(), &exc);
+      sbo_update_vlocal(npts, s->nspin, scf->vpsl, vh.data(), vxc.data(), scf->vloc);
     }
     if (s->periodic) {
       for (int d = 0; d < 3; ++d) s->vec_Ac[d] = Ac_tot[3 * itt + d];
@@ -1009,7 +1019,6 @@ int sbo_rt_run_scf(sbo_system* s, double* psi_a, double* psi_b, double* work, in
                    const double* zc, int n_hamil, const double* Ac_ext, double* Ac_ind,
                    double* Ac_tot, int trans_longi, double* curr, double* rbox, double* rho_work,
                    const double* vpsl, const double brl[9], double* vloc) {
-  if (s->nspin != 1) return -1;
   const ScfUpdate u{vpsl, brl, vloc};
   const double* saved = s->V_local;
   s->V_local = vloc;
@@ -1024,7 +1033,7 @@ int sbo_rt_run_scf_cg(sbo_system* s, double* psi_a, double* psi_b, double* work,
                       int trans_longi, double* curr, double* rbox, double* rho_work, const double* vpsl,
                       double* vloc, double* vh, int layout, int lmax, const double* rion, int natom,
                       const int npole_xyz[3], double threshold, int maxiter, int* iters) {
-  if (s->nspin != 1 || s->periodic) return -1;
+  if (s->periodic) return -1;
   ScfCg cg{layout, lmax, rion, natom, {npole_xyz[0], npole_xyz[1], npole_xyz[2]}, threshold, maxiter, vh, iters};
   ScfUpdate u{vpsl, nullptr, vloc, &cg};
   const double* saved = s->V_local;

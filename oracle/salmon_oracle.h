@@ -174,6 +174,9 @@ void sbo_inner_product_real(const sbo_system* s, const double* x, const double* 
  * src/poisson/poisson_periodic.f90:23-242) and update_vlocal
  * (src/common/hamiltonian.f90:813-843).  Interior arrays, x fastest.           */
 void sbo_exc_cor_pz(long n, const double* rho, double hvol, double* vxc, double* E_xc);
+/* exchange_correlation, nspin = 2, xc = 'PZ' (exc_cor_pz_sp / PZxc_sp,
+ * builtin_pz_sp.f90:23-95): rho_s(n, 2) -> vxc_s(n, 2), E_xc               */
+void sbo_exc_cor_pz_sp(long n, const double* rho_s, double hvol, double* vxc_s, double* E_xc);
 void sbo_poisson_coef(const int num[3], const double brl[9], double* coef);
 void sbo_dft_table(int n, double* eg);
 void sbo_poisson_ft(const int num[3], const double brl[9], const double* rho, double* vh);

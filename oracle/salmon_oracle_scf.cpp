@@ -43,6 +43,45 @@ void pzxc(double trho, double* exc, double* dexc_drho) {
   *dexc_drho = de;
 }
 
+// PZxc_sp, src/xc/builtin_pz_sp.f90:43-95: Slater exchange with the spin
+// interpolation f(zeta) = ((1+zeta)^(4/3) + (1-zeta)^(4/3) - 2) / (2^(4/3) - 2)
+// between the unpolarised (U) and polarised (P) Perdew-Zunger 1981 correlation
+// fits; vxc_s(js) for js = up (sign +1), down (-1).
+void pzxc_sp(double trho, const double trho_s[2], double* exc_out, double vxc_s[2]) {
+  const double gammaU = -0.1423, gammaP = -0.0843, beta1U = 1.0529, beta2U = 0.3334, beta1P = 1.3981,
+               beta2P = 0.2611, AU = 0.0311, BU = -0.048, CU = 0.002, DU = -0.0116, AP = 0.01555, BP = -0.0269,
+               CP = 0.0007, DP = -0.0048;
+  const double sgn[2] = {1.0, -1.0};
+  const double rs = std::pow(3.0 / (4.0 * PI * trho), 1.0 / 3.0);
+  const double zeta = (trho_s[0] - trho_s[1]) / trho;
+  const double fden = std::pow(2.0, 4.0 / 3.0) - 2.0;
+  const double sf = (std::pow(1.0 + zeta, 4.0 / 3.0) + std::pow(1.0 - zeta, 4.0 / 3.0) - 2.0) / fden;
+  const double dsf = 4.0 / 3.0 * (std::pow(1.0 + zeta, 1.0 / 3.0) - std::pow(1.0 - zeta, 1.0 / 3.0)) / fden;
+  const double cx = 3.0 / 4.0 * std::pow(3.0 / (2 * PI), 2.0 / 3.0);
+  const double a = -std::pow(2.0, 1.0 / 3.0) + 1.0;
+  double exc = -cx / rs + a * cx / rs * sf;
+  for (int js = 0; js < 2; ++js)
+    vxc_s[js] = exc - 1.0 / 3.0 * cx / rs + 1.0 / 3.0 * a * cx / rs * sf + a * cx / rs * (sgn[js] - zeta) * dsf;
+  double ecu, ecp, vcu, vcp;
+  if (rs > 1.0) {
+    const double q = std::sqrt(rs);
+    const double du = 1.0 + beta1U * q + beta2U * rs, dp = 1.0 + beta1P * q + beta2P * rs;
+    ecu = gammaU / du;
+    ecp = gammaP / dp;
+    vcu = gammaU * (1.0 + 7.0 / 6.0 * beta1U * q + 4.0 / 3.0 * beta2U * rs) / (du * du);
+    vcp = gammaP * (1.0 + 7.0 / 6.0 * beta1P * q + 4.0 / 3.0 * beta2P * rs) / (dp * dp);
+  } else {
+    const double l = std::log(rs);
+    ecu = AU * l + BU + CU * rs * l + DU * rs;
+    ecp = AP * l + BP + CP * rs * l + DP * rs;
+    vcu = AU * l + (BU - AU / 3.0) + 2.0 / 3.0 * CU * rs * l + (2.0 * DU - CU) / 3.0 * rs;
+    vcp = AP * l + (BP - AP / 3.0) + 2.0 / 3.0 * CP * rs * l + (2.0 * DP - CP) / 3.0 * rs;
+  }
+  exc = exc + ecu + sf * (ecp - ecu);
+  for (int js = 0; js < 2; ++js) vxc_s[js] = vxc_s[js] + vcu + sf * (vcp - vcu) + (ecp - ecu) * (sgn[js] - zeta) * dsf;
+  *exc_out = exc;
+}
+
 // Index folding of fg%coef, initialization.f90:700-702: m = ix-1 in 0..n-1
 // maps to m - n when m >= (n+1)/2 (Fortran sign(1, m - (n+1)/2) = +1 there).
 int fold(int m, int n) { return (m - (n + 1) / 2 >= 0) ? m - n : m; }
@@ -65,6 +104,27 @@ void sbo_exc_cor_pz(long n, const double* rho, double hvol, double* vxc, double*
     pzxc(trho, &e, &de);
     eexc[i] = e * trho;
     vxc[i] = e + trho * de;
+  }
+  double tot = 0.0;
+  for (long i = 0; i < n; ++i) tot = tot + eexc[i];
+  *E_xc = tot * hvol;
+}
+
+// exchange_correlation for nspin = 2 with xc = 'PZ' (exc_cor_pz_sp,
+// builtin_pz_sp.f90:23-40): rho_s(n, 2), trho = rho_up + rho_dn + 1e-20,
+// trho_s = rho_s + 5e-21, vxc_s(n, 2), E_xc = hvol * sum(e_xc trho) summed
+// with x fastest.
+void sbo_exc_cor_pz_sp(long n, const double* rho_s, double hvol, double* vxc_s, double* E_xc) {
+  std::vector<double> eexc(n);
+#pragma omp parallel for
+  for (long i = 0; i < n; ++i) {
+    const double trho = rho_s[i] + rho_s[n + i] + 1e-20;
+    const double ts[2] = {rho_s[i] + 5e-21, rho_s[n + i] + 5e-21};
+    double e, v[2];
+    pzxc_sp(trho, ts, &e, v);
+    eexc[i] = e * trho;
+    vxc_s[i] = v[0];
+    vxc_s[n + i] = v[1];
   }
   double tot = 0.0;
   for (long i = 0; i < n; ++i) tot = tot + eexc[i];

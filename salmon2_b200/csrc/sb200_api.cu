@@ -107,6 +107,7 @@ int check_device_flag(sb200_ctx* c) {
   SB_CUDA(cudaMemcpy(&flag, c->d_err, sizeof(int), cudaMemcpyDeviceToHost));
   if (flag != 0) {
     SB_CUDA(cudaMemset(c->d_err, 0, sizeof(int)));
+    SB_CUDA(cudaDeviceSynchronize());
     return set_error(SB200_ERR_TIMEOUT, "a bounded device wait expired (a bulk copy did not complete)");
   }
   return SB200_OK;
@@ -147,6 +148,9 @@ template <typename T>
 int upload(T** d, const std::vector<T>& h) {
   TRY(dalloc(d, h.size()));
   if (!h.empty()) SB_CUDA(cudaMemcpy(*d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+  // a copy from pageable memory may still be landing when cudaMemcpy returns;
+  // the context's stream does not wait for the legacy stream
+  SB_CUDA(cudaDeviceSynchronize());
   return SB200_OK;
 }
 
@@ -341,6 +345,7 @@ int sb200_ctx_create(int device, sb200_ctx** out) {
     return r;
   }
   cudaMemset(c->d_result, 0, 16 * sizeof(double));
+  cudaDeviceSynchronize();  // the legacy-stream fills land before the context's non-blocking stream runs
   *out = c;
   return SB200_OK;
 }
@@ -546,6 +551,7 @@ int sb200_set_vlocal(sb200_ctx* c, const double* V_local) {
   SB_CUDA(cudaMemcpy(tmp.data(), c->d_vloc, n * sizeof(double), cudaMemcpyDeviceToHost));
   for (size_t i = 0; i < n; ++i) v32[i] = (float)tmp[i];
   SB_CUDA(cudaMemcpy(c->d_vloc32, v32.data(), n * sizeof(float), cudaMemcpyHostToDevice));
+  SB_CUDA(cudaDeviceSynchronize());  // landed before the context's (non-blocking) stream reads it
   c->vloc_set = true;
   return SB200_OK;
 }
@@ -722,6 +728,7 @@ int sb200_set_pp(sb200_ctx* c, int natom, int nps, int nlma, const int* mps, con
     if (!g.periodic) {  // isolated: exp(i 0.r) = 1
       std::vector<double2> one(p.npair > 0 ? p.npair : 1, make_double2(1.0, 0.0));
       SB_CUDA(cudaMemcpy(p.d_pair_ph, one.data(), one.size() * sizeof(double2), cudaMemcpyHostToDevice));
+      SB_CUDA(cudaDeviceSynchronize());
     }
   }
   TRY(dalloc(&p.d_ent_zk, (size_t)p.nk_phase * (nent > 0 ? nent : 1)));
@@ -731,6 +738,7 @@ int sb200_set_pp(sb200_ctx* c, int natom, int nps, int nlma, const int* mps, con
     std::vector<double2> zk(nent > 0 ? nent : 1, make_double2(0.0, 0.0));
     for (int e = 0; e < nent; ++e) zk[e] = make_double2(ent_uv[e], 0.0);
     SB_CUDA(cudaMemcpy(p.d_ent_zk, zk.data(), zk.size() * sizeof(double2), cudaMemcpyHostToDevice));
+    SB_CUDA(cudaDeviceSynchronize());
   }
   TRY(ensure_work(c));
   TRY(refresh_k(c));

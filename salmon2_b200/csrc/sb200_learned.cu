@@ -388,6 +388,7 @@ int net_ensure(sb200_ctx* c, int batch) {
     SB_CUDA(cudaMemset(n->d_w, 0, NPARAM * sizeof(float)));
     SB_CUDA(cudaMemset(n->d_m, 0, NPARAM * sizeof(float)));
     SB_CUDA(cudaMemset(n->d_v, 0, NPARAM * sizeof(float)));
+    SB_CUDA(cudaDeviceSynchronize());
   }
   if (n->npts != c->g.npts || n->cap_batch < batch) {
     dfree(n->x0);
@@ -567,6 +568,7 @@ int sb200_learned_init(sb200_ctx* c, const float* params, int nparam, int batch)
   else SB_CUDA(cudaMemset(n->d_w, 0, NPARAM * sizeof(float)));
   SB_CUDA(cudaMemset(n->d_m, 0, NPARAM * sizeof(float)));
   SB_CUDA(cudaMemset(n->d_v, 0, NPARAM * sizeof(float)));
+  SB_CUDA(cudaDeviceSynchronize());  // before kernels on the context's non-blocking stream
   n->adam_t = 0;
   k_to_bf16<<<gsz(NPARAM), 256, 0, c->stream>>>(n->d_w, n->d_wb, NPARAM);
   SB_LAUNCH_CHECK("k_to_bf16");

@@ -886,6 +886,7 @@ int blk_build_tables(sb200_ctx* c, const std::vector<int>& pt_lin, const std::ve
   SB_CUDA(cudaMemcpy(p.d_blk_uv, uv4.data(), uv4.size() * sizeof(double), cudaMemcpyHostToDevice));
   SB_CUDA(cudaMemcpy(p.d_blk_r, r3.data(), r3.size() * sizeof(double), cudaMemcpyHostToDevice));
   SB_CUDA(cudaMemcpy(p.d_blk_sap, sap.data(), sap.size() * sizeof(int), cudaMemcpyHostToDevice));
+  SB_CUDA(cudaDeviceSynchronize());  // landed before the context's (non-blocking) stream reads them
   p.blk_tpad = TP;
   return SB200_OK;
 }

@@ -177,7 +177,8 @@ int sb200_write_restart(sb200_ctx* c, const char* dir, int method_wf_distributor
   const char* src = reinterpret_cast<const char*>(psi);
   auto block = [&](int ik, int io, int is) -> int {  // orbital block (1-based ik, io, is) to host
     const size_t orb = (size_t)(is - 1) + (size_t)o.nspin * ((size_t)(io - 1) + (size_t)o.no * (ik - 1));
-    SB_CUDA(cudaMemcpy(host.data(), src + orb * npts * esz, npts * esz, cudaMemcpyDefault));
+    SB_CUDA(cudaMemcpyAsync(host.data(), src + orb * npts * esz, npts * esz, cudaMemcpyDefault, c->stream));
+    SB_CUDA(cudaStreamSynchronize(c->stream));
     return SB200_OK;
   };
   if (method_wf_distributor == 0) {  // 'single': wfn.bin
@@ -208,8 +209,9 @@ int sb200_write_restart(sb200_ctx* c, const char* dir, int method_wf_distributor
   double *vh, *s1, *s2;
   if (scf_vh_stock(c, &vh, &s1, &s2)) {  // Vh_stock.bin (write_Vh_stock, non-self form)
     std::vector<double> a(npts), b(npts);
-    SB_CUDA(cudaMemcpy(a.data(), s1, npts * sizeof(double), cudaMemcpyDeviceToHost));
-    SB_CUDA(cudaMemcpy(b.data(), s2, npts * sizeof(double), cudaMemcpyDeviceToHost));
+    SB_CUDA(cudaMemcpyAsync(a.data(), s1, npts * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    SB_CUDA(cudaMemcpyAsync(b.data(), s2, npts * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    SB_CUDA(cudaStreamSynchronize(c->stream));
     File f(join(d, "Vh_stock.bin"), "wb");
     if (!f.f || !put_record(f.f, a.data(), npts * sizeof(double)) ||
         !put_record(f.f, b.data(), npts * sizeof(double)))
@@ -271,11 +273,14 @@ int sb200_read_restart(sb200_ctx* c, const char* dir, int method_wf_distributor,
   auto store = [&](int ik, int io, int is) -> int {  // host block of global (ik, io, is) to psi
     const size_t orb = (size_t)(is - 1) + (size_t)o.nspin * ((size_t)(io - io_s) + (size_t)o.no * (ik - ik_s));
     double2* dst = reinterpret_cast<double2*>(psi) + orb * npts;
+    // copies and the widening kernel in order on the context's stream, finished
+    // before the host buffer is refilled
     if (!is_real) {
-      SB_CUDA(cudaMemcpy(dst, host.data(), npts * esz, cudaMemcpyHostToDevice));
+      SB_CUDA(cudaMemcpyAsync(dst, host.data(), npts * esz, cudaMemcpyHostToDevice, c->stream));
+      SB_CUDA(cudaStreamSynchronize(c->stream));
       return SB200_OK;
     }
-    SB_CUDA(cudaMemcpy(d_real, host.data(), npts * esz, cudaMemcpyHostToDevice));
+    SB_CUDA(cudaMemcpyAsync(d_real, host.data(), npts * esz, cudaMemcpyHostToDevice, c->stream));
     long nb = ((long)npts + 255) / 256;
     if (nb > 148L * 8) nb = 148L * 8;
     k_widen_real<<<(unsigned)nb, 256, 0, c->stream>>>(d_real, dst, (long)npts);
@@ -343,8 +348,9 @@ int sb200_read_restart(sb200_ctx* c, const char* dir, int method_wf_distributor,
       std::vector<double> a(npts), b(npts);
       if (!get_doubles(f.f, a.data(), npts) || !get_doubles(f.f, b.data(), npts))
         return set_error(SB200_ERR_INVALID_ARG, "cannot read " + join(d, "Vh_stock.bin"));
-      SB_CUDA(cudaMemcpy(s1, a.data(), npts * sizeof(double), cudaMemcpyHostToDevice));
-      SB_CUDA(cudaMemcpy(s2, b.data(), npts * sizeof(double), cudaMemcpyHostToDevice));
+      SB_CUDA(cudaMemcpyAsync(s1, a.data(), npts * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+      SB_CUDA(cudaMemcpyAsync(s2, b.data(), npts * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+      SB_CUDA(cudaStreamSynchronize(c->stream));
       RS_TRY(scf_restart_potential(c, reinterpret_cast<const double2*>(psi)));
     }
   }

@@ -100,6 +100,8 @@ struct ScfState {
   // of the extrapolation
   bool cg_on = false;
   int* d_step0 = nullptr;     // a zero step counter (the restart's stock update)
+  double* d_rho_tot = nullptr;  // [npts] rho_up + rho_dn (nspin = 2)
+  size_t spin_cap = 0;          // spins d_rho / d_vxc hold
   double* d_stock1 = nullptr;
   double* d_stock2 = nullptr;
 };
@@ -241,6 +243,76 @@ __global__ void __launch_bounds__(SCF_THREADS) k_exc_pz(const double* __restrict
     __syncthreads();
   }
   if (threadIdx.x == 0) part[blockIdx.x] = red[0];
+}
+
+// PZxc_sp, src/xc/builtin_pz_sp.f90:43-95: Slater exchange with the spin
+// interpolation f(zeta) between the unpolarised and polarised Perdew-Zunger
+// 1981 correlation fits; v[0] spin up (sign +1), v[1] spin down (-1).
+__device__ __forceinline__ void pzxc_sp_dev(double trho, double tu, double td, double& exc, double (&v)[2]) {
+  const double gammaU = -0.1423, gammaP = -0.0843, beta1U = 1.0529, beta2U = 0.3334, beta1P = 1.3981,
+               beta2P = 0.2611, AU = 0.0311, BU = -0.048, CU = 0.002, DU = -0.0116, AP = 0.01555, BP = -0.0269,
+               CP = 0.0007, DP = -0.0048;
+  const double rs = pow(3.0 / (4.0 * SCF_PI * trho), 1.0 / 3.0);
+  const double zeta = (tu - td) / trho;
+  const double fden = pow(2.0, 4.0 / 3.0) - 2.0;
+  const double sf = (pow(1.0 + zeta, 4.0 / 3.0) + pow(1.0 - zeta, 4.0 / 3.0) - 2.0) / fden;
+  const double dsf = 4.0 / 3.0 * (pow(1.0 + zeta, 1.0 / 3.0) - pow(1.0 - zeta, 1.0 / 3.0)) / fden;
+  const double cx = 3.0 / 4.0 * pow(3.0 / (2 * SCF_PI), 2.0 / 3.0);
+  const double a = -pow(2.0, 1.0 / 3.0) + 1.0;
+  double e = -cx / rs + a * cx / rs * sf;
+  const double sgn[2] = {1.0, -1.0};
+#pragma unroll
+  for (int js = 0; js < 2; ++js)
+    v[js] = e - 1.0 / 3.0 * cx / rs + 1.0 / 3.0 * a * cx / rs * sf + a * cx / rs * (sgn[js] - zeta) * dsf;
+  double ecu, ecp, vcu, vcp;
+  if (rs > 1.0) {
+    const double q = sqrt(rs);
+    const double du = 1.0 + beta1U * q + beta2U * rs, dp = 1.0 + beta1P * q + beta2P * rs;
+    ecu = gammaU / du;
+    ecp = gammaP / dp;
+    vcu = gammaU * (1.0 + 7.0 / 6.0 * beta1U * q + 4.0 / 3.0 * beta2U * rs) / (du * du);
+    vcp = gammaP * (1.0 + 7.0 / 6.0 * beta1P * q + 4.0 / 3.0 * beta2P * rs) / (dp * dp);
+  } else {
+    const double l = log(rs);
+    ecu = AU * l + BU + CU * rs * l + DU * rs;
+    ecp = AP * l + BP + CP * rs * l + DP * rs;
+    vcu = AU * l + (BU - AU / 3.0) + 2.0 / 3.0 * CU * rs * l + (2.0 * DU - CU) / 3.0 * rs;
+    vcp = AP * l + (BP - AP / 3.0) + 2.0 / 3.0 * CP * rs * l + (2.0 * DP - CP) / 3.0 * rs;
+  }
+  e = e + ecu + sf * (ecp - ecu);
+#pragma unroll
+  for (int js = 0; js < 2; ++js) v[js] = v[js] + vcu + sf * (vcp - vcu) + (ecp - ecu) * (sgn[js] - zeta) * dsf;
+  exc = e;
+}
+
+// exc_cor_pz_sp (builtin_pz_sp.f90:23-40): rho_s(n, 2) -> vxc_s(n, 2), per-block
+// partial sums of e_xc * trho (trho = rho_up + rho_dn + 1e-20, each spin
+// density + 5e-21) in a fixed tree order.
+__global__ void __launch_bounds__(SCF_THREADS) k_exc_pz_sp(const double* __restrict__ rho, double* __restrict__ vxc,
+                                                           long n, double* __restrict__ part) {
+  __shared__ double red[SCF_THREADS];
+  double s = 0.0;
+  for (long i = blockIdx.x * (long)SCF_THREADS + threadIdx.x; i < n; i += (long)gridDim.x * SCF_THREADS) {
+    const double trho = rho[i] + rho[n + i] + 1e-20;
+    double e, v[2];
+    pzxc_sp_dev(trho, rho[i] + 5e-21, rho[n + i] + 5e-21, e, v);
+    vxc[i] = v[0];
+    vxc[n + i] = v[1];
+    s += e * trho;
+  }
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int st = SCF_THREADS / 2; st > 0; st >>= 1) {
+    if (threadIdx.x < st) red[threadIdx.x] += red[threadIdx.x + st];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) part[blockIdx.x] = red[0];
+}
+
+// rho = rho_up + rho_dn (time_evolution_step.f90:160-170: rho%f summed over spins)
+__global__ void k_rho_total(const double* __restrict__ rho_s, double* __restrict__ rho, long n) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+    rho[i] = (0.0 + rho_s[i]) + rho_s[n + i];
 }
 
 // E_xc = hvol * sum of the block partials, in block order (one thread).
@@ -566,7 +638,10 @@ int scf_launch_xc(sb200_ctx* c, const double* d_rho, double* d_vxc, int kind, bo
   ScfState* s = scf_of(c);
   const double cst = 0.75 * std::pow(3.0 / (2.0 * SCF_PI), 2.0 / 3.0);
   TRY_S(scf_mark(c, kind, true));
-  k_exc_pz<<<SCF_XC_BLOCKS, SCF_THREADS, 0, c->stream>>>(d_rho, d_vxc, s->npts, cst, s->d_part);
+  if (c->orb.nspin == 2)
+    k_exc_pz_sp<<<SCF_XC_BLOCKS, SCF_THREADS, 0, c->stream>>>(d_rho, d_vxc, s->npts, s->d_part);
+  else
+    k_exc_pz<<<SCF_XC_BLOCKS, SCF_THREADS, 0, c->stream>>>(d_rho, d_vxc, s->npts, cst, s->d_part);
   TRY_S(scf_mark(c, kind, false));
   if (!total) return SB200_OK;
   TRY_S(scf_mark(c, kind, true));
@@ -581,6 +656,17 @@ int scf_launch_update(sb200_ctx* c, const double* vpsl, const double* vh, const 
   k_update_vlocal<<<scf_grid_blocks(n * nspin), SCF_THREADS, 0, c->stream>>>(vpsl, vh, vxc, c->d_vloc, c->d_vloc32,
                                                                             n, nspin);
   return scf_mark(c, kind, false);
+}
+
+// the density the Hartree solve takes: rho itself (nspin = 1) or rho_up + rho_dn
+const double* scf_total_density(sb200_ctx* c, int kind) {
+  ScfState* s = scf_of(c);
+  if (c->orb.nspin != 2) return s->d_rho;
+  const long n = s->npts;
+  scf_mark(c, kind, true);
+  k_rho_total<<<scf_grid_blocks(n), SCF_THREADS, 0, c->stream>>>(s->d_rho, s->d_rho_tot, n);
+  scf_mark(c, kind, false);
+  return s->d_rho_tot;
 }
 
 }  // namespace
@@ -622,16 +708,17 @@ int scf_rt_issue(sb200_ctx* c, const double2* psi) {
   if (!s || !s->rt_on) return SB200_OK;
   TRY_S(launch_density(c, psi, s->d_rho, SB200_KIND_POTENTIAL));
   TRY_S(scf_density_allreduce(c, s->d_rho));
+  const double* rho_h = scf_total_density(c, SB200_KIND_POTENTIAL);
   if (c->g.periodic) {
-    TRY_S(scf_launch_hartree(c, s->d_rho, s->d_vh, SB200_KIND_POTENTIAL));
+    TRY_S(scf_launch_hartree(c, rho_h, s->d_vh, SB200_KIND_POTENTIAL));
   } else if (s->cg_on) {  // time_evolution_step.f90:186-198 with method_poisson = 'cg'
     TRY_S(scf_mark(c, SB200_KIND_POTENTIAL, true));
     TRY_S(pcg_vh_stock(c, c->rt.d_step, c->rt.loop_mit0, s->d_vh, s->d_stock1, s->d_stock2, true));
-    TRY_S(pcg_issue(c, s->d_rho, s->d_vh, nullptr));
+    TRY_S(pcg_issue(c, rho_h, s->d_vh, nullptr));
     TRY_S(pcg_vh_stock(c, c->rt.d_step, c->rt.loop_mit0, s->d_vh, s->d_stock1, s->d_stock2, false));
     TRY_S(scf_mark(c, SB200_KIND_POTENTIAL, false));
   } else {
-    TRY_S(scf_launch_hartree_isolated(c, s->d_rho, s->d_vh, SB200_KIND_POTENTIAL));
+    TRY_S(scf_launch_hartree_isolated(c, rho_h, s->d_vh, SB200_KIND_POTENTIAL));
   }
   TRY_S(scf_launch_xc(c, s->d_rho, s->d_vxc, SB200_KIND_POTENTIAL, false));
   TRY_S(scf_launch_update(c, s->d_vpsl, s->d_vh, s->d_vxc, SB200_KIND_POTENTIAL));
@@ -666,8 +753,9 @@ int scf_restart_potential(sb200_ctx* c, const double2* psi) {
   TRY_S(density_prepare(c));
   TRY_S(launch_density(c, psi, s->d_rho));
   TRY_S(scf_density_allreduce(c, s->d_rho));
+  const double* rho_h = scf_total_density(c, -1);
   TRY_S(pcg_vh_stock(c, s->d_step0, 0, s->d_vh, s->d_stock1, s->d_stock2, true));
-  TRY_S(pcg_issue(c, s->d_rho, s->d_vh, nullptr));
+  TRY_S(pcg_issue(c, rho_h, s->d_vh, nullptr));
   TRY_S(scf_launch_xc(c, s->d_rho, s->d_vxc, -1, false));
   TRY_S(scf_launch_update(c, s->d_vpsl, s->d_vh, s->d_vxc, -1));
   TRY_S(pcg_vh_stock(c, s->d_step0, 0, s->d_vh, s->d_stock1, s->d_stock2, false));
@@ -696,6 +784,7 @@ void scf_free(sb200_ctx* c) {
   dfree(s->d_itab);
   dfree(s->d_stock1);
   dfree(s->d_step0);
+  dfree(s->d_rho_tot);
   dfree(s->d_stock2);
   delete s;
   c->scf = nullptr;
@@ -710,21 +799,20 @@ extern "C" {
 int sb200_exc_cor_pz(sb200_ctx* c, const double* rho, double* Vxc, double* E_xc) {
   TRY_S(scf_ready(c));
   if (!rho || !Vxc) return set_error(SB200_ERR_INVALID_ARG, "null argument");
-  if (c->orb.nspin != 1)
-    return set_error(SB200_ERR_UNSUPPORTED, "sb200_exc_cor_pz: the PZ functional here is the nspin = 1 form");
   ScfDevGuard dg(c->device);
   TRY_S(scf_ensure(c));
   ScfState* s = scf_of(c);
   const long n = s->npts;
-  TRY_S(scf_stage_in(c, (size_t)n));
+  const size_t m = (size_t)n * c->orb.nspin;  // rho_s / Vxc_s of every spin
+  TRY_S(scf_stage_in(c, m));
   const double* d_rho = nullptr;
-  TRY_S(scf_input(c, rho, (size_t)n, s->d_in, &d_rho));
+  TRY_S(scf_input(c, rho, m, s->d_in, &d_rho));
   const bool out_dev = scf_is_device(Vxc);
-  if (!out_dev) TRY_S(scf_stage_out(c, (size_t)n));
+  if (!out_dev) TRY_S(scf_stage_out(c, m));
   double* d_v = out_dev ? Vxc : s->d_out;
   TRY_S(scf_launch_xc(c, d_rho, d_v, -1));
   SB_LAUNCH_CHECK("k_exc_pz");
-  if (!out_dev) SB_CUDA(cudaMemcpyAsync(Vxc, d_v, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  if (!out_dev) SB_CUDA(cudaMemcpyAsync(Vxc, d_v, m * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   double e = 0.0;
   SB_CUDA(cudaMemcpyAsync(&e, s->d_part + SCF_XC_BLOCKS, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   SB_CUDA(cudaStreamSynchronize(c->stream));
@@ -844,8 +932,6 @@ int sb200_set_self_consistent(sb200_ctx* c, int enable, const double* Vpsl, cons
     return SB200_OK;
   }
   if (!Vpsl || !primitive_b) return set_error(SB200_ERR_INVALID_ARG, "null argument");
-  if (c->orb.nspin != 1)
-    return set_error(SB200_ERR_UNSUPPORTED, "the self-consistent time loop is the nspin = 1 form");
   if (!c->vloc_set) return set_error(SB200_ERR_STATE, "set V_local (sb200_set_vlocal / sb200_update_vlocal) first");
   TRY_S(scf_ensure(c));
   if (c->g.periodic)
@@ -854,10 +940,18 @@ int sb200_set_self_consistent(sb200_ctx* c, int enable, const double* Vpsl, cons
     TRY_S(scf_itables(c, primitive_b));
   ScfState* s = scf_of(c);
   const size_t n = (size_t)s->npts;
+  const size_t ns = (size_t)c->orb.nspin;
+  if (s->spin_cap < ns) {  // the per-spin arrays (rho_s, Vxc_s)
+    dfree(s->d_rho);
+    dfree(s->d_vxc);
+    s->spin_cap = 0;
+  }
   if (!s->d_vpsl) TRY_S(dalloc(&s->d_vpsl, n));
-  if (!s->d_rho) TRY_S(dalloc(&s->d_rho, n));
+  if (!s->d_rho) TRY_S(dalloc(&s->d_rho, n * ns));
   if (!s->d_vh) TRY_S(dalloc(&s->d_vh, n));
-  if (!s->d_vxc) TRY_S(dalloc(&s->d_vxc, n));
+  if (!s->d_vxc) TRY_S(dalloc(&s->d_vxc, n * ns));
+  s->spin_cap = ns;
+  if (ns == 2 && !s->d_rho_tot) TRY_S(dalloc(&s->d_rho_tot, n));
   SB_CUDA(cudaMemcpyAsync(s->d_vpsl, Vpsl, n * sizeof(double), cudaMemcpyDefault, c->stream));
   SB_CUDA(cudaStreamSynchronize(c->stream));
   TRY_S(density_prepare(c));

@@ -244,11 +244,12 @@ class Context:
         return C.c_void_p(a.data_ptr()), a
 
     def exc_cor_pz(self, rho):
-        """exchange_correlation with xc = 'PZ' for nspin = 1 (salmon_xc.f90:58-343):
-        returns (Vxc as an (nx, ny, nz) Fortran-order array, E_xc)."""
+        """exchange_correlation with xc = 'PZ' (salmon_xc.f90:58-343): nspin = 1,
+        rho (nx, ny, nz) -> (Vxc (nx, ny, nz), E_xc); nspin = 2, the spin
+        densities (nx, ny, nz, 2) -> (Vxc_s (nx, ny, nz, 2), E_xc), Fortran order."""
         g = self.sys.grid
         p, keep = self._scalar_field(rho)
-        v = np.zeros(g.shape, order="F")
+        v = np.zeros(g.shape + ((2,) if self.sys.nspin == 2 else ()), order="F")
         e = C.c_double(0.0)
         check(lib().sb200_exc_cor_pz(self.h, p, C.c_void_p(v.ctypes.data), C.byref(e)))
         return v, e.value
@@ -334,22 +335,28 @@ class Context:
 
     def update_potential(self, psi, vpsl, primitive_b, poisson="ft"):
         """The self-consistent part of one time step on the device
-        (time_evolution_step.f90:160-207, nspin = 1; Hartree by poisson_ft on a
+        (time_evolution_step.f90:160-207, nspin = 1 or 2; Hartree by poisson_ft on a
         periodic grid, poisson_isolated_ft on an isolated one, or with
         poisson = "cg" poisson_isolated_cg from zero with the default multipole
         boundary): rho = calc_density(psi), Vh = hartree(rho),
         Vxc = exchange_correlation(rho), V_local = Vpsl + Vh + Vxc.  vpsl: a
         device tensor (nx*ny*nz, x fastest) or a numpy array.  Nothing is copied
-        to the host; returns E_xc.  The potential stays in self.last_vh."""
+        to the host; returns E_xc.  The potential stays in self.last_vh.  With
+        nspin = 2 the Hartree potential is that of rho_up + rho_dn and Vxc the
+        spin-polarised form."""
         torch = self.torch
-        if self.sys.nspin != 1:
-            raise SB200Error(3, "update_potential: the PZ potential here is the nspin = 1 form")
+        ns = self.sys.nspin
         n = int(np.prod(self.sys.grid.shape))
         if getattr(self, "_pot_buf", None) is None:
-            self._pot_buf = torch.empty((3, n), dtype=torch.float64, device=f"cuda:{self.device}")
-        rho, vh, vxc = self._pot_buf
+            self._pot_buf = torch.empty((2 * ns + 2, n), dtype=torch.float64, device=f"cuda:{self.device}")
+        buf = self._pot_buf
+        rho_s, vh, vxc = buf[0:ns], buf[ns], buf[ns + 1:2 * ns + 1]
         b = np.asfortranarray(primitive_b, dtype=np.float64)
-        check(lib().sb200_calc_density(self.h, C.c_void_p(psi.data_ptr()), C.c_void_p(rho.data_ptr())))
+        check(lib().sb200_calc_density(self.h, C.c_void_p(psi.data_ptr()), C.c_void_p(rho_s.data_ptr())))
+        rho = rho_s[0]
+        if ns == 2:  # rho = sum of rho_s (time_evolution_step.f90:160-170)
+            rho = buf[2 * ns + 1]
+            torch.add(rho_s[0], rho_s[1], out=rho)
         if poisson == "cg" and not self.sys.grid.periodic:
             vh.zero_()
             ri = np.ascontiguousarray(np.asarray(self.sys.rion, dtype=np.float64).reshape(3, -1, order="F").T)
@@ -361,7 +368,7 @@ class Context:
             check(hartree(self.h, _ptr(b), C.c_void_p(rho.data_ptr()), C.c_void_p(vh.data_ptr())))
         self.last_vh = vh
         e = C.c_double(0.0)
-        check(lib().sb200_exc_cor_pz(self.h, C.c_void_p(rho.data_ptr()), C.c_void_p(vxc.data_ptr()), C.byref(e)))
+        check(lib().sb200_exc_cor_pz(self.h, C.c_void_p(rho_s.data_ptr()), C.c_void_p(vxc.data_ptr()), C.byref(e)))
         pa, keep = self._scalar_field(vpsl)
         check(lib().sb200_update_vlocal(self.h, pa, C.c_void_p(vh.data_ptr()), C.c_void_p(vxc.data_ptr())))
         return e.value

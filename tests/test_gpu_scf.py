@@ -500,3 +500,81 @@ def test_rt_propagate_self_consistent_isolated_cg(nt):
     assert np.max(np.abs(d_got - d_ref)) <= 1e-8 * np.max(np.abs(d_ref))
     assert S.rel_err(ctx.download(res["psi"]), ref["psi"]) < TOL_LOOP
     ctx.close()
+
+
+def test_exc_cor_pz_spin_polarised_against_oracle():
+    """exc_cor_pz_sp on the GPU (nspin = 2: spin densities in, Vxc per spin out)
+    against the oracle's restatement, on the orbitals' spin densities and on
+    random spin densities over rs 0.17 .. 29 and all polarisations."""
+    from salmon2_b200.rt import Context
+    s = S.periodic_small(nspin=2)
+    ctx = Context(s)
+    rho_s = Oracle(s).density(s.psi)
+    rng = np.random.default_rng(9)
+    wide = np.exp(rng.uniform(np.log(1e-5), np.log(50.0), rho_s.shape))
+    wide[..., 1] *= rng.uniform(0.0, 1.0, wide.shape[:3])  # zeta over (0, 1)
+    for f in (rho_s, wide):
+        v, e = ctx.exc_cor_pz(f)
+        vr, er = OR.exc_cor_pz_sp(f, s.grid.hvol)
+        assert v.shape == f.shape
+        assert S.rel_err(v, vr) < TOL
+        assert abs(e - er) <= TOL * abs(er)
+    ctx.close()
+
+
+@pytest.mark.parametrize("kind", ["periodic", "isolated_cg"])
+def test_rt_propagate_self_consistent_spin_polarised(kind):
+    """The self-consistent loop with nspin = 2 (Hartree of rho_up + rho_dn, the
+    spin-polarised PZ, V_local per spin) inside the loop's CUDA graph against
+    the oracle's loop: J(t) (periodic) and the dipole every step, the final
+    orbitals and the potential left behind."""
+    import dataclasses as dc
+    from salmon2_b200 import synth
+    from salmon2_b200.rt import Context
+    nt = 6
+    if kind == "periodic":
+        s = S.periodic_small(nspin=2)
+        dt = 0.08
+        Ac = synth.asin2cos(nt, dt, omega=0.05696, f0=0.05696 * 2e-2, tw=nt * dt)
+    else:
+        s0 = synth.isolated_system(num=24, no=3, natom=2, seed=15, nspin=2, name="isolated24_sp")
+        s = dc.replace(s0, psi=synth.impulse_kick(s0.grid, s0.psi, 1e-3))
+        dt, Ac = 0.05, None
+    zc = synth.taylor_zc(dt)
+    brl = _brl(s)
+    vpsl = np.array(s.V_local[..., 0])
+    O = _oracle(s)
+    rho0_s = O.density(s.psi)
+    rho0 = rho0_s[..., 0] + rho0_s[..., 1]
+    vxc0 = OR.exc_cor_pz_sp(rho0_s, s.grid.hvol)[0]
+    cg = None
+    if kind == "periodic":
+        vh0 = OR.poisson_ft(rho0, brl)
+    else:
+        vh0, _ = O.poisson_isolated_cg(rho0)
+        cg = dict(vh0=vh0)
+    v0 = OR.update_vlocal(vpsl, vh0, vxc0)
+    ref = O.rt_run_scf(s.psi, nt, dt, zc, vpsl, brl, v0, Ac_ext=Ac, cg=cg)
+    ctx = Context(s)
+    a, b, w = ctx.upload(s.psi), ctx.zeros(), ctx.zeros()
+    ctx.update_vlocal(vpsl, vh0, vxc0)
+    if cg is not None:
+        ctx.set_hartree_cg(vh0)
+    ctx.set_self_consistent(True, vpsl, brl)
+    res = ctx.rt_propagate(a, b, w, nt, dt, zc, Ac_ext=Ac)
+    if kind == "periodic":
+        jmax = np.max(np.abs(ref["curr"]))
+        assert jmax > 0 and np.max(np.abs(res["curr"] - ref["curr"])) <= TOL_LOOP * jmax
+        assert S.rel_err(res["rbox"], ref["rbox"]) < TOL_LOOP
+    else:
+        d_ref = ref["rbox"][:3] - ref["rbox"][:3, :1]
+        d_got = res["rbox"][:3] - res["rbox"][:3, :1]
+        assert np.max(np.abs(d_got - d_ref)) <= 1e-8 * np.max(np.abs(d_ref))
+    assert S.rel_err(ctx.download(res["psi"]), ref["psi"]) < TOL_LOOP
+    O.V[...] = ref["V_local"]
+    O.set_vec_Ac((0.0, 0.0, 0.0))
+    ctx.set_vec_Ac((0.0, 0.0, 0.0))
+    h = ctx.zeros()
+    ctx.hpsi(res["psi"], h)
+    assert S.rel_err(ctx.download(h), O.hpsi(ref["psi"])) < TOL_LOOP
+    ctx.close()

@@ -263,3 +263,44 @@ def test_rt_run_scf_cg_equals_the_loop_written_out():
     assert np.max(np.abs(ref["psi"] - psi)) <= 1e-13 * np.max(np.abs(psi))
     assert np.max(np.abs(ref["Vh"] - vh)) <= 1e-13 * np.max(np.abs(vh))
     assert np.max(np.abs(ref["V_local"] - step.V[..., 0])) <= 1e-13 * np.max(np.abs(step.V))
+
+
+def test_spin_polarised_pz_is_the_derivative_of_its_energy_and_meets_the_limits():
+    """exc_cor_pz_sp (builtin_pz_sp.f90): Vxc_s = d(rho e_xc)/d rho_s (central
+    differences on the two spin densities, both rs branches); at zeta = 0 the
+    unpolarised PZ up to the two forms' density offsets (1e-10 against 1e-20);
+    at zeta -> 1 the polarised exchange 2^(1/3) e_x plus the polarised
+    correlation fit."""
+    import oracle as OR
+    rng = np.random.default_rng(41)
+    up = rng.uniform(0.002, 0.6, (6, 5, 4))
+    dn = rng.uniform(0.002, 0.6, (6, 5, 4))
+    hv = 0.37
+    v, e = OR.exc_cor_pz_sp(np.stack([up, dn], axis=-1), hv)
+    for s in range(2):
+        h = 1e-6 * (up if s == 0 else dn)
+        # the energy is a sum of local terms: move one point's spin density at a time
+        for idx in [(0, 0, 0), (3, 2, 1), (5, 4, 3)]:
+            dp = [a.copy() for a in (up, dn)]
+            dm = [a.copy() for a in (up, dn)]
+            dp[s][idx] += h[idx]
+            dm[s][idx] -= h[idx]
+            Ep = OR.exc_cor_pz_sp(np.stack(dp, axis=-1), 1.0)[1]
+            Em = OR.exc_cor_pz_sp(np.stack(dm, axis=-1), 1.0)[1]
+            assert abs((Ep - Em) / (2 * h[idx]) - v[idx + (s,)]) < 1e-6 * abs(v[idx + (s,)])
+    r = rng.uniform(0.05, 0.6, (4, 4, 4))
+    v1, e1 = OR.exc_cor_pz(r, hv)
+    v2, e2 = OR.exc_cor_pz_sp(np.stack([r / 2, r / 2], axis=-1), hv)
+    assert np.max(np.abs(v2[..., 0] - v1)) < 1e-8 * np.max(np.abs(v1))
+    assert np.array_equal(v2[..., 0], v2[..., 1]) and abs(e2 - e1) < 1e-8 * abs(e1)
+    # fully polarised: E_xc / (hvol * sum rho) per point from the P fit
+    for rho in (0.3, 0.02):  # rs < 1 and rs > 1
+        E = OR.exc_cor_pz_sp(np.stack([np.full((1, 1, 1), rho), np.zeros((1, 1, 1))], axis=-1), 1.0)[1]
+        t = rho + 1e-20
+        rs = (3.0 / (4.0 * np.pi * t)) ** (1.0 / 3.0)
+        cx = 0.75 * (3.0 / (2 * np.pi)) ** (2.0 / 3.0)
+        if rs > 1:
+            ec = -0.0843 / (1.0 + 1.3981 * np.sqrt(rs) + 0.2611 * rs)
+        else:
+            ec = 0.01555 * np.log(rs) - 0.0269 + 0.0007 * rs * np.log(rs) - 0.0048 * rs
+        assert abs(E / t - (-(2.0 ** (1.0 / 3.0)) * cx / rs + ec)) < 1e-9 * abs(E / t)

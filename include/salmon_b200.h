@@ -204,6 +204,18 @@ int sb200_set_lattice(sb200_ctx* ctx, const double rmatrix_B[9], const double co
  * (src/common/stencil.f90:295-315, src/common/zstencil_microac_core/typical/seq.f90). */
 int sb200_set_micro_ac(sb200_ctx* ctx, const double* Ac_micro, const double* div_Ac);
 
+/* absorbing_boundary = 'z' (yn_z = 1; 0 = 'none', the default): hpsi adds
+ * -i w(z) psi with w = w0 (dr - z) / dr for z <= dr and w0 (z - (al_z - dr)) / dr
+ * for z >= al_z - dr (z = iz * hgs(3) of the global plane index, al_z = al(3)
+ * the cell length, w0 = imagnary_potential_w0, dr = imagnary_potential_dr),
+ * after the stencil and before the nonlocal term; ttpsi includes it.  Taken by
+ * sb200_hpsi, sb200_taylor and sb200_rt_propagate through the per-point
+ * kernels (orthogonal cells, FP64; the mixed form refuses it).
+ * Replaces: add_imaginary_potential_for_absorbing_boundary_z
+ * (src/common/hamiltonian.f90:760-807) as hpsi calls it (:231-234, :300-303). */
+int sb200_set_absorbing_boundary(sb200_ctx* ctx, int yn_z, double imagnary_potential_w0,
+                                 double imagnary_potential_dr, double al_z);
+
 /* yn_symmetrized_stencil (1 = 'y', 0 = 'n', the default): the single-scale
  * hpsi takes the symmetrized form, h = (V + lap0) psi - lap psi / 2
  * + |k + A(r)|^2 psi / 2 - (i/2) ((k + A(r)).grad psi + div((k + A) psi)), the

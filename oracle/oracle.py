@@ -38,6 +38,7 @@ class SboSystem(C.Structure):
         ("nonorth", C.c_int), ("rmatrix_B", C.c_double * 9), ("coef_F", C.c_double * 6),
         ("ac_micro", _dp), ("div_ac", _dp),
         ("symmetrized", C.c_int),
+        ("cap_on", C.c_int), ("cap_w0", C.c_double), ("cap_dr", C.c_double), ("cap_al", C.c_double),
     ]
 
 
@@ -259,6 +260,17 @@ class Oracle:
         cur = np.zeros((3, self.sys.nspin), order="F")
         lib().sbo_calc_current(C.byref(self.s), _p(a), _p(cur))
         return cur
+
+    def set_absorbing_boundary(self, w0=None, dr=None, al_z=None):
+        """absorbing_boundary = 'z' (imagnary_potential_w0 / _dr, al(3); default the
+        grid's nz * hgs(3)); w0 None switches it off."""
+        if w0 is None:
+            self.s.cap_on = 0
+            return
+        g = self.sys.grid
+        self.s.cap_on = 1
+        self.s.cap_w0, self.s.cap_dr = float(w0), float(dr)
+        self.s.cap_al = float(g.num[2] * g.hgs[2]) if al_z is None else float(al_z)
 
     def microscopic_current(self, psi):
         """calc_microscopic_current: (3, nx, ny, nz), Fortran order."""

@@ -472,6 +472,27 @@ void sbo_dpseudo(const sbo_system* s, const double* tpsi, double* htpsi) {
   }
 }
 
+// add_imaginary_potential_for_absorbing_boundary_z (hamiltonian.f90:760-807):
+// on each plane z = iz hgs(3), w = (0, -w0 (z1 - z) / dr) below z1 = dr,
+// (0, -w0 (z - z2) / dr) above z2 = al(3) - dr, and htpsi += w tpsi.
+static void cap_add(const sbo_system* s, const Idx& I, const double* tpsi, double* htpsi) {
+  const double z1 = s->cap_dr, z2 = s->cap_al - s->cap_dr;
+#pragma omp parallel for
+  for (long o = 0; o < I.norb(); ++o)
+    for (int iz = s->is[2]; iz <= s->ie[2]; ++iz) {
+      const double z = iz * s->hgs[2];
+      zc_t w;
+      if (z <= z1) w = zc_t(0.0, -s->cap_w0 * (z1 - z) / s->cap_dr);
+      else if (z >= z2) w = zc_t(0.0, -s->cap_w0 * (z - z2) / s->cap_dr);
+      else continue;
+      for (int iy = s->is[1]; iy <= s->ie[1]; ++iy)
+        for (int ix = s->is[0]; ix <= s->ie[0]; ++ix) {
+          const long i = I.vol * o + I.a(ix, iy, iz);
+          st(htpsi, i, ld(htpsi, i) + w * ld(tpsi, i));
+        }
+    }
+}
+
 // hpsi, complex, orthogonal lattice: hamiltonian.f90:139-235 then zpseudo :424-435;
 // non-orthogonal lattice: hamiltonian.f90:306-357 (kAc Cartesian, k_lap0 =
 // coef_lap0 + |kAc|^2 / 2, Bk = rmatrix_B kAc) then zpseudo.
@@ -492,6 +513,7 @@ void sbo_hpsi(const sbo_system* s, const double* tpsi, double* htpsi) {
             zstencil_microac_one(s, I, tpsi + 2 * I.vol * o, htpsi + 2 * I.vol * o, s->V_local + nxy * (is - 1),
                                  s->vec_k + 3 * (ik - 1));
         }
+    if (s->cap_on) cap_add(s, I, tpsi, htpsi);  // hamiltonian.f90:300-303
     if (s->nlma > 0) sbo_zpseudo(s, tpsi, htpsi);
     return;
   }
@@ -535,6 +557,7 @@ void sbo_hpsi(const sbo_system* s, const double* tpsi, double* htpsi) {
                        s->V_local + nxy * (is - 1), k_lap0, s->coef_lap, k_nabt, false);
         }
   }
+  if (s->cap_on) cap_add(s, I, tpsi, htpsi);  // hamiltonian.f90:231-234
   if (s->nlma > 0) sbo_zpseudo(s, tpsi, htpsi);
 }
 

@@ -80,6 +80,10 @@ typedef struct {
   const double *div_ac;
   /* yn_symmetrized_stencil = 'y': zstencil_microAc_symmetrized (div_ac unused) */
   int symmetrized;
+  /* absorbing_boundary = 'z' (hamiltonian.f90:760-807): imagnary_potential_w0,
+   * imagnary_potential_dr, al(3) */
+  int cap_on;
+  double cap_w0, cap_dr, cap_al;
 } sbo_system;
 
 void sbo_set_threads(int n);

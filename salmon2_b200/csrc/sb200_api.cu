@@ -390,6 +390,7 @@ int sb200_ctx_destroy(sb200_ctx* c) {
   dfree(c->d_acm);
   dfree(c->d_divac);
   dfree(c->d_mcur);
+  dfree(c->d_cap);
   for (cudaEvent_t e : c->ev) cudaEventDestroy(e);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
   delete c;
@@ -773,6 +774,8 @@ int sb200_set_lattice(sb200_ctx* c, const double rmatrix_B[9], const double coef
     for (int i = 0; i < 6; ++i) c->g.coefF[i] = i < 3 ? 1.0 : 0.0;
   } else {
     if (!c->g.periodic) return set_error(SB200_ERR_UNSUPPORTED, "a non-orthogonal lattice needs a periodic grid");
+    if (c->cap_on)
+      return set_error(SB200_ERR_UNSUPPORTED, "the absorbing boundary is for orthogonal cells (inputoutput.f90:2789-2795)");
     for (int i = 0; i < 9; ++i) c->g.rB[i] = rmatrix_B[i];
     for (int i = 0; i < 6; ++i) c->g.coefF[i] = coef_F[i];
     c->g.nonorth = 1;
@@ -804,6 +807,34 @@ int sb200_set_micro_ac(sb200_ctx* c, const double* Ac_micro, const double* div_A
     SB_CUDA(cudaMemsetAsync(c->d_divac, 0, n * sizeof(double), c->stream));
   SB_CUDA(cudaStreamSynchronize(c->stream));
   c->microac = 1;
+  return SB200_OK;
+}
+
+int sb200_set_absorbing_boundary(sb200_ctx* c, int yn_z, double w0, double dr, double al_z) {
+  CHECK_CTX(c);
+  if (!c->g.set) return set_error(SB200_ERR_STATE, "sb200_set_grid has not been called");
+  if (!yn_z) {
+    c->cap_on = 0;
+    return SB200_OK;
+  }
+  if (c->g.nonorth)
+    return set_error(SB200_ERR_UNSUPPORTED, "the absorbing boundary is for orthogonal cells (inputoutput.f90:2789-2795)");
+  if (!(dr > 0.0) || !(al_z > 0.0)) return set_error(SB200_ERR_INVALID_ARG, "imagnary_potential_dr and al(3) must be > 0");
+  DeviceGuard dg(c->device);
+  // add_imaginary_potential_for_absorbing_boundary_z (hamiltonian.f90:760-807):
+  // z = iz hgs(3); -i w0 (z1 - z) / dr below z1 = dr, -i w0 (z - z2) / dr above
+  // z2 = al(3) - dr, nothing between; the table holds the w of each plane
+  const int nz = c->g.nz;
+  std::vector<double> w(nz, 0.0);
+  const double z1 = dr, z2 = al_z - dr;
+  for (int k = 0; k < nz; ++k) {
+    const double z = (double)(c->g.is[2] + k) * c->g.hgs[2];
+    if (z <= z1) w[k] = w0 * (z1 - z) / dr;
+    else if (z >= z2) w[k] = w0 * (z - z2) / dr;
+  }
+  dfree(c->d_cap);
+  TRY(upload(&c->d_cap, w));
+  c->cap_on = 1;
   return SB200_OK;
 }
 

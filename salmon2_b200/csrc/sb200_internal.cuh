@@ -196,6 +196,9 @@ struct sb200_ctx {
   // single-scale Maxwell-TDDFT (sb200_set_micro_ac): Ac_micro [npts][3] and div Ac [npts]
   int microac = 0;
   int micro_sym = 0;  // sb200_set_symmetrized_stencil
+  // absorbing boundary along z (sb200_set_absorbing_boundary): w(z) per plane
+  int cap_on = 0;
+  double* d_cap = nullptr;  // [nz]
   double* d_acm = nullptr;
   double* d_divac = nullptr;
   // microscopic current (sb200_calc_microscopic_current): chunk sums and the result

@@ -197,7 +197,19 @@ struct HArgs {
   const double2* ent_zk;
   const double2* proj;
   double2 zc;
+  const double* cap;  // absorbing boundary: w(z) per plane, or null
 };
+
+// the absorbing boundary's -i w(z) psi (add_imaginary_potential_for_absorbing_boundary_z,
+// hamiltonian.f90:760-807), after the stencil and before the nonlocal term
+__device__ __forceinline__ void add_cap(const HArgs& a, int z, double2 c, double2& h) {
+  if (!a.cap) return;
+  const double wv = __ldg(a.cap + z);
+  if (wv != 0.0) {
+    h.x += wv * c.y;
+    h.y -= wv * c.x;
+  }
+}
 
 template <int MODE>
 __global__ void __launch_bounds__(256) k_hpsi(const double2* __restrict__ in, double2* __restrict__ hout,
@@ -266,6 +278,7 @@ __global__ void __launch_bounds__(256) k_hpsi(const double2* __restrict__ in, do
   double2 h;
   h.x = vl * c.x + lap0 * c.x - 0.5 * v.x + w.y;
   h.y = vl * c.y + lap0 * c.y - 0.5 * v.y - w.x;
+  add_cap(a, z, c, h);
   if (MODE == 9) {  // ttpsi = htpsi - V_local tpsi before the nonlocal term (hamiltonian.f90:364-414)
     hout[(long)o * a.npts + p] = make_double2(h.x - vl * c.x, h.y - vl * c.y);
     return;
@@ -631,6 +644,7 @@ HArgs make_hargs(const sb200_ctx* c, double2 zc) {
   a.ent_zk = c->pp.d_ent_zk;
   a.proj = c->d_proj;
   a.zc = zc;
+  a.cap = c->cap_on ? c->d_cap : nullptr;
   return a;
 }
 
@@ -898,6 +912,7 @@ __global__ void __launch_bounds__(256) k_hpsi_micro(const double2* __restrict__ 
     h.x = dg * c.x - 0.5 * v.x + hk * c.x + kw.y + 0.5 * div * c.y;
     h.y = dg * c.y - 0.5 * v.y + hk * c.y - kw.x - 0.5 * div * c.x;
   }
+  add_cap(a, z, c, h);
   if (a.nlma > 0) {
     const int pm = __ldg(a.pmap + p);
     if (pm >= 0) {
@@ -1059,7 +1074,9 @@ int launch_micro_current(sb200_ctx* c, const double2* psi, double* curr, double*
 int launch_hpsi(sb200_ctx* c, const HpsiLaunch& L) {
   if (c->microac) return launch_hpsi_micro(c, L);
   if (c->g.nonorth) return launch_hpsi_nonorth(c, L);
-  if (c->stencil_variant == 1 || L.mode >= 5) return launch_hpsi_tiled(c, L);
+  if (c->cap_on && L.mode >= 5)
+    return set_error(SB200_ERR_UNSUPPORTED, "the absorbing boundary has no mixed-precision form");
+  if (!c->cap_on && (c->stencil_variant == 1 || L.mode >= 5)) return launch_hpsi_tiled(c, L);
   const double2* IN = (const double2*)L.in;
   double2* HOUT = (double2*)L.hout;
   HArgs a;
@@ -1081,6 +1098,7 @@ int launch_hpsi(sb200_ctx* c, const HpsiLaunch& L) {
   a.ent_zk = c->pp.d_ent_zk;
   a.proj = c->d_proj;
   a.zc = L.zc;
+  a.cap = c->cap_on ? c->d_cap : nullptr;
   dim3 grid((unsigned)((c->g.npts + 255) / 256), c->orb.norb);
   switch (L.mode) {
     case 0: k_hpsi<0><<<grid, 256, 0, c->stream>>>(IN, HOUT, L.out, a); break;

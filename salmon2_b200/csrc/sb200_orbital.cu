@@ -909,7 +909,7 @@ __global__ void __launch_bounds__(NT2, 1) k_term_orbital_tma(const double2* __re
 
 bool orbital_kernel_applies(const sb200_ctx* c) {
   const GridInfo& g = c->g;
-  return g.periodic && !g.nonorth && !c->microac && g.nx == N && g.ny == N && g.nz == N && c->stencil_variant == 1 &&
+  return g.periodic && !g.nonorth && !c->microac && !c->cap_on && g.nx == N && g.ny == N && g.nz == N && c->stencil_variant == 1 &&
          c->pp.nlma <= ORB_MAX_NLMA && c->precision == SB200_PREC_FP64;
 }
 

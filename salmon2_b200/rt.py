@@ -104,6 +104,16 @@ class Context:
         check(lib().sb200_set_micro_ac(self.h, C.c_void_p(a.ctypes.data),
                                        None if d is None else C.c_void_p(d.ctypes.data)))
 
+    def set_absorbing_boundary(self, w0=None, dr=None, al_z=None):
+        """absorbing_boundary = 'z' with imagnary_potential_w0 / _dr and the cell
+        length al(3) (default: the grid's nz * hgs(3)); w0 None switches it off."""
+        if w0 is None:
+            check(lib().sb200_set_absorbing_boundary(self.h, 0, 0.0, 0.0, 0.0))
+            return
+        g = self.sys.grid
+        L = float(g.num[2] * g.hgs[2]) if al_z is None else float(al_z)
+        check(lib().sb200_set_absorbing_boundary(self.h, 1, float(w0), float(dr), L))
+
     def calc_microscopic_current(self, psi):
         """calc_microscopic_current (density_matrix.f90:726-845): (3, nx, ny, nz),
         Fortran order."""

@@ -396,3 +396,23 @@ def test_microscopic_current_of_lattice_plane_waves():
     assert cur.shape == (3,) + g.shape
     for d in range(3):
         assert np.max(np.abs(cur[d] - want[d])) <= 1e-12 * max(1.0, np.max(np.abs(want)))
+
+
+def test_absorbing_boundary_adds_minus_i_w_psi_on_the_edge_planes():
+    """add_imaginary_potential_for_absorbing_boundary_z: hpsi with the absorbing
+    boundary minus hpsi without is -i w(z) psi, w = w0 (dr - z)/dr for z <= dr,
+    w0 (z - (L - dr))/dr for z >= L - dr, zero between (z = iz hgs(3))."""
+    s = S.periodic_small()
+    g = s.grid
+    w0, dr = 0.3, 2.0
+    L = float(g.num[2] * g.hgs[2])
+    O1, O2 = Oracle(s), Oracle(s)
+    O2.set_absorbing_boundary(w0, dr)
+    h1, h2 = O1.hpsi(s.psi), O2.hpsi(s.psi)
+    sl = g.interior_slices()
+    z = np.arange(g.is_[2], g.ie[2] + 1) * g.hgs[2]
+    w = np.where(z <= dr, w0 * (dr - z) / dr, np.where(z >= L - dr, w0 * (z - (L - dr)) / dr, 0.0))
+    assert np.count_nonzero(w) >= 4 and np.count_nonzero(w == 0) >= 4
+    d = (h2 - h1)[sl]
+    want = -1j * w[None, None, :, None, None, None] * s.psi[sl]
+    assert np.max(np.abs(d - want)) <= 1e-13 * np.max(np.abs(h1))

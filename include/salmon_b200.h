@@ -204,6 +204,17 @@ int sb200_set_lattice(sb200_ctx* ctx, const double rmatrix_B[9], const double co
  * (src/common/stencil.f90:295-315, src/common/zstencil_microac_core/typical/seq.f90). */
 int sb200_set_micro_ac(sb200_ctx* ctx, const double* Ac_micro, const double* div_Ac);
 
+/* An isolated system driven by a pulse in the length gauge (ae_shape1 /=
+ * 'impulse'; on = 1, 0 = off, the default): every step of sb200_rt_propagate
+ * takes V_local + E_ext(itt).r (lg%coordinate) for its Taylor expansion, with
+ * E_ext(itt) = -(Ac_ext(itt+1) - Ac_ext(itt)) / dt from the loop's Ac_ext,
+ * and leaves the field-free V_local (with the self-consistent update, that of
+ * the last step) behind.  Isolated grids only (periodic ones take A(t)).
+ * Replaces: calcVbox (src/rt/em_field.f90:422-548), the E_ext table of
+ * initialization_rt (src/rt/initialization_rt.f90:180-183) and V_local +
+ * Vbox of time_evolution_step (src/rt/time_evolution_step.f90:95-116).       */
+int sb200_set_length_gauge(sb200_ctx* ctx, int on);
+
 /* absorbing_boundary = 'z' (yn_z = 1; 0 = 'none', the default): hpsi adds
  * -i w(z) psi with w = w0 (dr - z) / dr for z <= dr and w0 (z - (al_z - dr)) / dr
  * for z >= al_z - dr (z = iz * hgs(3) of the global plane index, al_z = al(3)

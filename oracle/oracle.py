@@ -39,6 +39,7 @@ class SboSystem(C.Structure):
         ("ac_micro", _dp), ("div_ac", _dp),
         ("symmetrized", C.c_int),
         ("cap_on", C.c_int), ("cap_w0", C.c_double), ("cap_dr", C.c_double), ("cap_al", C.c_double),
+        ("length_gauge", C.c_int),
     ]
 
 
@@ -260,6 +261,11 @@ class Oracle:
         cur = np.zeros((3, self.sys.nspin), order="F")
         lib().sbo_calc_current(C.byref(self.s), _p(a), _p(cur))
         return cur
+
+    def set_length_gauge(self, on=True):
+        """ae_shape1 /= 'impulse' on an isolated grid: each step's Taylor expansion
+        takes V_local + E_ext(itt).r (calcVbox)."""
+        self.s.length_gauge = 1 if on else 0
 
     def set_absorbing_boundary(self, w0=None, dr=None, al_z=None):
         """absorbing_boundary = 'z' (imagnary_potential_w0 / _dr, al(3); default the

@@ -964,13 +964,36 @@ static int rt_run_impl(sbo_system* s, double* psi_a, double* psi_b, double* work
   double* in = psi_a;
   double* out = psi_b;
   int which = 1;
+  // length gauge (calcVbox, em_field.f90:422-548; time_evolution_step.f90:95-116):
+  // E_ext(itt) = -(Ac_ext(itt+1) - Ac_ext(itt)) / dt (initialization_rt.f90:180-183)
+  const bool lgauge = !s->periodic && s->length_gauge;
+  std::vector<double> veff(lgauge ? npts * s->nspin : 0);
+  std::vector<double> cx[3];
+  if (lgauge)
+    for (int d = 0; d < 3; ++d)  // lg%coordinate, initialization.f90:1125-1190
+      for (int i = s->is[d]; i <= s->ie[d]; ++i)
+        cx[d].push_back(s->lg_num[d] % 2 == 1 ? i * s->hgs[d] : (i - 0.5) * s->hgs[d]);
   for (int itt = 1; itt <= nt; ++itt) {
+    const double* v_base = s->V_local;
+    if (lgauge) {
+      double E[3];
+      for (int d = 0; d < 3; ++d) E[d] = -(Ac_ext[3 * (itt + 1) + d] - Ac_ext[3 * itt + d]) / dt;
+      const long nx = (long)cx[0].size(), ny = (long)cx[1].size();
+      for (int is = 0; is < s->nspin; ++is)
+        for (long p = 0; p < npts; ++p) {
+          const long x = p % nx, y = (p / nx) % ny, z = p / (nx * ny);
+          const double vb = 0.0 + (E[0] * cx[0][x] + E[1] * cx[1][y] + E[2] * cx[2][z]);
+          veff[is * npts + p] = v_base[is * npts + p] + vb;
+        }
+      s->V_local = veff.data();
+    }
     if (s->periodic) {
       for (int d = 0; d < 3; ++d)
         s->vec_Ac[d] = 0.5 * (Ac_tot[3 * itt + d] + Ac_tot[3 * (itt - 1) + d]);
       if (s->nlma > 0) sbo_update_kvector_nonlocalpt(s);
     }
     sbo_taylor(s, in, out, work, zc, n_hamil);
+    s->V_local = v_base;  // the step's update_vlocal: the field-free potential again
     sbo_calc_density(s, out, rho_work);
     if (scf) {
       const int num[3] = {s->ie[0] - s->is[0] + 1, s->ie[1] - s->is[1] + 1, s->ie[2] - s->is[2] + 1};

@@ -84,6 +84,9 @@ typedef struct {
    * imagnary_potential_dr, al(3) */
   int cap_on;
   double cap_w0, cap_dr, cap_al;
+  /* isolated grid, pulse in the length gauge (ae_shape1 /= 'impulse'):
+   * V_local + E_ext(itt).r in each step's Taylor expansion                  */
+  int length_gauge;
 } sbo_system;
 
 void sbo_set_threads(int n);

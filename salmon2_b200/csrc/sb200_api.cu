@@ -292,6 +292,7 @@ int issue_rt_step(sb200_ctx* c, double2* in, double2* out, double2* work, const 
     TIMED(c, SB200_KIND_FINAL, launch_finalize(c, -1, 0, trans_longi, dt, -1, true));
     return scf_rt_issue(c, out);
   }
+  if (c->lg_active) TRY(launch_vbox(c, c->timing ? SB200_KIND_POTENTIAL : -1));
   TRY(issue_taylor(c, in, out, work, zc, n_hamil));
   TIMED(c, SB200_KIND_OBS, launch_observables(c, out));
   if (c->g.periodic) TIMED(c, SB200_KIND_MOMENTS, launch_project_moments(c, out));
@@ -391,6 +392,8 @@ int sb200_ctx_destroy(sb200_ctx* c) {
   dfree(c->d_divac);
   dfree(c->d_mcur);
   dfree(c->d_cap);
+  dfree(c->d_vloc_base);
+  dfree(c->d_eext);
   for (cudaEvent_t e : c->ev) cudaEventDestroy(e);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
   delete c;
@@ -810,6 +813,15 @@ int sb200_set_micro_ac(sb200_ctx* c, const double* Ac_micro, const double* div_A
   return SB200_OK;
 }
 
+int sb200_set_length_gauge(sb200_ctx* c, int on) {
+  CHECK_CTX(c);
+  if (!c->g.set) return set_error(SB200_ERR_STATE, "sb200_set_grid has not been called");
+  if (on && c->g.periodic)
+    return set_error(SB200_ERR_UNSUPPORTED, "the length gauge is for isolated grids (periodic ones take A(t))");
+  c->length_gauge = on ? 1 : 0;
+  return SB200_OK;
+}
+
 int sb200_set_absorbing_boundary(sb200_ctx* c, int yn_z, double w0, double dr, double al_z) {
   CHECK_CTX(c);
   if (!c->g.set) return set_error(SB200_ERR_STATE, "sb200_set_grid has not been called");
@@ -1100,6 +1112,29 @@ int sb200_rt_propagate(sb200_ctx* c, double* psi_a, double* psi_b, double* work,
   double2* W = (double2*)work;
   TRY(scf_rt_prepare(c));
   TRY(nonorth_prepare(c));
+  if (c->length_gauge && !c->g.periodic) {  // E_ext(itt) = -(Ac_ext(itt+1) - Ac_ext(itt)) / dt, initialization_rt.f90:180-183
+    std::vector<double> ac(na, 0.0), e(na, 0.0);
+    if (Ac_ext) SB_CUDA(cudaMemcpy(ac.data(), Ac_ext, na * sizeof(double), cudaMemcpyDefault));
+    for (int itt = 0; itt <= nt; ++itt)
+      for (int d = 0; d < 3; ++d) e[3 * itt + d] = -(ac[3 * (itt + 1) + d] - ac[3 * itt + d]) / dt;
+    for (int d = 0; d < 3; ++d) e[3 * (nt + 1) + d] = e[3 * nt + d];
+    if (c->eext_cap < na) {
+      dfree(c->d_eext);
+      c->eext_cap = 0;
+      TRY(dalloc(&c->d_eext, na));
+      c->eext_cap = na;
+    }
+    const size_t nv = (size_t)c->g.npts * c->orb.nspin;
+    if (c->vloc_base_cap < nv) {
+      dfree(c->d_vloc_base);
+      c->vloc_base_cap = 0;
+      TRY(dalloc(&c->d_vloc_base, nv));
+      c->vloc_base_cap = nv;
+    }
+    SB_CUDA(cudaMemcpyAsync(c->d_eext, e.data(), na * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    SB_CUDA(cudaMemcpyAsync(c->d_vloc_base, c->d_vloc, nv * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+    c->lg_active = 1;
+  }
   SB_CUDA(cudaStreamSynchronize(c->stream));
 
   // Two steps (A->B, B->A) captured as one CUDA graph and replayed.
@@ -1149,6 +1184,11 @@ int sb200_rt_propagate(sb200_ctx* c, double* psi_a, double* psi_b, double* work,
   SB_CUDA(cudaStreamSynchronize(c->stream));
   SB_CUDA(cudaGetLastError());
   TRY(check_device_flag(c));
+  if (c->lg_active) {  // the field-free V_local the last step's update_vlocal leaves
+    c->lg_active = 0;
+    TRY(launch_vloc_restore(c));
+    SB_CUDA(cudaStreamSynchronize(c->stream));
+  }
   r.last_mit = r.loop_mit0 + nt;
   r.last_nt = nt;
   r.start_mit = 0;

@@ -196,6 +196,13 @@ struct sb200_ctx {
   // single-scale Maxwell-TDDFT (sb200_set_micro_ac): Ac_micro [npts][3] and div Ac [npts]
   int microac = 0;
   int micro_sym = 0;  // sb200_set_symmetrized_stencil
+  // isolated grid driven by a pulse in the length gauge (sb200_set_length_gauge):
+  // during a loop (lg_active) V_local = V_base + E_ext(itt).r before each step
+  int length_gauge = 0, lg_active = 0;
+  double* d_vloc_base = nullptr;  // [nspin][npts]
+  size_t vloc_base_cap = 0;
+  double* d_eext = nullptr;       // (3, 0:nt+1)
+  size_t eext_cap = 0;
   // absorbing boundary along z (sb200_set_absorbing_boundary): w(z) per plane
   int cap_on = 0;
   double* d_cap = nullptr;  // [nz]
@@ -283,6 +290,10 @@ int launch_finalize(sb200_ctx* c, int itt_host, int nt, int trans_longi, double 
                     bool fused_obs = false);
 // kind >= 0: each launch bracketed for sb200_kernel_times (SB200_KIND_*)
 int launch_density(sb200_ctx* c, const double2* psi, double* rho, int kind = -1);
+// length gauge: V_local = V_base + E_ext(itt).r (itt from the device counter),
+// and the field-free V_local back from V_base after the loop
+int launch_vbox(sb200_ctx* c, int kind = -1);
+int launch_vloc_restore(sb200_ctx* c);
 int density_prepare(sb200_ctx* c);
 // microscopic current [npts][3] into curr (device); part: micro_current_part_len(c) doubles
 size_t micro_current_part_len(const sb200_ctx* c);

@@ -960,6 +960,61 @@ int launch_hpsi_micro(sb200_ctx* c, const HpsiLaunch& L) {
 }
 
 // ---------------------------------------------------------------------------
+// Isolated system driven by a pulse in the length gauge (ae_shape1 /= 'impulse'):
+// calcVbox (em_field.f90:422-548) Vbox = E_ext(itt).r with lg%coordinate, and
+// V_local = V_local + Vbox before the Taylor step (time_evolution_step.f90:102-116);
+// the step's update_vlocal restores the field-free potential, kept here in base.
+// ---------------------------------------------------------------------------
+__global__ void k_vbox(const double* __restrict__ base, double* __restrict__ v, float* __restrict__ v32,
+                       const double* __restrict__ eext, const int* __restrict__ step, long n, int nspin, int nx,
+                       int ny, double o0, double o1, double o2, double h0, double h1, double h2) {
+  const int itt = *step;
+  const double e0 = eext[3 * itt], e1 = eext[3 * itt + 1], e2 = eext[3 * itt + 2];
+  const long tot = n * nspin;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < tot; i += (long)gridDim.x * blockDim.x) {
+    const long p = i % n;
+    const int x = (int)(p % nx), y = (int)((p / nx) % ny), z = (int)(p / ((long)nx * ny));
+    const double vb = 0.0 + (e0 * ((o0 + x) * h0) + e1 * ((o1 + y) * h1) + e2 * ((o2 + z) * h2));
+    const double val = base[i] + vb;
+    v[i] = val;
+    v32[i] = (float)val;
+  }
+}
+
+__global__ void k_vloc_restore(const double* __restrict__ base, double* __restrict__ v, float* __restrict__ v32,
+                               long tot) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < tot; i += (long)gridDim.x * blockDim.x) {
+    v[i] = base[i];
+    v32[i] = (float)base[i];
+  }
+}
+
+int launch_vbox(sb200_ctx* c, int kind) {
+  const long n = c->g.npts;
+  const int nspin = c->orb.nspin;
+  double o[3];
+  for (int d = 0; d < 3; ++d) o[d] = (double)c->g.is[d] - ((c->g.lg_num[d] % 2 == 1) ? 0.0 : 0.5);
+  long nb = (n * nspin + 255) / 256;
+  if (nb > 148L * 8) nb = 148L * 8;
+  if (kind >= 0 && kernel_timing_mark(c, kind, true)) return SB200_ERR_CUDA;
+  k_vbox<<<(unsigned)nb, 256, 0, c->stream>>>(c->d_vloc_base, c->d_vloc, c->d_vloc32, c->d_eext, c->rt.d_step, n,
+                                              nspin, c->g.nx, c->g.ny, o[0], o[1], o[2], c->g.hgs[0], c->g.hgs[1],
+                                              c->g.hgs[2]);
+  SB_LAUNCH_CHECK("k_vbox");
+  if (kind >= 0 && kernel_timing_mark(c, kind, false)) return SB200_ERR_CUDA;
+  return SB200_OK;
+}
+
+int launch_vloc_restore(sb200_ctx* c) {
+  const long tot = c->g.npts * c->orb.nspin;
+  long nb = (tot + 255) / 256;
+  if (nb > 148L * 8) nb = 148L * 8;
+  k_vloc_restore<<<(unsigned)nb, 256, 0, c->stream>>>(c->d_vloc_base, c->d_vloc, c->d_vloc32, tot);
+  SB_LAUNCH_CHECK("k_vloc_restore");
+  return SB200_OK;
+}
+
+// ---------------------------------------------------------------------------
 // Microscopic current density of the single-scale theory,
 // calc_microscopic_current / micro_current (density_matrix.f90:726-845):
 // j_d(r) = sum_{k,o,s} rocc wtk (Im(conj(psi) dpsi_d) + k_d |psi|^2) with dpsi_d

@@ -653,7 +653,9 @@ int scf_launch_update(sb200_ctx* c, const double* vpsl, const double* vh, const 
   const long n = scf_of(c)->npts;
   const int nspin = c->orb.nspin;
   TRY_S(scf_mark(c, kind, true));
-  k_update_vlocal<<<scf_grid_blocks(n * nspin), SCF_THREADS, 0, c->stream>>>(vpsl, vh, vxc, c->d_vloc, c->d_vloc32,
+  // in a length-gauge loop the update is the field-free base the next step adds E.r to
+  double* target = c->lg_active ? c->d_vloc_base : c->d_vloc;
+  k_update_vlocal<<<scf_grid_blocks(n * nspin), SCF_THREADS, 0, c->stream>>>(vpsl, vh, vxc, target, c->d_vloc32,
                                                                             n, nspin);
   return scf_mark(c, kind, false);
 }

@@ -184,6 +184,12 @@ module salmon_b200
       real(c_double), intent(in) :: Ac_micro(3, *), div_Ac(*)
     end function
 
+    integer(c_int) function sb200_set_length_gauge(ctx, on) bind(c, name="sb200_set_length_gauge")
+      import
+      type(c_ptr), value :: ctx
+      integer(c_int), value :: on
+    end function
+
     integer(c_int) function sb200_set_absorbing_boundary(ctx, yn_z, imagnary_potential_w0, imagnary_potential_dr, &
         al_z) bind(c, name="sb200_set_absorbing_boundary")
       import

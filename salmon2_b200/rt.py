@@ -104,6 +104,11 @@ class Context:
         check(lib().sb200_set_micro_ac(self.h, C.c_void_p(a.ctypes.data),
                                        None if d is None else C.c_void_p(d.ctypes.data)))
 
+    def set_length_gauge(self, on=True):
+        """An isolated system driven by a pulse in the length gauge (ae_shape1 /=
+        'impulse'): rt_propagate adds E_ext(itt).r to V_local every step."""
+        check(lib().sb200_set_length_gauge(self.h, 1 if on else 0))
+
     def set_absorbing_boundary(self, w0=None, dr=None, al_z=None):
         """absorbing_boundary = 'z' with imagnary_potential_w0 / _dr and the cell
         length al(3) (default: the grid's nz * hgs(3)); w0 None switches it off."""

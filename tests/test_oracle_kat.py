@@ -416,3 +416,26 @@ def test_absorbing_boundary_adds_minus_i_w_psi_on_the_edge_planes():
     d = (h2 - h1)[sl]
     want = -1j * w[None, None, :, None, None, None] * s.psi[sl]
     assert np.max(np.abs(d - want)) <= 1e-13 * np.max(np.abs(h1))
+
+
+def test_length_gauge_with_a_constant_field_is_a_static_potential():
+    """calcVbox: with Ac_ext(t) = -E t (a constant E = -dA/dt), every step takes
+    V_local + E.r; the loop equals the fixed-potential loop with that potential
+    built here from lg%coordinate (odd and even extents)."""
+    import dataclasses as dc
+    from salmon2_b200 import synth
+    for s in (S.isolated_small(), S.isolated_odd()):
+        g = s.grid
+        nt, dt = 3, 0.05
+        E = np.array([0.02, -0.01, 0.03])
+        Ac = np.asfortranarray(-E[:, None] * (np.arange(nt + 2) * dt)[None, :])
+        zc = synth.taylor_zc(dt)
+        O = Oracle(s)
+        O.set_length_gauge(True)
+        a = O.rt_run(s.psi, nt, dt, zc, Ac_ext=Ac)
+        X = np.meshgrid(*[g.coordinate(d) for d in range(3)], indexing="ij")
+        vb = E[0] * X[0] + E[1] * X[1] + E[2] * X[2]
+        s2 = dc.replace(s, V_local=np.asfortranarray(s.V_local + vb[..., None]))
+        b = Oracle(s2).rt_run(s.psi, nt, dt, zc)
+        assert np.max(np.abs(a["psi"] - b["psi"])) <= 1e-12 * np.max(np.abs(b["psi"]))
+        assert np.max(np.abs(a["rbox"] - b["rbox"])) <= 1e-12 * np.max(np.abs(b["rbox"]))

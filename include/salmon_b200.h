@@ -204,6 +204,18 @@ int sb200_set_lattice(sb200_ctx* ctx, const double rmatrix_B[9], const double co
  * (src/common/stencil.f90:295-315, src/common/zstencil_microac_core/typical/seq.f90). */
 int sb200_set_micro_ac(sb200_ctx* ctx, const double* Ac_micro, const double* div_Ac);
 
+/* propagator (0 = 'middlepoint', the default; 1 = 'aetrs'): with AETRS every
+ * step of sb200_rt_propagate is two half steps with the zc the caller passes
+ * (those of -i dt/2): the first with A(itt) and V_local, then V_local
+ * extrapolated as 3 V - 3 V_old1 + V_old2 (the stored potentials start as the
+ * loop's initial V_local) and A(itt+1) predicted as Ac_ext(itt+1) +
+ * 2 Ac_ind(itt) - Ac_ind(itt-1), the second half step; the current, the
+ * fields, the density and the self-consistent update as for the middle point.
+ * Replaces: the propagator = 'aetrs' branch of time_evolution_step and
+ * time_evolution_half_step_etrs (src/rt/time_evolution_step.f90:117-147,
+ * 430-470), with vloc_old of initialization_rt (:287-292).                    */
+int sb200_set_propagator(sb200_ctx* ctx, int aetrs);
+
 /* An isolated system driven by a pulse in the length gauge (ae_shape1 /=
  * 'impulse'; on = 1, 0 = off, the default): every step of sb200_rt_propagate
  * takes V_local + E_ext(itt).r (lg%coordinate) for its Taylor expansion, with

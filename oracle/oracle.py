@@ -39,7 +39,7 @@ class SboSystem(C.Structure):
         ("ac_micro", _dp), ("div_ac", _dp),
         ("symmetrized", C.c_int),
         ("cap_on", C.c_int), ("cap_w0", C.c_double), ("cap_dr", C.c_double), ("cap_al", C.c_double),
-        ("length_gauge", C.c_int),
+        ("length_gauge", C.c_int), ("aetrs", C.c_int),
     ]
 
 
@@ -261,6 +261,11 @@ class Oracle:
         cur = np.zeros((3, self.sys.nspin), order="F")
         lib().sbo_calc_current(C.byref(self.s), _p(a), _p(cur))
         return cur
+
+    def set_propagator(self, name="middlepoint"):
+        """propagator: 'middlepoint' (default) or 'aetrs' (give it the zc of the
+        half step, synth.taylor_zc(dt, aetrs=True))."""
+        self.s.aetrs = 1 if name == "aetrs" else 0
 
     def set_length_gauge(self, on=True):
         """ae_shape1 /= 'impulse' on an isolated grid: each step's Taylor expansion

@@ -973,6 +973,14 @@ static int rt_run_impl(sbo_system* s, double* psi_a, double* psi_b, double* work
     for (int d = 0; d < 3; ++d)  // lg%coordinate, initialization.f90:1125-1190
       for (int i = s->is[d]; i <= s->ie[d]; ++i)
         cx[d].push_back(s->lg_num[d] % 2 == 1 ? i * s->hgs[d] : (i - 0.5) * s->hgs[d]);
+  // AETRS: the stored potentials, vloc_old(:,1:2) = V_local (initialization_rt.f90:287-292)
+  const long nv = npts * s->nspin;
+  std::vector<double> old1, old2, vuse;
+  if (s->aetrs) {
+    old1.assign(s->V_local, s->V_local + nv);
+    old2 = old1;
+    vuse.resize(nv);
+  }
   for (int itt = 1; itt <= nt; ++itt) {
     const double* v_base = s->V_local;
     if (lgauge) {
@@ -987,12 +995,41 @@ static int rt_run_impl(sbo_system* s, double* psi_a, double* psi_b, double* work
         }
       s->V_local = veff.data();
     }
-    if (s->periodic) {
+    if (s->periodic) {  // middlepoint: (A(itt) + A(itt-1)) / 2; aetrs: A(itt)
       for (int d = 0; d < 3; ++d)
-        s->vec_Ac[d] = 0.5 * (Ac_tot[3 * itt + d] + Ac_tot[3 * (itt - 1) + d]);
+        s->vec_Ac[d] = s->aetrs ? Ac_tot[3 * itt + d] : 0.5 * (Ac_tot[3 * itt + d] + Ac_tot[3 * (itt - 1) + d]);
       if (s->nlma > 0) sbo_update_kvector_nonlocalpt(s);
     }
     sbo_taylor(s, in, out, work, zc, n_hamil);
+    if (s->aetrs) {  // time_evolution_half_step_etrs, time_evolution_step.f90:430-470
+      const double* V = s->V_local;
+      double E[3] = {0.0, 0.0, 0.0};
+      if (lgauge) {  // E_ext(itt + 1), with E_ext(nt + 1) = E_ext(nt)
+        const int j = itt + 1 <= nt ? itt + 1 : nt;
+        for (int d = 0; d < 3; ++d) E[d] = -(Ac_ext[3 * (j + 1) + d] - Ac_ext[3 * j + d]) / dt;
+      }
+      const long nx = s->ie[0] - s->is[0] + 1, ny = s->ie[1] - s->is[1] + 1;
+      for (long i = 0; i < nv; ++i) {
+        const double vn = 3.0 * V[i] - 3.0 * old1[i] + old2[i];
+        old2[i] = old1[i];
+        old1[i] = V[i];
+        vuse[i] = vn;
+        if (lgauge) {  // + Vbox(itt + 1)
+          const long p = i % npts;
+          const long x = p % nx, y = (p / nx) % ny, z = p / (nx * ny);
+          vuse[i] = vuse[i] + (0.0 + (E[0] * cx[0][x] + E[1] * cx[1][y] + E[2] * cx[2][z]));
+        }
+      }
+      s->V_local = vuse.data();
+      if (s->periodic) {
+        for (int d = 0; d < 3; ++d)
+          s->vec_Ac[d] = Ac_ext[3 * (itt + 1) + d] + 2.0 * Ac_ind[3 * itt + d] - Ac_ind[3 * (itt - 1) + d];
+        if (s->nlma > 0) sbo_update_kvector_nonlocalpt(s);
+      }
+      Idx I(s);
+      std::copy(out, out + 2 * I.vol * I.norb(), in);  // spsi_in%zwf = spsi_out%zwf
+      sbo_taylor(s, in, out, work, zc, n_hamil);
+    }
     s->V_local = v_base;  // the step's update_vlocal: the field-free potential again
     sbo_calc_density(s, out, rho_work);
     if (scf) {

@@ -87,6 +87,9 @@ typedef struct {
   /* isolated grid, pulse in the length gauge (ae_shape1 /= 'impulse'):
    * V_local + E_ext(itt).r in each step's Taylor expansion                  */
   int length_gauge;
+  /* propagator = 'aetrs' (time_evolution_step.f90:117-147, 430-470): half
+   * steps (zc of -i dt/2) around the extrapolated potential                  */
+  int aetrs;
 } sbo_system;
 
 void sbo_set_threads(int n);

@@ -283,9 +283,30 @@ int issue_taylor(sb200_ctx* c, double2* tin, double2* tout, double2* work, const
   return SB200_OK;
 }
 
-// one time_evolution_step on the device (itt from the device counter)
+// one time_evolution_step on the device (itt from the device counter); with
+// AETRS the step's result is back in `in` (out is the half step's scratch)
 int issue_rt_step(sb200_ctx* c, double2* in, double2* out, double2* work, const double2* zc, int n_hamil,
                   int trans_longi, double dt) {
+  if (c->aetrs) {
+    // propagator = 'aetrs' (time_evolution_step.f90:117-147, 430-470; zc of the
+    // half step -i dt/2): a half step with A(itt) and V(t), then V extrapolated
+    // (3 V - 3 V_old1 + V_old2) and A(itt+1) predicted, the second half step
+    if (c->g.periodic) TIMED(c, SB200_KIND_PREP, launch_prep_k(c, c->rt.d_Ac_tot, 2, -1, c->d_kcoef, true));
+    if (c->lg_active) TRY(launch_vbox(c, c->timing ? SB200_KIND_POTENTIAL : -1));
+    TRY(issue_taylor(c, in, out, work, zc, n_hamil));
+    TIMED(c, SB200_KIND_POTENTIAL, launch_aetrs_vloc(c));
+    if (c->g.periodic) TIMED(c, SB200_KIND_PREP, launch_prep_k(c, c->rt.d_Ac_ext, 3, -1, c->d_kcoef, true));
+    if (orbital_kernel_applies(c)) {
+      TRY(issue_taylor(c, out, in, work, zc, n_hamil, true));
+      TIMED(c, SB200_KIND_FINAL, launch_finalize(c, -1, 0, trans_longi, dt, -1, true));
+      return scf_rt_issue(c, in);
+    }
+    TRY(issue_taylor(c, out, in, work, zc, n_hamil));
+    TIMED(c, SB200_KIND_OBS, launch_observables(c, in));
+    if (c->g.periodic) TIMED(c, SB200_KIND_MOMENTS, launch_project_moments(c, in));
+    TIMED(c, SB200_KIND_FINAL, launch_finalize(c, -1, 0, trans_longi, dt, -1));
+    return scf_rt_issue(c, in);
+  }
   if (c->g.periodic) TIMED(c, SB200_KIND_PREP, launch_prep_k(c, c->rt.d_Ac_tot, 1, -1, c->d_kcoef, true));
   if (orbital_kernel_applies(c)) {  // observables fused into the last Taylor term
     TRY(issue_taylor(c, in, out, work, zc, n_hamil, true));
@@ -394,6 +415,7 @@ int sb200_ctx_destroy(sb200_ctx* c) {
   dfree(c->d_cap);
   dfree(c->d_vloc_base);
   dfree(c->d_eext);
+  dfree(c->d_vloc_old);
   for (cudaEvent_t e : c->ev) cudaEventDestroy(e);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
   delete c;
@@ -813,6 +835,13 @@ int sb200_set_micro_ac(sb200_ctx* c, const double* Ac_micro, const double* div_A
   return SB200_OK;
 }
 
+int sb200_set_propagator(sb200_ctx* c, int aetrs) {
+  CHECK_CTX(c);
+  if (aetrs != 0 && aetrs != 1) return set_error(SB200_ERR_INVALID_ARG, "propagator: 0 = middlepoint, 1 = aetrs");
+  c->aetrs = aetrs;
+  return SB200_OK;
+}
+
 int sb200_set_length_gauge(sb200_ctx* c, int on) {
   CHECK_CTX(c);
   if (!c->g.set) return set_error(SB200_ERR_STATE, "sb200_set_grid has not been called");
@@ -1135,17 +1164,32 @@ int sb200_rt_propagate(sb200_ctx* c, double* psi_a, double* psi_b, double* work,
     SB_CUDA(cudaMemcpyAsync(c->d_vloc_base, c->d_vloc, nv * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
     c->lg_active = 1;
   }
+  if (c->aetrs) {  // vloc_old(:,1:2) = V_local (initialization_rt.f90:287-292)
+    const size_t nv = (size_t)c->g.npts * c->orb.nspin;
+    if (c->vloc_old_cap < 2 * nv) {
+      dfree(c->d_vloc_old);
+      c->vloc_old_cap = 0;
+      TRY(dalloc(&c->d_vloc_old, 2 * nv));
+      c->vloc_old_cap = 2 * nv;
+    }
+    SB_CUDA(cudaMemcpyAsync(c->d_vloc_old, c->d_vloc, nv * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+    SB_CUDA(cudaMemcpyAsync(c->d_vloc_old + nv, c->d_vloc, nv * sizeof(double), cudaMemcpyDeviceToDevice,
+                            c->stream));
+  }
   SB_CUDA(cudaStreamSynchronize(c->stream));
 
   // Two steps (A->B, B->A) captured as one CUDA graph and replayed.
   cudaGraphExec_t exec2 = nullptr;
   const int pairs = c->timing ? 0 : nt / 2;
   int rc = SB200_OK;
+  // with AETRS every step maps A -> A (B its half-step scratch)
+  double2* A2 = c->aetrs ? A : B;
+  double2* B2 = c->aetrs ? B : A;
   if (c->timing) {  // instrumented: every launch bracketed by events, no graph
     for (int i = 0; i + 1 < nt; i += 2) {
       TRY(issue_rt_step(c, A, B, W, z.data(), n_hamil, trans_longi, dt));
       TRY(timing_flush(c));
-      TRY(issue_rt_step(c, B, A, W, z.data(), n_hamil, trans_longi, dt));
+      TRY(issue_rt_step(c, A2, B2, W, z.data(), n_hamil, trans_longi, dt));
       TRY(timing_flush(c));
     }
   }
@@ -1153,7 +1197,7 @@ int sb200_rt_propagate(sb200_ctx* c, double* psi_a, double* psi_b, double* work,
     cudaGraph_t graph = nullptr;
     SB_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
     rc = issue_rt_step(c, A, B, W, z.data(), n_hamil, trans_longi, dt);
-    if (rc == SB200_OK) rc = issue_rt_step(c, B, A, W, z.data(), n_hamil, trans_longi, dt);
+    if (rc == SB200_OK) rc = issue_rt_step(c, A2, B2, W, z.data(), n_hamil, trans_longi, dt);
     cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
     if (rc != SB200_OK) {
       if (graph) cudaGraphDestroy(graph);
@@ -1173,7 +1217,7 @@ int sb200_rt_propagate(sb200_ctx* c, double* psi_a, double* psi_b, double* work,
   double2* final_buf = A;
   if (nt % 2 == 1) {
     TRY(issue_rt_step(c, A, B, W, z.data(), n_hamil, trans_longi, dt));
-    final_buf = B;
+    final_buf = c->aetrs ? A : B;
   }
   if (curr_out && nt > 0)
     SB_CUDA(cudaMemcpyAsync(curr_out, r.d_curr, 3 * (size_t)nt * sizeof(double), cudaMemcpyDefault, c->stream));

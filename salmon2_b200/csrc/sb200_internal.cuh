@@ -203,6 +203,10 @@ struct sb200_ctx {
   size_t vloc_base_cap = 0;
   double* d_eext = nullptr;       // (3, 0:nt+1)
   size_t eext_cap = 0;
+  // propagator = 'aetrs' (sb200_set_propagator): the two stored potentials
+  int aetrs = 0;
+  double* d_vloc_old = nullptr;  // [2][nspin][npts]
+  size_t vloc_old_cap = 0;
   // absorbing boundary along z (sb200_set_absorbing_boundary): w(z) per plane
   int cap_on = 0;
   double* d_cap = nullptr;  // [nz]
@@ -294,6 +298,8 @@ int launch_density(sb200_ctx* c, const double2* psi, double* rho, int kind = -1)
 // and the field-free V_local back from V_base after the loop
 int launch_vbox(sb200_ctx* c, int kind = -1);
 int launch_vloc_restore(sb200_ctx* c);
+// AETRS: the extrapolated V_local between the half steps
+int launch_aetrs_vloc(sb200_ctx* c);
 int density_prepare(sb200_ctx* c);
 // microscopic current [npts][3] into curr (device); part: micro_current_part_len(c) doubles
 size_t micro_current_part_len(const sb200_ctx* c);

@@ -18,7 +18,8 @@ struct PrepArgs {
   int itt;                      // < 0: read *step
   double coef_lap0, coef_nab[12];
   const double* vec_k;          // [nk][3]
-  const double* A;              // a_mode 0: A[3]; else Ac_tot(3, 0:nt+1)
+  const double* A;              // a_mode 0: A[3]; 1, 2: Ac_tot(3, 0:nt+1); 3: Ac_ext
+  const double* A2;             // a_mode 3: Ac_ind(3, 0:nt+1)
   const int* step;
   const double* pt_r;           // [totpts][3]
   double* kcoef;                // [nk][KC]
@@ -42,7 +43,9 @@ __global__ void k_prep(PrepArgs a) {
   for (int d = 0; d < 3; ++d) {
     if (a.a_mode == 0) A[d] = a.A[d];
     else if (a.a_mode == 1) A[d] = 0.5 * (a.A[3 * itt + d] + a.A[3 * (itt - 1) + d]);
-    else A[d] = a.A[3 * itt + d];
+    else if (a.a_mode == 2) A[d] = a.A[3 * itt + d];
+    else  // the AETRS prediction of A(itt+1), time_evolution_step.f90:466-470
+      A[d] = a.A[3 * (itt + 1) + d] + 2.0 * a.A2[3 * itt + d] - a.A2[3 * (itt - 1) + d];
   }
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < items; i += (long)gridDim.x * blockDim.x) {
     const int k = (int)(i / per);
@@ -524,6 +527,7 @@ int launch_prep_k(sb200_ctx* c, const double* d_A, int a_mode, int itt, double* 
   for (int i = 0; i < 12; ++i) a.coef_nab[i] = c->g.coef_nab[i];
   a.vec_k = c->d_vec_k;
   a.A = d_A;
+  a.A2 = c->rt.d_Ac_ind;
   a.step = c->rt.d_step;
   a.pt_r = c->pp.d_pt_r;
   a.kcoef = d_kcoef;
@@ -1002,6 +1006,53 @@ int launch_vbox(sb200_ctx* c, int kind) {
                                               c->g.hgs[2]);
   SB_LAUNCH_CHECK("k_vbox");
   if (kind >= 0 && kernel_timing_mark(c, kind, false)) return SB200_ERR_CUDA;
+  return SB200_OK;
+}
+
+// AETRS between the half steps (time_evolution_half_step_etrs,
+// time_evolution_step.f90:430-463): V_new = 3 V - 3 V_old1 + V_old2, V_old2 =
+// V_old1, V_old1 = V, V = V_new, plus Vbox(itt+1) in the length gauge
+__global__ void k_aetrs_vloc(double* __restrict__ v, float* __restrict__ v32, double* __restrict__ old1,
+                             double* __restrict__ old2, const double* __restrict__ eext,
+                             const int* __restrict__ step, long n, int nspin, int nx, int ny, double o0, double o1,
+                             double o2, double h0, double h1, double h2) {
+  double e0 = 0.0, e1 = 0.0, e2 = 0.0;
+  if (eext) {
+    const int itt = *step + 1;
+    e0 = eext[3 * itt];
+    e1 = eext[3 * itt + 1];
+    e2 = eext[3 * itt + 2];
+  }
+  const long tot = n * nspin;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < tot; i += (long)gridDim.x * blockDim.x) {
+    const double vc = v[i];
+    double vn = 3.0 * vc - 3.0 * old1[i] + old2[i];
+    old2[i] = old1[i];
+    old1[i] = vc;
+    if (eext) {
+      const long p = i % n;
+      const int x = (int)(p % nx), y = (int)((p / nx) % ny), z = (int)(p / ((long)nx * ny));
+      vn = vn + (0.0 + (e0 * ((o0 + x) * h0) + e1 * ((o1 + y) * h1) + e2 * ((o2 + z) * h2)));
+    }
+    v[i] = vn;
+    v32[i] = (float)vn;
+  }
+}
+
+int launch_aetrs_vloc(sb200_ctx* c) {
+  const long n = c->g.npts;
+  const int nspin = c->orb.nspin;
+  double o[3];
+  for (int d = 0; d < 3; ++d) o[d] = (double)c->g.is[d] - ((c->g.lg_num[d] % 2 == 1) ? 0.0 : 0.5);
+  long nb = (n * nspin + 255) / 256;
+  if (nb > 148L * 8) nb = 148L * 8;
+  double* old1 = c->d_vloc_old;
+  double* old2 = c->d_vloc_old + (size_t)n * nspin;
+  k_aetrs_vloc<<<(unsigned)nb, 256, 0, c->stream>>>(c->d_vloc, c->d_vloc32, old1, old2,
+                                                    c->lg_active ? c->d_eext : nullptr, c->rt.d_step, n, nspin,
+                                                    c->g.nx, c->g.ny, o[0], o[1], o[2], c->g.hgs[0], c->g.hgs[1],
+                                                    c->g.hgs[2]);
+  SB_LAUNCH_CHECK("k_aetrs_vloc");
   return SB200_OK;
 }
 

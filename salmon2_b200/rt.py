@@ -104,6 +104,11 @@ class Context:
         check(lib().sb200_set_micro_ac(self.h, C.c_void_p(a.ctypes.data),
                                        None if d is None else C.c_void_p(d.ctypes.data)))
 
+    def set_propagator(self, name="middlepoint"):
+        """propagator = 'middlepoint' or 'aetrs' (rt_propagate then takes the zc of
+        the half step, synth.taylor_zc(dt, aetrs=True))."""
+        check(lib().sb200_set_propagator(self.h, {"middlepoint": 0, "aetrs": 1}[name]))
+
     def set_length_gauge(self, on=True):
         """An isolated system driven by a pulse in the length gauge (ae_shape1 /=
         'impulse'): rt_propagate adds E_ext(itt).r to V_local every step."""

@@ -439,3 +439,18 @@ def test_length_gauge_with_a_constant_field_is_a_static_potential():
         b = Oracle(s2).rt_run(s.psi, nt, dt, zc)
         assert np.max(np.abs(a["psi"] - b["psi"])) <= 1e-12 * np.max(np.abs(b["psi"]))
         assert np.max(np.abs(a["rbox"] - b["rbox"])) <= 1e-12 * np.max(np.abs(b["rbox"]))
+
+
+def test_aetrs_step_with_a_static_hamiltonian_is_two_half_steps():
+    """propagator = 'aetrs': with no field and a fixed potential the
+    extrapolated V equals V and A(itt+1) equals A(itt), so a step is two
+    applications of the half-step Taylor series (zc of -i dt/2)."""
+    from salmon2_b200 import synth
+    s = S.isolated_small()
+    dt = 0.05
+    zh = synth.taylor_zc(dt, aetrs=True)
+    O = Oracle(s)
+    want = O.taylor(O.taylor(s.psi, zh), zh)
+    O.set_propagator("aetrs")
+    got = O.rt_run(s.psi, 1, dt, zh)["psi"]
+    assert np.max(np.abs(got - want)) <= 1e-13 * np.max(np.abs(want))

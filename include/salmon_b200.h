@@ -204,6 +204,17 @@ int sb200_set_lattice(sb200_ctx* ctx, const double rmatrix_B[9], const double co
  * (src/common/stencil.f90:295-315, src/common/zstencil_microac_core/typical/seq.f90). */
 int sb200_set_micro_ac(sb200_ctx* ctx, const double* Ac_micro, const double* div_Ac);
 
+/* yn_predictor_corrector (1 = 'y', 0 = 'n', the default; the middle-point
+ * propagator): every step of sb200_rt_propagate first propagates a copy of the
+ * orbitals, takes the potential of the predicted density (with
+ * sb200_set_self_consistent: Hartree from the current Vh, exchange-
+ * correlation, update_vlocal; with a fixed potential the loop's initial
+ * V_local), sets V_local = (V_step + V_predicted) / 2 and then propagates the
+ * orbitals with it.
+ * Replaces: predictor_corrector (src/rt/time_evolution_step.f90:139-143,
+ * 374-428).                                                                    */
+int sb200_set_predictor_corrector(sb200_ctx* ctx, int yn);
+
 /* propagator (0 = 'middlepoint', the default; 1 = 'aetrs'): with AETRS every
  * step of sb200_rt_propagate is two half steps with the zc the caller passes
  * (those of -i dt/2): the first with A(itt) and V_local, then V_local

@@ -975,6 +975,17 @@ static int rt_run_impl(sbo_system* s, double* psi_a, double* psi_b, double* work
         cx[d].push_back(s->lg_num[d] % 2 == 1 ? i * s->hgs[d] : (i - 0.5) * s->hgs[d]);
   // AETRS: the stored potentials, vloc_old(:,1:2) = V_local (initialization_rt.f90:287-292)
   const long nv = npts * s->nspin;
+  // predictor_corrector (time_evolution_step.f90:374-428): the loop's initial
+  // potential (update_vlocal of a fixed potential), V_tmp, psi_tmp
+  const bool pc = s->pred_corr && !s->aetrs;
+  std::vector<double> pc_v0, pc_v, pc_psi, pc_vnew, pc_rho(pc && s->nspin == 2 ? npts : 0);
+  if (pc) {
+    Idx I(s);
+    pc_v0.assign(s->V_local, s->V_local + nv);
+    pc_v.resize(nv);
+    pc_vnew.resize(nv);
+    pc_psi.resize(2 * I.vol * I.norb());
+  }
   std::vector<double> old1, old2, vuse;
   if (s->aetrs) {
     old1.assign(s->V_local, s->V_local + nv);
@@ -999,6 +1010,40 @@ static int rt_run_impl(sbo_system* s, double* psi_a, double* psi_b, double* work
       for (int d = 0; d < 3; ++d)
         s->vec_Ac[d] = s->aetrs ? Ac_tot[3 * itt + d] : 0.5 * (Ac_tot[3 * itt + d] + Ac_tot[3 * (itt - 1) + d]);
       if (s->nlma > 0) sbo_update_kvector_nonlocalpt(s);
+    }
+    if (pc) {
+      const double* Vt = s->V_local;  // V_tmp
+      std::copy(in, in + pc_psi.size(), pc_psi.begin());
+      sbo_taylor(s, in, out, work, zc, n_hamil);
+      sbo_calc_density(s, out, rho_work);
+      const double* Vn = pc_v0.data();
+      if (scf) {
+        const int num[3] = {s->ie[0] - s->is[0] + 1, s->ie[1] - s->is[1] + 1, s->ie[2] - s->is[2] + 1};
+        const double* rho_h = rho_work;
+        if (s->nspin == 2) {
+          for (long i = 0; i < npts; ++i) pc_rho[i] = (0.0 + rho_work[i]) + rho_work[npts + i];
+          rho_h = pc_rho.data();
+        }
+        double exc = 0.0;
+        if (s->periodic) {
+          sbo_poisson_ft(num, scf->brl, rho_h, vh.data());
+        } else if (cg) {  // hartree from the current Vh (no extrapolation here)
+          int it = 0;
+          sbo_poisson_isolated_cg(s, rho_h, vh.data(), cg->layout, cg->lmax, cg->rion, cg->natom, cg->npole,
+                                  cg->threshold, cg->maxiter, &it);
+        } else {
+          sbo_poisson_isolated_ft(num, scf->brl, rho_h, vh.data());
+        }
+        if (s->nspin == 2)
+          sbo_exc_cor_pz_sp(npts, rho_work, s->hvol, vxc.data(), &exc);
+        else
+          sbo_exc_cor_pz(npts, rho_work, s->hvol, vxc.data(), &exc);
+        sbo_update_vlocal(npts, s->nspin, scf->vpsl, vh.data(), vxc.data(), pc_vnew.data());
+        Vn = pc_vnew.data();
+      }
+      for (long i = 0; i < nv; ++i) pc_v[i] = 0.5 * (Vt[i] + Vn[i]);
+      std::copy(pc_psi.begin(), pc_psi.end(), in);
+      s->V_local = pc_v.data();
     }
     sbo_taylor(s, in, out, work, zc, n_hamil);
     if (s->aetrs) {  // time_evolution_half_step_etrs, time_evolution_step.f90:430-470

@@ -90,6 +90,8 @@ typedef struct {
   /* propagator = 'aetrs' (time_evolution_step.f90:117-147, 430-470): half
    * steps (zc of -i dt/2) around the extrapolated potential                  */
   int aetrs;
+  /* yn_predictor_corrector = 'y' (time_evolution_step.f90:374-428)           */
+  int pred_corr;
 } sbo_system;
 
 void sbo_set_threads(int n);

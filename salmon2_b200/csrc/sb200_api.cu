@@ -308,12 +308,20 @@ int issue_rt_step(sb200_ctx* c, double2* in, double2* out, double2* work, const 
     return scf_rt_issue(c, in);
   }
   if (c->g.periodic) TIMED(c, SB200_KIND_PREP, launch_prep_k(c, c->rt.d_Ac_tot, 1, -1, c->d_kcoef, true));
+  if (c->lg_active) TRY(launch_vbox(c, c->timing ? SB200_KIND_POTENTIAL : -1));
+  if (c->pred_corr) {  // predictor_corrector, time_evolution_step.f90:139-143, 374-428
+    const size_t nv = (size_t)c->g.npts * c->orb.nspin, nb = (size_t)c->g.npts * c->orb.norb;
+    SB_CUDA(cudaMemcpyAsync(c->d_pc_v, c->d_vloc, nv * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+    SB_CUDA(cudaMemcpyAsync(c->d_pc_psi, in, nb * sizeof(double2), cudaMemcpyDeviceToDevice, c->stream));
+    TRY(issue_taylor(c, in, out, work, zc, n_hamil));
+    TRY(scf_pc_potential(c, out, c->d_pc_v, c->d_pc_v + nv));
+    SB_CUDA(cudaMemcpyAsync(in, c->d_pc_psi, nb * sizeof(double2), cudaMemcpyDeviceToDevice, c->stream));
+  }
   if (orbital_kernel_applies(c)) {  // observables fused into the last Taylor term
     TRY(issue_taylor(c, in, out, work, zc, n_hamil, true));
     TIMED(c, SB200_KIND_FINAL, launch_finalize(c, -1, 0, trans_longi, dt, -1, true));
     return scf_rt_issue(c, out);
   }
-  if (c->lg_active) TRY(launch_vbox(c, c->timing ? SB200_KIND_POTENTIAL : -1));
   TRY(issue_taylor(c, in, out, work, zc, n_hamil));
   TIMED(c, SB200_KIND_OBS, launch_observables(c, out));
   if (c->g.periodic) TIMED(c, SB200_KIND_MOMENTS, launch_project_moments(c, out));
@@ -416,6 +424,8 @@ int sb200_ctx_destroy(sb200_ctx* c) {
   dfree(c->d_vloc_base);
   dfree(c->d_eext);
   dfree(c->d_vloc_old);
+  dfree(c->d_pc_psi);
+  dfree(c->d_pc_v);
   for (cudaEvent_t e : c->ev) cudaEventDestroy(e);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
   delete c;
@@ -835,6 +845,13 @@ int sb200_set_micro_ac(sb200_ctx* c, const double* Ac_micro, const double* div_A
   return SB200_OK;
 }
 
+int sb200_set_predictor_corrector(sb200_ctx* c, int yn) {
+  CHECK_CTX(c);
+  if (yn != 0 && yn != 1) return set_error(SB200_ERR_INVALID_ARG, "yn_predictor_corrector is 0 or 1");
+  c->pred_corr = yn;
+  return SB200_OK;
+}
+
 int sb200_set_propagator(sb200_ctx* c, int aetrs) {
   CHECK_CTX(c);
   if (aetrs != 0 && aetrs != 1) return set_error(SB200_ERR_INVALID_ARG, "propagator: 0 = middlepoint, 1 = aetrs");
@@ -1163,6 +1180,22 @@ int sb200_rt_propagate(sb200_ctx* c, double* psi_a, double* psi_b, double* work,
     SB_CUDA(cudaMemcpyAsync(c->d_eext, e.data(), na * sizeof(double), cudaMemcpyHostToDevice, c->stream));
     SB_CUDA(cudaMemcpyAsync(c->d_vloc_base, c->d_vloc, nv * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
     c->lg_active = 1;
+  }
+  if (c->pred_corr && !c->aetrs) {  // the step's saved input, V_tmp and the initial V0
+    const size_t nv = (size_t)c->g.npts * c->orb.nspin, nb = (size_t)c->g.npts * c->orb.norb;
+    if (c->pc_psi_cap < nb) {
+      dfree(c->d_pc_psi);
+      c->pc_psi_cap = 0;
+      TRY(dalloc(&c->d_pc_psi, nb));
+      c->pc_psi_cap = nb;
+    }
+    if (c->pc_v_cap < 2 * nv) {
+      dfree(c->d_pc_v);
+      c->pc_v_cap = 0;
+      TRY(dalloc(&c->d_pc_v, 2 * nv));
+      c->pc_v_cap = 2 * nv;
+    }
+    SB_CUDA(cudaMemcpyAsync(c->d_pc_v + nv, c->d_vloc, nv * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
   }
   if (c->aetrs) {  // vloc_old(:,1:2) = V_local (initialization_rt.f90:287-292)
     const size_t nv = (size_t)c->g.npts * c->orb.nspin;

@@ -203,6 +203,14 @@ struct sb200_ctx {
   size_t vloc_base_cap = 0;
   double* d_eext = nullptr;       // (3, 0:nt+1)
   size_t eext_cap = 0;
+  // yn_predictor_corrector = 'y' (sb200_set_predictor_corrector): the step's
+  // input orbitals and V_local kept across the predictor, and the loop's
+  // initial (field-free) V_local for a fixed potential
+  int pred_corr = 0;
+  double2* d_pc_psi = nullptr;  // [norb][npts]
+  size_t pc_psi_cap = 0;
+  double* d_pc_v = nullptr;     // [2][nspin][npts]: V_tmp, V0
+  size_t pc_v_cap = 0;
   // propagator = 'aetrs' (sb200_set_propagator): the two stored potentials
   int aetrs = 0;
   double* d_vloc_old = nullptr;  // [2][nspin][npts]
@@ -338,6 +346,9 @@ int pcg_vh_stock(sb200_ctx* c, const int* d_step, int offset, double* d_vh, doub
 // sb200_set_self_consistent enabled it)
 int scf_rt_prepare(sb200_ctx* c);
 int scf_rt_issue(sb200_ctx* c, const double2* psi);
+// predictor_corrector (time_evolution_step.f90:374-428): V_local = (V_tmp + V_new) / 2
+// with V_new the potential of the predicted orbitals psi (self-consistent) or v0
+int scf_pc_potential(sb200_ctx* c, const double2* psi, const double* vtmp, const double* v0);
 // initialization_rt.f90:268-283 with yn_restart = 'y' (isolated, CG): Vh from the
 // stored potentials, the Hartree solve of psi's density, stock update, V_local
 int scf_restart_potential(sb200_ctx* c, const double2* psi);

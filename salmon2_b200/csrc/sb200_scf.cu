@@ -309,6 +309,22 @@ __global__ void __launch_bounds__(SCF_THREADS) k_exc_pz_sp(const double* __restr
   if (threadIdx.x == 0) part[blockIdx.x] = red[0];
 }
 
+// predictor_corrector's V_local = 0.5 (V_tmp + V_new), V_new = Vpsl + Vh + Vxc(is)
+// (update_vlocal) or the fixed v0
+__global__ void k_pc_vloc(const double* __restrict__ vtmp, const double* __restrict__ vpsl,
+                          const double* __restrict__ vh, const double* __restrict__ vxc,
+                          const double* __restrict__ v0, double* __restrict__ v, float* __restrict__ v32, long n,
+                          int nspin) {
+  const long tot = n * nspin;
+  for (long i = blockIdx.x * (long)SCF_THREADS + threadIdx.x; i < tot; i += (long)gridDim.x * SCF_THREADS) {
+    const long p = i % n;
+    const double vn = v0 ? v0[i] : vpsl[p] + vh[p] + vxc[i];
+    const double val = 0.5 * (vtmp[i] + vn);
+    v[i] = val;
+    v32[i] = (float)val;
+  }
+}
+
 // rho = rho_up + rho_dn (time_evolution_step.f90:160-170: rho%f summed over spins)
 __global__ void k_rho_total(const double* __restrict__ rho_s, double* __restrict__ rho, long n) {
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
@@ -725,6 +741,40 @@ int scf_rt_issue(sb200_ctx* c, const double2* psi) {
   TRY_S(scf_launch_xc(c, s->d_rho, s->d_vxc, SB200_KIND_POTENTIAL, false));
   TRY_S(scf_launch_update(c, s->d_vpsl, s->d_vh, s->d_vxc, SB200_KIND_POTENTIAL));
   SB_LAUNCH_CHECK("self-consistent potential update");
+  return SB200_OK;
+}
+
+// predictor_corrector (time_evolution_step.f90:374-428) after the predicted
+// Taylor step: the density of psi, with yn_fix_func = 'n' its Hartree (the
+// hartree call from the current Vh, no extrapolation) and exchange-correlation
+// potentials, update_vlocal, then V_local = (V_tmp + V_local) / 2; with a
+// fixed potential update_vlocal gives v0
+int scf_pc_potential(sb200_ctx* c, const double2* psi, const double* vtmp, const double* v0) {
+  ScfState* s = scf_of(c);
+  const long n = c->g.npts;
+  const int nspin = c->orb.nspin;
+  const bool scf = s && s->rt_on;
+  if (scf) {
+    TRY_S(launch_density(c, psi, s->d_rho, SB200_KIND_POTENTIAL));
+    TRY_S(scf_density_allreduce(c, s->d_rho));
+    const double* rho_h = scf_total_density(c, SB200_KIND_POTENTIAL);
+    if (c->g.periodic) {
+      TRY_S(scf_launch_hartree(c, rho_h, s->d_vh, SB200_KIND_POTENTIAL));
+    } else if (s->cg_on) {
+      TRY_S(scf_mark(c, SB200_KIND_POTENTIAL, true));
+      TRY_S(pcg_issue(c, rho_h, s->d_vh, nullptr));
+      TRY_S(scf_mark(c, SB200_KIND_POTENTIAL, false));
+    } else {
+      TRY_S(scf_launch_hartree_isolated(c, rho_h, s->d_vh, SB200_KIND_POTENTIAL));
+    }
+    TRY_S(scf_launch_xc(c, s->d_rho, s->d_vxc, SB200_KIND_POTENTIAL, false));
+  }
+  TRY_S(scf_mark(c, SB200_KIND_POTENTIAL, true));
+  k_pc_vloc<<<scf_grid_blocks(n * nspin), SCF_THREADS, 0, c->stream>>>(
+      vtmp, scf ? s->d_vpsl : nullptr, scf ? s->d_vh : nullptr, scf ? s->d_vxc : nullptr, scf ? nullptr : v0,
+      c->d_vloc, c->d_vloc32, n, nspin);
+  TRY_S(scf_mark(c, SB200_KIND_POTENTIAL, false));
+  SB_LAUNCH_CHECK("k_pc_vloc");
   return SB200_OK;
 }
 

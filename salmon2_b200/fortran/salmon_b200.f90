@@ -184,6 +184,12 @@ module salmon_b200
       real(c_double), intent(in) :: Ac_micro(3, *), div_Ac(*)
     end function
 
+    integer(c_int) function sb200_set_predictor_corrector(ctx, yn) bind(c, name="sb200_set_predictor_corrector")
+      import
+      type(c_ptr), value :: ctx
+      integer(c_int), value :: yn
+    end function
+
     integer(c_int) function sb200_set_propagator(ctx, aetrs) bind(c, name="sb200_set_propagator")
       import
       type(c_ptr), value :: ctx

@@ -104,6 +104,10 @@ class Context:
         check(lib().sb200_set_micro_ac(self.h, C.c_void_p(a.ctypes.data),
                                        None if d is None else C.c_void_p(d.ctypes.data)))
 
+    def set_predictor_corrector(self, on=True):
+        """yn_predictor_corrector = 'y' (time_evolution_step's predictor_corrector)."""
+        check(lib().sb200_set_predictor_corrector(self.h, 1 if on else 0))
+
     def set_propagator(self, name="middlepoint"):
         """propagator = 'middlepoint' or 'aetrs' (rt_propagate then takes the zc of
         the half step, synth.taylor_zc(dt, aetrs=True))."""

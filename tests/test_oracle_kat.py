@@ -454,3 +454,26 @@ def test_aetrs_step_with_a_static_hamiltonian_is_two_half_steps():
     O.set_propagator("aetrs")
     got = O.rt_run(s.psi, 1, dt, zh)["psi"]
     assert np.max(np.abs(got - want)) <= 1e-13 * np.max(np.abs(want))
+
+
+def test_predictor_corrector_averages_the_potentials():
+    """predictor_corrector with a fixed potential: V = (V_tmp + V0) / 2.  Without
+    a field V_tmp = V0 and the loop is the plain one exactly; in the length
+    gauge V_tmp = V0 + E.r, so the loop is the length-gauge loop of half the
+    field."""
+    from salmon2_b200 import synth
+    s = S.isolated_small()
+    nt, dt = 3, 0.05
+    zc = synth.taylor_zc(dt)
+    O1, O2 = Oracle(s), Oracle(s)
+    O2.set_predictor_corrector(True)
+    a, b = O1.rt_run(s.psi, nt, dt, zc), O2.rt_run(s.psi, nt, dt, zc)
+    assert np.array_equal(a["psi"], b["psi"]) and np.array_equal(a["rbox"], b["rbox"])
+    Ac = synth.asin2cos(nt, dt, omega=0.2, f0=0.05, tw=nt * dt, epdir=(0.3, -0.2, 0.93))
+    O3, O4 = Oracle(s), Oracle(s)
+    O3.set_length_gauge(True)
+    O3.set_predictor_corrector(True)
+    O4.set_length_gauge(True)
+    c = O3.rt_run(s.psi, nt, dt, zc, Ac_ext=Ac)
+    d = O4.rt_run(s.psi, nt, dt, zc, Ac_ext=np.asfortranarray(0.5 * Ac))
+    assert np.max(np.abs(c["psi"] - d["psi"])) <= 1e-12 * np.max(np.abs(d["psi"]))

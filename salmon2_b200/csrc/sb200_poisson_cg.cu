@@ -33,6 +33,7 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <cstdlib>
 #include <string>
 #include <vector>
 
@@ -47,7 +48,9 @@ constexpr int MCH = 2048;      // points per block of the pole sums
 constexpr int NLM_MAX = 25;    // lmax <= 4
 constexpr int POLE_W = 32;     // doubles per pole entry: centre (3), itrho, rholm (25)
 constexpr int PCG_CHUNK = 16;  // iterations between host checks of the convergence flag
-constexpr int PCG_UNROLL = 2;  // iterations per body of the conditional node
+// default iterations per body of the conditional node (SB200_PCG_UNROLL: 1..16;
+// on the 64^3 isolated self-consistent loop 8 runs 3 % faster than 2, 16 no faster)
+constexpr int PCG_UNROLL = 8;
 constexpr double PCG_PI = 3.141592653589793;
 
 // scalars of the iteration (device)
@@ -491,6 +494,7 @@ struct PcgState {
   PArgs base{};               // the configured solve (rho, vh set per call)
   bool configured = false;
   cudaStream_t side = nullptr;  // captures the body of the conditional node
+  int unroll = PCG_UNROLL;      // CG iterations per body of the conditional node
 };
 
 PcgState* pcg_of(sb200_ctx* c) { return static_cast<PcgState*>(c->pcg); }
@@ -621,6 +625,10 @@ int pcg_configure(sb200_ctx* c, int layout, int lmax, const double* rion, int na
   PcgState* s = pcg_of(c);
   if (!s) {
     s = new PcgState();
+    if (const char* v = std::getenv("SB200_PCG_UNROLL")) {
+      const int u = std::atoi(v);
+      if (u >= 1 && u <= 16) s->unroll = u;
+    }
     c->pcg = s;
     SB_CUDA(cudaMallocHost((void**)&s->host_sc, 8 * sizeof(double)));
     SB_CUDA(cudaStreamCreateWithFlags(&s->side, cudaStreamNonBlocking));
@@ -729,7 +737,7 @@ int pcg_issue(sb200_ctx* c, const double* d_rho, double* d_vh, int* iterations) 
     cudaGraph_t body = cp.conditional.phGraph_out[0];
     SB_CUDA(cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies));
     SB_CUDA(cudaStreamBeginCaptureToGraph(s->side, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
-    for (int u = 0; u < PCG_UNROLL; ++u) {
+    for (int u = 0; u < s->unroll; ++u) {
       k_pcg_direction<<<gb, PT, 0, s->side>>>(a);
       k_pcg_update<<<gb, PT, 0, s->side>>>(a, h, 1);
     }

@@ -204,6 +204,15 @@ int sb200_set_lattice(sb200_ctx* ctx, const double rmatrix_B[9], const double co
  * (src/common/stencil.f90:295-315, src/common/zstencil_microac_core/typical/seq.f90). */
 int sb200_set_micro_ac(sb200_ctx* ctx, const double* Ac_micro, const double* div_Ac);
 
+/* gram_schmidt_interval (the reference's default -1: never; values below 1
+ * leave the loop without it): with N >= 1 every step of sb200_rt_propagate
+ * whose global step itt is a multiple of N orthonormalises psi(t+dt)
+ * (sb200_gram_schmidt_complex) before its density and current, inside the
+ * loop's CUDA graph as a conditional node.
+ * Replaces: the gram_schmidt call of time_evolution_step
+ * (src/rt/time_evolution_step.f90:149-152).                                   */
+int sb200_set_gram_schmidt_interval(sb200_ctx* ctx, int gram_schmidt_interval);
+
 /* yn_predictor_corrector (1 = 'y', 0 = 'n', the default; the middle-point
  * propagator): every step of sb200_rt_propagate first propagates a copy of the
  * orbitals, takes the potential of the predicted density (with

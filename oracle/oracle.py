@@ -39,7 +39,7 @@ class SboSystem(C.Structure):
         ("ac_micro", _dp), ("div_ac", _dp),
         ("symmetrized", C.c_int),
         ("cap_on", C.c_int), ("cap_w0", C.c_double), ("cap_dr", C.c_double), ("cap_al", C.c_double),
-        ("length_gauge", C.c_int), ("aetrs", C.c_int), ("pred_corr", C.c_int),
+        ("length_gauge", C.c_int), ("aetrs", C.c_int), ("pred_corr", C.c_int), ("gs_interval", C.c_int),
     ]
 
 
@@ -261,6 +261,9 @@ class Oracle:
         cur = np.zeros((3, self.sys.nspin), order="F")
         lib().sbo_calc_current(C.byref(self.s), _p(a), _p(cur))
         return cur
+
+    def set_gram_schmidt_interval(self, n):
+        self.s.gs_interval = int(n)
 
     def set_predictor_corrector(self, on=True):
         """yn_predictor_corrector = 'y' (time_evolution_step's predictor_corrector)."""

@@ -1076,6 +1076,8 @@ static int rt_run_impl(sbo_system* s, double* psi_a, double* psi_b, double* work
       sbo_taylor(s, in, out, work, zc, n_hamil);
     }
     s->V_local = v_base;  // the step's update_vlocal: the field-free potential again
+    if (s->gs_interval >= 1 && itt % s->gs_interval == 0)  // time_evolution_step.f90:149-152
+      sbo_gram_schmidt_complex(s, out);
     sbo_calc_density(s, out, rho_work);
     if (scf) {
       const int num[3] = {s->ie[0] - s->is[0] + 1, s->ie[1] - s->is[1] + 1, s->ie[2] - s->is[2] + 1};

@@ -92,6 +92,9 @@ typedef struct {
   int aetrs;
   /* yn_predictor_corrector = 'y' (time_evolution_step.f90:374-428)           */
   int pred_corr;
+  /* gram_schmidt_interval >= 1: gram_schmidt of psi(t+dt) every N steps
+   * (time_evolution_step.f90:149-152)                                        */
+  int gs_interval;
 } sbo_system;
 
 void sbo_set_threads(int n);

@@ -72,6 +72,7 @@ SIGNATURES = {
     "sb200_set_length_gauge": (C.c_int, [_vp, C.c_int]),
     "sb200_set_propagator": (C.c_int, [_vp, C.c_int]),
     "sb200_set_predictor_corrector": (C.c_int, [_vp, C.c_int]),
+    "sb200_set_gram_schmidt_interval": (C.c_int, [_vp, C.c_int]),
     "sb200_calc_microscopic_current": (C.c_int, [_vp, _vp, _vp]),
     "sb200_init_ps_ky": (C.c_int, [C.c_int, C.POINTER(C.c_char_p), _ip, _ip, C.c_int, _ip, _ip, _dp, C.c_double,
                                    C.c_int, _ip, _dp, _ip, _ip, _ip, _ip, _dp, _dp, _ip, _dp, _dp]),

@@ -283,6 +283,57 @@ int issue_taylor(sb200_ctx* c, double2* tin, double2* tout, double2* work, const
   return SB200_OK;
 }
 
+// the condition of the Gram-Schmidt node: mod(itt, interval) == 0 with the
+// global step itt (time_evolution_step.f90:149-152)
+__global__ void k_gs_condition(cudaGraphConditionalHandle h, const int* step, int offset, int interval) {
+  const int itt = *step + offset;
+  cudaGraphSetConditional(h, (itt % interval == 0) ? 1u : 0u);
+}
+
+// gram_schmidt every gs_interval steps, on psi (the step's result, before its
+// density and current): a conditional IF node inside a capture, a host check of
+// the step counter otherwise
+int issue_rt_gram_schmidt(sb200_ctx* c, double2* psi) {
+  double2* part = c->d_gs_scratch;
+  double2* coeff = c->d_gs_scratch + gs_complex_part_len(c);
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  cudaGraph_t g = nullptr;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t nd = 0;
+  SB_CUDA(cudaStreamGetCaptureInfo(c->stream, &cs, nullptr, &g, &deps, &nd));
+  if (cs != cudaStreamCaptureStatusActive) {
+    int step = 0;
+    SB_CUDA(cudaMemcpyAsync(&step, c->rt.d_step, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    SB_CUDA(cudaStreamSynchronize(c->stream));
+    if ((step + c->rt.loop_mit0) % c->gs_interval != 0) return SB200_OK;
+    return gs_complex_issue(c, psi, part, coeff);
+  }
+  cudaGraphConditionalHandle h;
+  SB_CUDA(cudaGraphConditionalHandleCreate(&h, g, 0u, cudaGraphCondAssignDefault));
+  k_gs_condition<<<1, 1, 0, c->stream>>>(h, c->rt.d_step, c->rt.loop_mit0, c->gs_interval);
+  SB_CUDA(cudaGetLastError());
+  SB_CUDA(cudaStreamGetCaptureInfo(c->stream, &cs, nullptr, &g, &deps, &nd));
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = h;
+  cp.conditional.type = cudaGraphCondTypeIf;
+  cp.conditional.size = 1;
+  cudaGraphNode_t node;
+  SB_CUDA(cudaGraphAddNode(&node, g, deps, nd, &cp));
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
+  SB_CUDA(cudaStreamUpdateCaptureDependencies(c->stream, &node, 1, cudaStreamSetCaptureDependencies));
+  SB_CUDA(cudaStreamBeginCaptureToGraph(c->gs_side, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+  cudaStream_t keep = c->stream;
+  c->stream = c->gs_side;  // the launch sequence issues on c->stream
+  const int r = gs_complex_issue(c, psi, part, coeff);
+  c->stream = keep;
+  cudaGraph_t captured = nullptr;
+  const cudaError_t ee = cudaStreamEndCapture(c->gs_side, &captured);
+  if (r != SB200_OK) return r;
+  if (ee != cudaSuccess) return cuda_error(ee, "cudaStreamEndCapture (Gram-Schmidt body)");
+  return SB200_OK;
+}
+
 // one time_evolution_step on the device (itt from the device counter); with
 // AETRS the step's result is back in `in` (out is the half step's scratch)
 int issue_rt_step(sb200_ctx* c, double2* in, double2* out, double2* work, const double2* zc, int n_hamil,
@@ -296,12 +347,13 @@ int issue_rt_step(sb200_ctx* c, double2* in, double2* out, double2* work, const 
     TRY(issue_taylor(c, in, out, work, zc, n_hamil));
     TIMED(c, SB200_KIND_POTENTIAL, launch_aetrs_vloc(c));
     if (c->g.periodic) TIMED(c, SB200_KIND_PREP, launch_prep_k(c, c->rt.d_Ac_ext, 3, -1, c->d_kcoef, true));
-    if (orbital_kernel_applies(c)) {
+    if (orbital_kernel_applies(c) && c->gs_interval < 1) {
       TRY(issue_taylor(c, out, in, work, zc, n_hamil, true));
       TIMED(c, SB200_KIND_FINAL, launch_finalize(c, -1, 0, trans_longi, dt, -1, true));
       return scf_rt_issue(c, in);
     }
     TRY(issue_taylor(c, out, in, work, zc, n_hamil));
+    if (c->gs_interval >= 1) TRY(issue_rt_gram_schmidt(c, in));
     TIMED(c, SB200_KIND_OBS, launch_observables(c, in));
     if (c->g.periodic) TIMED(c, SB200_KIND_MOMENTS, launch_project_moments(c, in));
     TIMED(c, SB200_KIND_FINAL, launch_finalize(c, -1, 0, trans_longi, dt, -1));
@@ -317,12 +369,13 @@ int issue_rt_step(sb200_ctx* c, double2* in, double2* out, double2* work, const 
     TRY(scf_pc_potential(c, out, c->d_pc_v, c->d_pc_v + nv));
     SB_CUDA(cudaMemcpyAsync(in, c->d_pc_psi, nb * sizeof(double2), cudaMemcpyDeviceToDevice, c->stream));
   }
-  if (orbital_kernel_applies(c)) {  // observables fused into the last Taylor term
+  if (orbital_kernel_applies(c) && c->gs_interval < 1) {  // observables fused into the last Taylor term
     TRY(issue_taylor(c, in, out, work, zc, n_hamil, true));
     TIMED(c, SB200_KIND_FINAL, launch_finalize(c, -1, 0, trans_longi, dt, -1, true));
     return scf_rt_issue(c, out);
   }
   TRY(issue_taylor(c, in, out, work, zc, n_hamil));
+  if (c->gs_interval >= 1) TRY(issue_rt_gram_schmidt(c, out));
   TIMED(c, SB200_KIND_OBS, launch_observables(c, out));
   if (c->g.periodic) TIMED(c, SB200_KIND_MOMENTS, launch_project_moments(c, out));
   TIMED(c, SB200_KIND_FINAL, launch_finalize(c, -1, 0, trans_longi, dt, -1));
@@ -426,6 +479,8 @@ int sb200_ctx_destroy(sb200_ctx* c) {
   dfree(c->d_vloc_old);
   dfree(c->d_pc_psi);
   dfree(c->d_pc_v);
+  dfree(c->d_gs_scratch);
+  if (c->gs_side) cudaStreamDestroy(c->gs_side);
   for (cudaEvent_t e : c->ev) cudaEventDestroy(e);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
   delete c;
@@ -845,6 +900,12 @@ int sb200_set_micro_ac(sb200_ctx* c, const double* Ac_micro, const double* div_A
   return SB200_OK;
 }
 
+int sb200_set_gram_schmidt_interval(sb200_ctx* c, int gram_schmidt_interval) {
+  CHECK_CTX(c);
+  c->gs_interval = gram_schmidt_interval;
+  return SB200_OK;
+}
+
 int sb200_set_predictor_corrector(sb200_ctx* c, int yn) {
   CHECK_CTX(c);
   if (yn != 0 && yn != 1) return set_error(SB200_ERR_INVALID_ARG, "yn_predictor_corrector is 0 or 1");
@@ -1180,6 +1241,16 @@ int sb200_rt_propagate(sb200_ctx* c, double* psi_a, double* psi_b, double* work,
     SB_CUDA(cudaMemcpyAsync(c->d_eext, e.data(), na * sizeof(double), cudaMemcpyHostToDevice, c->stream));
     SB_CUDA(cudaMemcpyAsync(c->d_vloc_base, c->d_vloc, nv * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
     c->lg_active = 1;
+  }
+  if (c->gs_interval >= 1) {  // the loop's Gram-Schmidt: scratch and body stream
+    const size_t need = gs_complex_part_len(c) + (size_t)c->orb.no;
+    if (c->gs_scratch_cap < need) {
+      dfree(c->d_gs_scratch);
+      c->gs_scratch_cap = 0;
+      TRY(dalloc(&c->d_gs_scratch, need));
+      c->gs_scratch_cap = need;
+    }
+    if (!c->gs_side) SB_CUDA(cudaStreamCreateWithFlags(&c->gs_side, cudaStreamNonBlocking));
   }
   if (c->pred_corr && !c->aetrs) {  // the step's saved input, V_tmp and the initial V0
     const size_t nv = (size_t)c->g.npts * c->orb.nspin, nb = (size_t)c->g.npts * c->orb.norb;

@@ -892,6 +892,45 @@ int sb200_gram_schmidt_real(sb200_ctx* c, double* psi) {
   return SB200_OK;
 }
 
+}  // extern "C"
+
+namespace sb200 {
+// scratch of gs_complex_issue: part [no][nb], coeff [no]
+size_t gs_complex_part_len(const sb200_ctx* c) {
+  const long nb = (c->g.npts + DOT_PTS - 1) / DOT_PTS;
+  return (size_t)c->orb.no * (size_t)nb;
+}
+
+// gram_schmidt_col_complex8's launches for every (k, spin) group, on the
+// context's stream, with caller-given scratch: no allocation, no host wait
+// (also issued inside the time loop's CUDA graph)
+int gs_complex_issue(sb200_ctx* c, double2* z, double2* part, double2* coeff) {
+  const int nspin = c->orb.nspin, no = c->orb.no, nk = c->orb.nk;
+  const long npts = c->g.npts;
+  const int nb = (int)((npts + DOT_PTS - 1) / DOT_PTS);
+  const long stride = (long)nspin * npts;
+  for (int ik = 0; ik < nk; ++ik)
+    for (int is = 0; is < nspin; ++is) {
+      double2* base = z + npts * ((long)is + (long)nspin * no * ik);
+      for (int io1 = 0; io1 < no; ++io1) {
+        double2* w1 = base + stride * io1;
+        if (io1 > 0) {
+          k_zgs_dots<<<dim3(nb, io1), RT, 0, c->stream>>>(base, stride, io1, npts, part, nb);
+          k_zgs_coeff<<<(io1 + 127) / 128, 128, 0, c->stream>>>(part, nb, io1, c->g.hvol, coeff);
+          k_zgs_sub<<<gridsz(npts), 256, 0, c->stream>>>(base, stride, io1, coeff, npts);
+        }
+        k_zsq_part<<<nb, RT, 0, c->stream>>>(w1, npts, (double*)part);
+        k_zscale_norm<<<gridsz(npts), 256, 0, c->stream>>>(w1, npts, (const double*)part, nb, c->g.hvol);
+      }
+      const cudaError_t e = cudaGetLastError();
+      if (e != cudaSuccess) return cuda_error(e, "complex Gram-Schmidt");
+    }
+  return SB200_OK;
+}
+}  // namespace sb200
+
+extern "C" {
+
 // gram_schmidt_col_complex8 (gram_schmidt_orth.f90:1069-1242) for every
 // (k, spin) group of the complex orbital block, orbitals in order.
 int sb200_gram_schmidt_complex(sb200_ctx* c, double* psi) {
@@ -906,24 +945,9 @@ int sb200_gram_schmidt_complex(sb200_ctx* c, double* psi) {
   double2* coeff = nullptr;
   TRY_GS(dalloc(&part, (size_t)no * nb));
   int r = dalloc(&coeff, (size_t)no);
-  double2* z = (double2*)psi;
-  const long stride = (long)nspin * npts;
-  for (int ik = 0; ik < nk && r == SB200_OK; ++ik)
-    for (int is = 0; is < nspin && r == SB200_OK; ++is) {
-      double2* base = z + npts * ((long)is + (long)nspin * no * ik);
-      for (int io1 = 0; io1 < no; ++io1) {
-        double2* w1 = base + stride * io1;
-        if (io1 > 0) {
-          k_zgs_dots<<<dim3(nb, io1), RT, 0, c->stream>>>(base, stride, io1, npts, part, nb);
-          k_zgs_coeff<<<(io1 + 127) / 128, 128, 0, c->stream>>>(part, nb, io1, c->g.hvol, coeff);
-          k_zgs_sub<<<gridsz(npts), 256, 0, c->stream>>>(base, stride, io1, coeff, npts);
-        }
-        k_zsq_part<<<nb, RT, 0, c->stream>>>(w1, npts, (double*)part);
-        k_zscale_norm<<<gridsz(npts), 256, 0, c->stream>>>(w1, npts, (const double*)part, nb, c->g.hvol);
-      }
-      const cudaError_t e = cudaGetLastError();
-      if (e != cudaSuccess) r = cuda_error(e, "complex Gram-Schmidt");
-    }
+  (void)nspin;
+  (void)nk;
+  if (r == SB200_OK) r = gs_complex_issue(c, (double2*)psi, part, coeff);
   if (r == SB200_OK) {
     const cudaError_t e = cudaStreamSynchronize(c->stream);
     if (e != cudaSuccess) r = cuda_error(e, "complex Gram-Schmidt");

@@ -203,6 +203,13 @@ struct sb200_ctx {
   size_t vloc_base_cap = 0;
   double* d_eext = nullptr;       // (3, 0:nt+1)
   size_t eext_cap = 0;
+  // gram_schmidt_interval >= 1 (sb200_set_gram_schmidt_interval): the loop's
+  // Gram-Schmidt of psi(t+dt) every gs_interval steps, its scratch and the
+  // stream that captures the body of its conditional node
+  int gs_interval = -1;
+  double2* d_gs_scratch = nullptr;  // part [no][nb], then coeff [no]
+  size_t gs_scratch_cap = 0;
+  cudaStream_t gs_side = nullptr;
   // yn_predictor_corrector = 'y' (sb200_set_predictor_corrector): the step's
   // input orbitals and V_local kept across the predictor, and the loop's
   // initial (field-free) V_local for a fixed potential
@@ -346,6 +353,9 @@ int pcg_vh_stock(sb200_ctx* c, const int* d_step, int offset, double* d_vh, doub
 // sb200_set_self_consistent enabled it)
 int scf_rt_prepare(sb200_ctx* c);
 int scf_rt_issue(sb200_ctx* c, const double2* psi);
+// gram_schmidt_col_complex8's launches with caller-given scratch (sb200_gs.cu)
+size_t gs_complex_part_len(const sb200_ctx* c);
+int gs_complex_issue(sb200_ctx* c, double2* z, double2* part, double2* coeff);
 // predictor_corrector (time_evolution_step.f90:374-428): V_local = (V_tmp + V_new) / 2
 // with V_new the potential of the predicted orbitals psi (self-consistent) or v0
 int scf_pc_potential(sb200_ctx* c, const double2* psi, const double* vtmp, const double* v0);

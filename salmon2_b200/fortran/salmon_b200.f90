@@ -184,6 +184,13 @@ module salmon_b200
       real(c_double), intent(in) :: Ac_micro(3, *), div_Ac(*)
     end function
 
+    integer(c_int) function sb200_set_gram_schmidt_interval(ctx, gram_schmidt_interval) &
+        bind(c, name="sb200_set_gram_schmidt_interval")
+      import
+      type(c_ptr), value :: ctx
+      integer(c_int), value :: gram_schmidt_interval
+    end function
+
     integer(c_int) function sb200_set_predictor_corrector(ctx, yn) bind(c, name="sb200_set_predictor_corrector")
       import
       type(c_ptr), value :: ctx

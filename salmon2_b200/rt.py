@@ -104,6 +104,10 @@ class Context:
         check(lib().sb200_set_micro_ac(self.h, C.c_void_p(a.ctypes.data),
                                        None if d is None else C.c_void_p(d.ctypes.data)))
 
+    def set_gram_schmidt_interval(self, n):
+        """gram_schmidt_interval: rt_propagate orthonormalises psi(t+dt) every n steps."""
+        check(lib().sb200_set_gram_schmidt_interval(self.h, int(n)))
+
     def set_predictor_corrector(self, on=True):
         """yn_predictor_corrector = 'y' (time_evolution_step's predictor_corrector)."""
         check(lib().sb200_set_predictor_corrector(self.h, 1 if on else 0))

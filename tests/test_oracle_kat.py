@@ -477,3 +477,25 @@ def test_predictor_corrector_averages_the_potentials():
     c = O3.rt_run(s.psi, nt, dt, zc, Ac_ext=Ac)
     d = O4.rt_run(s.psi, nt, dt, zc, Ac_ext=np.asfortranarray(0.5 * Ac))
     assert np.max(np.abs(c["psi"] - d["psi"])) <= 1e-12 * np.max(np.abs(d["psi"]))
+
+
+def test_gram_schmidt_interval_in_the_loop():
+    """gram_schmidt every N steps of the loop (time_evolution_step.f90:149-152):
+    the orbitals leave an N-step loop orthonormal (hvol metric) when N divides
+    the step count, and a loop of N - 1 steps is the plain loop exactly."""
+    from salmon2_b200 import synth
+    s = S.periodic_small()
+    g = s.grid
+    dt = 0.02
+    zc = synth.taylor_zc(dt)
+    psi0 = s.psi * 1.3  # not normalised: the Gram-Schmidt step shows
+    O1, O2 = Oracle(s), Oracle(s)
+    O2.set_gram_schmidt_interval(3)
+    a = O1.rt_run(psi0, 2, dt, zc)
+    b = O2.rt_run(psi0, 2, dt, zc)
+    assert np.array_equal(a["psi"], b["psi"])
+    c = O2.rt_run(psi0, 3, dt, zc)["psi"][g.interior_slices()]
+    for ik in range(s.nk):
+        M = c[..., 0, :, ik].reshape(-1, s.no, order="F")
+        G = g.hvol * (M.conj().T @ M)
+        assert np.max(np.abs(G - np.eye(s.no))) < 1e-12

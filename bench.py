@@ -13,7 +13,8 @@ computed every step.  Metric: grid-point x orbital Taylor steps per second
 * ``e2e``: the same metric through the reference-facing C ABI with host
   buffers: per bench step the pinned reference-layout orbitals are uploaded
   (sb200_orbitals_from_ref), propagated, and J(t) plus the final orbitals are
-  read back to the host (sb200_orbitals_to_ref).
+  read back to the host (sb200_orbitals_to_ref) into the same buffer, which
+  the next step uploads: the propagation continues through host memory.
 * ``roofline``: the kernel that applies H (on this workload k_step_orbital,
   the whole Taylor step of one orbital per CTA), timed with CUDA events on the
   library's stream in an instrumented replay right after the timed region;
@@ -596,15 +597,18 @@ def main():
     ms_max = float(t.item())
     value = units_rank * world * args.steps / (ms_max / 1e3)
 
-    # e2e: host (pinned, reference layout) -> device -> propagate -> host
-    host_in = torch.from_numpy(np.ascontiguousarray(s.psi.ravel(order="F").view(np.float64))).pin_memory()
-    host_out = torch.empty_like(host_in).pin_memory()
-    bytes_io = host_in.numel() * 8
+    # e2e: host (pinned, reference layout) -> device -> propagate -> host, the
+    # propagation carried on from the host copy of the state (so the
+    # self-consistent potential and the CG guess match the orbitals, as in the
+    # device-resident loop above, which also continues its state step to step)
+    host_state = torch.from_numpy(np.ascontiguousarray(s.psi.ravel(order="F").view(np.float64))).pin_memory()
+    ctx.download(res["psi"], out=host_state)
+    bytes_io = host_state.numel() * 8
 
     def e2e_step():
-        ctx.upload(host_in, out=a)
+        ctx.upload(host_state, out=a)
         res = ctx.rt_propagate(a, b, w, nt, dt, zc, Ac_ext=Ac)
-        ctx.download(res["psi"], out=host_out)
+        ctx.download(res["psi"], out=host_state)
         return res
 
     e2e_step()

@@ -414,7 +414,7 @@ int sb200_ctx_create(int device, sb200_ctx** out) {
   if (const char* v = getenv("SB200_STENCIL")) c->stencil_variant = (v[0] == 'n') ? 0 : 1;
   if (const char* v = getenv("SB200_ORBITAL"))
     c->orbital_variant = (v[0] == 'p') ? 1 : (v[0] == 't') ? 0 : (v[0] == 'u') ? 3 : (v[0] == 's') ? 2 : 4;
-  if (const char* v = getenv("SB200_PROJECT")) c->project_variant = (v[0] == 'w') ? 0 : (v[0] == 'd') ? 2 : 1;
+  if (const char* v = getenv("SB200_PROJECT")) c->project_variant = (v[0] == 'w') ? 0 : (v[0] == 'd') ? 2 : (v[0] == 's') ? 3 : 1;
   if (const char* v = getenv("SB200_BLK_DEPTH")) c->blk_depth = (v[0] == '4') ? 4 : 2;
   if (const char* v = getenv("SB200_BLK_SPLIT")) c->blk_split = (v[0] == '0') ? 0 : 1;
   if (const char* v = getenv("SB200_BLK_PREFETCH")) c->blk_prefetch = (v[0] == '0') ? 0 : 1;

@@ -202,7 +202,10 @@ __global__ void __launch_bounds__(128) k_project_batch(const BPSys* __restrict__
   const int s = find_sys(first, nsys, w);
   const long l = w - first[s];
   const int natom = sys[s].a.natom;
-  project_atom<4, TIN>((const TIN*)in[s], sys[s].proj, sys[s].a, (int)(l % natom), (int)(l / natom));
+  // the summation order the system's own context uses (project_atom_split is
+  // the one-warp form of k_project_split), so batch and solo give the same bits
+  if (sys[s].a.split) project_atom_split<4, TIN>((const TIN*)in[s], sys[s].proj, sys[s].a, (int)(l % natom), (int)(l / natom));
+  else project_atom<4, TIN>((const TIN*)in[s], sys[s].proj, sys[s].a, (int)(l % natom), (int)(l / natom));
 }
 
 __global__ void __launch_bounds__(OBS_THREADS) k_observables_batch(const BOSys* __restrict__ sys,

@@ -42,6 +42,7 @@ __device__ __forceinline__ double2 ldz(const double2* __restrict__ p, long i, bo
 struct ProjArgs {
   long npts;
   int natom, nlma, nps, totpts, nspin_no, phase_per_k;
+  int split;  // 1: the eight-warp summation order of project_sub (few pairs), 0: project_atom's
   const int *atom_start, *mps, *lma_start, *nproj, *pt_lin;
   const double *uv, *rinv, *pt_r;
   const double2* phase;
@@ -84,6 +85,67 @@ __device__ __forceinline__ void project_atom(const TIN* __restrict__ in, double2
         if (q0 + q < np) {
           const int lma = lma0 + q0 + q;
           proj[(long)o * a.nlma + lma] = cscal(a.rinv[lma], acc[q]);
+        }
+    }
+  }
+}
+
+// The eight-warp summation order for few (orbital, atom) pairs: sub-sum w
+// (0..7) of projectors q0 .. q0 + NP - 1 takes sphere points w*32 + lane +
+// 256 k in increasing k, butterfly-reduced over the warp.  A CTA of eight
+// warps computes the sub-sums side by side (k_project_split), one warp of the
+// batched kernel one after the other; both add them in w order, so the two
+// give the same bits.
+template <int NP, typename TIN>
+__device__ __forceinline__ void project_sub(const TIN* __restrict__ psi, const double2* __restrict__ ph,
+                                            const ProjArgs& a, const int start, const int m, const int lma0,
+                                            const int np, const int q0, const int w, double2 (&acc)[NP]) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int q = 0; q < NP; ++q) acc[q] = make_double2(0.0, 0.0);
+#pragma unroll 2
+  for (int j = w * 32 + lane; j < m; j += 256) {
+    const TIN vi = __ldg(psi + a.pt_lin[start + j]);
+    const double2 v = make_double2((double)vi.x, (double)vi.y);
+    const double2 ev = cmul(__ldg(ph + j), v);
+#pragma unroll
+    for (int q = 0; q < NP; ++q)
+      if (q0 + q < np) acc[q] = cadd(acc[q], cscal(__ldg(a.uv + (long)(lma0 + q0 + q) * a.nps + j), ev));
+  }
+#pragma unroll
+  for (int q = 0; q < NP; ++q) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      acc[q].x += __shfl_xor_sync(0xffffffffu, acc[q].x, off);
+      acc[q].y += __shfl_xor_sync(0xffffffffu, acc[q].y, off);
+    }
+  }
+}
+
+// One warp, the eight-warp order: the projections of one (orbital, atom).
+template <int NP, typename TIN>
+__device__ __forceinline__ void project_atom_split(const TIN* __restrict__ in, double2* __restrict__ proj,
+                                                   const ProjArgs& a, const int atom, const int o) {
+  const int lane = threadIdx.x & 31;
+  const int ik = o / a.nspin_no;
+  const TIN* psi = in + (long)o * a.npts;
+  const int start = a.atom_start[atom], m = a.mps[atom];
+  const int lma0 = a.lma_start[atom], np = a.nproj[atom];
+  const double2* ph = a.phase + (a.phase_per_k ? (long)ik * a.totpts : 0L) + start;
+  for (int q0 = 0; q0 < np; q0 += NP) {
+    double2 tot[NP], acc[NP];
+    project_sub<NP, TIN>(psi, ph, a, start, m, lma0, np, q0, 0, tot);
+    for (int w = 1; w < 8; ++w) {
+      project_sub<NP, TIN>(psi, ph, a, start, m, lma0, np, q0, w, acc);
+#pragma unroll
+      for (int q = 0; q < NP; ++q) tot[q] = cadd(tot[q], acc[q]);
+    }
+    if (lane == 0) {
+#pragma unroll
+      for (int q = 0; q < NP; ++q)
+        if (q0 + q < np) {
+          const int lma = lma0 + q0 + q;
+          proj[(long)o * a.nlma + lma] = cscal(a.rinv[lma], tot[q]);
         }
     }
   }

@@ -169,8 +169,9 @@ struct sb200_ctx {
   int orbital_variant = 4;     // 16^3 periodic grids: 4 fused Taylor step with register blocking (when its
                                // tables fit, else form 2), 2 fused step with the KB tables staged in shared memory
                                // (when they fit), 3 fused without staging, 0 one launch per term, 1 persistent per term
-  int project_variant = 1;     // KB projections: 1 tensor cores where a k-point fills a 16-orbital tile,
-                               // 2 tensor cores always, 0 one warp per (orbital, atom)
+  int project_variant = 1;     // KB projections: 1 tensor cores where a k-point fills a 16-orbital tile, else
+                               // a CTA per (orbital, atom) below 1184 pairs, else a warp per pair; 2 tensor
+                               // cores always, 0 one warp per (orbital, atom), 3 one CTA per (orbital, atom)
   int blk_depth = 2;           // z depth of the register block of the blocked fused step (2: 512 threads, 4: 256)
   int blk_split = 1;           // blocked fused step: KB projections by two warps per atom, overlapped with the
                                // stencil (1), or one warp per atom between the terms (0)

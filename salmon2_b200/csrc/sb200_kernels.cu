@@ -112,6 +112,39 @@ __global__ void __launch_bounds__(128) k_project(const TIN* __restrict__ in, dou
   project_atom<NP, TIN>(in, proj, a, atom, blockIdx.y);
 }
 
+// Small systems (few orbitals x atoms): one (atom, orbital) pair per CTA of
+// eight warps; warp w computes sub-sum w of project_sub, the sub-sums are
+// added in warp order in shared memory (a fixed order) and scaled by rinv.
+template <int NP, typename TIN>
+__global__ void __launch_bounds__(256) k_project_split(const TIN* __restrict__ in, double2* __restrict__ proj,
+                                                       ProjArgs a) {
+  __shared__ double2 red[8][NP];
+  const int atom = blockIdx.x, o = blockIdx.y;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int ik = o / a.nspin_no;
+  const TIN* psi = in + (long)o * a.npts;
+  const int start = a.atom_start[atom], m = a.mps[atom];
+  const int lma0 = a.lma_start[atom], np = a.nproj[atom];
+  const double2* ph = a.phase + (a.phase_per_k ? (long)ik * a.totpts : 0L) + start;
+  for (int q0 = 0; q0 < np; q0 += NP) {
+    double2 acc[NP];
+    project_sub<NP, TIN>(psi, ph, a, start, m, lma0, np, q0, warp, acc);
+    if (lane == 0) {
+#pragma unroll
+      for (int q = 0; q < NP; ++q) red[warp][q] = acc[q];
+    }
+    __syncthreads();
+    if (threadIdx.x < NP && q0 + (int)threadIdx.x < np) {
+      const int q = threadIdx.x;
+      double2 t = red[0][q];
+      for (int w = 1; w < 8; ++w) t = cadd(t, red[w][q]);
+      const int lma = lma0 + q0 + q;
+      proj[(long)o * a.nlma + lma] = cscal(a.rinv[lma], t);
+    }
+    __syncthreads();
+  }
+}
+
 // Nonlocal current pieces per (orbital, atom): sum over the atom's projectors
 // of Im(conj(<r_d zekr|psi>) * rinv <zekr|psi>)  (density_matrix.f90:532-591).
 // (at most 128 registers: four CTAs per SM)
@@ -552,6 +585,10 @@ ProjArgs make_proj_args(const sb200_ctx* c) {
   ProjArgs a;
   a.npts = c->g.npts;
   a.natom = c->pp.natom;
+  // the eight-warp order while the pairs are fewer than 8 per SM (148 SMs),
+  // or always with project_variant 3; the batched kernel follows the flag too
+  a.split = (c->project_variant == 3 ||
+             (c->project_variant == 1 && (long)c->pp.natom * c->orb.norb < 148L * 8)) ? 1 : 0;
   a.nlma = c->pp.nlma;
   a.nps = c->pp.nps;
   a.totpts = c->pp.totpts;
@@ -572,13 +609,21 @@ ProjArgs make_proj_args(const sb200_ctx* c) {
 int launch_project(sb200_ctx* c, const void* in, double2* proj, bool in32) {
   if (c->pp.nlma == 0) return SB200_OK;
   // the tensor-core form (sb200_project_mma.cu) when a k-point has at least
-  // one full 16-orbital tile, else one warp per (orbital, atom)
+  // one full 16-orbital tile, else one CTA per (orbital, atom) while the pairs
+  // are fewer than 8 per SM (148 SMs), else one warp per pair
   const int nspin_no = c->orb.nspin * c->orb.no;
   if (c->project_variant == 2 || (c->project_variant == 1 && nspin_no >= 16)) {
     const int r = launch_project_dmma(c, in, proj, in32);
     if (r != SB200_ERR_UNSUPPORTED) return r;
   }
   ProjArgs a = make_proj_args(c);
+  if (a.split) {
+    dim3 grid(a.natom, c->orb.norb);
+    if (in32) k_project_split<4, float2><<<grid, 256, 0, c->stream>>>((const float2*)in, proj, a);
+    else k_project_split<4, double2><<<grid, 256, 0, c->stream>>>((const double2*)in, proj, a);
+    SB_LAUNCH_CHECK("k_project_split");
+    return SB200_OK;
+  }
   dim3 grid((a.natom + 3) / 4, c->orb.norb);
   if (in32) k_project<4, float2><<<grid, 128, 0, c->stream>>>((const float2*)in, proj, a);
   else k_project<4, double2><<<grid, 128, 0, c->stream>>>((const double2*)in, proj, a);

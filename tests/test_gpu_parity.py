@@ -460,14 +460,15 @@ def _iso_eighteen():
     return synth.isolated_system(num=(20, 24, 22), no=18, natom=3, seed=47, name="iso18")
 
 
-@pytest.mark.parametrize("variant", ["dmma", "warp"])
+@pytest.mark.parametrize("variant", ["dmma", "warp", "split"])
 @pytest.mark.parametrize("make", [_p12_twenty_orbitals, _p12_two_spins_ten, _iso_eighteen, S.periodic_small],
                          ids=lambda f: f.__name__)
 def test_projection_forms_against_oracle(make, variant, monkeypatch):
     """The KB projections on the FP64 tensor cores (mma.sync m8n8k4 over
-    16-orbital tiles, SB200_PROJECT=dmma) and in the warp-per-(orbital, atom)
-    form, under H psi and a Taylor step, against the oracle: full and partial
-    tiles, two spins, isolated grids, fewer orbitals than a tile."""
+    16-orbital tiles, SB200_PROJECT=dmma), in the warp-per-(orbital, atom)
+    form and in the CTA-per-(orbital, atom) form (SB200_PROJECT=split), under
+    H psi and a Taylor step, against the oracle: full and partial tiles, two
+    spins, isolated grids, fewer orbitals than a tile."""
     from salmon2_b200 import synth
     monkeypatch.setenv("SB200_PROJECT", variant)
     sysm = make()

@@ -15,8 +15,10 @@ computed every step.  Metric: grid-point x orbital Taylor steps per second
   (sb200_orbitals_from_ref), propagated, and J(t) plus the final orbitals are
   read back to the host (sb200_orbitals_to_ref) into the same buffer, which
   the next step uploads: the propagation continues through host memory.
-* ``roofline``: the kernel that applies H (on this workload k_step_orbital,
-  the whole Taylor step of one orbital per CTA), timed with CUDA events on the
+  ``--workload isolated`` instead starts every bench step (both legs) from the
+  kicked orbitals: its configuration is the run of nt steps after the kick.
+* ``roofline``: the kernel that applies H (on this workload k_step_blk, the
+  whole Taylor step of a block of orbitals per CTA), timed with CUDA events on the
   library's stream in an instrumented replay right after the timed region;
   algorithmic bytes 224 B per unit per Taylor step.
 * ``cpu_baseline``: the CPU oracle (a C++/OpenMP restatement of the
@@ -125,6 +127,12 @@ def config_dict(args, s, nt, world):
         "projectors": s.pp.nlma, "taylor_steps_per_bench_step": nt, "units_per_bench_step_per_rank": units,
         "precision": args.precision,
         "self_consistent": bool(getattr(args, "self_consistent", False)),
+        "bench_step": ("the kicked orbitals copied in (device leg) or uploaded (e2e leg), "
+                       + ("their density, Hartree and PZ-LDA potential, " if getattr(
+                           args, "self_consistent", False) else "")
+                       + f"then {nt} steps: every step times the first {nt} steps after the kick"
+                       if args.workload == "isolated" else
+                       f"{nt} steps continuing the previous step's orbitals (e2e: through host memory)"),
         "parallelism": f"replicas x{world}" if args.workload == "isolated" else f"k-point shards x{world}",
         "l2": ("inputs larger than L2 (3 orbital blocks of %.0f MB each)" % (units / nt * 16 / 1e6)
                if units / nt * 16 * 3 > 126e6 else
@@ -564,12 +572,34 @@ def main():
         # then the update every step
         brl = np.diag([2.0 * np.pi / (n * h) for n, h in zip(s.grid.shape, s.grid.hgs)])
         vpsl = torch.from_numpy(np.ascontiguousarray(s.V_local[..., 0].ravel(order="F"))).cuda(local)
-        if s.grid.periodic or args.poisson == "ft":
-            ctx.update_potential(a, vpsl, brl)
-        else:  # method_poisson = 'cg': CG from the extrapolated potential every step
-            ctx.update_potential(a, vpsl, brl, poisson="cg")
-            ctx.set_hartree_cg(ctx.last_vh)
-        ctx.set_self_consistent(True, vpsl, brl)
+
+    def set_up():
+        """The self-consistent loop's initial potential from the orbitals in a
+        (initialization_rt): V_local, the Hartree potential and, with CG, its
+        extrapolation history; on the context's stream."""
+        if not args.self_consistent:
+            return
+        with torch.cuda.stream(stream):
+            if s.grid.periodic or args.poisson == "ft":
+                ctx.update_potential(a, vpsl, brl)
+            else:  # method_poisson = 'cg': CG from the extrapolated potential every step
+                ctx.update_potential(a, vpsl, brl, poisson="cg")
+                ctx.set_hartree_cg(ctx.last_vh)
+            ctx.set_self_consistent(True, vpsl, brl)
+
+    # the isolated-molecule workload is the run of nt steps after the kick: every
+    # bench step starts again from the kicked orbitals (and, self-consistent, from
+    # their potential), so each step times the same stretch of the dynamics
+    restart = args.workload == "isolated"
+    psi0 = ctx.upload(s.psi) if restart else None
+
+    def restart_from_kick():
+        if restart:
+            with torch.cuda.stream(stream):
+                a.copy_(psi0)
+            set_up()
+
+    set_up()
 
     def barrier():
         if world > 1:
@@ -577,6 +607,7 @@ def main():
         torch.cuda.synchronize()
 
     def one_step():
+        restart_from_kick()
         return ctx.rt_propagate(a, b, w, nt, dt, zc, Ac_ext=Ac)
 
     for _ in range(args.warmup):
@@ -597,18 +628,23 @@ def main():
     ms_max = float(t.item())
     value = units_rank * world * args.steps / (ms_max / 1e3)
 
-    # e2e: host (pinned, reference layout) -> device -> propagate -> host, the
-    # propagation carried on from the host copy of the state (so the
-    # self-consistent potential and the CG guess match the orbitals, as in the
-    # device-resident loop above, which also continues its state step to step)
+    # e2e: host (pinned, reference layout) -> device -> propagate -> host.  The
+    # isolated workload uploads the kicked orbitals every step (and sets up
+    # their potential) as the device-resident loop above does; the periodic ones
+    # carry the propagation on through host memory: each step uploads what the
+    # previous one read back
     host_state = torch.from_numpy(np.ascontiguousarray(s.psi.ravel(order="F").view(np.float64))).pin_memory()
-    ctx.download(res["psi"], out=host_state)
+    host_out = torch.empty_like(host_state).pin_memory() if restart else host_state
+    if not restart:
+        ctx.download(res["psi"], out=host_state)
     bytes_io = host_state.numel() * 8
 
     def e2e_step():
         ctx.upload(host_state, out=a)
+        if restart:
+            set_up()
         res = ctx.rt_propagate(a, b, w, nt, dt, zc, Ac_ext=Ac)
-        ctx.download(res["psi"], out=host_state)
+        ctx.download(res["psi"], out=host_out)
         return res
 
     e2e_step()
@@ -626,6 +662,8 @@ def main():
     e2e_value = units_rank * world * ne2e / (float(te.item()) / 1e3)
 
     # instrumented replay for per-kernel device times (roofline + shares)
+    restart_from_kick()
+    torch.cuda.synchronize()
     ctx.set_timing(True)
     ctx.kernel_times(reset=True)
     nt_i = min(nt, 200)

@@ -108,7 +108,7 @@ int check_device_flag(sb200_ctx* c) {
   if (flag != 0) {
     SB_CUDA(cudaMemset(c->d_err, 0, sizeof(int)));
     SB_CUDA(cudaDeviceSynchronize());
-    return set_error(SB200_ERR_TIMEOUT, "a bounded device wait expired (a bulk copy did not complete)");
+    return set_error(SB200_ERR_TIMEOUT, "a bounded device wait expired (a bulk copy or a grid barrier did not complete)");
   }
   return SB200_OK;
 }

@@ -30,6 +30,15 @@
 // WHILE node whose condition the convergence test clears, so the loop runs
 // without the host.  zk and the two pk buffers are padded by the 4-point halo,
 // which stays zero, so the stencil needs no bounds tests.
+//
+// The default form runs all iterations in ONE cooperative launch
+// (k_pcg_solve, at most two blocks of 512 threads per SM, all co-resident):
+// (A) and (B) as above, each followed by a grid barrier after which every block
+// sums the per-block partials itself, in block order, so all blocks take the
+// same decisions.  The barrier's wait is bounded: on expiry it sets an abort
+// word that releases the other blocks and the context's error flag, which the
+// host turns into SB200_ERR_TIMEOUT.  The two-launch form stays for
+// SB200_PCG_PERSISTENT=0 and where a cooperative launch cannot be captured.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -52,6 +61,8 @@ constexpr int PCG_CHUNK = 16;  // iterations between host checks of the converge
 // on the 64^3 isolated self-consistent loop 8 runs 3 % faster than 2, 16 no faster)
 constexpr int PCG_UNROLL = 8;
 constexpr double PCG_PI = 3.141592653589793;
+constexpr int PTP = 512;                          // threads per block of the one-launch solve
+constexpr long long PCG_WAIT_CYCLES = 2000000000LL;  // a grid barrier gives up after ~1 s of SM clocks
 
 // scalars of the iteration (device)
 // (SC_NEXT: the iteration the next launch pair performs)
@@ -79,6 +90,7 @@ struct PArgs {
   double* pole;         // [npole][POLE_W]
   double* psum;         // [npole][nchunk][NLM_MAX] pole partial sums
   const int* cell;      // layout 3: [npole][6] interior offset boxes (x0, x1, y0, y1, z0, z1)
+  int* err;             // the context's device error flag (a bounded wait expired)
   int* owner;           // layout 2: nearest atom of each interior point
   const double* rion;   // [natom][3]
   double threshold;
@@ -130,6 +142,7 @@ __device__ __forceinline__ void ylm_all(double x, double y, double z, double (&Y
 __device__ __forceinline__ int l_of(int lm) { return lm < 1 ? 0 : lm < 4 ? 1 : lm < 9 ? 2 : lm < 16 ? 3 : 4; }
 
 // block-wide sum of one value per thread; every thread gets the total (fixed order)
+template <int NT = PT>
 __device__ __forceinline__ double block_sum(double v, double* red) {
   const int t = threadIdx.x, lane = t & 31, w = t >> 5;
 #pragma unroll
@@ -139,11 +152,11 @@ __device__ __forceinline__ double block_sum(double v, double* red) {
   __syncthreads();
   double s = 0.0;
   if (t == 0) {
-    for (int i = 0; i < PT / 32; ++i) s += red[i];
-    red[PT / 32] = s;
+    for (int i = 0; i < NT / 32; ++i) s += red[i];
+    red[NT / 32] = s;
   }
   __syncthreads();
-  return red[PT / 32];
+  return red[NT / 32];
 }
 
 // The block's partial to part[blockIdx.x]; true in the block that finished last,
@@ -393,6 +406,8 @@ __global__ void __launch_bounds__(PT) k_pcg_first(PArgs a) {
       a.sc[SC_ITER] = 0.0;
       a.sc[SC_NEXT] = 1.0;
       *a.counter = 0u;
+      a.counter[1] = 0u;  // grid barrier of k_pcg_solve: arrivals
+      a.counter[3] = 0u;  // and its abort word
     }
   }
 }
@@ -470,6 +485,138 @@ __global__ void __launch_bounds__(PT) k_pcg_update(PArgs a, cudaGraphConditional
   }
 }
 
+// Grid barrier of k_pcg_solve (every block resident: cooperative launch).
+// counter[1] counts arrivals over the whole solve (k_pcg_first zeroes it), so
+// barrier k of a block waits for k * gridDim.x arrivals; counter[3] is the
+// abort word.  Thread 0 of each block fences its block's writes, arrives and
+// polls the count; the wait is bounded by the SM clock, and on expiry it sets
+// the abort word and the context's error flag.  False: leave the solve.
+__device__ __forceinline__ bool grid_barrier(const PArgs& a, unsigned int& target) {
+  __shared__ int ok;
+  target += gridDim.x;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned int* cnt = a.counter + 1;
+    volatile unsigned int* abort_word = a.counter + 3;
+    int good = 1;
+    __threadfence();
+    atomicAdd(a.counter + 1, 1u);
+    const long long t0 = clock64();
+    unsigned int polls = 0;
+    while ((int)(*cnt - target) < 0) {
+      if ((++polls & 63u) == 0u) {
+        if (*abort_word != 0u) {
+          good = 0;
+          break;
+        }
+        if (clock64() - t0 > PCG_WAIT_CYCLES) {
+          atomicExch(a.counter + 3, 1u);
+          atomicExch(a.err, 1);
+          a.sc[SC_DONE] = 3.0;
+          good = 0;
+          break;
+        }
+      }
+    }
+    __threadfence();
+    ok = good;
+  }
+  __syncthreads();
+  return ok != 0;
+}
+
+// the sum of the nb per-block partials p[0 .. nb) in block order, in every block
+__device__ __forceinline__ double grid_total(const double* p, int nb, double* red) {
+  double v = 0.0;
+  for (int i = threadIdx.x; i < nb; i += PTP) v += __ldcg(p + i);
+  return block_sum<PTP>(v, red);
+}
+
+// All CG iterations of one solve in one launch (after k_pcg_first): the
+// iteration of k_pcg_direction + k_pcg_update with the scalars kept in
+// registers; block 0 writes them back at the end.  The arrays written during
+// the launch (zk, pk, rlap, vh) are read with coherent loads, not __ldg.
+__global__ void __launch_bounds__(PTP, 2) k_pcg_solve(PArgs a) {
+  __shared__ double red[PTP / 32 + 1];
+  double* partA = a.part;
+  double* partB = a.part + gridDim.x;
+  const int nb = (int)gridDim.x;
+  // rows (y, z) of the grid go to warps in turn, the lanes of a warp along x:
+  // 32-bit divisions by ny instead of three 64-bit divisions per point
+  const int rows = a.ny * a.nz, lane = threadIdx.x & 31;
+  const int warp0 = (int)((blockIdx.x * PTP + threadIdx.x) >> 5), nwarps = nb * (PTP / 32);
+  unsigned int target = 0u;
+  double sum1 = a.sc[SC_SUM1], ck = 0.0;
+  double done = 0.0, iter = 0.0;
+  int it = 1;
+  for (; it <= a.maxiter; ++it) {
+    const double* zk = a.zk;
+    const double* po = a.pk[(it + 1) & 1];
+    double* pn = a.pk[it & 1];
+    const bool first = it == 1;
+    auto pk_new = [&](long i) { return first ? zk[i] : zk[i] + ck * po[i]; };
+    double s = 0.0;
+    // one loop over this lane's points: x steps by 32 along a row, then the
+    // next row of the warp (a nested loop would let the compiler hoist the 50
+    // neighbour addresses of a row into registers)
+    for (int r = warp0, x = lane; r < rows;) {
+      if (x < a.nx) {
+        const long c = padi(a, x, r % a.ny, r / a.ny);
+        const double lv = lap_at(a, c, pk_new);
+        pn[c] = pk_new(c);
+        a.rlap[(long)r * a.nx + x] = lv;
+        s += zk[c] * lv;
+      }
+      x += 32;
+      if (x >= a.nx) {
+        x = lane;
+        r += nwarps;
+      }
+    }
+    s = block_sum<PTP>(s, red);
+    if (threadIdx.x == 0) partA[blockIdx.x] = s;
+    if (!grid_barrier(a, target)) return;
+    const double ak = sum1 / grid_total(partA, nb, red) / a.hvol;
+    s = 0.0;
+    for (int r = warp0, x = lane; r < rows;) {
+      if (x < a.nx) {
+        const long c = padi(a, x, r % a.ny, r / a.ny), q = (long)r * a.nx + x;
+        a.vh[q] = a.vh[q] + ak * pn[c];
+        const double zv = a.zk[c] - ak * a.rlap[q];
+        a.zk[c] = zv;
+        s += zv * zv;
+      }
+      x += 32;
+      if (x >= a.nx) {
+        x = lane;
+        r += nwarps;
+      }
+    }
+    s = block_sum<PTP>(s, red);
+    if (threadIdx.x == 0) partB[blockIdx.x] = s;
+    if (!grid_barrier(a, target)) return;
+    const double sum2 = grid_total(partB, nb, red) * a.hvol;
+    if (fabs(sum2) < a.threshold * (double)a.N) {
+      done = 1.0;
+      iter = (double)it;
+      break;
+    }
+    ck = sum2 / sum1;
+    sum1 = sum2;
+    if (it >= a.maxiter) {
+      done = 2.0;
+      iter = (double)(a.maxiter + 1);
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    a.sc[SC_SUM1] = sum1;
+    a.sc[SC_CK] = ck;
+    a.sc[SC_DONE] = done;
+    a.sc[SC_ITER] = iter;
+    a.sc[SC_NEXT] = (double)(done == 1.0 ? it + 1 : it);
+  }
+}
+
 // Vh extrapolation of the isolated time step (time_evolution_step.f90:187-190,
 // 196-198): with the global step itt = (device step counter, itt + 1 after
 // finalize) - 1 + offset not 1, Vh = 2 stock1 - stock2 and stock2 = stock1
@@ -495,6 +642,7 @@ struct PcgState {
   bool configured = false;
   cudaStream_t side = nullptr;  // captures the body of the conditional node
   int unroll = PCG_UNROLL;      // CG iterations per body of the conditional node
+  int solve_grid = 0;           // blocks of k_pcg_solve (0: the two-launch form)
 };
 
 PcgState* pcg_of(sb200_ctx* c) { return static_cast<PcgState*>(c->pcg); }
@@ -512,6 +660,56 @@ int grid_blocks(long n) {
   long b = (n + PT - 1) / PT;
   if (b > 148L * bps) b = 148L * bps;
   return (int)(b < 1 ? 1 : b);
+}
+
+// One cooperative launch of k_pcg_solve on st (captured or not).
+cudaError_t launch_solve(const PArgs& a, int grid, cudaStream_t st) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = dim3(PTP);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeCooperative;
+  at[0].val.cooperative = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k_pcg_solve, a);
+}
+
+// Blocks of the one-launch solve: at most two per SM (one with
+// SB200_PCG_SOLVE_BLOCKS_PER_SM=1) and no more than the points need, within
+// what the device keeps resident; 0 when disabled
+// (SB200_PCG_PERSISTENT=0), when the kernel cannot be resident, or when a
+// cooperative launch cannot be captured into a graph on this driver (checked
+// once by capturing one on the side stream; the probe graph never runs).
+int solve_grid_for(long n, cudaStream_t side, int device) {
+  if (const char* v = std::getenv("SB200_PCG_PERSISTENT"))
+    if (v[0] == '0') return 0;
+  int coop = 0, sms = 0, per_sm = 0;
+  if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device) != cudaSuccess || !coop ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg_solve, PTP, 0) != cudaSuccess || per_sm < 1) {
+    cudaGetLastError();
+    return 0;
+  }
+  int bps = 2;  // SB200_PCG_SOLVE_BLOCKS_PER_SM: 1 or 2 (default 2)
+  if (const char* v = std::getenv("SB200_PCG_SOLVE_BLOCKS_PER_SM")) bps = (std::atoi(v) == 1) ? 1 : 2;
+  long g = (long)sms * (per_sm < bps ? per_sm : bps);
+  const long need = (n + PTP - 1) / PTP;
+  if (g > need) g = need;
+  if (g < 1) return 0;
+  PArgs probe{};
+  if (cudaStreamBeginCapture(side, cudaStreamCaptureModeRelaxed) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  const cudaError_t le = launch_solve(probe, (int)g, side);
+  cudaGraph_t pg = nullptr;
+  const cudaError_t ee = cudaStreamEndCapture(side, &pg);
+  if (pg) cudaGraphDestroy(pg);
+  cudaGetLastError();
+  return (le == cudaSuccess && ee == cudaSuccess) ? (int)g : 0;
 }
 
 }  // namespace
@@ -622,15 +820,6 @@ int pcg_configure(sb200_ctx* c, int layout, int lmax, const double* rion, int na
   a.nchunk = (int)((pole_pts + MCH - 1) / MCH);
   // device arena
   auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
-  const int nblk = grid_blocks(a.N);
-  const size_t b_pad = al(P * sizeof(double)), b_int = al(a.N * sizeof(double));
-  const size_t b_part = al((size_t)nblk * sizeof(double)), b_sc = al(8 * sizeof(double) + sizeof(unsigned int) * 8);
-  const size_t b_pole = al((size_t)a.npole * POLE_W * sizeof(double));
-  const size_t b_psum = al((size_t)a.npole * a.nchunk * NLM_MAX * sizeof(double));
-  const size_t b_cell = al(cell_h.size() * sizeof(int) + 4);
-  const size_t b_owner = layout == 2 ? al(a.N * sizeof(int)) : 0;
-  const size_t b_rion = al((size_t)(natom > 0 ? natom : 1) * 3 * sizeof(double));
-  const size_t need = 4 * b_pad + 3 * b_int + b_part + b_sc + b_pole + b_psum + b_cell + b_owner + b_rion;
   PcgState* s = pcg_of(c);
   if (!s) {
     s = new PcgState();
@@ -641,7 +830,18 @@ int pcg_configure(sb200_ctx* c, int layout, int lmax, const double* rion, int na
     c->pcg = s;
     SB_CUDA(cudaMallocHost((void**)&s->host_sc, 8 * sizeof(double)));
     SB_CUDA(cudaStreamCreateWithFlags(&s->side, cudaStreamNonBlocking));
+    s->solve_grid = solve_grid_for(a.N, s->side, c->device);
   }
+  const int nblk = grid_blocks(a.N);
+  const long n_part = nblk > 2L * s->solve_grid ? nblk : 2L * s->solve_grid;  // k_pcg_solve: two partial arrays
+  const size_t b_pad = al(P * sizeof(double)), b_int = al(a.N * sizeof(double));
+  const size_t b_part = al((size_t)n_part * sizeof(double)), b_sc = al(8 * sizeof(double) + sizeof(unsigned int) * 8);
+  const size_t b_pole = al((size_t)a.npole * POLE_W * sizeof(double));
+  const size_t b_psum = al((size_t)a.npole * a.nchunk * NLM_MAX * sizeof(double));
+  const size_t b_cell = al(cell_h.size() * sizeof(int) + 4);
+  const size_t b_owner = layout == 2 ? al(a.N * sizeof(int)) : 0;
+  const size_t b_rion = al((size_t)(natom > 0 ? natom : 1) * 3 * sizeof(double));
+  const size_t need = 4 * b_pad + 3 * b_int + b_part + b_sc + b_pole + b_psum + b_cell + b_owner + b_rion;
   s->configured = false;
   if (s->cap < need) {
     if (s->arena) cudaFree(s->arena);
@@ -683,11 +883,12 @@ int pcg_configure(sb200_ctx* c, int layout, int lmax, const double* rion, int na
   p += b_owner;
   double* rion_d = (double*)p;
   a.rion = rion_d;
+  a.err = c->d_err;
   cudaStream_t st = c->stream;
   // the padded arrays start at zero (their halos stay zero; vb's face halos are
-  // rewritten by every solve), the block counter at zero
+  // rewritten by every solve), the block counter and the grid barrier at zero
   SB_CUDA(cudaMemsetAsync(a.vb, 0, 4 * b_pad, st));
-  SB_CUDA(cudaMemsetAsync(a.counter, 0, sizeof(unsigned int), st));
+  SB_CUDA(cudaMemsetAsync(a.counter, 0, 8 * sizeof(unsigned int), st));
   SB_CUDA(cudaMemcpyAsync(a.pole, pole_h.data(), pole_h.size() * sizeof(double), cudaMemcpyHostToDevice, st));
   if (!cell_h.empty())
     SB_CUDA(cudaMemcpyAsync(cell_d, cell_h.data(), cell_h.size() * sizeof(int), cudaMemcpyHostToDevice, st));
@@ -733,6 +934,19 @@ int pcg_issue(sb200_ctx* c, const double* d_rho, double* d_vh, int* iterations) 
   const cudaGraphNode_t* deps = nullptr;
   size_t nd = 0;
   SB_CUDA(cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &nd));
+  if (s->solve_grid > 0) {  // every iteration in one cooperative launch
+    const cudaError_t le = launch_solve(a, s->solve_grid, st);
+    if (le != cudaSuccess) return cuda_error(le, "k_pcg_solve (cooperative launch)");
+    if (cs == cudaStreamCaptureStatusActive) return SB200_OK;
+    SB_CUDA(cudaMemcpyAsync(s->host_sc, a.sc, SC_COUNT * sizeof(double), cudaMemcpyDeviceToHost, st));
+    SB_CUDA(cudaStreamSynchronize(st));
+    if (s->host_sc[SC_DONE] == 3.0) {
+      SB_CUDA(cudaMemset(a.err, 0, sizeof(int)));
+      return set_error(SB200_ERR_TIMEOUT, "k_pcg_solve: a grid barrier wait expired");
+    }
+    if (iterations) *iterations = (int)s->host_sc[SC_ITER];
+    return SB200_OK;
+  }
   if (cs == cudaStreamCaptureStatusActive) {
     cudaGraphConditionalHandle h;
     SB_CUDA(cudaGraphConditionalHandleCreate(&h, g, 1u, cudaGraphCondAssignDefault));

@@ -467,10 +467,11 @@ def test_hartree_isolated_cg_refuses_periodic_and_bad_layout():
 def test_rt_propagate_self_consistent_isolated_cg(nt):
     """The isolated self-consistent loop with method_poisson = 'cg' (the
     reference's default): each step's Hartree potential by CG from the
-    extrapolated potential (time_evolution_step.f90:186-198), the iterations
-    inside the loop's CUDA graph as a conditional node (the odd last step of
-    nt = 5 runs outside the graph), against the oracle's loop: dipole every
-    step, final orbitals."""
+    extrapolated potential (time_evolution_step.f90:186-198), the solve
+    inside the loop's CUDA graph (the odd last step of
+    nt = 5 runs outside the graph; the iterations in one cooperative launch
+    by default), against the oracle's loop: dipole every step, final
+    orbitals."""
     import dataclasses as dc
     from salmon2_b200 import synth
     from salmon2_b200.rt import Context
@@ -500,6 +501,43 @@ def test_rt_propagate_self_consistent_isolated_cg(nt):
     assert np.max(np.abs(d_got - d_ref)) <= 1e-8 * np.max(np.abs(d_ref))
     assert S.rel_err(ctx.download(res["psi"]), ref["psi"]) < TOL_LOOP
     ctx.close()
+
+
+@pytest.mark.parametrize("layout", [1, 3])
+def test_hartree_isolated_cg_one_launch_equals_two_launch_form(layout, monkeypatch):
+    """The CG solve in one cooperative launch (default, grid barriers between
+    the two halves of each iteration) against the two-launch form
+    (SB200_PCG_PERSISTENT=0) on a 64^3 grid, where the one-launch form runs
+    on two blocks per SM: the same iteration count within one and the same
+    potential within 1e-10 relative (the per-block partial sums are cut
+    differently); then a short isolated self-consistent loop with CG under
+    each form: the same orbitals within 1e-10."""
+    import dataclasses as dc
+    from salmon2_b200 import synth
+    from salmon2_b200.rt import Context
+
+    s0 = synth.isolated_system(num=64, h_aa=0.25, no=2, natom=2, seed=9, name="iso64cg")
+    s = dc.replace(s0, psi=synth.impulse_kick(s0.grid, s0.psi, 1e-3))
+    rho = Oracle(s).density(s.psi)[..., 0]
+    out = {}
+    for form in ("1", "0"):
+        monkeypatch.setenv("SB200_PCG_PERSISTENT", form)
+        ctx = Context(s)
+        v, it = ctx.hartree_isolated_cg(rho, layout=layout)
+        a, b, w = ctx.upload(s.psi), ctx.zeros(), ctx.zeros()
+        vpsl = np.array(s.V_local[..., 0])
+        ctx.update_vlocal(vpsl, v, OR.exc_cor_pz(rho, s.grid.hvol)[0])
+        ctx.set_hartree_cg(v, layout=layout)
+        ctx.set_self_consistent(True, vpsl, _brl(s))
+        res = ctx.rt_propagate(a, b, w, 4, 0.05, synth.taylor_zc(0.05))
+        out[form] = (v, it, ctx.download(res["psi"]))
+        ctx.close()
+    (v1, it1, p1), (v0, it0, p0) = out["1"], out["0"]
+    print(f"CG one launch / two launches, layout {layout}: iterations {it1} / {it0}, "
+          f"potential rel {S.rel_err(v1, v0):.3e}, orbitals rel {S.rel_err(p1, p0):.3e}")
+    assert it1 < 1000 and abs(it1 - it0) <= 1
+    assert S.rel_err(v1, v0) < 1e-10
+    assert S.rel_err(p1, p0) < 1e-10
 
 
 def test_exc_cor_pz_spin_polarised_against_oracle():

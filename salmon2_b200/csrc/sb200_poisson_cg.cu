@@ -488,22 +488,30 @@ __global__ void __launch_bounds__(PT) k_pcg_update(PArgs a, cudaGraphConditional
 // Grid barrier of k_pcg_solve (every block resident: cooperative launch).
 // counter[1] counts arrivals over the whole solve (k_pcg_first zeroes it), so
 // barrier k of a block waits for k * gridDim.x arrivals; counter[3] is the
-// abort word.  Thread 0 of each block fences its block's writes, arrives and
-// polls the count; the wait is bounded by the SM clock, and on expiry it sets
-// the abort word and the context's error flag.  False: leave the solve.
+// abort word.  After the block barrier, thread 0 arrives with a release
+// reduction (publishing the block's writes at GPU scope) and polls the count
+// with acquire loads; the wait is bounded by the SM clock, and on expiry it
+// sets the abort word and the context's error flag.  False: leave the solve.
+__device__ __forceinline__ unsigned int ld_acquire_gpu(const unsigned int* p) {
+  unsigned int v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void red_release_gpu(unsigned int* p, unsigned int v) {
+  asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
 __device__ __forceinline__ bool grid_barrier(const PArgs& a, unsigned int& target) {
   __shared__ int ok;
   target += gridDim.x;
   __syncthreads();
   if (threadIdx.x == 0) {
-    volatile unsigned int* cnt = a.counter + 1;
     volatile unsigned int* abort_word = a.counter + 3;
     int good = 1;
-    __threadfence();
-    atomicAdd(a.counter + 1, 1u);
+    red_release_gpu(a.counter + 1, 1u);
     const long long t0 = clock64();
     unsigned int polls = 0;
-    while ((int)(*cnt - target) < 0) {
+    while ((int)(ld_acquire_gpu(a.counter + 1) - target) < 0) {
       if ((++polls & 63u) == 0u) {
         if (*abort_word != 0u) {
           good = 0;
@@ -518,7 +526,6 @@ __device__ __forceinline__ bool grid_barrier(const PArgs& a, unsigned int& targe
         }
       }
     }
-    __threadfence();
     ok = good;
   }
   __syncthreads();

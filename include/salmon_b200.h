@@ -562,6 +562,17 @@ int sb200_hartree_isolated_cg(sb200_ctx* ctx, const double* rho, double* Vh, int
                               int lmax_multipole, const double* Rion, int natom, const int num_multipole_xyz[3],
                               double threshold_cg, int maxiter, int* iterations);
 
+/* Check of the bounded grid barrier that the one-launch CG solve uses
+ * between the halves of each iteration: eight barriers over the solve's
+ * cooperative grid.  withhold = 0: SB200_OK.  withhold != 0: one block leaves
+ * without arriving, the others' waits expire after about a second of SM clock,
+ * and the call returns SB200_ERR_TIMEOUT with the context still usable (the
+ * failure report a stalled solve gives).  Needs the CG solve configured (a
+ * prior sb200_hartree_isolated_cg or sb200_set_hartree_cg); SB200_ERR_UNSUPPORTED
+ * when the two-launch form is in use.  No reference counterpart: failure
+ * detection of this library's own device wait.                                 */
+int sb200_check_grid_barrier(sb200_ctx* ctx, int withhold);
+
 /* Selects the CG Hartree solve (sb200_hartree_isolated_cg, same arguments) for
  * the isolated self-consistent time loop (sb200_set_self_consistent) in place
  * of the doubled-box transforms, the reference's default for isolated systems.

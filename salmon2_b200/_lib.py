@@ -63,6 +63,7 @@ SIGNATURES = {
     "sb200_hartree_periodic": (C.c_int, [_vp, _dp, _vp, _vp]),
     "sb200_update_vlocal": (C.c_int, [_vp, _vp, _vp, _vp]),
     "sb200_hartree_isolated_ft": (C.c_int, [_vp, _dp, _vp, _vp]),
+    "sb200_check_grid_barrier": (C.c_int, [_vp, C.c_int]),
     "sb200_hartree_isolated_cg": (C.c_int, [_vp, _vp, _vp, C.c_int, C.c_int, _dp, C.c_int, _ip, C.c_double,
                                             C.c_int, _ip]),
     "sb200_set_lattice": (C.c_int, [_vp, _dp, _dp]),

@@ -624,6 +624,17 @@ __global__ void __launch_bounds__(PTP, 2) k_pcg_solve(PArgs a) {
   }
 }
 
+// Check of the grid barrier: `rounds` barriers over the solve's cooperative
+// grid.  With withhold != 0 block 0 leaves without arriving, so the other
+// blocks' bounded waits expire (about a second of SM clock) and set the abort
+// word and the context's error flag, as a stalled solve would.
+__global__ void __launch_bounds__(PTP, 2) k_barrier_check(PArgs a, int rounds, int withhold) {
+  unsigned int target = 0u;
+  if (withhold && blockIdx.x == 0) return;
+  for (int r = 0; r < rounds; ++r)
+    if (!grid_barrier(a, target)) return;
+}
+
 // Vh extrapolation of the isolated time step (time_evolution_step.f90:187-190,
 // 196-198): with the global step itt = (device step counter, itt + 1 after
 // finalize) - 1 + offset not 1, Vh = 2 stock1 - stock2 and stock2 = stock1
@@ -669,8 +680,9 @@ int grid_blocks(long n) {
   return (int)(b < 1 ? 1 : b);
 }
 
-// One cooperative launch of k_pcg_solve on st (captured or not).
-cudaError_t launch_solve(const PArgs& a, int grid, cudaStream_t st) {
+// One cooperative launch of a kernel of PTP threads per block on st (captured or not).
+template <typename... Args>
+cudaError_t launch_coop(void (*kernel)(PArgs, Args...), int grid, cudaStream_t st, const PArgs& a, Args... args) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)grid);
   cfg.blockDim = dim3(PTP);
@@ -681,8 +693,10 @@ cudaError_t launch_solve(const PArgs& a, int grid, cudaStream_t st) {
   at[0].val.cooperative = 1;
   cfg.attrs = at;
   cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, k_pcg_solve, a);
+  return cudaLaunchKernelEx(&cfg, kernel, a, args...);
 }
+
+cudaError_t launch_solve(const PArgs& a, int grid, cudaStream_t st) { return launch_coop(k_pcg_solve, grid, st, a); }
 
 // Blocks of the one-launch solve: at most two per SM (one with
 // SB200_PCG_SOLVE_BLOCKS_PER_SM=1) and no more than the points need, within
@@ -1022,6 +1036,41 @@ int hartree_isolated_cg(sb200_ctx* c, const double* rho, double* vh, int layout,
 }
 
 }  // namespace sb200
+
+namespace sb200 {
+namespace {
+int check_grid_barrier(sb200_ctx* c, int withhold) {
+  PcgState* s = pcg_of(c);
+  if (!s || !s->configured) return set_error(SB200_ERR_STATE, "the CG Hartree solve is not configured");
+  if (s->solve_grid < 1) return set_error(SB200_ERR_UNSUPPORTED, "the one-launch CG solve is not in use");
+  const PArgs& a = s->base;
+  cudaStream_t st = c->stream;
+  SB_CUDA(cudaMemsetAsync(a.counter + 1, 0, 3 * sizeof(unsigned int), st));
+  const cudaError_t le = launch_coop(k_barrier_check, s->solve_grid, st, a, 8, withhold ? 1 : 0);
+  if (le != cudaSuccess) return cuda_error(le, "k_barrier_check (cooperative launch)");
+  SB_CUDA(cudaStreamSynchronize(st));
+  int flag = 0;
+  SB_CUDA(cudaMemcpy(&flag, c->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+  SB_CUDA(cudaMemsetAsync(a.counter + 1, 0, 3 * sizeof(unsigned int), st));
+  SB_CUDA(cudaStreamSynchronize(st));
+  if (flag != 0) {
+    SB_CUDA(cudaMemset(c->d_err, 0, sizeof(int)));
+    return set_error(SB200_ERR_TIMEOUT, "grid barrier: a bounded wait expired (a block did not arrive)");
+  }
+  return SB200_OK;
+}
+}  // namespace
+}  // namespace sb200
+
+extern "C" int sb200_check_grid_barrier(sb200_ctx* c, int withhold) {
+  if (!c) return sb200::set_error(SB200_ERR_INVALID_ARG, "null ctx");
+  int prev = -1;
+  if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+  if (prev != c->device) cudaSetDevice(c->device);
+  const int r = sb200::check_grid_barrier(c, withhold);
+  if (prev >= 0 && prev != c->device) cudaSetDevice(prev);
+  return r;
+}
 
 extern "C" int sb200_hartree_isolated_cg(sb200_ctx* c, const double* rho, double* Vh, int layout_multipole,
                                          int lmax_multipole, const double* Rion, int natom,

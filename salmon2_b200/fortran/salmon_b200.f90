@@ -373,6 +373,12 @@ module salmon_b200
       integer(c_int), intent(out) :: iterations
     end function
 
+    integer(c_int) function sb200_check_grid_barrier(ctx, withhold) bind(c, name="sb200_check_grid_barrier")
+      import
+      type(c_ptr), value :: ctx
+      integer(c_int), value :: withhold
+    end function
+
     integer(c_int) function sb200_set_hartree_cg(ctx, Vh0, layout_multipole, lmax_multipole, Rion, natom, &
         num_multipole_xyz, threshold_cg, maxiter) bind(c, name="sb200_set_hartree_cg")
       import

@@ -540,6 +540,29 @@ def test_hartree_isolated_cg_one_launch_equals_two_launch_form(layout, monkeypat
     assert S.rel_err(p1, p0) < 1e-10
 
 
+def test_cg_grid_barrier_wait_expires_with_an_error():
+    """The one-launch CG solve's grid barrier is a bounded wait: when one block
+    of the cooperative grid never arrives (sb200_check_grid_barrier with
+    withhold), the others give up after about a second and the call returns
+    SB200_ERR_TIMEOUT; the context stays usable: the check then passes and a
+    CG solve gives the same potential as before."""
+    from salmon2_b200 import _lib
+    from salmon2_b200.rt import Context
+
+    s = S.isolated_small()
+    ctx = Context(s)
+    rho = Oracle(s).density(s.psi)[..., 0]
+    v0, it0 = ctx.hartree_isolated_cg(rho)
+    assert _lib.lib().sb200_check_grid_barrier(ctx.h, 0) == 0
+    rc = _lib.lib().sb200_check_grid_barrier(ctx.h, 1)
+    assert rc == 6  # SB200_ERR_TIMEOUT
+    assert b"grid barrier" in _lib.lib().sb200_last_error()
+    assert _lib.lib().sb200_check_grid_barrier(ctx.h, 0) == 0
+    v1, it1 = ctx.hartree_isolated_cg(rho)
+    assert it1 == it0 and np.array_equal(v1, v0)
+    ctx.close()
+
+
 def test_exc_cor_pz_spin_polarised_against_oracle():
     """exc_cor_pz_sp on the GPU (nspin = 2: spin densities in, Vxc per spin out)
     against the oracle's restatement, on the orbitals' spin densities and on

@@ -131,6 +131,57 @@ __device__ __forceinline__ C2 kb_pairs(C2 h, int pm, const double2* __restrict__
   return h;
 }
 
+// The first (point, atom) pair of a point, loaded one plane ahead by the
+// tensor-copy sweep (nearly every point inside a sphere has exactly one pair,
+// so the scatter's dependent loads leave the critical path).  The weights and
+// the conjugate phase are kept in the stencil's type: the same values
+// kb_pairs converts at use.
+template <typename R>
+struct Pair1 {
+  int lm;  // pair_lma of the pair (0: no pair)
+  R u[4];
+  R ex, ey;
+};
+
+template <typename R>
+__device__ __forceinline__ void load_pair1(Pair1<R>& f, int pm, const TiledArgs& a, const double2* __restrict__ ph) {
+  f.lm = 0;
+  if (pm < 0 || (pm & 255) == 0) return;
+  const int p0 = pm >> 8;
+  f.lm = __ldg(a.pair_lma + p0);
+  const double2 u01 = __ldg((const double2*)(a.pair_uv + 4L * p0));
+  const double2 u23 = __ldg((const double2*)(a.pair_uv + 4L * p0 + 2));
+  const double2 e = __ldg(ph + p0);
+  f.u[0] = (R)u01.x;
+  f.u[1] = (R)u01.y;
+  f.u[2] = (R)u23.x;
+  f.u[3] = (R)u23.y;
+  f.ex = (R)e.x;
+  f.ey = -(R)e.y;
+}
+
+// kb_pairs with its first pair taken from f (loaded ahead); the others, in the
+// same order, as kb_pairs loads them: the same sums, bit for bit
+template <typename R, typename C2 = typename Cx<R>::T>
+__device__ __forceinline__ C2 kb_pairs_ahead(C2 h, int pm, const double2* __restrict__ P, const TiledArgs& a,
+                                             int ik, const Pair1<R>& f) {
+  const int p0 = pm >> 8, p1 = p0 + (pm & 255);
+  if (p1 <= p0) return h;
+  {
+    const int l0 = f.lm & 0xffffff, np = f.lm >> 24;
+    C2 sp = Cx<R>::make(0, 0);
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+      if (q < np) {
+        const double2 pv = P[l0 + q];
+        sp = cfma(f.u[q], Cx<R>::make((R)pv.x, (R)pv.y), sp);
+      }
+    h = cadd(h, cmul(Cx<R>::make(f.ex, f.ey), sp));
+  }
+  if (p1 > p0 + 1) h = kb_pairs<R>(h, ((p0 + 1) << 8) | (p1 - p0 - 1), P, a, ik);
+  return h;
+}
+
 // wrap (periodic) or test (Dirichlet) a coordinate that may be up to 4 outside
 __device__ __forceinline__ int wrapc(int q, int n, int periodic, bool& ok) {
   if (periodic) {

@@ -179,6 +179,16 @@ __device__ __forceinline__ bool tma_body(const TmaMaps& maps, void* __restrict__
     else vsrc = (const R*)(a.vloc32 + (long)ispin * a.npts);
     R vl_n = active ? __ldg(vsrc + (long)zc0 * sz + pxy) : (R)0;
     int pm_n = (active && a.nlma > 0) ? __ldg(a.pmap + (long)zc0 * sz + pxy) : -1;
+    // pair form of the KB scatter: the first pair of the next plane's point
+    // is loaded at the end of each step, from pm_n (loaded at its start); in
+    // the modes whose registers have room for it (the inner FP64 terms and
+    // the FP32 terms; in the others it would spill)
+    constexpr bool AHEAD = (MODE == 2 || MODE == 3 || MODE >= 6);
+    const bool pairs = AHEAD && a.nlma > 0 && a.use_pairs;
+    const double2* pair_ph = pairs ? a.pair_ph + (a.phase_per_k ? (long)ik * a.npair : 0L) : nullptr;
+    Pair1<R> f1;
+    f1.lm = 0;
+    if (pairs) load_pair1<R>(f1, pm_n, a, pair_ph);
     // FP64 stencils: the window rotates through the registers -- in step j of
     // a group of nine, plane z - 4 + i sits in w[(j + i) % 9] (constant
     // indices, no moves); FP32 stencils (issue-bound, code-size sensitive)
@@ -242,7 +252,8 @@ __device__ __forceinline__ bool tma_body(const TmaMaps& maps, void* __restrict__
           h.y -= ww.x;
         }
         if (a.nlma > 0 && pm >= 0 && a.use_pairs) {
-          h = kb_pairs<R>(h, pm, ps_smem ? psm : a.proj + (long)o * a.nlma, a, ik);
+          if (AHEAD) h = kb_pairs_ahead<R>(h, pm, ps_smem ? psm : a.proj + (long)o * a.nlma, a, ik, f1);
+          else h = kb_pairs<R>(h, pm, ps_smem ? psm : a.proj + (long)o * a.nlma, a, ik);
         } else if (a.nlma > 0 && pm >= 0) {
           const double2* pj = ps_smem ? psm : a.proj + (long)o * a.nlma;
           const double2* zk = a.ent_zk + (a.phase_per_k ? (long)ik * a.nent : 0L);
@@ -289,6 +300,7 @@ __device__ __forceinline__ bool tma_body(const TmaMaps& maps, void* __restrict__
           const C2 tt = cadd(Cx<R>::make((R)dd.x, (R)dd.y), cmul(czc, h));
           acc[gi] = cadd(accr[ti], make_double2((double)tt.x, (double)tt.y));
         }
+        if (pairs && k + 1 < nsteps) load_pair1<R>(f1, pm_n, a, pair_ph);
       }
       // warp 0 waits for the next step's copies before the step barrier, so the
       // other warps find them complete at their own (first) try-wait and

@@ -13,7 +13,8 @@
 // points (padded to a multiple of 2), q the atom's (at most 4) projectors.
 // One CTA of 64 threads per (atom, 16-orbital tile, k-point): the sphere
 // values of its 16 orbitals are gathered from HBM by cp.async straight into
-// the A tile (16-byte copies, the complex value's two doubles side by side),
+// the A tile (16-byte copies, the complex value's two doubles side by side;
+// FP32 input: 8-byte copies, widened in place after the wait),
 // the B tile is built from the k-point's phases and uV, and each warp runs
 // the K/4 DMMA steps of one 8-orbital half.  Row strides of both tiles are
 // 12 modulo 16 doubles, so the fragment loads of a half-warp hit 16
@@ -35,6 +36,10 @@ constexpr int PT = 64;   // threads per CTA
 __device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc) {
   const uint32_t d = (uint32_t)__cvta_generic_to_shared(smem_dst);
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* smem_dst, const void* gsrc) {
+  const uint32_t d = (uint32_t)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(gsrc) : "memory");
 }
 __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
@@ -73,13 +78,10 @@ __global__ void __launch_bounds__(PT) k_project_dmma(const TIN* __restrict__ in,
     for (int r = 0; r < MT; ++r) {
       double* dst = As + r * stride + 2 * j;
       if (r < nrow) {
-        if (sizeof(TIN) == 16) {
-          cp_async16(dst, src + (long)r * a.npts);
-        } else {
-          const TIN v = __ldg(src + (long)r * a.npts);
-          dst[0] = (double)v.x;
-          dst[1] = (double)v.y;
-        }
+        // FP64: the value itself; FP32: its 8 bytes into the first slot,
+        // widened in place by the same thread after the wait below
+        if (sizeof(TIN) == 16) cp_async16(dst, src + (long)r * a.npts);
+        else cp_async8(dst, src + (long)r * a.npts);
       } else {
         dst[0] = 0.0;
         dst[1] = 0.0;
@@ -105,6 +107,15 @@ __global__ void __launch_bounds__(PT) k_project_dmma(const TIN* __restrict__ in,
     }
   }
   cp_async_wait_all();
+  if (sizeof(TIN) == 8) {  // each thread widens the FP32 values it copied
+    for (int j = t; j < m; j += PT)
+      for (int r = 0; r < nrow; ++r) {
+        double* dst = As + r * stride + 2 * j;
+        const float2 v = *reinterpret_cast<const float2*>(dst);
+        dst[0] = (double)v.x;
+        dst[1] = (double)v.y;
+      }
+  }
   __syncthreads();
   // each warp: rows 8 warp .. 8 warp + 7 of C over all k steps
   double d0 = 0.0, d1 = 0.0;

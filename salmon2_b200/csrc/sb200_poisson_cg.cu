@@ -548,10 +548,13 @@ __global__ void __launch_bounds__(PTP, 2) k_pcg_solve(PArgs a) {
   double* partA = a.part;
   double* partB = a.part + gridDim.x;
   const int nb = (int)gridDim.x;
-  // rows (y, z) of the grid go to warps in turn, the lanes of a warp along x:
+  // rows (y, z) of the grid: each block an even, contiguous share (its warps
+  // take the share's rows in turn, so neighbouring rows meet in one SM's L1
+  // and no SM carries more rows than another), the lanes of a warp along x;
   // 32-bit divisions by ny instead of three 64-bit divisions per point
   const int rows = a.ny * a.nz, lane = threadIdx.x & 31;
-  const int warp0 = (int)((blockIdx.x * PTP + threadIdx.x) >> 5), nwarps = nb * (PTP / 32);
+  const int r_end = (int)(((long)(blockIdx.x + 1) * rows) / nb);
+  const int warp0 = (int)(((long)blockIdx.x * rows) / nb) + (int)(threadIdx.x >> 5), nwarps = PTP / 32;
   unsigned int target = 0u;
   double sum1 = a.sc[SC_SUM1], ck = 0.0;
   double done = 0.0, iter = 0.0;
@@ -566,7 +569,7 @@ __global__ void __launch_bounds__(PTP, 2) k_pcg_solve(PArgs a) {
     // one loop over this lane's points: x steps by 32 along a row, then the
     // next row of the warp (a nested loop would let the compiler hoist the 50
     // neighbour addresses of a row into registers)
-    for (int r = warp0, x = lane; r < rows;) {
+    for (int r = warp0, x = lane; r < r_end;) {
       if (x < a.nx) {
         const long c = padi(a, x, r % a.ny, r / a.ny);
         const double lv = lap_at(a, c, pk_new);
@@ -585,7 +588,7 @@ __global__ void __launch_bounds__(PTP, 2) k_pcg_solve(PArgs a) {
     if (!grid_barrier(a, target)) return;
     const double ak = sum1 / grid_total(partA, nb, red) / a.hvol;
     s = 0.0;
-    for (int r = warp0, x = lane; r < rows;) {
+    for (int r = warp0, x = lane; r < r_end;) {
       if (x < a.nx) {
         const long c = padi(a, x, r % a.ny, r / a.ny), q = (long)r * a.nx + x;
         a.vh[q] = a.vh[q] + ak * pn[c];

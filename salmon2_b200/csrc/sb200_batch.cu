@@ -226,7 +226,7 @@ struct BCSys {
 };
 __global__ void __launch_bounds__(256) k_collapse_batch(const BCSys* __restrict__ sys, const long* __restrict__ first,
                                                         int nsys) {
-  const long item = blockIdx.x * 256L + threadIdx.x;
+  const long item = (blockIdx.x * 256L + threadIdx.x) >> 5;  // one warp per item (the solo kernel's order)
   if (item >= first[nsys]) return;
   const int s = find_sys(first, nsys, item);
   collapse_item(sys[s].part, sys[s].nblk, nullptr, 0, item - first[s], sys[s].out);
@@ -497,7 +497,8 @@ int launch_obs_final_batch(sb200_batch* b, int parity, int which) {
         b->d_osys, b->d_ofirst, b->d_opsi + (size_t)parity * b->nsys, b->nsys);
     SB_LAUNCH_CHECK("k_observables_batch");
   } else {
-    k_collapse_batch<<<(unsigned)((b->c_total + 255) / 256), 256, 0, b->stream>>>(b->d_csys, b->d_cfirst, b->nsys);
+    k_collapse_batch<<<(unsigned)((b->c_total * 32 + 255) / 256), 256, 0, b->stream>>>(b->d_csys, b->d_cfirst,
+                                                                                      b->nsys);
     SB_LAUNCH_CHECK("k_collapse_batch");
     k_finalize_batch<<<b->nsys, 256, 0, b->stream>>>(b->d_fin);
     SB_LAUNCH_CHECK("k_finalize_batch");

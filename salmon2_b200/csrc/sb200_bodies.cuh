@@ -326,20 +326,24 @@ __device__ __forceinline__ void finalize_body(const FinArgs& a) {
 // nonlocal-current pieces [norb][natom][3], blocks and atoms in ascending
 // order (the order the final reduction adds them): out [norb][OBS_NQ + 3].
 // Thread per (orbital, quantity).
+// One item (orbital o, quantity i) per warp: lane l sums the partials
+// l, l + 32, ... in order, then a butterfly over the warp (a fixed order; for
+// one or two partials the plain sum).  Called by all 32 lanes of the warp.
 __device__ __forceinline__ void collapse_item(const double* __restrict__ part, int nblk,
                                               const double* __restrict__ jw, int natom, long item,
                                               double* __restrict__ out) {
+  const int lane = threadIdx.x & 31;
   const long o = item / (OBS_NQ + 3);
   const int i = (int)(item % (OBS_NQ + 3));
   double s = 0.0;
   if (i < OBS_NQ) {
-#pragma unroll 4
-    for (int b = 0; b < nblk; ++b) s += part[(o * nblk + b) * OBS_NQ + i];
+    for (int b = lane; b < nblk; b += 32) s += part[(o * nblk + b) * OBS_NQ + i];
   } else if (jw != nullptr) {
-#pragma unroll 4
-    for (int at = 0; at < natom; ++at) s += jw[3 * (o * natom + at) + (i - OBS_NQ)];
+    for (int at = lane; at < natom; at += 32) s += jw[3 * (o * natom + at) + (i - OBS_NQ)];
   }
-  out[item] = s;
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+  if (lane == 0) out[item] = s;
 }
 
 }  // namespace body

@@ -445,7 +445,7 @@ __global__ void __launch_bounds__(256) k_finalize(FinArgs a) { finalize_body(a);
 __global__ void __launch_bounds__(256) k_collapse(const double* __restrict__ part, int nblk,
                                                   const double* __restrict__ jw, int natom, long nitems,
                                                   double* __restrict__ out) {
-  const long item = blockIdx.x * 256L + threadIdx.x;
+  const long item = (blockIdx.x * 256L + threadIdx.x) >> 5;  // one warp per item
   if (item < nitems) collapse_item(part, nblk, jw, natom, item, out);
 }
 
@@ -1355,11 +1355,11 @@ int launch_finalize(sb200_ctx* c, int itt, int nt, int trans_longi, double dt, i
   (void)nt;
   FinArgs a = make_fin_args(c, itt, trans_longi, dt, spin_filter, fused_obs);
   if (a.nblk > 1 || (a.jw != nullptr && a.jw_natom > 1)) {
-    // per-orbital sums first, in parallel (same order of additions), so the
-    // one-CTA final reduction reads one record per orbital
+    // per-orbital sums first, a warp per (orbital, quantity), so the one-CTA
+    // final reduction reads one record per orbital
     const long nitems = (long)c->orb.norb * (OBS_NQ + 3);
-    k_collapse<<<(unsigned)((nitems + 255) / 256), 256, 0, c->stream>>>(a.part, a.nblk, a.jw, a.jw_natom, nitems,
-                                                                        c->d_obs1);
+    k_collapse<<<(unsigned)((nitems * 32 + 255) / 256), 256, 0, c->stream>>>(a.part, a.nblk, a.jw, a.jw_natom,
+                                                                             nitems, c->d_obs1);
     SB_LAUNCH_CHECK("k_collapse");
     a.part = c->d_obs1;
     a.nblk = 1;

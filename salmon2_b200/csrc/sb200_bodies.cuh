@@ -174,9 +174,10 @@ __device__ __forceinline__ void obs_block(const double2* __restrict__ in, double
   for (int it = 0; it < OBS_PTS_PER_THREAD; ++it) {
     const long p = base + (long)it * OBS_THREADS + threadIdx.x;
     if (p >= a.npts) break;
-    const int x = (int)(p % a.nx);
-    const int y = (int)((p / a.nx) % a.ny);
-    const int z = (int)(p / ((long)a.nx * a.ny));
+    const int pi = (int)p;  // a point of one orbital's grid: 32-bit index arithmetic
+    const int x = pi % a.nx;
+    const int y = (pi / a.nx) % a.ny;
+    const int z = pi / (a.nx * a.ny);
     const double2 c = __ldg(src + p);
     const double r2 = c.x * c.x + c.y * c.y;
     q[0] += r2;

@@ -181,9 +181,9 @@ __device__ __forceinline__ bool tma_body(const TmaMaps& maps, void* __restrict__
     int pm_n = (active && a.nlma > 0) ? __ldg(a.pmap + (long)zc0 * sz + pxy) : -1;
     // pair form of the KB scatter: the first pair of the next plane's point
     // is loaded at the end of each step, from pm_n (loaded at its start); in
-    // the modes whose registers have room for it (the inner FP64 terms and
-    // the FP32 terms; in the others it would spill)
-    constexpr bool AHEAD = (MODE == 2 || MODE == 3 || MODE >= 6);
+    // the inner FP64 terms and the FP32 terms, and in the first FP64 term of
+    // periodic grids (where it spills a little but still gains; measured)
+    constexpr bool AHEAD = (MODE == 2 || MODE == 3 || MODE >= 6 || (MODE == 1 && PER));
     const bool pairs = AHEAD && a.nlma > 0 && a.use_pairs;
     const double2* pair_ph = pairs ? a.pair_ph + (a.phase_per_k ? (long)ik * a.npair : 0L) : nullptr;
     Pair1<R> f1;

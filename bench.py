@@ -635,7 +635,7 @@ def main():
     # previous one read back
     host_state = torch.from_numpy(np.ascontiguousarray(s.psi.ravel(order="F").view(np.float64))).pin_memory()
     host_out = torch.empty_like(host_state).pin_memory() if restart else host_state
-    if not restart:
+    if not restart and args.steps > 0:
         ctx.download(res["psi"], out=host_state)
     bytes_io = host_state.numel() * 8
 
